@@ -1,0 +1,11 @@
+"""B200-native depth-kernel stage of DAzi (surface-wave azimuthal anisotropy
+tomography): Rayleigh phase velocities and the dc/dVs and Gc/Gs sensitivity
+kernels, computed by hand-written sm_100a CUDA kernels behind a C-ABI
+(include/dazi_dk.h).  The Python side mirrors the reference's Fortran
+interfaces `depthkernel` and `depthkernelTI`.
+"""
+from .depthkernel import depthkernel, depthkernel_vpvsrho, DepthKernelError  # noqa: F401
+from ._lib import DaziError, FORM_PLAIN, FORM_ADJOINT  # noqa: F401
+
+__all__ = ["depthkernel", "depthkernel_vpvsrho", "DepthKernelError", "DaziError",
+           "FORM_PLAIN", "FORM_ADJOINT"]

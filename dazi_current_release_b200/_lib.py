@@ -1,0 +1,89 @@
+"""Loader of the in-tree CUDA library libdazi_dk.so (C-ABI, include/dazi_dk.h).
+
+The library must be built (python -m dazi_current_release_b200.build); there is
+no CPU fallback: a missing library or a machine without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+from . import build as _build
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_i32p = ctypes.POINTER(ctypes.c_int)
+_int = ctypes.c_int
+
+DAZI_OK = 0
+DAZI_WARN_NOROOT = 1
+DAZI_ERR_BADARG = -1
+DAZI_ERR_LIMITS = -2
+DAZI_ERR_CUDA = -3
+DAZI_ERR_TIMEOUT = -4
+DAZI_ERR_NOMEM = -5
+DAZI_ERR_NODEVICE = -6
+FORM_PLAIN = 0
+FORM_ADJOINT = 1
+
+# every symbol include/dazi_dk.h declares
+EXPORTS = (
+    "dazi_dk_iso", "dazi_dk_iso_vpvsrho", "dazi_dk_last_status", "dazi_dk_iso_dev",
+    "dazi_dk_last_error", "dazi_dk_version", "dazi_dk_finalize",
+)
+
+
+class DaziError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"dazi_dk error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def lib_path() -> str:
+    return _build.LIB
+
+
+def load(build_if_missing: bool = True):
+    """Load libdazi_dk.so and declare the C signatures."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = _build.LIB
+    if not os.path.exists(path):
+        if not build_if_missing:
+            raise FileNotFoundError(f"{path} is not built")
+        _build.build()
+    L = ctypes.CDLL(path)
+    ip = ctypes.POINTER(ctypes.c_int)
+    fp = _f32p
+    L.dazi_dk_iso.argtypes = [ip, ip, ip, fp, _f64p, _f64p, _f64p, _f64p, ip, ip, ip, _f64p, fp,
+                              fp, _int, _int, _int]
+    L.dazi_dk_iso.restype = _int
+    L.dazi_dk_iso_vpvsrho.argtypes = [ip, ip, ip, fp, fp, fp, _f64p, _f64p, _f64p, _f64p, ip, ip,
+                                      ip, _f64p, fp, fp, _int, _int, _int]
+    L.dazi_dk_iso_vpvsrho.restype = _int
+    L.dazi_dk_last_status.argtypes = [_i32p, ctypes.c_longlong]
+    L.dazi_dk_last_status.restype = _int
+    vp_ = ctypes.c_void_p
+    L.dazi_dk_iso_dev.argtypes = [_int, _int, _int, vp_, vp_, vp_, vp_, vp_, vp_, vp_, _int, vp_,
+                                  vp_, ctypes.c_float, _int, _int, _int, vp_, vp_]
+    L.dazi_dk_iso_dev.restype = _int
+    L.dazi_dk_last_error.argtypes = []
+    L.dazi_dk_last_error.restype = ctypes.c_char_p
+    L.dazi_dk_version.argtypes = []
+    L.dazi_dk_version.restype = _int
+    L.dazi_dk_finalize.argtypes = []
+    L.dazi_dk_finalize.restype = None
+    _lib = L
+    return L
+
+
+def check(code: int) -> int:
+    """Raise DaziError for negative return codes; pass 0/1 through."""
+    if code < 0:
+        msg = load().dazi_dk_last_error().decode(errors="replace")
+        raise DaziError(code, msg)
+    return code

@@ -1,0 +1,378 @@
+// C-ABI of libdazi_dk.so: argument checks, device buffers, launches.
+//
+// The host entries mirror the reference's Fortran interfaces
+// (code/src_inv_iso_joint/CalSurfG.f90:1-15 depthkernel,
+//  code/src_inv_iso_joint/depthkernelTI.f90:2-14 depthkernelTI) and the
+// column-range contract of the tile worker
+// (code/depthkernel_lab/depthkernel_ti_worker.f90:19-38).
+#include <cuda_runtime.h>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "../../include/dazi_dk.h"
+#include "dk_kernels.cuh"
+
+using namespace dk;
+
+namespace {
+
+char g_err[512] = "no error";
+
+void set_err(const char* fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+}
+
+#define CK(call)                                                                   \
+    do {                                                                           \
+        cudaError_t e_ = (call);                                                   \
+        if (e_ != cudaSuccess) {                                                   \
+            set_err("CUDA error %s at %s:%d (%s)", cudaGetErrorString(e_),        \
+                    __FILE__, __LINE__, #call);                                    \
+            return DAZI_ERR_CUDA;                                                  \
+        }                                                                          \
+    } while (0)
+
+// Grow-only device buffer.
+struct DBuf {
+    void* p = nullptr;
+    size_t n = 0;
+    int ensure(size_t bytes)
+    {
+        if (bytes <= n) return 0;
+        if (p) cudaFree(p);
+        p = nullptr; n = 0;
+        if (cudaMalloc(&p, bytes) != cudaSuccess) {
+            cudaGetLastError();
+            set_err("device allocation of %zu bytes failed", bytes);
+            return DAZI_ERR_NOMEM;
+        }
+        n = bytes;
+        return 0;
+    }
+    void release() { if (p) cudaFree(p); p = nullptr; n = 0; }
+    template <class T> T* as() const { return reinterpret_cast<T*>(p); }
+};
+
+struct Context {
+    bool ready = false;
+    int device = -1;
+    cudaStream_t stream = nullptr;
+    // host-entry staging
+    DBuf vel, vp, rho, per, depz, pv, svs, svp, srh, status;
+    // work buffers
+    DBuf geo, cscratch, layers, croot;
+    // geometry cache key
+    std::vector<float> geo_depz;
+    float geo_minthk = -1.f;
+    int geo_rmax = 0;
+    std::vector<int> last_status;
+    long long last_ncol = 0;
+};
+
+Context g_ctx;
+std::mutex g_mu;
+
+int ensure_context()
+{
+    if (g_ctx.ready) return 0;
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        set_err("no CUDA device visible (%s)", cudaGetErrorString(e));
+        return DAZI_ERR_NODEVICE;
+    }
+    CK(cudaGetDevice(&g_ctx.device));
+    CK(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
+    g_ctx.ready = true;
+    return 0;
+}
+
+// Geometry of the depth grid on the device (cached by content).
+int prepare_geometry(const float* h_depz, int nz, float minthk, cudaStream_t st)
+{
+    if (g_ctx.geo.p && g_ctx.geo_minthk == minthk && (int)g_ctx.geo_depz.size() == nz &&
+        std::memcmp(g_ctx.geo_depz.data(), h_depz, sizeof(float) * nz) == 0)
+        return 0;
+    int r;
+    if ((r = g_ctx.geo.ensure(sizeof(Geometry)))) return r;
+    if ((r = g_ctx.depz.ensure(sizeof(float) * nz))) return r;
+    CK(cudaMemcpyAsync(g_ctx.depz.p, h_depz, sizeof(float) * nz, cudaMemcpyHostToDevice, st));
+    geometry_kernel<<<1, 1, 0, st>>>(g_ctx.depz.as<float>(), nz, minthk, g_ctx.geo.as<Geometry>());
+    CK(cudaGetLastError());
+    int rmax = 0;
+    CK(cudaMemcpyAsync(&rmax, &g_ctx.geo.as<Geometry>()->rmax, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (rmax <= 0) {
+        g_ctx.geo_minthk = -1.f;
+        set_err("refined layer count exceeds %d (nz=%d, minthk=%g)", NL, nz, (double)minthk);
+        return DAZI_ERR_LIMITS;
+    }
+    g_ctx.geo_depz.assign(h_depz, h_depz + nz);
+    g_ctx.geo_minthk = minthk;
+    g_ctx.geo_rmax = rmax;
+    return 0;
+}
+
+int check_grid(int nx, int ny, int nz, int kmax, const float* depz, float minthk,
+               long long col_start, long long col_count)
+{
+    if (nx < 1 || ny < 1) { set_err("nx, ny must be >= 1"); return DAZI_ERR_BADARG; }
+    if (nz < 2 || nz > NZMAX) { set_err("nz=%d outside [2, %d]", nz, NZMAX); return DAZI_ERR_LIMITS; }
+    if (kmax < 1 || kmax > NP) { set_err("kmaxRc=%d outside [1, %d]", kmax, NP); return DAZI_ERR_LIMITS; }
+    if (!(minthk > 0.f) || !std::isfinite(minthk)) { set_err("minthk must be > 0"); return DAZI_ERR_BADARG; }
+    for (int i = 0; i < nz; ++i)
+        if (!std::isfinite(depz[i]) || (i > 0 && !(depz[i] > depz[i - 1]))) {
+            set_err("depz must be finite and strictly increasing (node %d)", i + 1);
+            return DAZI_ERR_BADARG;
+        }
+    const long long ncol = (long long)nx * ny;
+    if (col_start < 1 || col_count < 0 || col_start - 1 + col_count > ncol) {
+        set_err("column range [%lld, %lld) outside 1..%lld", col_start, col_start + col_count, ncol);
+        return DAZI_ERR_BADARG;
+    }
+    return 0;
+}
+
+int check_periods(const double* t, int kmax)
+{
+    for (int k = 0; k < kmax; ++k)
+        if (!(t[k] > 0.0) || !std::isfinite(t[k])) {
+            set_err("period %d is not a positive finite number", k + 1);
+            return DAZI_ERR_BADARG;
+        }
+    return 0;
+}
+
+// Core of the iso stage on device pointers (stream-ordered, no sync).
+int iso_device(int nx, int ny, int nz, const float* vel, const float* vp, const float* rho,
+               double* pv, double* svs, double* svp, double* srh, int kmax, const double* per,
+               long long col_start, long long col_count, int form, int* status, cudaStream_t st)
+{
+    const long long ncol = (long long)nx * ny;
+    if (col_count == 0) return 0;
+    const Geometry* geo = g_ctx.geo.as<Geometry>();
+    const double tol = 1.0e-6;   // surfdisp96.f:608
+    int r;
+    if (svs && form == DAZI_FORM_PLAIN) {
+        const int nmod = 1 + 6 * nz;
+        const size_t per_col = sizeof(float) * (size_t)nmod * kmax;
+        const long long cap = 512ll << 20;
+        long long tile = (long long)(cap / per_col);
+        if (tile < 1) tile = 1;
+        if (tile > col_count) tile = col_count;
+        if ((r = g_ctx.cscratch.ensure(per_col * tile))) return r;
+        int threads = ((nmod + 31) / 32) * 32;
+        if (threads > 256) threads = 256;
+        const size_t smem = fd_smem_bytes();
+        for (long long c0 = 0; c0 < col_count; c0 += tile) {
+            const long long n = (col_count - c0 < tile) ? col_count - c0 : tile;
+            FdArgs a;
+            a.geo = geo; a.nz = nz; a.kmax = kmax; a.ncol = ncol;
+            a.col0 = col_start - 1 + c0;
+            a.vel = vel; a.vp = vp; a.rho = rho; a.periods = per;
+            a.pv = pv; a.sen_vs = svs; a.sen_vp = svp; a.sen_rho = srh;
+            a.status = status; a.cscratch = g_ctx.cscratch.as<float>();
+            a.dln = 0.01f; a.tol = tol;
+            fd_column_kernel<<<(unsigned)n, threads, smem, st>>>(a);
+            CK(cudaGetLastError());
+        }
+        return 0;
+    }
+    if (svs && form != DAZI_FORM_PLAIN) {
+        set_err("form %d is not available in this build", form);
+        return DAZI_ERR_BADARG;
+    }
+    // pv only: one thread per column
+    if ((r = g_ctx.layers.ensure(sizeof(float4) * NL * (size_t)col_count))) return r;
+    BuildArgs b;
+    b.geo = geo; b.nz = nz; b.ncol = ncol; b.col0 = col_start - 1; b.ncols = col_count;
+    b.vel = vel; b.vp = vp; b.rho = rho; b.layers = g_ctx.layers.as<float4>();
+    const int bt = 128;
+    const unsigned nb = (unsigned)((col_count + bt - 1) / bt);
+    build_layers_kernel<<<nb, bt, 0, st>>>(b);
+    CK(cudaGetLastError());
+    RootArgs a;
+    a.geo = geo; a.kmax = kmax; a.ncol = ncol; a.col0 = col_start - 1; a.ncols = col_count;
+    a.layers = g_ctx.layers.as<float4>(); a.periods = per; a.tol = tol;
+    a.pv = pv; a.croot = nullptr; a.evals = nullptr; a.status = status;
+    root_kernel<<<nb, bt, 0, st>>>(a);
+    CK(cudaGetLastError());
+    return 0;
+}
+
+int iso_host(const int* pnx, const int* pny, const int* pnz, const float* vel, const float* vp,
+             const float* rho, double* pv, double* svs, double* svp, double* srh,
+             const int* iwave, const int* igr, const int* pkmax, const double* tRc,
+             const float* depz, const float* pminthk, int col_start, int col_count, int form)
+{
+    if (!pnx || !pny || !pnz || !vel || !pv || !iwave || !igr || !pkmax || !tRc || !depz || !pminthk) {
+        set_err("null argument");
+        return DAZI_ERR_BADARG;
+    }
+    if (*iwave != 2 || *igr != 0) {
+        set_err("only Rayleigh (iwave=2) phase velocity (igr=0) is supported (got %d, %d)", *iwave, *igr);
+        return DAZI_ERR_BADARG;
+    }
+    if ((svs == nullptr) != (svp == nullptr) || (svs == nullptr) != (srh == nullptr)) {
+        set_err("sen_vsRc, sen_vpRc, sen_rhoRc must be all set or all NULL");
+        return DAZI_ERR_BADARG;
+    }
+    if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
+    if (form != DAZI_FORM_PLAIN && form != DAZI_FORM_ADJOINT) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    const int nx = *pnx, ny = *pny, nz = *pnz, kmax = *pkmax;
+    const float minthk = *pminthk;
+    int r;
+    if ((r = check_grid(nx, ny, nz, kmax, depz, minthk, col_start, col_count))) return r;
+    if ((r = check_periods(tRc, kmax))) return r;
+    const long long ncol = (long long)nx * ny;
+    const size_t nvel = (size_t)ncol * nz;
+    for (long long c = col_start - 1; c < col_start - 1 + col_count; ++c)
+        for (int i = 0; i < nz; ++i) {
+            const float v = vel[c + ncol * i];
+            if (!(v > 0.f) || !std::isfinite(v)) {
+                set_err("vel(column %lld, node %d) = %g is not a positive finite velocity", c + 1, i + 1, (double)v);
+                return DAZI_ERR_BADARG;
+            }
+            if (vp && (!(vp[c + ncol * i] > 0.f) || !(rho[c + ncol * i] > 0.f))) {
+                set_err("vp/rho(column %lld, node %d) not positive", c + 1, i + 1);
+                return DAZI_ERR_BADARG;
+            }
+        }
+    std::lock_guard<std::mutex> lk(g_mu);
+    if ((r = ensure_context())) return r;
+    cudaStream_t st = g_ctx.stream;
+    if ((r = prepare_geometry(depz, nz, minthk, st))) return r;
+    const bool kern = svs != nullptr;
+    const size_t npv = (size_t)ncol * kmax, nsen = npv * nz;
+    if ((r = g_ctx.vel.ensure(sizeof(float) * nvel))) return r;
+    if (vp && ((r = g_ctx.vp.ensure(sizeof(float) * nvel)) || (r = g_ctx.rho.ensure(sizeof(float) * nvel)))) return r;
+    if ((r = g_ctx.per.ensure(sizeof(double) * kmax))) return r;
+    if ((r = g_ctx.pv.ensure(sizeof(double) * npv))) return r;
+    if ((r = g_ctx.status.ensure(sizeof(int) * ncol))) return r;
+    if (kern && ((r = g_ctx.svs.ensure(sizeof(double) * nsen)) || (r = g_ctx.svp.ensure(sizeof(double) * nsen)) ||
+                 (r = g_ctx.srh.ensure(sizeof(double) * nsen))))
+        return r;
+    CK(cudaMemcpyAsync(g_ctx.vel.p, vel, sizeof(float) * nvel, cudaMemcpyHostToDevice, st));
+    if (vp) {
+        CK(cudaMemcpyAsync(g_ctx.vp.p, vp, sizeof(float) * nvel, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(g_ctx.rho.p, rho, sizeof(float) * nvel, cudaMemcpyHostToDevice, st));
+    }
+    CK(cudaMemcpyAsync(g_ctx.per.p, tRc, sizeof(double) * kmax, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(g_ctx.status.p, 0, sizeof(int) * ncol, st));
+    r = iso_device(nx, ny, nz, g_ctx.vel.as<float>(), vp ? g_ctx.vp.as<float>() : nullptr,
+                   vp ? g_ctx.rho.as<float>() : nullptr, g_ctx.pv.as<double>(),
+                   kern ? g_ctx.svs.as<double>() : nullptr, kern ? g_ctx.svp.as<double>() : nullptr,
+                   kern ? g_ctx.srh.as<double>() : nullptr, kmax, g_ctx.per.as<double>(),
+                   col_start, col_count, form, g_ctx.status.as<int>(), st);
+    if (r) return r;
+    // Copy back only the written columns: pvRc(:, k) and sen(:, k, i) hold
+    // the range contiguously in each (k[, i]) slab.
+    const size_t c0 = (size_t)(col_start - 1), cn = (size_t)col_count;
+    CK(cudaMemcpy2DAsync(pv + c0, sizeof(double) * ncol, g_ctx.pv.as<double>() + c0, sizeof(double) * ncol,
+                         sizeof(double) * cn, kmax, cudaMemcpyDeviceToHost, st));
+    if (kern) {
+        double* hs[3] = {svs, svp, srh};
+        DBuf* ds[3] = {&g_ctx.svs, &g_ctx.svp, &g_ctx.srh};
+        for (int q = 0; q < 3; ++q)
+            CK(cudaMemcpy2DAsync(hs[q] + c0, sizeof(double) * ncol, ds[q]->as<double>() + c0,
+                                 sizeof(double) * ncol, sizeof(double) * cn, (size_t)kmax * nz,
+                                 cudaMemcpyDeviceToHost, st));
+    }
+    g_ctx.last_status.resize(ncol);
+    CK(cudaMemcpyAsync(g_ctx.last_status.data(), g_ctx.status.p, sizeof(int) * ncol, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    g_ctx.last_ncol = ncol;
+    for (long long c = col_start - 1; c < col_start - 1 + col_count; ++c)
+        if (g_ctx.last_status[c] != 0) return DAZI_WARN_NOROOT;
+    return DAZI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dazi_dk_iso(const int* nx, const int* ny, const int* nz, const float* vel, double* pvRc,
+                double* sen_vsRc, double* sen_vpRc, double* sen_rhoRc, const int* iwave,
+                const int* igr, const int* kmaxRc, const double* tRc, const float* depz,
+                const float* minthk, int col_start, int col_count, int form)
+{
+    return iso_host(nx, ny, nz, vel, nullptr, nullptr, pvRc, sen_vsRc, sen_vpRc, sen_rhoRc, iwave,
+                    igr, kmaxRc, tRc, depz, minthk, col_start, col_count, form);
+}
+
+int dazi_dk_iso_vpvsrho(const int* nx, const int* ny, const int* nz, const float* vel,
+                        const float* vp, const float* rho, double* pvRc, double* sen_vsRc,
+                        double* sen_vpRc, double* sen_rhoRc, const int* iwave, const int* igr,
+                        const int* kmaxRc, const double* tRc, const float* depz,
+                        const float* minthk, int col_start, int col_count, int form)
+{
+    if (!vp || !rho) { set_err("vp and rho are required"); return DAZI_ERR_BADARG; }
+    return iso_host(nx, ny, nz, vel, vp, rho, pvRc, sen_vsRc, sen_vpRc, sen_rhoRc, iwave, igr,
+                    kmaxRc, tRc, depz, minthk, col_start, col_count, form);
+}
+
+int dazi_dk_last_status(int* status, long long n)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (g_ctx.last_status.empty() || !status) { set_err("no status available"); return DAZI_ERR_BADARG; }
+    const long long m = n < (long long)g_ctx.last_status.size() ? n : (long long)g_ctx.last_status.size();
+    std::memcpy(status, g_ctx.last_status.data(), sizeof(int) * (size_t)m);
+    return 0;
+}
+
+int dazi_dk_iso_dev(int nx, int ny, int nz, const float* vel, const float* vp, const float* rho,
+                    double* pvRc, double* sen_vsRc, double* sen_vpRc, double* sen_rhoRc, int kmaxRc,
+                    const double* tRc, const float* depz, float minthk, int col_start, int col_count,
+                    int form, int* status, void* stream)
+{
+    if (!vel || !pvRc || !tRc || !depz) { set_err("null argument"); return DAZI_ERR_BADARG; }
+    if ((sen_vsRc == nullptr) != (sen_vpRc == nullptr) || (sen_vsRc == nullptr) != (sen_rhoRc == nullptr)) {
+        set_err("sen_* must be all set or all NULL");
+        return DAZI_ERR_BADARG;
+    }
+    if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
+    if (form != DAZI_FORM_PLAIN && form != DAZI_FORM_ADJOINT) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    if (nz < 2 || nz > NZMAX) { set_err("nz=%d outside [2, %d]", nz, NZMAX); return DAZI_ERR_LIMITS; }
+    if (kmaxRc < 1 || kmaxRc > NP) { set_err("kmaxRc=%d outside [1, %d]", kmaxRc, NP); return DAZI_ERR_LIMITS; }
+    std::lock_guard<std::mutex> lk(g_mu);
+    int r;
+    if ((r = ensure_context())) return r;
+    cudaStream_t st = stream ? (cudaStream_t)stream : g_ctx.stream;
+    std::vector<float> hd(nz);
+    std::vector<double> ht(kmaxRc);
+    CK(cudaMemcpyAsync(hd.data(), depz, sizeof(float) * nz, cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(ht.data(), tRc, sizeof(double) * kmaxRc, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if ((r = check_grid(nx, ny, nz, kmaxRc, hd.data(), minthk, col_start, col_count))) return r;
+    if ((r = check_periods(ht.data(), kmaxRc))) return r;
+    if ((r = prepare_geometry(hd.data(), nz, minthk, st))) return r;
+    return iso_device(nx, ny, nz, vel, vp, rho, pvRc, sen_vsRc, sen_vpRc, sen_rhoRc, kmaxRc, tRc,
+                      col_start, col_count, form, status, st);
+}
+
+const char* dazi_dk_last_error(void) { return g_err; }
+
+int dazi_dk_version(void) { return 100; }
+
+void dazi_dk_finalize(void)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_ctx.ready) return;
+    DBuf* all[] = {&g_ctx.vel, &g_ctx.vp, &g_ctx.rho, &g_ctx.per, &g_ctx.depz, &g_ctx.pv,
+                   &g_ctx.svs, &g_ctx.svp, &g_ctx.srh, &g_ctx.status, &g_ctx.geo,
+                   &g_ctx.cscratch, &g_ctx.layers, &g_ctx.croot};
+    for (DBuf* b : all) b->release();
+    if (g_ctx.stream) cudaStreamDestroy(g_ctx.stream);
+    g_ctx = Context();
+}
+
+}  // extern "C"

@@ -1,0 +1,56 @@
+// Kernel argument blocks and launch entry points shared by the C-ABI layer.
+#pragma once
+#include <cuda_runtime.h>
+#include "dk_model.cuh"
+
+namespace dk {
+
+struct FdArgs {
+    const Geometry* geo;
+    int nz, kmax;
+    long long ncol;      // nx*ny (column stride of the Fortran arrays)
+    long long col0;      // first column (0-based) of this launch
+    const float* vel;    // (nx, ny, nz) Fortran order
+    const float* vp;     // optional explicit Vp (same layout) or nullptr
+    const float* rho;    // optional explicit rho or nullptr
+    const double* periods;
+    double* pv;          // (ncol, K)
+    double* sen_vs;      // (ncol, K, nz) or nullptr
+    double* sen_vp;
+    double* sen_rho;
+    int* status;         // (ncol) first failing period (1-based) or 0
+    float* cscratch;     // [columns in launch][1 + 6 nz][K]
+    float dln;
+    double tol;
+};
+
+struct BuildArgs {
+    const Geometry* geo;
+    int nz;
+    long long ncol, col0, ncols;
+    const float* vel;
+    const float* vp;
+    const float* rho;
+    float4* layers;      // [ncols][NL] flattened (d, a, b, rho)
+};
+
+struct RootArgs {
+    const Geometry* geo;
+    int kmax;
+    long long ncol, col0, ncols;
+    const float4* layers;
+    const double* periods;
+    double tol;
+    double* pv;          // (ncol, K) FP32-valued like the reference
+    double* croot;       // [ncols][K] FP64 roots, or nullptr
+    int* evals;          // (ncol, K) secular evaluations, or nullptr
+    int* status;
+};
+
+__global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);
+__global__ void fd_column_kernel(FdArgs a);
+__global__ void build_layers_kernel(BuildArgs a);
+__global__ void root_kernel(RootArgs a);
+size_t fd_smem_bytes();
+
+}  // namespace dk

@@ -1,0 +1,106 @@
+/*
+ * dazi_dk.h — C-ABI of the B200 depth-kernel library (libdazi_dk.so).
+ *
+ * Drop-in replacement for DAzi's per-column dispersion and depth-kernel
+ * stage.  All arrays use the reference's Fortran layouts:
+ *   vel, vp, rho   (nx, ny, nz)            real*4, column-major
+ *   pvRc           (nx*ny, kmaxRc)         real*8
+ *   sen_*Rc        (nx*ny, kmaxRc, nz)     real*8
+ *   Lsen_Gsc       (nx*ny, kmaxRc, nz-1)   real*4
+ *   tRc            (kmaxRc)                real*8, ascending periods (s)
+ *   depz           (nz)                    real*4, node depths (km)
+ * Column index post = ii + (jj-1)*nx (1-based), as in the reference.
+ * Scalars that the reference passes by reference stay pointers so the
+ * Fortran side can bind them without the VALUE attribute; the column range
+ * and the form selector are passed by value.
+ *
+ * Only Rayleigh (iwave = 2) phase velocity (igr = 0) is accepted, the only
+ * combination DAzi calls (CalSurfG_parallel.f90:1967-1976); other values
+ * return DAZI_ERR_BADARG.
+ *
+ * Limits (the reference's compiled limits, surfdisp96.f:57-59):
+ *   nz <= 200, kmaxRc <= 160, refined layers <= 200.
+ *
+ * Errors: 0 on success; DAZI_WARN_NOROOT (> 0) when at least one column had
+ * a period without a fundamental-mode root — that period and every later one
+ * of the column are zero in pvRc and in the kernels, as surfdisp96.f:1700-1770
+ * leaves them; negative codes are errors and leave the outputs unspecified.
+ * The library never exits or aborts; device code never traps.
+ *
+ * Threading: one host thread at a time (the reference calls the stage from
+ * one thread outside its OpenMP regions, CalSurfG_parallel.f90:1967-1976).
+ * The library owns its device buffers and stream; dazi_dk_finalize() frees
+ * them.
+ */
+#ifndef DAZI_DK_H
+#define DAZI_DK_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DAZI_OK            0
+#define DAZI_WARN_NOROOT   1
+#define DAZI_ERR_BADARG   -1
+#define DAZI_ERR_LIMITS   -2
+#define DAZI_ERR_CUDA     -3
+#define DAZI_ERR_TIMEOUT  -4
+#define DAZI_ERR_NOMEM    -5
+#define DAZI_ERR_NODEVICE -6
+
+/* form selector */
+#define DAZI_FORM_PLAIN    0   /* perturb-and-recompute, as the reference */
+#define DAZI_FORM_ADJOINT  1   /* implicit differentiation of the root     */
+
+/* Replaces depthkernel() of code/src_inv_iso_joint/CalSurfG.f90:1-15
+ * (default_fortran_fd backend, CalSurfG.f90:86-107), for the 1-based column
+ * range [col_start, col_start + col_count).  Writes pvRc and the three
+ * kernels of those columns.  sen_* may all be NULL to compute pvRc only
+ * (depthkernel_column_phase_fd, DepthKernel1D.f90:1-23). */
+int dazi_dk_iso(const int *nx, const int *ny, const int *nz, const float *vel,
+                double *pvRc, double *sen_vsRc, double *sen_vpRc,
+                double *sen_rhoRc, const int *iwave, const int *igr,
+                const int *kmaxRc, const double *tRc, const float *depz,
+                const float *minthk, int col_start, int col_count, int form);
+
+/* As dazi_dk_iso with explicit Vp and rho arrays in place of the Brocher
+ * relations (depthkernel_empirical_vp_rho, DepthKernel1D.f90:187-200);
+ * the finite differences still perturb Vs, Vp and rho independently. */
+int dazi_dk_iso_vpvsrho(const int *nx, const int *ny, const int *nz,
+                        const float *vel, const float *vp, const float *rho,
+                        double *pvRc, double *sen_vsRc, double *sen_vpRc,
+                        double *sen_rhoRc, const int *iwave, const int *igr,
+                        const int *kmaxRc, const double *tRc,
+                        const float *depz, const float *minthk,
+                        int col_start, int col_count, int form);
+
+/* Per-column status of the last call: first period (1-based) without a root,
+ * 0 when all periods have one.  status has nx*ny entries; only the columns
+ * of the last call's range are written.  Returns 0, or DAZI_ERR_BADARG if no
+ * call was made yet. */
+int dazi_dk_last_status(int *status, long long n);
+
+/* Device-pointer entry of the iso stage for callers that already hold the
+ * data in HBM (the PyTorch binding).  All array pointers are device
+ * pointers; vp/rho may be NULL (Brocher); sen_* may be NULL; status (nx*ny
+ * ints, device) may be NULL.  stream is a cudaStream_t (NULL = default). */
+int dazi_dk_iso_dev(int nx, int ny, int nz, const float *vel, const float *vp,
+                    const float *rho, double *pvRc, double *sen_vsRc,
+                    double *sen_vpRc, double *sen_rhoRc, int kmaxRc,
+                    const double *tRc, const float *depz, float minthk,
+                    int col_start, int col_count, int form, int *status,
+                    void *stream);
+
+/* Message of the last error (static storage, never NULL). */
+const char *dazi_dk_last_error(void);
+
+/* Library version as 10000*major + 100*minor + patch. */
+int dazi_dk_version(void);
+
+/* Releases every device buffer and stream the library created. */
+void dazi_dk_finalize(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DAZI_DK_H */

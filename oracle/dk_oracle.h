@@ -1,0 +1,37 @@
+/* CPU oracle (test infrastructure only): C restatement of the reference
+ * depth-kernel stage.  See dk_oracle.c and tregn_oracle.c for citations. */
+#ifndef DK_ORACLE_H
+#define DK_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+void or_brocher(int nz, const float *vs, float *vp, float *rho);
+int or_refine(float minthk0, int nz, const float *dep, const float *vp,
+              const float *vs, const float *rho, float *rthk, float *rvp,
+              float *rvs, float *rrho, int *nsublay);
+int or_surfdisp96(const float *thkm, const float *vpm, const float *vsm,
+                  const float *rhom, int nlayer, int iflsph, int iwave,
+                  int mode, int igr, int kmax, const double *t, double *cg);
+int or_surfdisp96_ex(const float *thkm, const float *vpm, const float *vsm,
+                     const float *rhom, int nlayer, int iflsph, int iwave,
+                     int mode, int igr, int kmax, const double *t, double *cg,
+                     double tol, int round_f32, int *evals_per_period);
+int or_column_fd(int nz, const float *vs, const float *vp, const float *rho,
+                 int kmax, const double *periods, int iwave, int igr,
+                 const float *depz, float minthk, float dlnvs, float dlnvp,
+                 float dlnrho, double tol, int round_f32, double *pv,
+                 double *sen_vs, double *sen_vp, double *sen_rho, long *evals);
+int or_depthkernel(int nx, int ny, int nz, const float *vel,
+                   const float *vp_in, const float *rho_in, double *pvRc,
+                   double *sen_vs, double *sen_vp, double *sen_rho, int iwave,
+                   int igr, int kmax, const double *tRc, const float *depz,
+                   float minthk, int col_start, int col_count, int nthreads,
+                   double tol, int round_f32, int *status_out, long *evals_out);
+int or_phase(int nx, int ny, int nz, const float *vel, const float *vp_in,
+             const float *rho_in, double *pvRc, int iwave, int igr, int kmax,
+             const double *tRc, const float *depz, float minthk, int nthreads,
+             double tol, int round_f32, int *evals_cp, int *status_out);
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,192 @@
+"""ctypes front end of the CPU oracle (test infrastructure only).
+
+The oracle restates the reference Fortran depth-kernel stage in C
+(oracle/dk_oracle.c, oracle/tregn_oracle.c).  Only the tests, the smoke check
+and bench.py's CPU-baseline leg import this module, and only as the checker or
+the timed CPU baseline; the shipped library never calls it.
+
+Array conventions follow the reference Fortran interfaces
+(code/src_inv_iso_joint/CalSurfG.f90:1-15 and depthkernelTI.f90:2-14):
+``vel`` is (nx, ny, nz) in Fortran order, outputs are (nx*ny, kmax[, nz]) in
+Fortran order.  numpy arrays passed here use ``order="F"``.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "liboracle_dk.so")
+_lib = None
+
+_f32p = ctypes.POINTER(ctypes.c_float)
+_f64p = ctypes.POINTER(ctypes.c_double)
+_i32p = ctypes.POINTER(ctypes.c_int)
+_i64p = ctypes.POINTER(ctypes.c_long)
+
+
+def build() -> str:
+    """Compile the oracle with its Makefile (gcc, no GPU needed)."""
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+    return _LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        L = ctypes.CDLL(_LIB_PATH)
+        L.or_brocher.argtypes = [ctypes.c_int, _f32p, _f32p, _f32p]
+        L.or_brocher.restype = None
+        L.or_refine.argtypes = [ctypes.c_float, ctypes.c_int, _f32p, _f32p, _f32p, _f32p,
+                                _f32p, _f32p, _f32p, _f32p, _i32p]
+        L.or_refine.restype = ctypes.c_int
+        L.or_surfdisp96_ex.argtypes = [_f32p, _f32p, _f32p, _f32p, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                       _f64p, _f64p, ctypes.c_double, ctypes.c_int, _i32p]
+        L.or_surfdisp96_ex.restype = ctypes.c_int
+        L.or_depthkernel.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p,
+                                     _f64p, _f64p, _f64p, _f64p, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_int, _f64p, _f32p, ctypes.c_float, ctypes.c_int,
+                                     ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                                     _i32p, _i64p]
+        L.or_depthkernel.restype = ctypes.c_int
+        L.or_phase.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p,
+                               _f64p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f64p, _f32p,
+                               ctypes.c_float, ctypes.c_int, ctypes.c_double, ctypes.c_int,
+                               _i32p, _i32p]
+        L.or_phase.restype = ctypes.c_int
+        if hasattr(L, "or_depthkernelTI"):
+            L.or_depthkernelTI.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p,
+                                           _f32p, _f64p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                           _f64p, _f32p, ctypes.c_float, _f32p, ctypes.c_int,
+                                           ctypes.c_int, ctypes.c_int, _i32p]
+            L.or_depthkernelTI.restype = ctypes.c_int
+            L.or_tregn96.argtypes = [ctypes.c_int, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
+                                     _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
+                                     ctypes.c_int, _f32p, _f32p, _f32p, _f32p, _f32p]
+            L.or_tregn96.restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def _p(a, ct):
+    return None if a is None else a.ctypes.data_as(ct)
+
+
+def brocher(vs):
+    vs = np.ascontiguousarray(vs, dtype=np.float32)
+    vp = np.empty_like(vs)
+    rho = np.empty_like(vs)
+    lib().or_brocher(vs.size, _p(vs, _f32p), _p(vp, _f32p), _p(rho, _f32p))
+    return vp, rho
+
+
+def refine(minthk, dep, vp, vs, rho):
+    """Grid-to-layer refinement; returns (rthk, rvp, rvs, rrho, nsublay)."""
+    dep = np.ascontiguousarray(dep, np.float32)
+    vp = np.ascontiguousarray(vp, np.float32)
+    vs = np.ascontiguousarray(vs, np.float32)
+    rho = np.ascontiguousarray(rho, np.float32)
+    out = [np.zeros(200, np.float32) for _ in range(4)]
+    ns = np.zeros(200, np.int32)
+    r = lib().or_refine(ctypes.c_float(minthk), dep.size, _p(dep, _f32p), _p(vp, _f32p),
+                        _p(vs, _f32p), _p(rho, _f32p), *[_p(o, _f32p) for o in out],
+                        _p(ns, _i32p))
+    if r < 0:
+        raise ValueError("refined layer count exceeds 200")
+    return tuple(o[:r].copy() for o in out) + (ns[: dep.size - 1].copy(),)
+
+
+def surfdisp96(thk, vp, vs, rho, periods, iwave=2, igr=0, mode=1, iflsph=1,
+               tol=1e-6, round_f32=True):
+    """Returns (cg[kmax], status, evals[kmax])."""
+    thk = np.ascontiguousarray(thk, np.float32)
+    vp = np.ascontiguousarray(vp, np.float32)
+    vs = np.ascontiguousarray(vs, np.float32)
+    rho = np.ascontiguousarray(rho, np.float32)
+    t = np.ascontiguousarray(periods, np.float64)
+    cg = np.zeros(t.size, np.float64)
+    ev = np.zeros(t.size, np.int32)
+    st = lib().or_surfdisp96_ex(_p(thk, _f32p), _p(vp, _f32p), _p(vs, _f32p), _p(rho, _f32p),
+                                thk.size, iflsph, iwave, mode, igr, t.size, _p(t, _f64p),
+                                _p(cg, _f64p), tol, int(round_f32), _p(ev, _i32p))
+    return cg, st, ev
+
+
+def depthkernel(vel, depz, periods, minthk, vp=None, rho=None, iwave=2, igr=0,
+                col_start=1, col_count=None, nthreads=0, tol=1e-6, round_f32=True,
+                kernels=True):
+    """Oracle of ``depthkernel`` (CalSurfG.f90:1-113, default_fortran_fd).
+
+    Returns dict with pvRc (nxy,K), sen_vs/sen_vp/sen_rho (nxy,K,nz) F-order,
+    status (nxy,) and evals (total secular evaluations).
+    """
+    vel = np.asfortranarray(vel, np.float32)
+    nx, ny, nz = vel.shape
+    t = np.ascontiguousarray(periods, np.float64)
+    K = t.size
+    depz = np.ascontiguousarray(depz, np.float32)
+    nxy = nx * ny
+    if col_count is None:
+        col_count = nxy - col_start + 1
+    vp_a = None if vp is None else np.asfortranarray(vp, np.float32)
+    rho_a = None if rho is None else np.asfortranarray(rho, np.float32)
+    pv = np.zeros((nxy, K), np.float64, order="F")
+    if kernels:
+        svs = np.zeros((nxy, K, nz), np.float64, order="F")
+        svp = np.zeros_like(svs)
+        srh = np.zeros_like(svs)
+    else:
+        svs = svp = srh = None
+    status = np.zeros(nxy, np.int32)
+    ev = ctypes.c_long(0)
+    if kernels:
+        r = lib().or_depthkernel(nx, ny, nz, _p(vel, _f32p), _p(vp_a, _f32p), _p(rho_a, _f32p),
+                                 _p(pv, _f64p), _p(svs, _f64p), _p(svp, _f64p), _p(srh, _f64p),
+                                 iwave, igr, K, _p(t, _f64p), _p(depz, _f32p),
+                                 ctypes.c_float(minthk), col_start, col_count, nthreads, tol,
+                                 int(round_f32), _p(status, _i32p), ctypes.byref(ev))
+        if r != 0:
+            raise RuntimeError(f"oracle depthkernel failed ({r})")
+        return dict(pvRc=pv, sen_vs=svs, sen_vp=svp, sen_rho=srh, status=status,
+                    evals=ev.value)
+    evcp = np.zeros((nxy, K), np.int32, order="F")
+    r = lib().or_phase(nx, ny, nz, _p(vel, _f32p), _p(vp_a, _f32p), _p(rho_a, _f32p),
+                       _p(pv, _f64p), iwave, igr, K, _p(t, _f64p), _p(depz, _f32p),
+                       ctypes.c_float(minthk), nthreads, tol, int(round_f32),
+                       _p(evcp, _i32p), _p(status, _i32p))
+    if r != 0:
+        raise RuntimeError(f"oracle phase failed ({r})")
+    return dict(pvRc=pv, status=status, evals_cp=evcp)
+
+
+def depthkernel_ti(vel, depz, periods, minthk, vp=None, rho=None, iwave=2, igr=0,
+                   nthreads=0):
+    """Oracle of ``depthkernelTI`` (depthkernelTI.f90:2-193).
+
+    Returns dict with pvRc (nxy,K) float64 and Lsen_Gsc (nxy,K,nz-1) float32,
+    both F-order, plus status (nxy,).
+    """
+    vel = np.asfortranarray(vel, np.float32)
+    nx, ny, nz = vel.shape
+    t = np.ascontiguousarray(periods, np.float64)
+    K = t.size
+    depz = np.ascontiguousarray(depz, np.float32)
+    nxy = nx * ny
+    vp_a = None if vp is None else np.asfortranarray(vp, np.float32)
+    rho_a = None if rho is None else np.asfortranarray(rho, np.float32)
+    pv = np.zeros((nxy, K), np.float64, order="F")
+    lsen = np.zeros((nxy, K, nz - 1), np.float32, order="F")
+    status = np.zeros(nxy, np.int32)
+    r = lib().or_depthkernelTI(nx, ny, nz, _p(vel, _f32p), _p(vp_a, _f32p), _p(rho_a, _f32p),
+                               _p(pv, _f64p), iwave, igr, K, _p(t, _f64p), _p(depz, _f32p),
+                               ctypes.c_float(minthk), _p(lsen, _f32p), 1, nxy, nthreads,
+                               _p(status, _i32p))
+    if r != 0:
+        raise RuntimeError(f"oracle depthkernelTI failed ({r})")
+    return dict(pvRc=pv, Lsen_Gsc=lsen, status=status)
