@@ -1,0 +1,340 @@
+#!/usr/bin/env python
+"""Benchmark of the depth-kernel stage: kernel column-periods per second.
+
+One column-period = the Rayleigh phase velocity c(T) of one column plus its
+Vs-type kernels (dc/dVs, dc/dVp, dc/drho at every node).  A "step" is one
+pass of the stage over the whole workload.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload config1]
+                    [--form plain|adjoint] [--impl ours|reference]
+
+value      device-timed throughput, inputs resident in HBM (device entry
+           dazi_dk_iso_dev on torch's stream, CUDA events per step, L2
+           flushed between steps outside the timed events)
+e2e        the same through the host C-ABI entry dazi_dk_iso with pinned host
+           buffers: host->device inputs and device->host outputs every step
+roofline   FP64 CUDA-core bound: algorithmic FLOPs (180 per layer per secular
+           evaluation, evaluations counted by the kernels) / kernel time,
+           against the FP64 FMA peak measured live by dazi_dk_fp64_peak
+cpu_baseline  the CPU oracle (C restatement of the reference Fortran, OpenMP
+           over columns) on a bounded sample of the same workload
+
+Multi-GPU (torchrun): columns are independent, so every rank runs the same
+per-GPU workload with no data-path collective (weak scaling); the step time
+is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+FLOP_PER_LAYER_EVAL = 180   # FP64 flops per layer per secular evaluation
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--workload", default="config1")
+    p.add_argument("--form", default="plain", choices=["plain", "adjoint"])
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--cpu-sample-s", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_setup(args):
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if ws > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        backend = "nccl" if args.impl == "ours" else "gloo"
+        dist.init_process_group(backend=backend, timeout=timedelta(seconds=300))
+    return ws, rank, local
+
+
+def load_case(name):
+    from dazi_current_release_b200 import synthetic as S
+    return S.GRID_CONFIGS[name]()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons while the timed region runs."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.path = None
+
+    def __enter__(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.path or not os.path.exists(self.path):
+            return None
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx),
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_baseline(case, sample_s, form_kernels=True):
+    """Oracle FD (the reference algorithm) on as many columns as fit in about
+    sample_s seconds on all host threads; returns column-periods/s."""
+    from oracle import oracle as O
+    cores = os.cpu_count() or 1
+    nx, ny, nz = case.vel.shape
+    K = case.periods.size
+    flat = np.asfortranarray(case.vel.reshape(nx * ny, 1, nz))
+    vp = None if case.vp is None else np.asfortranarray(case.vp.reshape(nx * ny, 1, nz))
+    rho = None if case.rho is None else np.asfortranarray(case.rho.reshape(nx * ny, 1, nz))
+    ncols = max(1, min(nx * ny, cores))
+    t0 = time.perf_counter()
+    O.depthkernel(flat[:ncols], case.depz, case.periods, case.minthk,
+                  vp=None if vp is None else vp[:ncols], rho=None if rho is None else rho[:ncols],
+                  nthreads=cores)
+    t1 = time.perf_counter()
+    per_col = (t1 - t0) / ncols * cores
+    n2 = int(max(ncols, min(nx * ny, sample_s / max(per_col, 1e-9) * cores)))
+    n2 = max(cores, (n2 // cores) * cores) if n2 >= cores else n2
+    n2 = min(n2, nx * ny)
+    t0 = time.perf_counter()
+    O.depthkernel(flat[:n2], case.depz, case.periods, case.minthk,
+                  vp=None if vp is None else vp[:n2], rho=None if rho is None else rho[:n2],
+                  nthreads=cores)
+    dt = time.perf_counter() - t0
+    return {"value": n2 * K / dt, "unit": "column-periods/s", "cores": cores,
+            "kind": "port",
+            "sample": f"{n2} of {nx*ny} columns x {K} periods, oracle FD (1+6nz surfdisp96 "
+                      f"per column), {dt:.1f} s on {cores} threads"}
+
+
+def run_reference(args, ws, rank):
+    case = load_case(args.workload)
+    if rank != 0:
+        return
+    nx, ny, nz = case.vel.shape
+    K = case.periods.size
+    vals = []
+    for _ in range(args.warmup):
+        pass
+    for _ in range(args.steps):
+        cb = cpu_baseline(case, args.cpu_sample_s / max(args.steps, 1))
+        vals.append(cb["value"])
+    v = float(np.median(vals))
+    line = {"impl": "reference", "metric": "kernel column-periods/s", "value": v,
+            "unit": "column-periods/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": nx * ny * K / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": args.workload, "columns": nx * ny,
+                                            "periods": K, "nodes": nz, "minthk": case.minthk},
+            "cpu_baseline": {"value": v, "unit": "column-periods/s", "cores": cb["cores"],
+                             "kind": cb["kind"], "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": "column-periods/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_setup(args)
+    if args.impl == "reference":
+        run_reference(args, ws, rank)
+        return
+    import torch
+    from dazi_current_release_b200 import _lib
+    from dazi_current_release_b200.depthkernel import _run_iso
+    L = _lib.load(build_if_missing=False)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    case = load_case(args.workload)
+    nx, ny, nz = case.vel.shape
+    K = case.periods.size
+    nxy = nx * ny
+    form = _lib.FORM_PLAIN if args.form == "plain" else _lib.FORM_ADJOINT
+
+    # ---------------- device-resident timing (value)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a.ravel(order="F"))).to(dev)  # noqa: E731
+    vel = t(case.vel)
+    vp = None if case.vp is None else t(case.vp)
+    rho = None if case.rho is None else t(case.rho)
+    per = torch.from_numpy(case.periods.copy()).to(dev)
+    depz = torch.from_numpy(case.depz.copy()).to(dev)
+    pv = torch.zeros(nxy * K, dtype=torch.float64, device=dev)
+    sen = [torch.zeros(nxy * K * nz, dtype=torch.float64, device=dev) for _ in range(3)]
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    ptr = lambda x: None if x is None else ctypes.c_void_p(x.data_ptr())  # noqa: E731
+
+    def step():
+        rc = L.dazi_dk_iso_dev(nx, ny, nz, ptr(vel), ptr(vp), ptr(rho), ptr(pv), ptr(sen[0]),
+                               ptr(sen[1]), ptr(sen[2]), K, ptr(per), ptr(depz),
+                               ctypes.c_float(case.minthk), 1, nxy, form, None,
+                               ctypes.c_void_p(stream.cuda_stream))
+        _lib.check(rc)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    ev = ctypes.c_longlong(0)
+    lev = ctypes.c_longlong(0)
+    _lib.check(L.dazi_dk_last_work(ctypes.byref(ev), ctypes.byref(lev)))
+    evals_per_step, layer_evals_per_step = ev.value, lev.value
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(local) as clk:
+        for i in range(args.steps):
+            flush.zero_()                      # L2 flush, outside the timed events
+            starts[i].record(stream)
+            step()
+            ends[i].record(stream)
+        torch.cuda.synchronize(dev)
+    if ws > 1:
+        torch.distributed.barrier()
+    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
+    total_ms = float(sum(step_ms))
+    if ws > 1:
+        tt = torch.tensor([total_ms], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(tt.item())
+    ms_per_step = total_ms / args.steps
+    value = ws * nxy * K / (ms_per_step * 1e-3)
+
+    # ---------------- end to end through the host C-ABI (pinned buffers)
+    pin = lambda shape, dt: torch.empty(shape, dtype=dt, pin_memory=True).numpy()  # noqa: E731
+    h_vel = pin((nxy * nz,), torch.float32)
+    h_vel[:] = case.vel.ravel(order="F")
+    h_vel = h_vel.reshape((nx, ny, nz), order="F")
+    h_pv = pin((nxy * K,), torch.float64).reshape((nxy, K), order="F")
+    h_sen = tuple(pin((nxy * K * nz,), torch.float64).reshape((nxy, K, nz), order="F")
+                  for _ in range(3))
+    if case.vp is not None:
+        h_vp = pin((nxy * nz,), torch.float32)
+        h_vp[:] = case.vp.ravel(order="F")
+        h_rho = pin((nxy * nz,), torch.float32)
+        h_rho[:] = case.rho.ravel(order="F")
+        h_vp = h_vp.reshape((nx, ny, nz), order="F")
+        h_rho = h_rho.reshape((nx, ny, nz), order="F")
+    else:
+        h_vp = h_rho = None
+
+    def e2e_step():
+        _run_iso(nx, ny, nz, h_vel, h_vp, h_rho, 2, 0, K, case.periods, case.depz, case.minthk,
+                 form, 1, None, True, pvRc=h_pv, sen=h_sen)
+
+    e2e_step()
+    if ws > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if ws > 1:
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    h2d = nxy * nz * 4 * (3 if case.vp is not None else 1) + K * 8
+    d2h = nxy * K * 8 * (1 + 3 * nz) + nxy * 4
+
+    # ---------------- roofline
+    peak = ctypes.c_double(0.0)
+    _lib.check(L.dazi_dk_fp64_peak(ctypes.byref(peak)))
+    flops = layer_evals_per_step * FLOP_PER_LAYER_EVAL
+    achieved = flops / (ms_per_step * 1e-3) / 1e12
+    peak_tf = peak.value / 1e3
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(tpath):
+        try:
+            tr = json.load(open(tpath))
+            traffic = tr.get(f"{args.workload}:{args.form}")
+        except (ValueError, OSError):
+            traffic = None
+
+    line = {
+        "metric": "kernel column-periods/s", "value": value, "unit": "column-periods/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": args.workload, "form": args.form, "columns": nxy, "periods": K,
+                   "nodes": nz, "minthk": case.minthk, "parallelism": f"columns x {ws} GPU",
+                   "l2": "flushed between steps (256 MiB write outside the timed events)"},
+        "e2e": {"value": ws * nxy * K / e2e_s, "unit": "column-periods/s",
+                "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+        "roofline": {"bound": "fp64", "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
+                     "frac": achieved / peak_tf if peak_tf > 0 else None, "traffic": traffic,
+                     "peak_source": "measured in-run FP64 FMA probe (dazi_dk_fp64_peak)",
+                     "flops_per_step": flops, "secular_evals_per_step": evals_per_step},
+        "gpu_launches": args.steps * 1,
+    }
+    clocks = clk.summary()
+    if clocks:
+        line["clocks"] = clocks
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(case, args.cpu_sample_s)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -29,7 +29,7 @@ FORM_ADJOINT = 1
 # every symbol include/dazi_dk.h declares
 EXPORTS = (
     "dazi_dk_iso", "dazi_dk_iso_vpvsrho", "dazi_dk_last_status", "dazi_dk_iso_dev",
-    "dazi_dk_last_error", "dazi_dk_version", "dazi_dk_finalize",
+    "dazi_dk_last_error", "dazi_dk_version", "dazi_dk_finalize", "dazi_dk_fp64_peak", "dazi_dk_last_work",
 )
 
 
@@ -75,6 +75,10 @@ def load(build_if_missing: bool = True):
     L.dazi_dk_last_error.restype = ctypes.c_char_p
     L.dazi_dk_version.argtypes = []
     L.dazi_dk_version.restype = _int
+    L.dazi_dk_last_work.argtypes = [ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+    L.dazi_dk_last_work.restype = _int
+    L.dazi_dk_fp64_peak.argtypes = [_f64p]
+    L.dazi_dk_fp64_peak.restype = _int
     L.dazi_dk_finalize.argtypes = []
     L.dazi_dk_finalize.restype = None
     _lib = L

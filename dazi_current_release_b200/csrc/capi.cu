@@ -68,7 +68,8 @@ struct Context {
     // host-entry staging
     DBuf vel, vp, rho, per, depz, pv, svs, svp, srh, status;
     // work buffers
-    DBuf geo, cscratch, layers, croot;
+    DBuf geo, cscratch, layers, layersd, croot, counters;
+    int last_rmax = 0;
     // geometry cache key
     std::vector<float> geo_depz;
     float geo_minthk = -1.f;
@@ -162,6 +163,10 @@ int iso_device(int nx, int ny, int nz, const float* vel, const float* vp, const 
     const Geometry* geo = g_ctx.geo.as<Geometry>();
     const double tol = 1.0e-6;   // surfdisp96.f:608
     int r;
+    if ((r = g_ctx.counters.ensure(sizeof(unsigned long long) * 4))) return r;
+    CK(cudaMemsetAsync(g_ctx.counters.p, 0, sizeof(unsigned long long) * 4, st));
+    g_ctx.last_rmax = g_ctx.geo_rmax;
+    unsigned long long* nevals = g_ctx.counters.as<unsigned long long>();
     if (svs && form == DAZI_FORM_PLAIN) {
         const int nmod = 1 + 6 * nz;
         const size_t per_col = sizeof(float) * (size_t)nmod * kmax;
@@ -181,7 +186,7 @@ int iso_device(int nx, int ny, int nz, const float* vel, const float* vp, const 
             a.vel = vel; a.vp = vp; a.rho = rho; a.periods = per;
             a.pv = pv; a.sen_vs = svs; a.sen_vp = svp; a.sen_rho = srh;
             a.status = status; a.cscratch = g_ctx.cscratch.as<float>();
-            a.dln = 0.01f; a.tol = tol;
+            a.dln = 0.01f; a.tol = tol; a.nevals = nevals;
             fd_column_kernel<<<(unsigned)n, threads, smem, st>>>(a);
             CK(cudaGetLastError());
         }
@@ -192,18 +197,22 @@ int iso_device(int nx, int ny, int nz, const float* vel, const float* vp, const 
         return DAZI_ERR_BADARG;
     }
     // pv only: one thread per column
-    if ((r = g_ctx.layers.ensure(sizeof(float4) * NL * (size_t)col_count))) return r;
+    const size_t nl = (size_t)g_ctx.geo_rmax * (size_t)col_count;
+    if ((r = g_ctx.layers.ensure(sizeof(float4) * nl))) return r;
+    if ((r = g_ctx.layersd.ensure(sizeof(LayerD) * nl))) return r;
     BuildArgs b;
     b.geo = geo; b.nz = nz; b.ncol = ncol; b.col0 = col_start - 1; b.ncols = col_count;
     b.vel = vel; b.vp = vp; b.rho = rho; b.layers = g_ctx.layers.as<float4>();
+    b.layersd = g_ctx.layersd.as<LayerD>();
     const int bt = 128;
     const unsigned nb = (unsigned)((col_count + bt - 1) / bt);
     build_layers_kernel<<<nb, bt, 0, st>>>(b);
     CK(cudaGetLastError());
     RootArgs a;
     a.geo = geo; a.kmax = kmax; a.ncol = ncol; a.col0 = col_start - 1; a.ncols = col_count;
-    a.layers = g_ctx.layers.as<float4>(); a.periods = per; a.tol = tol;
-    a.pv = pv; a.croot = nullptr; a.evals = nullptr; a.status = status;
+    a.layers = g_ctx.layers.as<float4>(); a.layersd = g_ctx.layersd.as<LayerD>();
+    a.periods = per; a.tol = tol;
+    a.pv = pv; a.croot = nullptr; a.evals = nullptr; a.status = status; a.nevals = nevals;
     root_kernel<<<nb, bt, 0, st>>>(a);
     CK(cudaGetLastError());
     return 0;
@@ -346,7 +355,7 @@ int dazi_dk_iso_dev(int nx, int ny, int nz, const float* vel, const float* vp, c
     std::lock_guard<std::mutex> lk(g_mu);
     int r;
     if ((r = ensure_context())) return r;
-    cudaStream_t st = stream ? (cudaStream_t)stream : g_ctx.stream;
+    cudaStream_t st = (cudaStream_t)stream;   // NULL: the legacy default stream
     std::vector<float> hd(nz);
     std::vector<double> ht(kmaxRc);
     CK(cudaMemcpyAsync(hd.data(), depz, sizeof(float) * nz, cudaMemcpyDeviceToHost, st));
@@ -359,6 +368,17 @@ int dazi_dk_iso_dev(int nx, int ny, int nz, const float* vel, const float* vp, c
                       col_start, col_count, form, status, st);
 }
 
+int dazi_dk_last_work(long long* secular_evals, long long* layer_evals)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_ctx.ready || !g_ctx.counters.p) { set_err("no call made yet"); return DAZI_ERR_BADARG; }
+    unsigned long long h[4] = {0, 0, 0, 0};
+    CK(cudaMemcpy(h, g_ctx.counters.p, sizeof(h), cudaMemcpyDeviceToHost));
+    if (secular_evals) *secular_evals = (long long)h[0];
+    if (layer_evals) *layer_evals = (long long)h[0] * (long long)g_ctx.last_rmax;
+    return 0;
+}
+
 const char* dazi_dk_last_error(void) { return g_err; }
 
 int dazi_dk_version(void) { return 100; }
@@ -369,7 +389,7 @@ void dazi_dk_finalize(void)
     if (!g_ctx.ready) return;
     DBuf* all[] = {&g_ctx.vel, &g_ctx.vp, &g_ctx.rho, &g_ctx.per, &g_ctx.depz, &g_ctx.pv,
                    &g_ctx.svs, &g_ctx.svp, &g_ctx.srh, &g_ctx.status, &g_ctx.geo,
-                   &g_ctx.cscratch, &g_ctx.layers, &g_ctx.croot};
+                   &g_ctx.cscratch, &g_ctx.layers, &g_ctx.layersd, &g_ctx.croot, &g_ctx.counters};
     for (DBuf* b : all) b->release();
     if (g_ctx.stream) cudaStreamDestroy(g_ctx.stream);
     g_ctx = Context();

@@ -20,6 +20,7 @@ struct FdArgs {
     double* sen_rho;
     int* status;         // (ncol) first failing period (1-based) or 0
     float* cscratch;     // [columns in launch][1 + 6 nz][K]
+    unsigned long long* nevals;  // secular evaluations (accumulated), or nullptr
     float dln;
     double tol;
 };
@@ -31,7 +32,8 @@ struct BuildArgs {
     const float* vel;
     const float* vp;
     const float* rho;
-    float4* layers;      // [ncols][NL] flattened (d, a, b, rho)
+    float4* layers;      // [rmax][ncols] flattened (d, a, b, rho)
+    LayerD* layersd;     // [rmax][ncols] FP64 per-layer constants
 };
 
 struct RootArgs {
@@ -39,12 +41,14 @@ struct RootArgs {
     int kmax;
     long long ncol, col0, ncols;
     const float4* layers;
+    const LayerD* layersd;
     const double* periods;
     double tol;
     double* pv;          // (ncol, K) FP32-valued like the reference
     double* croot;       // [ncols][K] FP64 roots, or nullptr
     int* evals;          // (ncol, K) secular evaluations, or nullptr
     int* status;
+    unsigned long long* nevals;  // secular evaluations (accumulated), or nullptr
 };
 
 __global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);

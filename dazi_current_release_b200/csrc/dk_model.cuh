@@ -136,6 +136,29 @@ __device__ __forceinline__ float4 flat_layer(const Geometry& g, int m, const flo
     return L;
 }
 
+// Per-layer constants the secular function needs, precomputed once per model
+// so the layer loop has no division by model parameters.
+struct LayerD {
+    double d;      // flattened thickness
+    double ia;     // 1 / Vp
+    double ib;     // 1 / Vs
+    double b2;     // Vs^2
+    double rho;    // density
+    double irho;   // 1 / density
+};
+
+__device__ __forceinline__ LayerD make_layerd(float4 L)
+{
+    LayerD o;
+    o.d = (double)L.x;
+    o.ia = 1.0 / (double)L.y;
+    o.ib = 1.0 / (double)L.z;
+    o.b2 = (double)L.z * (double)L.z;
+    o.rho = (double)L.w;
+    o.irho = 1.0 / (double)L.w;
+    return o;
+}
+
 // gtsolh(), surfdisp96.f:361-382: Rayleigh half-space speed, real*4.
 __device__ inline float gtsolh(float a, float b)
 {

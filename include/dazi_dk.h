@@ -83,13 +83,25 @@ int dazi_dk_last_status(int *status, long long n);
 /* Device-pointer entry of the iso stage for callers that already hold the
  * data in HBM (the PyTorch binding).  All array pointers are device
  * pointers; vp/rho may be NULL (Brocher); sen_* may be NULL; status (nx*ny
- * ints, device) may be NULL.  stream is a cudaStream_t (NULL = default). */
+ * ints, device) may be NULL.  stream is a cudaStream_t; NULL means the
+ * legacy default stream.  Work is stream-ordered and the call returns
+ * without waiting for it (only the tiny depz/tRc read-back synchronises). */
 int dazi_dk_iso_dev(int nx, int ny, int nz, const float *vel, const float *vp,
                     const float *rho, double *pvRc, double *sen_vsRc,
                     double *sen_vpRc, double *sen_rhoRc, int kmaxRc,
                     const double *tRc, const float *depz, float minthk,
                     int col_start, int col_count, int form, int *status,
                     void *stream);
+
+/* Work done by the last call, for roofline accounting: the number of
+ * Rayleigh secular-function evaluations (each one a pass over the refined
+ * layer stack) and evaluations x layers.  Synchronises with the device. */
+int dazi_dk_last_work(long long *secular_evals, long long *layer_evals);
+
+/* Diagnostic: measured FP64 FMA throughput of the current device in
+ * GFLOP/s (best of 5 launches of an FMA-chain kernel).  The stage's kernels
+ * run on the FP64 CUDA-core pipe; this is their roofline denominator. */
+int dazi_dk_fp64_peak(double *gflops);
 
 /* Message of the last error (static storage, never NULL). */
 const char *dazi_dk_last_error(void);
