@@ -68,7 +68,7 @@ struct Context {
     // host-entry staging
     DBuf vel, vp, rho, per, depz, pv, svs, svp, srh, status;
     // work buffers
-    DBuf geo, cscratch, layers, layersd, croot, counters;
+    DBuf geo, cscratch, layers, layersd, croot, counters, adjscr;
     int last_rmax = 0;
     // geometry cache key
     std::vector<float> geo_depz;
@@ -192,11 +192,7 @@ int iso_device(int nx, int ny, int nz, const float* vel, const float* vp, const 
         }
         return 0;
     }
-    if (svs && form != DAZI_FORM_PLAIN) {
-        set_err("form %d is not available in this build", form);
-        return DAZI_ERR_BADARG;
-    }
-    // pv only: one thread per column
+    // pv (and, for the adjoint form, the roots): one thread per column
     const size_t nl = (size_t)g_ctx.geo_rmax * (size_t)col_count;
     if ((r = g_ctx.layers.ensure(sizeof(float4) * nl))) return r;
     if ((r = g_ctx.layersd.ensure(sizeof(LayerD) * nl))) return r;
@@ -213,7 +209,35 @@ int iso_device(int nx, int ny, int nz, const float* vel, const float* vp, const 
     a.layers = g_ctx.layers.as<float4>(); a.layersd = g_ctx.layersd.as<LayerD>();
     a.periods = per; a.tol = tol;
     a.pv = pv; a.croot = nullptr; a.evals = nullptr; a.status = status; a.nevals = nevals;
+    const bool adj = svs && form == DAZI_FORM_ADJOINT;
+    if (adj) {
+        if ((r = g_ctx.croot.ensure(sizeof(double) * (size_t)kmax * (size_t)col_count))) return r;
+        a.croot = g_ctx.croot.as<double>();
+    }
     root_kernel<<<nb, bt, 0, st>>>(a);
+    CK(cudaGetLastError());
+    if (!adj) return 0;
+    // adjoint sweeps: one thread per (column, period), a persistent grid so
+    // the per-thread scratch slots are bounded by the resident threads
+    int dev = 0, sms = 0, per_sm = 0;
+    CK(cudaGetDevice(&dev));
+    CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    const int at = 128;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adjoint_kernel, at, 0));
+    if (per_sm < 1) per_sm = 1;
+    long long nblk = (long long)sms * per_sm;
+    const long long nitems = col_count * (long long)kmax;
+    const long long need = (nitems + at - 1) / at;
+    if (nblk > need) nblk = need;
+    const long long nslots = nblk * at;
+    const size_t scr = sizeof(double) * 6 * (size_t)(g_ctx.geo_rmax - 1 > 0 ? g_ctx.geo_rmax - 1 : 1) * (size_t)nslots;
+    if ((r = g_ctx.adjscr.ensure(scr))) return r;
+    AdjArgs j;
+    j.geo = geo; j.nz = nz; j.kmax = kmax; j.ncol = ncol; j.col0 = col_start - 1;
+    j.ncols = col_count; j.layers = g_ctx.layers.as<float4>(); j.periods = per;
+    j.croot = g_ctx.croot.as<double>(); j.sen_vs = svs; j.sen_vp = svp; j.sen_rho = srh;
+    j.scratch = g_ctx.adjscr.as<double>();
+    adjoint_kernel<<<(unsigned)nblk, at, 0, st>>>(j);
     CK(cudaGetLastError());
     return 0;
 }
@@ -389,7 +413,7 @@ void dazi_dk_finalize(void)
     if (!g_ctx.ready) return;
     DBuf* all[] = {&g_ctx.vel, &g_ctx.vp, &g_ctx.rho, &g_ctx.per, &g_ctx.depz, &g_ctx.pv,
                    &g_ctx.svs, &g_ctx.svp, &g_ctx.srh, &g_ctx.status, &g_ctx.geo,
-                   &g_ctx.cscratch, &g_ctx.layers, &g_ctx.layersd, &g_ctx.croot, &g_ctx.counters};
+                   &g_ctx.cscratch, &g_ctx.layers, &g_ctx.layersd, &g_ctx.croot, &g_ctx.counters, &g_ctx.adjscr};
     for (DBuf* b : all) b->release();
     if (g_ctx.stream) cudaStreamDestroy(g_ctx.stream);
     g_ctx = Context();

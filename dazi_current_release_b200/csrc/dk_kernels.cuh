@@ -51,6 +51,21 @@ struct RootArgs {
     unsigned long long* nevals;  // secular evaluations (accumulated), or nullptr
 };
 
+struct AdjArgs {
+    const Geometry* geo;
+    int nz, kmax;
+    long long ncol, col0, ncols;
+    const float4* layers;   // [rmax][ncols]
+    const double* periods;
+    const double* croot;    // [K][ncols] roots (0 where no root)
+    double* sen_vs;         // (ncol, K, nz) Fortran layout
+    double* sen_vp;
+    double* sen_rho;
+    double* scratch;        // [(rmax-1)*6][grid threads]
+};
+
+__global__ void adjoint_kernel(AdjArgs a);
+
 __global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);
 __global__ void fd_column_kernel(FdArgs a);
 __global__ void build_layers_kernel(BuildArgs a);

@@ -162,7 +162,9 @@ struct RootSM {
 
     // Runs the machine until it requests an evaluation (returns true, with
     // ceval/omega set) or finishes (returns false).  Results go through
-    // out(k, c, evals): c is the FP64 root, 0 for periods without a root.
+    // out(k, c, ctight, evals): c is the reference's FP64 root (converged to
+    // |c1 - c2| <= tol * c1, surfdisp96.f:608), ctight the secant root inside
+    // that final bracket (error O(bracket^2)); both 0 without a root.
     template <class Out>
     __device__ bool next(double F, const double* periods, Out& out)
     {
@@ -258,8 +260,15 @@ struct RootSM {
     template <class Out>
     __device__ bool finish(Out& out)
     {
-        if (c3 > (double)betmx) { out(k, 0.0, evals); fail(); return false; }
-        out(k, c3, evals);
+        if (c3 > (double)betmx) { out(k, 0.0, 0.0, evals); fail(); return false; }
+        // secant root inside the final bracket [c1, c2] (opposite signs)
+        double ct = c3;
+        const double dd = del2 - del1;
+        if (dd != 0.0 && fsign1(del1) != fsign1(del2)) {
+            const double s = c1 - del1 * (c2 - c1) / dd;
+            if (s >= fmin(c1, c2) && s <= fmax(c1, c2)) ct = s;
+        }
+        out(k, c3, ct, evals);
         cprev = c3;
         ++k;
         phase = START;
@@ -352,7 +361,7 @@ __device__ int solve_model_warp(bool active, const M& mdl, int mmax, double cc, 
         }
     }
     if (active && sm.fail_k >= 0)
-        for (int kk = sm.fail_k; kk < kmax; ++kk) out(kk, 0.0, kk == sm.fail_k ? sm.evals : 0);
+        for (int kk = sm.fail_k; kk < kmax; ++kk) out(kk, 0.0, 0.0, kk == sm.fail_k ? sm.evals : 0);
     if (total_evals) *total_evals = tot;
     return active ? sm.fail_k : -1;
 }

@@ -1,0 +1,449 @@
+// Adjoint form of the isotropic depth kernel: implicit differentiation of
+// the Rayleigh dispersion root.
+//
+// At a root c of the secular function F(c; m) (dltar4, surfdisp96.f:767-865)
+//     dc/dm = -(dF/dm) / (dF/dc),   dF/dc = -(wvno/c) dF/dwvno,
+// for every layer parameter m (flattened Vp, Vs, density).  The kernels the
+// reference obtains by perturb-and-recompute (DepthKernel1D.f90:102-185,
+// sen_X = (c(X+dX/2) - c(X-dX/2))/dX at each depth node) are these
+// derivatives chained through the Earth flattening (surfdisp96.f:480-547:
+// a_flat = a*tmp, b_flat = b*tmp, rho_flat = rho*btp**-2.275) and the
+// sublayer interpolation (CalSurfG.f90:2527-2529: each sublayer value is
+// (1-f) v(i) + f v(i+1), f = (2j-1)/(2 nsublay)).
+//
+// F is a chain of 5x5 compound-matrix products, e(m) = e(m+1) CA_m / n_m from
+// the half-space up to the surface, F = e(0)[0].  With the top-down vectors
+// g(0) = (1,0,0,0,0), g(m+1) = CA_m g(m) / n_m, F = e(m).g(m) at every m, so
+//     dF/dtheta_m = e(m+1) . (dCA_m/dtheta) . g(m) / n_m.
+// One thread owns one (column, period):
+//   1. bottom-up sweep at the root, storing e(m+1) and 1/n_m per layer in a
+//      global scratch slot of the thread (6 doubles per layer, [layer][slot]
+//      so a warp's stores coalesce); the 5x5 matrices are not stored;
+//   2. top-down sweep that recomputes CA_m with forward-mode tangents in
+//      (Vp_m, Vs_m, wvno) -- density enters each element as a power, so its
+//      derivative is read off the values -- and accumulates the node kernels.
+// The evanescent layer functions carry factored-out exponentials (var(),
+// surfdisp96.f:868-985); the tangents treat those scale factors as constants,
+// which differentiates the true secular function times one positive factor
+// common to every derivative, so the ratio is exact even slightly off the
+// root.  The root itself is the phase-1 root refined by a secant step inside
+// the reference's final Neville bracket.
+#include "dk_secular.cuh"
+#include "dk_kernels.cuh"
+
+namespace dk {
+
+// ------------------------------------------------------------ tangent type
+struct D3 {
+    double v, d0, d1, d2;
+};
+__device__ __forceinline__ D3 mk(double v) { return {v, 0.0, 0.0, 0.0}; }
+__device__ __forceinline__ D3 operator+(const D3& a, const D3& b) { return {a.v + b.v, a.d0 + b.d0, a.d1 + b.d1, a.d2 + b.d2}; }
+__device__ __forceinline__ D3 operator-(const D3& a, const D3& b) { return {a.v - b.v, a.d0 - b.d0, a.d1 - b.d1, a.d2 - b.d2}; }
+__device__ __forceinline__ D3 operator-(const D3& a) { return {-a.v, -a.d0, -a.d1, -a.d2}; }
+__device__ __forceinline__ D3 operator*(const D3& a, const D3& b)
+{
+    return {a.v * b.v, fma(a.v, b.d0, a.d0 * b.v), fma(a.v, b.d1, a.d1 * b.v), fma(a.v, b.d2, a.d2 * b.v)};
+}
+__device__ __forceinline__ D3 operator*(double s, const D3& a) { return {s * a.v, s * a.d0, s * a.d1, s * a.d2}; }
+__device__ __forceinline__ D3 operator*(const D3& a, double s) { return s * a; }
+__device__ __forceinline__ D3 operator+(const D3& a, double s) { return {a.v + s, a.d0, a.d1, a.d2}; }
+__device__ __forceinline__ D3 operator-(const D3& a, double s) { return {a.v - s, a.d0, a.d1, a.d2}; }
+__device__ __forceinline__ D3 operator-(double s, const D3& a) { return {s - a.v, -a.d0, -a.d1, -a.d2}; }
+// a / b given ib = 1/b.v
+__device__ __forceinline__ D3 div_by(const D3& a, const D3& b, double ib)
+{
+    const double q = a.v * ib;
+    return {q, (a.d0 - q * b.d0) * ib, (a.d1 - q * b.d1) * ib, (a.d2 - q * b.d2) * ib};
+}
+
+// Layer functions of var() with tangents.  P (or S) part for one wave type:
+// vertical wavenumber r = sqrt(|wvno^2 - xk^2|), phase arg = r*d, and the
+// (cos, sin/r, r*sin) triple in oscillatory or scaled-hyperbolic form.
+struct WaveD3 {
+    D3 r, cosf, sinr, rsin;   // cos, sin/r, r*sin  (x = -r sin in the oscillatory case)
+    double scale_exp;         // factored-out exponent (0 when oscillatory)
+    bool evan;
+};
+
+__device__ __forceinline__ void wave_d3(const D3& wvno, const D3& xk, double d, WaveD3& o)
+{
+    const D3 s = wvno + xk;
+    const D3 t = wvno - xk;
+    const double sg = t.v < 0.0 ? -1.0 : 1.0;
+    const D3 prod = s * (sg * t);                 // (wvno + xk) |wvno - xk|
+    const double r = sqrt(prod.v);
+    const double ir = r > 0.0 ? 1.0 / r : 0.0;
+    const double h = 0.5 * ir;
+    o.r = {r, prod.d0 * h, prod.d1 * h, prod.d2 * h};
+    const D3 p = o.r * d;
+    if (wvno.v < xk.v) {
+        double sp, cp;
+        sincos(p.v, &sp, &cp);
+        o.evan = false;
+        o.scale_exp = 0.0;
+        o.cosf = {cp, -sp * p.d0, -sp * p.d1, -sp * p.d2};
+        const D3 sn = {sp, cp * p.d0, cp * p.d1, cp * p.d2};
+        o.sinr = div_by(sn, o.r, ir);
+        o.rsin = -(o.r * sn);                      // x = -r sin(p), z = -r sin(q)
+    } else if (wvno.v == xk.v) {
+        o.evan = false;
+        o.scale_exp = 0.0;
+        o.cosf = mk(1.0);
+        o.sinr = mk(d);
+        o.rsin = mk(0.0);
+    } else {
+        const double ep = exp(-p.v);
+        const double fac = (p.v < 16.0) ? ep * ep : 0.0;
+        const double cs = (1.0 + fac) * 0.5, ss = (1.0 - fac) * 0.5;
+        o.evan = true;
+        o.scale_exp = p.v;
+        // d(cosh) = sinh dp, d(sinh) = cosh dp, with the scale e^-p held
+        o.cosf = {cs, ss * p.d0, ss * p.d1, ss * p.d2};
+        const D3 sn = {ss, cs * p.d0, cs * p.d1, cs * p.d2};
+        o.sinr = div_by(sn, o.r, ir);
+        o.rsin = o.r * sn;
+    }
+}
+
+// The 19 distinct compound-matrix entries (dnka(), surfdisp96.f:1018-1062).
+template <class T>
+struct CAset {
+    T c11, c12, c13, c14, c15, c21, c22, c23, c24, c41, c42, c43, c51, c53, c31, c32, c33, c34, c35;
+};
+
+template <class T>
+__device__ __forceinline__ void dnka_t(CAset<T>& C, const T& wvno2, const T& gam, const T& gammk,
+                                       double rho, double irho, const T& a0, const T& cosp,
+                                       const T& w, const T& x, const T& cosq, const T& y,
+                                       const T& z)
+{
+    const T cpcq = cosp * cosq, cpy = cosp * y, cpz = cosp * z;
+    const T cqw = cosq * w, cqx = cosq * x;
+    const T xy = x * y, xz = x * z, wy = w * y, wz = w * z;
+    const T gamm1 = gam - 1.0, twgm1 = gam + gamm1, gmgmk = gam * gammk;
+    const T gmgm1 = gam * gamm1, gm1sq = gamm1 * gamm1;
+    const double rho2 = rho * rho, r2inv = irho * irho;
+    const T a0pq = a0 - cpcq;
+    C.c11 = cpcq - 2.0 * gmgm1 * a0pq - gmgmk * xz - wvno2 * gm1sq * wy;
+    C.c12 = (wvno2 * cpy - cqx) * irho;
+    C.c13 = -(twgm1 * a0pq + gammk * xz + wvno2 * gamm1 * wy) * irho;
+    C.c14 = (cpz - wvno2 * cqw) * irho;
+    C.c15 = -(2.0 * wvno2 * a0pq + xz + wvno2 * wvno2 * wy) * r2inv;
+    C.c21 = (gmgmk * cpz - gm1sq * cqw) * rho;
+    C.c22 = cpcq;
+    C.c23 = gammk * cpz - gamm1 * cqw;
+    C.c24 = -wz;
+    C.c41 = (gm1sq * cpy - gmgmk * cqx) * rho;
+    C.c42 = -xy;
+    C.c43 = gamm1 * cpy - gammk * cqx;
+    C.c51 = -(2.0 * gmgmk * gm1sq * a0pq + gmgmk * gmgmk * xz + gm1sq * gm1sq * wy) * rho2;
+    C.c53 = -(gammk * gamm1 * twgm1 * a0pq + gam * gammk * gammk * xz + gamm1 * gm1sq * wy) * rho;
+    const T tt = -2.0 * wvno2;
+    C.c31 = tt * C.c53;
+    C.c32 = tt * C.c43;
+    C.c33 = a0 + 2.0 * (cpcq - C.c11);
+    C.c34 = tt * C.c23;
+    C.c35 = tt * C.c13;
+}
+
+// Half-space starting vector (dltar4, surfdisp96.f:789-808) with tangents.
+__device__ __forceinline__ void halfspace_d3(const D3& wvno, const D3& xka, const D3& xkb,
+                                             const D3& gammk, double rho, D3 e[5])
+{
+    const D3 wvno2 = wvno * wvno;
+    const D3 sa = wvno + xka, ta = wvno - xka;
+    const D3 pa = sa * ((ta.v < 0.0 ? -1.0 : 1.0) * ta);
+    const D3 sb = wvno + xkb, tb = wvno - xkb;
+    const D3 pb = sb * ((tb.v < 0.0 ? -1.0 : 1.0) * tb);
+    const double ra = sqrt(pa.v), rb = sqrt(pb.v);
+    const double ha = ra > 0 ? 0.5 / ra : 0.0, hb = rb > 0 ? 0.5 / rb : 0.0;
+    const D3 Ra = {ra, pa.d0 * ha, pa.d1 * ha, pa.d2 * ha};
+    const D3 Rb = {rb, pb.d0 * hb, pb.d1 * hb, pb.d2 * hb};
+    const D3 gam = gammk * wvno2;
+    const D3 gamm1 = gam - 1.0;
+    const D3 rab = Ra * Rb;
+    e[0] = (rho * rho) * (gamm1 * gamm1 - gam * gammk * rab);
+    e[1] = -rho * Ra;
+    e[2] = rho * (gamm1 - gammk * rab);
+    e[3] = rho * Rb;
+    e[4] = wvno2 - rab;
+}
+
+// sum_ij u_i CA_ij v_j for the value and the three tangents, plus the
+// density derivative (entries scale as rho^pow).
+struct Contract {
+    double v, d0, d1, d2, drho;
+};
+
+__device__ __forceinline__ void acc_entry(Contract& s, double uv, const D3& c, int pw)
+{
+    s.v = fma(uv, c.v, s.v);
+    s.d0 = fma(uv, c.d0, s.d0);
+    s.d1 = fma(uv, c.d1, s.d1);
+    s.d2 = fma(uv, c.d2, s.d2);
+    if (pw) s.drho = fma(uv * (double)pw, c.v, s.drho);
+}
+
+__device__ __forceinline__ Contract contract(const CAset<D3>& C, const double u[5], const double g[5])
+{
+    Contract s = {0, 0, 0, 0, 0};
+    // row 1: c11 c12 c13 c14 c15
+    acc_entry(s, u[0] * g[0], C.c11, 0); acc_entry(s, u[0] * g[1], C.c12, -1);
+    acc_entry(s, u[0] * g[2], C.c13, -1); acc_entry(s, u[0] * g[3], C.c14, -1);
+    acc_entry(s, u[0] * g[4], C.c15, -2);
+    // row 2: c21 c22 c23 c24 c14
+    acc_entry(s, u[1] * g[0], C.c21, 1); acc_entry(s, u[1] * g[1], C.c22, 0);
+    acc_entry(s, u[1] * g[2], C.c23, 0); acc_entry(s, u[1] * g[3], C.c24, 0);
+    acc_entry(s, u[1] * g[4], C.c14, -1);
+    // row 3: c31 c32 c33 c34 c35
+    acc_entry(s, u[2] * g[0], C.c31, 1); acc_entry(s, u[2] * g[1], C.c32, 0);
+    acc_entry(s, u[2] * g[2], C.c33, 0); acc_entry(s, u[2] * g[3], C.c34, 0);
+    acc_entry(s, u[2] * g[4], C.c35, -1);
+    // row 4: c41 c42 c43 c22 c12
+    acc_entry(s, u[3] * g[0], C.c41, 1); acc_entry(s, u[3] * g[1], C.c42, 0);
+    acc_entry(s, u[3] * g[2], C.c43, 0); acc_entry(s, u[3] * g[3], C.c22, 0);
+    acc_entry(s, u[3] * g[4], C.c12, -1);
+    // row 5: c51 c41 c53 c21 c11
+    acc_entry(s, u[4] * g[0], C.c51, 2); acc_entry(s, u[4] * g[1], C.c41, 1);
+    acc_entry(s, u[4] * g[2], C.c53, 1); acc_entry(s, u[4] * g[3], C.c21, 1);
+    acc_entry(s, u[4] * g[4], C.c11, 0);
+    return s;
+}
+
+// g_new = CA g (values only)
+__device__ __forceinline__ void matvec(const CAset<D3>& C, const double g[5], double o[5])
+{
+    o[0] = C.c11.v * g[0] + C.c12.v * g[1] + C.c13.v * g[2] + C.c14.v * g[3] + C.c15.v * g[4];
+    o[1] = C.c21.v * g[0] + C.c22.v * g[1] + C.c23.v * g[2] + C.c24.v * g[3] + C.c14.v * g[4];
+    o[2] = C.c31.v * g[0] + C.c32.v * g[1] + C.c33.v * g[2] + C.c34.v * g[3] + C.c35.v * g[4];
+    o[3] = C.c41.v * g[0] + C.c42.v * g[1] + C.c43.v * g[2] + C.c22.v * g[3] + C.c12.v * g[4];
+    o[4] = C.c51.v * g[0] + C.c41.v * g[1] + C.c53.v * g[2] + C.c21.v * g[3] + C.c11.v * g[4];
+}
+
+// Build the tangent CA of layer m.  Tangent directions: 0 = Vp_m, 1 = Vs_m,
+// 2 = wvno.
+__device__ __forceinline__ void layer_ca_d3(const float4& L, double wvno_v, double omega,
+                                            CAset<D3>& C)
+{
+    const double a = (double)L.y, b = (double)L.z, rho = (double)L.w, d = (double)L.x;
+    const double ia = 1.0 / a, ib = 1.0 / b;
+    const D3 wvno = {wvno_v, 0.0, 0.0, 1.0};
+    const double xka_v = omega * ia, xkb_v = omega * ib;
+    const D3 xka = {xka_v, -xka_v * ia, 0.0, 0.0};     // d(omega/a)/da
+    const D3 xkb = {xkb_v, 0.0, -xkb_v * ib, 0.0};
+    const double gk = 2.0 * b * b / (omega * omega);
+    const D3 gammk = {gk, 0.0, 2.0 * gk * ib, 0.0};
+    const D3 wvno2 = wvno * wvno;
+    const D3 gam = gammk * wvno2;
+    WaveD3 P, S;
+    wave_d3(wvno, xka, d, P);
+    wave_d3(wvno, xkb, d, S);
+    const double exa = (P.evan ? P.scale_exp : 0.0) + (S.evan ? S.scale_exp : 0.0);
+    double a0v = 0.0;
+    if (exa < 60.0) {
+        const double ep = P.evan ? exp(-P.scale_exp) : 1.0;
+        const double eq = S.evan ? exp(-S.scale_exp) : 1.0;
+        a0v = ep * eq;
+    }
+    const D3 a0 = mk(a0v);   // the "1" of cosh^2 - sinh^2 under the held scale
+    dnka_t(C, wvno2, gam, gammk, rho, 1.0 / rho, a0, P.cosf, P.sinr, P.rsin, S.cosf, S.sinr, S.rsin);
+}
+
+// Value-only layer functions (same expressions as wave_d3 without tangents).
+__device__ __forceinline__ void wave_val(double wvno, double xk, double d, double& cosf,
+                                         double& sinr, double& rsin, bool& evan, double& sexp)
+{
+    const double r = sqrt((wvno + xk) * fabs(wvno - xk));
+    const double p = r * d;
+    if (wvno < xk) {
+        double sp, cp;
+        sincos(p, &sp, &cp);
+        evan = false; sexp = 0.0;
+        cosf = cp; sinr = sp / r; rsin = -r * sp;
+    } else if (wvno == xk) {
+        evan = false; sexp = 0.0;
+        cosf = 1.0; sinr = d; rsin = 0.0;
+    } else {
+        const double ep = exp(-p);
+        const double fac = (p < 16.0) ? ep * ep : 0.0;
+        evan = true; sexp = p;
+        cosf = (1.0 + fac) * 0.5;
+        const double ss = (1.0 - fac) * 0.5;
+        sinr = ss / r; rsin = r * ss;
+    }
+}
+
+// One bottom-up step f = e CA_m (values); returns the max-norm of f.
+__device__ __forceinline__ double layer_step_val(const float4& L, double wvno, double omega,
+                                                 const double e[5], double f[5])
+{
+    const double a = (double)L.y, b = (double)L.z, rho = (double)L.w, d = (double)L.x;
+    const double wvno2 = wvno * wvno;
+    const double gammk = 2.0 * b * b / (omega * omega);
+    const double gam = gammk * wvno2;
+    double cp, wp, xp, cq, yq, zq, ep_, eq_;
+    bool evp, evq;
+    wave_val(wvno, omega / a, d, cp, wp, xp, evp, ep_);
+    wave_val(wvno, omega / b, d, cq, yq, zq, evq, eq_);
+    const double exa = (evp ? ep_ : 0.0) + (evq ? eq_ : 0.0);
+    const double a0 = (exa < 60.0) ? exp(-exa) : 0.0;
+    CAset<double> C;
+    dnka_t(C, wvno2, gam, gammk, rho, 1.0 / rho, a0, cp, wp, xp, cq, yq, zq);
+    f[0] = e[0] * C.c11 + e[1] * C.c21 + e[2] * C.c31 + e[3] * C.c41 + e[4] * C.c51;
+    f[1] = e[0] * C.c12 + e[1] * C.c22 + e[2] * C.c32 + e[3] * C.c42 + e[4] * C.c41;
+    f[2] = e[0] * C.c13 + e[1] * C.c23 + e[2] * C.c33 + e[3] * C.c43 + e[4] * C.c53;
+    f[3] = e[0] * C.c14 + e[1] * C.c24 + e[2] * C.c34 + e[3] * C.c22 + e[4] * C.c21;
+    f[4] = e[0] * C.c15 + e[1] * C.c14 + e[2] * C.c35 + e[3] * C.c12 + e[4] * C.c11;
+    double t1 = fmax(fmax(fmax(fabs(f[0]), fabs(f[1])), fmax(fabs(f[2]), fabs(f[3]))), fabs(f[4]));
+    if (t1 < 1.0e-40) t1 = 1.0;
+    return t1;
+}
+
+// ---------------------------------------------------------------- kernel
+__global__ void __launch_bounds__(128)
+adjoint_kernel(AdjArgs a)
+{
+    __shared__ double s_per[NP];
+    for (int k = threadIdx.x; k < a.kmax; k += blockDim.x) s_per[k] = a.periods[k];
+    __syncthreads();
+    const Geometry* g = a.geo;
+    const int rmax = g->rmax, nz = a.nz, K = a.kmax;
+    const long long nslots = (long long)gridDim.x * blockDim.x;
+    const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nitems = a.ncols * K;
+    const long long ncol = a.ncol;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < nitems; base += nslots) {
+        const long long it = base + threadIdx.x;
+        const bool inrange = it < nitems;
+        const int k = inrange ? (int)(it / a.ncols) : 0;
+        const long long c = inrange ? it % a.ncols : 0;
+        const long long post = a.col0 + c;
+        const double croot = inrange ? a.croot[c + a.ncols * k] : 0.0;
+        const bool active = inrange && croot > 0.0;
+        double* dvs = a.sen_vs + post + ncol * ((long long)k);
+        double* dvp = a.sen_vp + post + ncol * ((long long)k);
+        double* drh = a.sen_rho + post + ncol * ((long long)k);
+        const long long nstride = ncol * (long long)K;   // node stride in the outputs
+        if (!active) {
+            if (inrange)
+                for (int i = 0; i < nz; ++i) { dvs[nstride * i] = 0.0; dvp[nstride * i] = 0.0; drh[nstride * i] = 0.0; }
+            continue;
+        }
+        const double omega = TWOPI / s_per[k];
+        const double wvno = omega / croot;
+        const float4* lay = a.layers + c;                 // [m][ncols]
+        const long long lstride = a.ncols;
+        double* scr = a.scratch + slot;                   // [(m*6 + comp)][nslots]
+        // ---- 1. bottom-up sweep: store e(m+1) and 1/n_m for m = rmax-2 .. 0
+        double e[5];
+        {
+            const float4 L = lay[(long long)(rmax - 1) * lstride];
+            const double aa = L.y, bb = L.z;
+            const D3 w = mk(wvno);
+            const D3 xka = mk(omega / aa), xkb = mk(omega / bb);
+            const D3 gk = mk(2.0 * bb * bb / (omega * omega));
+            D3 h[5];
+            halfspace_d3(w, xka, xkb, gk, (double)L.w, h);
+            for (int q = 0; q < 5; ++q) e[q] = h[q].v;
+        }
+        for (int m = rmax - 2; m >= 0; --m) {
+            const float4 L = lay[(long long)m * lstride];
+            double f[5];
+            const double nrm = layer_step_val(L, wvno, omega, e, f);
+            double* sp = scr + (long long)m * 6 * nslots;
+            for (int q = 0; q < 5; ++q) sp[q * nslots] = e[q];
+            const double inv = 1.0 / nrm;
+            sp[5 * nslots] = inv;
+            for (int q = 0; q < 5; ++q) e[q] = f[q] * inv;
+        }
+        // ---- 2. top-down sweep with tangents
+        double gv[5] = {1.0, 0.0, 0.0, 0.0, 0.0};
+        double dFdw = 0.0;
+        double acc_vs = 0.0, acc_vp = 0.0, acc_rh = 0.0;   // current node (top of interval)
+        double nxt_vs = 0.0, nxt_vp = 0.0, nxt_rh = 0.0;   // next node (bottom of interval)
+        int cur_node = 0;
+        int gexp = 0;   // g is kept as gv * 2^gexp
+        for (int m = 0; m <= rmax - 2; ++m) {
+            const int node = g->node[m];
+            if (node != cur_node) {
+                // interval cur_node finished: node cur_node is complete
+                dvs[nstride * cur_node] = acc_vs;
+                dvp[nstride * cur_node] = acc_vp;
+                drh[nstride * cur_node] = acc_rh;
+                acc_vs = nxt_vs; acc_vp = nxt_vp; acc_rh = nxt_rh;
+                nxt_vs = nxt_vp = nxt_rh = 0.0;
+                cur_node = node;
+            }
+            const float4 L = lay[(long long)m * lstride];
+            CAset<D3> C;
+            layer_ca_d3(L, wvno, omega, C);
+            const double* sp = scr + (long long)m * 6 * nslots;
+            double u[5];
+            for (int q = 0; q < 5; ++q) u[q] = sp[q * nslots];
+            const double inv = sp[5 * nslots];
+            const Contract s = contract(C, u, gv);
+            const double sc = ldexp(inv, gexp);
+            dFdw = fma(s.d2, sc, dFdw);
+            const double dFda = s.d0 * sc, dFdb = s.d1 * sc, dFdr = s.drho * sc / (double)L.w;
+            // chain to nodes: a_flat = tmp * ((1-f) vp_i + f vp_i+1), etc.
+            const double tmpm = g->tmp[m], rf = (double)g->rhofac[m];
+            const double fw = (double)g->sub[m] / (double)g->den[m];
+            acc_vp = fma(dFda * tmpm, 1.0 - fw, acc_vp); nxt_vp = fma(dFda * tmpm, fw, nxt_vp);
+            acc_vs = fma(dFdb * tmpm, 1.0 - fw, acc_vs); nxt_vs = fma(dFdb * tmpm, fw, nxt_vs);
+            acc_rh = fma(dFdr * rf, 1.0 - fw, acc_rh);   nxt_rh = fma(dFdr * rf, fw, nxt_rh);
+            double gn[5];
+            matvec(C, gv, gn);
+            double mx = 0.0;
+            for (int q = 0; q < 5; ++q) { gn[q] *= inv; mx = fmax(mx, fabs(gn[q])); }
+            int ex = 0;
+            if (mx > 0.0) frexp(mx, &ex);
+            for (int q = 0; q < 5; ++q) gv[q] = ldexp(gn[q], -ex);
+            gexp += ex;
+        }
+        // half-space: all remaining contributions go to node nz-1 (together
+        // with the bottom sublayers of interval nz-2 already in nxt_*)
+        {
+            const int m = rmax - 1;
+            const float4 L = lay[(long long)m * lstride];
+            const double aa = L.y, bb = L.z, rho = L.w;
+            const D3 w = {wvno, 0.0, 0.0, 1.0};
+            const D3 xka = {omega / aa, -omega / (aa * aa), 0.0, 0.0};
+            const D3 xkb = {omega / bb, 0.0, -omega / (bb * bb), 0.0};
+            const double gkv = 2.0 * bb * bb / (omega * omega);
+            const D3 gk = {gkv, 0.0, 2.0 * gkv / bb, 0.0};
+            D3 h[5];
+            halfspace_d3(w, xka, xkb, gk, rho, h);
+            const double sc = ldexp(1.0, gexp);
+            double s0 = 0, s1 = 0, s2 = 0, sr = 0;
+            const int pw[5] = {2, 1, 1, 1, 0};
+            for (int q = 0; q < 5; ++q) {
+                s0 = fma(h[q].d0, gv[q], s0);
+                s1 = fma(h[q].d1, gv[q], s1);
+                s2 = fma(h[q].d2, gv[q], s2);
+                sr = fma((double)pw[q] * h[q].v, gv[q], sr);
+            }
+            dFdw = fma(s2, sc, dFdw);
+            const double tmpm = g->tmp[m], rf = (double)g->rhofac[m];
+            // finish node nz-2 (if the loop ended inside its interval) and nz-1
+            dvs[nstride * cur_node] = acc_vs;
+            dvp[nstride * cur_node] = acc_vp;
+            drh[nstride * cur_node] = acc_rh;
+            nxt_vp = fma(s0 * sc, tmpm, nxt_vp);
+            nxt_vs = fma(s1 * sc, tmpm, nxt_vs);
+            nxt_rh = fma(sr * sc / rho, rf, nxt_rh);
+            dvs[nstride * (nz - 1)] = nxt_vs;
+            dvp[nstride * (nz - 1)] = nxt_vp;
+            drh[nstride * (nz - 1)] = nxt_rh;
+        }
+        // ---- 3. dc/dm = -F_m / F_c = (c / (wvno F_wvno)) F_m
+        const double scale = croot / (wvno * dFdw);
+        for (int i = 0; i < nz; ++i) {
+            dvs[nstride * i] *= scale;
+            dvp[nstride * i] *= scale;
+            drh[nstride * i] *= scale;
+        }
+    }
+}
+
+}  // namespace dk

@@ -129,7 +129,7 @@ fd_column_kernel(FdArgs a)
         const int q = r * nthr + tid;
         const bool active = q < nmod;
         float* myc = cbuf + (size_t)(active ? q : 0) * K;
-        auto out = [&](int k, double c, int ev) { myc[k] = (float)c; };
+        auto out = [&](int k, double c, double ct, int ev) { myc[k] = (float)c; };
         PerturbedModel mdl;
         mdl.lay = S.lay; mdl.ld = S.ld; mdl.g = g;
         mdl.node_val = S.vs; mdl.pnode = 0; mdl.par = 0; mdl.pval = 0.f;
@@ -217,9 +217,9 @@ root_kernel(RootArgs a)
     const int K = a.kmax;
     const int rmax = a.geo->rmax;
     ColumnModel mdl{a.layersd + cc_, a.ncols};
-    auto out = [&](int k, double cval, int ev) {
+    auto out = [&](int k, double cval, double ctight, int ev) {
         a.pv[post + a.ncol * k] = (double)(float)cval;
-        if (a.croot) a.croot[cc_ + a.ncols * k] = cval;
+        if (a.croot) a.croot[cc_ + a.ncols * k] = ctight;
         if (a.evals) a.evals[post + a.ncol * k] = ev;
     };
     double cc = 0.0;

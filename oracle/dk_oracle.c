@@ -109,12 +109,16 @@ int or_refine(float minthk0, int nz, const float *dep, const float *vp,
 /* Layer model after Earth flattening (surfdisp96.f COMMON/modl).           */
 typedef struct {
     int mmax, llw;
-    float d[NL], a[NL], b[NL], rho[NL], rtp[NL], dtp[NL], btp[NL];
-    float dhalf;          /* SAVE dhalf of sphere()                          */
+    int f32;              /* 1: store model values as real*4 (the reference) */
+    double d[NL], a[NL], b[NL], rho[NL], rtp[NL], dtp[NL], btp[NL];
+    double dhalf;         /* SAVE dhalf of sphere()                          */
     double del1st;        /* SAVE del1st of getsol()                         */
     double tol;           /* nevill relative tolerance (reference: 1e-6)     */
     long evals;           /* secular-function evaluations                    */
 } sd_model;
+
+/* A store into a real*4 model array; identity in exact-model mode. */
+static inline double rf(const sd_model *m, double x) { return m->f32 ? (double)(float)x : x; }
 
 /* sphere(), surfdisp96.f:480-547 */
 static void sd_sphere(sd_model *m, int ifunc, int iflag)
@@ -122,22 +126,22 @@ static void sd_sphere(sd_model *m, int ifunc, int iflag)
     const double ar = 6370.0;
     double dr = 0.0, r0 = ar;
     int n = m->mmax;
-    m->d[n - 1] = 1.0f;
+    m->d[n - 1] = 1.0;
     if (iflag == 0) {
         for (int i = 0; i < n; ++i) {
             m->dtp[i] = m->d[i];
             m->rtp[i] = m->rho[i];
         }
         for (int i = 0; i < n; ++i) {
-            dr = dr + (double)m->d[i];
+            dr = dr + m->d[i];
             double r1 = ar - dr;
             double z0 = ar * log(ar / r0);
             double z1 = ar * log(ar / r1);
-            m->d[i] = (float)(z1 - z0);
+            m->d[i] = rf(m, z1 - z0);
             double tmp = (ar + ar) / (r0 + r1);
-            m->a[i] = (float)((double)m->a[i] * tmp);
-            m->b[i] = (float)((double)m->b[i] * tmp);
-            m->btp[i] = (float)tmp;
+            m->a[i] = rf(m, m->a[i] * tmp);
+            m->b[i] = rf(m, m->b[i] * tmp);
+            m->btp[i] = rf(m, tmp);
             r0 = r1;
         }
         m->dhalf = m->d[n - 1];
@@ -145,15 +149,22 @@ static void sd_sphere(sd_model *m, int ifunc, int iflag)
         m->d[n - 1] = m->dhalf;
         for (int i = 0; i < n; ++i) {
             if (ifunc == 1) {
-                /* btp**(-5): integer power, expanded then inverted */
-                float x = m->btp[i], x2 = x * x, x5 = (x2 * x) * x2;
-                m->rho[i] = m->rtp[i] * (1.0f / x5);
+                if (m->f32) {
+                    /* btp**(-5): integer power, expanded then inverted */
+                    float x = (float)m->btp[i], x2 = x * x, x5 = (x2 * x) * x2;
+                    m->rho[i] = (double)((float)m->rtp[i] * (1.0f / x5));
+                } else {
+                    m->rho[i] = m->rtp[i] * pow(m->btp[i], -5.0);
+                }
+            } else if (ifunc == 2) {
+                if (m->f32)
+                    m->rho[i] = (double)((float)m->rtp[i] * powf((float)m->btp[i], -2.275f));
+                else
+                    m->rho[i] = m->rtp[i] * pow(m->btp[i], (double)-2.275f);
             }
-            else if (ifunc == 2)
-                m->rho[i] = m->rtp[i] * powf(m->btp[i], -2.275f);
         }
     }
-    m->d[n - 1] = 0.0f;
+    m->d[n - 1] = 0.0;
 }
 
 /* gtsolh(), surfdisp96.f:361-382: Rayleigh speed of a half-space, float.   */
@@ -484,15 +495,16 @@ static int sd_getsol(sd_model *m, double t1, double *c1p, double clow,
  * evaluation count of each period.  round_f32 = 1 reproduces the reference
  * output cg(k) = sngl(c(k)); 0 returns the unrounded double root.
  * Returns 0, or the 1-based index of the first period with no root.       */
-int or_surfdisp96_ex(const float *thkm, const float *vpm, const float *vsm,
-                     const float *rhom, int nlayer, int iflsph, int iwave,
-                     int mode, int igr, int kmax, const double *t, double *cg,
-                     double tol, int round_f32, int *evals_per_period)
+static int sd_run(const double *thkm, const double *vpm, const double *vsm,
+                  const double *rhom, int nlayer, int iflsph, int iwave, int mode,
+                  int igr, int kmax, const double *t, double *cg, double tol,
+                  int model_f32, int round_f32, int *evals_per_period)
 {
     if (nlayer < 1 || nlayer > NL || kmax < 1 || kmax > NP) return -1;
     sd_model mdl;
     sd_model *m = &mdl;
     m->mmax = nlayer;
+    m->f32 = model_f32 ? 1 : 0;
     m->tol = tol;
     m->evals = 0;
     m->del1st = 0.0;
@@ -503,18 +515,19 @@ int or_surfdisp96_ex(const float *thkm, const float *vpm, const float *vsm,
     if (iwave == 1) idispl = kmax; else if (iwave == 2) idispr = kmax;
     const float ddc0 = 0.005f, sone0 = 1.500f, h0 = 0.005f;
     m->llw = 1;
-    if (m->b[0] <= 0.0f) m->llw = 2;
+    if (m->b[0] <= 0.0) m->llw = 2;
     const double one = 1.0e-2;
     if (iflsph == 1) sd_sphere(m, 0, 0);
     int jmn = 0, jsol = 1;
     float betmx = -1.e20f, betmn = 1.e20f;
     for (int i = 0; i < m->mmax; ++i) {
-        if (m->b[i] > 0.01f && m->b[i] < betmn) {
-            betmn = m->b[i]; jmn = i; jsol = 1;
-        } else if (m->b[i] <= 0.01f && m->a[i] < betmn) {
-            betmn = m->a[i]; jmn = i; jsol = 0;
+        float bi = (float)m->b[i], ai = (float)m->a[i];
+        if (bi > 0.01f && bi < betmn) {
+            betmn = bi; jmn = i; jsol = 1;
+        } else if (bi <= 0.01f && ai < betmn) {
+            betmn = ai; jmn = i; jsol = 0;
         }
-        if (m->b[i] > betmx) betmx = m->b[i];
+        if (bi > betmx) betmx = bi;
     }
     int first_fail = 0;
     double c[NP], cb[NP];
@@ -527,7 +540,7 @@ int or_surfdisp96_ex(const float *thkm, const float *vpm, const float *vsm,
         double onea = (double)sone;
         float cc1;
         if (jsol == 0) cc1 = betmn;
-        else cc1 = sd_gtsolh(m->a[jmn], m->b[jmn]);
+        else cc1 = sd_gtsolh((float)m->a[jmn], (float)m->b[jmn]);
         cc1 = 0.95f * cc1;
         cc1 = 0.90f * cc1;
         double cc = (double)cc1;
@@ -608,6 +621,19 @@ int or_surfdisp96_ex(const float *thkm, const float *vpm, const float *vsm,
     return first_fail;
 }
 
+int or_surfdisp96_ex(const float *thkm, const float *vpm, const float *vsm,
+                     const float *rhom, int nlayer, int iflsph, int iwave,
+                     int mode, int igr, int kmax, const double *t, double *cg,
+                     double tol, int round_f32, int *evals_per_period)
+{
+    double d[NL], a[NL], b[NL], r[NL];
+    if (nlayer < 1 || nlayer > NL) return -1;
+    for (int i = 0; i < nlayer; ++i) { d[i] = thkm[i]; a[i] = vpm[i]; b[i] = vsm[i]; r[i] = rhom[i]; }
+    /* the reference model is real*4 whatever the output rounding */
+    return sd_run(d, a, b, r, nlayer, iflsph, iwave, mode, igr, kmax, t, cg, tol, 1,
+                  round_f32, evals_per_period);
+}
+
 int or_surfdisp96(const float *thkm, const float *vpm, const float *vsm,
                   const float *rhom, int nlayer, int iflsph, int iwave,
                   int mode, int igr, int kmax, const double *t, double *cg)
@@ -617,59 +643,115 @@ int or_surfdisp96(const float *thkm, const float *vpm, const float *vsm,
 }
 
 /* ------------------------------------------------------------------------ */
+/* Double-precision layer split for the exact-model mode (same arithmetic as
+ * or_refine without real*4 stores).                                         */
+static int refine_d(double minthk0, int nz, const double *dep, const double *vp,
+                    const double *vs, const double *rho, double *rthk, double *rvp,
+                    double *rvs, double *rrho)
+{
+    int k = 0;
+    for (int i = 0; i < nz - 1; ++i) {
+        /* the sublayer count uses the real*4 rule so the layering is the
+         * reference's */
+        float thkf = (float)dep[i + 1] - (float)dep[i];
+        int ns = (int)((thkf + 1.0e-4f) / (thkf / (float)minthk0)) + 1;
+        if (k + ns + 1 > NL) return -1;
+        double thk = dep[i + 1] - dep[i];
+        for (int j = 1; j <= ns; ++j) {
+            double f = (double)(2 * j - 1) / (double)(2 * ns);
+            rthk[k] = thk / ns;
+            rvp[k] = vp[i] + f * (vp[i + 1] - vp[i]);
+            rvs[k] = vs[i] + f * (vs[i + 1] - vs[i]);
+            rrho[k] = rho[i] + f * (rho[i + 1] - rho[i]);
+            ++k;
+        }
+    }
+    rthk[k] = 0.0; rvp[k] = vp[nz - 1]; rvs[k] = vs[nz - 1]; rrho[k] = rho[nz - 1];
+    return k + 1;
+}
+
 /* One column: pv plus central finite-difference kernels,
  * DepthKernel1D.f90:102-185.  vp/rho given explicitly (the reference's
- * depthkernel derives them from vs by Brocher first).  The perturbations
- * and divisors follow the Fortran single-precision arithmetic:
- *   vs_pert = vs -/+ 0.5*dln*vs   (float)
- *   sen     = (cg2 - cg1) / (dble)(dln*vs)                                 */
+ * depthkernel derives them from vs by Brocher first).
+ * precision 0 (the reference): real*4 model arithmetic, root to tol, output
+ *   sngl(c), perturbation and divisor in single precision:
+ *     vs_pert = vs -/+ 0.5*dln*vs  (float),  sen = (cg2 - cg1)/dble(dln*vs)
+ * precision 1: as 0 but the roots are not rounded to FP32;
+ * precision 2 (exact-model checker): the model pipeline in double, no FP32
+ *   stores anywhere, divisor = the exact step.  With a tight tol and a small
+ *   dln this resolves the derivative itself.                               */
 int or_column_fd(int nz, const float *vs, const float *vp, const float *rho,
                  int kmax, const double *periods, int iwave, int igr,
                  const float *depz, float minthk, float dlnvs, float dlnvp,
-                 float dlnrho, double tol, int round_f32, double *pv,
+                 float dlnrho, double tol, int precision, double *pv,
                  double *sen_vs, double *sen_vp, double *sen_rho,
                  long *evals)
 {
     if (kmax > NP || nz > NL || nz < 2) return -1;
-    float depm[NL], vpm[NL], vsm[NL], rhom[NL];
-    float rthk[NL], rvp[NL], rvs[NL], rrho[NL];
     double cg0[NP], cg1[NP], cg2[NP];
     int ev[NP];
     long tot = 0;
-    int rmax = or_refine(minthk, nz, depz, vp, vs, rho, rthk, rvp, rvs, rrho, NULL);
-    if (rmax < 0) return -2;
-    int st = or_surfdisp96_ex(rthk, rvp, rvs, rrho, rmax, 1, iwave, 1, igr,
-                              kmax, periods, cg0, tol, round_f32, ev);
-    for (int k = 0; k < kmax; ++k) { pv[k] = cg0[k]; tot += ev[k]; }
-    int status = st;
+    const int model_f32 = precision < 2, out_f32 = precision == 0;
+    double rthk[NL], rvp[NL], rvs[NL], rrho[NL];
+    float fthk[NL], fvp[NL], fvs[NL], frho[NL];
+    float depm[NL], vpm[NL], vsm[NL], rhom[NL];
+    double ddep[NL], dvp[NL], dvs[NL], drho[NL];
     for (int i = 0; i < nz; ++i) {
         depm[i] = depz[i]; vsm[i] = vs[i]; vpm[i] = vp[i]; rhom[i] = rho[i];
+        ddep[i] = depz[i]; dvs[i] = vs[i]; dvp[i] = vp[i]; drho[i] = rho[i];
     }
-    const float half = 0.5f;
+    /* model -> roots for the current node arrays */
+#define RUN_MODEL(CG)                                                                 \
+    do {                                                                              \
+        int rm_;                                                                      \
+        if (model_f32) {                                                              \
+            rm_ = or_refine(minthk, nz, depm, vpm, vsm, rhom, fthk, fvp, fvs, frho, NULL); \
+            if (rm_ < 0) return -2;                                                   \
+            for (int q_ = 0; q_ < rm_; ++q_) {                                        \
+                rthk[q_] = fthk[q_]; rvp[q_] = fvp[q_]; rvs[q_] = fvs[q_]; rrho[q_] = frho[q_]; \
+            }                                                                         \
+        } else {                                                                      \
+            rm_ = refine_d(minthk, nz, ddep, dvp, dvs, drho, rthk, rvp, rvs, rrho);   \
+            if (rm_ < 0) return -2;                                                   \
+        }                                                                             \
+        st_ = sd_run(rthk, rvp, rvs, rrho, rm_, 1, iwave, 1, igr, kmax, periods, CG,  \
+                     tol, model_f32, out_f32, ev);                                    \
+        for (int k_ = 0; k_ < kmax; ++k_) tot += ev[k_];                              \
+    } while (0)
+    int st_ = 0;
+    RUN_MODEL(cg0);
+    const int status = st_;
+    for (int k = 0; k < kmax; ++k) pv[k] = cg0[k];
     for (int i = 0; i < nz; ++i) {
-        /* three parameters, each perturbed down then up */
         for (int par = 0; par < 3; ++par) {
             float *arr = par == 0 ? vsm : (par == 1 ? vpm : rhom);
+            double *darr = par == 0 ? dvs : (par == 1 ? dvp : drho);
             const float *base = par == 0 ? vs : (par == 1 ? vp : rho);
             float dln = par == 0 ? dlnvs : (par == 1 ? dlnvp : dlnrho);
             double *sen = par == 0 ? sen_vs : (par == 1 ? sen_vp : sen_rho);
-            float delta = (half * dln) * base[i];
-            arr[i] = base[i] - delta;
-            rmax = or_refine(minthk, nz, depm, vpm, vsm, rhom, rthk, rvp, rvs, rrho, NULL);
-            or_surfdisp96_ex(rthk, rvp, rvs, rrho, rmax, 1, iwave, 1, igr, kmax,
-                             periods, cg1, tol, round_f32, ev);
-            for (int k = 0; k < kmax; ++k) tot += ev[k];
-            arr[i] = base[i] + delta;
-            rmax = or_refine(minthk, nz, depm, vpm, vsm, rhom, rthk, rvp, rvs, rrho, NULL);
-            or_surfdisp96_ex(rthk, rvp, rvs, rrho, rmax, 1, iwave, 1, igr, kmax,
-                             periods, cg2, tol, round_f32, ev);
-            for (int k = 0; k < kmax; ++k) tot += ev[k];
-            arr[i] = base[i];
-            double div = (double)(dln * base[i]);
+            double div;
+            if (model_f32) {
+                const float delta = (0.5f * dln) * base[i];
+                arr[i] = base[i] - delta;
+                RUN_MODEL(cg1);
+                arr[i] = base[i] + delta;
+                RUN_MODEL(cg2);
+                arr[i] = base[i];
+                div = (double)(dln * base[i]);
+            } else {
+                const double delta = 0.5 * (double)dln * (double)base[i];
+                darr[i] = (double)base[i] - delta;
+                RUN_MODEL(cg1);
+                darr[i] = (double)base[i] + delta;
+                RUN_MODEL(cg2);
+                darr[i] = base[i];
+                div = 2.0 * delta;
+            }
             for (int k = 0; k < kmax; ++k)
                 sen[(size_t)i * kmax + k] = (cg2[k] - cg1[k]) / div;
         }
     }
+#undef RUN_MODEL
     if (evals) *evals = tot;
     return status;
 }
@@ -679,6 +761,8 @@ int or_column_fd(int nz, const float *vs, const float *vp, const float *rho,
  * vel is (nx,ny,nz) Fortran order; outputs are (nx*ny,kmax[,nz]) Fortran
  * order, written only for the selected columns.  vp_in/rho_in, when not
  * NULL, replace the Brocher relations (same layout as vel).
+ * dln is the relative step (the reference uses 0.01, CalSurfG.f90:33-35);
+ * precision as in or_column_fd (0 = the reference).
  * status_out (may be NULL, length nx*ny) receives the 1-based first failing
  * period per column, 0 when every period has a root.                       */
 int or_depthkernel(int nx, int ny, int nz, const float *vel,
@@ -686,12 +770,12 @@ int or_depthkernel(int nx, int ny, int nz, const float *vel,
                    double *sen_vs, double *sen_vp, double *sen_rho, int iwave,
                    int igr, int kmax, const double *tRc, const float *depz,
                    float minthk, int col_start, int col_count, int nthreads,
-                   double tol, int round_f32, int *status_out, long *evals_out)
+                   double tol, int precision, float dln, int *status_out, long *evals_out)
 {
     if (nx < 1 || ny < 1 || nz < 2 || nz > NL || kmax < 1 || kmax > NP) return -1;
     const long ncol = (long)nx * ny;
     if (col_start < 1 || col_count < 0 || col_start - 1 + (long)col_count > ncol) return -1;
-    const float dln = 0.01f;
+    if (!(dln > 0.0f)) dln = 0.01f;   /* CalSurfG.f90:33-35 */
     long total_evals = 0;
     int bad = 0;
 #ifdef _OPENMP
@@ -713,7 +797,7 @@ int or_depthkernel(int nx, int ny, int nz, const float *vel,
         }
         long ev = 0;
         int st = or_column_fd(nz, vs, vp, rho, kmax, tRc, iwave, igr, depz,
-                              minthk, dln, dln, dln, tol, round_f32, pv, svs,
+                              minthk, dln, dln, dln, tol, precision, pv, svs,
                               svp, srh, &ev);
         if (st < 0) bad |= 1;
         total_evals += ev;

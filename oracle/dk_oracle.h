@@ -19,14 +19,15 @@ int or_surfdisp96_ex(const float *thkm, const float *vpm, const float *vsm,
 int or_column_fd(int nz, const float *vs, const float *vp, const float *rho,
                  int kmax, const double *periods, int iwave, int igr,
                  const float *depz, float minthk, float dlnvs, float dlnvp,
-                 float dlnrho, double tol, int round_f32, double *pv,
+                 float dlnrho, double tol, int precision, double *pv,
                  double *sen_vs, double *sen_vp, double *sen_rho, long *evals);
 int or_depthkernel(int nx, int ny, int nz, const float *vel,
                    const float *vp_in, const float *rho_in, double *pvRc,
                    double *sen_vs, double *sen_vp, double *sen_rho, int iwave,
                    int igr, int kmax, const double *tRc, const float *depz,
                    float minthk, int col_start, int col_count, int nthreads,
-                   double tol, int round_f32, int *status_out, long *evals_out);
+                   double tol, int precision, float dln, int *status_out,
+                   long *evals_out);
 int or_phase(int nx, int ny, int nz, const float *vel, const float *vp_in,
              const float *rho_in, double *pvRc, int iwave, int igr, int kmax,
              const double *tRc, const float *depz, float minthk, int nthreads,

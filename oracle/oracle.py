@@ -53,7 +53,7 @@ def lib():
                                      _f64p, _f64p, _f64p, _f64p, ctypes.c_int, ctypes.c_int,
                                      ctypes.c_int, _f64p, _f32p, ctypes.c_float, ctypes.c_int,
                                      ctypes.c_int, ctypes.c_int, ctypes.c_double, ctypes.c_int,
-                                     _i32p, _i64p]
+                                     ctypes.c_float, _i32p, _i64p]
         L.or_depthkernel.restype = ctypes.c_int
         L.or_phase.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p,
                                _f64p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f64p, _f32p,
@@ -120,8 +120,13 @@ def surfdisp96(thk, vp, vs, rho, periods, iwave=2, igr=0, mode=1, iflsph=1,
 
 def depthkernel(vel, depz, periods, minthk, vp=None, rho=None, iwave=2, igr=0,
                 col_start=1, col_count=None, nthreads=0, tol=1e-6, round_f32=True,
-                kernels=True):
+                kernels=True, dln=0.01, exact=False):
     """Oracle of ``depthkernel`` (CalSurfG.f90:1-113, default_fortran_fd).
+
+    round_f32=False keeps the roots unrounded; exact=True runs the whole model
+    pipeline in double (no real*4 stores) with the exact FD step, which with a
+    tight tol and small dln resolves the derivative itself (a checker, not the
+    reference's arithmetic).
 
     Returns dict with pvRc (nxy,K), sen_vs/sen_vp/sen_rho (nxy,K,nz) F-order,
     status (nxy,) and evals (total secular evaluations).
@@ -150,7 +155,9 @@ def depthkernel(vel, depz, periods, minthk, vp=None, rho=None, iwave=2, igr=0,
                                  _p(pv, _f64p), _p(svs, _f64p), _p(svp, _f64p), _p(srh, _f64p),
                                  iwave, igr, K, _p(t, _f64p), _p(depz, _f32p),
                                  ctypes.c_float(minthk), col_start, col_count, nthreads, tol,
-                                 int(round_f32), _p(status, _i32p), ctypes.byref(ev))
+                                 2 if exact else (0 if round_f32 else 1), ctypes.c_float(dln),
+                                 _p(status, _i32p),
+                                 ctypes.byref(ev))
         if r != 0:
             raise RuntimeError(f"oracle depthkernel failed ({r})")
         return dict(pvRc=pv, sen_vs=svs, sen_vp=svp, sen_rho=srh, status=status,
