@@ -634,6 +634,14 @@ int or_surfdisp96_ex(const float *thkm, const float *vpm, const float *vsm,
                   round_f32, evals_per_period);
 }
 
+/* Exact-model variant (checker): double model arrays, no real*4 stores. */
+int or_surfdisp96_d(const double *thkm, const double *vpm, const double *vsm,
+                    const double *rhom, int nlayer, int iflsph, int kmax,
+                    const double *t, double *cg, double tol)
+{
+    return sd_run(thkm, vpm, vsm, rhom, nlayer, iflsph, 2, 1, 0, kmax, t, cg, tol, 0, 0, NULL);
+}
+
 int or_surfdisp96(const float *thkm, const float *vpm, const float *vsm,
                   const float *rhom, int nlayer, int iflsph, int iwave,
                   int mode, int igr, int kmax, const double *t, double *cg)

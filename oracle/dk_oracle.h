@@ -32,6 +32,26 @@ int or_phase(int nx, int ny, int nz, const float *vel, const float *vp_in,
              const float *rho_in, double *pvRc, int iwave, int igr, int kmax,
              const double *tRc, const float *depz, float minthk, int nthreads,
              double tol, int round_f32, int *evals_cp, int *status_out);
+int or_surfdisp96_d(const double *thkm, const double *vpm, const double *vsm,
+                    const double *rhom, int nlayer, int iflsph, int kmax,
+                    const double *t, double *cg, double tol);
+int or_tregn96(int nl, const float *d_in, const float *TA_in, const float *TC_in,
+               const float *TF_in, const float *TL_in, const float *TN_in,
+               const float *TRho_in, const float *qai_in, const float *qbi_in,
+               const float *etapi_in, const float *etasi_in, const float *frefpi_in,
+               const float *frefsi_in, int nt, const float *t_in, const float *cp_in,
+               float *dcdah_out, float *dcdbv_out, float *dcdn_out);
+int or_tregn96_ex(int nl, const float *d_in, const float *TA_in, const float *TC_in,
+                  const float *TF_in, const float *TL_in, const float *TN_in,
+                  const float *TRho_in, const float *qai_in, const float *qbi_in,
+                  const float *etapi_in, const float *etasi_in, const float *frefpi_in,
+                  const float *frefsi_in, int nt, const float *t_in, const float *cp_in,
+                  float *dcdah_out, float *dcdbv_out, float *dcdn_out, int nsph, int dogam,
+                  double *full);
+int or_depthkernelTI(int nx, int ny, int nz, const float *vel, const float *vp_in,
+                     const float *rho_in, double *pvRc, int iwave, int igr, int kmax,
+                     const double *tRc, const float *depz, float minthk, float *Lsen,
+                     int col_start, int col_count, int nthreads, int *status_out);
 #ifdef __cplusplus
 }
 #endif

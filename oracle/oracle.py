@@ -70,6 +70,11 @@ def lib():
                                      _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p,
                                      ctypes.c_int, _f32p, _f32p, _f32p, _f32p, _f32p]
             L.or_tregn96.restype = ctypes.c_int
+            L.or_tregn96_ex.argtypes = L.or_tregn96.argtypes + [ctypes.c_int, ctypes.c_int, _f64p]
+            L.or_tregn96_ex.restype = ctypes.c_int
+        L.or_surfdisp96_d.argtypes = [_f64p, _f64p, _f64p, _f64p, ctypes.c_int, ctypes.c_int,
+                                      ctypes.c_int, _f64p, _f64p, ctypes.c_double]
+        L.or_surfdisp96_d.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -197,3 +202,39 @@ def depthkernel_ti(vel, depz, periods, minthk, vp=None, rho=None, iwave=2, igr=0
     if r != 0:
         raise RuntimeError(f"oracle depthkernelTI failed ({r})")
     return dict(pvRc=pv, Lsen_Gsc=lsen, status=status)
+
+
+def surfdisp96_d(thk, vp, vs, rho, periods, iflsph=1, tol=1e-13):
+    """Exact-model surfdisp96 (double model arrays, unrounded roots): a
+    checker for derivatives, not the reference's arithmetic."""
+    a = [np.ascontiguousarray(x, np.float64) for x in (thk, vp, vs, rho)]
+    t = np.ascontiguousarray(periods, np.float64)
+    cg = np.zeros(t.size)
+    st = lib().or_surfdisp96_d(*[_p(x, _f64p) for x in a], a[0].size, iflsph, t.size,
+                               _p(t, _f64p), _p(cg, _f64p), tol)
+    return cg, st
+
+
+def tregn96(thk, TA, TC, TF, TL, TN, rho, periods, cp, nsph=1, dogam=1, full=False):
+    """tregn96 partials (dcdah, dcdbv, dcdn as (K, nl) float32); with
+    full=True also the FP64 partials [K, 7, nl] (ah, av, bh, bv, n, r, and
+    c after the Q shift in [:, 6, 0])."""
+    nl = len(thk)
+    f = lambda x: np.ascontiguousarray(x, np.float32)  # noqa: E731
+    arr = [f(thk), f(TA), f(TC), f(TF), f(TL), f(TN), f(rho)]
+    qp = np.full(nl, 150.0, np.float32)
+    qs = np.full(nl, 50.0, np.float32)
+    z = np.zeros(nl, np.float32)
+    one = np.ones(nl, np.float32)
+    t = f(periods)
+    c = f(cp)
+    K = t.size
+    out = [np.zeros((K, nl), np.float32) for _ in range(3)]
+    fb = np.zeros((K, 7, nl)) if full else None
+    r = lib().or_tregn96_ex(nl, *[_p(x, _f32p) for x in arr], _p(qp, _f32p), _p(qs, _f32p),
+                            _p(z, _f32p), _p(z, _f32p), _p(one, _f32p), _p(one, _f32p), K,
+                            _p(t, _f32p), _p(c, _f32p), *[_p(o, _f32p) for o in out],
+                            int(nsph), int(dogam), _p(fb, _f64p))
+    if r != 0:
+        raise RuntimeError("oracle tregn96 failed")
+    return (tuple(out) + (fb,)) if full else tuple(out)
