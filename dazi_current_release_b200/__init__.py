@@ -4,8 +4,10 @@ kernels, computed by hand-written sm_100a CUDA kernels behind a C-ABI
 (include/dazi_dk.h).  The Python side mirrors the reference's Fortran
 interfaces `depthkernel` and `depthkernelTI`.
 """
-from .depthkernel import depthkernel, depthkernel_vpvsrho, DepthKernelError  # noqa: F401
+from .depthkernel import (depthkernel, depthkernel_vpvsrho, depthkernelTI,  # noqa: F401
+                          depthkernel_fused, DepthKernelError)
 from ._lib import DaziError, FORM_PLAIN, FORM_ADJOINT  # noqa: F401
 
-__all__ = ["depthkernel", "depthkernel_vpvsrho", "DepthKernelError", "DaziError",
+__all__ = ["depthkernel", "depthkernel_vpvsrho", "depthkernelTI", "depthkernel_fused",
+           "DepthKernelError", "DaziError",
            "FORM_PLAIN", "FORM_ADJOINT"]

@@ -23,6 +23,7 @@ DAZI_ERR_CUDA = -3
 DAZI_ERR_TIMEOUT = -4
 DAZI_ERR_NOMEM = -5
 DAZI_ERR_NODEVICE = -6
+DAZI_ERR_MODEL = -7
 FORM_PLAIN = 0
 FORM_ADJOINT = 1
 
@@ -30,6 +31,7 @@ FORM_ADJOINT = 1
 EXPORTS = (
     "dazi_dk_iso", "dazi_dk_iso_vpvsrho", "dazi_dk_last_status", "dazi_dk_iso_dev",
     "dazi_dk_last_error", "dazi_dk_version", "dazi_dk_finalize", "dazi_dk_fp64_peak", "dazi_dk_last_work",
+    "dazi_dk_ti", "dazi_dk_fused", "dazi_dk_fused_dev", "dazi_dk_last_launches",
 )
 
 
@@ -71,6 +73,16 @@ def load(build_if_missing: bool = True):
     L.dazi_dk_iso_dev.argtypes = [_int, _int, _int, vp_, vp_, vp_, vp_, vp_, vp_, vp_, _int, vp_,
                                   vp_, ctypes.c_float, _int, _int, _int, vp_, vp_]
     L.dazi_dk_iso_dev.restype = _int
+    L.dazi_dk_ti.argtypes = [ip, ip, ip, fp, _f64p, ip, ip, ip, _f64p, fp, fp, fp, _int, _int]
+    L.dazi_dk_ti.restype = _int
+    L.dazi_dk_fused.argtypes = [ip, ip, ip, fp, fp, fp, _f64p, _f64p, _f64p, _f64p, fp, ip, ip, ip,
+                                _f64p, fp, fp, _int, _int, _int]
+    L.dazi_dk_fused.restype = _int
+    L.dazi_dk_fused_dev.argtypes = [_int, _int, _int, vp_, vp_, vp_, vp_, vp_, vp_, vp_, vp_, _int,
+                                    vp_, vp_, ctypes.c_float, _int, _int, _int, vp_, vp_]
+    L.dazi_dk_fused_dev.restype = _int
+    L.dazi_dk_last_launches.argtypes = []
+    L.dazi_dk_last_launches.restype = _int
     L.dazi_dk_last_error.argtypes = []
     L.dazi_dk_last_error.restype = ctypes.c_char_p
     L.dazi_dk_version.argtypes = []

@@ -34,6 +34,7 @@ struct BuildArgs {
     const float* rho;
     float4* layers;      // [rmax][ncols] flattened (d, a, b, rho)
     LayerD* layersd;     // [rmax][ncols] FP64 per-layer constants
+    float4* tilayers;    // [rmax][ncols] unflattened refined (vp, vs, rho), or nullptr
 };
 
 struct RootArgs {
@@ -65,6 +66,20 @@ struct AdjArgs {
 };
 
 __global__ void adjoint_kernel(AdjArgs a);
+
+struct TiArgs {
+    const Geometry* geo;
+    int nz, kmax;
+    long long ncol, col0, ncols;
+    const float4* tilayers; // [rmax][ncols] refined (vp, vs, rho)
+    const double* periods;
+    const double* pv;       // (ncol, K) phase velocities (FP32-valued)
+    float* lsen;            // (ncol, K, nz-1) Fortran layout
+    double* scratch;        // [rmax*6][grid threads]
+    int* errflag;           // set to 1 when an Lsen_Gsc value is not finite
+};
+
+__global__ void ti_kernel(TiArgs a);
 
 __global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);
 __global__ void fd_column_kernel(FdArgs a);

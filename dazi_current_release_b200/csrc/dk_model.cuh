@@ -38,6 +38,12 @@ struct Geometry {
     float rhofac[NL];        // btp**(-2.275) in single precision
     double tmp[NL];          // flattening velocity factor in double
     float rthk[NL];          // refined thickness before flattening
+    // tregn96's own flattening of the TI model (R = 6371 km,
+    // tregn96.f:774-841) and its sphericity factors (bldsph, :1301-1383)
+    float tdflat[NL];        // flattened thickness (0 for the half-space)
+    double f275[NL];         // tmp**(-0.275): moduli A, C, L, N
+    double f2275[NL];        // tmp**(-2.275): density
+    float vtp[NL];           // partial-derivative velocity factor
 };
 
 // ---------------------------------------------------------------- Brocher
@@ -110,6 +116,34 @@ __device__ inline int build_geometry(Geometry& g, const float* depz, int nz, flo
         // powf(btp, -2.275f), formed in double and rounded once
         g.rhofac[m] = (float)pow((double)btp, (double)(-2.275f));
         r0 = r1;
+    }
+    // sphere_tdisp96(): radius 6371 (a real*4 constant), the half-space
+    // again entered with thickness 1
+    {
+        const double ar2 = (double)6371.0f;
+        double q0 = ar2;
+        for (int m = 0; m < rmax; ++m) {
+            const float dm = (m == rmax - 1) ? 1.0f : g.rthk[m];
+            const double q1 = __dsub_rn(q0, (double)dm);
+            const double z0 = __dmul_rn(ar2, log(__ddiv_rn(ar2, q0)));
+            const double z1 = __dmul_rn(ar2, log(__ddiv_rn(ar2, q1)));
+            const float td = (float)__dsub_rn(z1, z0);
+            g.tdflat[m] = (m == rmax - 1) ? 0.0f : td;
+            const double t2 = __ddiv_rn(__dadd_rn(ar2, ar2), __dadd_rn(q0, q1));
+            g.f2275[m] = pow(t2, (double)(-2.275f));
+            g.f275[m] = pow(t2, (double)(-0.2750f));
+            // bldsph() reads the flattened thickness, the half-space as 1
+            g.vtp[m] = td;   // temporary: flattened thickness incl. half-space
+            q0 = q1;
+        }
+        const double ar = 6370.0;
+        double p0 = ar;
+        for (int m = 0; m < rmax; ++m) {
+            const double zd = (m == rmax - 1) ? 1.0 : (double)g.vtp[m];
+            const double p1 = __dmul_rn(p0, exp(-__ddiv_rn(zd, ar)));
+            g.vtp[m] = (float)__ddiv_rn(__dadd_rn(ar, ar), __dadd_rn(p0, p1));
+            p0 = p1;
+        }
     }
     return rmax;
 }

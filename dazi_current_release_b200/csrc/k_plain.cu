@@ -201,6 +201,18 @@ __global__ void build_layers_kernel(BuildArgs a)
         const float4 L = flat_layer(*g, m, vp, vs, rho);
         a.layers[(long long)m * a.ncols + c] = L;
         a.layersd[(long long)m * a.ncols + c] = make_layerd(L);
+        if (a.tilayers) {
+            const int i = g->node[m];
+            float4 t;
+            if (m == g->rmax - 1) { t.x = vp[i]; t.y = vs[i]; t.z = rho[i]; }
+            else {
+                t.x = sublayer_value(vp[i], vp[i + 1], g->sub[m], g->den[m]);
+                t.y = sublayer_value(vs[i], vs[i + 1], g->sub[m], g->den[m]);
+                t.z = sublayer_value(rho[i], rho[i + 1], g->sub[m], g->den[m]);
+            }
+            t.w = 0.0f;
+            a.tilayers[(long long)m * a.ncols + c] = t;
+        }
     }
 }
 

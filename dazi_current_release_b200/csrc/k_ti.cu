@@ -1,0 +1,793 @@
+// Gc/Gs (azimuthal anisotropy) depth kernel Lsen_Gsc on the GPU.
+//
+// Reference: depthkernelTI (code/src_inv_iso_joint/depthkernelTI.f90:86-169)
+// turns each column into a transversely isotropic layer stack
+// (TA = TC = rho Vp^2, TL = TN = rho Vs^2, TF = TA - 2 TL, Q = 150/50) and
+// calls CPS tregn96 (tregn96.f:52-722) with the surfdisp96 phase velocities.
+// tregn96 computes the Rayleigh eigenfunctions at that velocity -- a complex
+// compound-matrix up-sweep (up, dnka_tregn) combined with a Haskell
+// down-sweep (down, hska) -- then the variational partials from layer energy
+// integrals (energy, intijr), the attenuation shift of c (gammap) and the
+// sphericity factors (sprayl).  The splice then forms, per depth interval j,
+//     Lsen_Gsc(j) = sum_{sublayers k of j} dc/dA_k TA_k + dc/dL_k TL_k.
+//
+// One thread owns one (column, period).  The eigenvalues of an isotropic
+// input layer are real (their discriminant is (omega^2 (1/Vs^2 - 1/Vp^2))^2),
+// so the up- and down-sweeps run in real arithmetic: an oscillatory layer
+// (negative eigenvalue, imaginary vertical wavenumber) maps onto cos/sin
+// forms exactly as tregn96's complex varsv evaluates them.  Only the energy
+// integrals, where the eigenvector matrices carry imaginary wavenumbers,
+// use complex arithmetic.  The up-sweep's compound vectors go to a global
+// scratch slot per thread ([layer][slot], coalesced); the down-sweep builds
+// eigenfunctions and energy integrals interface by interface and stores the
+// raw partials in the same slots for the final normalised splice.
+#include "dk_secular.cuh"
+#include "dk_kernels.cuh"
+
+namespace dk {
+
+// ------------------------------------------------------------ complex
+struct zc { double re, im; };
+__device__ __forceinline__ zc Z(double r, double i = 0.0) { return {r, i}; }
+__device__ __forceinline__ zc operator+(zc a, zc b) { return {a.re + b.re, a.im + b.im}; }
+__device__ __forceinline__ zc operator-(zc a, zc b) { return {a.re - b.re, a.im - b.im}; }
+__device__ __forceinline__ zc operator-(zc a) { return {-a.re, -a.im}; }
+__device__ __forceinline__ zc operator*(zc a, zc b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
+__device__ __forceinline__ zc operator*(double s, zc a) { return {s * a.re, s * a.im}; }
+__device__ __forceinline__ zc zdiv(zc a, zc b)
+{
+    if (fabs(b.re) >= fabs(b.im)) {
+        const double r = b.im / b.re, den = b.re + b.im * r;
+        return {(a.re + a.im * r) / den, (a.im - a.re * r) / den};
+    }
+    const double r = b.re / b.im, den = b.re * r + b.im;
+    return {(a.re * r + a.im) / den, (a.im * r - a.re) / den};
+}
+__device__ __forceinline__ double zabs(zc a) { return hypot(a.re, a.im); }
+__device__ __forceinline__ zc zsqrt(zc a)
+{
+    // principal square root (branch cut on the negative real axis)
+    const double m = hypot(a.re, a.im);
+    double re = sqrt(0.5 * (m + fabs(a.re)));
+    if (re == 0.0) return Z(0.0, 0.0);
+    double im = a.im / (2.0 * re);
+    if (a.re < 0.0) { const double t = fabs(im); im = copysign(re, a.im); re = t; }
+    return {re, im};
+}
+__device__ __forceinline__ zc zexp(zc a)
+{
+    double s, c;
+    sincos(a.im, &s, &c);
+    const double e = exp(a.re);
+    return {e * c, e * s};
+}
+
+// ------------------------------------------------------- TI layer model
+// Flattened TI values of one layer as tregn96 holds them (real*4 stores).
+struct TiLayer {
+    double d, TA, TC, TF, TL, TN, rho;
+};
+
+// Column refined values (unflattened) -> tregn96's model of layer m.
+__device__ __forceinline__ TiLayer ti_layer(const Geometry& g, int m, float rvp, float rvs, float rrh)
+{
+    // depthkernelTI.f90:124-131 (real*4)
+    const float TA = __fmul_rn(rrh, __fmul_rn(rvp, rvp));
+    const float TL = __fmul_rn(rrh, __fmul_rn(rvs, rvs));
+    const float TF = __fsub_rn(TA, __fmul_rn(2.0f, TL));
+    // sphere_tdisp96 (tregn96.f:796-834): TF is not mapped
+    TiLayer o;
+    o.d = (double)g.tdflat[m];
+    o.rho = (double)(float)__dmul_rn((double)rrh, g.f2275[m]);
+    o.TA = (double)(float)__dmul_rn((double)TA, g.f275[m]);
+    o.TC = o.TA;
+    o.TL = (double)(float)__dmul_rn((double)TL, g.f275[m]);
+    o.TN = o.TL;
+    o.TF = (double)TF;
+    return o;
+}
+
+// gettiegn() (tregn96.f:3166-3361) for real eigenvalues.  rp/rsv are the
+// vertical wavenumbers: a non-negative real value, or (osc = true) the
+// magnitude of an imaginary one.
+struct TiEig {
+    double x11, x21, x31, x41, x12, x22, x32, x42, np, nsv;
+    double rp, rsv;
+    bool oscp, oscs;
+    bool ok;
+};
+
+// The same with complex eigenvectors and wavenumbers (general case).
+struct TiEigZ {
+    zc x11, x21, x31, x41, x12, x22, x32, x42, np, nsv, rp, rsv;
+};
+
+__device__ __forceinline__ void ti_eigen(const TiLayer& L, double omg, double wvn, double wvno2, TiEig& o)
+{
+    const double TA = L.TA, TC = L.TC, TF = L.TF, TL = L.TL, TRho = L.rho;
+    const double om2 = omg * omg;
+    const double a = wvn * TF / TC, b = 1.0 / TC;
+    const double c = -TRho * om2 + wvn * wvn * (TA - TF * TF / TC);
+    const double d = -wvn, e = 1.0 / TL, f = -TRho * om2;
+    const double ddef = wvn * wvn - TRho * om2 / TL;
+    const double aabc = wvn * wvn * TA / TC - TRho * om2 / TC;
+    const double bb = 2.0 * a * d + e * c + f * b;
+    const double cc = ddef * aabc;
+    const double disc = bb * bb - 4.0 * cc;
+    o.ok = disc >= 0.0;
+    const double srt = sqrt(fmax(disc, 0.0));
+    double L1 = 0.5 * (bb + srt);
+    double L2 = fabs(L1) > 0.0 ? cc / L1 : 0.5 * (bb - srt);
+    if (fabs(wvno2 - L2) < fabs(wvno2 - L1)) { const double t = L1; L1 = L2; L2 = t; }
+    o.oscp = L1 < 0.0;
+    o.oscs = L2 < 0.0;
+    o.rp = sqrt(fabs(L1));
+    o.rsv = sqrt(fabs(L2));
+    const double bcaa = b * c + a * a, ddef2 = d * d + e * f;
+    double x12 = b * d - a * e;
+    double x22 = b * L2 - e * bcaa;
+    double x32 = L2 - (a * d + c * e);
+    double x42 = -a * L2 + d * bcaa;
+    double x11 = -e * L1 + b * ddef2;
+    double x21 = b * d - a * e;
+    double x31 = d * L1 - a * ddef2;
+    double x41 = -(L1 - a * d - b * f);
+    if (wvn != 0.0) {
+        const double z1 = wvn / x11;
+        x11 *= z1; x21 *= z1; x31 *= z1; x41 *= z1;
+        const double z2 = wvn / x22;
+        x12 *= z2; x22 *= z2; x32 *= z2; x42 *= z2;
+    }
+    o.x11 = x11; o.x21 = x21; o.x31 = x31; o.x41 = x41;
+    o.x12 = x12; o.x22 = x22; o.x32 = x32; o.x42 = x42;
+    o.np = x11 * x41 - x21 * x31;
+    o.nsv = x12 * x42 - x22 * x32;
+}
+
+// varsv() (tregn96.f:3363-3475) on the real representation.
+struct TiVar {
+    double cosp, rsinp, sinpr, cosq, rsinq, sinqr, pex, svex;
+};
+
+__device__ __forceinline__ void ti_var_one(double r, bool osc, double dm, double& cosf,
+                                           double& rsin, double& sinr, double& ex)
+{
+    if (!osc) {
+        const double pr = r * dm;
+        ex = pr;
+        const double fac = pr < 15.0 ? exp(-2.0 * pr) : 0.0;
+        cosf = 0.5 * (1.0 + fac);
+        const double sn = 0.5 * (1.0 - fac);
+        rsin = r * sn;
+        sinr = (fabs(pr) < 1.0e-5 && r < 1.0e-5) ? dm : sn / r;
+    } else {
+        const double pi = r * dm;
+        ex = 0.0;
+        double sn, cs;
+        sincos(pi, &sn, &cs);
+        cosf = cs;
+        rsin = -r * sn;                               // (i r)(i sin)
+        sinr = (r < 1.0e-5) ? dm : sn / r;            // (i sin)/(i r)
+    }
+}
+
+// Compound-matrix element tables of dnka_tregn (tregn96.f:1992-2987): each
+// needed element tca(I,J) is a signed sum of x(a,k)x(b,k) x(c,l)x(d,l) times
+// trig factors of modes k and l (f: 0 = cos, 1 = sin/r, 2 = r sin,
+// 3 = the exact same-mode value 4 a_k^2 exp(-ex)), in two groups subtracted.
+struct TT { signed char sg, a, b, k, c, d, l, fk, fl, grp; };
+__constant__ TT c_tt[70] = {
+    // tca(1,1) 0..5
+    {-1,1,3,1,2,4,1,3,3,0}, {-1,1,4,1,2,3,2,0,0,0}, {-1,1,4,2,2,3,1,0,0,0},
+    {+1,1,3,1,2,4,2,1,1,0}, {+1,1,3,2,2,4,1,2,2,0}, {-1,1,3,2,2,4,2,3,3,0},
+    // tca(1,2) 6..9
+    {-1,1,4,1,2,2,2,0,1,0}, {-1,1,4,2,2,2,1,0,2,0}, {-1,1,2,1,2,4,2,0,1,1}, {-1,1,2,2,2,4,1,0,2,1},
+    // tca(1,3) 10..15
+    {+1,1,4,1,2,1,1,3,3,0}, {+1,1,4,1,1,2,2,0,0,0}, {+1,1,4,2,2,1,1,0,0,0},
+    {-1,1,1,1,2,4,2,1,1,0}, {-1,1,1,2,2,4,1,2,2,0}, {+1,1,4,2,1,2,2,3,3,0},
+    // tca(1,5) 16..19
+    {-1,1,3,1,1,2,2,1,0,0}, {-1,1,3,2,2,1,1,2,0,0}, {-1,1,1,1,2,3,2,1,0,1}, {-1,1,1,2,2,3,1,2,0,1},
+    // tca(1,6) 20..25
+    {-1,1,2,1,1,2,2,0,0,0}, {-1,1,2,2,2,1,1,0,0,0}, {+1,1,1,1,2,2,2,1,1,0},
+    {+1,1,1,2,2,2,1,2,2,0}, {-1,1,2,1,2,1,1,3,3,0}, {-1,1,2,2,1,2,2,3,3,0},
+    // tca(2,1) 26..29
+    {-1,1,4,1,3,3,2,0,2,0}, {-1,1,4,2,3,3,1,0,1,0}, {-1,1,3,1,3,4,2,1,0,1}, {-1,1,3,2,3,4,1,2,0,1},
+    // tca(2,2) 30..33
+    {-1,1,4,1,3,2,2,0,0,0}, {+1,1,2,1,3,4,2,0,0,0}, {-1,1,4,2,3,2,1,0,0,0}, {+1,1,2,2,3,4,1,0,0,0},
+    // tca(2,3) 34..37
+    {+1,1,4,1,3,1,2,0,2,0}, {+1,1,4,2,3,1,1,0,1,0}, {+1,1,1,1,3,4,2,1,0,1}, {+1,1,1,2,3,4,1,2,0,1},
+    // tca(2,5) 38..41
+    {-1,1,3,1,3,1,2,1,2,0}, {-1,1,3,2,3,1,1,2,1,0}, {-1,1,1,1,3,3,2,1,2,1}, {-1,1,1,2,3,3,1,2,1,1},
+    // tca(3,1) 42..47
+    {-1,1,4,1,4,3,2,0,0,0}, {-1,1,4,2,4,3,1,0,0,0}, {+1,1,3,2,4,4,1,2,2,0},
+    {+1,1,3,1,4,4,2,1,1,0}, {-1,1,4,1,4,3,1,3,3,0}, {-1,1,4,2,4,3,2,3,3,0},
+    // tca(3,2) 48..51
+    {-1,1,4,1,4,2,2,0,1,0}, {-1,1,4,2,4,2,1,0,2,0}, {-1,1,2,1,4,4,2,0,1,1}, {-1,1,2,2,4,4,1,0,2,1},
+    // tca(3,3) 52..57
+    {+1,1,4,1,4,1,2,0,0,0}, {+1,1,4,2,4,1,1,0,0,0}, {-1,1,1,1,4,4,2,1,1,0},
+    {-1,1,1,2,4,4,1,2,2,0}, {+1,1,4,1,4,1,1,3,3,0}, {+1,1,4,2,4,1,2,3,3,0},
+    // tca(5,1) 58..61
+    {-1,2,4,1,4,3,2,2,0,0}, {-1,2,4,2,4,3,1,1,0,0}, {-1,2,3,1,4,4,2,0,1,1}, {-1,2,3,2,4,4,1,0,2,1},
+    // tca(5,2) 62..65
+    {-1,2,4,1,4,2,2,2,1,0}, {-1,2,4,2,4,2,1,1,2,0}, {+1,2,2,1,4,4,2,2,1,0}, {+1,2,2,2,4,4,1,1,2,0},
+    // tca(6,1) 66..71 -> only 4 slots left: stored in c_tt61 below
+};
+__constant__ TT c_tt61[6] = {
+    {-1,3,4,1,4,3,2,0,0,0}, {-1,3,4,2,4,3,1,0,0,0}, {+1,3,3,1,4,4,2,1,1,0},
+    {+1,3,3,2,4,4,1,2,2,0}, {-1,3,4,1,4,3,1,3,3,0}, {-1,3,4,2,4,3,2,3,3,0}};
+
+// element order: t11 t12 t13 t15 t16 t21 t22 t23 t25 t31 t32 t33 t51 t52 (t61)
+__constant__ unsigned char c_tt_off[15] = {0, 6, 10, 16, 20, 26, 30, 34, 38, 42, 48, 52, 58, 62, 66};
+
+__device__ __forceinline__ double tca_sum(int lo, int hi, const TT* tab, const double xs[5][3],
+                                          const double fac[3][4])
+{
+    double g0 = 0.0, g1 = 0.0;
+    for (int i = lo; i < hi; ++i) {
+        const TT t = tab[i];
+        double v = (xs[t.a][t.k] * xs[t.b][t.k]) * (xs[t.c][t.l] * xs[t.d][t.l]);
+        if (t.sg < 0) v = -v;
+        v = (t.fk == 3) ? v * fac[t.k][3] : (v * fac[t.k][t.fk]) * fac[t.l][t.fl];
+        if (t.grp) g1 += v; else g0 += v;
+    }
+    return g0 - g1;
+}
+
+// dnka_tregn (elastic) in real arithmetic: the reduced 5x5 compound matrix.
+__device__ __forceinline__ void ti_compound(const TiEig& E, const TiVar& v, double ca[5][5])
+{
+    const double ex = v.pex + v.svex;
+    const double dfac = ex > 35.0 ? 0.0 : exp(-ex);
+    const double a1 = 0.5 / E.np, a2 = 0.5 / E.nsv;
+    double fac[3][4];
+    fac[1][0] = 2.0 * a1 * v.cosp; fac[1][1] = 2.0 * a1 * v.sinpr; fac[1][2] = 2.0 * a1 * v.rsinp;
+    fac[1][3] = 4.0 * a1 * a1 * dfac;
+    fac[2][0] = 2.0 * a2 * v.cosq; fac[2][1] = 2.0 * a2 * v.sinqr; fac[2][2] = 2.0 * a2 * v.rsinq;
+    fac[2][3] = 4.0 * a2 * a2 * dfac;
+    double xs[5][3];
+    xs[1][1] = E.x11; xs[2][1] = E.x21; xs[3][1] = E.x31; xs[4][1] = E.x41;
+    xs[1][2] = E.x12; xs[2][2] = E.x22; xs[3][2] = E.x32; xs[4][2] = E.x42;
+    double t[15];
+#pragma unroll
+    for (int q = 0; q < 14; ++q) t[q] = tca_sum(c_tt_off[q], q == 13 ? 66 : c_tt_off[q + 1], c_tt, xs, fac);
+    t[14] = tca_sum(0, 6, c_tt61, xs, fac);
+    const double t11 = t[0], t12 = t[1], t13 = t[2], t15 = t[3], t16 = t[4], t21 = t[5];
+    const double t22 = t[6], t23 = t[7], t25 = t[8], t31 = t[9], t32 = t[10], t33 = t[11];
+    const double t51 = t[12], t52 = t[13], t61 = t[14];
+    ca[0][0] = t11; ca[0][1] = t12; ca[0][2] = t13; ca[0][3] = t15; ca[0][4] = t16;
+    ca[1][0] = t21; ca[1][1] = t22; ca[1][2] = t23; ca[1][3] = t25; ca[1][4] = t15;
+    ca[2][0] = 2.0 * t31; ca[2][1] = 2.0 * t32; ca[2][2] = 2.0 * t33 - dfac;
+    ca[2][3] = -2.0 * t23; ca[2][4] = -2.0 * t13;
+    ca[3][0] = t51; ca[3][1] = t52; ca[3][2] = -t32; ca[3][3] = t22; ca[3][4] = t12;
+    ca[4][0] = t61; ca[4][1] = t51; ca[4][2] = -t31; ca[4][3] = t21; ca[4][4] = t11;
+}
+
+// E and E^-1 of a layer (evalg, tregn96.f:3055-3105) as complex matrices.
+__device__ __forceinline__ void ti_emat(const TiEigZ& E, zc e[4][4], zc ei[4][4])
+{
+    const zc rp = E.rp, rsv = E.rsv;
+    const zc x11 = E.x11, x21 = E.x21, x31 = E.x31, x41 = E.x41;
+    const zc x12 = E.x12, x22 = E.x22, x32 = E.x32, x42 = E.x42;
+    const zc d1 = (2.0 * rp) * E.np, d2 = (2.0 * rsv) * E.nsv;
+    const zc i1 = zdiv(Z(1.0), d1), i2 = zdiv(Z(1.0), d2);   // 1/(2 rp NP), 1/(2 rsv NSV)
+    ei[0][0] = (x41 * rp) * i1;    ei[1][0] = x42 * i2;
+    ei[2][0] = (x41 * rp) * i1;    ei[3][0] = -(x42 * i2);
+    ei[0][1] = -(x31 * i1);        ei[1][1] = -((x32 * rsv) * i2);
+    ei[2][1] = x31 * i1;           ei[3][1] = -((x32 * rsv) * i2);
+    ei[0][2] = -((x21 * rp) * i1); ei[1][2] = -(x22 * i2);
+    ei[2][2] = -((x21 * rp) * i1); ei[3][2] = x22 * i2;
+    ei[0][3] = x11 * i1;           ei[1][3] = (x12 * rsv) * i2;
+    ei[2][3] = -(x11 * i1);        ei[3][3] = (x12 * rsv) * i2;
+    e[0][0] = x11; e[1][0] = x21 * rp; e[2][0] = x31; e[3][0] = x41 * rp;
+    e[0][1] = x12 * rsv; e[1][1] = x22; e[2][1] = x32 * rsv; e[3][1] = x42;
+    e[0][2] = x11; e[1][2] = -(x21 * rp); e[2][2] = x31; e[3][2] = -(x41 * rp);
+    e[0][3] = -(x12 * rsv); e[1][3] = x22; e[2][3] = -(x32 * rsv); e[3][3] = x42;
+}
+
+__device__ __forceinline__ void eig_to_z(const TiEig& E, TiEigZ& o)
+{
+    o.x11 = Z(E.x11); o.x21 = Z(E.x21); o.x31 = Z(E.x31); o.x41 = Z(E.x41);
+    o.x12 = Z(E.x12); o.x22 = Z(E.x22); o.x32 = Z(E.x32); o.x42 = Z(E.x42);
+    o.np = Z(E.np); o.nsv = Z(E.nsv);
+    o.rp = E.oscp ? Z(0.0, E.rp) : Z(E.rp);
+    o.rsv = E.oscs ? Z(0.0, E.rsv) : Z(E.rsv);
+}
+
+// ffunc/gfunc/h1func/h2func (tregn96.f:1385-1473)
+__device__ __forceinline__ zc ti_f(zc nub, double dm)
+{
+    if (zabs(nub) < 1.0e-08) return Z(dm);
+    const zc arg = dm * nub;
+    const zc ex = arg.re < 40.0 ? zexp(-2.0 * arg) : Z(0.0);
+    return zdiv(Z(1.0) - ex, 2.0 * nub);
+}
+__device__ __forceinline__ zc ti_g(zc nub, double dm)
+{
+    const zc arg = dm * nub;
+    return arg.re < 75.0 ? dm * zexp(-arg) : Z(0.0);
+}
+__device__ __forceinline__ zc ti_h1(zc nua, zc nub, double dm)
+{
+    const zc s = nub + nua;
+    if (zabs(s) < 1.0e-08) return Z(dm);
+    const zc arg = dm * s;
+    const zc ex = arg.re < 40.0 ? zexp(-arg) : Z(0.0);
+    return zdiv(Z(1.0) - ex, s);
+}
+__device__ __forceinline__ zc ti_h2(zc nua, zc nub, double dm)
+{
+    if (zabs(nub - nua) < 1.0e-08) return Z(dm);
+    const zc ap = dm * nua, aq = dm * nub;
+    const zc ep = ap.re < 40.0 ? zexp(-ap) : Z(0.0);
+    const zc eq = aq.re < 40.0 ? zexp(-aq) : Z(0.0);
+    return zdiv(eq - ep, nua - nub);
+}
+
+// The six energy integrals of a layer (intijr, tregn96.f:4073-4245):
+// (1,1) (1,3) (2,2) (2,4) (3,3) (4,4).  top/bot = (ur, uz, tz, tr) at the
+// layer's top and bottom interface; half = the lower half-space.
+__device__ __forceinline__ void ti_integrals(const TiEigZ& E, double dm, const double top[4],
+                                             const double bot[4], bool half, double out[6])
+{
+    zc e[4][4], ei[4][4];
+    ti_emat(E, e, ei);
+    const zc ra = E.rp, rb = E.rsv;
+    auto pot = [&](int r, const double u[4]) {
+        return (u[0] * ei[r][0] + u[1] * ei[r][1]) + (u[2] * ei[r][2] + u[3] * ei[r][3]);
+    };
+    const zc km1pd = pot(2, top), km1sd = pot(3, top);
+    constexpr int IJ[6][2] = {{0, 0}, {0, 2}, {1, 1}, {1, 3}, {2, 2}, {3, 3}};
+    if (!half) {
+        const zc kmpu = pot(0, bot), kmsu = pot(1, bot);
+        const zc FA = ti_f(ra, dm), GA = ti_g(ra, dm), FB = ti_f(rb, dm), GB = ti_g(rb, dm);
+        const zc H1 = ti_h1(ra, rb, dm), H2 = ti_h2(ra, rb, dm);
+        const zc pu2 = kmpu * kmpu, pd2 = km1pd * km1pd, su2 = kmsu * kmsu, sd2 = km1sd * km1sd;
+        const zc pusu = kmpu * kmsu, pdsd = km1pd * km1sd, pusd = kmpu * km1sd, pdsu = km1pd * kmsu;
+        const zc pupd = kmpu * km1pd, susd = kmsu * km1sd;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const int i = IJ[q][0], j = IJ[q][1];
+            auto EE = [&](int a, int b) { return e[i][a] * e[j][b]; };
+            auto SY = [&](int a, int b) { return EE(a, b) + EE(b, a); };
+            zc r = (EE(0, 0) * pu2) * FA;
+            r = r + (EE(2, 2) * pd2) * FA;
+            r = r + (EE(1, 1) * su2) * FB;
+            r = r + (EE(3, 3) * sd2) * FB;
+            r = r + H1 * (SY(0, 1) * pusu + SY(2, 3) * pdsd);
+            r = r + H2 * (SY(0, 3) * pusd + SY(1, 2) * pdsu);
+            r = r + GA * (SY(0, 2) * pupd);
+            r = r + GB * (SY(1, 3) * susd);
+            out[q] = r.re;
+        }
+    } else {
+        const zc pd2 = km1pd * km1pd, sd2 = km1sd * km1sd, pdsd = km1pd * km1sd;
+        const zc i2a = zdiv(Z(1.0), 2.0 * ra), iab = zdiv(Z(1.0), ra + rb), i2b = zdiv(Z(1.0), 2.0 * rb);
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+            const int i = IJ[q][0], j = IJ[q][1];
+            auto EE = [&](int a, int b) { return e[i][a] * e[j][b]; };
+            zc r = (EE(2, 2) * pd2) * i2a;
+            r = r + ((EE(2, 3) + EE(3, 2)) * pdsd) * iab;
+            r = r + (EE(3, 3) * sd2) * i2b;
+            out[q] = r.re;
+        }
+    }
+}
+
+// ----------------------------------------------------- complex layer path
+// A layer whose TI eigenvalues form a complex-conjugate pair (deep layers
+// at short periods, where tregn96's flattening leaves F unmapped and eta
+// departs from 1).  The layer's propagators are real by construction; as in
+// tregn96 the compound and Haskell matrices are formed in complex arithmetic
+// and their real parts carried on.
+__device__ void ti_eigen_z(const TiLayer& L, double omg, double wvn, double wvno2, TiEigZ& o)
+{
+    const double TA = L.TA, TC = L.TC, TF = L.TF, TL = L.TL, TRho = L.rho;
+    const double om2 = omg * omg;
+    const zc a = Z(wvn * TF / TC), b = Z(1.0 / TC);
+    const zc c = Z(-TRho * om2 + wvn * wvn * (TA - TF * TF / TC));
+    const zc d = Z(-wvn), e = Z(1.0 / TL), f = Z(-TRho * om2);
+    const zc ddef = Z(wvn * wvn - TRho * om2 / TL);
+    const zc aabc = Z(wvn * wvn * TA / TC - TRho * om2 / TC);
+    const zc bb = (2.0 * (a * d) + e * c) + f * b;
+    const zc cc = ddef * aabc;
+    zc srt = zsqrt(bb * bb - 4.0 * cc);
+    if (srt.im < 0.0) srt = -srt;
+    zc L1, L2;
+    if (bb.re < 0.0 && srt.re < 0.0) {
+        L2 = 0.5 * (bb - srt);
+        L1 = zabs(L2) > 0.0 ? zdiv(cc, L2) : 0.5 * (bb + srt);
+    } else {
+        L1 = 0.5 * (bb + srt);
+        L2 = zabs(L1) > 0.0 ? zdiv(cc, L1) : 0.5 * (bb - srt);
+    }
+    if (zabs(Z(wvno2) - L2) < zabs(Z(wvno2) - L1)) { const zc t = L1; L1 = L2; L2 = t; }
+    zc rp = zsqrt(L1), rsv = zsqrt(L2);
+    if (rp.re < 0.0) rp = -rp;
+    if (rsv.re < 0.0) rsv = -rsv;
+    const zc bcaa = b * c + a * a, ddef2 = d * d + e * f;
+    zc x12 = b * d - a * e;
+    zc x22 = b * L2 - e * bcaa;
+    zc x32 = L2 - (a * d + c * e);
+    zc x42 = -(a * L2) + d * bcaa;
+    zc x11 = -(e * L1) + b * ddef2;
+    zc x21 = b * d - a * e;
+    zc x31 = d * L1 - a * ddef2;
+    zc x41 = -((L1 - a * d) - b * f);
+    if (wvn != 0.0) {
+        const zc z1 = zdiv(Z(wvn), x11);
+        x11 = x11 * z1; x21 = x21 * z1; x31 = x31 * z1; x41 = x41 * z1;
+        const zc z2 = zdiv(Z(wvn), x22);
+        x12 = x12 * z2; x22 = x22 * z2; x32 = x32 * z2; x42 = x42 * z2;
+    }
+    o.x11 = x11; o.x21 = x21; o.x31 = x31; o.x41 = x41;
+    o.x12 = x12; o.x22 = x22; o.x32 = x32; o.x42 = x42;
+    o.np = x11 * x41 - x21 * x31;
+    o.nsv = x12 * x42 - x22 * x32;
+    o.rp = rp;
+    o.rsv = rsv;
+}
+
+struct TiVarZ {
+    zc cosp, rsinp, sinpr, cosq, rsinq, sinqr;
+    double pex, svex;
+};
+
+__device__ __forceinline__ void ti_var_z_one(zc r, double dm, zc& cosf, zc& rsin, zc& sinr, double& ex)
+{
+    const zc p = dm * r;
+    ex = p.re;
+    double sn, cs;
+    sincos(p.im, &sn, &cs);
+    const zc ep = Z(cs / 2.0, sn / 2.0), em = Z(ep.re, -ep.im);
+    const double fac = p.re < 15.0 ? exp(-2.0 * p.re) : 0.0;
+    cosf = ep + fac * em;
+    const zc s = ep - fac * em;
+    rsin = r * s;
+    sinr = (fabs(p.re) < 1.0e-5 && zabs(r) < 1.0e-5) ? Z(dm) : zdiv(s, r);
+}
+
+__device__ void ti_compound_z(const TiEigZ& E, const TiVarZ& v, double ca[5][5])
+{
+    const double ex = v.pex + v.svex;
+    const double dfac = ex > 35.0 ? 0.0 : exp(-ex);
+    const zc a1 = zdiv(Z(0.5), E.np), a2 = zdiv(Z(0.5), E.nsv);
+    zc fac[3][4];
+    fac[1][0] = (2.0 * a1) * v.cosp; fac[1][1] = (2.0 * a1) * v.sinpr; fac[1][2] = (2.0 * a1) * v.rsinp;
+    fac[1][3] = (4.0 * dfac) * (a1 * a1);
+    fac[2][0] = (2.0 * a2) * v.cosq; fac[2][1] = (2.0 * a2) * v.sinqr; fac[2][2] = (2.0 * a2) * v.rsinq;
+    fac[2][3] = (4.0 * dfac) * (a2 * a2);
+    zc xs[5][3];
+    xs[1][1] = E.x11; xs[2][1] = E.x21; xs[3][1] = E.x31; xs[4][1] = E.x41;
+    xs[1][2] = E.x12; xs[2][2] = E.x22; xs[3][2] = E.x32; xs[4][2] = E.x42;
+    double t[15];
+    for (int q = 0; q < 15; ++q) {
+        const TT* tab = q < 14 ? c_tt : c_tt61;
+        const int lo = q < 14 ? c_tt_off[q] : 0;
+        const int hi = q < 13 ? c_tt_off[q + 1] : (q == 13 ? 66 : 6);
+        zc g0 = Z(0.0), g1 = Z(0.0);
+        for (int i = lo; i < hi; ++i) {
+            const TT tt = tab[i];
+            zc w = (xs[tt.a][tt.k] * xs[tt.b][tt.k]) * (xs[tt.c][tt.l] * xs[tt.d][tt.l]);
+            if (tt.sg < 0) w = -w;
+            w = (tt.fk == 3) ? w * fac[tt.k][3] : (w * fac[tt.k][tt.fk]) * fac[tt.l][tt.fl];
+            if (tt.grp) g1 = g1 + w; else g0 = g0 + w;
+        }
+        t[q] = (g0 - g1).re;
+    }
+    const double t11 = t[0], t12 = t[1], t13 = t[2], t15 = t[3], t16 = t[4], t21 = t[5];
+    const double t22 = t[6], t23 = t[7], t25 = t[8], t31 = t[9], t32 = t[10], t33 = t[11];
+    const double t51 = t[12], t52 = t[13], t61 = t[14];
+    ca[0][0] = t11; ca[0][1] = t12; ca[0][2] = t13; ca[0][3] = t15; ca[0][4] = t16;
+    ca[1][0] = t21; ca[1][1] = t22; ca[1][2] = t23; ca[1][3] = t25; ca[1][4] = t15;
+    ca[2][0] = 2.0 * t31; ca[2][1] = 2.0 * t32; ca[2][2] = 2.0 * t33 - dfac;
+    ca[2][3] = -2.0 * t23; ca[2][4] = -2.0 * t13;
+    ca[3][0] = t51; ca[3][1] = t52; ca[3][2] = -t32; ca[3][3] = t22; ca[3][4] = t12;
+    ca[4][0] = t61; ca[4][1] = t51; ca[4][2] = -t31; ca[4][3] = t21; ca[4][4] = t11;
+}
+
+__device__ void ti_haskell_z(const TiEigZ& E, const TiVarZ& V, double v[4], double& cpex)
+{
+    double fp = 1.0, fs = 1.0;
+    if (V.pex > V.svex) {
+        const double dd = V.pex - V.svex;
+        fs = dd > 40.0 ? 0.0 : exp(-dd);
+        cpex = V.pex;
+    } else {
+        const double dd = V.svex - V.pex;
+        fp = dd > 40.0 ? 0.0 : exp(-dd);
+        cpex = V.svex;
+    }
+    const zc cosp = zdiv(fp * V.cosp, E.np), sinpr = zdiv(fp * V.sinpr, E.np), rsinp = zdiv(fp * V.rsinp, E.np);
+    const zc cossv = zdiv(fs * V.cosq, E.nsv), sinsvr = zdiv(fs * V.sinqr, E.nsv), rsinsv = zdiv(fs * V.rsinq, E.nsv);
+    const zc x11 = E.x11, x21 = E.x21, x31 = E.x31, x41 = E.x41;
+    const zc x12 = E.x12, x22 = E.x22, x32 = E.x32, x42 = E.x42;
+    double A[4][4];
+    A[0][0] = ((x11 * x41) * cosp + (x12 * x42) * cossv).re;
+    A[0][1] = (-((x11 * x31) * sinpr) - (x12 * x32) * rsinsv).re;
+    A[0][2] = (-((x11 * x21) * cosp) - (x12 * x22) * cossv).re;
+    A[0][3] = ((x11 * x11) * sinpr + (x12 * x12) * rsinsv).re;
+    A[1][0] = ((x21 * x41) * rsinp + (x22 * x42) * sinsvr).re;
+    A[1][1] = (-((x21 * x31) * cosp) - (x22 * x32) * cossv).re;
+    A[1][2] = (-((x21 * x21) * rsinp) - (x22 * x22) * sinsvr).re;
+    A[2][0] = ((x31 * x41) * cosp + (x32 * x42) * cossv).re;
+    A[2][1] = (-((x31 * x31) * sinpr) - (x32 * x32) * rsinsv).re;
+    A[3][0] = ((x41 * x41) * rsinp + (x42 * x42) * sinsvr).re;
+    A[1][3] = -A[0][2]; A[2][2] = A[1][1]; A[2][3] = -A[0][1];
+    A[3][1] = -A[2][0]; A[3][2] = -A[1][0]; A[3][3] = A[0][0];
+    double o[4];
+    for (int i = 0; i < 4; ++i) o[i] = A[i][0] * v[0] + A[i][1] * v[1] + A[i][2] * v[2] + A[i][3] * v[3];
+    for (int i = 0; i < 4; ++i) v[i] = o[i];
+}
+
+// Haskell matrix (hska, tregn96.f:3477-3559) applied to v: v <- AA v.
+__device__ __forceinline__ void ti_haskell(const TiEig& E, const TiVar& V, double v[4], double& cpex)
+{
+    double fp = 1.0, fs = 1.0;
+    if (V.pex > V.svex) {
+        const double dd = V.pex - V.svex;
+        fs = dd > 40.0 ? 0.0 : exp(-dd);
+        cpex = V.pex;
+    } else {
+        const double dd = V.svex - V.pex;
+        fp = dd > 40.0 ? 0.0 : exp(-dd);
+        cpex = V.svex;
+    }
+    const double inp = 1.0 / E.np, ins = 1.0 / E.nsv;
+    const double cosp = fp * V.cosp * inp, sinpr = fp * V.sinpr * inp, rsinp = fp * V.rsinp * inp;
+    const double cossv = fs * V.cosq * ins, sinsvr = fs * V.sinqr * ins, rsinsv = fs * V.rsinq * ins;
+    const double x11 = E.x11, x21 = E.x21, x31 = E.x31, x41 = E.x41;
+    const double x12 = E.x12, x22 = E.x22, x32 = E.x32, x42 = E.x42;
+    double A[4][4];
+    A[0][0] = x11 * x41 * cosp + x12 * x42 * cossv;
+    A[0][1] = -x11 * x31 * sinpr - x12 * x32 * rsinsv;
+    A[0][2] = -x11 * x21 * cosp - x12 * x22 * cossv;
+    A[0][3] = x11 * x11 * sinpr + x12 * x12 * rsinsv;
+    A[1][0] = x21 * x41 * rsinp + x22 * x42 * sinsvr;
+    A[1][1] = -x21 * x31 * cosp - x22 * x32 * cossv;
+    A[1][2] = -x21 * x21 * rsinp - x22 * x22 * sinsvr;
+    A[2][0] = x31 * x41 * cosp + x32 * x42 * cossv;
+    A[2][1] = -x31 * x31 * sinpr - x32 * x32 * rsinsv;
+    A[3][0] = x41 * x41 * rsinp + x42 * x42 * sinsvr;
+    A[1][3] = -A[0][2]; A[2][2] = A[1][1]; A[2][3] = -A[0][1];
+    A[3][1] = -A[2][0]; A[3][2] = -A[1][0]; A[3][3] = A[0][0];
+    double o[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) o[i] = A[i][0] * v[0] + A[i][1] * v[1] + A[i][2] * v[2] + A[i][3] * v[3];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = o[i];
+}
+
+// Max-norm scaling by a power of two (exact; the exponent is carried in
+// ex2 as a natural-log amount, like cnormc/rnormc's log(t1)).
+__device__ __forceinline__ double pow2_normalise(double* v, int n)
+{
+    double mx = 0.0;
+    for (int i = 0; i < n; ++i) mx = fmax(mx, fabs(v[i]));
+    if (!(mx > 1.0e-40)) return 0.0;
+    int ex;
+    frexp(mx, &ex);
+    for (int i = 0; i < n; ++i) v[i] = ldexp(v[i], -ex);
+    return (double)ex * 0.6931471805599453;
+}
+
+__device__ __forceinline__ void col_refined(const Geometry& g, int m, const float4* ti, long long stride,
+                                            float& rvp, float& rvs, float& rrh)
+{
+    const float4 t = ti[(long long)m * stride];
+    rvp = t.x; rvs = t.y; rrh = t.z;
+}
+
+__global__ void __launch_bounds__(128)
+ti_kernel(TiArgs a)
+{
+    __shared__ double s_per[NP];
+    for (int k = threadIdx.x; k < a.kmax; k += blockDim.x) s_per[k] = a.periods[k];
+    __syncthreads();
+    const Geometry& g = *a.geo;
+    const int rmax = g.rmax, nz = a.nz, K = a.kmax;
+    const long long nslots = (long long)gridDim.x * blockDim.x;
+    const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nitems = a.ncols * K;
+    const long long ncol = a.ncol;
+    for (long long base = (long long)blockIdx.x * blockDim.x; base < nitems; base += nslots) {
+        const long long it = base + threadIdx.x;
+        if (it >= nitems) continue;
+        const int k = (int)(it / a.ncols);
+        const long long c = it % a.ncols;
+        const long long post = a.col0 + c;
+        float* lout = a.lsen + post + ncol * (long long)k;
+        const long long jstride = ncol * (long long)K;
+        const float cpf = (float)a.pv[post + ncol * (long long)k];
+        if (!(cpf > 0.0f)) {
+            for (int j = 0; j < nz - 1; ++j) lout[jstride * j] = 0.0f;
+            continue;
+        }
+        const float4* ti = a.tilayers + c;
+        const long long ls = a.ncols;
+        double* scr = a.scratch + slot;          // [(m*6 + q)][nslots]
+        // tregn96.f:430-479: twopi real*4, t and cp real*4
+        const float twopi = 6.2831855f;
+        const double omega = (double)twopi / (double)(float)s_per[k];
+        const double wvno = omega / (double)cpf;
+        const double wvno2 = wvno * wvno;
+        // ---- up(): compound vectors from the half-space upward
+        double cdv[5];
+        double exsum = 0.0;
+        {
+            // half-space: E^-1 rows 1-2 and their 2x2 minors (evalg, up)
+            float rvp, rvs, rrh;
+            col_refined(g, rmax - 1, ti, ls, rvp, rvs, rrh);
+            const TiLayer L = ti_layer(g, rmax - 1, rvp, rvs, rrh);
+            TiEigZ E;
+            ti_eigen_z(L, omega, wvno, wvno2, E);
+            zc e[4][4], G[4][4];
+            ti_emat(E, e, G);
+            cdv[0] = (G[0][0] * G[1][1] - G[0][1] * G[1][0]).re;
+            cdv[1] = (G[0][0] * G[1][2] - G[0][2] * G[1][0]).re;
+            cdv[2] = (G[0][0] * G[1][3] - G[0][3] * G[1][0]).re;
+            cdv[3] = (G[0][1] * G[1][3] - G[0][3] * G[1][1]).re;
+            cdv[4] = (G[0][2] * G[1][3] - G[0][3] * G[1][2]).re;
+            double* sp = scr + (long long)(rmax - 1) * 6 * nslots;
+            for (int q = 0; q < 5; ++q) sp[q * nslots] = cdv[q];
+            sp[5 * nslots] = 0.0;
+        }
+        for (int m = rmax - 2; m >= 0; --m) {
+            float rvp, rvs, rrh;
+            col_refined(g, m, ti, ls, rvp, rvs, rrh);
+            const TiLayer L = ti_layer(g, m, rvp, rvs, rrh);
+            TiEig E;
+            ti_eigen(L, omega, wvno, wvno2, E);
+            double ca[5][5];
+            double pexsv;
+            if (E.ok) {
+                TiVar V;
+                ti_var_one(E.rp, E.oscp, L.d, V.cosp, V.rsinp, V.sinpr, V.pex);
+                ti_var_one(E.rsv, E.oscs, L.d, V.cosq, V.rsinq, V.sinqr, V.svex);
+                ti_compound(E, V, ca);
+                pexsv = V.pex + V.svex;
+            } else {
+                TiEigZ EZ;
+                ti_eigen_z(L, omega, wvno, wvno2, EZ);
+                TiVarZ VZ;
+                ti_var_z_one(EZ.rp, L.d, VZ.cosp, VZ.rsinp, VZ.sinpr, VZ.pex);
+                ti_var_z_one(EZ.rsv, L.d, VZ.cosq, VZ.rsinq, VZ.sinqr, VZ.svex);
+                ti_compound_z(EZ, VZ, ca);
+                pexsv = VZ.pex + VZ.svex;
+            }
+            double ee[5];
+#pragma unroll
+            for (int i = 0; i < 5; ++i)
+                ee[i] = cdv[0] * ca[0][i] + cdv[1] * ca[1][i] + cdv[2] * ca[2][i] + cdv[3] * ca[3][i] + cdv[4] * ca[4][i];
+            const double exn = pow2_normalise(ee, 5);
+            exsum = exsum + pexsv + exn;
+            double* sp = scr + (long long)m * 6 * nslots;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) { cdv[q] = ee[q]; sp[q * nslots] = ee[q]; }
+            sp[5 * nslots] = exsum;
+        }
+        // ---- down() + svfunc() + energy(): interface by interface
+        const double exe0 = exsum;     // exe(1)
+        const double f1213 = -cdv[1];
+        double top[4] = {cdv[2] / cdv[1], 1.0, 0.0, 0.0};   // ur, uz, tz, tr at the surface
+        double vv[4] = {1.0, 0.0, 0.0, 0.0};
+        double exa = 0.0;
+        double sumi0 = 0.0, sumi1 = 0.0, sumi2 = 0.0, gsum = 0.0;
+        const double pi_ = 3.141592653589493;   // gammap's constant, as in the reference
+        for (int m = 0; m < rmax; ++m) {
+            float rvp, rvs, rrh;
+            col_refined(g, m, ti, ls, rvp, rvs, rrh);
+            const TiLayer L = ti_layer(g, m, rvp, rvs, rrh);
+            TiEig E;
+            ti_eigen(L, omega, wvno, wvno2, E);
+            TiEigZ EZ;
+            if (E.ok) eig_to_z(E, EZ);
+            else ti_eigen_z(L, omega, wvno, wvno2, EZ);
+            double bot[4] = {0.0, 0.0, 0.0, 0.0};
+            const bool half = (m == rmax - 1);
+            if (!half) {
+                double cpex;
+                if (E.ok) {
+                    TiVar V;
+                    ti_var_one(E.rp, E.oscp, L.d, V.cosp, V.rsinp, V.sinpr, V.pex);
+                    ti_var_one(E.rsv, E.oscs, L.d, V.cosq, V.rsinq, V.sinqr, V.svex);
+                    ti_haskell(E, V, vv, cpex);
+                } else {
+                    TiVarZ VZ;
+                    ti_var_z_one(EZ.rp, L.d, VZ.cosp, VZ.rsinp, VZ.sinpr, VZ.pex);
+                    ti_var_z_one(EZ.rsv, L.d, VZ.cosq, VZ.rsinq, VZ.sinqr, VZ.svex);
+                    ti_haskell_z(EZ, VZ, vv, cpex);
+                }
+                const double ex2 = pow2_normalise(vv, 4);
+                exa = exa + cpex + ex2;
+                // eigenfunctions at interface m+1 (svfunc)
+                const double* sp = scr + (long long)(m + 1) * 6 * nslots;
+                const double cd1 = sp[0], cd2 = sp[nslots], cd3 = sp[2 * nslots];
+                const double cd4 = -cd3, cd5 = sp[3 * nslots], cd6 = sp[4 * nslots];
+                const double exe = sp[5 * nslots];
+                const double tz1 = -vv[3], tz2 = -vv[2], tz3 = vv[1], tz4 = vv[0];
+                const double uu1 = tz2 * cd6 - tz3 * cd5 + tz4 * cd4;
+                const double uu2 = -tz1 * cd6 + tz3 * cd3 - tz4 * cd2;
+                const double uu3 = tz1 * cd5 - tz2 * cd3 + tz4 * cd1;
+                const double uu4 = -tz1 * cd4 + tz2 * cd2 - tz3 * cd1;
+                const double ext = exa + exe - exe0;
+                if (ext > -80.0 && ext < 80.0) {
+                    const double fact = exp(ext) / f1213;
+                    bot[0] = uu1 * fact; bot[1] = uu2 * fact; bot[2] = uu3 * fact; bot[3] = uu4 * fact;
+                }
+            }
+            // energy integrals of layer m (typelyr 0, or 1 for the half-space)
+            double I[6];
+            ti_integrals(EZ, L.d, top, bot, half, I);
+            const double TA = L.TA, TC = L.TC, TF = L.TF, TL = L.TL, TN = L.TN, rho = L.rho;
+            const double ah = sqrt(TA / rho), av = sqrt(TC / rho), bh = sqrt(TN / rho), bv = sqrt(TL / rho);
+            const double eta = TF / (TA - 2.0 * TL);
+            const double a12 = -wvno, a14 = 1.0 / TL, a21 = wvno * TF / TC, a23 = 1.0 / TC;
+            const double URUR = I[0], UZUZ = I[2];
+            const double DURDUR = a12 * a12 * I[2] + 2.0 * a12 * a14 * I[3] + a14 * a14 * I[5];
+            const double DUZDUZ = a21 * a21 * I[0] + 2.0 * a21 * a23 * I[1] + a23 * a23 * I[4];
+            const double URDUZ = a21 * I[0] + a23 * I[1];
+            const double UZDUR = a12 * I[2] + a14 * I[3];
+            sumi0 += rho * (URUR + UZUZ);
+            sumi1 += TL * UZUZ + TA * URUR;
+            sumi2 += TL * UZDUR - TF * URDUZ;
+            const double facah = rho * ah * (URUR - 2.0 * eta * URDUZ / wvno);
+            const double facav = rho * av * DUZDUZ / wvno2;
+            const double facbv = rho * bv * (UZUZ + 2.0 * UZDUR / wvno + DURDUR / wvno2 + 4.0 * eta * URDUZ / wvno);
+            const double facn = -TF * URDUZ / (wvno * eta);
+            // gammap() (facbh = 0; Q = 150 / 50, reference frequency 1 Hz)
+            const double lw = log(omega / (2.0 * pi_ * 1.0)) / pi_;
+            gsum += lw * (facbv * bv * (double)(1.0f / 50.0f));
+            gsum += lw * ((facav * av + facah * ah) * (double)(1.0f / 150.0f));
+            (void)bh;
+            // raw partials for the splice (slot m is free: its compound
+            // vector was consumed one step earlier)
+            double* so = scr + (long long)m * 6 * nslots;
+            so[0] = facah; so[nslots] = facbv; so[2 * nslots] = facn;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) top[i] = bot[i];
+        }
+        // ---- normalisation, attenuation shift, sphericity, splice
+        const double ugr = (wvno * sumi1 + sumi2) / (omega * sumi0);
+        const double un = ugr * sumi0;
+        const double dcq = gsum / un;
+        const double cq = omega / wvno + dcq;
+        const double wq = omega / cq;
+        const double c2 = omega / wq;
+        const double tq = c2 / (2.0 * 6370.0 * omega);
+        const double tm = sqrt(1.0 + tq * tq);
+        const double tm3 = tm * tm * tm;
+        int m = 0;
+        for (int j = 0; j < nz - 1; ++j) {
+            float acc = 0.0f;
+            const int ns = g.nsub_of_node[j];
+            for (int q = 0; q < ns; ++q, ++m) {
+                float rvp, rvs, rrh;
+                col_refined(g, m, ti, ls, rvp, rvs, rrh);
+                const double* so = scr + (long long)m * 6 * nslots;
+                const double vt = (double)g.vtp[m];
+                double vah = so[0] / un * vt / tm3;
+                double vbv = so[nslots] / un * vt / tm3;
+                double vn = so[2 * nslots] / un;
+                const float dah = fabs(vah) < 1.0e-36 ? 0.0f : (float)vah;
+                const float dbv = fabs(vbv) < 1.0e-36 ? 0.0f : (float)vbv;
+                const float dn = fabs(vn) < 1.0e-36 ? 0.0f : (float)vn;
+                // depthkernelTI.f90:152-162 (real*4)
+                const float TA = __fmul_rn(rrh, __fmul_rn(rvp, rvp));
+                const float TL = __fmul_rn(rrh, __fmul_rn(rvs, rvs));
+                const float TF = __fmul_rn(1.0f, __fsub_rn(TA, __fmul_rn(2.0f, TL)));
+                const float den = __fsub_rn(TA, __fmul_rn(2.0f, TL));
+                const float den2 = __fmul_rn(den, den);
+                const float dA = __fsub_rn(__fmul_rn(__fdiv_rn(0.5f, __fmul_rn(rrh, rvp)), dah),
+                                           __fmul_rn(__fdiv_rn(TF, den2), dn));
+                const float dL = __fadd_rn(__fmul_rn(__fdiv_rn(0.5f, __fmul_rn(rrh, rvs)), dbv),
+                                           __fmul_rn(__fdiv_rn(__fmul_rn(2.0f, TF), den2), dn));
+                acc = __fadd_rn(__fadd_rn(acc, __fmul_rn(dA, TA)), __fmul_rn(dL, TL));
+            }
+            lout[jstride * j] = acc;
+            if (!isfinite(acc) && a.errflag) atomicOr(a.errflag, 1);
+        }
+    }
+}
+
+}  // namespace dk

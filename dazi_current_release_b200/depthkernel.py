@@ -113,6 +113,70 @@ def depthkernel_vpvsrho(nx, ny, nz, vel, vp, rho, iwave, igr, kmaxRc, tRc, depz,
                     col_start, col_count, kernels)
 
 
+def _run_fused(nx, ny, nz, vel, vp, rho, iwave, igr, kmaxRc, tRc, depz, minthk, form,
+               col_start, col_count, kernels, lsen, pvRc=None, sen=None, Lsen=None):
+    L = _lib.load()
+    vel = _f32(vel, (nx, ny, nz))
+    if vp is not None:
+        vp = _f32(vp, (nx, ny, nz))
+        rho = _f32(rho, (nx, ny, nz))
+    tRc = np.ascontiguousarray(tRc, dtype=np.float64)
+    depz = np.ascontiguousarray(depz, dtype=np.float32)
+    if tRc.size != kmaxRc or depz.size != nz:
+        raise ValueError("tRc must have kmaxRc entries and depz nz entries")
+    nxy = nx * ny
+    if col_count is None:
+        col_count = nxy - col_start + 1
+    if pvRc is None:
+        pvRc = np.zeros((nxy, kmaxRc), np.float64, order="F")
+    if kernels and sen is None:
+        sen = tuple(np.zeros((nxy, kmaxRc, nz), np.float64, order="F") for _ in range(3))
+    if lsen and Lsen is None:
+        Lsen = np.zeros((nxy, kmaxRc, nz - 1), np.float32, order="F")
+    f64p = ctypes.POINTER(ctypes.c_double)
+    f32p = ctypes.POINTER(ctypes.c_float)
+    ci = ctypes.c_int
+    rc = L.dazi_dk_fused(ctypes.byref(ci(nx)), ctypes.byref(ci(ny)), ctypes.byref(ci(nz)),
+                         _ptr(vel, f32p), _ptr(vp, f32p), _ptr(rho, f32p), _ptr(pvRc, f64p),
+                         *(tuple(_ptr(x, f64p) for x in sen) if kernels else (None,) * 3),
+                         _ptr(Lsen, f32p) if lsen else None,
+                         ctypes.byref(ci(iwave)), ctypes.byref(ci(igr)), ctypes.byref(ci(kmaxRc)),
+                         _ptr(tRc, f64p), _ptr(depz, f32p), ctypes.byref(ctypes.c_float(minthk)),
+                         int(col_start), int(col_count), int(form))
+    _lib.check(rc)
+    out = (pvRc,)
+    if kernels:
+        out += tuple(sen)
+    if lsen:
+        out += (Lsen,)
+    return out
+
+
+def depthkernelTI(nx, ny, nz, vel, iwave, igr, kmaxRc, tRc, depz, minthk, *, vp=None, rho=None,
+                  col_start=1, col_count=None):
+    """depthkernelTI(nx,ny,nz,vel,pvRc,iwave,igr,kmaxRc,tRc,depz,minthk,Lsen_Gsc)
+
+    code/src_inv_iso_joint/depthkernelTI.f90:2-193.  Returns
+    (pvRc, Lsen_Gsc): pvRc(nx*ny,kmaxRc) real*8 and Lsen_Gsc(nx*ny,kmaxRc,nz-1)
+    real*4, Fortran order.  DAZI_DEPTHKERNEL_TI_BACKEND must be unset or b200.
+    """
+    name = os.environ.get(ENV_TI, "").strip() or "b200"
+    if name not in ("b200", "b200_adjoint"):
+        raise DepthKernelError(9201, f"unknown Depth kernel TI backend {name!r}")
+    return _run_fused(nx, ny, nz, vel, vp, rho, iwave, igr, kmaxRc, tRc, depz, minthk,
+                      _lib.FORM_PLAIN, col_start, col_count, False, True)
+
+
+def depthkernel_fused(nx, ny, nz, vel, iwave, igr, kmaxRc, tRc, depz, minthk, *, vp=None,
+                      rho=None, form=None, col_start=1, col_count=None):
+    """Both stages with one phase-velocity pass: returns
+    (pvRc, sen_vsRc, sen_vpRc, sen_rhoRc, Lsen_Gsc)."""
+    if form is None:
+        form = resolve_form(ENV_ISO)
+    return _run_fused(nx, ny, nz, vel, vp, rho, iwave, igr, kmaxRc, tRc, depz, minthk, form,
+                      col_start, col_count, True, True)
+
+
 def last_status(nxy: int) -> np.ndarray:
     st = np.zeros(nxy, np.int32)
     _lib.check(_lib.load().dazi_dk_last_status(st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)),

@@ -47,6 +47,7 @@ extern "C" {
 #define DAZI_ERR_TIMEOUT  -4
 #define DAZI_ERR_NOMEM    -5
 #define DAZI_ERR_NODEVICE -6
+#define DAZI_ERR_MODEL    -7   /* non-finite kernel (degenerate layer)     */
 
 /* form selector */
 #define DAZI_FORM_PLAIN    0   /* perturb-and-recompute, as the reference */
@@ -74,6 +75,28 @@ int dazi_dk_iso_vpvsrho(const int *nx, const int *ny, const int *nz,
                         const float *depz, const float *minthk,
                         int col_start, int col_count, int form);
 
+/* Replaces depthkernelTI() of code/src_inv_iso_joint/depthkernelTI.f90:2-14
+ * (default_fortran_tregn96 backend, depthkernelTI.f90:86-169): pvRc and
+ * the Gc/Gs kernel Lsen_Gsc(nx*ny, kmaxRc, nz-1) of the column range.
+ * Periods without a root leave their Lsen_Gsc entries at zero. */
+int dazi_dk_ti(const int *nx, const int *ny, const int *nz, const float *vel,
+               double *pvRc, const int *iwave, const int *igr,
+               const int *kmaxRc, const double *tRc, const float *depz,
+               const float *minthk, float *Lsen_Gsc, int col_start,
+               int col_count);
+
+/* Both stages in one call: pvRc computed once (the reference computes it in
+ * depthkernelTI and again in depthkernel, CalSurfG_parallel.f90:1972-1975).
+ * vp/rho may be NULL (Brocher relations); sen_* may all be NULL; Lsen_Gsc
+ * may be NULL. */
+int dazi_dk_fused(const int *nx, const int *ny, const int *nz,
+                  const float *vel, const float *vp, const float *rho,
+                  double *pvRc, double *sen_vsRc, double *sen_vpRc,
+                  double *sen_rhoRc, float *Lsen_Gsc, const int *iwave,
+                  const int *igr, const int *kmaxRc, const double *tRc,
+                  const float *depz, const float *minthk, int col_start,
+                  int col_count, int form);
+
 /* Per-column status of the last call: first period (1-based) without a root,
  * 0 when all periods have one.  status has nx*ny entries; only the columns
  * of the last call's range are written.  Returns 0, or DAZI_ERR_BADARG if no
@@ -92,6 +115,18 @@ int dazi_dk_iso_dev(int nx, int ny, int nz, const float *vel, const float *vp,
                     const double *tRc, const float *depz, float minthk,
                     int col_start, int col_count, int form, int *status,
                     void *stream);
+
+/* Device-pointer form of dazi_dk_fused (same conventions as
+ * dazi_dk_iso_dev). */
+int dazi_dk_fused_dev(int nx, int ny, int nz, const float *vel, const float *vp,
+                      const float *rho, double *pvRc, double *sen_vsRc,
+                      double *sen_vpRc, double *sen_rhoRc, float *Lsen_Gsc,
+                      int kmaxRc, const double *tRc, const float *depz,
+                      float minthk, int col_start, int col_count, int form,
+                      int *status, void *stream);
+
+/* Number of kernel launches the last call issued (all on its stream). */
+int dazi_dk_last_launches(void);
 
 /* Work done by the last call, for roofline accounting: the number of
  * Rayleigh secular-function evaluations (each one a pass over the refined
