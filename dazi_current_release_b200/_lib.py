@@ -32,6 +32,7 @@ EXPORTS = (
     "dazi_dk_iso", "dazi_dk_iso_vpvsrho", "dazi_dk_last_status", "dazi_dk_iso_dev",
     "dazi_dk_last_error", "dazi_dk_version", "dazi_dk_finalize", "dazi_dk_fp64_peak", "dazi_dk_last_work",
     "dazi_dk_ti", "dazi_dk_fused", "dazi_dk_fused_dev", "dazi_dk_last_launches",
+    "dazi_dk_iso_noalloc_dev",
 )
 
 
@@ -81,6 +82,8 @@ def load(build_if_missing: bool = True):
     L.dazi_dk_fused_dev.argtypes = [_int, _int, _int, vp_, vp_, vp_, vp_, vp_, vp_, vp_, vp_, _int,
                                     vp_, vp_, ctypes.c_float, _int, _int, _int, vp_, vp_]
     L.dazi_dk_fused_dev.restype = _int
+    L.dazi_dk_iso_noalloc_dev.argtypes = L.dazi_dk_iso_dev.argtypes
+    L.dazi_dk_iso_noalloc_dev.restype = _int
     L.dazi_dk_last_launches.argtypes = []
     L.dazi_dk_last_launches.restype = _int
     L.dazi_dk_last_error.argtypes = []

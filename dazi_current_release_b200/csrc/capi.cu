@@ -446,6 +446,11 @@ int stage_dev(int nx, int ny, int nz, const float* vel, const float* vp, const f
 
 }  // namespace
 
+namespace dk {
+// Error message hook for entry points defined in other translation units.
+void set_last_error(const char* msg) { set_err("%s", msg); }
+}  // namespace dk
+
 extern "C" {
 
 int dazi_dk_iso(const int* nx, const int* ny, const int* nz, const float* vel, double* pvRc,

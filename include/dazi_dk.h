@@ -125,6 +125,27 @@ int dazi_dk_fused_dev(int nx, int ny, int nz, const float *vel, const float *vp,
                       float minthk, int col_start, int col_count, int form,
                       int *status, void *stream);
 
+/* Allocation-free variant of dazi_dk_iso_dev for the plain form.  No
+ * counterpart in the reference.  For callers that cannot let a library call
+ * cudaMalloc (a driver under another framework's allocator or a fixed memory
+ * budget, or a pipeline that must avoid cudaMalloc's device-wide
+ * synchronisation): the caller passes device inputs and outputs; the only
+ * other device memory is a file-scope static array of 4 Mi floats (16 MiB)
+ * plus the depth-grid geometry, held on every GPU that loads the library
+ * until exit.  Columns run in tiles of 16 MiB / (4 (1 + 6 nz) kmaxRc) bytes;
+ * a column whose scratch exceeds the array is rejected with
+ * DAZI_ERR_LIMITS.  All calls share the array: calls whose GPU work overlaps
+ * race and must be ordered by the caller.  The first call on a device does
+ * that device's set-up (cudaGetSymbolAddress); make it before any stream
+ * capture.  Returns once the work is queued on `stream` (NULL = legacy
+ * default stream); no-root periods are reported through `status`. */
+int dazi_dk_iso_noalloc_dev(int nx, int ny, int nz, const float *vel,
+                            const float *vp, const float *rho, double *pvRc,
+                            double *sen_vsRc, double *sen_vpRc,
+                            double *sen_rhoRc, int kmaxRc, const double *tRc,
+                            const float *depz, float minthk, int col_start,
+                            int col_count, int *status, void *stream);
+
 /* Number of kernel launches the last call issued (all on its stream). */
 int dazi_dk_last_launches(void);
 
