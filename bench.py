@@ -2,17 +2,21 @@
 """Benchmark of the depth-kernel stage: kernel column-periods per second.
 
 One column-period = the Rayleigh phase velocity c(T) of one column plus its
-Vs-type kernels (dc/dVs, dc/dVp, dc/drho at every node).  A "step" is one
-pass of the stage over the whole workload.
+Vs-type kernels (dc/dVs, dc/dVp, dc/drho at every node) plus its Gc/Gs kernel
+(Lsen_Gsc at every depth interval).  A "step" is one pass of the stage over
+the whole workload (dazi_dk_fused: one phase-velocity pass feeds both).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--workload config1]
                     [--form plain|adjoint] [--impl ours|reference]
 
-value      device-timed throughput, inputs resident in HBM (device entry
-           dazi_dk_iso_dev on torch's stream, CUDA events per step, L2
-           flushed between steps outside the timed events)
-e2e        the same through the host C-ABI entry dazi_dk_iso with pinned host
-           buffers: host->device inputs and device->host outputs every step
+value      device-timed throughput of the chosen form (--form, default the
+           adjoint form), inputs resident in HBM (device entry
+           dazi_dk_fused_dev on torch's stream, CUDA events per step, L2
+           flushed between steps outside the timed events); the other form is
+           timed the same way and reported as "plain" / "adjoint"
+e2e        the same through the host C-ABI entry dazi_dk_fused with pinned
+           host buffers: host->device inputs and device->host outputs every
+           step
 roofline   FP64 CUDA-core bound: algorithmic FLOPs (180 per layer per secular
            evaluation, evaluations counted by the kernels) / kernel time,
            against the FP64 FMA peak measured live by dazi_dk_fp64_peak
@@ -50,7 +54,8 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--workload", default="config1")
-    p.add_argument("--form", default="plain", choices=["plain", "adjoint"])
+    p.add_argument("--form", default="adjoint", choices=["plain", "adjoint"])
+    p.add_argument("--no-other-form", action="store_true")
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-sample-s", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -132,8 +137,19 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def _cpu_stage(O, flat, vp, rho, case, n, cores):
+    """The reference's full stage on the first n columns: depthkernelTI
+    (surfdisp96 + tregn96 + splice) and depthkernel (1 + 6 nz surfdisp96)."""
+    sl = lambda a: None if a is None else a[:n]  # noqa: E731
+    O.depthkernel_ti(flat[:n], case.depz, case.periods, case.minthk, vp=sl(vp), rho=sl(rho),
+                     nthreads=cores)
+    O.depthkernel(flat[:n], case.depz, case.periods, case.minthk, vp=sl(vp), rho=sl(rho),
+                  nthreads=cores)
+
+
 def cpu_baseline(case, sample_s, form_kernels=True):
-    """Oracle FD (the reference algorithm) on as many columns as fit in about
+    """Oracle of the reference stage (depthkernelTI + depthkernel FD, the
+    reference algorithm restated in C) on as many columns as fit in about
     sample_s seconds on all host threads; returns column-periods/s."""
     from oracle import oracle as O
     cores = os.cpu_count() or 1
@@ -144,23 +160,20 @@ def cpu_baseline(case, sample_s, form_kernels=True):
     rho = None if case.rho is None else np.asfortranarray(case.rho.reshape(nx * ny, 1, nz))
     ncols = max(1, min(nx * ny, cores))
     t0 = time.perf_counter()
-    O.depthkernel(flat[:ncols], case.depz, case.periods, case.minthk,
-                  vp=None if vp is None else vp[:ncols], rho=None if rho is None else rho[:ncols],
-                  nthreads=cores)
+    _cpu_stage(O, flat, vp, rho, case, ncols, cores)
     t1 = time.perf_counter()
     per_col = (t1 - t0) / ncols * cores
     n2 = int(max(ncols, min(nx * ny, sample_s / max(per_col, 1e-9) * cores)))
     n2 = max(cores, (n2 // cores) * cores) if n2 >= cores else n2
     n2 = min(n2, nx * ny)
     t0 = time.perf_counter()
-    O.depthkernel(flat[:n2], case.depz, case.periods, case.minthk,
-                  vp=None if vp is None else vp[:n2], rho=None if rho is None else rho[:n2],
-                  nthreads=cores)
+    _cpu_stage(O, flat, vp, rho, case, n2, cores)
     dt = time.perf_counter() - t0
     return {"value": n2 * K / dt, "unit": "column-periods/s", "cores": cores,
             "kind": "port",
-            "sample": f"{n2} of {nx*ny} columns x {K} periods, oracle FD (1+6nz surfdisp96 "
-                      f"per column), {dt:.1f} s on {cores} threads"}
+            "sample": f"{n2} of {nx*ny} columns x {K} periods, oracle of depthkernelTI + "
+                      f"depthkernel (FD: 1+6nz surfdisp96 per column), {dt:.1f} s on "
+                      f"{cores} threads"}
 
 
 def run_reference(args, ws, rank):
@@ -197,7 +210,7 @@ def main():
         return
     import torch
     from dazi_current_release_b200 import _lib
-    from dazi_current_release_b200.depthkernel import _run_iso
+    from dazi_current_release_b200.depthkernel import _run_fused
     L = _lib.load(build_if_missing=False)
     dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
@@ -216,45 +229,57 @@ def main():
     depz = torch.from_numpy(case.depz.copy()).to(dev)
     pv = torch.zeros(nxy * K, dtype=torch.float64, device=dev)
     sen = [torch.zeros(nxy * K * nz, dtype=torch.float64, device=dev) for _ in range(3)]
+    lsen = torch.zeros(nxy * K * (nz - 1), dtype=torch.float32, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
     ptr = lambda x: None if x is None else ctypes.c_void_p(x.data_ptr())  # noqa: E731
 
-    def step():
-        rc = L.dazi_dk_iso_dev(nx, ny, nz, ptr(vel), ptr(vp), ptr(rho), ptr(pv), ptr(sen[0]),
-                               ptr(sen[1]), ptr(sen[2]), K, ptr(per), ptr(depz),
-                               ctypes.c_float(case.minthk), 1, nxy, form, None,
-                               ctypes.c_void_p(stream.cuda_stream))
+    def step(f):
+        rc = L.dazi_dk_fused_dev(nx, ny, nz, ptr(vel), ptr(vp), ptr(rho), ptr(pv), ptr(sen[0]),
+                                 ptr(sen[1]), ptr(sen[2]), ptr(lsen), K, ptr(per), ptr(depz),
+                                 ctypes.c_float(case.minthk), 1, nxy, f, None,
+                                 ctypes.c_void_p(stream.cuda_stream))
         _lib.check(rc)
 
-    for _ in range(args.warmup):
-        step()
-    torch.cuda.synchronize(dev)
-    ev = ctypes.c_longlong(0)
-    lev = ctypes.c_longlong(0)
-    _lib.check(L.dazi_dk_last_work(ctypes.byref(ev), ctypes.byref(lev)))
-    evals_per_step, layer_evals_per_step = ev.value, lev.value
-    starts = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    ends = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps)]
-    if ws > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize(dev)
-    with ClockSampler(local) as clk:
-        for i in range(args.steps):
+    def timed(f, steps, warmup, sampler=None):
+        for _ in range(warmup):
+            step(f)
+        torch.cuda.synchronize(dev)
+        ev = ctypes.c_longlong(0)
+        lev = ctypes.c_longlong(0)
+        _lib.check(L.dazi_dk_last_work(ctypes.byref(ev), ctypes.byref(lev)))
+        launches = L.dazi_dk_last_launches()
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        if ws > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize(dev)
+        for i in range(steps):
             flush.zero_()                      # L2 flush, outside the timed events
             starts[i].record(stream)
-            step()
+            step(f)
             ends[i].record(stream)
         torch.cuda.synchronize(dev)
-    if ws > 1:
-        torch.distributed.barrier()
-    step_ms = [s.elapsed_time(e) for s, e in zip(starts, ends)]
-    total_ms = float(sum(step_ms))
-    if ws > 1:
-        tt = torch.tensor([total_ms], dtype=torch.float64, device=dev)
-        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(tt.item())
-    ms_per_step = total_ms / args.steps
+        if ws > 1:
+            torch.distributed.barrier()
+        total = float(sum(s.elapsed_time(e) for s, e in zip(starts, ends)))
+        if ws > 1:
+            tt = torch.tensor([total], dtype=torch.float64, device=dev)
+            torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+            total = float(tt.item())
+        return total / steps, ev.value, lev.value, launches
+
+    other = None
+    if not args.no_other_form:
+        of = _lib.FORM_PLAIN if form == _lib.FORM_ADJOINT else _lib.FORM_ADJOINT
+        o_steps = max(1, min(args.steps, 2))
+        oms, _, olev, _ = timed(of, o_steps, 1)
+        other = {"form": "plain" if of == _lib.FORM_PLAIN else "adjoint",
+                 "value": ws * nxy * K / (oms * 1e-3), "ms_per_step": oms, "steps": o_steps,
+                 "flops_per_step": olev * FLOP_PER_LAYER_EVAL}
+    with ClockSampler(local) as clk:
+        ms_per_step, evals_per_step, layer_evals_per_step, launches = timed(
+            form, args.steps, args.warmup)
     value = ws * nxy * K / (ms_per_step * 1e-3)
 
     # ---------------- end to end through the host C-ABI (pinned buffers)
@@ -265,6 +290,7 @@ def main():
     h_pv = pin((nxy * K,), torch.float64).reshape((nxy, K), order="F")
     h_sen = tuple(pin((nxy * K * nz,), torch.float64).reshape((nxy, K, nz), order="F")
                   for _ in range(3))
+    h_lsen = pin((nxy * K * (nz - 1),), torch.float32).reshape((nxy, K, nz - 1), order="F")
     if case.vp is not None:
         h_vp = pin((nxy * nz,), torch.float32)
         h_vp[:] = case.vp.ravel(order="F")
@@ -276,8 +302,8 @@ def main():
         h_vp = h_rho = None
 
     def e2e_step():
-        _run_iso(nx, ny, nz, h_vel, h_vp, h_rho, 2, 0, K, case.periods, case.depz, case.minthk,
-                 form, 1, None, True, pvRc=h_pv, sen=h_sen)
+        _run_fused(nx, ny, nz, h_vel, h_vp, h_rho, 2, 0, K, case.periods, case.depz, case.minthk,
+                   form, 1, None, True, True, pvRc=h_pv, sen=h_sen, Lsen=h_lsen)
 
     e2e_step()
     if ws > 1:
@@ -291,7 +317,7 @@ def main():
         torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
         e2e_s = float(tt.item())
     h2d = nxy * nz * 4 * (3 if case.vp is not None else 1) + K * 8
-    d2h = nxy * K * 8 * (1 + 3 * nz) + nxy * 4
+    d2h = nxy * K * 8 * (1 + 3 * nz) + nxy * K * 4 * (nz - 1) + nxy * 4
 
     # ---------------- roofline
     peak = ctypes.c_double(0.0)
@@ -322,8 +348,11 @@ def main():
                      "frac": achieved / peak_tf if peak_tf > 0 else None, "traffic": traffic,
                      "peak_source": "measured in-run FP64 FMA probe (dazi_dk_fp64_peak)",
                      "flops_per_step": flops, "secular_evals_per_step": evals_per_step},
-        "gpu_launches": args.steps * 1,
+        "gpu_launches": args.steps * launches,
     }
+    if other:
+        line[other["form"]] = other
+        line[args.form] = {"form": args.form, "value": value, "ms_per_step": ms_per_step}
     clocks = clk.summary()
     if clocks:
         line["clocks"] = clocks

@@ -179,6 +179,7 @@ def depthkernel(vel, depz, periods, minthk, vp=None, rho=None, iwave=2, igr=0,
 
 def depthkernel_ti(vel, depz, periods, minthk, vp=None, rho=None, iwave=2, igr=0,
                    nthreads=0):
+    # (nthreads: OpenMP threads over columns; 0 = all)
     """Oracle of ``depthkernelTI`` (depthkernelTI.f90:2-193).
 
     Returns dict with pvRc (nxy,K) float64 and Lsen_Gsc (nxy,K,nz-1) float32,
