@@ -32,7 +32,7 @@ EXPORTS = (
     "dazi_dk_iso", "dazi_dk_iso_vpvsrho", "dazi_dk_last_status", "dazi_dk_iso_dev",
     "dazi_dk_last_error", "dazi_dk_version", "dazi_dk_finalize", "dazi_dk_fp64_peak", "dazi_dk_last_work",
     "dazi_dk_ti", "dazi_dk_fused", "dazi_dk_fused_dev", "dazi_dk_last_launches",
-    "dazi_dk_iso_noalloc_dev",
+    "dazi_dk_iso_noalloc_dev", "dazi_dk_batch", "dazi_dk_batch_dev",
 )
 
 
@@ -84,6 +84,13 @@ def load(build_if_missing: bool = True):
     L.dazi_dk_fused_dev.restype = _int
     L.dazi_dk_iso_noalloc_dev.argtypes = L.dazi_dk_iso_dev.argtypes
     L.dazi_dk_iso_noalloc_dev.restype = _int
+    i64p = ctypes.POINTER(ctypes.c_longlong)
+    ll = ctypes.c_longlong
+    L.dazi_dk_batch.argtypes = [ll, i64p, fp, fp, fp, fp, i64p, _f64p, ctypes.c_float, _f64p, i64p,
+                                _f64p, _f64p, _f64p, i64p, fp, _int, _i32p]
+    L.dazi_dk_batch.restype = _int
+    L.dazi_dk_batch_dev.argtypes = [ll] + [vp_] * 7 + [ctypes.c_float] + [vp_] * 7 + [_int, vp_, vp_]
+    L.dazi_dk_batch_dev.restype = _int
     L.dazi_dk_last_launches.argtypes = []
     L.dazi_dk_last_launches.restype = _int
     L.dazi_dk_last_error.argtypes = []

@@ -14,6 +14,8 @@
 #include <vector>
 
 #include "../../include/dazi_dk.h"
+#include <cub/cub.cuh>
+
 #include "dk_kernels.cuh"
 
 using namespace dk;
@@ -68,7 +70,12 @@ struct Context {
     // host-entry staging
     DBuf vel, vp, rho, per, depz, pv, svs, svp, srh, status;
     // work buffers
-    DBuf geo, cscratch, layers, layersd, tilayers, croot, counters, adjscr, tiscr, lsen;
+    DBuf geo, cscratch, croot, counters, adjscr, tiscr, lsen;
+    // per-call layer tables
+    DBuf keys, keys2, cidx, cidx2, rmaxb, trecs, ttasks, tlbase, ttbase, cubtmp;
+    DBuf tflat, tld, tti, tch, tmeta, ttasklist, cbufoff;
+    // batch staging (host entry)
+    DBuf bnode, bper, bdep, bvs, bvp, brho, bperiods, bsenoff, blsoff, bpv, bsvs, bsvp, bsrh, blsen, bstatus;
     int last_launches = 0;
     int last_rmax = 0;
     // geometry cache key
@@ -178,7 +185,145 @@ int launch_persistent_grid(const void* fn, long long nitems, int threads, long l
     return 0;
 }
 
-// The stage on device pointers (stream-ordered, no host synchronisation).
+// Build the per-layer tables of a call (dk_table.cuh): count layers,
+// sort the columns by (layers, periods), lay out 32-column tiles, build.
+// One host synchronisation (to size the tables).
+int build_tables(const ColSrc& src, long long ncols, const PrepOut& po, long long pv_sk,
+                 long long sen_sk, long long ls_sk, cudaStream_t st, Tables& T)
+{
+    int r;
+    const long long ntiles = (ncols + TILE - 1) / TILE;
+    if ((r = g_ctx.keys.ensure(sizeof(unsigned) * ncols)) || (r = g_ctx.keys2.ensure(sizeof(unsigned) * ncols)) ||
+        (r = g_ctx.cidx.ensure(sizeof(int) * ncols)) || (r = g_ctx.cidx2.ensure(sizeof(int) * ncols)) ||
+        (r = g_ctx.rmaxb.ensure(sizeof(int) * ncols + 16)) ||
+        (r = g_ctx.trecs.ensure(sizeof(long long) * ntiles)) || (r = g_ctx.ttasks.ensure(sizeof(long long) * ntiles)) ||
+        (r = g_ctx.tlbase.ensure(sizeof(long long) * ntiles)) || (r = g_ctx.ttbase.ensure(sizeof(long long) * ntiles)))
+        return r;
+    int* err = reinterpret_cast<int*>(g_ctx.rmaxb.as<char>() + sizeof(int) * ncols);
+    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+    const int bt = 128;
+    const unsigned nb = (unsigned)((ncols + bt - 1) / bt);
+    prep_count_kernel<<<nb, bt, 0, st>>>(src, ncols, g_ctx.keys.as<unsigned>(), g_ctx.cidx.as<int>(),
+                                         g_ctx.rmaxb.as<int>(), err);
+    CK(cudaGetLastError());
+    size_t tb1 = 0, tb2 = 0, tb3 = 0;
+    CK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb1, g_ctx.keys.as<unsigned>(), g_ctx.keys2.as<unsigned>(),
+                                                 g_ctx.cidx.as<int>(), g_ctx.cidx2.as<int>(), (int)ncols, 0, 16, st));
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, g_ctx.trecs.as<long long>(), g_ctx.tlbase.as<long long>(),
+                                     (int)ntiles, st));
+    tb3 = tb1 > tb2 ? tb1 : tb2;
+    if ((r = g_ctx.cubtmp.ensure(tb3 + 16))) return r;
+    CK(cub::DeviceRadixSort::SortPairsDescending(g_ctx.cubtmp.p, tb3, g_ctx.keys.as<unsigned>(), g_ctx.keys2.as<unsigned>(),
+                                                 g_ctx.cidx.as<int>(), g_ctx.cidx2.as<int>(), (int)ncols, 0, 16, st));
+    const unsigned ntb = (unsigned)((ntiles + bt - 1) / bt);
+    prep_tile_kernel<<<ntb, bt, 0, st>>>(ncols, g_ctx.cidx2.as<int>(), g_ctx.rmaxb.as<int>(), src,
+                                         g_ctx.trecs.as<long long>(), g_ctx.ttasks.as<long long>());
+    CK(cudaGetLastError());
+    size_t tbs = tb3;
+    CK(cub::DeviceScan::ExclusiveSum(g_ctx.cubtmp.p, tbs, g_ctx.trecs.as<long long>(), g_ctx.tlbase.as<long long>(),
+                                     (int)ntiles, st));
+    tbs = tb3;
+    CK(cub::DeviceScan::ExclusiveSum(g_ctx.cubtmp.p, tbs, g_ctx.ttasks.as<long long>(), g_ctx.ttbase.as<long long>(),
+                                     (int)ntiles, st));
+    long long last[4] = {0, 0, 0, 0};
+    int herr = 0;
+    CK(cudaMemcpyAsync(&last[0], g_ctx.tlbase.as<long long>() + ntiles - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last[1], g_ctx.trecs.as<long long>() + ntiles - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last[2], g_ctx.ttbase.as<long long>() + ntiles - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last[3], g_ctx.ttasks.as<long long>() + ntiles - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (herr) {
+        set_err("invalid column (%s%s%s%s%s)", (herr & 1) ? "nz outside [2,200] " : "",
+                (herr & 2) ? "period count outside [1,160] " : "", (herr & 4) ? "depths not increasing " : "",
+                (herr & 8) ? "more than 200 refined layers " : "", (herr & 16) ? "non-positive velocity/density" : "");
+        return (herr & (1 | 2 | 8)) ? DAZI_ERR_LIMITS : DAZI_ERR_BADARG;
+    }
+    const long long nrec = last[0] + last[1], ntask = last[2] + last[3];
+    if ((r = g_ctx.tflat.ensure(sizeof(float4) * nrec)) || (r = g_ctx.tld.ensure(sizeof(LayerD) * nrec)) ||
+        (r = g_ctx.tti.ensure(sizeof(TiRec) * nrec)) || (r = g_ctx.tch.ensure(sizeof(ChainRec) * nrec)) ||
+        (r = g_ctx.tmeta.ensure(sizeof(ColMeta) * ncols)) || (r = g_ctx.ttasklist.ensure(sizeof(int2) * ntask)))
+        return r;
+    T.flat = g_ctx.tflat.as<float4>(); T.ld = g_ctx.tld.as<LayerD>(); T.ti = g_ctx.tti.as<TiRec>();
+    T.ch = g_ctx.tch.as<ChainRec>(); T.meta = g_ctx.tmeta.as<ColMeta>();
+    T.tile_lbase = g_ctx.tlbase.as<long long>(); T.tasks = g_ctx.ttasklist.as<int2>();
+    T.ntasks = ntask; T.ncols = ncols; T.pv_sk = pv_sk; T.sen_sk = sen_sk; T.ls_sk = ls_sk;
+    prep_tasks_kernel<<<ntb, bt, 0, st>>>(ntiles, g_ctx.ttasks.as<long long>(), g_ctx.ttbase.as<long long>(),
+                                          T.tasks);
+    CK(cudaGetLastError());
+    prep_build_kernel<<<nb, bt, 0, st>>>(src, po, T, g_ctx.cidx2.as<int>(), g_ctx.ttbase.as<long long>());
+    CK(cudaGetLastError());
+    g_ctx.last_launches += 5;
+    return 0;
+}
+
+// The per-(column, period) kernels and the root search over built tables.
+int run_tables(const Tables& T, const double* per, const StageOut& o, int form, bool fd_done,
+               cudaStream_t st)
+{
+    int r;
+    unsigned long long* nevals = g_ctx.counters.as<unsigned long long>();
+    int* errflag = reinterpret_cast<int*>(nevals + 1);
+    unsigned* queues = reinterpret_cast<unsigned*>(nevals + 2);
+    const bool adj = o.svs && form == DAZI_FORM_ADJOINT;
+    long long maxr = 0;
+    {
+        // largest layer count (first sorted column) for the scratch sizes
+        ColMeta m0;
+        CK(cudaMemcpyAsync(&m0, T.meta, sizeof(ColMeta), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        maxr = m0.rmax;
+    }
+    if (!fd_done) {
+        RootArgs a;
+        a.T = T; a.periods = per; a.tol = 1.0e-6;   // surfdisp96.f:608
+        a.pv = o.pv; a.croot = nullptr; a.status = o.status; a.nevals = nevals;
+        if (adj) {
+            if ((r = g_ctx.croot.ensure(sizeof(double) * TILE * (size_t)T.ntasks))) return r;
+            a.croot = g_ctx.croot.as<double>();
+        }
+        const int bt = 128;
+        root_kernel<<<(unsigned)((T.ncols + bt - 1) / bt), bt, 0, st>>>(a);
+        CK(cudaGetLastError());
+        ++g_ctx.last_launches;
+    }
+    const long long nitems = T.ntasks * TILE;
+    if (adj) {
+        const int at = 128;
+        long long nblk;
+        if ((r = launch_persistent_grid((const void*)adjoint_kernel, nitems, at, nblk))) return r;
+        const long long nslots = nblk * at;
+        const size_t scr = sizeof(double) * 6 * (size_t)(maxr > 1 ? maxr - 1 : 1) * (size_t)nslots;
+        if ((r = g_ctx.adjscr.ensure(scr))) return r;
+        CK(cudaMemsetAsync(queues, 0, sizeof(unsigned), st));
+        AdjArgs j;
+        j.T = T; j.periods = per; j.croot = g_ctx.croot.as<double>();
+        j.sen_vs = o.svs; j.sen_vp = o.svp; j.sen_rho = o.srh;
+        j.scratch = g_ctx.adjscr.as<double>(); j.queue = queues;
+        adjoint_kernel<<<(unsigned)nblk, at, 0, st>>>(j);
+        CK(cudaGetLastError());
+        ++g_ctx.last_launches;
+    }
+    if (o.lsen) {
+        const int at = 128;
+        long long nblk;
+        if ((r = launch_persistent_grid((const void*)ti_kernel, nitems, at, nblk))) return r;
+        const long long nslots = nblk * at;
+        const size_t scr = sizeof(double) * 6 * (size_t)maxr * (size_t)nslots;
+        if ((r = g_ctx.tiscr.ensure(scr))) return r;
+        CK(cudaMemsetAsync(queues + 1, 0, sizeof(unsigned), st));
+        TiArgs t;
+        t.T = T; t.periods = per; t.pv = o.pv; t.lsen = o.lsen;
+        t.scratch = g_ctx.tiscr.as<double>(); t.queue = queues + 1; t.errflag = errflag;
+        ti_kernel<<<(unsigned)nblk, at, 0, st>>>(t);
+        CK(cudaGetLastError());
+        ++g_ctx.last_launches;
+    }
+    return 0;
+}
+
+// The stage on device pointers (stream-ordered; one small host sync sizes
+// the layer tables).
 //   plain   + kernels: one CTA per column runs the 1 + 6 nz models (FD)
 //   adjoint + kernels: per-column root search, then per-(column, period)
 //                      adjoint sweeps
@@ -190,14 +335,10 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
     const long long ncol = (long long)nx * ny;
     if (col_count == 0) return 0;
     const Geometry* geo = g_ctx.geo.as<Geometry>();
-    const double tol = 1.0e-6;   // surfdisp96.f:608
-    const int rmax = g_ctx.geo_rmax;
     int r;
     if ((r = g_ctx.counters.ensure(sizeof(unsigned long long) * 4))) return r;
     CK(cudaMemsetAsync(g_ctx.counters.p, 0, sizeof(unsigned long long) * 4, st));
-    g_ctx.last_rmax = rmax;
-    unsigned long long* nevals = g_ctx.counters.as<unsigned long long>();
-    int* errflag = reinterpret_cast<int*>(nevals + 1);
+    g_ctx.last_rmax = g_ctx.geo_rmax;
     g_ctx.last_launches = 0;
     const bool fd = o.svs && form == DAZI_FORM_PLAIN;
     if (fd) {
@@ -219,78 +360,93 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
             a.vel = vel; a.vp = vp; a.rho = rho; a.periods = per;
             a.pv = o.pv; a.sen_vs = o.svs; a.sen_vp = o.svp; a.sen_rho = o.srh;
             a.status = o.status; a.cscratch = g_ctx.cscratch.as<float>();
-            a.dln = 0.01f; a.tol = tol; a.nevals = nevals;
+            a.dln = 0.01f; a.tol = 1.0e-6; a.nevals = g_ctx.counters.as<unsigned long long>();
             fd_column_kernel<<<(unsigned)n, threads, smem, st>>>(a);
             CK(cudaGetLastError());
             ++g_ctx.last_launches;
         }
         if (!o.lsen) return 0;
     }
-    // per-column layer tables
-    const size_t nl = (size_t)rmax * (size_t)col_count;
-    if ((r = g_ctx.layers.ensure(sizeof(float4) * nl))) return r;
-    if ((r = g_ctx.layersd.ensure(sizeof(LayerD) * nl))) return r;
-    if (o.lsen && (r = g_ctx.tilayers.ensure(sizeof(float4) * nl))) return r;
-    BuildArgs b;
-    b.geo = geo; b.nz = nz; b.ncol = ncol; b.col0 = col_start - 1; b.ncols = col_count;
-    b.vel = vel; b.vp = vp; b.rho = rho; b.layers = g_ctx.layers.as<float4>();
-    b.layersd = g_ctx.layersd.as<LayerD>();
-    b.tilayers = o.lsen ? g_ctx.tilayers.as<float4>() : nullptr;
-    const int bt = 128;
-    const unsigned nb = (unsigned)((col_count + bt - 1) / bt);
-    build_layers_kernel<<<nb, bt, 0, st>>>(b);
-    CK(cudaGetLastError());
-    ++g_ctx.last_launches;
-    const bool adj = o.svs && form == DAZI_FORM_ADJOINT;
-    if (!fd) {
-        RootArgs a;
-        a.geo = geo; a.kmax = kmax; a.ncol = ncol; a.col0 = col_start - 1; a.ncols = col_count;
-        a.layers = g_ctx.layers.as<float4>(); a.layersd = g_ctx.layersd.as<LayerD>();
-        a.periods = per; a.tol = tol;
-        a.pv = o.pv; a.croot = nullptr; a.evals = nullptr; a.status = o.status; a.nevals = nevals;
-        if (adj) {
-            if ((r = g_ctx.croot.ensure(sizeof(double) * (size_t)kmax * (size_t)col_count))) return r;
-            a.croot = g_ctx.croot.as<double>();
+    ColSrc src;
+    src.ragged = false; src.ncol = ncol; src.col0 = col_start - 1;
+    src.vel = vel; src.vp = vp; src.rho = rho; src.depz = g_ctx.depz.as<float>();
+    src.node_off = nullptr; src.per_off = nullptr; src.nz = nz; src.K = kmax;
+    src.minthk = g_ctx.geo_minthk;
+    PrepOut po{nullptr, nullptr};
+    Tables T;
+    if ((r = build_tables(src, col_count, po, ncol, ncol, ncol, st, T))) return r;
+    return run_tables(T, per, o, form, fd, st);
+}
+
+// Ragged batch on device pointers.
+struct BatchIn {
+    long long ncols;
+    const long long* node_off;
+    const float* depz;
+    const float* vs;
+    const float* vp;
+    const float* rho;
+    const long long* per_off;
+    const double* periods;
+    float minthk;
+    const long long* sen_off;
+    const long long* ls_off;
+};
+
+int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
+{
+    if (B.ncols == 0) return 0;
+    int r;
+    if ((r = g_ctx.counters.ensure(sizeof(unsigned long long) * 4))) return r;
+    CK(cudaMemsetAsync(g_ctx.counters.p, 0, sizeof(unsigned long long) * 4, st));
+    g_ctx.last_launches = 0;
+    g_ctx.last_rmax = 0;
+    ColSrc src;
+    src.ragged = true; src.ncol = 0; src.col0 = 0;
+    src.vel = B.vs; src.vp = B.vp; src.rho = B.rho; src.depz = B.depz;
+    src.node_off = B.node_off; src.per_off = B.per_off; src.nz = 0; src.K = 0;
+    src.minthk = B.minthk;
+    PrepOut po{B.sen_off, B.ls_off};
+    Tables T;
+    if ((r = build_tables(src, B.ncols, po, 1, 1, 1, st, T))) return r;
+    const bool fd = o.svs && form == DAZI_FORM_PLAIN;
+    if (fd) {
+        // plain form: one CTA per column, scratch offsets per column
+        std::vector<long long> hoff(B.ncols + 1), hn(B.ncols + 1), hp(B.ncols + 1);
+        CK(cudaMemcpyAsync(hn.data(), B.node_off, sizeof(long long) * (B.ncols + 1), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(hp.data(), B.per_off, sizeof(long long) * (B.ncols + 1), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        hoff[0] = 0;
+        long long maxcol = 0;
+        for (long long c = 0; c < B.ncols; ++c) {
+            const long long need = (1 + 6 * (hn[c + 1] - hn[c])) * (hp[c + 1] - hp[c]);
+            hoff[c + 1] = hoff[c] + need;
+            if (need > maxcol) maxcol = need;
         }
-        root_kernel<<<nb, bt, 0, st>>>(a);
-        CK(cudaGetLastError());
-        ++g_ctx.last_launches;
+        if ((r = g_ctx.cbufoff.ensure(sizeof(long long) * (B.ncols + 1)))) return r;
+        CK(cudaMemcpyAsync(g_ctx.cbufoff.p, hoff.data(), sizeof(long long) * (B.ncols + 1), cudaMemcpyHostToDevice, st));
+        const long long capf = std::max<long long>(maxcol, (512ll << 20) / 4);
+        if ((r = g_ctx.cscratch.ensure(sizeof(float) * capf))) return r;
+        long long c0 = 0;
+        while (c0 < B.ncols) {
+            long long c1 = c0;
+            while (c1 < B.ncols && hoff[c1 + 1] - hoff[c0] <= capf) ++c1;
+            FdArgs a;
+            a.geo = nullptr; a.nz = 0; a.kmax = 0; a.ncol = 0; a.col0 = c0;
+            a.vel = B.vs; a.vp = B.vp; a.rho = B.rho; a.periods = B.periods;
+            a.pv = o.pv; a.sen_vs = o.svs; a.sen_vp = o.svp; a.sen_rho = o.srh;
+            a.status = o.status; a.cscratch = g_ctx.cscratch.as<float>();
+            a.dln = 0.01f; a.tol = 1.0e-6; a.nevals = g_ctx.counters.as<unsigned long long>();
+            FdBatch fb;
+            fb.node_off = B.node_off; fb.per_off = B.per_off; fb.depz = B.depz; fb.minthk = B.minthk;
+            fb.sen_off = B.sen_off; fb.cbuf_off = g_ctx.cbufoff.as<long long>();
+            fd_batch_kernel<<<(unsigned)(c1 - c0), 256, fd_batch_smem_bytes(), st>>>(a, fb);
+            CK(cudaGetLastError());
+            ++g_ctx.last_launches;
+            c0 = c1;
+        }
     }
-    const long long nitems = col_count * (long long)kmax;
-    if (adj) {
-        // adjoint sweeps: one thread per (column, period) on a persistent
-        // grid, so the per-thread scratch slots are bounded by residency
-        const int at = 128;
-        long long nblk;
-        if ((r = launch_persistent_grid((const void*)adjoint_kernel, nitems, at, nblk))) return r;
-        const long long nslots = nblk * at;
-        const size_t scr = sizeof(double) * 6 * (size_t)(rmax > 1 ? rmax - 1 : 1) * (size_t)nslots;
-        if ((r = g_ctx.adjscr.ensure(scr))) return r;
-        AdjArgs j;
-        j.geo = geo; j.nz = nz; j.kmax = kmax; j.ncol = ncol; j.col0 = col_start - 1;
-        j.ncols = col_count; j.layers = g_ctx.layers.as<float4>(); j.periods = per;
-        j.croot = g_ctx.croot.as<double>(); j.sen_vs = o.svs; j.sen_vp = o.svp; j.sen_rho = o.srh;
-        j.scratch = g_ctx.adjscr.as<double>();
-        adjoint_kernel<<<(unsigned)nblk, at, 0, st>>>(j);
-        CK(cudaGetLastError());
-        ++g_ctx.last_launches;
-    }
-    if (o.lsen) {
-        const int at = 128;
-        long long nblk;
-        if ((r = launch_persistent_grid((const void*)ti_kernel, nitems, at, nblk))) return r;
-        const long long nslots = nblk * at;
-        const size_t scr = sizeof(double) * 6 * (size_t)rmax * (size_t)nslots;
-        if ((r = g_ctx.tiscr.ensure(scr))) return r;
-        TiArgs t;
-        t.geo = geo; t.nz = nz; t.kmax = kmax; t.ncol = ncol; t.col0 = col_start - 1;
-        t.ncols = col_count; t.tilayers = g_ctx.tilayers.as<float4>(); t.periods = per;
-        t.pv = o.pv; t.lsen = o.lsen; t.scratch = g_ctx.tiscr.as<double>(); t.errflag = errflag;
-        ti_kernel<<<(unsigned)nblk, at, 0, st>>>(t);
-        CK(cudaGetLastError());
-        ++g_ctx.last_launches;
-    }
-    return 0;
+    return run_tables(T, B.periods, o, form, fd, st);
 }
 
 int check_values(const float* vel, const float* vp, const float* rho, long long ncol, int nz,
@@ -522,6 +678,121 @@ int dazi_dk_fused_dev(int nx, int ny, int nz, const float* vel, const float* vp,
                      kmaxRc, tRc, depz, minthk, col_start, col_count, form, status, stream);
 }
 
+int dazi_dk_batch_dev(long long ncols, const long long* node_off, const float* depz, const float* vs,
+                      const float* vp, const float* rho, const long long* per_off,
+                      const double* periods, float minthk, double* pv, const long long* sen_off,
+                      double* sen_vs, double* sen_vp, double* sen_rho, const long long* ls_off,
+                      float* lsen, int form, int* status, void* stream)
+{
+    if (ncols < 0 || (ncols > 0 && (!node_off || !depz || !vs || !per_off || !periods || !pv))) {
+        set_err("null argument");
+        return DAZI_ERR_BADARG;
+    }
+    if ((sen_vs == nullptr) != (sen_vp == nullptr) || (sen_vs == nullptr) != (sen_rho == nullptr) ||
+        (sen_vs && !sen_off) || (lsen && !ls_off)) {
+        set_err("kernel outputs need sen_off / ls_off and all three sen arrays");
+        return DAZI_ERR_BADARG;
+    }
+    if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
+    if (form != DAZI_FORM_PLAIN && form != DAZI_FORM_ADJOINT) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    if (!(minthk > 0.f) || !std::isfinite(minthk)) { set_err("minthk must be > 0"); return DAZI_ERR_BADARG; }
+    std::lock_guard<std::mutex> lk(g_mu);
+    int r;
+    if ((r = ensure_context())) return r;
+    BatchIn B{ncols, node_off, depz, vs, vp, rho, per_off, periods, minthk, sen_off, ls_off};
+    StageOut o;
+    o.pv = pv; o.svs = sen_vs; o.svp = sen_vp; o.srh = sen_rho; o.lsen = lsen; o.status = status;
+    return batch_device(B, o, form, (cudaStream_t)stream);
+}
+
+int dazi_dk_batch(long long ncols, const long long* node_off, const float* depz, const float* vs,
+                  const float* vp, const float* rho, const long long* per_off, const double* periods,
+                  float minthk, double* pv, const long long* sen_off, double* sen_vs, double* sen_vp,
+                  double* sen_rho, const long long* ls_off, float* lsen, int form, int* status)
+{
+    if (ncols < 0 || (ncols > 0 && (!node_off || !depz || !vs || !per_off || !periods || !pv))) {
+        set_err("null argument");
+        return DAZI_ERR_BADARG;
+    }
+    if ((sen_vs == nullptr) != (sen_vp == nullptr) || (sen_vs == nullptr) != (sen_rho == nullptr) ||
+        (sen_vs && !sen_off) || (lsen && !ls_off)) {
+        set_err("kernel outputs need sen_off / ls_off and all three sen arrays");
+        return DAZI_ERR_BADARG;
+    }
+    if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
+    if (form != DAZI_FORM_PLAIN && form != DAZI_FORM_ADJOINT) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    if (!(minthk > 0.f) || !std::isfinite(minthk)) { set_err("minthk must be > 0"); return DAZI_ERR_BADARG; }
+    if (ncols == 0) return DAZI_OK;
+    for (long long c = 0; c < ncols; ++c)
+        if (node_off[c + 1] < node_off[c] || per_off[c + 1] < per_off[c]) {
+            set_err("offsets must be non-decreasing (column %lld)", c);
+            return DAZI_ERR_BADARG;
+        }
+    for (long long c = 0; c < ncols; ++c)
+        for (long long p = per_off[c]; p < per_off[c + 1]; ++p)
+            if (!(periods[p] > 0.0) || !std::isfinite(periods[p])) {
+                set_err("period %lld is not a positive finite number", p);
+                return DAZI_ERR_BADARG;
+            }
+    const long long nn = node_off[ncols], np_ = per_off[ncols];
+    const long long ns = sen_vs ? sen_off[ncols] : 0, nl = lsen ? ls_off[ncols] : 0;
+    std::lock_guard<std::mutex> lk(g_mu);
+    int r;
+    if ((r = ensure_context())) return r;
+    cudaStream_t st = g_ctx.stream;
+    const size_t o1 = sizeof(long long) * (ncols + 1);
+    if ((r = g_ctx.bnode.ensure(o1)) || (r = g_ctx.bper.ensure(o1)) || (r = g_ctx.bdep.ensure(sizeof(float) * nn)) ||
+        (r = g_ctx.bvs.ensure(sizeof(float) * nn)) || (r = g_ctx.bperiods.ensure(sizeof(double) * np_)) ||
+        (r = g_ctx.bpv.ensure(sizeof(double) * np_)) || (r = g_ctx.bstatus.ensure(sizeof(int) * ncols)))
+        return r;
+    if (vp && ((r = g_ctx.bvp.ensure(sizeof(float) * nn)) || (r = g_ctx.brho.ensure(sizeof(float) * nn)))) return r;
+    if (sen_vs && ((r = g_ctx.bsenoff.ensure(o1)) || (r = g_ctx.bsvs.ensure(sizeof(double) * ns)) ||
+                   (r = g_ctx.bsvp.ensure(sizeof(double) * ns)) || (r = g_ctx.bsrh.ensure(sizeof(double) * ns))))
+        return r;
+    if (lsen && ((r = g_ctx.blsoff.ensure(o1)) || (r = g_ctx.blsen.ensure(sizeof(float) * nl)))) return r;
+    CK(cudaMemcpyAsync(g_ctx.bnode.p, node_off, o1, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(g_ctx.bper.p, per_off, o1, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(g_ctx.bdep.p, depz, sizeof(float) * nn, cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(g_ctx.bvs.p, vs, sizeof(float) * nn, cudaMemcpyHostToDevice, st));
+    if (vp) {
+        CK(cudaMemcpyAsync(g_ctx.bvp.p, vp, sizeof(float) * nn, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(g_ctx.brho.p, rho, sizeof(float) * nn, cudaMemcpyHostToDevice, st));
+    }
+    CK(cudaMemcpyAsync(g_ctx.bperiods.p, periods, sizeof(double) * np_, cudaMemcpyHostToDevice, st));
+    if (sen_vs) CK(cudaMemcpyAsync(g_ctx.bsenoff.p, sen_off, o1, cudaMemcpyHostToDevice, st));
+    if (lsen) CK(cudaMemcpyAsync(g_ctx.blsoff.p, ls_off, o1, cudaMemcpyHostToDevice, st));
+    CK(cudaMemsetAsync(g_ctx.bstatus.p, 0, sizeof(int) * ncols, st));
+    BatchIn B{ncols, g_ctx.bnode.as<long long>(), g_ctx.bdep.as<float>(), g_ctx.bvs.as<float>(),
+              vp ? g_ctx.bvp.as<float>() : nullptr, vp ? g_ctx.brho.as<float>() : nullptr,
+              g_ctx.bper.as<long long>(), g_ctx.bperiods.as<double>(), minthk,
+              sen_vs ? g_ctx.bsenoff.as<long long>() : nullptr, lsen ? g_ctx.blsoff.as<long long>() : nullptr};
+    StageOut o;
+    o.pv = g_ctx.bpv.as<double>();
+    o.svs = sen_vs ? g_ctx.bsvs.as<double>() : nullptr;
+    o.svp = sen_vs ? g_ctx.bsvp.as<double>() : nullptr;
+    o.srh = sen_vs ? g_ctx.bsrh.as<double>() : nullptr;
+    o.lsen = lsen ? g_ctx.blsen.as<float>() : nullptr;
+    o.status = g_ctx.bstatus.as<int>();
+    if ((r = batch_device(B, o, form, st))) return r;
+    CK(cudaMemcpyAsync(pv, o.pv, sizeof(double) * np_, cudaMemcpyDeviceToHost, st));
+    if (sen_vs) {
+        CK(cudaMemcpyAsync(sen_vs, o.svs, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(sen_vp, o.svp, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(sen_rho, o.srh, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+    }
+    if (lsen) CK(cudaMemcpyAsync(lsen, o.lsen, sizeof(float) * nl, cudaMemcpyDeviceToHost, st));
+    std::vector<int> hst(ncols);
+    CK(cudaMemcpyAsync(hst.data(), o.status, sizeof(int) * ncols, cudaMemcpyDeviceToHost, st));
+    int hflag = 0;
+    CK(cudaMemcpyAsync(&hflag, g_ctx.counters.as<unsigned long long>() + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (status) std::memcpy(status, hst.data(), sizeof(int) * ncols);
+    if (hflag) { set_err("non-finite Lsen_Gsc value (degenerate layer: Vp <= Vs?)"); return DAZI_ERR_MODEL; }
+    for (long long c = 0; c < ncols; ++c)
+        if (hst[c] != 0) return DAZI_WARN_NOROOT;
+    return DAZI_OK;
+}
+
 int dazi_dk_last_launches(void)
 {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -549,8 +820,14 @@ void dazi_dk_finalize(void)
     if (!g_ctx.ready) return;
     DBuf* all[] = {&g_ctx.vel, &g_ctx.vp, &g_ctx.rho, &g_ctx.per, &g_ctx.depz, &g_ctx.pv,
                    &g_ctx.svs, &g_ctx.svp, &g_ctx.srh, &g_ctx.status, &g_ctx.geo,
-                   &g_ctx.cscratch, &g_ctx.layers, &g_ctx.layersd, &g_ctx.croot, &g_ctx.counters, &g_ctx.adjscr, &g_ctx.tilayers,
-                   &g_ctx.tiscr, &g_ctx.lsen};
+                   &g_ctx.cscratch, &g_ctx.croot, &g_ctx.counters, &g_ctx.adjscr,
+                   &g_ctx.tiscr, &g_ctx.lsen, &g_ctx.keys, &g_ctx.keys2, &g_ctx.cidx, &g_ctx.cidx2,
+                   &g_ctx.rmaxb, &g_ctx.trecs, &g_ctx.ttasks, &g_ctx.tlbase, &g_ctx.ttbase,
+                   &g_ctx.cubtmp, &g_ctx.tflat, &g_ctx.tld, &g_ctx.tti, &g_ctx.tch, &g_ctx.tmeta,
+                   &g_ctx.ttasklist, &g_ctx.cbufoff, &g_ctx.bnode, &g_ctx.bper, &g_ctx.bdep,
+                   &g_ctx.bvs, &g_ctx.bvp, &g_ctx.brho, &g_ctx.bperiods, &g_ctx.bsenoff,
+                   &g_ctx.blsoff, &g_ctx.bpv, &g_ctx.bsvs, &g_ctx.bsvp, &g_ctx.bsrh, &g_ctx.blsen,
+                   &g_ctx.bstatus};
     for (DBuf* b : all) b->release();
     if (g_ctx.stream) cudaStreamDestroy(g_ctx.stream);
     g_ctx = Context();

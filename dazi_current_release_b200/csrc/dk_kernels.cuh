@@ -1,7 +1,7 @@
 // Kernel argument blocks and launch entry points shared by the C-ABI layer.
 #pragma once
 #include <cuda_runtime.h>
-#include "dk_model.cuh"
+#include "dk_table.cuh"
 
 namespace dk {
 
@@ -25,66 +25,102 @@ struct FdArgs {
     double tol;
 };
 
-struct BuildArgs {
-    const Geometry* geo;
-    int nz;
-    long long ncol, col0, ncols;
-    const float* vel;
-    const float* vp;
-    const float* rho;
-    float4* layers;      // [rmax][ncols] flattened (d, a, b, rho)
-    LayerD* layersd;     // [rmax][ncols] FP64 per-layer constants
-    float4* tilayers;    // [rmax][ncols] unflattened refined (vp, vs, rho), or nullptr
+struct PrepOut {
+    const long long* sen_off;   // ragged: first kernel entry of each column
+    const long long* ls_off;    // ragged: first Lsen entry of each column
 };
 
 struct RootArgs {
-    const Geometry* geo;
-    int kmax;
-    long long ncol, col0, ncols;
-    const float4* layers;
-    const LayerD* layersd;
+    Tables T;
     const double* periods;
     double tol;
-    double* pv;          // (ncol, K) FP32-valued like the reference
-    double* croot;       // [ncols][K] FP64 roots, or nullptr
-    int* evals;          // (ncol, K) secular evaluations, or nullptr
-    int* status;
+    double* pv;             // FP32-valued phase velocities (reference output)
+    double* croot;          // [task * 32 + lane] FP64 roots for the adjoint, or nullptr
+    int* status;            // [status_i] first failing period (1-based) or 0
     unsigned long long* nevals;  // secular evaluations (accumulated), or nullptr
 };
 
 struct AdjArgs {
-    const Geometry* geo;
-    int nz, kmax;
-    long long ncol, col0, ncols;
-    const float4* layers;   // [rmax][ncols]
+    Tables T;
     const double* periods;
-    const double* croot;    // [K][ncols] roots (0 where no root)
-    double* sen_vs;         // (ncol, K, nz) Fortran layout
+    const double* croot;    // [task * 32 + lane]
+    double* sen_vs;
     double* sen_vp;
     double* sen_rho;
     double* scratch;        // [(rmax-1)*6][grid threads]
+    unsigned* queue;        // work-queue counter (zeroed before the launch)
 };
 
-__global__ void adjoint_kernel(AdjArgs a);
-
 struct TiArgs {
-    const Geometry* geo;
-    int nz, kmax;
-    long long ncol, col0, ncols;
-    const float4* tilayers; // [rmax][ncols] refined (vp, vs, rho)
+    Tables T;
     const double* periods;
-    const double* pv;       // (ncol, K) phase velocities (FP32-valued)
-    float* lsen;            // (ncol, K, nz-1) Fortran layout
+    const double* pv;       // phase velocities (FP32-valued)
+    float* lsen;
     double* scratch;        // [rmax*6][grid threads]
+    unsigned* queue;        // work-queue counter (zeroed before the launch)
     int* errflag;           // set to 1 when an Lsen_Gsc value is not finite
 };
 
+// Column source: regular grid (Fortran (nx,ny,nz) arrays, shared depz and
+// periods) or ragged batch (CSR node and period arrays).
+struct ColSrc {
+    bool ragged;
+    long long ncol, col0;          // grid: column stride and first column
+    const float* vel;              // grid: vel(nx,ny,nz); ragged: vs by node_off
+    const float* vp;
+    const float* rho;
+    const float* depz;             // grid: depz(nz); ragged: by node_off
+    const long long* node_off;     // ragged
+    const long long* per_off;      // ragged
+    int nz, K;                     // grid
+    float minthk;
+    __device__ __forceinline__ int col_nz(long long c) const
+    {
+        return ragged ? (int)(node_off[c + 1] - node_off[c]) : nz;
+    }
+    __device__ __forceinline__ int col_K(long long c) const
+    {
+        return ragged ? (int)(per_off[c + 1] - per_off[c]) : K;
+    }
+    __device__ __forceinline__ float dep(long long c, int i) const
+    {
+        return ragged ? depz[node_off[c] + i] : depz[i];
+    }
+    __device__ __forceinline__ void node(long long c, int i, float& vs, float& vpo, float& rh) const
+    {
+        const long long idx = ragged ? node_off[c] + i : (col0 + c) + ncol * i;
+        vs = vel[idx];
+        if (vp) { vpo = vp[idx]; rh = rho[idx]; }
+        else brocher(vs, vpo, rh);
+    }
+};
+
+__global__ void prep_count_kernel(ColSrc src, long long ncols, unsigned* keys, int* colidx,
+                                  int* rmax_out, int* err);
+__global__ void prep_tile_kernel(long long ncols, const int* sorted_col, const int* rmax,
+                                 ColSrc src, long long* tile_recs, long long* tile_tasks);
+__global__ void prep_tasks_kernel(long long ntiles, const long long* tile_tasks,
+                                  const long long* tile_tbase, int2* tasks);
+__global__ void prep_build_kernel(ColSrc src, PrepOut o, Tables T, const int* sorted_col,
+                                  const long long* tile_tbase);
+__global__ void root_kernel(RootArgs a);
+__global__ void adjoint_kernel(AdjArgs a);
 __global__ void ti_kernel(TiArgs a);
 
 __global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);
 __global__ void fd_column_kernel(FdArgs a);
-__global__ void build_layers_kernel(BuildArgs a);
-__global__ void root_kernel(RootArgs a);
 size_t fd_smem_bytes();
+
+// Ragged batch source of the finite-difference kernel.
+struct FdBatch {
+    const long long* node_off;
+    const long long* per_off;
+    const float* depz;
+    float minthk;
+    const long long* sen_off;     // first kernel entry of each column
+    const long long* cbuf_off;    // scratch offset (floats) of each column
+};
+__global__ void fd_batch_kernel(FdArgs a, FdBatch b);
+size_t fd_batch_smem_bytes();
 
 }  // namespace dk

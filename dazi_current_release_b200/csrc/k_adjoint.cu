@@ -301,44 +301,51 @@ __device__ __forceinline__ double layer_step_val(const float4& L, double wvno, d
 }
 
 // ---------------------------------------------------------------- kernel
+// Warp-level work queue over (tile, period) tasks: a warp takes one task and
+// its 32 lanes are the tile's 32 columns at that period.
+__device__ __forceinline__ long long next_task(unsigned* queue)
+{
+    unsigned t = 0;
+    if ((threadIdx.x & 31) == 0) t = atomicAdd(queue, 1u);
+    return (long long)__shfl_sync(0xffffffffu, t, 0);
+}
+
 __global__ void __launch_bounds__(128)
 adjoint_kernel(AdjArgs a)
 {
-    __shared__ double s_per[NP];
-    for (int k = threadIdx.x; k < a.kmax; k += blockDim.x) s_per[k] = a.periods[k];
-    __syncthreads();
-    const Geometry* g = a.geo;
-    const int rmax = g->rmax, nz = a.nz, K = a.kmax;
+    const Tables& T = a.T;
     const long long nslots = (long long)gridDim.x * blockDim.x;
     const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long nitems = a.ncols * K;
-    const long long ncol = a.ncol;
-    for (long long base = (long long)blockIdx.x * blockDim.x; base < nitems; base += nslots) {
-        const long long it = base + threadIdx.x;
-        const bool inrange = it < nitems;
-        const int k = inrange ? (int)(it / a.ncols) : 0;
-        const long long c = inrange ? it % a.ncols : 0;
-        const long long post = a.col0 + c;
-        const double croot = inrange ? a.croot[c + a.ncols * k] : 0.0;
-        const bool active = inrange && croot > 0.0;
-        double* dvs = a.sen_vs + post + ncol * ((long long)k);
-        double* dvp = a.sen_vp + post + ncol * ((long long)k);
-        double* drh = a.sen_rho + post + ncol * ((long long)k);
-        const long long nstride = ncol * (long long)K;   // node stride in the outputs
-        if (!active) {
-            if (inrange)
-                for (int i = 0; i < nz; ++i) { dvs[nstride * i] = 0.0; dvp[nstride * i] = 0.0; drh[nstride * i] = 0.0; }
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        const long long task = next_task(a.queue);
+        if (task >= T.ntasks) break;
+        const int2 tk = T.tasks[task];
+        const long long s = (long long)tk.x * TILE + lane;
+        const int k = tk.y;
+        if (s >= T.ncols) continue;
+        const ColMeta M = T.meta[s];
+        if (k >= M.K) continue;
+        const double croot = a.croot[task * TILE + lane];
+        const int nz = M.nz, rmax = M.rmax;
+        double* dvs = a.sen_vs + M.sen_b + T.sen_sk * k;
+        double* dvp = a.sen_vp + M.sen_b + T.sen_sk * k;
+        double* drh = a.sen_rho + M.sen_b + T.sen_sk * k;
+        const long long nstride = M.sen_is;   // node stride in the outputs
+        if (!(croot > 0.0)) {
+            for (int i = 0; i < nz; ++i) { dvs[nstride * i] = 0.0; dvp[nstride * i] = 0.0; drh[nstride * i] = 0.0; }
             continue;
         }
-        const double omega = TWOPI / s_per[k];
+        const double omega = TWOPI / a.periods[M.per_b + k];
         const double wvno = omega / croot;
-        const float4* lay = a.layers + c;                 // [m][ncols]
-        const long long lstride = a.ncols;
-        double* scr = a.scratch + slot;                   // [(m*6 + comp)][nslots]
+        const long long lbase = T.tile_lbase[tk.x] + lane;
+        const float4* lay = T.flat + lbase;            // layer m at lay[m * TILE]
+        const ChainRec* chr = T.ch + lbase;
+        double* scr = a.scratch + slot;                // [(m*6 + comp)][nslots]
         // ---- 1. bottom-up sweep: store e(m+1) and 1/n_m for m = rmax-2 .. 0
         double e[5];
         {
-            const float4 L = lay[(long long)(rmax - 1) * lstride];
+            const float4 L = lay[(long long)(rmax - 1) * TILE];
             const double aa = L.y, bb = L.z;
             const D3 w = mk(wvno);
             const D3 xka = mk(omega / aa), xkb = mk(omega / bb);
@@ -348,7 +355,7 @@ adjoint_kernel(AdjArgs a)
             for (int q = 0; q < 5; ++q) e[q] = h[q].v;
         }
         for (int m = rmax - 2; m >= 0; --m) {
-            const float4 L = lay[(long long)m * lstride];
+            const float4 L = lay[(long long)m * TILE];
             double f[5];
             const double nrm = layer_step_val(L, wvno, omega, e, f);
             double* sp = scr + (long long)m * 6 * nslots;
@@ -365,7 +372,8 @@ adjoint_kernel(AdjArgs a)
         int cur_node = 0;
         int gexp = 0;   // g is kept as gv * 2^gexp
         for (int m = 0; m <= rmax - 2; ++m) {
-            const int node = g->node[m];
+            const ChainRec ch = chr[(long long)m * TILE];
+            const int node = ch.node;
             if (node != cur_node) {
                 // interval cur_node finished: node cur_node is complete
                 dvs[nstride * cur_node] = acc_vs;
@@ -375,20 +383,20 @@ adjoint_kernel(AdjArgs a)
                 nxt_vs = nxt_vp = nxt_rh = 0.0;
                 cur_node = node;
             }
-            const float4 L = lay[(long long)m * lstride];
+            const float4 L = lay[(long long)m * TILE];
             CAset<D3> C;
             layer_ca_d3(L, wvno, omega, C);
             const double* sp = scr + (long long)m * 6 * nslots;
             double u[5];
             for (int q = 0; q < 5; ++q) u[q] = sp[q * nslots];
             const double inv = sp[5 * nslots];
-            const Contract s = contract(C, u, gv);
+            const Contract sc5 = contract(C, u, gv);
             const double sc = ldexp(inv, gexp);
-            dFdw = fma(s.d2, sc, dFdw);
-            const double dFda = s.d0 * sc, dFdb = s.d1 * sc, dFdr = s.drho * sc / (double)L.w;
+            dFdw = fma(sc5.d2, sc, dFdw);
+            const double dFda = sc5.d0 * sc, dFdb = sc5.d1 * sc, dFdr = sc5.drho * sc / (double)L.w;
             // chain to nodes: a_flat = tmp * ((1-f) vp_i + f vp_i+1), etc.
-            const double tmpm = g->tmp[m], rf = (double)g->rhofac[m];
-            const double fw = (double)g->sub[m] / (double)g->den[m];
+            const double tmpm = ch.tmp, rf = (double)ch.rhofac;
+            const double fw = (double)ch.sub / (double)ch.den;
             acc_vp = fma(dFda * tmpm, 1.0 - fw, acc_vp); nxt_vp = fma(dFda * tmpm, fw, nxt_vp);
             acc_vs = fma(dFdb * tmpm, 1.0 - fw, acc_vs); nxt_vs = fma(dFdb * tmpm, fw, nxt_vs);
             acc_rh = fma(dFdr * rf, 1.0 - fw, acc_rh);   nxt_rh = fma(dFdr * rf, fw, nxt_rh);
@@ -401,11 +409,12 @@ adjoint_kernel(AdjArgs a)
             for (int q = 0; q < 5; ++q) gv[q] = ldexp(gn[q], -ex);
             gexp += ex;
         }
-        // half-space: all remaining contributions go to node nz-1 (together
+        // half-space: the remaining contributions go to node nz-1 (together
         // with the bottom sublayers of interval nz-2 already in nxt_*)
         {
             const int m = rmax - 1;
-            const float4 L = lay[(long long)m * lstride];
+            const float4 L = lay[(long long)m * TILE];
+            const ChainRec ch = chr[(long long)m * TILE];
             const double aa = L.y, bb = L.z, rho = L.w;
             const D3 w = {wvno, 0.0, 0.0, 1.0};
             const D3 xka = {omega / aa, -omega / (aa * aa), 0.0, 0.0};
@@ -424,8 +433,7 @@ adjoint_kernel(AdjArgs a)
                 sr = fma((double)pw[q] * h[q].v, gv[q], sr);
             }
             dFdw = fma(s2, sc, dFdw);
-            const double tmpm = g->tmp[m], rf = (double)g->rhofac[m];
-            // finish node nz-2 (if the loop ended inside its interval) and nz-1
+            const double tmpm = ch.tmp, rf = (double)ch.rhofac;
             dvs[nstride * cur_node] = acc_vs;
             dvp[nstride * cur_node] = acc_vp;
             drh[nstride * cur_node] = acc_rh;

@@ -93,23 +93,27 @@ struct FdSmem {
 };
 
 size_t fd_smem_bytes() { return sizeof(FdSmem); }
+size_t fd_batch_smem_bytes() { return sizeof(FdSmem) + sizeof(Geometry); }
 
-__global__ void __launch_bounds__(256)
-fd_column_kernel(FdArgs a)
+// One column of the finite-difference form: what the shared body needs.
+struct FdColumn {
+    const Geometry* g;
+    int nz, K;
+    long long pv_b, pv_sk;            // pv index = pv_b + pv_sk * k
+    long long sen_b, sen_sk, sen_is;  // kernel index = sen_b + sen_sk * k + sen_is * i
+    long long status_i;
+    float* cbuf;                      // [1 + 6 nz][K] FP32 phase velocities
+};
+
+// Body shared by the grid and ragged kernels.  Node values and periods are
+// already in S.vs/S.vp/S.rho and S.per; the whole block participates.
+__device__ void fd_column_body(const FdColumn& C, FdSmem& S, const FdArgs& a)
 {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    FdSmem& S = *reinterpret_cast<FdSmem*>(smem_raw);
-    const Geometry* g = a.geo;
-    const int nz = a.nz, K = a.kmax, rmax = g->rmax;
+    const Geometry* g = C.g;
+    const int nz = C.nz, K = C.K, rmax = g->rmax;
     const int nmod = 1 + 6 * nz;
-    const long long post = (long long)a.col0 + blockIdx.x;   // 0-based column
-    const long long ncol = a.ncol;
     const int tid = threadIdx.x, nthr = blockDim.x;
-    // FP32 phase velocities of the column's 1 + 6 nz models, [model][K]
-    float* cbuf = a.cscratch + (size_t)blockIdx.x * nmod * K;
-
-    load_column(tid, nthr, nz, post, ncol, a.vel, a.vp, a.rho, S.vs, S.vp, S.rho);
-    for (int k = tid; k < K; k += nthr) S.per[k] = a.periods[k];
+    float* cbuf = C.cbuf;
     if (tid == 0) {
         int acc = 0;
         for (int i = 0; i < nz - 1; ++i) { S.first[i] = acc; acc += g->nsub_of_node[i]; }
@@ -150,15 +154,15 @@ fd_column_kernel(FdArgs a)
         if (active) scan_start([&](int m) { return mdl.layerf(m); }, rmax, cc, betmx);
         int nev = 0;
         const int fk = solve_model_warp(active, mdl, rmax, cc, betmx, S.per, K, a.tol, out, &nev);
-        if (active && q == 0 && a.status) a.status[post] = fk < 0 ? 0 : fk + 1;
+        if (active && q == 0 && a.status) a.status[C.status_i] = fk < 0 ? 0 : fk + 1;
         if (a.nevals) {
             const unsigned long long w = __reduce_add_sync(0xffffffffu, (unsigned)nev);
             if ((tid & 31) == 0 && w) atomicAdd(a.nevals, w);
         }
     }
     __syncthreads();
-    // pv and the finite-difference quotients, Fortran (ncol, K[, nz]) layout
-    for (int k = tid; k < K; k += nthr) a.pv[post + ncol * k] = (double)cbuf[k];
+    // pv and the finite-difference quotients
+    for (int k = tid; k < K; k += nthr) a.pv[C.pv_b + C.pv_sk * k] = (double)cbuf[k];
     if (a.sen_vs) {
         const int nent = 3 * nz * K;
         for (int e = tid; e < nent; e += nthr) {
@@ -169,80 +173,96 @@ fd_column_kernel(FdArgs a)
             const double cp = (double)cbuf[(size_t)(base + 1) * K + k];
             const double div = (double)__fmul_rn(a.dln, nv[i]);
             double* dst = par == 0 ? a.sen_vs : (par == 1 ? a.sen_vp : a.sen_rho);
-            dst[post + ncol * ((long long)k + (long long)K * i)] = (cp - cm) / div;
+            dst[C.sen_b + C.sen_sk * k + C.sen_is * i] = (cp - cm) / div;
         }
     }
+}
+
+__global__ void __launch_bounds__(256)
+fd_column_kernel(FdArgs a)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FdSmem& S = *reinterpret_cast<FdSmem*>(smem_raw);
+    const int nz = a.nz, K = a.kmax;
+    const long long post = (long long)a.col0 + blockIdx.x;   // 0-based column
+    const long long ncol = a.ncol;
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    load_column(tid, nthr, nz, post, ncol, a.vel, a.vp, a.rho, S.vs, S.vp, S.rho);
+    for (int k = tid; k < K; k += nthr) S.per[k] = a.periods[k];
+    FdColumn C;
+    C.g = a.geo; C.nz = nz; C.K = K;
+    C.pv_b = post; C.pv_sk = ncol;
+    C.sen_b = post; C.sen_sk = ncol; C.sen_is = ncol * (long long)K;
+    C.status_i = post;
+    C.cbuf = a.cscratch + (size_t)blockIdx.x * (1 + 6 * nz) * K;
+    fd_column_body(C, S, a);
+}
+
+// Ragged batch: column c = col0 + blockIdx.x has its own depth grid and
+// periods (CSR offsets); its geometry is built in shared memory.
+__global__ void __launch_bounds__(256)
+fd_batch_kernel(FdArgs a, FdBatch b)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    FdSmem& S = *reinterpret_cast<FdSmem*>(smem_raw);
+    Geometry& G = *reinterpret_cast<Geometry*>(smem_raw + sizeof(FdSmem));
+    const long long c = (long long)a.col0 + blockIdx.x;
+    const long long n0 = b.node_off[c], p0 = b.per_off[c];
+    const int nz = (int)(b.node_off[c + 1] - n0), K = (int)(b.per_off[c + 1] - p0);
+    const int tid = threadIdx.x, nthr = blockDim.x;
+    for (int i = tid; i < nz; i += nthr) {
+        const float vs = a.vel[n0 + i];
+        float vp, rho;
+        if (a.vp) { vp = a.vp[n0 + i]; rho = a.rho[n0 + i]; }
+        else brocher(vs, vp, rho);
+        S.vs[i] = vs; S.vp[i] = vp; S.rho[i] = rho;
+    }
+    for (int k = tid; k < K; k += nthr) S.per[k] = a.periods[p0 + k];
+    if (tid == 0) build_geometry(G, b.depz + n0, nz, b.minthk);
+    __syncthreads();
+    FdColumn C;
+    C.g = &G; C.nz = nz; C.K = K;
+    C.pv_b = p0; C.pv_sk = 1;
+    C.sen_b = b.sen_off ? b.sen_off[c] : 0; C.sen_sk = 1; C.sen_is = K;
+    C.status_i = c;
+    C.cbuf = a.cscratch + b.cbuf_off[c] - b.cbuf_off[a.col0];
+    fd_column_body(C, S, a);
 }
 
 // ------------------------------------------------------------------------
-// One thread per column: the base-model root search (pv, and the FP64 roots
-// the adjoint form differentiates).  Layer tables are [layer][column] so a
-// warp's 32 columns read one layer with coalesced loads.
-struct ColumnModel {
+// One thread per column (sorted position): the base-model root search (pv,
+// and the FP64 roots the adjoint form differentiates).  A warp is one tile of
+// the layer tables, so its 32 columns read each layer with coalesced loads.
+struct TableModel {
     const LayerD* ld;
-    long long stride;
-    __device__ __forceinline__ LayerD layer(int m) const { return ld[(long long)m * stride]; }
+    long long base;
+    __device__ __forceinline__ LayerD layer(int m) const { return ld[base + (long long)m * TILE]; }
 };
-
-__global__ void build_layers_kernel(BuildArgs a)
-{
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= a.ncols) return;
-    const long long post = a.col0 + c;
-    const Geometry* g = a.geo;
-    float vs[NZMAX], vp[NZMAX], rho[NZMAX];
-    const int nz = a.nz;
-    for (int i = 0; i < nz; ++i) {
-        vs[i] = a.vel[post + a.ncol * i];
-        if (a.vp) { vp[i] = a.vp[post + a.ncol * i]; rho[i] = a.rho[post + a.ncol * i]; }
-        else brocher(vs[i], vp[i], rho[i]);
-    }
-    for (int m = 0; m < g->rmax; ++m) {
-        const float4 L = flat_layer(*g, m, vp, vs, rho);
-        a.layers[(long long)m * a.ncols + c] = L;
-        a.layersd[(long long)m * a.ncols + c] = make_layerd(L);
-        if (a.tilayers) {
-            const int i = g->node[m];
-            float4 t;
-            if (m == g->rmax - 1) { t.x = vp[i]; t.y = vs[i]; t.z = rho[i]; }
-            else {
-                t.x = sublayer_value(vp[i], vp[i + 1], g->sub[m], g->den[m]);
-                t.y = sublayer_value(vs[i], vs[i + 1], g->sub[m], g->den[m]);
-                t.z = sublayer_value(rho[i], rho[i + 1], g->sub[m], g->den[m]);
-            }
-            t.w = 0.0f;
-            a.tilayers[(long long)m * a.ncols + c] = t;
-        }
-    }
-}
 
 __global__ void __launch_bounds__(128)
 root_kernel(RootArgs a)
 {
-    __shared__ double s_per[NP];
-    for (int k = threadIdx.x; k < a.kmax; k += blockDim.x) s_per[k] = a.periods[k];
-    __syncthreads();
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool active = c < a.ncols;
-    const long long cc_ = active ? c : 0;
-    const long long post = a.col0 + cc_;
-    const int K = a.kmax;
-    const int rmax = a.geo->rmax;
-    ColumnModel mdl{a.layersd + cc_, a.ncols};
+    const Tables& T = a.T;
+    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const bool active = s < T.ncols;
+    const long long ss = active ? s : 0;
+    const ColMeta M = T.meta[ss];
+    const long long base = T.tile_lbase[ss / TILE] + (ss % TILE);
+    const double* per = a.periods + M.per_b;
+    TableModel mdl{T.ld, base};
     auto out = [&](int k, double cval, double ctight, int ev) {
-        a.pv[post + a.ncol * k] = (double)(float)cval;
-        if (a.croot) a.croot[cc_ + a.ncols * k] = ctight;
-        if (a.evals) a.evals[post + a.ncol * k] = ev;
+        a.pv[M.pv_b + T.pv_sk * k] = (double)(float)cval;
+        if (a.croot) a.croot[M.cr_b + (long long)TILE * k] = ctight;
     };
     double cc = 0.0;
     float betmx = 0.f;
     if (active) {
-        const float4* lf = a.layers + cc_;
-        scan_start([&](int m) { return lf[(long long)m * a.ncols]; }, rmax, cc, betmx);
+        const float4* lf = T.flat + base;
+        scan_start([&](int m) { return lf[(long long)m * TILE]; }, M.rmax, cc, betmx);
     }
     int nev = 0;
-    const int fk = solve_model_warp(active, mdl, rmax, cc, betmx, s_per, K, a.tol, out, &nev);
-    if (active && a.status) a.status[post] = fk < 0 ? 0 : fk + 1;
+    const int fk = solve_model_warp(active, mdl, M.rmax, cc, betmx, per, M.K, a.tol, out, &nev);
+    if (active && a.status) a.status[M.status_i] = fk < 0 ? 0 : fk + 1;
     if (a.nevals) {
         const unsigned long long w = __reduce_add_sync(0xffffffffu, (unsigned)nev);
         if ((threadIdx.x & 31) == 0 && w) atomicAdd(a.nevals, w);

@@ -21,6 +21,8 @@
 // scratch slot per thread ([layer][slot], coalesced); the down-sweep builds
 // eigenfunctions and energy integrals interface by interface and stores the
 // raw partials in the same slots for the final normalised splice.
+#include <utility>
+
 #include "dk_secular.cuh"
 #include "dk_kernels.cuh"
 
@@ -68,22 +70,22 @@ struct TiLayer {
     double d, TA, TC, TF, TL, TN, rho;
 };
 
-// Column refined values (unflattened) -> tregn96's model of layer m.
-__device__ __forceinline__ TiLayer ti_layer(const Geometry& g, int m, float rvp, float rvs, float rrh)
+// Layer record -> tregn96's model of the layer.  TA = TC = rho Vp^2 and
+// TL = TN = rho Vs^2 (depthkernelTI.f90:124-131, real*4) are stored already
+// flattened (sphere_tdisp96, tregn96.f:796-834); TF = TA - 2 TL is not
+// mapped by the flattening, so it is formed from the unflattened values.
+__device__ __forceinline__ TiLayer ti_layer(const TiRec& r)
 {
-    // depthkernelTI.f90:124-131 (real*4)
-    const float TA = __fmul_rn(rrh, __fmul_rn(rvp, rvp));
-    const float TL = __fmul_rn(rrh, __fmul_rn(rvs, rvs));
-    const float TF = __fsub_rn(TA, __fmul_rn(2.0f, TL));
-    // sphere_tdisp96 (tregn96.f:796-834): TF is not mapped
+    const float TAu = __fmul_rn(r.rrho, __fmul_rn(r.rvp, r.rvp));
+    const float TLu = __fmul_rn(r.rrho, __fmul_rn(r.rvs, r.rvs));
     TiLayer o;
-    o.d = (double)g.tdflat[m];
-    o.rho = (double)(float)__dmul_rn((double)rrh, g.f2275[m]);
-    o.TA = (double)(float)__dmul_rn((double)TA, g.f275[m]);
+    o.d = (double)r.td;
+    o.rho = (double)r.rho;
+    o.TA = (double)r.TA;
     o.TC = o.TA;
-    o.TL = (double)(float)__dmul_rn((double)TL, g.f275[m]);
+    o.TL = (double)r.TL;
     o.TN = o.TL;
-    o.TF = (double)TF;
+    o.TF = (double)__fsub_rn(TAu, __fmul_rn(2.0f, TLu));
     return o;
 }
 
@@ -176,61 +178,92 @@ __device__ __forceinline__ void ti_var_one(double r, bool osc, double dm, double
 // trig factors of modes k and l (f: 0 = cos, 1 = sin/r, 2 = r sin,
 // 3 = the exact same-mode value 4 a_k^2 exp(-ex)), in two groups subtracted.
 struct TT { signed char sg, a, b, k, c, d, l, fk, fl, grp; };
-__constant__ TT c_tt[70] = {
-    // tca(1,1) 0..5
-    {-1,1,3,1,2,4,1,3,3,0}, {-1,1,4,1,2,3,2,0,0,0}, {-1,1,4,2,2,3,1,0,0,0},
-    {+1,1,3,1,2,4,2,1,1,0}, {+1,1,3,2,2,4,1,2,2,0}, {-1,1,3,2,2,4,2,3,3,0},
-    // tca(1,2) 6..9
+// All terms, element after element: terms kTTo[q] .. kTTo[q+1]-1 form the
+// q-th needed element, in the order t11 t12 t13 t15 t16 t21 t22 t23 t25 t31
+// t32 t33 t51 t52 t61.
+constexpr TT kTT[72] = {
+    // tca(1,1)
+    {-1,1,3,1,2,4,1,3,3,0}, {-1,1,4,1,2,3,2,0,0,0}, {-1,1,4,2,2,3,1,0,0,0}, {+1,1,3,1,2,4,2,1,1,0}, {+1,1,3,2,2,4,1,2,2,0}, {-1,1,3,2,2,4,2,3,3,0},
+    // tca(1,2)
     {-1,1,4,1,2,2,2,0,1,0}, {-1,1,4,2,2,2,1,0,2,0}, {-1,1,2,1,2,4,2,0,1,1}, {-1,1,2,2,2,4,1,0,2,1},
-    // tca(1,3) 10..15
-    {+1,1,4,1,2,1,1,3,3,0}, {+1,1,4,1,1,2,2,0,0,0}, {+1,1,4,2,2,1,1,0,0,0},
-    {-1,1,1,1,2,4,2,1,1,0}, {-1,1,1,2,2,4,1,2,2,0}, {+1,1,4,2,1,2,2,3,3,0},
-    // tca(1,5) 16..19
+    // tca(1,3)
+    {+1,1,4,1,2,1,1,3,3,0}, {+1,1,4,1,1,2,2,0,0,0}, {+1,1,4,2,2,1,1,0,0,0}, {-1,1,1,1,2,4,2,1,1,0}, {-1,1,1,2,2,4,1,2,2,0}, {+1,1,4,2,1,2,2,3,3,0},
+    // tca(1,5)
     {-1,1,3,1,1,2,2,1,0,0}, {-1,1,3,2,2,1,1,2,0,0}, {-1,1,1,1,2,3,2,1,0,1}, {-1,1,1,2,2,3,1,2,0,1},
-    // tca(1,6) 20..25
-    {-1,1,2,1,1,2,2,0,0,0}, {-1,1,2,2,2,1,1,0,0,0}, {+1,1,1,1,2,2,2,1,1,0},
-    {+1,1,1,2,2,2,1,2,2,0}, {-1,1,2,1,2,1,1,3,3,0}, {-1,1,2,2,1,2,2,3,3,0},
-    // tca(2,1) 26..29
+    // tca(1,6)
+    {-1,1,2,1,1,2,2,0,0,0}, {-1,1,2,2,2,1,1,0,0,0}, {+1,1,1,1,2,2,2,1,1,0}, {+1,1,1,2,2,2,1,2,2,0}, {-1,1,2,1,2,1,1,3,3,0}, {-1,1,2,2,1,2,2,3,3,0},
+    // tca(2,1)
     {-1,1,4,1,3,3,2,0,2,0}, {-1,1,4,2,3,3,1,0,1,0}, {-1,1,3,1,3,4,2,1,0,1}, {-1,1,3,2,3,4,1,2,0,1},
-    // tca(2,2) 30..33
+    // tca(2,2)
     {-1,1,4,1,3,2,2,0,0,0}, {+1,1,2,1,3,4,2,0,0,0}, {-1,1,4,2,3,2,1,0,0,0}, {+1,1,2,2,3,4,1,0,0,0},
-    // tca(2,3) 34..37
+    // tca(2,3)
     {+1,1,4,1,3,1,2,0,2,0}, {+1,1,4,2,3,1,1,0,1,0}, {+1,1,1,1,3,4,2,1,0,1}, {+1,1,1,2,3,4,1,2,0,1},
-    // tca(2,5) 38..41
+    // tca(2,5)
     {-1,1,3,1,3,1,2,1,2,0}, {-1,1,3,2,3,1,1,2,1,0}, {-1,1,1,1,3,3,2,1,2,1}, {-1,1,1,2,3,3,1,2,1,1},
-    // tca(3,1) 42..47
-    {-1,1,4,1,4,3,2,0,0,0}, {-1,1,4,2,4,3,1,0,0,0}, {+1,1,3,2,4,4,1,2,2,0},
-    {+1,1,3,1,4,4,2,1,1,0}, {-1,1,4,1,4,3,1,3,3,0}, {-1,1,4,2,4,3,2,3,3,0},
-    // tca(3,2) 48..51
+    // tca(3,1)
+    {-1,1,4,1,4,3,2,0,0,0}, {-1,1,4,2,4,3,1,0,0,0}, {+1,1,3,2,4,4,1,2,2,0}, {+1,1,3,1,4,4,2,1,1,0}, {-1,1,4,1,4,3,1,3,3,0}, {-1,1,4,2,4,3,2,3,3,0},
+    // tca(3,2)
     {-1,1,4,1,4,2,2,0,1,0}, {-1,1,4,2,4,2,1,0,2,0}, {-1,1,2,1,4,4,2,0,1,1}, {-1,1,2,2,4,4,1,0,2,1},
-    // tca(3,3) 52..57
-    {+1,1,4,1,4,1,2,0,0,0}, {+1,1,4,2,4,1,1,0,0,0}, {-1,1,1,1,4,4,2,1,1,0},
-    {-1,1,1,2,4,4,1,2,2,0}, {+1,1,4,1,4,1,1,3,3,0}, {+1,1,4,2,4,1,2,3,3,0},
-    // tca(5,1) 58..61
+    // tca(3,3)
+    {+1,1,4,1,4,1,2,0,0,0}, {+1,1,4,2,4,1,1,0,0,0}, {-1,1,1,1,4,4,2,1,1,0}, {-1,1,1,2,4,4,1,2,2,0}, {+1,1,4,1,4,1,1,3,3,0}, {+1,1,4,2,4,1,2,3,3,0},
+    // tca(5,1)
     {-1,2,4,1,4,3,2,2,0,0}, {-1,2,4,2,4,3,1,1,0,0}, {-1,2,3,1,4,4,2,0,1,1}, {-1,2,3,2,4,4,1,0,2,1},
-    // tca(5,2) 62..65
+    // tca(5,2)
     {-1,2,4,1,4,2,2,2,1,0}, {-1,2,4,2,4,2,1,1,2,0}, {+1,2,2,1,4,4,2,2,1,0}, {+1,2,2,2,4,4,1,1,2,0},
-    // tca(6,1) 66..71 -> only 4 slots left: stored in c_tt61 below
+    // tca(6,1)
+    {-1,3,4,1,4,3,2,0,0,0}, {-1,3,4,2,4,3,1,0,0,0}, {+1,3,3,1,4,4,2,1,1,0}, {+1,3,3,2,4,4,1,2,2,0}, {-1,3,4,1,4,3,1,3,3,0}, {-1,3,4,2,4,3,2,3,3,0},
 };
-__constant__ TT c_tt61[6] = {
-    {-1,3,4,1,4,3,2,0,0,0}, {-1,3,4,2,4,3,1,0,0,0}, {+1,3,3,1,4,4,2,1,1,0},
-    {+1,3,3,2,4,4,1,2,2,0}, {-1,3,4,1,4,3,1,3,3,0}, {-1,3,4,2,4,3,2,3,3,0}};
+constexpr int kTTo[16] = {0, 6, 10, 16, 20, 26, 30, 34, 38, 42, 48, 52, 58, 62, 66, 72};
+__constant__ int c_tto[16] = {0, 6, 10, 16, 20, 26, 30, 34, 38, 42, 48, 52, 58, 62, 66, 72};
+__constant__ TT c_tt[72] = {
+    {-1,1,3,1,2,4,1,3,3,0}, {-1,1,4,1,2,3,2,0,0,0}, {-1,1,4,2,2,3,1,0,0,0}, {+1,1,3,1,2,4,2,1,1,0}, {+1,1,3,2,2,4,1,2,2,0}, {-1,1,3,2,2,4,2,3,3,0},
+    {-1,1,4,1,2,2,2,0,1,0}, {-1,1,4,2,2,2,1,0,2,0}, {-1,1,2,1,2,4,2,0,1,1}, {-1,1,2,2,2,4,1,0,2,1},
+    {+1,1,4,1,2,1,1,3,3,0}, {+1,1,4,1,1,2,2,0,0,0}, {+1,1,4,2,2,1,1,0,0,0}, {-1,1,1,1,2,4,2,1,1,0}, {-1,1,1,2,2,4,1,2,2,0}, {+1,1,4,2,1,2,2,3,3,0},
+    {-1,1,3,1,1,2,2,1,0,0}, {-1,1,3,2,2,1,1,2,0,0}, {-1,1,1,1,2,3,2,1,0,1}, {-1,1,1,2,2,3,1,2,0,1},
+    {-1,1,2,1,1,2,2,0,0,0}, {-1,1,2,2,2,1,1,0,0,0}, {+1,1,1,1,2,2,2,1,1,0}, {+1,1,1,2,2,2,1,2,2,0}, {-1,1,2,1,2,1,1,3,3,0}, {-1,1,2,2,1,2,2,3,3,0},
+    {-1,1,4,1,3,3,2,0,2,0}, {-1,1,4,2,3,3,1,0,1,0}, {-1,1,3,1,3,4,2,1,0,1}, {-1,1,3,2,3,4,1,2,0,1},
+    {-1,1,4,1,3,2,2,0,0,0}, {+1,1,2,1,3,4,2,0,0,0}, {-1,1,4,2,3,2,1,0,0,0}, {+1,1,2,2,3,4,1,0,0,0},
+    {+1,1,4,1,3,1,2,0,2,0}, {+1,1,4,2,3,1,1,0,1,0}, {+1,1,1,1,3,4,2,1,0,1}, {+1,1,1,2,3,4,1,2,0,1},
+    {-1,1,3,1,3,1,2,1,2,0}, {-1,1,3,2,3,1,1,2,1,0}, {-1,1,1,1,3,3,2,1,2,1}, {-1,1,1,2,3,3,1,2,1,1},
+    {-1,1,4,1,4,3,2,0,0,0}, {-1,1,4,2,4,3,1,0,0,0}, {+1,1,3,2,4,4,1,2,2,0}, {+1,1,3,1,4,4,2,1,1,0}, {-1,1,4,1,4,3,1,3,3,0}, {-1,1,4,2,4,3,2,3,3,0},
+    {-1,1,4,1,4,2,2,0,1,0}, {-1,1,4,2,4,2,1,0,2,0}, {-1,1,2,1,4,4,2,0,1,1}, {-1,1,2,2,4,4,1,0,2,1},
+    {+1,1,4,1,4,1,2,0,0,0}, {+1,1,4,2,4,1,1,0,0,0}, {-1,1,1,1,4,4,2,1,1,0}, {-1,1,1,2,4,4,1,2,2,0}, {+1,1,4,1,4,1,1,3,3,0}, {+1,1,4,2,4,1,2,3,3,0},
+    {-1,2,4,1,4,3,2,2,0,0}, {-1,2,4,2,4,3,1,1,0,0}, {-1,2,3,1,4,4,2,0,1,1}, {-1,2,3,2,4,4,1,0,2,1},
+    {-1,2,4,1,4,2,2,2,1,0}, {-1,2,4,2,4,2,1,1,2,0}, {+1,2,2,1,4,4,2,2,1,0}, {+1,2,2,2,4,4,1,1,2,0},
+    {-1,3,4,1,4,3,2,0,0,0}, {-1,3,4,2,4,3,1,0,0,0}, {+1,3,3,1,4,4,2,1,1,0}, {+1,3,3,2,4,4,1,2,2,0}, {-1,3,4,1,4,3,1,3,3,0}, {-1,3,4,2,4,3,2,3,3,0},
+};
 
-// element order: t11 t12 t13 t15 t16 t21 t22 t23 t25 t31 t32 t33 t51 t52 (t61)
-__constant__ unsigned char c_tt_off[15] = {0, 6, 10, 16, 20, 26, 30, 34, 38, 42, 48, 52, 58, 62, 66};
-
-__device__ __forceinline__ double tca_sum(int lo, int hi, const TT* tab, const double xs[5][3],
-                                          const double fac[3][4])
+// One term with compile-time indices (registers only).
+template <int I, class T, class F>
+__device__ __forceinline__ T tca_term(const T (&xs)[5][3], const F (&fac)[3][4])
 {
-    double g0 = 0.0, g1 = 0.0;
-    for (int i = lo; i < hi; ++i) {
-        const TT t = tab[i];
-        double v = (xs[t.a][t.k] * xs[t.b][t.k]) * (xs[t.c][t.l] * xs[t.d][t.l]);
-        if (t.sg < 0) v = -v;
-        v = (t.fk == 3) ? v * fac[t.k][3] : (v * fac[t.k][t.fk]) * fac[t.l][t.fl];
-        if (t.grp) g1 += v; else g0 += v;
-    }
+    constexpr TT t = kTT[I];
+    T v = (xs[t.a][t.k] * xs[t.b][t.k]) * (xs[t.c][t.l] * xs[t.d][t.l]);
+    if constexpr (t.sg < 0) v = -v;
+    if constexpr (t.fk == 3) return v * fac[t.k][3];
+    else return (v * fac[t.k][t.fk]) * fac[t.l][t.fl];
+}
+
+template <class T, class F, int... Is>
+__device__ __forceinline__ T tca_expand(const T (&xs)[5][3], const F (&fac)[3][4],
+                                        std::integer_sequence<int, Is...>)
+{
+    T g0 = T(0.0), g1 = T(0.0);
+    ((kTT[Is].grp ? (g1 = g1 + tca_term<Is>(xs, fac)) : (g0 = g0 + tca_term<Is>(xs, fac))), ...);
     return g0 - g1;
+}
+
+template <int LO, class S> struct Shift;
+template <int LO, int... Is>
+struct Shift<LO, std::integer_sequence<int, Is...>> {
+    using type = std::integer_sequence<int, (LO + Is)...>;
+};
+
+template <int Q, class T, class F>
+__device__ __forceinline__ T tca_elem(const T (&xs)[5][3], const F (&fac)[3][4])
+{
+    using S = typename Shift<kTTo[Q], std::make_integer_sequence<int, kTTo[Q + 1] - kTTo[Q]>>::type;
+    return tca_expand(xs, fac, S{});
 }
 
 // dnka_tregn (elastic) in real arithmetic: the reduced 5x5 compound matrix.
@@ -248,9 +281,11 @@ __device__ __forceinline__ void ti_compound(const TiEig& E, const TiVar& v, doub
     xs[1][1] = E.x11; xs[2][1] = E.x21; xs[3][1] = E.x31; xs[4][1] = E.x41;
     xs[1][2] = E.x12; xs[2][2] = E.x22; xs[3][2] = E.x32; xs[4][2] = E.x42;
     double t[15];
-#pragma unroll
-    for (int q = 0; q < 14; ++q) t[q] = tca_sum(c_tt_off[q], q == 13 ? 66 : c_tt_off[q + 1], c_tt, xs, fac);
-    t[14] = tca_sum(0, 6, c_tt61, xs, fac);
+    t[0] = tca_elem<0>(xs, fac);   t[1] = tca_elem<1>(xs, fac);   t[2] = tca_elem<2>(xs, fac);
+    t[3] = tca_elem<3>(xs, fac);   t[4] = tca_elem<4>(xs, fac);   t[5] = tca_elem<5>(xs, fac);
+    t[6] = tca_elem<6>(xs, fac);   t[7] = tca_elem<7>(xs, fac);   t[8] = tca_elem<8>(xs, fac);
+    t[9] = tca_elem<9>(xs, fac);   t[10] = tca_elem<10>(xs, fac); t[11] = tca_elem<11>(xs, fac);
+    t[12] = tca_elem<12>(xs, fac); t[13] = tca_elem<13>(xs, fac); t[14] = tca_elem<14>(xs, fac);
     const double t11 = t[0], t12 = t[1], t13 = t[2], t15 = t[3], t16 = t[4], t21 = t[5];
     const double t22 = t[6], t23 = t[7], t25 = t[8], t31 = t[9], t32 = t[10], t33 = t[11];
     const double t51 = t[12], t52 = t[13], t61 = t[14];
@@ -462,9 +497,9 @@ __device__ void ti_compound_z(const TiEigZ& E, const TiVarZ& v, double ca[5][5])
     xs[1][2] = E.x12; xs[2][2] = E.x22; xs[3][2] = E.x32; xs[4][2] = E.x42;
     double t[15];
     for (int q = 0; q < 15; ++q) {
-        const TT* tab = q < 14 ? c_tt : c_tt61;
-        const int lo = q < 14 ? c_tt_off[q] : 0;
-        const int hi = q < 13 ? c_tt_off[q + 1] : (q == 13 ? 66 : 6);
+        const TT* tab = c_tt;
+        const int lo = c_tto[q];
+        const int hi = c_tto[q + 1];
         zc g0 = Z(0.0), g1 = Z(0.0);
         for (int i = lo; i < hi; ++i) {
             const TT tt = tab[i];
@@ -571,44 +606,44 @@ __device__ __forceinline__ double pow2_normalise(double* v, int n)
     return (double)ex * 0.6931471805599453;
 }
 
-__device__ __forceinline__ void col_refined(const Geometry& g, int m, const float4* ti, long long stride,
-                                            float& rvp, float& rvs, float& rrh)
+__device__ __forceinline__ long long ti_next_task(unsigned* queue)
 {
-    const float4 t = ti[(long long)m * stride];
-    rvp = t.x; rvs = t.y; rrh = t.z;
+    unsigned t = 0;
+    if ((threadIdx.x & 31) == 0) t = atomicAdd(queue, 1u);
+    return (long long)__shfl_sync(0xffffffffu, t, 0);
 }
 
 __global__ void __launch_bounds__(128)
 ti_kernel(TiArgs a)
 {
-    __shared__ double s_per[NP];
-    for (int k = threadIdx.x; k < a.kmax; k += blockDim.x) s_per[k] = a.periods[k];
-    __syncthreads();
-    const Geometry& g = *a.geo;
-    const int rmax = g.rmax, nz = a.nz, K = a.kmax;
+    const Tables& T = a.T;
     const long long nslots = (long long)gridDim.x * blockDim.x;
     const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const long long nitems = a.ncols * K;
-    const long long ncol = a.ncol;
-    for (long long base = (long long)blockIdx.x * blockDim.x; base < nitems; base += nslots) {
-        const long long it = base + threadIdx.x;
-        if (it >= nitems) continue;
-        const int k = (int)(it / a.ncols);
-        const long long c = it % a.ncols;
-        const long long post = a.col0 + c;
-        float* lout = a.lsen + post + ncol * (long long)k;
-        const long long jstride = ncol * (long long)K;
-        const float cpf = (float)a.pv[post + ncol * (long long)k];
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        const long long task = ti_next_task(a.queue);
+        if (task >= T.ntasks) break;
+        const int2 tk = T.tasks[task];
+        const long long s = (long long)tk.x * TILE + lane;
+        const int k = tk.y;
+        if (s >= T.ncols) continue;
+        const ColMeta M = T.meta[s];
+        if (k >= M.K) continue;
+        const int rmax = M.rmax, nz = M.nz;
+        float* lout = a.lsen + M.ls_b + T.ls_sk * k;
+        const long long jstride = M.ls_is;
+        const float cpf = (float)a.pv[M.pv_b + T.pv_sk * k];
         if (!(cpf > 0.0f)) {
             for (int j = 0; j < nz - 1; ++j) lout[jstride * j] = 0.0f;
             continue;
         }
-        const float4* ti = a.tilayers + c;
-        const long long ls = a.ncols;
-        double* scr = a.scratch + slot;          // [(m*6 + q)][nslots]
+        const long long lbase = T.tile_lbase[tk.x] + lane;
+        const TiRec* tir = T.ti + lbase;              // layer m at tir[m * TILE]
+        const ChainRec* chr = T.ch + lbase;
+        double* scr = a.scratch + slot;               // [(m*6 + q)][nslots]
         // tregn96.f:430-479: twopi real*4, t and cp real*4
         const float twopi = 6.2831855f;
-        const double omega = (double)twopi / (double)(float)s_per[k];
+        const double omega = (double)twopi / (double)(float)a.periods[M.per_b + k];
         const double wvno = omega / (double)cpf;
         const double wvno2 = wvno * wvno;
         // ---- up(): compound vectors from the half-space upward
@@ -616,9 +651,7 @@ ti_kernel(TiArgs a)
         double exsum = 0.0;
         {
             // half-space: E^-1 rows 1-2 and their 2x2 minors (evalg, up)
-            float rvp, rvs, rrh;
-            col_refined(g, rmax - 1, ti, ls, rvp, rvs, rrh);
-            const TiLayer L = ti_layer(g, rmax - 1, rvp, rvs, rrh);
+            const TiLayer L = ti_layer(tir[(long long)(rmax - 1) * TILE]);
             TiEigZ E;
             ti_eigen_z(L, omega, wvno, wvno2, E);
             zc e[4][4], G[4][4];
@@ -633,9 +666,7 @@ ti_kernel(TiArgs a)
             sp[5 * nslots] = 0.0;
         }
         for (int m = rmax - 2; m >= 0; --m) {
-            float rvp, rvs, rrh;
-            col_refined(g, m, ti, ls, rvp, rvs, rrh);
-            const TiLayer L = ti_layer(g, m, rvp, rvs, rrh);
+            const TiLayer L = ti_layer(tir[(long long)m * TILE]);
             TiEig E;
             ti_eigen(L, omega, wvno, wvno2, E);
             double ca[5][5];
@@ -675,9 +706,7 @@ ti_kernel(TiArgs a)
         double sumi0 = 0.0, sumi1 = 0.0, sumi2 = 0.0, gsum = 0.0;
         const double pi_ = 3.141592653589493;   // gammap's constant, as in the reference
         for (int m = 0; m < rmax; ++m) {
-            float rvp, rvs, rrh;
-            col_refined(g, m, ti, ls, rvp, rvs, rrh);
-            const TiLayer L = ti_layer(g, m, rvp, rvs, rrh);
+            const TiLayer L = ti_layer(tir[(long long)m * TILE]);
             TiEig E;
             ti_eigen(L, omega, wvno, wvno2, E);
             TiEigZ EZ;
@@ -760,12 +789,11 @@ ti_kernel(TiArgs a)
         int m = 0;
         for (int j = 0; j < nz - 1; ++j) {
             float acc = 0.0f;
-            const int ns = g.nsub_of_node[j];
-            for (int q = 0; q < ns; ++q, ++m) {
-                float rvp, rvs, rrh;
-                col_refined(g, m, ti, ls, rvp, rvs, rrh);
+            for (; m < rmax - 1 && chr[(long long)m * TILE].node == j; ++m) {
+                const TiRec R = tir[(long long)m * TILE];
+                const float rvp = R.rvp, rvs = R.rvs, rrh = R.rrho;
                 const double* so = scr + (long long)m * 6 * nslots;
-                const double vt = (double)g.vtp[m];
+                const double vt = (double)R.vtp;
                 double vah = so[0] / un * vt / tm3;
                 double vbv = so[nslots] / un * vt / tm3;
                 double vn = so[2 * nslots] / un;

@@ -146,6 +146,35 @@ int dazi_dk_iso_noalloc_dev(int nx, int ny, int nz, const float *vel,
                             const float *depz, float minthk, int col_start,
                             int col_count, int *status, void *stream);
 
+/* Ragged batch: columns with their own depth grids and period lists (for
+ * instance the cells of many Voronoi realisations), the extension that
+ * replaces the reference's fixed column tiles (pdsurf_tile_columns /
+ * ti_tile_columns, depthkernel_ti_process_batch.py:17-28).  CSR layout:
+ * column c has nodes node_off[c] .. node_off[c+1]-1 (depz, vs and optional
+ * vp, rho) and periods per_off[c] .. per_off[c+1]-1 (ascending).  Outputs:
+ * pv[per_off[c] + k]; sen_*[sen_off[c] + k + K_c i] (K_c periods x nz_c
+ * nodes, column-major as one column of the reference's arrays);
+ * lsen[ls_off[c] + k + K_c j] (K_c x (nz_c - 1)).  sen_* / lsen may be NULL
+ * (with their offsets).  status[c] as dazi_dk_last_status.  minthk is the
+ * common sublayer count.  Host-pointer form: */
+int dazi_dk_batch(long long ncols, const long long *node_off,
+                  const float *depz, const float *vs, const float *vp,
+                  const float *rho, const long long *per_off,
+                  const double *periods, float minthk, double *pv,
+                  const long long *sen_off, double *sen_vs, double *sen_vp,
+                  double *sen_rho, const long long *ls_off, float *lsen,
+                  int form, int *status);
+
+/* Device-pointer form of dazi_dk_batch (all arrays in device memory,
+ * stream-ordered on `stream`; one small synchronisation sizes the tables). */
+int dazi_dk_batch_dev(long long ncols, const long long *node_off,
+                      const float *depz, const float *vs, const float *vp,
+                      const float *rho, const long long *per_off,
+                      const double *periods, float minthk, double *pv,
+                      const long long *sen_off, double *sen_vs,
+                      double *sen_vp, double *sen_rho, const long long *ls_off,
+                      float *lsen, int form, int *status, void *stream);
+
 /* Number of kernel launches the last call issued (all on its stream). */
 int dazi_dk_last_launches(void);
 

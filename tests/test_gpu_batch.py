@@ -1,0 +1,84 @@
+"""Ragged batch (per-column depth grids and period lists) against the CPU
+oracle run column by column, for both forms."""
+import numpy as np
+import pytest
+
+from conftest import rel_l2
+import dazi_current_release_b200 as dk
+from dazi_current_release_b200 import synthetic as S
+from dazi_current_release_b200.batch import depthkernel_batch
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def small_batch():
+    return S.config3(realisations=1, columns=70, base_seed=1000)
+
+
+def _oracle_column(oracle, b, c, ti=True):
+    dep, vs, per = b.column(c)
+    vel = vs.reshape(1, 1, -1)
+    iso = oracle.depthkernel(vel, dep, per, b.minthk)
+    out = {"pv": iso["pvRc"][0], "svs": iso["sen_vs"][0], "svp": iso["sen_vp"][0],
+           "srh": iso["sen_rho"][0], "status": iso["status"][0]}
+    if ti:
+        out["lsen"] = oracle.depthkernel_ti(vel, dep, per, b.minthk)["Lsen_Gsc"][0]
+    return out
+
+
+def test_batch_plain_and_ti_match_oracle(oracle, small_batch):
+    b = small_batch
+    r = depthkernel_batch(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk,
+                          form=dk.FORM_PLAIN)
+    worst_ls = 0.0
+    for c in range(b.ncol):
+        ref = _oracle_column(oracle, b, c)
+        pv, svs, svp, srh, ls = r.column(c)
+        assert r["status"][c] == ref["status"]
+        np.testing.assert_array_equal(pv, ref["pv"])
+        for got, exp in ((svs, ref["svs"]), (svp, ref["svp"]), (srh, ref["srh"])):
+            assert rel_l2(got, exp) <= 1e-4
+        worst_ls = max(worst_ls, rel_l2(ls, ref["lsen"]))
+    print("batch plain: Lsen worst per-column rel-L2", worst_ls)
+    assert worst_ls <= 1e-5
+
+
+def test_batch_adjoint_matches_plain_within_reference_gates(oracle, small_batch):
+    b = small_batch
+    ra = depthkernel_batch(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk,
+                           form=dk.FORM_ADJOINT)
+    rp = depthkernel_batch(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk,
+                           form=dk.FORM_PLAIN)
+    np.testing.assert_array_equal(ra["pv"], rp["pv"])
+    np.testing.assert_array_equal(ra["lsen"], rp["lsen"])
+    gates = {"sen_vs": 1e-3, "sen_vp": 2e-3, "sen_rho": 2e-3}
+    worst = {n: 0.0 for n in gates}
+    for c in range(b.ncol):
+        a = ra.column(c)
+        p = rp.column(c)
+        for q, n in enumerate(("sen_vs", "sen_vp", "sen_rho")):
+            worst[n] = max(worst[n], rel_l2(a[1 + q], p[1 + q]))
+    print("batch adjoint vs plain worst per-column rel-L2", worst)
+    for n, w in worst.items():
+        assert w <= gates[n], (n, w)
+
+
+def test_grid_and_batch_agree(small_batch):
+    """A grid column run through the batch path gives the grid path's bits."""
+    case = S.subgrid(S.config1(), 3, 2)
+    nx, ny, nz = case.vel.shape
+    K = case.periods.size
+    pv, svs, svp, srh, ls = dk.depthkernel_fused(nx, ny, nz, case.vel, 2, 0, K, case.periods,
+                                                 case.depz, case.minthk, form=dk.FORM_ADJOINT)
+    n = nx * ny
+    node_off = np.arange(n + 1, dtype=np.int64) * nz
+    per_off = np.arange(n + 1, dtype=np.int64) * K
+    vs = case.vel.reshape(n, nz, order="F").ravel()
+    r = depthkernel_batch(node_off, np.tile(case.depz, n), vs, per_off, np.tile(case.periods, n),
+                          case.minthk, form=dk.FORM_ADJOINT)
+    for c in range(n):
+        p, a, b_, d, l = r.column(c)
+        np.testing.assert_array_equal(p, pv[c])
+        np.testing.assert_array_equal(a, svs[c])
+        np.testing.assert_array_equal(l, ls[c])
