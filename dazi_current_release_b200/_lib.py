@@ -32,7 +32,8 @@ EXPORTS = (
     "dazi_dk_iso", "dazi_dk_iso_vpvsrho", "dazi_dk_last_status", "dazi_dk_iso_dev",
     "dazi_dk_last_error", "dazi_dk_version", "dazi_dk_finalize", "dazi_dk_fp64_peak", "dazi_dk_last_work",
     "dazi_dk_ti", "dazi_dk_fused", "dazi_dk_fused_dev", "dazi_dk_last_launches",
-    "dazi_dk_iso_noalloc_dev", "dazi_dk_batch", "dazi_dk_batch_dev",
+    "dazi_dk_iso_noalloc_dev", "dazi_dk_batch", "dazi_dk_batch_dev", "dazi_dk_set_timing",
+    "dazi_dk_last_timing",
 )
 
 
@@ -91,6 +92,10 @@ def load(build_if_missing: bool = True):
     L.dazi_dk_batch.restype = _int
     L.dazi_dk_batch_dev.argtypes = [ll] + [vp_] * 7 + [ctypes.c_float] + [vp_] * 7 + [_int, vp_, vp_]
     L.dazi_dk_batch_dev.restype = _int
+    L.dazi_dk_set_timing.argtypes = [_int]
+    L.dazi_dk_set_timing.restype = _int
+    L.dazi_dk_last_timing.argtypes = [ctypes.POINTER(ctypes.c_char_p), _f64p, _int]
+    L.dazi_dk_last_timing.restype = _int
     L.dazi_dk_last_launches.argtypes = []
     L.dazi_dk_last_launches.restype = _int
     L.dazi_dk_last_error.argtypes = []
@@ -113,3 +118,12 @@ def check(code: int) -> int:
         msg = load().dazi_dk_last_error().decode(errors="replace")
         raise DaziError(code, msg)
     return code
+
+
+def last_timing(cap: int = 16) -> dict:
+    """Per-phase milliseconds of the last call (needs dazi_dk_set_timing(1))."""
+    L = load()
+    names = (ctypes.c_char_p * cap)()
+    ms = (ctypes.c_double * cap)()
+    n = check(L.dazi_dk_last_timing(names, ms, cap))
+    return {names[i].decode(): ms[i] for i in range(n)}

@@ -63,8 +63,18 @@ struct DBuf {
     template <class T> T* as() const { return reinterpret_cast<T*>(p); }
 };
 
+// Optional per-phase timing with CUDA events on the call's stream.
+struct PhaseTimer {
+    bool on = false;
+    int n = 0;
+    const char* name[16];
+    cudaEvent_t ev[17];
+    bool made = false;
+};
+
 struct Context {
     bool ready = false;
+    PhaseTimer timer;
     int device = -1;
     cudaStream_t stream = nullptr;
     // host-entry staging
@@ -88,6 +98,27 @@ struct Context {
 
 Context g_ctx;
 std::mutex g_mu;
+
+void phase_begin(cudaStream_t st)
+{
+    PhaseTimer& T = g_ctx.timer;
+    T.n = 0;
+    if (!T.on) return;
+    if (!T.made) {
+        for (int i = 0; i < 17; ++i) cudaEventCreate(&T.ev[i]);
+        T.made = true;
+    }
+    cudaEventRecord(T.ev[0], st);
+}
+
+void phase_mark(const char* name, cudaStream_t st)
+{
+    PhaseTimer& T = g_ctx.timer;
+    if (!T.on || T.n >= 16) return;
+    T.name[T.n] = name;
+    cudaEventRecord(T.ev[T.n + 1], st);
+    ++T.n;
+}
 
 int ensure_context()
 {
@@ -254,6 +285,7 @@ int build_tables(const ColSrc& src, long long ncols, const PrepOut& po, long lon
     prep_build_kernel<<<nb, bt, 0, st>>>(src, po, T, g_ctx.cidx2.as<int>(), g_ctx.ttbase.as<long long>());
     CK(cudaGetLastError());
     g_ctx.last_launches += 5;
+    phase_mark("prep", st);
     return 0;
 }
 
@@ -286,6 +318,7 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
         root_kernel<<<(unsigned)((T.ncols + bt - 1) / bt), bt, 0, st>>>(a);
         CK(cudaGetLastError());
         ++g_ctx.last_launches;
+        phase_mark("root", st);
     }
     const long long nitems = T.ntasks * TILE;
     if (adj) {
@@ -303,6 +336,7 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
         adjoint_kernel<<<(unsigned)nblk, at, 0, st>>>(j);
         CK(cudaGetLastError());
         ++g_ctx.last_launches;
+        phase_mark("adjoint", st);
     }
     if (o.lsen) {
         const int at = 128;
@@ -318,6 +352,7 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
         ti_kernel<<<(unsigned)nblk, at, 0, st>>>(t);
         CK(cudaGetLastError());
         ++g_ctx.last_launches;
+        phase_mark("ti", st);
     }
     return 0;
 }
@@ -340,6 +375,7 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
     CK(cudaMemsetAsync(g_ctx.counters.p, 0, sizeof(unsigned long long) * 4, st));
     g_ctx.last_rmax = g_ctx.geo_rmax;
     g_ctx.last_launches = 0;
+    phase_begin(st);
     const bool fd = o.svs && form == DAZI_FORM_PLAIN;
     if (fd) {
         const int nmod = 1 + 6 * nz;
@@ -365,6 +401,7 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
             CK(cudaGetLastError());
             ++g_ctx.last_launches;
         }
+        phase_mark("fd", st);
         if (!o.lsen) return 0;
     }
     ColSrc src;
@@ -401,6 +438,7 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
     CK(cudaMemsetAsync(g_ctx.counters.p, 0, sizeof(unsigned long long) * 4, st));
     g_ctx.last_launches = 0;
     g_ctx.last_rmax = 0;
+    phase_begin(st);
     ColSrc src;
     src.ragged = true; src.ncol = 0; src.col0 = 0;
     src.vel = B.vs; src.vp = B.vp; src.rho = B.rho; src.depz = B.depz;
@@ -445,6 +483,7 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
             ++g_ctx.last_launches;
             c0 = c1;
         }
+        phase_mark("fd", st);
     }
     return run_tables(T, B.periods, o, form, fd, st);
 }
@@ -793,6 +832,29 @@ int dazi_dk_batch(long long ncols, const long long* node_off, const float* depz,
     return DAZI_OK;
 }
 
+int dazi_dk_set_timing(int on)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    g_ctx.timer.on = on != 0;
+    return 0;
+}
+
+int dazi_dk_last_timing(const char** names, double* ms, int cap)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    PhaseTimer& T = g_ctx.timer;
+    if (!T.on || !T.made) return 0;
+    if (cudaEventSynchronize(T.ev[T.n]) != cudaSuccess) { cudaGetLastError(); set_err("event sync failed"); return DAZI_ERR_CUDA; }
+    const int n = T.n < cap ? T.n : cap;
+    for (int i = 0; i < n; ++i) {
+        float f = 0.f;
+        cudaEventElapsedTime(&f, T.ev[i], T.ev[i + 1]);
+        if (names) names[i] = T.name[i];
+        if (ms) ms[i] = f;
+    }
+    return n;
+}
+
 int dazi_dk_last_launches(void)
 {
     std::lock_guard<std::mutex> lk(g_mu);
@@ -806,7 +868,7 @@ int dazi_dk_last_work(long long* secular_evals, long long* layer_evals)
     unsigned long long h[4] = {0, 0, 0, 0};
     CK(cudaMemcpy(h, g_ctx.counters.p, sizeof(h), cudaMemcpyDeviceToHost));
     if (secular_evals) *secular_evals = (long long)h[0];
-    if (layer_evals) *layer_evals = (long long)h[0] * (long long)g_ctx.last_rmax;
+    if (layer_evals) *layer_evals = (long long)h[3];
     return 0;
 }
 

@@ -157,7 +157,8 @@ __device__ void fd_column_body(const FdColumn& C, FdSmem& S, const FdArgs& a)
         if (active && q == 0 && a.status) a.status[C.status_i] = fk < 0 ? 0 : fk + 1;
         if (a.nevals) {
             const unsigned long long w = __reduce_add_sync(0xffffffffu, (unsigned)nev);
-            if ((tid & 31) == 0 && w) atomicAdd(a.nevals, w);
+            const unsigned long long wl = __reduce_add_sync(0xffffffffu, (unsigned)(nev * rmax));
+            if ((tid & 31) == 0 && w) { atomicAdd(a.nevals, w); atomicAdd(a.nevals + 3, wl); }
         }
     }
     __syncthreads();
@@ -265,7 +266,8 @@ root_kernel(RootArgs a)
     if (active && a.status) a.status[M.status_i] = fk < 0 ? 0 : fk + 1;
     if (a.nevals) {
         const unsigned long long w = __reduce_add_sync(0xffffffffu, (unsigned)nev);
-        if ((threadIdx.x & 31) == 0 && w) atomicAdd(a.nevals, w);
+        const unsigned long long wl = __reduce_add_sync(0xffffffffu, (unsigned)(nev * (active ? M.rmax : 0)));
+        if ((threadIdx.x & 31) == 0 && w) { atomicAdd(a.nevals, w); atomicAdd(a.nevals + 3, wl); }
     }
 }
 

@@ -175,12 +175,20 @@ int dazi_dk_batch_dev(long long ncols, const long long *node_off,
                       double *sen_vp, double *sen_rho, const long long *ls_off,
                       float *lsen, int form, int *status, void *stream);
 
+/* Per-phase timing: with dazi_dk_set_timing(1), each call records CUDA
+ * events on its stream around its phases ("prep", "fd", "root", "adjoint",
+ * "ti"); dazi_dk_last_timing fills up to cap (name, milliseconds) pairs of
+ * the last call (waiting for its events) and returns their number. */
+int dazi_dk_set_timing(int on);
+int dazi_dk_last_timing(const char **names, double *ms, int cap);
+
 /* Number of kernel launches the last call issued (all on its stream). */
 int dazi_dk_last_launches(void);
 
 /* Work done by the last call, for roofline accounting: the number of
- * Rayleigh secular-function evaluations (each one a pass over the refined
- * layer stack) and evaluations x layers.  Synchronises with the device. */
+ * Rayleigh secular-function evaluations of the root searches (each one a
+ * pass over a refined layer stack) and the sum of evaluations x layers.
+ * Synchronises with the device. */
 int dazi_dk_last_work(long long *secular_evals, long long *layer_evals);
 
 /* Diagnostic: measured FP64 FMA throughput of the current device in

@@ -52,6 +52,10 @@ int or_depthkernelTI(int nx, int ny, int nz, const float *vel, const float *vp_i
                      const float *rho_in, double *pvRc, int iwave, int igr, int kmax,
                      const double *tRc, const float *depz, float minthk, float *Lsen,
                      int col_start, int col_count, int nthreads, int *status_out);
+int or_batch(long ncols, const long *node_off, const float *depz, const float *vs_all,
+             const long *per_off, const double *periods, float minthk, double *pv,
+             const long *sen_off, double *svs, double *svp, double *srh, const long *ls_off,
+             float *lsen, int nthreads);
 #ifdef __cplusplus
 }
 #endif

@@ -75,6 +75,9 @@ def lib():
         L.or_surfdisp96_d.argtypes = [_f64p, _f64p, _f64p, _f64p, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int, _f64p, _f64p, ctypes.c_double]
         L.or_surfdisp96_d.restype = ctypes.c_int
+        L.or_batch.argtypes = [ctypes.c_long, _i64p, _f32p, _f32p, _i64p, _f64p, ctypes.c_float,
+                               _f64p, _i64p, _f64p, _f64p, _f64p, _i64p, _f32p, ctypes.c_int]
+        L.or_batch.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -239,3 +242,27 @@ def tregn96(thk, TA, TC, TF, TL, TN, rho, periods, cp, nsph=1, dogam=1, full=Fal
     if r != 0:
         raise RuntimeError("oracle tregn96 failed")
     return (tuple(out) + (fb,)) if full else tuple(out)
+
+
+def batch(node_off, depz, vs, per_off, periods, minthk, kernels=True, lsen=True, nthreads=0):
+    """Oracle of the ragged batch (reference algorithms column by column,
+    OpenMP over columns).  Outputs in the batch layout (see or_batch)."""
+    node_off = np.ascontiguousarray(node_off, np.int64)
+    per_off = np.ascontiguousarray(per_off, np.int64)
+    nz = np.diff(node_off)
+    K = np.diff(per_off)
+    sen_off = np.concatenate([[0], np.cumsum(K * nz)]).astype(np.int64)
+    ls_off = np.concatenate([[0], np.cumsum(K * (nz - 1))]).astype(np.int64)
+    pv = np.zeros(int(per_off[-1]))
+    sen = [np.zeros(int(sen_off[-1])) for _ in range(3)] if kernels else [None] * 3
+    ls = np.zeros(int(ls_off[-1]), np.float32) if lsen else None
+    r = lib().or_batch(node_off.size - 1, _p(node_off, _i64p),
+                       _p(np.ascontiguousarray(depz, np.float32), _f32p),
+                       _p(np.ascontiguousarray(vs, np.float32), _f32p), _p(per_off, _i64p),
+                       _p(np.ascontiguousarray(periods, np.float64), _f64p), ctypes.c_float(minthk),
+                       _p(pv, _f64p), _p(sen_off, _i64p), _p(sen[0], _f64p), _p(sen[1], _f64p),
+                       _p(sen[2], _f64p), _p(ls_off, _i64p), _p(ls, _f32p), nthreads)
+    if r != 0:
+        raise RuntimeError("oracle batch failed")
+    return dict(pv=pv, sen_vs=sen[0], sen_vp=sen[1], sen_rho=sen[2], lsen=ls,
+                sen_off=sen_off, ls_off=ls_off)
