@@ -4,22 +4,32 @@
 One column-period = the Rayleigh phase velocity c(T) of one column plus its
 Vs-type kernels (dc/dVs, dc/dVp, dc/drho at every node) plus its Gc/Gs kernel
 (Lsen_Gsc at every depth interval).  A "step" is one pass of the stage over
-the whole workload (dazi_dk_fused: one phase-velocity pass feeds both).
+the whole workload (one phase-velocity pass feeds both kernel kinds).
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload config1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload config3]
                     [--form plain|adjoint] [--impl ours|reference]
 
+Default workload: the uneven batch, 100 realisations x 2500 columns (10-60
+layers, 8-40 periods each, sediments and low-velocity zones), through the
+ragged batch entries dazi_dk_batch_dev / dazi_dk_batch.  The grid workloads
+(config0/1/2/4: one depth grid for all columns) go through
+dazi_dk_fused_dev / dazi_dk_fused.
+
 value      device-timed throughput of the chosen form (--form, default the
-           adjoint form), inputs resident in HBM (device entry
-           dazi_dk_fused_dev on torch's stream, CUDA events per step, L2
-           flushed between steps outside the timed events); the other form is
-           timed the same way and reported as "plain" / "adjoint"
-e2e        the same through the host C-ABI entry dazi_dk_fused with pinned
-           host buffers: host->device inputs and device->host outputs every
-           step
-roofline   FP64 CUDA-core bound: algorithmic FLOPs (180 per layer per secular
-           evaluation, evaluations counted by the kernels) / kernel time,
-           against the FP64 FMA peak measured live by dazi_dk_fp64_peak
+           adjoint form) on the whole batch, inputs resident in HBM (device
+           entry on torch's stream, CUDA events per step, L2 flushed between
+           steps outside the timed events)
+same_columns  both forms timed the same way on the first --plain-cols
+           columns (the plain perturb-and-recompute form runs 1 + 6 nz root
+           searches per column and would take minutes on the whole batch)
+e2e        the same stage through the host C-ABI entry with pinned host
+           buffers: host->device inputs and device->host outputs every step
+roofline   FP64 CUDA-core bound of the dominant kernel (per-phase CUDA events
+           inside the library): root search 180 FP64 flops per layer per
+           secular evaluation (evaluations counted by the kernel); adjoint and
+           Gc/Gs sweeps the FP64 operations per layer item counted by ncu
+           (profiles/kernel_work.json) x the layer items of the call; peak the
+           FP64 FMA rate measured live by dazi_dk_fp64_peak
 cpu_baseline  the CPU oracle (C restatement of the reference Fortran, OpenMP
            over columns) on a bounded sample of the same workload
 
@@ -53,7 +63,11 @@ def parse():
     p.add_argument("--gpus", type=int, default=1)
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
-    p.add_argument("--workload", default="config1")
+    p.add_argument("--workload", default="config3")
+    p.add_argument("--realisations", type=int, default=100,
+                   help="ragged workload: realisations of 2500 columns per GPU")
+    p.add_argument("--plain-cols", type=int, default=25000,
+                   help="ragged workload: columns the plain form is timed on")
     p.add_argument("--form", default="adjoint", choices=["plain", "adjoint"])
     p.add_argument("--no-other-form", action="store_true")
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
@@ -79,6 +93,37 @@ def dist_setup(args):
 def load_case(name):
     from dazi_current_release_b200 import synthetic as S
     return S.GRID_CONFIGS[name]()
+
+
+def load_ragged(args, rank):
+    """The uneven-column batch (per rank its own realisations: weak scaling)."""
+    from dazi_current_release_b200 import synthetic as S
+    return S.config3(realisations=args.realisations, base_seed=1000 + 100000 * rank)
+
+
+def ragged_cpu_baseline(b, sample_s, cores=None):
+    """Oracle of the reference stage (depthkernel FD + depthkernelTI per
+    column, OpenMP over columns) on the first columns of the batch, as many
+    as fit in about sample_s seconds; returns column-periods/s."""
+    from oracle import oracle as O
+    cores = cores or os.cpu_count() or 1
+
+    def run(n):
+        no, po = b.node_off[:n + 1], b.per_off[:n + 1]
+        t0 = time.perf_counter()
+        O.batch(no, b.depz[:no[-1]], b.vs[:no[-1]], po, b.periods[:po[-1]], b.minthk,
+                nthreads=cores)
+        return time.perf_counter() - t0
+
+    n1 = min(b.ncol, cores)
+    dt1 = run(n1)
+    n2 = int(min(b.ncol, max(n1, sample_s / max(dt1, 1e-9) * n1)))
+    dt = run(n2) if n2 > n1 else dt1
+    cp = int(b.per_off[n2])
+    return {"value": cp / dt, "unit": "column-periods/s", "cores": cores, "kind": "port",
+            "sample": f"first {n2} of {b.ncol} columns ({cp} column-periods), oracle of "
+                      f"depthkernel (FD: 1+6nz surfdisp96 per column) + depthkernelTI, "
+                      f"{dt:.1f} s on {cores} threads"}
 
 
 class ClockSampler:
@@ -176,7 +221,42 @@ def cpu_baseline(case, sample_s, form_kernels=True):
                       f"{cores} threads"}
 
 
+def run_reference_ragged(args, ws, rank):
+    if rank != 0:
+        return
+    b = load_ragged(args, 0)
+    vals = []
+    for _ in range(args.steps):
+        cb = ragged_cpu_baseline(b, args.cpu_sample_s / max(args.steps, 1))
+        vals.append(cb["value"])
+    v = float(np.median(vals))
+    cp = b.column_periods
+    line = {"impl": "reference", "metric": "kernel column-periods/s", "value": v,
+            "unit": "column-periods/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": cp / v * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": ragged_config(args, b),
+            "cpu_baseline": {"value": v, "unit": "column-periods/s", "cores": cb["cores"],
+                             "kind": cb["kind"], "sample": cb["sample"]},
+            "e2e": {"value": v, "unit": "column-periods/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def ragged_config(args, b):
+    nz = np.diff(b.node_off)
+    K = np.diff(b.per_off)
+    return {"workload": args.workload, "form": args.form, "columns": int(b.ncol),
+            "column_periods": int(b.column_periods), "realisations": args.realisations,
+            "layers_per_column": [int(nz.min()) - 1, int(nz.max()) - 1],
+            "mean_layers": float(nz.mean() - 1), "periods_per_column": [int(K.min()), int(K.max())],
+            "mean_periods": float(K.mean()), "minthk": b.minthk,
+            "parallelism": "columns, one batch per GPU"}
+
+
 def run_reference(args, ws, rank):
+    if args.workload == "config3":
+        return run_reference_ragged(args, ws, rank)
     case = load_case(args.workload)
     if rank != 0:
         return
@@ -202,11 +282,204 @@ def run_reference(args, ws, rank):
     print(json.dumps(line), flush=True)
 
 
+def _events_timed(step, steps, warmup, dev, stream, flush, ws):
+    """Per-step CUDA events on the launching stream; L2 flushed between steps
+    outside the events; max over ranks.  Returns ms per step."""
+    import torch
+    for _ in range(warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    if ws > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize(dev)
+    for i in range(steps):
+        flush.zero_()
+        starts[i].record(stream)
+        step()
+        ends[i].record(stream)
+    torch.cuda.synchronize(dev)
+    if ws > 1:
+        torch.distributed.barrier()
+    total = float(sum(s.elapsed_time(e) for s, e in zip(starts, ends)))
+    if ws > 1:
+        tt = torch.tensor([total], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        total = float(tt.item())
+    return total / steps
+
+
+def _work_constants():
+    """FP64 operations per layer item of the adjoint and Gc/Gs sweeps,
+    counted by ncu (dadd + dmul + 2 dfma per thread instruction) on a sample
+    of the uneven batch and divided by the sample's layer items."""
+    path = os.path.join(ROOT, "profiles", "kernel_work.json")
+    try:
+        return json.load(open(path))
+    except (OSError, ValueError):
+        return {}
+
+
+def main_ragged(args, ws, rank, local):
+    import torch
+    from dazi_current_release_b200 import _lib
+    from dazi_current_release_b200.batch import output_offsets
+    L = _lib.load(build_if_missing=False)
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    b = load_ragged(args, rank)
+    ncol = b.ncol
+    sen_off, ls_off = output_offsets(b.node_off, b.per_off)
+    form = _lib.FORM_PLAIN if args.form == "plain" else _lib.FORM_ADJOINT
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    d_node, d_per, d_dep, d_vs = T(b.node_off), T(b.per_off), T(b.depz), T(b.vs)
+    d_periods, d_senoff, d_lsoff = T(b.periods), T(sen_off), T(ls_off)
+    ncp = int(b.per_off[-1])
+    pv = torch.zeros(ncp, dtype=torch.float64, device=dev)
+    sen = [torch.zeros(int(sen_off[-1]), dtype=torch.float64, device=dev) for _ in range(3)]
+    lsen = torch.zeros(int(ls_off[-1]), dtype=torch.float32, device=dev)
+    status = torch.zeros(ncol, dtype=torch.int32, device=dev)
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    ptr = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+
+    def step_fn(f, n):
+        def step():
+            rc = L.dazi_dk_batch_dev(n, ptr(d_node), ptr(d_dep), ptr(d_vs), None, None,
+                                     ptr(d_per), ptr(d_periods), ctypes.c_float(b.minthk),
+                                     ptr(pv), ptr(d_senoff), ptr(sen[0]), ptr(sen[1]),
+                                     ptr(sen[2]), ptr(d_lsoff), ptr(lsen), f, ptr(status),
+                                     ctypes.c_void_p(stream.cuda_stream))
+            _lib.check(rc)
+        return step
+
+    def work():
+        ev, lev, cpi, li = (ctypes.c_longlong(0) for _ in range(4))
+        _lib.check(L.dazi_dk_last_work(ctypes.byref(ev), ctypes.byref(lev)))
+        _lib.check(L.dazi_dk_last_items(ctypes.byref(cpi), ctypes.byref(li)))
+        return ev.value, lev.value, li.value
+
+    # both forms on the same sample of columns (the plain form on all 250k
+    # columns would take minutes per step)
+    ns = min(ncol, args.plain_cols)
+    ns_cp = int(b.per_off[ns])
+    sample = {}
+    if not args.no_other_form:
+        for fname, f in (("plain", _lib.FORM_PLAIN), ("adjoint", _lib.FORM_ADJOINT)):
+            ms = _events_timed(step_fn(f, ns), 1 if f == _lib.FORM_PLAIN else 2, 1, dev, stream,
+                               flush, ws)
+            sample[fname] = {"value": ws * ns_cp / (ms * 1e-3), "ms_per_step": ms}
+    with ClockSampler(local) as clk:
+        ms_per_step = _events_timed(step_fn(form, ncol), args.steps, args.warmup, dev, stream,
+                                    flush, ws)
+    launches = L.dazi_dk_last_launches()
+    evals, layer_evals, layer_items = work()
+    value = ws * ncp / (ms_per_step * 1e-3)
+
+    # per-phase device times of one more step (events inside the library)
+    _lib.check(L.dazi_dk_set_timing(1))
+    torch.cuda.synchronize(dev)
+    step_fn(form, ncol)()
+    phases = _lib.last_timing()
+    _lib.check(L.dazi_dk_set_timing(0))
+
+    # end to end: host C-ABI dazi_dk_batch with pinned host buffers
+    pin = lambda n, dt: torch.empty(n, dtype=dt, pin_memory=True).numpy()  # noqa: E731
+    h = {}
+    for name, arr in (("node", b.node_off), ("per", b.per_off), ("dep", b.depz), ("vs", b.vs),
+                      ("periods", b.periods), ("senoff", sen_off), ("lsoff", ls_off)):
+        h[name] = pin(arr.size, {np.dtype(np.int64): torch.int64, np.dtype(np.float32): torch.float32,
+                                 np.dtype(np.float64): torch.float64}[arr.dtype])
+        h[name][:] = arr
+    h_pv = pin(ncp, torch.float64)
+    h_sen = [pin(int(sen_off[-1]), torch.float64) for _ in range(3)]
+    h_ls = pin(int(ls_off[-1]), torch.float32)
+    h_st = pin(ncol, torch.int32)
+    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+
+    def e2e_step():
+        rc = L.dazi_dk_batch(ncol, P(h["node"]), P(h["dep"]), P(h["vs"]), None, None,
+                             P(h["per"]), P(h["periods"]), ctypes.c_float(b.minthk), P(h_pv),
+                             P(h["senoff"]), P(h_sen[0]), P(h_sen[1]), P(h_sen[2]),
+                             P(h["lsoff"]), P(h_ls), form, P(h_st))
+        _lib.check(rc)
+
+    e2e_step()
+    e2e_steps = max(1, min(args.steps, 3))
+    if ws > 1:
+        torch.distributed.barrier()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    if ws > 1:
+        tt = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(tt, op=torch.distributed.ReduceOp.MAX)
+        e2e_s = float(tt.item())
+    h2d = sum(h[k].nbytes for k in h)
+    d2h = h_pv.nbytes + sum(x.nbytes for x in h_sen) + h_ls.nbytes + h_st.nbytes
+
+    # roofline of the dominant kernel
+    peak = ctypes.c_double(0.0)
+    _lib.check(L.dazi_dk_fp64_peak(ctypes.byref(peak)))
+    peak_tf = peak.value / 1e3
+    consts = _work_constants()
+    flops = {"root": layer_evals * FLOP_PER_LAYER_EVAL}
+    for k in ("adjoint", "ti"):
+        f = consts.get(f"{k}_fp64_ops_per_layer_item")
+        if f:
+            flops[k] = f * layer_items
+    ph = dict(phases)
+    dom = max((n for n in ph if n != "prep"), key=lambda n: ph[n])
+    achieved = flops[dom] / (ph[dom] * 1e-3) / 1e12 if dom in flops else None
+    traffic = consts.get(f"{dom}_dram_bytes_per_layer_item")
+    roof = {"bound": "fp64", "kernel": {"root": "root_kernel", "adjoint": "adjoint_kernel",
+                                         "ti": "ti_kernel", "fd": "fd_batch_kernel"}.get(dom, dom),
+            "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
+            "frac": achieved / peak_tf if achieved and peak_tf > 0 else None,
+            "traffic": traffic * layer_items if traffic else None,
+            "peak_source": "measured in-run FP64 FMA probe (dazi_dk_fp64_peak)",
+            "kernel_ms": ph[dom], "flops_per_launch": flops.get(dom),
+            "phase_ms": ph, "layer_items": layer_items, "secular_evals": evals,
+            "root_layer_evals": layer_evals}
+    line = {
+        "metric": "kernel column-periods/s", "value": value, "unit": "column-periods/s",
+        "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": dict(ragged_config(args, b),
+                       l2="inputs and outputs far larger than L2; 256 MiB flush write between "
+                          "steps outside the timed events"),
+        "e2e": {"value": ws * ncp / e2e_s, "unit": "column-periods/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
+        "roofline": roof,
+        "gpu_launches": args.steps * launches,
+    }
+    if sample:
+        line["same_columns"] = dict(sample, columns=ns, column_periods=ns_cp,
+                                    adjoint_over_plain=sample["adjoint"]["value"] /
+                                    sample["plain"]["value"])
+    clocks = clk.summary()
+    if clocks:
+        line["clocks"] = clocks
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = ragged_cpu_baseline(b, args.cpu_sample_s)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
 def main():
     args = parse()
     ws, rank, local = dist_setup(args)
     if args.impl == "reference":
         run_reference(args, ws, rank)
+        return
+    if args.workload == "config3":
+        main_ragged(args, ws, rank, local)
         return
     import torch
     from dazi_current_release_b200 import _lib

@@ -33,7 +33,7 @@ EXPORTS = (
     "dazi_dk_last_error", "dazi_dk_version", "dazi_dk_finalize", "dazi_dk_fp64_peak", "dazi_dk_last_work",
     "dazi_dk_ti", "dazi_dk_fused", "dazi_dk_fused_dev", "dazi_dk_last_launches",
     "dazi_dk_iso_noalloc_dev", "dazi_dk_batch", "dazi_dk_batch_dev", "dazi_dk_set_timing",
-    "dazi_dk_last_timing",
+    "dazi_dk_last_timing", "dazi_dk_last_items",
 )
 
 
@@ -104,6 +104,8 @@ def load(build_if_missing: bool = True):
     L.dazi_dk_version.restype = _int
     L.dazi_dk_last_work.argtypes = [ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
     L.dazi_dk_last_work.restype = _int
+    L.dazi_dk_last_items.argtypes = [ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
+    L.dazi_dk_last_items.restype = _int
     L.dazi_dk_fp64_peak.argtypes = [_f64p]
     L.dazi_dk_fp64_peak.restype = _int
     L.dazi_dk_finalize.argtypes = []

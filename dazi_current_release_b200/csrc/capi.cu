@@ -371,8 +371,8 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
     if (col_count == 0) return 0;
     const Geometry* geo = g_ctx.geo.as<Geometry>();
     int r;
-    if ((r = g_ctx.counters.ensure(sizeof(unsigned long long) * 4))) return r;
-    CK(cudaMemsetAsync(g_ctx.counters.p, 0, sizeof(unsigned long long) * 4, st));
+    if ((r = g_ctx.counters.ensure(sizeof(unsigned long long) * 8))) return r;
+    CK(cudaMemsetAsync(g_ctx.counters.p, 0, sizeof(unsigned long long) * 8, st));
     g_ctx.last_rmax = g_ctx.geo_rmax;
     g_ctx.last_launches = 0;
     phase_begin(st);
@@ -409,7 +409,7 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
     src.vel = vel; src.vp = vp; src.rho = rho; src.depz = g_ctx.depz.as<float>();
     src.node_off = nullptr; src.per_off = nullptr; src.nz = nz; src.K = kmax;
     src.minthk = g_ctx.geo_minthk;
-    PrepOut po{nullptr, nullptr};
+    PrepOut po{nullptr, nullptr, g_ctx.counters.as<unsigned long long>() + 4};
     Tables T;
     if ((r = build_tables(src, col_count, po, ncol, ncol, ncol, st, T))) return r;
     return run_tables(T, per, o, form, fd, st);
@@ -434,8 +434,8 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
 {
     if (B.ncols == 0) return 0;
     int r;
-    if ((r = g_ctx.counters.ensure(sizeof(unsigned long long) * 4))) return r;
-    CK(cudaMemsetAsync(g_ctx.counters.p, 0, sizeof(unsigned long long) * 4, st));
+    if ((r = g_ctx.counters.ensure(sizeof(unsigned long long) * 8))) return r;
+    CK(cudaMemsetAsync(g_ctx.counters.p, 0, sizeof(unsigned long long) * 8, st));
     g_ctx.last_launches = 0;
     g_ctx.last_rmax = 0;
     phase_begin(st);
@@ -444,7 +444,7 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
     src.vel = B.vs; src.vp = B.vp; src.rho = B.rho; src.depz = B.depz;
     src.node_off = B.node_off; src.per_off = B.per_off; src.nz = 0; src.K = 0;
     src.minthk = B.minthk;
-    PrepOut po{B.sen_off, B.ls_off};
+    PrepOut po{B.sen_off, B.ls_off, g_ctx.counters.as<unsigned long long>() + 4};
     Tables T;
     if ((r = build_tables(src, B.ncols, po, 1, 1, 1, st, T))) return r;
     const bool fd = o.svs && form == DAZI_FORM_PLAIN;
@@ -869,6 +869,17 @@ int dazi_dk_last_work(long long* secular_evals, long long* layer_evals)
     CK(cudaMemcpy(h, g_ctx.counters.p, sizeof(h), cudaMemcpyDeviceToHost));
     if (secular_evals) *secular_evals = (long long)h[0];
     if (layer_evals) *layer_evals = (long long)h[3];
+    return 0;
+}
+
+int dazi_dk_last_items(long long* column_periods, long long* layer_items)
+{
+    std::lock_guard<std::mutex> lk(g_mu);
+    if (!g_ctx.ready || !g_ctx.counters.p) { set_err("no call made yet"); return DAZI_ERR_BADARG; }
+    unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    CK(cudaMemcpy(h, g_ctx.counters.p, sizeof(h), cudaMemcpyDeviceToHost));
+    if (column_periods) *column_periods = (long long)h[5];
+    if (layer_items) *layer_items = (long long)h[4];
     return 0;
 }
 

@@ -28,6 +28,7 @@ struct FdArgs {
 struct PrepOut {
     const long long* sen_off;   // ragged: first kernel entry of each column
     const long long* ls_off;    // ragged: first Lsen entry of each column
+    unsigned long long* work;   // [0] sum of K_c * rmax_c (layer items), [1] sum of K_c
 };
 
 struct RootArgs {

@@ -186,6 +186,10 @@ __global__ void prep_build_kernel(ColSrc src, PrepOut o, Tables T, const int* so
     }
     M.rmax = m;
     T.meta[s] = M;
+    if (o.work) {
+        atomicAdd(o.work, (unsigned long long)K * (unsigned long long)m);
+        atomicAdd(o.work + 1, (unsigned long long)K);
+    }
 }
 
 }  // namespace dk

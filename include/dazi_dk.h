@@ -191,6 +191,13 @@ int dazi_dk_last_launches(void);
  * Synchronises with the device. */
 int dazi_dk_last_work(long long *secular_evals, long long *layer_evals);
 
+/* Size of the last call's per-(column, period) work: the number of
+ * column-periods (sum of K_c) and of layer items (sum of K_c x refined layer
+ * count of the column), the units of the adjoint and Gc/Gs sweeps.  Counted
+ * when the layer tables are built (adjoint form, or Lsen requested); 0
+ * otherwise.  Synchronises with the device. */
+int dazi_dk_last_items(long long *column_periods, long long *layer_items);
+
 /* Diagnostic: measured FP64 FMA throughput of the current device in
  * GFLOP/s (best of 5 launches of an FMA-chain kernel).  The stage's kernels
  * run on the FP64 CUDA-core pipe; this is their roofline denominator. */
