@@ -3,7 +3,7 @@ oracle run column by column, for both forms."""
 import numpy as np
 import pytest
 
-from conftest import rel_l2
+from conftest import assert_pv_parity, rel_l2
 import dazi_current_release_b200 as dk
 from dazi_current_release_b200 import synthetic as S
 from dazi_current_release_b200.batch import depthkernel_batch
@@ -21,7 +21,9 @@ def _oracle_column(oracle, b, c, ti=True):
     vel = vs.reshape(1, 1, -1)
     iso = oracle.depthkernel(vel, dep, per, b.minthk)
     out = {"pv": iso["pvRc"][0], "svs": iso["sen_vs"][0], "svp": iso["sen_vp"][0],
-           "srh": iso["sen_rho"][0], "status": iso["status"][0]}
+           "srh": iso["sen_rho"][0], "status": iso["status"][0],
+           "pv_d": oracle.depthkernel(vel, dep, per, b.minthk, round_f32=False,
+                                      kernels=False)["pvRc"][0]}
     if ti:
         out["lsen"] = oracle.depthkernel_ti(vel, dep, per, b.minthk)["Lsen_Gsc"][0]
     return out
@@ -32,15 +34,17 @@ def test_batch_plain_and_ti_match_oracle(oracle, small_batch):
     r = depthkernel_batch(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk,
                           form=dk.FORM_PLAIN)
     worst_ls = 0.0
+    flips = 0
     for c in range(b.ncol):
         ref = _oracle_column(oracle, b, c)
         pv, svs, svp, srh, ls = r.column(c)
         assert r["status"][c] == ref["status"]
-        np.testing.assert_array_equal(pv, ref["pv"])
+        flips += assert_pv_parity(pv, ref["pv"], ref["pv_d"])
         for got, exp in ((svs, ref["svs"]), (svp, ref["svp"]), (srh, ref["srh"])):
             assert rel_l2(got, exp) <= 1e-4
         worst_ls = max(worst_ls, rel_l2(ls, ref["lsen"]))
-    print("batch plain: Lsen worst per-column rel-L2", worst_ls)
+    print("batch plain: Lsen worst per-column rel-L2", worst_ls, "midpoint flips", flips)
+    assert flips <= max(1, b.column_periods // 500)
     assert worst_ls <= 1e-5
 
 
