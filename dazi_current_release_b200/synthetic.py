@@ -181,8 +181,9 @@ class RaggedBatch:
 def config3(realisations: int = 100, columns: int = 2500, base_seed: int = 1000) -> RaggedBatch:
     """Per realisation r (seed base_seed + r), per column: L ~ U{10..60}
     layers; 1-3 sediment layers of total thickness U(0.3, 3) km with
-    Vs ~ U(0.8, 1.5) (increasing); the remaining thicknesses a Dirichlet
-    split of 100 km minus the sediment; Vs at the other nodes the 2.6-4.6
+    Vs ~ U(0.8, 1.5) (increasing), each at least 50 m thick; the remaining
+    thicknesses a Dirichlet split of 100 km minus the sediment, each at least
+    200 m; Vs at the other nodes the 2.6-4.6
     km/s gradient x (1 + 0.05 N(0,1)); in 20 % of the columns a -8 % low-
     velocity zone at 15-25 km; n ~ U{8..40} periods log-uniform in 3-60 s,
     sorted.  Vectorised over the columns of a realisation."""
@@ -210,7 +211,10 @@ def config3(realisations: int = 100, columns: int = 2500, base_seed: int = 1000)
         praw = np.exp(rng.uniform(np.log(3.0), np.log(60.0), (C, 40)))
         for c in range(C):
             nsc, Lc = ns[c], L[c]
-            thk = np.concatenate([sed[c] * g_sed[c, :nsc], (100.0 - sed[c]) * g_rest[c, :Lc - nsc]])
+            # floors of 50 m (sediments) and 200 m: no sliver layers
+            ts = 0.05 + (sed[c] - 0.05 * nsc) * g_sed[c, :nsc]
+            tr = 0.2 + (100.0 - sed[c] - 0.2 * (Lc - nsc)) * g_rest[c, :Lc - nsc]
+            thk = np.concatenate([ts, tr])
             z = np.concatenate([[0.0], np.cumsum(thk)])
             z[-1] = 100.0
             vs = (2.6 + 2.0 * z / 100.0) * (1.0 + 0.05 * noise[c, :Lc + 1])
