@@ -396,7 +396,11 @@ def main_ragged(args, ws, rank, local):
     h_sen = [pin(int(sen_off[-1]), torch.float64) for _ in range(3)]
     h_ls = pin(int(ls_off[-1]), torch.float32)
     h_st = pin(ncol, torch.int32)
-    P = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    CT = {np.dtype(np.int64): ctypes.c_longlong, np.dtype(np.float32): ctypes.c_float,
+          np.dtype(np.float64): ctypes.c_double, np.dtype(np.int32): ctypes.c_int}
+
+    def P(a):
+        return a.ctypes.data_as(ctypes.POINTER(CT[a.dtype]))
 
     def e2e_step():
         rc = L.dazi_dk_batch(ncol, P(h["node"]), P(h["dep"]), P(h["vs"]), None, None,
