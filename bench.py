@@ -55,7 +55,8 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-FLOP_PER_LAYER_EVAL = 180   # FP64 flops per layer per secular evaluation
+FLOP_PER_LAYER_EVAL = 180   # hand count of dltar4's FP64 arithmetic per layer (fallback when
+                             # the ncu-counted figure is absent)
 
 
 def parse():
@@ -429,20 +430,30 @@ def main_ragged(args, ws, rank, local):
     _lib.check(L.dazi_dk_fp64_peak(ctypes.byref(peak)))
     peak_tf = peak.value / 1e3
     consts = _work_constants()
-    flops = {"root": layer_evals * FLOP_PER_LAYER_EVAL}
-    for k in ("adjoint", "ti"):
-        f = consts.get(f"{k}_fp64_ops_per_layer_item")
+    units = {"root": ("layer_eval", layer_evals), "adjoint": ("layer_item", layer_items),
+             "ti": ("layer_item", layer_items)}
+    flops, traffic_of = {}, {}
+    for k, (uname, n) in units.items():
+        f = consts.get(f"{k}_fp64_ops_per_{uname}")
+        if f is None and k == "root":
+            f = FLOP_PER_LAYER_EVAL
         if f:
-            flops[k] = f * layer_items
+            flops[k] = f * n
+        t = consts.get(f"{k}_dram_bytes_per_{uname}")
+        if t:
+            traffic_of[k] = t * n
     ph = dict(phases)
     dom = max((n for n in ph if n != "prep"), key=lambda n: ph[n])
     achieved = flops[dom] / (ph[dom] * 1e-3) / 1e12 if dom in flops else None
-    traffic = consts.get(f"{dom}_dram_bytes_per_layer_item")
+    traffic = traffic_of.get(dom)
     roof = {"bound": "fp64", "kernel": {"root": "root_kernel", "adjoint": "adjoint_kernel",
                                          "ti": "ti_kernel", "fd": "fd_batch_kernel"}.get(dom, dom),
             "achieved": achieved, "peak": peak_tf, "unit": "TFLOP/s",
             "frac": achieved / peak_tf if achieved and peak_tf > 0 else None,
-            "traffic": traffic * layer_items if traffic else None,
+            "traffic": traffic,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per unit on a "
+                              "12500-column sample, scaled by the units of this launch",
+            "phase_tflops": {k: flops[k] / (ph[k] * 1e-3) / 1e12 for k in flops if k in ph},
             "peak_source": "measured in-run FP64 FMA probe (dazi_dk_fp64_peak)",
             "kernel_ms": ph[dom], "flops_per_launch": flops.get(dom),
             "phase_ms": ph, "layer_items": layer_items, "secular_evals": evals,
@@ -599,7 +610,8 @@ def main():
     # ---------------- roofline
     peak = ctypes.c_double(0.0)
     _lib.check(L.dazi_dk_fp64_peak(ctypes.byref(peak)))
-    flops = layer_evals_per_step * FLOP_PER_LAYER_EVAL
+    flops = layer_evals_per_step * _work_constants().get("root_fp64_ops_per_layer_eval",
+                                                         FLOP_PER_LAYER_EVAL)
     achieved = flops / (ms_per_step * 1e-3) / 1e12
     peak_tf = peak.value / 1e3
     traffic = None
