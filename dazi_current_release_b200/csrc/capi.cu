@@ -83,7 +83,7 @@ struct Context {
     DBuf geo, cscratch, croot, counters, adjscr, tiscr, lsen;
     // per-call layer tables
     DBuf keys, keys2, cidx, cidx2, rmaxb, trecs, ttasks, tlbase, ttbase, cubtmp;
-    DBuf tflat, tld, tti, tch, tmeta, ttasklist, cbufoff;
+    DBuf tflat, tld, tti, tsp, tch, tmeta, ttasklist, cbufoff;
     // batch staging (host entry)
     DBuf bnode, bper, bdep, bvs, bvp, brho, bperiods, bsenoff, blsoff, bpv, bsvs, bsvp, bsrh, blsen, bstatus;
     int last_launches = 0;
@@ -272,10 +272,10 @@ int build_tables(const ColSrc& src, long long ncols, const PrepOut& po, long lon
     }
     const long long nrec = last[0] + last[1], ntask = last[2] + last[3];
     if ((r = g_ctx.tflat.ensure(sizeof(float4) * nrec)) || (r = g_ctx.tld.ensure(sizeof(LayerD) * nrec)) ||
-        (r = g_ctx.tti.ensure(sizeof(TiRec) * nrec)) || (r = g_ctx.tch.ensure(sizeof(ChainRec) * nrec)) ||
+        (r = g_ctx.tti.ensure(sizeof(TiRec) * nrec)) || (r = g_ctx.tsp.ensure(sizeof(SpRec) * nrec)) || (r = g_ctx.tch.ensure(sizeof(ChainRec) * nrec)) ||
         (r = g_ctx.tmeta.ensure(sizeof(ColMeta) * ncols)) || (r = g_ctx.ttasklist.ensure(sizeof(int2) * ntask)))
         return r;
-    T.flat = g_ctx.tflat.as<float4>(); T.ld = g_ctx.tld.as<LayerD>(); T.ti = g_ctx.tti.as<TiRec>();
+    T.flat = g_ctx.tflat.as<float4>(); T.ld = g_ctx.tld.as<LayerD>(); T.ti = g_ctx.tti.as<TiRec>(); T.sp = g_ctx.tsp.as<SpRec>();
     T.ch = g_ctx.tch.as<ChainRec>(); T.meta = g_ctx.tmeta.as<ColMeta>();
     T.tile_lbase = g_ctx.tlbase.as<long long>(); T.tasks = g_ctx.ttasklist.as<int2>();
     T.ntasks = ntask; T.ncols = ncols; T.pv_sk = pv_sk; T.sen_sk = sen_sk; T.ls_sk = ls_sk;
@@ -896,7 +896,7 @@ void dazi_dk_finalize(void)
                    &g_ctx.cscratch, &g_ctx.croot, &g_ctx.counters, &g_ctx.adjscr,
                    &g_ctx.tiscr, &g_ctx.lsen, &g_ctx.keys, &g_ctx.keys2, &g_ctx.cidx, &g_ctx.cidx2,
                    &g_ctx.rmaxb, &g_ctx.trecs, &g_ctx.ttasks, &g_ctx.tlbase, &g_ctx.ttbase,
-                   &g_ctx.cubtmp, &g_ctx.tflat, &g_ctx.tld, &g_ctx.tti, &g_ctx.tch, &g_ctx.tmeta,
+                   &g_ctx.cubtmp, &g_ctx.tflat, &g_ctx.tld, &g_ctx.tti, &g_ctx.tsp, &g_ctx.tch, &g_ctx.tmeta,
                    &g_ctx.ttasklist, &g_ctx.cbufoff, &g_ctx.bnode, &g_ctx.bper, &g_ctx.bdep,
                    &g_ctx.bvs, &g_ctx.bvp, &g_ctx.brho, &g_ctx.bperiods, &g_ctx.bsenoff,
                    &g_ctx.blsoff, &g_ctx.bpv, &g_ctx.bsvs, &g_ctx.bsvp, &g_ctx.bsrh, &g_ctx.blsen,

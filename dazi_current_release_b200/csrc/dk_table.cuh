@@ -17,12 +17,25 @@ namespace dk {
 
 constexpr int TILE = 32;
 
-// TI model of one refined layer: tregn96's flattened values (real*4 stores)
-// and the unflattened refined values the Lsen_Gsc splice uses.
+// TI model of one refined layer as tregn96 holds it (real*4 stores of the
+// flattened A = C, L = N, density and thickness, widened to double) with the
+// period-independent combinations its eigenvector and energy formulas
+// divide by, formed once per layer instead of once per (layer, period).
 struct TiRec {
-    float TA, TL, rho, td;    // flattened A (= C), L (= N), density, thickness
-    float vtp;                // partial-derivative sphericity factor
-    float rvp, rvs, rrho;     // refined values before flattening
+    double TA, TL, rho, TF;   // TF = TA - 2 TL of the unflattened values
+    double iTA, iTL;          // 1 / TC, 1 / TL           (TC = TA)
+    double TFoTA, TAF;        // TF / TC, TA - TF^2 / TC
+    double rhoTA, rhoTL;      // rho / TC, rho / TL
+    double ah, bv;            // sqrt(TA / rho) (= av), sqrt(TL / rho) (= bh)
+    double eta, ieta;         // TF / (TA - 2 TL), its reciprocal
+    double td;                // flattened thickness (0 for the half-space)
+};
+
+// The Lsen_Gsc splice of one refined layer (depthkernelTI.f90:152-162, real*4):
+//   dA = cA1 dcdah - cA2 dcdn,  dL = cL1 dcdbv + cL2 dcdn,
+//   Lsen += dA TA + dL TL   (unflattened TA, TL), and sprayl's vtp.
+struct SpRec {
+    float vtp, cA1, cA2, cL1, cL2, TA, TL, pad;
 };
 
 // What the adjoint needs to chain layer derivatives to node derivatives.
@@ -50,6 +63,7 @@ struct Tables {
     float4* flat;             // (d, a, b, rho) flattened, surfdisp96
     LayerD* ld;               // secular-function constants
     TiRec* ti;                // tregn96 model
+    SpRec* sp;                // Lsen_Gsc splice
     ChainRec* ch;             // adjoint chain rule
     ColMeta* meta;            // [sorted position]
     long long* tile_lbase;    // [tile] first record of the tile

@@ -169,17 +169,45 @@ __global__ void prep_build_kernel(ColSrc src, PrepOut o, Tables T, const int* so
             p0 = p1;
             const float TAu = __fmul_rn(rrh, __fmul_rn(rvp, rvp));
             const float TLu = __fmul_rn(rrh, __fmul_rn(rvs, rvs));
+            // tregn96's model: A, L and rho flattened (real*4 stores), F
+            // left unmapped (depthkernelTI.f90:124-131 with sphere_tdisp96)
+            const float fTA = (float)__dmul_rn((double)TAu, pow(t2, (double)(-0.2750f)));
+            const float fTL = (float)__dmul_rn((double)TLu, pow(t2, (double)(-0.2750f)));
+            const float frh = (float)__dmul_rn((double)rrh, pow(t2, (double)(-2.275f)));
             TiRec tr;
-            tr.TA = (float)__dmul_rn((double)TAu, pow(t2, (double)(-0.2750f)));
-            tr.TL = (float)__dmul_rn((double)TLu, pow(t2, (double)(-0.2750f)));
-            tr.rho = (float)__dmul_rn((double)rrh, pow(t2, (double)(-2.275f)));
-            tr.td = half ? 0.0f : td;
-            tr.vtp = vtp;
-            tr.rvp = rvp; tr.rvs = rvs; tr.rrho = rrh;
+            tr.TA = (double)fTA;
+            tr.TL = (double)fTL;
+            tr.rho = (double)frh;
+            tr.TF = (double)__fsub_rn(TAu, __fmul_rn(2.0f, TLu));
+            tr.iTA = 1.0 / tr.TA;
+            tr.iTL = 1.0 / tr.TL;
+            tr.TFoTA = tr.TF / tr.TA;
+            tr.TAF = tr.TA - tr.TF * tr.TF / tr.TA;
+            tr.rhoTA = tr.rho / tr.TA;
+            tr.rhoTL = tr.rho / tr.TL;
+            tr.ah = sqrt(tr.TA / tr.rho);
+            tr.bv = sqrt(tr.TL / tr.rho);
+            tr.eta = tr.TF / (tr.TA - 2.0 * tr.TL);
+            tr.ieta = 1.0 / tr.eta;
+            tr.td = half ? 0.0 : (double)td;
+            // splice coefficients, real*4 as depthkernelTI.f90:152-162
+            SpRec sr;
+            const float TFs = __fmul_rn(1.0f, __fsub_rn(TAu, __fmul_rn(2.0f, TLu)));
+            const float den = __fsub_rn(TAu, __fmul_rn(2.0f, TLu));
+            const float den2 = __fmul_rn(den, den);
+            sr.vtp = vtp;
+            sr.cA1 = __fdiv_rn(0.5f, __fmul_rn(rrh, rvp));
+            sr.cA2 = __fdiv_rn(TFs, den2);
+            sr.cL1 = __fdiv_rn(0.5f, __fmul_rn(rrh, rvs));
+            sr.cL2 = __fdiv_rn(__fmul_rn(2.0f, TFs), den2);
+            sr.TA = TAu;
+            sr.TL = TLu;
+            sr.pad = 0.0f;
             const long long ix = rec_index(T, s, m);
             T.flat[ix] = L;
             T.ld[ix] = make_layerd(L);
             T.ti[ix] = tr;
+            T.sp[ix] = sr;
             T.ch[ix] = ch;
         }
         vs0 = vs1; vp0 = vp1; rh0 = rh1;

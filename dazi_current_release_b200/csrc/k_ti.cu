@@ -65,28 +65,13 @@ __device__ __forceinline__ zc zexp(zc a)
 }
 
 // ------------------------------------------------------- TI layer model
-// Flattened TI values of one layer as tregn96 holds them (real*4 stores).
-struct TiLayer {
-    double d, TA, TC, TF, TL, TN, rho;
-};
+// A layer as tregn96 holds it: TiRec (dk_table.cuh) with TC = TA, TN = TL
+// (depthkernelTI.f90:124-131) and the period-independent combinations.
+using TiLayer = TiRec;
 
-// Layer record -> tregn96's model of the layer.  TA = TC = rho Vp^2 and
-// TL = TN = rho Vs^2 (depthkernelTI.f90:124-131, real*4) are stored already
-// flattened (sphere_tdisp96, tregn96.f:796-834); TF = TA - 2 TL is not
-// mapped by the flattening, so it is formed from the unflattened values.
-__device__ __forceinline__ TiLayer ti_layer(const TiRec& r)
+__device__ __forceinline__ TiLayer ti_layer(const TiRec* p)
 {
-    const float TAu = __fmul_rn(r.rrho, __fmul_rn(r.rvp, r.rvp));
-    const float TLu = __fmul_rn(r.rrho, __fmul_rn(r.rvs, r.rvs));
-    TiLayer o;
-    o.d = (double)r.td;
-    o.rho = (double)r.rho;
-    o.TA = (double)r.TA;
-    o.TC = o.TA;
-    o.TL = (double)r.TL;
-    o.TN = o.TL;
-    o.TF = (double)__fsub_rn(TAu, __fmul_rn(2.0f, TLu));
-    return o;
+    return *p;
 }
 
 // gettiegn() (tregn96.f:3166-3361) for real eigenvalues.  rp/rsv are the
@@ -106,13 +91,13 @@ struct TiEigZ {
 
 __device__ __forceinline__ void ti_eigen(const TiLayer& L, double omg, double wvn, double wvno2, TiEig& o)
 {
-    const double TA = L.TA, TC = L.TC, TF = L.TF, TL = L.TL, TRho = L.rho;
     const double om2 = omg * omg;
-    const double a = wvn * TF / TC, b = 1.0 / TC;
-    const double c = -TRho * om2 + wvn * wvn * (TA - TF * TF / TC);
-    const double d = -wvn, e = 1.0 / TL, f = -TRho * om2;
-    const double ddef = wvn * wvn - TRho * om2 / TL;
-    const double aabc = wvn * wvn * TA / TC - TRho * om2 / TC;
+    const double wvn2 = wvn * wvn;
+    const double a = wvn * L.TFoTA, b = L.iTA;
+    const double c = -L.rho * om2 + wvn2 * L.TAF;
+    const double d = -wvn, e = L.iTL, f = -L.rho * om2;
+    const double ddef = wvn2 - om2 * L.rhoTL;
+    const double aabc = wvn2 - om2 * L.rhoTA;
     const double bb = 2.0 * a * d + e * c + f * b;
     const double cc = ddef * aabc;
     const double disc = bb * bb - 4.0 * cc;
@@ -360,9 +345,10 @@ __device__ __forceinline__ zc ti_h2(zc nua, zc nub, double dm)
 
 // The six energy integrals of a layer (intijr, tregn96.f:4073-4245):
 // (1,1) (1,3) (2,2) (2,4) (3,3) (4,4).  top/bot = (ur, uz, tz, tr) at the
-// layer's top and bottom interface; half = the lower half-space.
-__device__ __forceinline__ void ti_integrals(const TiEigZ& E, double dm, const double top[4],
-                                             const double bot[4], bool half, double out[6])
+// layer's top and bottom interface; half = the lower half-space.  fg holds
+// the layer's ffunc/gfunc/h1func/h2func values (FA, GA, FB, GB, H1, H2).
+__device__ __forceinline__ void ti_integrals_z(const TiEigZ& E, const zc fg[6], const double top[4],
+                                               const double bot[4], bool half, double out[6])
 {
     zc e[4][4], ei[4][4];
     ti_emat(E, e, ei);
@@ -374,8 +360,7 @@ __device__ __forceinline__ void ti_integrals(const TiEigZ& E, double dm, const d
     constexpr int IJ[6][2] = {{0, 0}, {0, 2}, {1, 1}, {1, 3}, {2, 2}, {3, 3}};
     if (!half) {
         const zc kmpu = pot(0, bot), kmsu = pot(1, bot);
-        const zc FA = ti_f(ra, dm), GA = ti_g(ra, dm), FB = ti_f(rb, dm), GB = ti_g(rb, dm);
-        const zc H1 = ti_h1(ra, rb, dm), H2 = ti_h2(ra, rb, dm);
+        const zc FA = fg[0], GA = fg[1], FB = fg[2], GB = fg[3], H1 = fg[4], H2 = fg[5];
         const zc pu2 = kmpu * kmpu, pd2 = km1pd * km1pd, su2 = kmsu * kmsu, sd2 = km1sd * km1sd;
         const zc pusu = kmpu * kmsu, pdsd = km1pd * km1sd, pusd = kmpu * km1sd, pdsu = km1pd * kmsu;
         const zc pupd = kmpu * km1pd, susd = kmsu * km1sd;
@@ -409,6 +394,103 @@ __device__ __forceinline__ void ti_integrals(const TiEigZ& E, double dm, const d
     }
 }
 
+// One wave of a layer with a real eigenvalue: varsv's quantities
+// (tregn96.f:3363-3475) and ea = exp(-nu d), the one transcendental that
+// ffunc/gfunc/h1func/h2func also need (real nu = r: exp(-r d); imaginary
+// nu = i r: cos(r d) - i sin(r d)).  exp(-2 nu d) is formed as ea^2 and
+// exp(-(nu_a + nu_b) d) as ea eb, with the reference's cut-offs.
+struct TiWave {
+    double cosf, rsin, sinr, ex;
+    double er, ei;
+};
+
+__device__ __forceinline__ TiWave ti_wave(double r, bool osc, double dm)
+{
+    TiWave w;
+    if (!osc) {
+        const double pr = r * dm;
+        w.ex = pr;
+        const double e1 = exp(-pr);
+        const double fac = pr < 15.0 ? e1 * e1 : 0.0;
+        w.cosf = 0.5 * (1.0 + fac);
+        const double sn = 0.5 * (1.0 - fac);
+        w.rsin = r * sn;
+        w.sinr = (fabs(pr) < 1.0e-5 && r < 1.0e-5) ? dm : sn / r;
+        w.er = e1;
+        w.ei = 0.0;
+    } else {
+        const double pi = r * dm;
+        w.ex = 0.0;
+        double sn, cs;
+        sincos(pi, &sn, &cs);
+        w.cosf = cs;
+        w.rsin = -r * sn;                             // (i r)(i sin)
+        w.sinr = (r < 1.0e-5) ? dm : sn / r;          // (i sin)/(i r)
+        w.er = cs;
+        w.ei = -sn;
+    }
+    return w;
+}
+
+// Energy integrals of an evanescent layer (both vertical wavenumbers real):
+// the same sums as ti_integrals_z in real arithmetic.
+__device__ __forceinline__ void ti_integrals_real(const TiEig& E, const TiWave& P, const TiWave& S,
+                                                  double dm, const double top[4], const double bot[4],
+                                                  double out[6])
+{
+    const double ra = E.rp, rb = E.rsv;
+    const double xa = dm * ra, xb = dm * rb;
+    const double ea = P.er, eb = S.er;
+    const double FA = ra < 1.0e-08 ? dm : (1.0 - (xa < 40.0 ? ea * ea : 0.0)) / (2.0 * ra);
+    const double FB = rb < 1.0e-08 ? dm : (1.0 - (xb < 40.0 ? eb * eb : 0.0)) / (2.0 * rb);
+    const double GA = xa < 75.0 ? dm * ea : 0.0;
+    const double GB = xb < 75.0 ? dm * eb : 0.0;
+    const double sab = rb + ra;
+    const double H1 = sab < 1.0e-08 ? dm : (1.0 - (dm * sab < 40.0 ? ea * eb : 0.0)) / sab;
+    const double H2 = fabs(rb - ra) < 1.0e-08 ? dm
+                      : ((xb < 40.0 ? eb : 0.0) - (xa < 40.0 ? ea : 0.0)) / (ra - rb);
+    const double x11 = E.x11, x21 = E.x21, x31 = E.x31, x41 = E.x41;
+    const double x12 = E.x12, x22 = E.x22, x32 = E.x32, x42 = E.x42;
+    const double i1 = 1.0 / ((2.0 * ra) * E.np), i2 = 1.0 / ((2.0 * rb) * E.nsv);
+    double e[4][4], ei[4][4];
+    ei[0][0] = (x41 * ra) * i1;    ei[1][0] = x42 * i2;
+    ei[2][0] = (x41 * ra) * i1;    ei[3][0] = -(x42 * i2);
+    ei[0][1] = -(x31 * i1);        ei[1][1] = -((x32 * rb) * i2);
+    ei[2][1] = x31 * i1;           ei[3][1] = -((x32 * rb) * i2);
+    ei[0][2] = -((x21 * ra) * i1); ei[1][2] = -(x22 * i2);
+    ei[2][2] = -((x21 * ra) * i1); ei[3][2] = x22 * i2;
+    ei[0][3] = x11 * i1;           ei[1][3] = (x12 * rb) * i2;
+    ei[2][3] = -(x11 * i1);        ei[3][3] = (x12 * rb) * i2;
+    e[0][0] = x11; e[1][0] = x21 * ra; e[2][0] = x31; e[3][0] = x41 * ra;
+    e[0][1] = x12 * rb; e[1][1] = x22; e[2][1] = x32 * rb; e[3][1] = x42;
+    e[0][2] = x11; e[1][2] = -(x21 * ra); e[2][2] = x31; e[3][2] = -(x41 * ra);
+    e[0][3] = -(x12 * rb); e[1][3] = x22; e[2][3] = -(x32 * rb); e[3][3] = x42;
+    auto pot = [&](int r, const double u[4]) {
+        return (u[0] * ei[r][0] + u[1] * ei[r][1]) + (u[2] * ei[r][2] + u[3] * ei[r][3]);
+    };
+    const double km1pd = pot(2, top), km1sd = pot(3, top);
+    const double kmpu = pot(0, bot), kmsu = pot(1, bot);
+    const double pu2 = kmpu * kmpu, pd2 = km1pd * km1pd, su2 = kmsu * kmsu, sd2 = km1sd * km1sd;
+    const double pusu = kmpu * kmsu, pdsd = km1pd * km1sd, pusd = kmpu * km1sd, pdsu = km1pd * kmsu;
+    const double pupd = kmpu * km1pd, susd = kmsu * km1sd;
+    constexpr int IJ[6][2] = {{0, 0}, {0, 2}, {1, 1}, {1, 3}, {2, 2}, {3, 3}};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const int i = IJ[q][0], j = IJ[q][1];
+        auto EE = [&](int a, int b) { return e[i][a] * e[j][b]; };
+        auto SY = [&](int a, int b) { return EE(a, b) + EE(b, a); };
+        double r = (EE(0, 0) * pu2) * FA;
+        r = r + (EE(2, 2) * pd2) * FA;
+        r = r + (EE(1, 1) * su2) * FB;
+        r = r + (EE(3, 3) * sd2) * FB;
+        r = r + H1 * (SY(0, 1) * pusu + SY(2, 3) * pdsd);
+        r = r + H2 * (SY(0, 3) * pusd + SY(1, 2) * pdsu);
+        r = r + GA * (SY(0, 2) * pupd);
+        r = r + GB * (SY(1, 3) * susd);
+        out[q] = r;
+    }
+}
+
 // ----------------------------------------------------- complex layer path
 // A layer whose TI eigenvalues form a complex-conjugate pair (deep layers
 // at short periods, where tregn96's flattening leaves F unmapped and eta
@@ -417,13 +499,13 @@ __device__ __forceinline__ void ti_integrals(const TiEigZ& E, double dm, const d
 // and their real parts carried on.
 __device__ void ti_eigen_z(const TiLayer& L, double omg, double wvn, double wvno2, TiEigZ& o)
 {
-    const double TA = L.TA, TC = L.TC, TF = L.TF, TL = L.TL, TRho = L.rho;
     const double om2 = omg * omg;
-    const zc a = Z(wvn * TF / TC), b = Z(1.0 / TC);
-    const zc c = Z(-TRho * om2 + wvn * wvn * (TA - TF * TF / TC));
-    const zc d = Z(-wvn), e = Z(1.0 / TL), f = Z(-TRho * om2);
-    const zc ddef = Z(wvn * wvn - TRho * om2 / TL);
-    const zc aabc = Z(wvn * wvn * TA / TC - TRho * om2 / TC);
+    const double wvn2 = wvn * wvn;
+    const zc a = Z(wvn * L.TFoTA), b = Z(L.iTA);
+    const zc c = Z(-L.rho * om2 + wvn2 * L.TAF);
+    const zc d = Z(-wvn), e = Z(L.iTL), f = Z(-L.rho * om2);
+    const zc ddef = Z(wvn2 - om2 * L.rhoTL);
+    const zc aabc = Z(wvn2 - om2 * L.rhoTA);
     const zc bb = (2.0 * (a * d) + e * c) + f * b;
     const zc cc = ddef * aabc;
     zc srt = zsqrt(bb * bb - 4.0 * cc);
@@ -593,6 +675,114 @@ __device__ __forceinline__ void ti_haskell(const TiEig& E, const TiVar& V, doubl
     for (int i = 0; i < 4; ++i) v[i] = o[i];
 }
 
+// ffunc/gfunc/h1func/h2func values (FA, GA, FB, GB, H1, H2) of a layer by
+// complex exponentials (layers with complex eigenvalues).
+__device__ __forceinline__ void ti_fgh_z(zc ra, zc rb, double dm, zc fg[6])
+{
+    fg[0] = ti_f(ra, dm); fg[1] = ti_g(ra, dm);
+    fg[2] = ti_f(rb, dm); fg[3] = ti_g(rb, dm);
+    fg[4] = ti_h1(ra, rb, dm); fg[5] = ti_h2(ra, rb, dm);
+}
+
+// The same from the waves' ea = exp(-nu d) (real eigenvalues).
+__device__ __forceinline__ void ti_fgh_w(zc ra, zc rb, const TiWave& P, const TiWave& S, double dm,
+                                         zc fg[6])
+{
+    const zc ea = Z(P.er, P.ei), eb = Z(S.er, S.ei);
+    const double xa = dm * ra.re, xb = dm * rb.re;
+    fg[0] = zabs(ra) < 1.0e-08 ? Z(dm) : zdiv(Z(1.0) - (xa < 40.0 ? ea * ea : Z(0.0)), 2.0 * ra);
+    fg[1] = xa < 75.0 ? dm * ea : Z(0.0);
+    fg[2] = zabs(rb) < 1.0e-08 ? Z(dm) : zdiv(Z(1.0) - (xb < 40.0 ? eb * eb : Z(0.0)), 2.0 * rb);
+    fg[3] = xb < 75.0 ? dm * eb : Z(0.0);
+    const zc sab = rb + ra;
+    fg[4] = zabs(sab) < 1.0e-08 ? Z(dm)
+            : zdiv(Z(1.0) - (dm * sab.re < 40.0 ? ea * eb : Z(0.0)), sab);
+    fg[5] = zabs(rb - ra) < 1.0e-08 ? Z(dm)
+            : zdiv((xb < 40.0 ? eb : Z(0.0)) - (xa < 40.0 ? ea : Z(0.0)), ra - rb);
+}
+
+// Small fixed-size vectors passed by value to the out-of-line paths (so
+// the hot loop keeps its vectors in registers).
+struct D4 { double v[4]; };
+struct D5 { double v[5]; };
+struct D6 { double v[6]; };
+struct UpOut { D5 ee; double pexsv; };
+struct DownOut { D4 vv; double cpex; };
+
+// Up-sweep step of a layer with complex eigenvalues: ee = cdv * CA.
+__device__ __noinline__ UpOut ti_up_general(TiLayer L, double omega, double wvno, double wvno2, D5 cdv)
+{
+    TiEigZ EZ;
+    ti_eigen_z(L, omega, wvno, wvno2, EZ);
+    TiVarZ VZ;
+    ti_var_z_one(EZ.rp, L.td, VZ.cosp, VZ.rsinp, VZ.sinpr, VZ.pex);
+    ti_var_z_one(EZ.rsv, L.td, VZ.cosq, VZ.rsinq, VZ.sinqr, VZ.svex);
+    double ca[5][5];
+    ti_compound_z(EZ, VZ, ca);
+    UpOut o;
+    for (int i = 0; i < 5; ++i)
+        o.ee.v[i] = cdv.v[0] * ca[0][i] + cdv.v[1] * ca[1][i] + cdv.v[2] * ca[2][i] +
+                    cdv.v[3] * ca[3][i] + cdv.v[4] * ca[4][i];
+    o.pexsv = VZ.pex + VZ.svex;
+    return o;
+}
+
+// Down-sweep Haskell step of a layer with complex eigenvalues.
+__device__ __noinline__ DownOut ti_down_general(TiLayer L, double omega, double wvno, double wvno2, D4 vv)
+{
+    TiEigZ EZ;
+    ti_eigen_z(L, omega, wvno, wvno2, EZ);
+    TiVarZ VZ;
+    ti_var_z_one(EZ.rp, L.td, VZ.cosp, VZ.rsinp, VZ.sinpr, VZ.pex);
+    ti_var_z_one(EZ.rsv, L.td, VZ.cosq, VZ.rsinq, VZ.sinqr, VZ.svex);
+    DownOut o;
+    o.vv = vv;
+    ti_haskell_z(EZ, VZ, o.vv.v, o.cpex);
+    return o;
+}
+
+// Energy integrals of a layer with an oscillatory wave (real eigenvalues,
+// imaginary vertical wavenumber): complex arithmetic, exponentials from the
+// waves.
+__device__ __noinline__ D6 ti_integrals_osc(TiEig E, TiWave P, TiWave S, double dm, D4 top, D4 bot)
+{
+    TiEigZ EZ;
+    eig_to_z(E, EZ);
+    zc fg[6];
+    ti_fgh_w(EZ.rp, EZ.rsv, P, S, dm, fg);
+    D6 o;
+    ti_integrals_z(EZ, fg, top.v, bot.v, false, o.v);
+    return o;
+}
+
+// Energy integrals of the half-space or of a layer with complex
+// eigenvalues (complex exponentials).
+__device__ __noinline__ D6 ti_integrals_general(TiLayer L, double omega, double wvno, double wvno2,
+                                                D4 top, D4 bot, bool half)
+{
+    TiEig E;
+    ti_eigen(L, omega, wvno, wvno2, E);
+    TiEigZ EZ;
+    if (E.ok) eig_to_z(E, EZ);
+    else ti_eigen_z(L, omega, wvno, wvno2, EZ);
+    zc fg[6];
+    if (!half) ti_fgh_z(EZ.rp, EZ.rsv, L.td, fg);
+    D6 o;
+    ti_integrals_z(EZ, fg, top.v, bot.v, half, o.v);
+    return o;
+}
+
+// Haskell step (hska) of an evanescent or oscillatory layer with real
+// eigenvalues, from its waves.
+__device__ __forceinline__ void ti_haskell_w(const TiEig& E, const TiWave& P, const TiWave& S, double v[4],
+                                             double& cpex)
+{
+    TiVar V;
+    V.cosp = P.cosf; V.rsinp = P.rsin; V.sinpr = P.sinr; V.pex = P.ex;
+    V.cosq = S.cosf; V.rsinq = S.rsin; V.sinqr = S.sinr; V.svex = S.ex;
+    ti_haskell(E, V, v, cpex);
+}
+
 // Max-norm scaling by a power of two (exact; the exponent is carried in
 // ex2 as a natural-log amount, like cnormc/rnormc's log(t1)).
 __device__ __forceinline__ double pow2_normalise(double* v, int n)
@@ -646,12 +836,13 @@ ti_kernel(TiArgs a)
         const double omega = (double)twopi / (double)(float)a.periods[M.per_b + k];
         const double wvno = omega / (double)cpf;
         const double wvno2 = wvno * wvno;
+        const double iwvno = 1.0 / wvno, iwvno2 = 1.0 / wvno2;
         // ---- up(): compound vectors from the half-space upward
         double cdv[5];
         double exsum = 0.0;
         {
             // half-space: E^-1 rows 1-2 and their 2x2 minors (evalg, up)
-            const TiLayer L = ti_layer(tir[(long long)(rmax - 1) * TILE]);
+            const TiLayer L = ti_layer(tir + (long long)(rmax - 1) * TILE);
             TiEigZ E;
             ti_eigen_z(L, omega, wvno, wvno2, E);
             zc e[4][4], G[4][4];
@@ -666,30 +857,30 @@ ti_kernel(TiArgs a)
             sp[5 * nslots] = 0.0;
         }
         for (int m = rmax - 2; m >= 0; --m) {
-            const TiLayer L = ti_layer(tir[(long long)m * TILE]);
+            const TiLayer L = ti_layer(tir + (long long)m * TILE);
             TiEig E;
             ti_eigen(L, omega, wvno, wvno2, E);
-            double ca[5][5];
+            double ee[5];
             double pexsv;
             if (E.ok) {
                 TiVar V;
-                ti_var_one(E.rp, E.oscp, L.d, V.cosp, V.rsinp, V.sinpr, V.pex);
-                ti_var_one(E.rsv, E.oscs, L.d, V.cosq, V.rsinq, V.sinqr, V.svex);
+                ti_var_one(E.rp, E.oscp, L.td, V.cosp, V.rsinp, V.sinpr, V.pex);
+                ti_var_one(E.rsv, E.oscs, L.td, V.cosq, V.rsinq, V.sinqr, V.svex);
+                double ca[5][5];
                 ti_compound(E, V, ca);
                 pexsv = V.pex + V.svex;
-            } else {
-                TiEigZ EZ;
-                ti_eigen_z(L, omega, wvno, wvno2, EZ);
-                TiVarZ VZ;
-                ti_var_z_one(EZ.rp, L.d, VZ.cosp, VZ.rsinp, VZ.sinpr, VZ.pex);
-                ti_var_z_one(EZ.rsv, L.d, VZ.cosq, VZ.rsinq, VZ.sinqr, VZ.svex);
-                ti_compound_z(EZ, VZ, ca);
-                pexsv = VZ.pex + VZ.svex;
-            }
-            double ee[5];
 #pragma unroll
-            for (int i = 0; i < 5; ++i)
-                ee[i] = cdv[0] * ca[0][i] + cdv[1] * ca[1][i] + cdv[2] * ca[2][i] + cdv[3] * ca[3][i] + cdv[4] * ca[4][i];
+                for (int i = 0; i < 5; ++i)
+                    ee[i] = cdv[0] * ca[0][i] + cdv[1] * ca[1][i] + cdv[2] * ca[2][i] + cdv[3] * ca[3][i] + cdv[4] * ca[4][i];
+            } else {
+                D5 c5;
+#pragma unroll
+                for (int i = 0; i < 5; ++i) c5.v[i] = cdv[i];
+                const UpOut u = ti_up_general(L, omega, wvno, wvno2, c5);
+#pragma unroll
+                for (int i = 0; i < 5; ++i) ee[i] = u.ee.v[i];
+                pexsv = u.pexsv;
+            }
             const double exn = pow2_normalise(ee, 5);
             exsum = exsum + pexsv + exn;
             double* sp = scr + (long long)m * 6 * nslots;
@@ -700,32 +891,37 @@ ti_kernel(TiArgs a)
         // ---- down() + svfunc() + energy(): interface by interface
         const double exe0 = exsum;     // exe(1)
         const double f1213 = -cdv[1];
+        const double if1213 = 1.0 / f1213;
         double top[4] = {cdv[2] / cdv[1], 1.0, 0.0, 0.0};   // ur, uz, tz, tr at the surface
         double vv[4] = {1.0, 0.0, 0.0, 0.0};
         double exa = 0.0;
         double sumi0 = 0.0, sumi1 = 0.0, sumi2 = 0.0, gsum = 0.0;
         const double pi_ = 3.141592653589493;   // gammap's constant, as in the reference
+        const double lw = log(omega / (2.0 * pi_ * 1.0)) / pi_;
         for (int m = 0; m < rmax; ++m) {
-            const TiLayer L = ti_layer(tir[(long long)m * TILE]);
+            const TiLayer L = ti_layer(tir + (long long)m * TILE);
             TiEig E;
             ti_eigen(L, omega, wvno, wvno2, E);
-            TiEigZ EZ;
-            if (E.ok) eig_to_z(E, EZ);
-            else ti_eigen_z(L, omega, wvno, wvno2, EZ);
             double bot[4] = {0.0, 0.0, 0.0, 0.0};
             const bool half = (m == rmax - 1);
+            const bool fast = E.ok && !half;
+            TiWave P, S;
+            if (fast) {
+                P = ti_wave(E.rp, E.oscp, L.td);
+                S = ti_wave(E.rsv, E.oscs, L.td);
+            }
             if (!half) {
                 double cpex;
-                if (E.ok) {
-                    TiVar V;
-                    ti_var_one(E.rp, E.oscp, L.d, V.cosp, V.rsinp, V.sinpr, V.pex);
-                    ti_var_one(E.rsv, E.oscs, L.d, V.cosq, V.rsinq, V.sinqr, V.svex);
-                    ti_haskell(E, V, vv, cpex);
+                if (fast) {
+                    ti_haskell_w(E, P, S, vv, cpex);
                 } else {
-                    TiVarZ VZ;
-                    ti_var_z_one(EZ.rp, L.d, VZ.cosp, VZ.rsinp, VZ.sinpr, VZ.pex);
-                    ti_var_z_one(EZ.rsv, L.d, VZ.cosq, VZ.rsinq, VZ.sinqr, VZ.svex);
-                    ti_haskell_z(EZ, VZ, vv, cpex);
+                    D4 v4;
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) v4.v[i] = vv[i];
+                    const DownOut d = ti_down_general(L, omega, wvno, wvno2, v4);
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) vv[i] = d.vv.v[i];
+                    cpex = d.cpex;
                 }
                 const double ex2 = pow2_normalise(vv, 4);
                 exa = exa + cpex + ex2;
@@ -741,17 +937,27 @@ ti_kernel(TiArgs a)
                 const double uu4 = -tz1 * cd4 + tz2 * cd2 - tz3 * cd1;
                 const double ext = exa + exe - exe0;
                 if (ext > -80.0 && ext < 80.0) {
-                    const double fact = exp(ext) / f1213;
+                    const double fact = exp(ext) * if1213;
                     bot[0] = uu1 * fact; bot[1] = uu2 * fact; bot[2] = uu3 * fact; bot[3] = uu4 * fact;
                 }
             }
             // energy integrals of layer m (typelyr 0, or 1 for the half-space)
             double I[6];
-            ti_integrals(EZ, L.d, top, bot, half, I);
-            const double TA = L.TA, TC = L.TC, TF = L.TF, TL = L.TL, TN = L.TN, rho = L.rho;
-            const double ah = sqrt(TA / rho), av = sqrt(TC / rho), bh = sqrt(TN / rho), bv = sqrt(TL / rho);
-            const double eta = TF / (TA - 2.0 * TL);
-            const double a12 = -wvno, a14 = 1.0 / TL, a21 = wvno * TF / TC, a23 = 1.0 / TC;
+            if (fast && !E.oscp && !E.oscs) {
+                ti_integrals_real(E, P, S, L.td, top, bot, I);
+            } else {
+                D4 t4, b4;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) { t4.v[i] = top[i]; b4.v[i] = bot[i]; }
+                const D6 r = fast ? ti_integrals_osc(E, P, S, L.td, t4, b4)
+                                  : ti_integrals_general(L, omega, wvno, wvno2, t4, b4, half);
+#pragma unroll
+                for (int i = 0; i < 6; ++i) I[i] = r.v[i];
+            }
+            const double TA = L.TA, TF = L.TF, TL = L.TL, rho = L.rho;
+            const double ah = L.ah, av = L.ah, bv = L.bv;
+            const double eta = L.eta;
+            const double a12 = -wvno, a14 = L.iTL, a21 = wvno * L.TFoTA, a23 = L.iTA;
             const double URUR = I[0], UZUZ = I[2];
             const double DURDUR = a12 * a12 * I[2] + 2.0 * a12 * a14 * I[3] + a14 * a14 * I[5];
             const double DUZDUZ = a21 * a21 * I[0] + 2.0 * a21 * a23 * I[1] + a23 * a23 * I[4];
@@ -760,15 +966,13 @@ ti_kernel(TiArgs a)
             sumi0 += rho * (URUR + UZUZ);
             sumi1 += TL * UZUZ + TA * URUR;
             sumi2 += TL * UZDUR - TF * URDUZ;
-            const double facah = rho * ah * (URUR - 2.0 * eta * URDUZ / wvno);
-            const double facav = rho * av * DUZDUZ / wvno2;
-            const double facbv = rho * bv * (UZUZ + 2.0 * UZDUR / wvno + DURDUR / wvno2 + 4.0 * eta * URDUZ / wvno);
-            const double facn = -TF * URDUZ / (wvno * eta);
+            const double facah = rho * ah * (URUR - 2.0 * eta * URDUZ * iwvno);
+            const double facav = rho * av * DUZDUZ * iwvno2;
+            const double facbv = rho * bv * (UZUZ + 2.0 * UZDUR * iwvno + DURDUR * iwvno2 + 4.0 * eta * URDUZ * iwvno);
+            const double facn = -TF * URDUZ * iwvno * L.ieta;
             // gammap() (facbh = 0; Q = 150 / 50, reference frequency 1 Hz)
-            const double lw = log(omega / (2.0 * pi_ * 1.0)) / pi_;
             gsum += lw * (facbv * bv * (double)(1.0f / 50.0f));
             gsum += lw * ((facav * av + facah * ah) * (double)(1.0f / 150.0f));
-            (void)bh;
             // raw partials for the splice (slot m is free: its compound
             // vector was consumed one step earlier)
             double* so = scr + (long long)m * 6 * nslots;
@@ -786,31 +990,25 @@ ti_kernel(TiArgs a)
         const double tq = c2 / (2.0 * 6370.0 * omega);
         const double tm = sqrt(1.0 + tq * tq);
         const double tm3 = tm * tm * tm;
+        const double iun = 1.0 / un, iuntm3 = iun / tm3;
+        const SpRec* spr = T.sp + lbase;
         int m = 0;
         for (int j = 0; j < nz - 1; ++j) {
             float acc = 0.0f;
             for (; m < rmax - 1 && chr[(long long)m * TILE].node == j; ++m) {
-                const TiRec R = tir[(long long)m * TILE];
-                const float rvp = R.rvp, rvs = R.rvs, rrh = R.rrho;
+                const SpRec R = spr[(long long)m * TILE];
                 const double* so = scr + (long long)m * 6 * nslots;
                 const double vt = (double)R.vtp;
-                double vah = so[0] / un * vt / tm3;
-                double vbv = so[nslots] / un * vt / tm3;
-                double vn = so[2 * nslots] / un;
+                const double vah = so[0] * vt * iuntm3;
+                const double vbv = so[nslots] * vt * iuntm3;
+                const double vn = so[2 * nslots] * iun;
                 const float dah = fabs(vah) < 1.0e-36 ? 0.0f : (float)vah;
                 const float dbv = fabs(vbv) < 1.0e-36 ? 0.0f : (float)vbv;
                 const float dn = fabs(vn) < 1.0e-36 ? 0.0f : (float)vn;
                 // depthkernelTI.f90:152-162 (real*4)
-                const float TA = __fmul_rn(rrh, __fmul_rn(rvp, rvp));
-                const float TL = __fmul_rn(rrh, __fmul_rn(rvs, rvs));
-                const float TF = __fmul_rn(1.0f, __fsub_rn(TA, __fmul_rn(2.0f, TL)));
-                const float den = __fsub_rn(TA, __fmul_rn(2.0f, TL));
-                const float den2 = __fmul_rn(den, den);
-                const float dA = __fsub_rn(__fmul_rn(__fdiv_rn(0.5f, __fmul_rn(rrh, rvp)), dah),
-                                           __fmul_rn(__fdiv_rn(TF, den2), dn));
-                const float dL = __fadd_rn(__fmul_rn(__fdiv_rn(0.5f, __fmul_rn(rrh, rvs)), dbv),
-                                           __fmul_rn(__fdiv_rn(__fmul_rn(2.0f, TF), den2), dn));
-                acc = __fadd_rn(__fadd_rn(acc, __fmul_rn(dA, TA)), __fmul_rn(dL, TL));
+                const float dA = __fsub_rn(__fmul_rn(R.cA1, dah), __fmul_rn(R.cA2, dn));
+                const float dL = __fadd_rn(__fmul_rn(R.cL1, dbv), __fmul_rn(R.cL2, dn));
+                acc = __fadd_rn(__fadd_rn(acc, __fmul_rn(dA, R.TA)), __fmul_rn(dL, R.TL));
             }
             lout[jstride * j] = acc;
             if (!isfinite(acc) && a.errflag) atomicOr(a.errflag, 1);
