@@ -332,7 +332,7 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
         AdjArgs j;
         j.T = T; j.periods = per; j.croot = g_ctx.croot.as<double>();
         j.sen_vs = o.svs; j.sen_vp = o.svp; j.sen_rho = o.srh;
-        j.scratch = g_ctx.adjscr.as<double>(); j.queue = queues;
+        j.scratch = g_ctx.adjscr.as<double>(); j.scr_layers = maxr > 1 ? maxr - 1 : 1; j.queue = queues;
         adjoint_kernel<<<(unsigned)nblk, at, 0, st>>>(j);
         CK(cudaGetLastError());
         ++g_ctx.last_launches;
@@ -343,12 +343,12 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
         long long nblk;
         if ((r = launch_persistent_grid((const void*)ti_kernel, nitems, at, nblk))) return r;
         const long long nslots = nblk * at;
-        const size_t scr = sizeof(double) * 6 * (size_t)maxr * (size_t)nslots;
+        const size_t scr = sizeof(double) * TI_SCR_Q * (size_t)maxr * (size_t)nslots;
         if ((r = g_ctx.tiscr.ensure(scr))) return r;
         CK(cudaMemsetAsync(queues + 1, 0, sizeof(unsigned), st));
         TiArgs t;
         t.T = T; t.periods = per; t.pv = o.pv; t.lsen = o.lsen;
-        t.scratch = g_ctx.tiscr.as<double>(); t.queue = queues + 1; t.errflag = errflag;
+        t.scratch = g_ctx.tiscr.as<double>(); t.scr_layers = maxr; t.queue = queues + 1; t.errflag = errflag;
         ti_kernel<<<(unsigned)nblk, at, 0, st>>>(t);
         CK(cudaGetLastError());
         ++g_ctx.last_launches;

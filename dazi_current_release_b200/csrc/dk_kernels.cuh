@@ -48,16 +48,24 @@ struct AdjArgs {
     double* sen_vs;
     double* sen_vp;
     double* sen_rho;
-    double* scratch;        // [(rmax-1)*6][grid threads]
+    double* scratch;        // per warp [scr_layers][6][32 lanes]
+    long long scr_layers;   // layer capacity of a warp's scratch block
     unsigned* queue;        // work-queue counter (zeroed before the launch)
 };
+
+// Doubles per refined layer in each persistent thread's Gc/Gs scratch:
+// the up-sweep's compound vector and exponent sum (6), then the layer's
+// eigen-solution (12), its two waves (5 + 5) and flags (1), which the
+// down-sweep reads back instead of recomputing them.
+constexpr int TI_SCR_Q = 29;
 
 struct TiArgs {
     Tables T;
     const double* periods;
     const double* pv;       // phase velocities (FP32-valued)
     float* lsen;
-    double* scratch;        // [rmax*6][grid threads]
+    double* scratch;        // per warp [scr_layers][TI_SCR_Q][32 lanes]
+    long long scr_layers;   // layer capacity of a warp's scratch block
     unsigned* queue;        // work-queue counter (zeroed before the launch)
     int* errflag;           // set to 1 when an Lsen_Gsc value is not finite
 };

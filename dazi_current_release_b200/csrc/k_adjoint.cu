@@ -17,8 +17,9 @@
 //     dF/dtheta_m = e(m+1) . (dCA_m/dtheta) . g(m) / n_m.
 // One thread owns one (column, period):
 //   1. bottom-up sweep at the root, storing e(m+1) and 1/n_m per layer in a
-//      global scratch slot of the thread (6 doubles per layer, [layer][slot]
-//      so a warp's stores coalesce); the 5x5 matrices are not stored;
+//      global scratch block of the thread's warp (6 doubles per layer,
+//      [layer][6][lane] so a warp's stores coalesce); the 5x5 matrices are
+//      not stored;
 //   2. top-down sweep that recomputes CA_m with forward-mode tangents in
 //      (Vp_m, Vs_m, wvno) -- density enters each element as a power, so its
 //      derivative is read off the values -- and accumulates the node kernels.
@@ -310,11 +311,17 @@ __device__ __forceinline__ long long next_task(unsigned* queue)
     return (long long)__shfl_sync(0xffffffffu, t, 0);
 }
 
-__global__ void __launch_bounds__(128)
+// Minimum resident blocks per SM the register allocation aims for.
+#ifndef DK_ADJ_MIN_BLOCKS
+#define DK_ADJ_MIN_BLOCKS 3
+#endif
+
+__global__ void __launch_bounds__(128, DK_ADJ_MIN_BLOCKS)
 adjoint_kernel(AdjArgs a)
 {
     const Tables& T = a.T;
-    const long long nslots = (long long)gridDim.x * blockDim.x;
+    // scratch: per warp [layer][6][lane] -- compile-time strides
+    constexpr long long nslots = TILE;
     const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     for (;;) {
@@ -341,7 +348,7 @@ adjoint_kernel(AdjArgs a)
         const long long lbase = T.tile_lbase[tk.x] + lane;
         const float4* lay = T.flat + lbase;            // layer m at lay[m * TILE]
         const ChainRec* chr = T.ch + lbase;
-        double* scr = a.scratch + slot;                // [(m*6 + comp)][nslots]
+        double* scr = a.scratch + (slot / TILE) * a.scr_layers * 6 * TILE + lane;
         // ---- 1. bottom-up sweep: store e(m+1) and 1/n_m for m = rmax-2 .. 0
         double e[5];
         {

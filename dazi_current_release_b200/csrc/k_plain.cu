@@ -240,7 +240,12 @@ struct TableModel {
     __device__ __forceinline__ LayerD layer(int m) const { return ld[base + (long long)m * TILE]; }
 };
 
-__global__ void __launch_bounds__(128)
+// Minimum resident blocks per SM the register allocation aims for.
+#ifndef DK_ROOT_MIN_BLOCKS
+#define DK_ROOT_MIN_BLOCKS 1
+#endif
+
+__global__ void __launch_bounds__(128, DK_ROOT_MIN_BLOCKS)
 root_kernel(RootArgs a)
 {
     const Tables& T = a.T;

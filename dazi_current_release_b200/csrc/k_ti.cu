@@ -796,6 +796,54 @@ __device__ __forceinline__ double pow2_normalise(double* v, int n)
     return (double)ex * 0.6931471805599453;
 }
 
+// Compound vector of the half-space: the 2x2 minors of rows 1-2 of its
+// E^-1 (evalg, up).
+__device__ __noinline__ D5 ti_halfspace_cdv(TiLayer L, double omega, double wvno, double wvno2)
+{
+    TiEigZ E;
+    ti_eigen_z(L, omega, wvno, wvno2, E);
+    zc e[4][4], G[4][4];
+    ti_emat(E, e, G);
+    D5 c;
+    c.v[0] = (G[0][0] * G[1][1] - G[0][1] * G[1][0]).re;
+    c.v[1] = (G[0][0] * G[1][2] - G[0][2] * G[1][0]).re;
+    c.v[2] = (G[0][0] * G[1][3] - G[0][3] * G[1][0]).re;
+    c.v[3] = (G[0][1] * G[1][3] - G[0][3] * G[1][1]).re;
+    c.v[4] = (G[0][2] * G[1][3] - G[0][3] * G[1][2]).re;
+    return c;
+}
+
+// Layer stash (scratch entries 6..28 of a layer): eigen-solution, waves
+// (cosf, rsin, sinr, ex or ei, er: an oscillatory wave has ex = 0, an
+// evanescent one ei = 0) and flags (1 real eigenvalues, 2 oscp, 4 oscs).
+__device__ __forceinline__ void ti_stash_store(double* st, long long ns, const TiEig& E, const TiWave& P,
+                                               const TiWave& S)
+{
+    st[6 * ns] = E.x11; st[7 * ns] = E.x21; st[8 * ns] = E.x31; st[9 * ns] = E.x41;
+    st[10 * ns] = E.x12; st[11 * ns] = E.x22; st[12 * ns] = E.x32; st[13 * ns] = E.x42;
+    st[14 * ns] = E.np; st[15 * ns] = E.nsv; st[16 * ns] = E.rp; st[17 * ns] = E.rsv;
+    st[18 * ns] = P.cosf; st[19 * ns] = P.rsin; st[20 * ns] = P.sinr;
+    st[21 * ns] = E.oscp ? P.ei : P.ex; st[22 * ns] = P.er;
+    st[23 * ns] = S.cosf; st[24 * ns] = S.rsin; st[25 * ns] = S.sinr;
+    st[26 * ns] = E.oscs ? S.ei : S.ex; st[27 * ns] = S.er;
+    st[28 * ns] = (double)(1 | (E.oscp ? 2 : 0) | (E.oscs ? 4 : 0));
+}
+
+__device__ __forceinline__ void ti_stash_load(const double* st, long long ns, int fl, TiEig& E, TiWave& P,
+                                              TiWave& S)
+{
+    E.x11 = st[6 * ns]; E.x21 = st[7 * ns]; E.x31 = st[8 * ns]; E.x41 = st[9 * ns];
+    E.x12 = st[10 * ns]; E.x22 = st[11 * ns]; E.x32 = st[12 * ns]; E.x42 = st[13 * ns];
+    E.np = st[14 * ns]; E.nsv = st[15 * ns]; E.rp = st[16 * ns]; E.rsv = st[17 * ns];
+    E.ok = true; E.oscp = (fl & 2) != 0; E.oscs = (fl & 4) != 0;
+    P.cosf = st[18 * ns]; P.rsin = st[19 * ns]; P.sinr = st[20 * ns];
+    const double p4 = st[21 * ns];
+    P.ex = E.oscp ? 0.0 : p4; P.ei = E.oscp ? p4 : 0.0; P.er = st[22 * ns];
+    S.cosf = st[23 * ns]; S.rsin = st[24 * ns]; S.sinr = st[25 * ns];
+    const double s4 = st[26 * ns];
+    S.ex = E.oscs ? 0.0 : s4; S.ei = E.oscs ? s4 : 0.0; S.er = st[27 * ns];
+}
+
 __device__ __forceinline__ long long ti_next_task(unsigned* queue)
 {
     unsigned t = 0;
@@ -803,11 +851,17 @@ __device__ __forceinline__ long long ti_next_task(unsigned* queue)
     return (long long)__shfl_sync(0xffffffffu, t, 0);
 }
 
-__global__ void __launch_bounds__(128)
+// Minimum resident blocks per SM the register allocation aims for.
+#ifndef DK_TI_MIN_BLOCKS
+#define DK_TI_MIN_BLOCKS 8
+#endif
+
+__global__ void __launch_bounds__(128, DK_TI_MIN_BLOCKS)
 ti_kernel(TiArgs a)
 {
     const Tables& T = a.T;
-    const long long nslots = (long long)gridDim.x * blockDim.x;
+    // scratch: per warp [layer][q][lane] -- compile-time strides
+    constexpr long long nslots = TILE;
     const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
     for (;;) {
@@ -830,7 +884,7 @@ ti_kernel(TiArgs a)
         const long long lbase = T.tile_lbase[tk.x] + lane;
         const TiRec* tir = T.ti + lbase;              // layer m at tir[m * TILE]
         const ChainRec* chr = T.ch + lbase;
-        double* scr = a.scratch + slot;               // [(m*6 + q)][nslots]
+        double* scr = a.scratch + (slot / TILE) * a.scr_layers * TI_SCR_Q * TILE + lane;
         // tregn96.f:430-479: twopi real*4, t and cp real*4
         const float twopi = 6.2831855f;
         const double omega = (double)twopi / (double)(float)a.periods[M.per_b + k];
@@ -838,40 +892,35 @@ ti_kernel(TiArgs a)
         const double wvno2 = wvno * wvno;
         const double iwvno = 1.0 / wvno, iwvno2 = 1.0 / wvno2;
         // ---- up(): compound vectors from the half-space upward
+        constexpr int Q = TI_SCR_Q;
         double cdv[5];
         double exsum = 0.0;
         {
-            // half-space: E^-1 rows 1-2 and their 2x2 minors (evalg, up)
-            const TiLayer L = ti_layer(tir + (long long)(rmax - 1) * TILE);
-            TiEigZ E;
-            ti_eigen_z(L, omega, wvno, wvno2, E);
-            zc e[4][4], G[4][4];
-            ti_emat(E, e, G);
-            cdv[0] = (G[0][0] * G[1][1] - G[0][1] * G[1][0]).re;
-            cdv[1] = (G[0][0] * G[1][2] - G[0][2] * G[1][0]).re;
-            cdv[2] = (G[0][0] * G[1][3] - G[0][3] * G[1][0]).re;
-            cdv[3] = (G[0][1] * G[1][3] - G[0][3] * G[1][1]).re;
-            cdv[4] = (G[0][2] * G[1][3] - G[0][3] * G[1][2]).re;
-            double* sp = scr + (long long)(rmax - 1) * 6 * nslots;
-            for (int q = 0; q < 5; ++q) sp[q * nslots] = cdv[q];
+            const D5 c = ti_halfspace_cdv(ti_layer(tir + (long long)(rmax - 1) * TILE), omega, wvno, wvno2);
+            double* sp = scr + (long long)(rmax - 1) * Q * nslots;
+#pragma unroll
+            for (int q = 0; q < 5; ++q) { cdv[q] = c.v[q]; sp[q * nslots] = cdv[q]; }
             sp[5 * nslots] = 0.0;
         }
         for (int m = rmax - 2; m >= 0; --m) {
             const TiLayer L = ti_layer(tir + (long long)m * TILE);
+            double* sp = scr + (long long)m * Q * nslots;
             TiEig E;
             ti_eigen(L, omega, wvno, wvno2, E);
             double ee[5];
             double pexsv;
             if (E.ok) {
+                const TiWave P = ti_wave(E.rp, E.oscp, L.td), S = ti_wave(E.rsv, E.oscs, L.td);
                 TiVar V;
-                ti_var_one(E.rp, E.oscp, L.td, V.cosp, V.rsinp, V.sinpr, V.pex);
-                ti_var_one(E.rsv, E.oscs, L.td, V.cosq, V.rsinq, V.sinqr, V.svex);
+                V.cosp = P.cosf; V.rsinp = P.rsin; V.sinpr = P.sinr; V.pex = P.ex;
+                V.cosq = S.cosf; V.rsinq = S.rsin; V.sinqr = S.sinr; V.svex = S.ex;
                 double ca[5][5];
                 ti_compound(E, V, ca);
-                pexsv = V.pex + V.svex;
+                pexsv = P.ex + S.ex;
 #pragma unroll
                 for (int i = 0; i < 5; ++i)
                     ee[i] = cdv[0] * ca[0][i] + cdv[1] * ca[1][i] + cdv[2] * ca[2][i] + cdv[3] * ca[3][i] + cdv[4] * ca[4][i];
+                ti_stash_store(sp, nslots, E, P, S);
             } else {
                 D5 c5;
 #pragma unroll
@@ -880,10 +929,10 @@ ti_kernel(TiArgs a)
 #pragma unroll
                 for (int i = 0; i < 5; ++i) ee[i] = u.ee.v[i];
                 pexsv = u.pexsv;
+                sp[28 * nslots] = 0.0;
             }
             const double exn = pow2_normalise(ee, 5);
             exsum = exsum + pexsv + exn;
-            double* sp = scr + (long long)m * 6 * nslots;
 #pragma unroll
             for (int q = 0; q < 5; ++q) { cdv[q] = ee[q]; sp[q * nslots] = ee[q]; }
             sp[5 * nslots] = exsum;
@@ -900,16 +949,14 @@ ti_kernel(TiArgs a)
         const double lw = log(omega / (2.0 * pi_ * 1.0)) / pi_;
         for (int m = 0; m < rmax; ++m) {
             const TiLayer L = ti_layer(tir + (long long)m * TILE);
-            TiEig E;
-            ti_eigen(L, omega, wvno, wvno2, E);
             double bot[4] = {0.0, 0.0, 0.0, 0.0};
             const bool half = (m == rmax - 1);
-            const bool fast = E.ok && !half;
+            const double* st = scr + (long long)m * Q * nslots;
+            const int fl = half ? 0 : (int)st[28 * nslots];
+            const bool fast = (fl & 1) != 0;
+            TiEig E;
             TiWave P, S;
-            if (fast) {
-                P = ti_wave(E.rp, E.oscp, L.td);
-                S = ti_wave(E.rsv, E.oscs, L.td);
-            }
+            if (fast) ti_stash_load(st, nslots, fl, E, P, S);
             if (!half) {
                 double cpex;
                 if (fast) {
@@ -926,7 +973,7 @@ ti_kernel(TiArgs a)
                 const double ex2 = pow2_normalise(vv, 4);
                 exa = exa + cpex + ex2;
                 // eigenfunctions at interface m+1 (svfunc)
-                const double* sp = scr + (long long)(m + 1) * 6 * nslots;
+                const double* sp = scr + (long long)(m + 1) * Q * nslots;
                 const double cd1 = sp[0], cd2 = sp[nslots], cd3 = sp[2 * nslots];
                 const double cd4 = -cd3, cd5 = sp[3 * nslots], cd6 = sp[4 * nslots];
                 const double exe = sp[5 * nslots];
@@ -975,7 +1022,7 @@ ti_kernel(TiArgs a)
             gsum += lw * ((facav * av + facah * ah) * (double)(1.0f / 150.0f));
             // raw partials for the splice (slot m is free: its compound
             // vector was consumed one step earlier)
-            double* so = scr + (long long)m * 6 * nslots;
+            double* so = scr + (long long)m * Q * nslots;
             so[0] = facah; so[nslots] = facbv; so[2 * nslots] = facn;
 #pragma unroll
             for (int i = 0; i < 4; ++i) top[i] = bot[i];
@@ -997,7 +1044,7 @@ ti_kernel(TiArgs a)
             float acc = 0.0f;
             for (; m < rmax - 1 && chr[(long long)m * TILE].node == j; ++m) {
                 const SpRec R = spr[(long long)m * TILE];
-                const double* so = scr + (long long)m * 6 * nslots;
+                const double* so = scr + (long long)m * Q * nslots;
                 const double vt = (double)R.vtp;
                 const double vah = so[0] * vt * iuntm3;
                 const double vbv = so[nslots] * vt * iuntm3;
