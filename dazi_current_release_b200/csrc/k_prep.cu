@@ -19,12 +19,10 @@ __device__ __forceinline__ int nsub_of(float thk, float minthk0)
     return (int)__fdiv_rn(__fadd_rn(thk, 1.0e-4f), minthk) + 1;
 }
 
-// rmax per column, validation and the sort key.
-__global__ void prep_count_kernel(ColSrc src, long long ncols, unsigned* keys, int* colidx,
-                                  int* rmax_out, int* err)
+// rmax of column c, validation and the sort key.
+__device__ __forceinline__ void prep_count_one(const ColSrc& src, long long c, unsigned* keys, int* colidx,
+                               int* rmax_out, int* err)
 {
-    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= ncols) return;
     const int nz = src.col_nz(c), K = src.col_K(c);
     int r = 0, bad = 0;
     if (nz < 2 || nz > NZMAX) bad |= 1;
@@ -48,6 +46,14 @@ __global__ void prep_count_kernel(ColSrc src, long long ncols, unsigned* keys, i
     rmax_out[c] = r;
     keys[c] = ((unsigned)r << 8) | (unsigned)(K > 255 ? 255 : K);
     colidx[c] = (int)c;
+}
+
+__global__ void prep_count_kernel(ColSrc src, long long ncols, unsigned* keys, int* colidx,
+                                  int* rmax_out, int* err)
+{
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= ncols) return;
+    prep_count_one(src, c, keys, colidx, rmax_out, err);
 }
 
 // Per tile (after sorting): its layer count, period count and record count.
@@ -78,13 +84,11 @@ __global__ void prep_tasks_kernel(long long ntiles, const long long* tile_tasks,
     for (long long k = 0; k < tile_tasks[t]; ++k) tasks[b + k] = make_int2((int)t, (int)k);
 }
 
-// Build the layer records and metadata of one column (thread per sorted
-// position).  Output addressing of the column goes into its ColMeta.
-__global__ void prep_build_kernel(ColSrc src, PrepOut o, Tables T, const int* sorted_col,
-                                  const long long* tile_tbase)
+// Build the layer records and metadata of the column at sorted position s.
+// Output addressing of the column goes into its ColMeta.
+__device__ __forceinline__ void prep_build_one(const ColSrc& src, const PrepOut& o, const Tables& T,
+                               const int* sorted_col, const long long* tile_tbase, long long s)
 {
-    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= T.ncols) return;
     const int c = sorted_col[s];
     const int nz = src.col_nz(c), K = src.col_K(c);
     ColMeta M;
@@ -218,6 +222,15 @@ __global__ void prep_build_kernel(ColSrc src, PrepOut o, Tables T, const int* so
         atomicAdd(o.work, (unsigned long long)K * (unsigned long long)m);
         atomicAdd(o.work + 1, (unsigned long long)K);
     }
+}
+
+// One thread per sorted position.
+__global__ void prep_build_kernel(ColSrc src, PrepOut o, Tables T, const int* sorted_col,
+                                  const long long* tile_tbase)
+{
+    const long long s = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= T.ncols) return;
+    prep_build_one(src, o, T, sorted_col, tile_tbase, s);
 }
 
 }  // namespace dk

@@ -856,35 +856,31 @@ __device__ __forceinline__ long long ti_next_task(unsigned* queue)
 #define DK_TI_MIN_BLOCKS 8
 #endif
 
-__global__ void __launch_bounds__(128, DK_TI_MIN_BLOCKS)
-ti_kernel(TiArgs a)
+// One (column, period) of the Gc/Gs kernel: lane `lane` of task `task`,
+// with the thread's scratch block at scr (layer m, entry q at
+// scr[(m * TI_SCR_Q + q) * TILE]).
+__device__ __forceinline__ void ti_task(const TiArgs& a, long long task, int lane, double* scr)
 {
     const Tables& T = a.T;
-    // scratch: per warp [layer][q][lane] -- compile-time strides
     constexpr long long nslots = TILE;
-    const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    const int lane = threadIdx.x & 31;
-    for (;;) {
-        const long long task = ti_next_task(a.queue);
-        if (task >= T.ntasks) break;
+    {
         const int2 tk = T.tasks[task];
         const long long s = (long long)tk.x * TILE + lane;
         const int k = tk.y;
-        if (s >= T.ncols) continue;
+        if (s >= T.ncols) return;
         const ColMeta M = T.meta[s];
-        if (k >= M.K) continue;
+        if (k >= M.K) return;
         const int rmax = M.rmax, nz = M.nz;
         float* lout = a.lsen + M.ls_b + T.ls_sk * k;
         const long long jstride = M.ls_is;
         const float cpf = (float)a.pv[M.pv_b + T.pv_sk * k];
         if (!(cpf > 0.0f)) {
             for (int j = 0; j < nz - 1; ++j) lout[jstride * j] = 0.0f;
-            continue;
+            return;
         }
         const long long lbase = T.tile_lbase[tk.x] + lane;
         const TiRec* tir = T.ti + lbase;              // layer m at tir[m * TILE]
         const ChainRec* chr = T.ch + lbase;
-        double* scr = a.scratch + (slot / TILE) * a.scr_layers * TI_SCR_Q * TILE + lane;
         // tregn96.f:430-479: twopi real*4, t and cp real*4
         const float twopi = 6.2831855f;
         const double omega = (double)twopi / (double)(float)a.periods[M.per_b + k];
@@ -1060,6 +1056,20 @@ ti_kernel(TiArgs a)
             lout[jstride * j] = acc;
             if (!isfinite(acc) && a.errflag) atomicOr(a.errflag, 1);
         }
+    }
+}
+
+__global__ void __launch_bounds__(128, DK_TI_MIN_BLOCKS)
+ti_kernel(TiArgs a)
+{
+    // scratch: per warp [layer][q][lane] -- compile-time strides
+    const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    double* scr = a.scratch + (slot / TILE) * a.scr_layers * TI_SCR_Q * TILE + lane;
+    for (;;) {
+        const long long task = ti_next_task(a.queue);
+        if (task >= a.T.ntasks) break;
+        ti_task(a, task, lane, scr);
     }
 }
 

@@ -66,3 +66,21 @@ def assert_pv_parity(got, ref, ref_unrounded, midpoint_rel=1e-8):
         assert dist <= midpoint_rel, \
             f"pv[{k}] flipped by one ulp but its double root is {dist:.2e} from the midpoint"
     return diff.size
+
+
+def assert_fd_parity(got, exp, x, dln=0.01, max_frac=0.02, tol=1.0e-6, cmax=8.0):
+    """Finite-difference kernels (K, nz) against the oracle's: equal, except
+    a few entries whose perturbed-model roots differ from the oracle's
+    within the root search's own convergence tolerance (|c1 - c2| <=
+    tol * c1, surfdisp96.f:608): a root on a float32 rounding midpoint (see
+    assert_pv_parity), or a Neville sequence that took another branch at a
+    point where F is zero to FP64 rounding.  Bound on the difference
+    quotient: |d| * dln * x_i <= 2 tol cmax.  x: the perturbed node values
+    (Vs, Vp or rho).  Returns the number of differing entries."""
+    got = np.asarray(got, np.float64)
+    exp = np.asarray(exp, np.float64)
+    d = np.abs(got - exp) * dln * np.asarray(x, np.float64)[None, :]
+    n = int(np.count_nonzero(got != exp))
+    assert (d <= 2.0 * tol * cmax).all(), f"FD kernel differs by {d.max():.3g} km/s in the difference"
+    assert n <= max(2, max_frac * got.size), f"{n} of {got.size} FD entries differ"
+    return n
