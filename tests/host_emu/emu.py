@@ -1,0 +1,38 @@
+"""Loader of the host build of the library's Gc/Gs device code (test
+infrastructure: checks the device arithmetic against the oracle on CPU)."""
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        subprocess.run(["make", "-s", "-C", HERE], check=True)
+        _lib = ctypes.CDLL(os.path.join(HERE, "_build", "libemu_ti.so"))
+    return _lib
+
+
+def ti_batch(node_off, depz, vs, per_off, periods, minthk, pv):
+    """Lsen_Gsc of a ragged batch (dazi_dk_batch layout) from the given
+    phase velocities, computed by the device code built for the host."""
+    P = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))  # noqa: E731
+    node_off = np.ascontiguousarray(node_off, np.int64)
+    per_off = np.ascontiguousarray(per_off, np.int64)
+    nz = np.diff(node_off)
+    K = np.diff(per_off)
+    ls_off = np.concatenate([[0], np.cumsum(K * (nz - 1))]).astype(np.int64)
+    ls = np.zeros(max(int(ls_off[-1]), 1), np.float32)
+    i64, f32, f64 = ctypes.c_longlong, ctypes.c_float, ctypes.c_double
+    rc = lib().emu_ti_batch(i64(node_off.size - 1), P(node_off, i64),
+                            P(np.ascontiguousarray(depz, np.float32), f32),
+                            P(np.ascontiguousarray(vs, np.float32), f32), P(per_off, i64),
+                            P(np.ascontiguousarray(periods, np.float64), f64), f32(minthk),
+                            P(np.ascontiguousarray(pv, np.float64), f64), P(ls_off, i64),
+                            P(ls, f32))
+    return rc, ls, ls_off
