@@ -251,8 +251,13 @@ __device__ __forceinline__ T tca_elem(const T (&xs)[5][3], const F (&fac)[3][4])
     return tca_expand(xs, fac, S{});
 }
 
-// dnka_tregn (elastic) in real arithmetic: the reduced 5x5 compound matrix.
-__device__ __forceinline__ void ti_compound(const TiEig& E, const TiVar& v, double ca[5][5])
+// The up-sweep step with the real compound matrix: ee = cdv * CA, each
+// tca element folded into ee as soon as it is formed (CA is never held):
+//   CA rows  (t11 t12 t13 t15 t16) (t21 t22 t23 t25 t15)
+//            (2t31 2t32 2t33-dfac -2t23 -2t13) (t51 t52 -t32 t22 t12)
+//            (t61 t51 -t31 t21 t11)
+__device__ __forceinline__ void ti_compound_apply(const TiEig& E, const TiVar& v, const double c[5],
+                                                  double ee[5])
 {
     const double ex = v.pex + v.svex;
     const double dfac = ex > 35.0 ? 0.0 : exp(-ex);
@@ -265,21 +270,25 @@ __device__ __forceinline__ void ti_compound(const TiEig& E, const TiVar& v, doub
     double xs[5][3];
     xs[1][1] = E.x11; xs[2][1] = E.x21; xs[3][1] = E.x31; xs[4][1] = E.x41;
     xs[1][2] = E.x12; xs[2][2] = E.x22; xs[3][2] = E.x32; xs[4][2] = E.x42;
-    double t[15];
-    t[0] = tca_elem<0>(xs, fac);   t[1] = tca_elem<1>(xs, fac);   t[2] = tca_elem<2>(xs, fac);
-    t[3] = tca_elem<3>(xs, fac);   t[4] = tca_elem<4>(xs, fac);   t[5] = tca_elem<5>(xs, fac);
-    t[6] = tca_elem<6>(xs, fac);   t[7] = tca_elem<7>(xs, fac);   t[8] = tca_elem<8>(xs, fac);
-    t[9] = tca_elem<9>(xs, fac);   t[10] = tca_elem<10>(xs, fac); t[11] = tca_elem<11>(xs, fac);
-    t[12] = tca_elem<12>(xs, fac); t[13] = tca_elem<13>(xs, fac); t[14] = tca_elem<14>(xs, fac);
-    const double t11 = t[0], t12 = t[1], t13 = t[2], t15 = t[3], t16 = t[4], t21 = t[5];
-    const double t22 = t[6], t23 = t[7], t25 = t[8], t31 = t[9], t32 = t[10], t33 = t[11];
-    const double t51 = t[12], t52 = t[13], t61 = t[14];
-    ca[0][0] = t11; ca[0][1] = t12; ca[0][2] = t13; ca[0][3] = t15; ca[0][4] = t16;
-    ca[1][0] = t21; ca[1][1] = t22; ca[1][2] = t23; ca[1][3] = t25; ca[1][4] = t15;
-    ca[2][0] = 2.0 * t31; ca[2][1] = 2.0 * t32; ca[2][2] = 2.0 * t33 - dfac;
-    ca[2][3] = -2.0 * t23; ca[2][4] = -2.0 * t13;
-    ca[3][0] = t51; ca[3][1] = t52; ca[3][2] = -t32; ca[3][3] = t22; ca[3][4] = t12;
-    ca[4][0] = t61; ca[4][1] = t51; ca[4][2] = -t31; ca[4][3] = t21; ca[4][4] = t11;
+    const double c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3], c4 = c[4];
+    const double c2x2 = 2.0 * c2;
+    double e0, e1, e2, e3, e4;
+    {   const double t = tca_elem<0>(xs, fac);  e0 = c0 * t;  e4 = c4 * t; }           // t11
+    {   const double t = tca_elem<1>(xs, fac);  e1 = c0 * t;  e4 += c3 * t; }          // t12
+    {   const double t = tca_elem<2>(xs, fac);  e2 = c0 * t;  e4 -= c2x2 * t; }        // t13
+    {   const double t = tca_elem<3>(xs, fac);  e3 = c0 * t;  e4 += c1 * t; }          // t15
+    {   const double t = tca_elem<4>(xs, fac);  e4 += c0 * t; }                         // t16
+    {   const double t = tca_elem<5>(xs, fac);  e0 += c1 * t; e3 += c4 * t; }          // t21
+    {   const double t = tca_elem<6>(xs, fac);  e1 += c1 * t; e3 += c3 * t; }          // t22
+    {   const double t = tca_elem<7>(xs, fac);  e2 += c1 * t; e3 -= c2x2 * t; }        // t23
+    {   const double t = tca_elem<8>(xs, fac);  e3 += c1 * t; }                         // t25
+    {   const double t = tca_elem<9>(xs, fac);  e0 += c2x2 * t; e2 -= c4 * t; }        // t31
+    {   const double t = tca_elem<10>(xs, fac); e1 += c2x2 * t; e2 -= c3 * t; }        // t32
+    {   const double t = tca_elem<11>(xs, fac); e2 += c2 * (2.0 * t - dfac); }          // t33
+    {   const double t = tca_elem<12>(xs, fac); e0 += c3 * t; e1 += c4 * t; }          // t51
+    {   const double t = tca_elem<13>(xs, fac); e1 += c3 * t; }                         // t52
+    {   const double t = tca_elem<14>(xs, fac); e0 += c4 * t; }                         // t61
+    ee[0] = e0; ee[1] = e1; ee[2] = e2; ee[3] = e3; ee[4] = e4;
 }
 
 // E and E^-1 of a layer (evalg, tregn96.f:3055-3105) as complex matrices.
@@ -910,12 +919,8 @@ __device__ __forceinline__ void ti_task(const TiArgs& a, long long task, int lan
                 TiVar V;
                 V.cosp = P.cosf; V.rsinp = P.rsin; V.sinpr = P.sinr; V.pex = P.ex;
                 V.cosq = S.cosf; V.rsinq = S.rsin; V.sinqr = S.sinr; V.svex = S.ex;
-                double ca[5][5];
-                ti_compound(E, V, ca);
+                ti_compound_apply(E, V, cdv, ee);
                 pexsv = P.ex + S.ex;
-#pragma unroll
-                for (int i = 0; i < 5; ++i)
-                    ee[i] = cdv[0] * ca[0][i] + cdv[1] * ca[1][i] + cdv[2] * ca[2][i] + cdv[3] * ca[3][i] + cdv[4] * ca[4][i];
                 ti_stash_store(sp, nslots, E, P, S);
             } else {
                 D5 c5;
