@@ -378,11 +378,19 @@ def main_ragged(args, ws, rank, local):
     evals, layer_evals, layer_items = work()
     value = ws * ncp / (ms_per_step * 1e-3)
 
-    # per-phase device times of one more step (events inside the library)
+    # per-phase device times of one more step (events inside the library),
+    # and of one step with every root-search evaluation in FP64
     _lib.check(L.dazi_dk_set_timing(1))
     torch.cuda.synchronize(dev)
     step_fn(form, ncol)()
     phases = _lib.last_timing()
+    scan64 = None
+    if form == _lib.FORM_ADJOINT:
+        pv32 = pv.clone()
+        step_fn(form | _lib.FORM_SCAN_FP64, ncol)()
+        ph64 = _lib.last_timing()
+        scan64 = {"root_ms_fp32_scan": phases.get("root"), "root_ms_fp64_scan": ph64.get("root"),
+                  "identical_roots": bool(torch.equal(pv32, pv))}
     _lib.check(L.dazi_dk_set_timing(0))
 
     # end to end: host C-ABI dazi_dk_batch with pinned host buffers
@@ -471,6 +479,8 @@ def main_ragged(args, ws, rank, local):
         "roofline": roof,
         "gpu_launches": args.steps * launches,
     }
+    if scan64:
+        line["root_scan"] = scan64
     if sample:
         line["same_columns"] = dict(sample, columns=ns, column_periods=ns_cp,
                                     adjoint_over_plain=sample["adjoint"]["value"] /

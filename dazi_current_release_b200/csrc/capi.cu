@@ -99,6 +99,12 @@ struct Context {
 Context g_ctx;
 std::mutex g_mu;
 
+bool valid_form(int form)
+{
+    const int f = form & ~DAZI_FORM_SCAN_FP64;
+    return f == DAZI_FORM_PLAIN || f == DAZI_FORM_ADJOINT;
+}
+
 void phase_begin(cudaStream_t st)
 {
     PhaseTimer& T = g_ctx.timer;
@@ -297,7 +303,7 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
     unsigned long long* nevals = g_ctx.counters.as<unsigned long long>();
     int* errflag = reinterpret_cast<int*>(nevals + 1);
     unsigned* queues = reinterpret_cast<unsigned*>(nevals + 2);
-    const bool adj = o.svs && form == DAZI_FORM_ADJOINT;
+    const bool adj = o.svs && (form & 1) == DAZI_FORM_ADJOINT;
     long long maxr = 0;
     {
         // largest layer count (first sorted column) for the scratch sizes
@@ -310,6 +316,7 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
         RootArgs a;
         a.T = T; a.periods = per; a.tol = 1.0e-6;   // surfdisp96.f:608
         a.pv = o.pv; a.croot = nullptr; a.status = o.status; a.nevals = nevals;
+        a.scan32 = (form & DAZI_FORM_SCAN_FP64) ? 0 : 1;
         if (adj) {
             if ((r = g_ctx.croot.ensure(sizeof(double) * TILE * (size_t)T.ntasks))) return r;
             a.croot = g_ctx.croot.as<double>();
@@ -376,7 +383,7 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
     g_ctx.last_rmax = g_ctx.geo_rmax;
     g_ctx.last_launches = 0;
     phase_begin(st);
-    const bool fd = o.svs && form == DAZI_FORM_PLAIN;
+    const bool fd = o.svs && (form & 1) == DAZI_FORM_PLAIN;
     if (fd) {
         const int nmod = 1 + 6 * nz;
         const size_t per_col = sizeof(float) * (size_t)nmod * kmax;
@@ -447,7 +454,7 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
     PrepOut po{B.sen_off, B.ls_off, g_ctx.counters.as<unsigned long long>() + 4};
     Tables T;
     if ((r = build_tables(src, B.ncols, po, 1, 1, 1, st, T))) return r;
-    const bool fd = o.svs && form == DAZI_FORM_PLAIN;
+    const bool fd = o.svs && (form & 1) == DAZI_FORM_PLAIN;
     if (fd) {
         // plain form: one CTA per column, scratch offsets per column
         std::vector<long long> hoff(B.ncols + 1), hn(B.ncols + 1), hp(B.ncols + 1);
@@ -526,7 +533,7 @@ int stage_host(const int* pnx, const int* pny, const int* pnz, const float* vel,
         return DAZI_ERR_BADARG;
     }
     if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
-    if (form != DAZI_FORM_PLAIN && form != DAZI_FORM_ADJOINT) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    if (!valid_form(form)) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
     const int nx = *pnx, ny = *pny, nz = *pnz, kmax = *pkmax;
     const float minthk = *pminthk;
     int r;
@@ -609,7 +616,7 @@ int check_dev_common(int nz, int kmaxRc, int form, const void* vp, const void* r
         return DAZI_ERR_BADARG;
     }
     if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
-    if (form != DAZI_FORM_PLAIN && form != DAZI_FORM_ADJOINT) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    if (!valid_form(form)) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
     if (nz < 2 || nz > NZMAX) { set_err("nz=%d outside [2, %d]", nz, NZMAX); return DAZI_ERR_LIMITS; }
     if (kmaxRc < 1 || kmaxRc > NP) { set_err("kmaxRc=%d outside [1, %d]", kmaxRc, NP); return DAZI_ERR_LIMITS; }
     return 0;
@@ -733,7 +740,7 @@ int dazi_dk_batch_dev(long long ncols, const long long* node_off, const float* d
         return DAZI_ERR_BADARG;
     }
     if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
-    if (form != DAZI_FORM_PLAIN && form != DAZI_FORM_ADJOINT) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    if (!valid_form(form)) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
     if (!(minthk > 0.f) || !std::isfinite(minthk)) { set_err("minthk must be > 0"); return DAZI_ERR_BADARG; }
     std::lock_guard<std::mutex> lk(g_mu);
     int r;
@@ -759,7 +766,7 @@ int dazi_dk_batch(long long ncols, const long long* node_off, const float* depz,
         return DAZI_ERR_BADARG;
     }
     if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
-    if (form != DAZI_FORM_PLAIN && form != DAZI_FORM_ADJOINT) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    if (!valid_form(form)) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
     if (!(minthk > 0.f) || !std::isfinite(minthk)) { set_err("minthk must be > 0"); return DAZI_ERR_BADARG; }
     if (ncols == 0) return DAZI_OK;
     for (long long c = 0; c < ncols; ++c)

@@ -39,6 +39,7 @@ struct RootArgs {
     double* croot;          // [task * 32 + lane] FP64 roots for the adjoint, or nullptr
     int* status;            // [status_i] first failing period (1-based) or 0
     unsigned long long* nevals;  // secular evaluations (accumulated), or nullptr
+    int scan32;             // FP32 coarse scan (with FP64 verification)
 };
 
 struct AdjArgs {

@@ -6,6 +6,13 @@
 //   nevill + half (refine)        surfdisp96.f:551-680
 //   surfdisp96 period loop        surfdisp96.f:52-354 (Rayleigh, phase, mode 1)
 //
+// Optional FP32 coarse scan (root search of the adjoint form): the getsol
+// scan steps evaluate the secular function in FP32 and use only its sign;
+// values below kScanTrust32 are re-evaluated in FP64, and both ends of a
+// detected bracket are evaluated in FP64 before nevill() (whose steps are
+// FP64), so the values nevill() sees are the reference's.  A bracket end
+// whose FP64 sign contradicts its FP32 sign restarts the period in FP64.
+//
 // The layer chain is a sequential product of 5x5 Dunkin compound matrices,
 // one model per thread; the tensor cores have no role here.  The root search
 // is written as a state machine that performs exactly one secular-function
@@ -135,12 +142,125 @@ __device__ __forceinline__ double dltar4(const M& mdl, int mmax, double wvno, do
     return e0;
 }
 
+// The same secular function in FP32, for the coarse trial-velocity scan.
+// Reads the flattened layer table (d, Vp, Vs, rho) directly; exponentials,
+// reciprocals and square roots in single precision.  Only the sign of the
+// result is used, and only where its magnitude exceeds kScanTrust32 (on the
+// normalised scale of F, |F| <= 1; the FP32 error measured on the uneven
+// batch stays below 7e-4, on high-contrast random columns below 0.15 at
+// |F| ~ 0.6); smaller values and every bracket end point are re-evaluated
+// in FP64.
+constexpr float kScanTrust32 = 0.05f;
+
+template <class LayerF>
+__device__ __forceinline__ float dltar4_f32(LayerF layerf, int mmax, float wvno, float omega)
+{
+    if (omega < 1.0e-4f) omega = 1.0e-4f;
+    const float wvno2 = wvno * wvno;
+    const float iom = 1.0f / omega;
+    const float tio2 = 2.0f * iom * iom;
+    float4 L = layerf(mmax - 1);
+    float xka = omega / L.y, xkb = omega / L.z;
+    float ra = sqrtf((wvno + xka) * fabsf(wvno - xka));
+    float rb = sqrtf((wvno + xkb) * fabsf(wvno - xkb));
+    float gammk = L.z * L.z * tio2;
+    float gam = gammk * wvno2;
+    float gamm1 = gam - 1.0f;
+    float rho1 = L.w;
+    float e0 = rho1 * rho1 * (gamm1 * gamm1 - gam * gammk * ra * rb);
+    float e1 = -rho1 * ra;
+    float e2 = rho1 * (gamm1 - gammk * ra * rb);
+    float e3 = rho1 * rb;
+    float e4 = wvno2 - ra * rb;
+#pragma unroll 1
+    for (int m = mmax - 2; m >= 0; --m) {
+        L = layerf(m);
+        const float dpth = L.x;
+        xka = omega / L.y; xkb = omega / L.z;
+        gammk = L.z * L.z * tio2;
+        gam = gammk * wvno2;
+        const float pa = (wvno + xka) * fabsf(wvno - xka);
+        const float pb = (wvno + xkb) * fabsf(wvno - xkb);
+        const float ira = rsqrtf(pa), irb = rsqrtf(pb);
+        ra = pa * ira; rb = pb * irb;
+        const float p = ra * dpth, q = rb * dpth;
+        float w, x, cosp, y, z, cosq, ep = 1.0f, eq = 1.0f;
+        bool evp = false, evq = false;
+        if (wvno < xka) {
+            float sp, cp;
+            sincosf(p, &sp, &cp);
+            w = sp * ira; x = -ra * sp; cosp = cp;
+        } else if (wvno == xka) {
+            cosp = 1.0f; w = dpth; x = 0.0f;
+        } else {
+            evp = true;
+            ep = __expf(-p);
+            const float fac = (p < 16.0f) ? ep * ep : 0.0f;
+            cosp = (1.0f + fac) * 0.5f;
+            const float sinp = (1.0f - fac) * 0.5f;
+            w = sinp * ira; x = ra * sinp;
+        }
+        if (wvno < xkb) {
+            float sq, cq;
+            sincosf(q, &sq, &cq);
+            y = sq * irb; z = -rb * sq; cosq = cq;
+        } else if (wvno == xkb) {
+            cosq = 1.0f; y = dpth; z = 0.0f;
+        } else {
+            evq = true;
+            eq = __expf(-q);
+            const float fac = (q < 16.0f) ? eq * eq : 0.0f;
+            cosq = (1.0f + fac) * 0.5f;
+            const float sinq = (1.0f - fac) * 0.5f;
+            y = sinq * irb; z = rb * sinq;
+        }
+        const float exa = (evp ? p : 0.0f) + (evq ? q : 0.0f);
+        const float a0 = (exa < 60.0f) ? ep * eq : 0.0f;
+        const float cpcq = cosp * cosq, cpy = cosp * y, cpz = cosp * z;
+        const float cqw = cosq * w, cqx = cosq * x;
+        const float xy = x * y, xz = x * z, wy = w * y, wz = w * z;
+        rho1 = L.w;
+        const float rinv = 1.0f / rho1, rho2 = rho1 * rho1, r2inv = rinv * rinv;
+        const float gamm1l = gam - 1.0f, twgm1 = gam + gamm1l, gmgmk = gam * gammk;
+        const float gmgm1 = gam * gamm1l, gm1sq = gamm1l * gamm1l;
+        const float a0pq = a0 - cpcq;
+        const float c11 = cpcq - 2.0f * gmgm1 * a0pq - gmgmk * xz - wvno2 * gm1sq * wy;
+        const float c12 = (wvno2 * cpy - cqx) * rinv;
+        const float c13 = -(twgm1 * a0pq + gammk * xz + wvno2 * gamm1l * wy) * rinv;
+        const float c14 = (cpz - wvno2 * cqw) * rinv;
+        const float c15 = -(2.0f * wvno2 * a0pq + xz + wvno2 * wvno2 * wy) * r2inv;
+        const float c21 = (gmgmk * cpz - gm1sq * cqw) * rho1;
+        const float c22 = cpcq;
+        const float c23 = gammk * cpz - gamm1l * cqw;
+        const float c24 = -wz;
+        const float c41 = (gm1sq * cpy - gmgmk * cqx) * rho1;
+        const float c42 = -xy;
+        const float c43 = gamm1l * cpy - gammk * cqx;
+        const float c51 = -(2.0f * gmgmk * gm1sq * a0pq + gmgmk * gmgmk * xz + gm1sq * gm1sq * wy) * rho2;
+        const float c53 = -(gammk * gamm1l * twgm1 * a0pq + gam * gammk * gammk * xz + gamm1l * gm1sq * wy) * rho1;
+        const float tt = -2.0f * wvno2;
+        const float c31 = tt * c53, c32 = tt * c43;
+        const float c33 = a0 + 2.0f * (cpcq - c11);
+        const float c34 = tt * c23, c35 = tt * c13;
+        const float f0 = e0 * c11 + e1 * c21 + e2 * c31 + e3 * c41 + e4 * c51;
+        const float f1 = e0 * c12 + e1 * c22 + e2 * c32 + e3 * c42 + e4 * c41;
+        const float f2 = e0 * c13 + e1 * c23 + e2 * c33 + e3 * c43 + e4 * c53;
+        const float f3 = e0 * c14 + e1 * c24 + e2 * c34 + e3 * c22 + e4 * c21;
+        const float f4 = e0 * c15 + e1 * c14 + e2 * c35 + e3 * c12 + e4 * c11;
+        float t1 = fmaxf(fmaxf(fmaxf(fabsf(f0), fabsf(f1)), fmaxf(fabsf(f2), fabsf(f3))), fabsf(f4));
+        if (!(t1 > 1.0e-30f)) t1 = 1.0f;
+        const float tinv = 1.0f / t1;
+        e0 = f0 * tinv; e1 = f1 * tinv; e2 = f2 * tinv; e3 = f3 * tinv; e4 = f4 * tinv;
+    }
+    return e0;
+}
+
 // ------------------------------------------------------------------------
 // Root search state machine.  One instance per model; `next()` consumes the
 // secular value of the last requested point and advances to the next point
 // to evaluate (or to the end of the model).
 struct RootSM {
-    enum Phase : int { START = 0, GS_FIRST, GS_SCAN, NEV_A, NEV_B, NEV_CD, DONE };
+    enum Phase : int { START = 0, GS_FIRST, GS_SCAN, VER1, VER2, NEV_A, NEV_B, NEV_CD, DONE };
     // model constants
     double cc, cm, dc, cmax, tol;
     float betmx;
@@ -148,13 +268,18 @@ struct RootSM {
     // period state
     int phase, k, idir, nev, nctrl, mm, evals, fail_k;
     bool ifirst;
+    // FP32 coarse scan: sc32 enables it, p64 forces FP64 for the rest of the
+    // current period (after a verification mismatch), want64 is the
+    // precision of the pending request, d1x/d2x mark del1/del2 as FP64 values
+    bool sc32, p64, want64, d1x, d2x;
     double c1, c2, c3, del1, del2, del3, clow, del1st, cprev, omega;
     double ceval;   // point to evaluate next
     double x[11], y[11];
 
-    __device__ void init(double cc_, float betmx_, int kmax_, double tol_)
+    __device__ void init(double cc_, float betmx_, int kmax_, double tol_, bool scan32 = false)
     {
         cc = cc_; cm = cc_; betmx = betmx_; kmax = kmax_; tol = tol_;
+        sc32 = scan32; p64 = false; want64 = true; d1x = d2x = true;
         dc = fabs((double)0.005f);
         cmax = (double)betmx_ + dc;
         k = 0; phase = START; fail_k = -1; del1st = 0.0; cprev = 0.0; evals = 0;
@@ -173,7 +298,7 @@ struct RootSM {
             case START: {
                 if (k >= kmax) { phase = DONE; return false; }
                 omega = TWOPI / periods[k];
-                evals = 0;
+                if (!p64) evals = 0;
                 if (k == 0) { c1 = cc; clow = cc; ifirst = true; }
                 else { c1 = cprev - 1.5 * dc; clow = cm; ifirst = false; }
                 phase = GS_FIRST;
@@ -181,24 +306,41 @@ struct RootSM {
             }
             case GS_FIRST: {
                 del1 = F;
+                d1x = true;
                 if (ifirst) del1st = del1;
                 const double plmn = fsign1(del1st) * fsign1(del1);
                 idir = (ifirst || plmn >= 0.0) ? +1 : -1;
                 return scan_next();
             }
             case GS_SCAN: {
+                // an FP32 value near zero is re-evaluated in FP64
+                if (!want64 && fabs(F) < (double)kScanTrust32) return request(c2);
                 del2 = F;
+                d2x = want64;
                 if (fsign1(del1) != fsign1(del2)) {
-                    // bracketed: nevill() starts with one halving
-                    nev = 1; nctrl = 1; mm = 1;
-                    c3 = 0.5 * (c1 + c2);
-                    phase = NEV_A;
-                    return request(c3);
+                    // bracketed: both end values in FP64 before nevill()
+                    if (!d1x) { phase = VER1; return request(c1); }
+                    if (!d2x) { phase = VER2; return request(c2); }
+                    return begin_nevill();
                 }
                 c1 = c2;
                 del1 = del2;
+                d1x = d2x;
                 if (c1 < cm || c1 >= cmax) { fail(); return false; }
                 return scan_next();
+            }
+            case VER1: {
+                if (fsign1(F) != fsign1(del1)) { restart_fp64(); continue; }
+                del1 = F;
+                d1x = true;
+                if (!d2x) { phase = VER2; return request(c2); }
+                return begin_nevill();
+            }
+            case VER2: {
+                if (fsign1(F) != fsign1(del2)) { restart_fp64(); continue; }
+                del2 = F;
+                d2x = true;
+                return begin_nevill();
             }
             case NEV_A:
             case NEV_CD: {
@@ -234,8 +376,36 @@ struct RootSM {
     __device__ bool request(double c)
     {
         ceval = c;
+        want64 = true;
         ++evals;
         return true;
+    }
+
+    // a scan point: FP32 unless disabled or the period was restarted
+    __device__ bool request_scan(double c)
+    {
+        ceval = c;
+        want64 = !(sc32 && !p64);
+        ++evals;
+        return true;
+    }
+
+    __device__ bool begin_nevill()
+    {
+        // nevill() starts with one halving
+        nev = 1; nctrl = 1; mm = 1;
+        c3 = 0.5 * (c1 + c2);
+        phase = NEV_A;
+        return request(c3);
+    }
+
+    // An FP32 sign disagreed with FP64 at a verified point: run the period
+    // again from its start with every evaluation in FP64 (the reference's
+    // sequence of points, hence its root).
+    __device__ void restart_fp64()
+    {
+        p64 = true;
+        phase = START;
     }
 
     __device__ bool scan_next()
@@ -246,7 +416,7 @@ struct RootSM {
             break;
         }
         phase = GS_SCAN;
-        return request(c2);
+        return request_scan(c2);
     }
 
     __device__ void fail()
@@ -271,6 +441,7 @@ struct RootSM {
         out(k, c3, ct, evals);
         cprev = c3;
         ++k;
+        p64 = false;
         phase = START;
         return true;
     }
@@ -346,15 +517,20 @@ __device__ void scan_start(LayerF layerf, int mmax, double& cc, float& betmx)
 template <class M, class Out>
 __device__ int solve_model_warp(bool active, const M& mdl, int mmax, double cc, float betmx,
                                 const double* periods, int kmax, double tol, Out& out,
-                                int* total_evals = nullptr)
+                                int* total_evals = nullptr, bool scan32 = false)
 {
     RootSM sm;
-    sm.init(cc, betmx, kmax, tol);
+    sm.init(cc, betmx, kmax, tol, M::kF32 && scan32);
     bool want = active ? sm.next(0.0, periods, out) : false;
     int tot = want ? 1 : 0;
     while (__any_sync(0xffffffffu, want)) {
         double F = 0.0;
-        if (want) F = dltar4(mdl, mmax, sm.omega / sm.ceval, sm.omega);
+        if constexpr (M::kF32) {
+            if (want && !sm.want64)
+                F = (double)dltar4_f32([&](int m) { return mdl.layerf(m); }, mmax,
+                                       (float)(sm.omega / sm.ceval), (float)sm.omega);
+        }
+        if (want && sm.want64) F = dltar4(mdl, mmax, sm.omega / sm.ceval, sm.omega);
         if (want) {
             want = sm.next(F, periods, out);
             tot += want ? 1 : 0;

@@ -24,12 +24,14 @@ namespace dk {
 
 // Base model staged in shared memory.
 struct SharedModel {
+    static constexpr bool kF32 = false;
     const LayerD* ld;
     __device__ __forceinline__ LayerD layer(int m) const { return ld[m]; }
 };
 
 // Perturbed model: shared base stack plus the recomputed affected layers.
 struct PerturbedModel {
+    static constexpr bool kF32 = false;
     const float4* lay;
     const LayerD* ld;
     const Geometry* g;
@@ -235,9 +237,12 @@ fd_batch_kernel(FdArgs a, FdBatch b)
 // and the FP64 roots the adjoint form differentiates).  A warp is one tile of
 // the layer tables, so its 32 columns read each layer with coalesced loads.
 struct TableModel {
+    static constexpr bool kF32 = true;
     const LayerD* ld;
+    const float4* flat;
     long long base;
     __device__ __forceinline__ LayerD layer(int m) const { return ld[base + (long long)m * TILE]; }
+    __device__ __forceinline__ float4 layerf(int m) const { return flat[base + (long long)m * TILE]; }
 };
 
 // Minimum resident blocks per SM the register allocation aims for.
@@ -255,7 +260,7 @@ root_kernel(RootArgs a)
     const ColMeta M = T.meta[ss];
     const long long base = T.tile_lbase[ss / TILE] + (ss % TILE);
     const double* per = a.periods + M.per_b;
-    TableModel mdl{T.ld, base};
+    TableModel mdl{T.ld, T.flat, base};
     auto out = [&](int k, double cval, double ctight, int ev) {
         a.pv[M.pv_b + T.pv_sk * k] = (double)(float)cval;
         if (a.croot) a.croot[M.cr_b + (long long)TILE * k] = ctight;
@@ -267,7 +272,8 @@ root_kernel(RootArgs a)
         scan_start([&](int m) { return lf[(long long)m * TILE]; }, M.rmax, cc, betmx);
     }
     int nev = 0;
-    const int fk = solve_model_warp(active, mdl, M.rmax, cc, betmx, per, M.K, a.tol, out, &nev);
+    const int fk = solve_model_warp(active, mdl, M.rmax, cc, betmx, per, M.K, a.tol, out, &nev,
+                                    a.scan32 != 0);
     if (active && a.status) a.status[M.status_i] = fk < 0 ? 0 : fk + 1;
     if (a.nevals) {
         const unsigned long long w = __reduce_add_sync(0xffffffffu, (unsigned)nev);

@@ -23,7 +23,8 @@ import numpy as np
 
 from . import _lib
 
-BACKENDS = {"b200": _lib.FORM_PLAIN, "b200_adjoint": _lib.FORM_ADJOINT}
+BACKENDS = {"b200": _lib.FORM_PLAIN, "b200_adjoint": _lib.FORM_ADJOINT,
+            "b200_adjoint_fp64scan": _lib.FORM_ADJOINT | _lib.FORM_SCAN_FP64}
 ENV_ISO = "DAZI_DEPTHKERNEL_BACKEND"
 ENV_TI = "DAZI_DEPTHKERNEL_TI_BACKEND"
 

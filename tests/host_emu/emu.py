@@ -1,4 +1,4 @@
-"""Loader of the host build of the library's Gc/Gs device code (test
+"""Loader of the host build of the library's device code (test
 infrastructure: checks the device arithmetic against the oracle on CPU)."""
 import ctypes
 import os
@@ -14,7 +14,7 @@ def lib():
     global _lib
     if _lib is None:
         subprocess.run(["make", "-s", "-C", HERE], check=True)
-        _lib = ctypes.CDLL(os.path.join(HERE, "_build", "libemu_ti.so"))
+        _lib = ctypes.CDLL(os.path.join(HERE, "_build", "libemu.so"))
     return _lib
 
 
@@ -36,3 +36,21 @@ def ti_batch(node_off, depz, vs, per_off, periods, minthk, pv):
                             P(np.ascontiguousarray(pv, np.float64), f64), P(ls_off, i64),
                             P(ls, f32))
     return rc, ls, ls_off
+
+
+def root_batch(node_off, depz, vs, per_off, periods, minthk, scan32=True):
+    """pv (sngl(c) as the library writes it), status and the number of
+    secular evaluations of the root search of a ragged batch."""
+    P = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))  # noqa: E731
+    node_off = np.ascontiguousarray(node_off, np.int64)
+    per_off = np.ascontiguousarray(per_off, np.int64)
+    pv = np.zeros(max(int(per_off[-1]), 1))
+    st = np.zeros(max(node_off.size - 1, 1), np.int32)
+    ev = ctypes.c_longlong(0)
+    i64, f32, f64 = ctypes.c_longlong, ctypes.c_float, ctypes.c_double
+    rc = lib().emu_root_batch(i64(node_off.size - 1), P(node_off, i64),
+                              P(np.ascontiguousarray(depz, np.float32), f32),
+                              P(np.ascontiguousarray(vs, np.float32), f32), P(per_off, i64),
+                              P(np.ascontiguousarray(periods, np.float64), f64), f32(minthk),
+                              int(scan32), P(pv, f64), P(st, ctypes.c_int), ctypes.byref(ev))
+    return rc, pv, st, ev.value

@@ -39,6 +39,11 @@ static inline double __dsub_rn(double a, double b) { return a - b; }
 static inline double __ddiv_rn(double a, double b) { return a / b; }
 static inline double __dsqrt_rn(double a) { return std::sqrt(a); }
 static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
+static inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
+static inline void __syncthreads() {}
+// CUDA's fast single-precision exponential (device approximation); the host
+// build uses the libm function (one translation unit includes this file)
+extern "C" float __expf(float x) noexcept { return expf(x); }
 struct EmuDim { unsigned x = 0, y = 0, z = 0; };
 static EmuDim threadIdx, blockIdx, blockDim, gridDim;
 static inline unsigned atomicAdd(unsigned* p, unsigned v) { unsigned o = *p; *p += v; return o; }

@@ -1,0 +1,136 @@
+// TEST INFRASTRUCTURE ONLY: the table build (k_prep.cu), the root search
+// (root_kernel, k_plain.cu) and the Gc/Gs sweep (k_ti.cu) of the library
+// compiled as host code and driven in the order the library drives them
+// (build_tables, run_tables in csrc/capi.cu: columns sorted by (refined
+// layers, periods), 32-column tiles, one task per (tile, period), one lane
+// per column; one root-search thread per column).  Used by the
+// tests/test_host_emu_*.py suites to check the device arithmetic against
+// the oracle on the CPU; the shipped library never uses it.
+#include "emu_shim.h"
+#include <numeric>
+#include <vector>
+namespace dk { alignas(16) unsigned char smem_raw[1 << 16]; }
+#include "../../dazi_current_release_b200/csrc/k_prep.cu"
+#include "../../dazi_current_release_b200/csrc/k_plain.cu"
+#include "../../dazi_current_release_b200/csrc/k_ti.cu"
+using namespace dk;
+
+namespace {
+
+struct HostTables {
+    std::vector<int> sorted;
+    std::vector<long long> lbase, tbase;
+    std::vector<int2> tasks;
+    std::vector<float4> flat;
+    std::vector<LayerD> ld;
+    std::vector<TiRec> ti;
+    std::vector<SpRec> sp;
+    std::vector<ChainRec> ch;
+    std::vector<ColMeta> meta;
+    Tables T;
+    int maxr = 1;
+};
+
+// build_tables (capi.cu) on the host.  Returns false for an invalid column.
+bool build_host(const ColSrc& src, long long ncols, const PrepOut& po, HostTables& H)
+{
+    std::vector<unsigned> keys(ncols);
+    std::vector<int> colidx(ncols), rmax(ncols);
+    int err = 0;
+    for (long long c = 0; c < ncols; ++c) prep_count_one(src, c, keys.data(), colidx.data(), rmax.data(), &err);
+    if (err) return false;
+    // stable descending order, as the library's radix sort of the keys
+    H.sorted.resize(ncols);
+    std::iota(H.sorted.begin(), H.sorted.end(), 0);
+    std::stable_sort(H.sorted.begin(), H.sorted.end(), [&](int a, int b) { return keys[a] > keys[b]; });
+    const long long ntiles = (ncols + TILE - 1) / TILE;
+    H.lbase.resize(ntiles); H.tbase.resize(ntiles);
+    std::vector<long long> trec(ntiles), ttask(ntiles);
+    for (long long t = 0; t < ntiles; ++t) {
+        int rm = 0, km = 0;
+        for (int l = 0; l < TILE && t * TILE + l < ncols; ++l) {
+            const int c = H.sorted[t * TILE + l];
+            rm = std::max(rm, rmax[c]);
+            km = std::max(km, src.col_K(c));
+        }
+        trec[t] = (long long)rm * TILE;
+        ttask[t] = km;
+        H.maxr = std::max(H.maxr, rm);
+    }
+    long long nrec = 0, ntask = 0;
+    for (long long t = 0; t < ntiles; ++t) {
+        H.lbase[t] = nrec; nrec += trec[t];
+        H.tbase[t] = ntask; ntask += ttask[t];
+    }
+    H.tasks.resize(ntask);
+    for (long long t = 0; t < ntiles; ++t)
+        for (long long k = 0; k < ttask[t]; ++k) H.tasks[H.tbase[t] + k] = make_int2((int)t, (int)k);
+    H.flat.resize(nrec); H.ld.resize(nrec); H.ti.resize(nrec); H.sp.resize(nrec); H.ch.resize(nrec);
+    H.meta.resize(ncols);
+    Tables& T = H.T;
+    T.flat = H.flat.data(); T.ld = H.ld.data(); T.ti = H.ti.data(); T.sp = H.sp.data(); T.ch = H.ch.data();
+    T.meta = H.meta.data(); T.tile_lbase = H.lbase.data(); T.tasks = H.tasks.data();
+    T.ntasks = ntask; T.ncols = ncols; T.pv_sk = 1; T.sen_sk = 1; T.ls_sk = 1;
+    for (long long s = 0; s < ncols; ++s) prep_build_one(src, po, T, H.sorted.data(), H.tbase.data(), s);
+    return true;
+}
+
+ColSrc ragged_src(const long long* node_off, const float* depz, const float* vs,
+                  const long long* per_off, float minthk)
+{
+    ColSrc src;
+    src.ragged = true; src.ncol = 0; src.col0 = 0;
+    src.vel = vs; src.vp = nullptr; src.rho = nullptr; src.depz = depz;
+    src.node_off = node_off; src.per_off = per_off; src.nz = 0; src.K = 0; src.minthk = minthk;
+    return src;
+}
+
+}  // namespace
+
+// Root search of a ragged batch (root_kernel, one thread per sorted
+// column): pv[per_off[c] + k] (sngl(c), as the library writes it), status
+// per column, the secular evaluations in *evals.  scan32 selects the FP32
+// coarse scan.
+extern "C" int emu_root_batch(long long ncols, const long long* node_off, const float* depz,
+                              const float* vs, const long long* per_off, const double* periods,
+                              float minthk, int scan32, double* pv, int* status, long long* evals)
+{
+    const ColSrc src = ragged_src(node_off, depz, vs, per_off, minthk);
+    HostTables H;
+    PrepOut po{nullptr, nullptr, nullptr};
+    if (!build_host(src, ncols, po, H)) return -1;
+    unsigned long long counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    RootArgs a;
+    a.T = H.T; a.periods = periods; a.tol = 1.0e-6; a.pv = pv; a.croot = nullptr;
+    a.status = status; a.nevals = counters; a.scan32 = scan32;
+    blockDim.x = 128;
+    for (long long s = 0; s < ncols; ++s) {
+        blockIdx.x = (unsigned)(s / 128);
+        threadIdx.x = (unsigned)(s % 128);
+        root_kernel(a);
+    }
+    *evals = (long long)counters[0];
+    return 0;
+}
+
+// Ragged batch (CSR layout of dazi_dk_batch) with given phase velocities pv;
+// writes lsen in the batch layout.  Returns 0, -1 for an invalid column,
+// -2 for a non-finite Lsen value.
+extern "C" int emu_ti_batch(long long ncols, const long long* node_off, const float* depz,
+                            const float* vs, const long long* per_off, const double* periods,
+                            float minthk, const double* pv, const long long* ls_off, float* lsen)
+{
+    const ColSrc src = ragged_src(node_off, depz, vs, per_off, minthk);
+    HostTables H;
+    PrepOut po{nullptr, ls_off, nullptr};
+    if (!build_host(src, ncols, po, H)) return -1;
+    std::vector<double> scratch((size_t)H.maxr * TI_SCR_Q * TILE);
+    unsigned queue = 0;
+    int errflag = 0;
+    TiArgs a;
+    a.T = H.T; a.periods = periods; a.pv = pv; a.lsen = lsen; a.scratch = scratch.data();
+    a.scr_layers = H.maxr; a.queue = &queue; a.errflag = &errflag;
+    for (long long task = 0; task < H.T.ntasks; ++task)
+        for (int lane = 0; lane < TILE; ++lane) ti_task(a, task, lane, scratch.data() + lane);
+    return errflag ? -2 : 0;
+}
