@@ -384,13 +384,13 @@ def main_ragged(args, ws, rank, local):
     torch.cuda.synchronize(dev)
     step_fn(form, ncol)()
     phases = _lib.last_timing()
-    scan64 = None
+    scan32 = None
     if form == _lib.FORM_ADJOINT:
-        pv32 = pv.clone()
-        step_fn(form | _lib.FORM_SCAN_FP64, ncol)()
-        ph64 = _lib.last_timing()
-        scan64 = {"root_ms_fp32_scan": phases.get("root"), "root_ms_fp64_scan": ph64.get("root"),
-                  "identical_roots": bool(torch.equal(pv32, pv))}
+        pv64 = pv.clone()
+        step_fn(form | _lib.FORM_SCAN_FP32, ncol)()
+        ph32 = _lib.last_timing()
+        scan32 = {"root_ms_fp64_scan": phases.get("root"), "root_ms_fp32_scan": ph32.get("root"),
+                  "identical_roots": bool(torch.equal(pv64, pv))}
     _lib.check(L.dazi_dk_set_timing(0))
 
     # end to end: host C-ABI dazi_dk_batch with pinned host buffers
@@ -479,8 +479,8 @@ def main_ragged(args, ws, rank, local):
         "roofline": roof,
         "gpu_launches": args.steps * launches,
     }
-    if scan64:
-        line["root_scan"] = scan64
+    if scan32:
+        line["root_scan"] = scan32
     if sample:
         line["same_columns"] = dict(sample, columns=ns, column_periods=ns_cp,
                                     adjoint_over_plain=sample["adjoint"]["value"] /

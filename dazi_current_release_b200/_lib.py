@@ -26,7 +26,7 @@ DAZI_ERR_NODEVICE = -6
 DAZI_ERR_MODEL = -7
 FORM_PLAIN = 0
 FORM_ADJOINT = 1
-FORM_SCAN_FP64 = 2      # flag: all root-search evaluations in FP64 (default: FP32 scan)
+FORM_SCAN_FP32 = 2      # flag: FP32 coarse scan verified in FP64 (default: all FP64)
 
 # every symbol include/dazi_dk.h declares
 EXPORTS = (

@@ -101,7 +101,7 @@ std::mutex g_mu;
 
 bool valid_form(int form)
 {
-    const int f = form & ~DAZI_FORM_SCAN_FP64;
+    const int f = form & ~DAZI_FORM_SCAN_FP32;
     return f == DAZI_FORM_PLAIN || f == DAZI_FORM_ADJOINT;
 }
 
@@ -316,7 +316,7 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
         RootArgs a;
         a.T = T; a.periods = per; a.tol = 1.0e-6;   // surfdisp96.f:608
         a.pv = o.pv; a.croot = nullptr; a.status = o.status; a.nevals = nevals;
-        a.scan32 = (form & DAZI_FORM_SCAN_FP64) ? 0 : 1;
+        a.scan32 = (form & DAZI_FORM_SCAN_FP32) ? 1 : 0;
         if (adj) {
             if ((r = g_ctx.croot.ensure(sizeof(double) * TILE * (size_t)T.ntasks))) return r;
             a.croot = g_ctx.croot.as<double>();

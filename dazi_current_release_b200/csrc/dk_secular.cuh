@@ -6,12 +6,16 @@
 //   nevill + half (refine)        surfdisp96.f:551-680
 //   surfdisp96 period loop        surfdisp96.f:52-354 (Rayleigh, phase, mode 1)
 //
-// Optional FP32 coarse scan (root search of the adjoint form): the getsol
+// Optional FP32 coarse scan (DAZI_FORM_SCAN_FP32): the getsol
 // scan steps evaluate the secular function in FP32 and use only its sign;
 // values below kScanTrust32 are re-evaluated in FP64, and both ends of a
 // detected bracket are evaluated in FP64 before nevill() (whose steps are
 // FP64), so the values nevill() sees are the reference's.  A bracket end
 // whose FP64 sign contradicts its FP32 sign restarts the period in FP64.
+// A warp step runs in FP32 only when all its waiting lanes scan.  The root
+// search is latency-bound (each lane a chain of dependent operations), so
+// FP32 evaluations are not much cheaper than FP64 ones here: the scan runs
+// in FP64 unless this flag asks otherwise.
 //
 // The layer chain is a sequential product of 5x5 Dunkin compound matrices,
 // one model per thread; the tensor cores have no role here.  The root search
@@ -149,7 +153,8 @@ __device__ __forceinline__ double dltar4(const M& mdl, int mmax, double wvno, do
 // normalised scale of F, |F| <= 1; the FP32 error measured on the uneven
 // batch stays below 7e-4, on high-contrast random columns below 0.15 at
 // |F| ~ 0.6); smaller values and every bracket end point are re-evaluated
-// in FP64.
+// in FP64.  The fast intrinsics (__sincosf, __expf, __fdividef) are enough
+// for a sign that is verified.
 constexpr float kScanTrust32 = 0.05f;
 
 template <class LayerF>
@@ -160,7 +165,7 @@ __device__ __forceinline__ float dltar4_f32(LayerF layerf, int mmax, float wvno,
     const float iom = 1.0f / omega;
     const float tio2 = 2.0f * iom * iom;
     float4 L = layerf(mmax - 1);
-    float xka = omega / L.y, xkb = omega / L.z;
+    float xka = __fdividef(omega, L.y), xkb = __fdividef(omega, L.z);
     float ra = sqrtf((wvno + xka) * fabsf(wvno - xka));
     float rb = sqrtf((wvno + xkb) * fabsf(wvno - xkb));
     float gammk = L.z * L.z * tio2;
@@ -176,7 +181,7 @@ __device__ __forceinline__ float dltar4_f32(LayerF layerf, int mmax, float wvno,
     for (int m = mmax - 2; m >= 0; --m) {
         L = layerf(m);
         const float dpth = L.x;
-        xka = omega / L.y; xkb = omega / L.z;
+        xka = __fdividef(omega, L.y); xkb = __fdividef(omega, L.z);
         gammk = L.z * L.z * tio2;
         gam = gammk * wvno2;
         const float pa = (wvno + xka) * fabsf(wvno - xka);
@@ -188,7 +193,7 @@ __device__ __forceinline__ float dltar4_f32(LayerF layerf, int mmax, float wvno,
         bool evp = false, evq = false;
         if (wvno < xka) {
             float sp, cp;
-            sincosf(p, &sp, &cp);
+            __sincosf(p, &sp, &cp);
             w = sp * ira; x = -ra * sp; cosp = cp;
         } else if (wvno == xka) {
             cosp = 1.0f; w = dpth; x = 0.0f;
@@ -202,7 +207,7 @@ __device__ __forceinline__ float dltar4_f32(LayerF layerf, int mmax, float wvno,
         }
         if (wvno < xkb) {
             float sq, cq;
-            sincosf(q, &sq, &cq);
+            __sincosf(q, &sq, &cq);
             y = sq * irb; z = -rb * sq; cosq = cq;
         } else if (wvno == xkb) {
             cosq = 1.0f; y = dpth; z = 0.0f;
@@ -220,7 +225,7 @@ __device__ __forceinline__ float dltar4_f32(LayerF layerf, int mmax, float wvno,
         const float cqw = cosq * w, cqx = cosq * x;
         const float xy = x * y, xz = x * z, wy = w * y, wz = w * z;
         rho1 = L.w;
-        const float rinv = 1.0f / rho1, rho2 = rho1 * rho1, r2inv = rinv * rinv;
+        const float rinv = __fdividef(1.0f, rho1), rho2 = rho1 * rho1, r2inv = rinv * rinv;
         const float gamm1l = gam - 1.0f, twgm1 = gam + gamm1l, gmgmk = gam * gammk;
         const float gmgm1 = gam * gamm1l, gm1sq = gamm1l * gamm1l;
         const float a0pq = a0 - cpcq;
@@ -249,7 +254,7 @@ __device__ __forceinline__ float dltar4_f32(LayerF layerf, int mmax, float wvno,
         const float f4 = e0 * c15 + e1 * c14 + e2 * c35 + e3 * c12 + e4 * c11;
         float t1 = fmaxf(fmaxf(fmaxf(fabsf(f0), fabsf(f1)), fmaxf(fabsf(f2), fabsf(f3))), fabsf(f4));
         if (!(t1 > 1.0e-30f)) t1 = 1.0f;
-        const float tinv = 1.0f / t1;
+        const float tinv = __fdividef(1.0f, t1);
         e0 = f0 * tinv; e1 = f1 * tinv; e2 = f2 * tinv; e3 = f3 * tinv; e4 = f4 * tinv;
     }
     return e0;
@@ -525,12 +530,20 @@ __device__ int solve_model_warp(bool active, const M& mdl, int mmax, double cc, 
     int tot = want ? 1 : 0;
     while (__any_sync(0xffffffffu, want)) {
         double F = 0.0;
+        // one precision per warp step: FP32 only when every waiting lane is
+        // on an FP32 scan step; otherwise all evaluate in FP64 (a scan lane
+        // then receives an exact value)
+        bool step32 = false;
+        if constexpr (M::kF32) step32 = !__any_sync(0xffffffffu, want && sm.want64);
         if constexpr (M::kF32) {
-            if (want && !sm.want64)
+            if (want && step32)
                 F = (double)dltar4_f32([&](int m) { return mdl.layerf(m); }, mmax,
                                        (float)(sm.omega / sm.ceval), (float)sm.omega);
         }
-        if (want && sm.want64) F = dltar4(mdl, mmax, sm.omega / sm.ceval, sm.omega);
+        if (want && !step32) {
+            F = dltar4(mdl, mmax, sm.omega / sm.ceval, sm.omega);
+            sm.want64 = true;
+        }
         if (want) {
             want = sm.next(F, periods, out);
             tot += want ? 1 : 0;

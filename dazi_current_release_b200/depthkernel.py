@@ -24,7 +24,7 @@ import numpy as np
 from . import _lib
 
 BACKENDS = {"b200": _lib.FORM_PLAIN, "b200_adjoint": _lib.FORM_ADJOINT,
-            "b200_adjoint_fp64scan": _lib.FORM_ADJOINT | _lib.FORM_SCAN_FP64}
+            "b200_adjoint_fp32scan": _lib.FORM_ADJOINT | _lib.FORM_SCAN_FP32}
 ENV_ISO = "DAZI_DEPTHKERNEL_BACKEND"
 ENV_TI = "DAZI_DEPTHKERNEL_TI_BACKEND"
 

@@ -52,11 +52,12 @@ extern "C" {
 /* form selector */
 #define DAZI_FORM_PLAIN    0   /* perturb-and-recompute, as the reference */
 #define DAZI_FORM_ADJOINT  1   /* implicit differentiation of the root     */
-/* flag, OR-ed into the form: every root-search evaluation in FP64.  By
- * default the root search of the adjoint form (and of the Lsen-only entry)
- * scans in FP32 and verifies in FP64 (same roots); the plain form always
- * evaluates in FP64. */
-#define DAZI_FORM_SCAN_FP64 2
+/* flag, OR-ed into the form: the root search of the adjoint form (and of
+ * the Lsen-only entry) scans for the bracket with the secular function in
+ * FP32, re-evaluating near-zero values and both bracket ends in FP64 (same
+ * roots as the default all-FP64 search).  The plain form always evaluates
+ * in FP64. */
+#define DAZI_FORM_SCAN_FP32 2
 
 /* Replaces depthkernel() of code/src_inv_iso_joint/CalSurfG.f90:1-15
  * (default_fortran_fd backend, CalSurfG.f90:86-107), for the 1-based column

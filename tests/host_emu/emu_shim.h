@@ -44,6 +44,8 @@ static inline void __syncthreads() {}
 // CUDA's fast single-precision exponential (device approximation); the host
 // build uses the libm function (one translation unit includes this file)
 extern "C" float __expf(float x) noexcept { return expf(x); }
+extern "C" float __fdividef(float a, float b) noexcept { return a / b; }
+extern "C" void __sincosf(float x, float* s, float* c) noexcept { sincosf(x, s, c); }
 struct EmuDim { unsigned x = 0, y = 0, z = 0; };
 static EmuDim threadIdx, blockIdx, blockDim, gridDim;
 static inline unsigned atomicAdd(unsigned* p, unsigned v) { unsigned o = *p; *p += v; return o; }

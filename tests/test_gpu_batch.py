@@ -7,6 +7,7 @@ from conftest import assert_pv_parity, rel_l2
 import dazi_current_release_b200 as dk
 from dazi_current_release_b200 import synthetic as S
 from dazi_current_release_b200.batch import depthkernel_batch
+from dazi_current_release_b200 import _lib as dk_lib
 
 pytestmark = pytest.mark.gpu
 
@@ -86,3 +87,15 @@ def test_grid_and_batch_agree(small_batch):
         np.testing.assert_array_equal(p, pv[c])
         np.testing.assert_array_equal(a, svs[c])
         np.testing.assert_array_equal(l, ls[c])
+
+
+def test_fp32_scan_gives_identical_roots(small_batch):
+    """DAZI_FORM_SCAN_FP32: the bracket scan in FP32 with FP64 verification
+    finds the same roots, statuses and kernels as the all-FP64 search."""
+    b = S.config3(realisations=1, columns=600, base_seed=1003)
+    r64 = depthkernel_batch(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk,
+                            form=dk.FORM_ADJOINT)
+    r32 = depthkernel_batch(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk,
+                            form=dk.FORM_ADJOINT | dk_lib.FORM_SCAN_FP32)
+    for k in ("pv", "status", "sen_vs", "sen_vp", "sen_rho", "lsen"):
+        np.testing.assert_array_equal(r32[k], r64[k], err_msg=k)
