@@ -16,9 +16,11 @@ ragged batch entries dazi_dk_batch_dev / dazi_dk_batch.  The grid workloads
 dazi_dk_fused_dev / dazi_dk_fused.
 
 value      device-timed throughput of the chosen form (--form, default the
-           adjoint form) on the whole batch, inputs resident in HBM (device
-           entry on torch's stream, CUDA events per step, L2 flushed between
-           steps outside the timed events)
+           adjoint form) on the whole batch, inputs resident in HBM: a plan
+           (dazi_dk_plan_*: structure bound once, kernel variants autotuned,
+           each step one CUDA-graph launch) on torch's stream, CUDA events per
+           step, L2 flushed between steps outside the timed events; the
+           per-call entry dazi_dk_batch_dev is timed beside it (per_call)
 same_columns  both forms timed the same way on the first --plain-cols
            columns (the plain perturb-and-recompute form runs 1 + 6 nz root
            searches per column and would take minutes on the whole batch)
@@ -371,11 +373,34 @@ def main_ragged(args, ws, rank, local):
             ms = _events_timed(step_fn(f, ns), 1 if f == _lib.FORM_PLAIN else 2, 1, dev, stream,
                                flush, ws)
             sample[fname] = {"value": ws * ns_cp / (ms * 1e-3), "ms_per_step": ms}
-    with ClockSampler(local) as clk:
-        ms_per_step = _events_timed(step_fn(form, ncol), args.steps, args.warmup, dev, stream,
-                                    flush, ws)
-    launches = L.dazi_dk_last_launches()
+    # per-call entry (tables rebuilt, one small host sync per call)
+    call_ms = _events_timed(step_fn(form, ncol), max(2, args.steps // 2), 1, dev, stream, flush,
+                            ws)
+    launches_call = L.dazi_dk_last_launches()
     evals, layer_evals, layer_items = work()
+    # plan: structure bound once, kernel variants autotuned on this batch,
+    # every step one CUDA-graph launch (layer values from the current
+    # velocities, root search, adjoint and Gc/Gs sweeps)
+    graph_info = None
+    if form & 1:
+        from dazi_current_release_b200.plan import BatchPlan
+        t0 = time.perf_counter()
+        plan = BatchPlan(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk, tune=True,
+                         scan32=bool(form & _lib.FORM_SCAN_FP32), device=dev)
+        plan_setup_s = time.perf_counter() - t0
+        with ClockSampler(local) as clk:
+            ms_per_step = _events_timed(plan.run, args.steps, args.warmup, dev, stream, flush, ws)
+        plan.status_check()
+        graph_info = {"autotuned": plan.config(), "setup_s": plan_setup_s,
+                      "same_roots_as_per_call": bool(torch.equal(plan.pv, pv))
+                      and bool(torch.equal(plan.status, status))}
+        plan.close()
+        launches = 4   # graph kernels per run: table values, root, adjoint, Gc/Gs
+    else:
+        with ClockSampler(local) as clk:
+            ms_per_step = _events_timed(step_fn(form, ncol), args.steps, args.warmup, dev,
+                                        stream, flush, ws)
+        launches = L.dazi_dk_last_launches()
     value = ws * ncp / (ms_per_step * 1e-3)
 
     # per-phase device times of one more step (events inside the library),
@@ -478,6 +503,9 @@ def main_ragged(args, ws, rank, local):
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
         "roofline": roof,
         "gpu_launches": args.steps * launches,
+        "graph": graph_info,
+        "per_call": {"value": ws * ncp / (call_ms * 1e-3), "ms_per_step": call_ms,
+                     "launches_per_call": launches_call},
     }
     if scan32:
         line["root_scan"] = scan32

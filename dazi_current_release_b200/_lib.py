@@ -34,7 +34,8 @@ EXPORTS = (
     "dazi_dk_last_error", "dazi_dk_version", "dazi_dk_finalize", "dazi_dk_fp64_peak", "dazi_dk_last_work",
     "dazi_dk_ti", "dazi_dk_fused", "dazi_dk_fused_dev", "dazi_dk_last_launches",
     "dazi_dk_iso_noalloc_dev", "dazi_dk_batch", "dazi_dk_batch_dev", "dazi_dk_set_timing",
-    "dazi_dk_last_timing", "dazi_dk_last_items",
+    "dazi_dk_last_timing", "dazi_dk_last_items", "dazi_dk_plan_create", "dazi_dk_plan_launch",
+    "dazi_dk_plan_status", "dazi_dk_plan_config", "dazi_dk_plan_destroy",
 )
 
 
@@ -107,6 +108,17 @@ def load(build_if_missing: bool = True):
     L.dazi_dk_last_work.restype = _int
     L.dazi_dk_last_items.argtypes = [ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_longlong)]
     L.dazi_dk_last_items.restype = _int
+    L.dazi_dk_plan_create.argtypes = ([ll] + [vp_] * 7 + [ctypes.c_float] + [vp_] * 7 +
+                                      [_int, vp_, _int, vp_, ctypes.POINTER(ctypes.c_void_p)])
+    L.dazi_dk_plan_create.restype = _int
+    L.dazi_dk_plan_launch.argtypes = [vp_, vp_]
+    L.dazi_dk_plan_launch.restype = _int
+    L.dazi_dk_plan_status.argtypes = [vp_]
+    L.dazi_dk_plan_status.restype = _int
+    L.dazi_dk_plan_config.argtypes = [vp_, _i32p, _i32p, _i32p, ctypes.POINTER(ctypes.c_float)]
+    L.dazi_dk_plan_config.restype = _int
+    L.dazi_dk_plan_destroy.argtypes = [vp_]
+    L.dazi_dk_plan_destroy.restype = _int
     L.dazi_dk_fp64_peak.argtypes = [_f64p]
     L.dazi_dk_fp64_peak.restype = _int
     L.dazi_dk_finalize.argtypes = []

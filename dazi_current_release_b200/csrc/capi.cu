@@ -63,6 +63,30 @@ struct DBuf {
     template <class T> T* as() const { return reinterpret_cast<T*>(p); }
 };
 
+// Device buffers of one table-driven computation: the layer tables, the
+// task list, the counters and the sweep scratch (the global entries share
+// one; every plan owns one).
+struct Work {
+    DBuf croot, counters, adjscr, tiscr;
+    DBuf keys, keys2, cidx, cidx2, rmaxb, trecs, ttasks, tlbase, ttbase, cubtmp;
+    DBuf tflat, tld, tti, tsp, tch, tmeta, ttasklist;
+    void release()
+    {
+        DBuf* all[] = {&croot, &counters, &adjscr, &tiscr, &keys, &keys2, &cidx, &cidx2, &rmaxb,
+                       &trecs, &ttasks, &tlbase, &ttbase, &cubtmp, &tflat, &tld, &tti, &tsp,
+                       &tch, &tmeta, &ttasklist};
+        for (DBuf* b : all) b->release();
+    }
+};
+
+// Kernel variants of the table-driven phases (chosen by the autotuner of a
+// plan; the global entries use the defaults).
+struct LaunchCfg {
+    int root_bt = 128;      // root_kernel threads per block: 64, 128, 256
+    int adj_minb = 3;       // adjoint_kernel blocks per SM: 2, 3, 4
+    int ti_minb = 8;        // ti_kernel blocks per SM: 4, 6, 8
+};
+
 // Optional per-phase timing with CUDA events on the call's stream.
 struct PhaseTimer {
     bool on = false;
@@ -80,10 +104,10 @@ struct Context {
     // host-entry staging
     DBuf vel, vp, rho, per, depz, pv, svs, svp, srh, status;
     // work buffers
-    DBuf geo, cscratch, croot, counters, adjscr, tiscr, lsen;
-    // per-call layer tables
-    DBuf keys, keys2, cidx, cidx2, rmaxb, trecs, ttasks, tlbase, ttbase, cubtmp;
-    DBuf tflat, tld, tti, tsp, tch, tmeta, ttasklist, cbufoff;
+    DBuf geo, cscratch, lsen;
+    // per-call layer tables, counters and sweep scratch
+    Work w;
+    DBuf cbufoff;
     // batch staging (host entry)
     DBuf bnode, bper, bdep, bvs, bvp, brho, bperiods, bsenoff, blsoff, bpv, bsvs, bsvp, bsrh, blsen, bstatus;
     int last_launches = 0;
@@ -226,48 +250,48 @@ int launch_persistent_grid(const void* fn, long long nitems, int threads, long l
 // sort the columns by (layers, periods), lay out 32-column tiles, build.
 // One host synchronisation (to size the tables).
 int build_tables(const ColSrc& src, long long ncols, const PrepOut& po, long long pv_sk,
-                 long long sen_sk, long long ls_sk, cudaStream_t st, Tables& T)
+                 long long sen_sk, long long ls_sk, cudaStream_t st, Tables& T, Work& W)
 {
     int r;
     const long long ntiles = (ncols + TILE - 1) / TILE;
-    if ((r = g_ctx.keys.ensure(sizeof(unsigned) * ncols)) || (r = g_ctx.keys2.ensure(sizeof(unsigned) * ncols)) ||
-        (r = g_ctx.cidx.ensure(sizeof(int) * ncols)) || (r = g_ctx.cidx2.ensure(sizeof(int) * ncols)) ||
-        (r = g_ctx.rmaxb.ensure(sizeof(int) * ncols + 16)) ||
-        (r = g_ctx.trecs.ensure(sizeof(long long) * ntiles)) || (r = g_ctx.ttasks.ensure(sizeof(long long) * ntiles)) ||
-        (r = g_ctx.tlbase.ensure(sizeof(long long) * ntiles)) || (r = g_ctx.ttbase.ensure(sizeof(long long) * ntiles)))
+    if ((r = W.keys.ensure(sizeof(unsigned) * ncols)) || (r = W.keys2.ensure(sizeof(unsigned) * ncols)) ||
+        (r = W.cidx.ensure(sizeof(int) * ncols)) || (r = W.cidx2.ensure(sizeof(int) * ncols)) ||
+        (r = W.rmaxb.ensure(sizeof(int) * ncols + 16)) ||
+        (r = W.trecs.ensure(sizeof(long long) * ntiles)) || (r = W.ttasks.ensure(sizeof(long long) * ntiles)) ||
+        (r = W.tlbase.ensure(sizeof(long long) * ntiles)) || (r = W.ttbase.ensure(sizeof(long long) * ntiles)))
         return r;
-    int* err = reinterpret_cast<int*>(g_ctx.rmaxb.as<char>() + sizeof(int) * ncols);
+    int* err = reinterpret_cast<int*>(W.rmaxb.as<char>() + sizeof(int) * ncols);
     CK(cudaMemsetAsync(err, 0, sizeof(int), st));
     const int bt = 128;
     const unsigned nb = (unsigned)((ncols + bt - 1) / bt);
-    prep_count_kernel<<<nb, bt, 0, st>>>(src, ncols, g_ctx.keys.as<unsigned>(), g_ctx.cidx.as<int>(),
-                                         g_ctx.rmaxb.as<int>(), err);
+    prep_count_kernel<<<nb, bt, 0, st>>>(src, ncols, W.keys.as<unsigned>(), W.cidx.as<int>(),
+                                         W.rmaxb.as<int>(), err);
     CK(cudaGetLastError());
     size_t tb1 = 0, tb2 = 0, tb3 = 0;
-    CK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb1, g_ctx.keys.as<unsigned>(), g_ctx.keys2.as<unsigned>(),
-                                                 g_ctx.cidx.as<int>(), g_ctx.cidx2.as<int>(), (int)ncols, 0, 16, st));
-    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, g_ctx.trecs.as<long long>(), g_ctx.tlbase.as<long long>(),
+    CK(cub::DeviceRadixSort::SortPairsDescending(nullptr, tb1, W.keys.as<unsigned>(), W.keys2.as<unsigned>(),
+                                                 W.cidx.as<int>(), W.cidx2.as<int>(), (int)ncols, 0, 16, st));
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb2, W.trecs.as<long long>(), W.tlbase.as<long long>(),
                                      (int)ntiles, st));
     tb3 = tb1 > tb2 ? tb1 : tb2;
-    if ((r = g_ctx.cubtmp.ensure(tb3 + 16))) return r;
-    CK(cub::DeviceRadixSort::SortPairsDescending(g_ctx.cubtmp.p, tb3, g_ctx.keys.as<unsigned>(), g_ctx.keys2.as<unsigned>(),
-                                                 g_ctx.cidx.as<int>(), g_ctx.cidx2.as<int>(), (int)ncols, 0, 16, st));
+    if ((r = W.cubtmp.ensure(tb3 + 16))) return r;
+    CK(cub::DeviceRadixSort::SortPairsDescending(W.cubtmp.p, tb3, W.keys.as<unsigned>(), W.keys2.as<unsigned>(),
+                                                 W.cidx.as<int>(), W.cidx2.as<int>(), (int)ncols, 0, 16, st));
     const unsigned ntb = (unsigned)((ntiles + bt - 1) / bt);
-    prep_tile_kernel<<<ntb, bt, 0, st>>>(ncols, g_ctx.cidx2.as<int>(), g_ctx.rmaxb.as<int>(), src,
-                                         g_ctx.trecs.as<long long>(), g_ctx.ttasks.as<long long>());
+    prep_tile_kernel<<<ntb, bt, 0, st>>>(ncols, W.cidx2.as<int>(), W.rmaxb.as<int>(), src,
+                                         W.trecs.as<long long>(), W.ttasks.as<long long>());
     CK(cudaGetLastError());
     size_t tbs = tb3;
-    CK(cub::DeviceScan::ExclusiveSum(g_ctx.cubtmp.p, tbs, g_ctx.trecs.as<long long>(), g_ctx.tlbase.as<long long>(),
+    CK(cub::DeviceScan::ExclusiveSum(W.cubtmp.p, tbs, W.trecs.as<long long>(), W.tlbase.as<long long>(),
                                      (int)ntiles, st));
     tbs = tb3;
-    CK(cub::DeviceScan::ExclusiveSum(g_ctx.cubtmp.p, tbs, g_ctx.ttasks.as<long long>(), g_ctx.ttbase.as<long long>(),
+    CK(cub::DeviceScan::ExclusiveSum(W.cubtmp.p, tbs, W.ttasks.as<long long>(), W.ttbase.as<long long>(),
                                      (int)ntiles, st));
     long long last[4] = {0, 0, 0, 0};
     int herr = 0;
-    CK(cudaMemcpyAsync(&last[0], g_ctx.tlbase.as<long long>() + ntiles - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&last[1], g_ctx.trecs.as<long long>() + ntiles - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&last[2], g_ctx.ttbase.as<long long>() + ntiles - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
-    CK(cudaMemcpyAsync(&last[3], g_ctx.ttasks.as<long long>() + ntiles - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last[0], W.tlbase.as<long long>() + ntiles - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last[1], W.trecs.as<long long>() + ntiles - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last[2], W.ttbase.as<long long>() + ntiles - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last[3], W.ttasks.as<long long>() + ntiles - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
     CK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (herr) {
@@ -277,90 +301,149 @@ int build_tables(const ColSrc& src, long long ncols, const PrepOut& po, long lon
         return (herr & (1 | 2 | 8)) ? DAZI_ERR_LIMITS : DAZI_ERR_BADARG;
     }
     const long long nrec = last[0] + last[1], ntask = last[2] + last[3];
-    if ((r = g_ctx.tflat.ensure(sizeof(float4) * nrec)) || (r = g_ctx.tld.ensure(sizeof(LayerD) * nrec)) ||
-        (r = g_ctx.tti.ensure(sizeof(TiRec) * nrec)) || (r = g_ctx.tsp.ensure(sizeof(SpRec) * nrec)) || (r = g_ctx.tch.ensure(sizeof(ChainRec) * nrec)) ||
-        (r = g_ctx.tmeta.ensure(sizeof(ColMeta) * ncols)) || (r = g_ctx.ttasklist.ensure(sizeof(int2) * ntask)))
+    if ((r = W.tflat.ensure(sizeof(float4) * nrec)) || (r = W.tld.ensure(sizeof(LayerD) * nrec)) ||
+        (r = W.tti.ensure(sizeof(TiRec) * nrec)) || (r = W.tsp.ensure(sizeof(SpRec) * nrec)) || (r = W.tch.ensure(sizeof(ChainRec) * nrec)) ||
+        (r = W.tmeta.ensure(sizeof(ColMeta) * ncols)) || (r = W.ttasklist.ensure(sizeof(int2) * ntask)))
         return r;
-    T.flat = g_ctx.tflat.as<float4>(); T.ld = g_ctx.tld.as<LayerD>(); T.ti = g_ctx.tti.as<TiRec>(); T.sp = g_ctx.tsp.as<SpRec>();
-    T.ch = g_ctx.tch.as<ChainRec>(); T.meta = g_ctx.tmeta.as<ColMeta>();
-    T.tile_lbase = g_ctx.tlbase.as<long long>(); T.tasks = g_ctx.ttasklist.as<int2>();
+    T.flat = W.tflat.as<float4>(); T.ld = W.tld.as<LayerD>(); T.ti = W.tti.as<TiRec>(); T.sp = W.tsp.as<SpRec>();
+    T.ch = W.tch.as<ChainRec>(); T.meta = W.tmeta.as<ColMeta>();
+    T.tile_lbase = W.tlbase.as<long long>(); T.tasks = W.ttasklist.as<int2>();
     T.ntasks = ntask; T.ncols = ncols; T.pv_sk = pv_sk; T.sen_sk = sen_sk; T.ls_sk = ls_sk;
-    prep_tasks_kernel<<<ntb, bt, 0, st>>>(ntiles, g_ctx.ttasks.as<long long>(), g_ctx.ttbase.as<long long>(),
+    prep_tasks_kernel<<<ntb, bt, 0, st>>>(ntiles, W.ttasks.as<long long>(), W.ttbase.as<long long>(),
                                           T.tasks);
     CK(cudaGetLastError());
-    prep_build_kernel<<<nb, bt, 0, st>>>(src, po, T, g_ctx.cidx2.as<int>(), g_ctx.ttbase.as<long long>());
+    prep_build_kernel<<<nb, bt, 0, st>>>(src, po, T, W.cidx2.as<int>(), W.ttbase.as<long long>());
     CK(cudaGetLastError());
     g_ctx.last_launches += 5;
     phase_mark("prep", st);
     return 0;
 }
 
-// The per-(column, period) kernels and the root search over built tables.
-int run_tables(const Tables& T, const double* per, const StageOut& o, int form, bool fd_done,
-               cudaStream_t st)
+// Kernel variants (instantiations of the templated kernels).
+const void* root_fn(int bt)
+{
+    return bt == 64 ? (const void*)root_kernel<64> : bt == 256 ? (const void*)root_kernel<256>
+                                                               : (const void*)root_kernel<128>;
+}
+const void* adjoint_fn(int minb)
+{
+    return minb == 2 ? (const void*)adjoint_kernel<2> : minb == 4 ? (const void*)adjoint_kernel<4>
+                                                                  : (const void*)adjoint_kernel<3>;
+}
+const void* ti_fn(int minb)
+{
+    return minb == 4 ? (const void*)ti_kernel<4> : minb == 6 ? (const void*)ti_kernel<6>
+                                                             : (const void*)ti_kernel<8>;
+}
+
+// Largest refined layer count of the tables (first sorted column): one
+// small read-back, done once per call (plans keep it).
+int table_maxr(const Tables& T, cudaStream_t st, long long& maxr)
+{
+    ColMeta m0;
+    CK(cudaMemcpyAsync(&m0, T.meta, sizeof(ColMeta), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    maxr = m0.rmax;
+    return 0;
+}
+
+// Scratch of the sweeps, sized for the persistent grids of the chosen
+// variants (allocation happens here, never inside a graph capture).
+int ensure_sweep_scratch(const Tables& T, bool adj, bool ti, long long maxr, const LaunchCfg& cfg,
+                         Work& W)
 {
     int r;
-    unsigned long long* nevals = g_ctx.counters.as<unsigned long long>();
-    int* errflag = reinterpret_cast<int*>(nevals + 1);
-    unsigned* queues = reinterpret_cast<unsigned*>(nevals + 2);
-    const bool adj = o.svs && (form & 1) == DAZI_FORM_ADJOINT;
-    long long maxr = 0;
-    {
-        // largest layer count (first sorted column) for the scratch sizes
-        ColMeta m0;
-        CK(cudaMemcpyAsync(&m0, T.meta, sizeof(ColMeta), cudaMemcpyDeviceToHost, st));
-        CK(cudaStreamSynchronize(st));
-        maxr = m0.rmax;
-    }
-    if (!fd_done) {
-        RootArgs a;
-        a.T = T; a.periods = per; a.tol = 1.0e-6;   // surfdisp96.f:608
-        a.pv = o.pv; a.croot = nullptr; a.status = o.status; a.nevals = nevals;
-        a.scan32 = (form & DAZI_FORM_SCAN_FP32) ? 1 : 0;
-        if (adj) {
-            if ((r = g_ctx.croot.ensure(sizeof(double) * TILE * (size_t)T.ntasks))) return r;
-            a.croot = g_ctx.croot.as<double>();
-        }
-        const int bt = 128;
-        root_kernel<<<(unsigned)((T.ncols + bt - 1) / bt), bt, 0, st>>>(a);
-        CK(cudaGetLastError());
-        ++g_ctx.last_launches;
-        phase_mark("root", st);
-    }
     const long long nitems = T.ntasks * TILE;
     if (adj) {
-        const int at = 128;
         long long nblk;
-        if ((r = launch_persistent_grid((const void*)adjoint_kernel, nitems, at, nblk))) return r;
-        const long long nslots = nblk * at;
-        const size_t scr = sizeof(double) * 6 * (size_t)(maxr > 1 ? maxr - 1 : 1) * (size_t)nslots;
-        if ((r = g_ctx.adjscr.ensure(scr))) return r;
-        CK(cudaMemsetAsync(queues, 0, sizeof(unsigned), st));
-        AdjArgs j;
-        j.T = T; j.periods = per; j.croot = g_ctx.croot.as<double>();
-        j.sen_vs = o.svs; j.sen_vp = o.svp; j.sen_rho = o.srh;
-        j.scratch = g_ctx.adjscr.as<double>(); j.scr_layers = maxr > 1 ? maxr - 1 : 1; j.queue = queues;
-        adjoint_kernel<<<(unsigned)nblk, at, 0, st>>>(j);
-        CK(cudaGetLastError());
-        ++g_ctx.last_launches;
-        phase_mark("adjoint", st);
+        if ((r = W.croot.ensure(sizeof(double) * TILE * (size_t)T.ntasks))) return r;
+        if ((r = launch_persistent_grid(adjoint_fn(cfg.adj_minb), nitems, 128, nblk))) return r;
+        const size_t scr = sizeof(double) * 6 * (size_t)(maxr > 1 ? maxr - 1 : 1) * (size_t)(nblk * 128);
+        if ((r = W.adjscr.ensure(scr))) return r;
     }
-    if (o.lsen) {
-        const int at = 128;
+    if (ti) {
         long long nblk;
-        if ((r = launch_persistent_grid((const void*)ti_kernel, nitems, at, nblk))) return r;
-        const long long nslots = nblk * at;
-        const size_t scr = sizeof(double) * TI_SCR_Q * (size_t)maxr * (size_t)nslots;
-        if ((r = g_ctx.tiscr.ensure(scr))) return r;
-        CK(cudaMemsetAsync(queues + 1, 0, sizeof(unsigned), st));
-        TiArgs t;
-        t.T = T; t.periods = per; t.pv = o.pv; t.lsen = o.lsen;
-        t.scratch = g_ctx.tiscr.as<double>(); t.scr_layers = maxr; t.queue = queues + 1; t.errflag = errflag;
-        ti_kernel<<<(unsigned)nblk, at, 0, st>>>(t);
-        CK(cudaGetLastError());
-        ++g_ctx.last_launches;
-        phase_mark("ti", st);
+        if ((r = launch_persistent_grid(ti_fn(cfg.ti_minb), nitems, 128, nblk))) return r;
+        const size_t scr = sizeof(double) * TI_SCR_Q * (size_t)maxr * (size_t)(nblk * 128);
+        if ((r = W.tiscr.ensure(scr))) return r;
     }
+    return 0;
+}
+
+int run_root(const Tables& T, const double* per, const StageOut& o, int form, bool adj, Work& W,
+             const LaunchCfg& cfg, cudaStream_t st)
+{
+    RootArgs a;
+    a.T = T; a.periods = per; a.tol = 1.0e-6;   // surfdisp96.f:608
+    a.pv = o.pv; a.croot = adj ? W.croot.as<double>() : nullptr; a.status = o.status;
+    a.nevals = W.counters.as<unsigned long long>();
+    a.scan32 = (form & DAZI_FORM_SCAN_FP32) ? 1 : 0;
+    const int bt = cfg.root_bt;
+    const unsigned nb = (unsigned)((T.ncols + bt - 1) / bt);
+    if (bt == 64) root_kernel<64><<<nb, 64, 0, st>>>(a);
+    else if (bt == 256) root_kernel<256><<<nb, 256, 0, st>>>(a);
+    else root_kernel<128><<<nb, 128, 0, st>>>(a);
+    CK(cudaGetLastError());
+    ++g_ctx.last_launches;
+    phase_mark("root", st);
+    return 0;
+}
+
+int run_adjoint(const Tables& T, const double* per, const StageOut& o, long long maxr, Work& W,
+                const LaunchCfg& cfg, cudaStream_t st)
+{
+    int r;
+    long long nblk;
+    if ((r = launch_persistent_grid(adjoint_fn(cfg.adj_minb), T.ntasks * TILE, 128, nblk))) return r;
+    unsigned* queues = reinterpret_cast<unsigned*>(W.counters.as<unsigned long long>() + 2);
+    CK(cudaMemsetAsync(queues, 0, sizeof(unsigned), st));
+    AdjArgs j;
+    j.T = T; j.periods = per; j.croot = W.croot.as<double>();
+    j.sen_vs = o.svs; j.sen_vp = o.svp; j.sen_rho = o.srh;
+    j.scratch = W.adjscr.as<double>(); j.scr_layers = maxr > 1 ? maxr - 1 : 1; j.queue = queues;
+    if (cfg.adj_minb == 2) adjoint_kernel<2><<<(unsigned)nblk, 128, 0, st>>>(j);
+    else if (cfg.adj_minb == 4) adjoint_kernel<4><<<(unsigned)nblk, 128, 0, st>>>(j);
+    else adjoint_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(j);
+    CK(cudaGetLastError());
+    ++g_ctx.last_launches;
+    phase_mark("adjoint", st);
+    return 0;
+}
+
+int run_ti(const Tables& T, const double* per, const StageOut& o, long long maxr, Work& W,
+           const LaunchCfg& cfg, cudaStream_t st)
+{
+    int r;
+    long long nblk;
+    if ((r = launch_persistent_grid(ti_fn(cfg.ti_minb), T.ntasks * TILE, 128, nblk))) return r;
+    unsigned long long* c = W.counters.as<unsigned long long>();
+    unsigned* queues = reinterpret_cast<unsigned*>(c + 2);
+    CK(cudaMemsetAsync(queues + 1, 0, sizeof(unsigned), st));
+    TiArgs t;
+    t.T = T; t.periods = per; t.pv = o.pv; t.lsen = o.lsen;
+    t.scratch = W.tiscr.as<double>(); t.scr_layers = maxr; t.queue = queues + 1;
+    t.errflag = reinterpret_cast<int*>(c + 1);
+    if (cfg.ti_minb == 4) ti_kernel<4><<<(unsigned)nblk, 128, 0, st>>>(t);
+    else if (cfg.ti_minb == 6) ti_kernel<6><<<(unsigned)nblk, 128, 0, st>>>(t);
+    else ti_kernel<8><<<(unsigned)nblk, 128, 0, st>>>(t);
+    CK(cudaGetLastError());
+    ++g_ctx.last_launches;
+    phase_mark("ti", st);
+    return 0;
+}
+
+// The per-(column, period) kernels and the root search over built tables.
+int run_tables(const Tables& T, const double* per, const StageOut& o, int form, bool fd_done,
+               cudaStream_t st, Work& W, const LaunchCfg& cfg)
+{
+    int r;
+    const bool adj = o.svs && (form & 1) == DAZI_FORM_ADJOINT;
+    long long maxr = 0;
+    if ((r = table_maxr(T, st, maxr))) return r;
+    if ((r = ensure_sweep_scratch(T, adj, o.lsen != nullptr, maxr, cfg, W))) return r;
+    if (!fd_done && (r = run_root(T, per, o, form, adj, W, cfg, st))) return r;
+    if (adj && (r = run_adjoint(T, per, o, maxr, W, cfg, st))) return r;
+    if (o.lsen && (r = run_ti(T, per, o, maxr, W, cfg, st))) return r;
     return 0;
 }
 
@@ -378,8 +461,8 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
     if (col_count == 0) return 0;
     const Geometry* geo = g_ctx.geo.as<Geometry>();
     int r;
-    if ((r = g_ctx.counters.ensure(sizeof(unsigned long long) * 8))) return r;
-    CK(cudaMemsetAsync(g_ctx.counters.p, 0, sizeof(unsigned long long) * 8, st));
+    if ((r = g_ctx.w.counters.ensure(sizeof(unsigned long long) * 8))) return r;
+    CK(cudaMemsetAsync(g_ctx.w.counters.p, 0, sizeof(unsigned long long) * 8, st));
     g_ctx.last_rmax = g_ctx.geo_rmax;
     g_ctx.last_launches = 0;
     phase_begin(st);
@@ -403,7 +486,7 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
             a.vel = vel; a.vp = vp; a.rho = rho; a.periods = per;
             a.pv = o.pv; a.sen_vs = o.svs; a.sen_vp = o.svp; a.sen_rho = o.srh;
             a.status = o.status; a.cscratch = g_ctx.cscratch.as<float>();
-            a.dln = 0.01f; a.tol = 1.0e-6; a.nevals = g_ctx.counters.as<unsigned long long>();
+            a.dln = 0.01f; a.tol = 1.0e-6; a.nevals = g_ctx.w.counters.as<unsigned long long>();
             fd_column_kernel<<<(unsigned)n, threads, smem, st>>>(a);
             CK(cudaGetLastError());
             ++g_ctx.last_launches;
@@ -416,10 +499,10 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
     src.vel = vel; src.vp = vp; src.rho = rho; src.depz = g_ctx.depz.as<float>();
     src.node_off = nullptr; src.per_off = nullptr; src.nz = nz; src.K = kmax;
     src.minthk = g_ctx.geo_minthk;
-    PrepOut po{nullptr, nullptr, g_ctx.counters.as<unsigned long long>() + 4};
+    PrepOut po{nullptr, nullptr, g_ctx.w.counters.as<unsigned long long>() + 4};
     Tables T;
-    if ((r = build_tables(src, col_count, po, ncol, ncol, ncol, st, T))) return r;
-    return run_tables(T, per, o, form, fd, st);
+    if ((r = build_tables(src, col_count, po, ncol, ncol, ncol, st, T, g_ctx.w))) return r;
+    return run_tables(T, per, o, form, fd, st, g_ctx.w, LaunchCfg());
 }
 
 // Ragged batch on device pointers.
@@ -441,8 +524,8 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
 {
     if (B.ncols == 0) return 0;
     int r;
-    if ((r = g_ctx.counters.ensure(sizeof(unsigned long long) * 8))) return r;
-    CK(cudaMemsetAsync(g_ctx.counters.p, 0, sizeof(unsigned long long) * 8, st));
+    if ((r = g_ctx.w.counters.ensure(sizeof(unsigned long long) * 8))) return r;
+    CK(cudaMemsetAsync(g_ctx.w.counters.p, 0, sizeof(unsigned long long) * 8, st));
     g_ctx.last_launches = 0;
     g_ctx.last_rmax = 0;
     phase_begin(st);
@@ -451,9 +534,9 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
     src.vel = B.vs; src.vp = B.vp; src.rho = B.rho; src.depz = B.depz;
     src.node_off = B.node_off; src.per_off = B.per_off; src.nz = 0; src.K = 0;
     src.minthk = B.minthk;
-    PrepOut po{B.sen_off, B.ls_off, g_ctx.counters.as<unsigned long long>() + 4};
+    PrepOut po{B.sen_off, B.ls_off, g_ctx.w.counters.as<unsigned long long>() + 4};
     Tables T;
-    if ((r = build_tables(src, B.ncols, po, 1, 1, 1, st, T))) return r;
+    if ((r = build_tables(src, B.ncols, po, 1, 1, 1, st, T, g_ctx.w))) return r;
     const bool fd = o.svs && (form & 1) == DAZI_FORM_PLAIN;
     if (fd) {
         // plain form: one CTA per column, scratch offsets per column
@@ -481,7 +564,7 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
             a.vel = B.vs; a.vp = B.vp; a.rho = B.rho; a.periods = B.periods;
             a.pv = o.pv; a.sen_vs = o.svs; a.sen_vp = o.svp; a.sen_rho = o.srh;
             a.status = o.status; a.cscratch = g_ctx.cscratch.as<float>();
-            a.dln = 0.01f; a.tol = 1.0e-6; a.nevals = g_ctx.counters.as<unsigned long long>();
+            a.dln = 0.01f; a.tol = 1.0e-6; a.nevals = g_ctx.w.counters.as<unsigned long long>();
             FdBatch fb;
             fb.node_off = B.node_off; fb.per_off = B.per_off; fb.depz = B.depz; fb.minthk = B.minthk;
             fb.sen_off = B.sen_off; fb.cbuf_off = g_ctx.cbufoff.as<long long>();
@@ -492,7 +575,162 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
         }
         phase_mark("fd", st);
     }
-    return run_tables(T, B.periods, o, form, fd, st);
+    return run_tables(T, B.periods, o, form, fd, st, g_ctx.w, LaunchCfg());
+}
+
+// ------------------------------------------------------------------ plans
+// A plan binds a ragged batch (structure and device buffers) once: the
+// structure part of the tables (refined layer counts, sort, tiles, tasks)
+// is built at creation, the kernel variants are picked by timing them on
+// this batch, and the per-run sequence -- layer values from the current
+// velocities, counters, root search, adjoint and Gc/Gs sweeps -- is
+// captured in a CUDA graph.  A run is one graph launch, with no host
+// synchronisation.
+struct Plan {
+    int device = -1;
+    cudaStream_t cs = nullptr;       // private stream (build, tuning, capture)
+    Work w;
+    ColSrc src;
+    PrepOut po;
+    Tables T;
+    StageOut o;
+    const double* periods = nullptr;
+    int form = DAZI_FORM_ADJOINT;
+    bool adj = false;
+    long long maxr = 0;
+    LaunchCfg cfg;
+    float best_ms[3] = {0.f, 0.f, 0.f};
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    void release()
+    {
+        if (exec) cudaGraphExecDestroy(exec);
+        if (graph) cudaGraphDestroy(graph);
+        exec = nullptr; graph = nullptr;
+        w.release();
+        if (cs) cudaStreamDestroy(cs);
+        cs = nullptr;
+    }
+};
+
+// Time one phase launcher on the plan's stream (best of two after a warm-up).
+template <class F>
+int time_phase(Plan& P, F launch, float& ms)
+{
+    cudaEvent_t a, b;
+    CK(cudaEventCreate(&a));
+    CK(cudaEventCreate(&b));
+    int r = launch();
+    float best = 1e30f;
+    for (int rep = 0; rep < 2 && !r; ++rep) {
+        cudaEventRecord(a, P.cs);
+        r = launch();
+        cudaEventRecord(b, P.cs);
+        if (!r && cudaEventSynchronize(b) == cudaSuccess) {
+            float t = 0.f;
+            cudaEventElapsedTime(&t, a, b);
+            if (t < best) best = t;
+        }
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    ms = best;
+    return r;
+}
+
+int plan_tune(Plan& P)
+{
+    int r;
+    const int root_c[3] = {64, 128, 256}, adj_c[3] = {2, 3, 4}, ti_c[3] = {4, 6, 8};
+    LaunchCfg c = P.cfg;
+    float best = 1e30f;
+    for (int bt : root_c) {
+        c.root_bt = bt;
+        float ms;
+        if ((r = time_phase(P, [&] { return run_root(P.T, P.periods, P.o, P.form, P.adj, P.w, c, P.cs); }, ms)))
+            return r;
+        if (ms < best) { best = ms; P.cfg.root_bt = bt; }
+    }
+    P.best_ms[0] = best;
+    c.root_bt = P.cfg.root_bt;
+    if (P.adj) {
+        best = 1e30f;
+        for (int mb : adj_c) {
+            c.adj_minb = mb;
+            float ms;
+            if ((r = ensure_sweep_scratch(P.T, true, false, P.maxr, c, P.w))) return r;
+            if ((r = time_phase(P, [&] { return run_adjoint(P.T, P.periods, P.o, P.maxr, P.w, c, P.cs); }, ms)))
+                return r;
+            if (ms < best) { best = ms; P.cfg.adj_minb = mb; }
+        }
+        P.best_ms[1] = best;
+        c.adj_minb = P.cfg.adj_minb;
+    }
+    if (P.o.lsen) {
+        best = 1e30f;
+        for (int mb : ti_c) {
+            c.ti_minb = mb;
+            float ms;
+            if ((r = ensure_sweep_scratch(P.T, false, true, P.maxr, c, P.w))) return r;
+            if ((r = time_phase(P, [&] { return run_ti(P.T, P.periods, P.o, P.maxr, P.w, c, P.cs); }, ms)))
+                return r;
+            if (ms < best) { best = ms; P.cfg.ti_minb = mb; }
+        }
+        P.best_ms[2] = best;
+    }
+    return 0;
+}
+
+// The per-run sequence on the plan's stream (captured).
+int plan_enqueue(Plan& P)
+{
+    int r;
+    CK(cudaMemsetAsync(P.w.counters.p, 0, sizeof(unsigned long long) * 8, P.cs));
+    const unsigned nb = (unsigned)((P.T.ncols + 127) / 128);
+    prep_build_kernel<<<nb, 128, 0, P.cs>>>(P.src, P.po, P.T, P.w.cidx2.as<int>(), P.w.ttbase.as<long long>());
+    CK(cudaGetLastError());
+    if ((r = run_root(P.T, P.periods, P.o, P.form, P.adj, P.w, P.cfg, P.cs))) return r;
+    if (P.adj && (r = run_adjoint(P.T, P.periods, P.o, P.maxr, P.w, P.cfg, P.cs))) return r;
+    if (P.o.lsen && (r = run_ti(P.T, P.periods, P.o, P.maxr, P.w, P.cfg, P.cs))) return r;
+    return 0;
+}
+
+int plan_create(const BatchIn& B, const StageOut& o, int form, bool tune, cudaStream_t user, Plan& P)
+{
+    int r;
+    CK(cudaGetDevice(&P.device));
+    CK(cudaStreamSynchronize(user));   // the inputs are ready
+    CK(cudaStreamCreateWithFlags(&P.cs, cudaStreamNonBlocking));
+    if ((r = P.w.counters.ensure(sizeof(unsigned long long) * 8))) return r;
+    CK(cudaMemsetAsync(P.w.counters.p, 0, sizeof(unsigned long long) * 8, P.cs));
+    P.src.ragged = true; P.src.ncol = 0; P.src.col0 = 0;
+    P.src.vel = B.vs; P.src.vp = B.vp; P.src.rho = B.rho; P.src.depz = B.depz;
+    P.src.node_off = B.node_off; P.src.per_off = B.per_off; P.src.nz = 0; P.src.K = 0;
+    P.src.minthk = B.minthk;
+    P.po = PrepOut{B.sen_off, B.ls_off, P.w.counters.as<unsigned long long>() + 4};
+    P.o = o;
+    P.form = form;
+    P.periods = B.periods;
+    P.adj = o.svs != nullptr;
+    if ((r = build_tables(P.src, B.ncols, P.po, 1, 1, 1, P.cs, P.T, P.w))) return r;
+    if ((r = table_maxr(P.T, P.cs, P.maxr))) return r;
+    if ((r = ensure_sweep_scratch(P.T, P.adj, o.lsen != nullptr, P.maxr, P.cfg, P.w))) return r;
+    if (tune && (r = plan_tune(P))) return r;
+    if ((r = ensure_sweep_scratch(P.T, P.adj, o.lsen != nullptr, P.maxr, P.cfg, P.w))) return r;
+    CK(cudaStreamSynchronize(P.cs));
+    // capture (per-phase timing stays out of the graph)
+    const bool timing = g_ctx.timer.on;
+    g_ctx.timer.on = false;
+    CK(cudaStreamBeginCapture(P.cs, cudaStreamCaptureModeThreadLocal));
+    r = plan_enqueue(P);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e = cudaStreamEndCapture(P.cs, &g);
+    g_ctx.timer.on = timing;
+    if (r) { if (g) cudaGraphDestroy(g); return r; }
+    if (e != cudaSuccess) { set_err("graph capture failed: %s", cudaGetErrorString(e)); return DAZI_ERR_CUDA; }
+    P.graph = g;
+    CK(cudaGraphInstantiate(&P.exec, P.graph, 0ULL));
+    return 0;
 }
 
 int check_values(const float* vel, const float* vp, const float* rho, long long ncol, int nz,
@@ -595,7 +833,7 @@ int stage_host(const int* pnx, const int* pny, const int* pnz, const float* vel,
     g_ctx.last_status.resize(ncol);
     CK(cudaMemcpyAsync(g_ctx.last_status.data(), g_ctx.status.p, sizeof(int) * ncol, cudaMemcpyDeviceToHost, st));
     int hflag[2] = {0, 0};
-    CK(cudaMemcpyAsync(hflag, g_ctx.counters.as<unsigned long long>() + 1, sizeof(int) * 2,
+    CK(cudaMemcpyAsync(hflag, g_ctx.w.counters.as<unsigned long long>() + 1, sizeof(int) * 2,
                        cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     g_ctx.last_ncol = ncol;
@@ -830,7 +1068,7 @@ int dazi_dk_batch(long long ncols, const long long* node_off, const float* depz,
     std::vector<int> hst(ncols);
     CK(cudaMemcpyAsync(hst.data(), o.status, sizeof(int) * ncols, cudaMemcpyDeviceToHost, st));
     int hflag = 0;
-    CK(cudaMemcpyAsync(&hflag, g_ctx.counters.as<unsigned long long>() + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&hflag, g_ctx.w.counters.as<unsigned long long>() + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
     if (status) std::memcpy(status, hst.data(), sizeof(int) * ncols);
     if (hflag) { set_err("non-finite Lsen_Gsc value (degenerate layer: Vp <= Vs?)"); return DAZI_ERR_MODEL; }
@@ -871,9 +1109,9 @@ int dazi_dk_last_launches(void)
 int dazi_dk_last_work(long long* secular_evals, long long* layer_evals)
 {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_ctx.ready || !g_ctx.counters.p) { set_err("no call made yet"); return DAZI_ERR_BADARG; }
+    if (!g_ctx.ready || !g_ctx.w.counters.p) { set_err("no call made yet"); return DAZI_ERR_BADARG; }
     unsigned long long h[4] = {0, 0, 0, 0};
-    CK(cudaMemcpy(h, g_ctx.counters.p, sizeof(h), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(h, g_ctx.w.counters.p, sizeof(h), cudaMemcpyDeviceToHost));
     if (secular_evals) *secular_evals = (long long)h[0];
     if (layer_evals) *layer_evals = (long long)h[3];
     return 0;
@@ -882,11 +1120,98 @@ int dazi_dk_last_work(long long* secular_evals, long long* layer_evals)
 int dazi_dk_last_items(long long* column_periods, long long* layer_items)
 {
     std::lock_guard<std::mutex> lk(g_mu);
-    if (!g_ctx.ready || !g_ctx.counters.p) { set_err("no call made yet"); return DAZI_ERR_BADARG; }
+    if (!g_ctx.ready || !g_ctx.w.counters.p) { set_err("no call made yet"); return DAZI_ERR_BADARG; }
     unsigned long long h[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    CK(cudaMemcpy(h, g_ctx.counters.p, sizeof(h), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpy(h, g_ctx.w.counters.p, sizeof(h), cudaMemcpyDeviceToHost));
     if (column_periods) *column_periods = (long long)h[5];
     if (layer_items) *layer_items = (long long)h[4];
+    return 0;
+}
+
+int dazi_dk_plan_create(long long ncols, const long long* node_off, const float* depz, const float* vs,
+                        const float* vp, const float* rho, const long long* per_off,
+                        const double* periods, float minthk, double* pv, const long long* sen_off,
+                        double* sen_vs, double* sen_vp, double* sen_rho, const long long* ls_off,
+                        float* lsen, int form, int* status, int tune, void* stream, void** plan)
+{
+    if (!plan) { set_err("null plan pointer"); return DAZI_ERR_BADARG; }
+    *plan = nullptr;
+    if (ncols < 1 || !node_off || !depz || !vs || !per_off || !periods || !pv || !status) {
+        set_err("null argument or empty batch");
+        return DAZI_ERR_BADARG;
+    }
+    if ((sen_vs == nullptr) != (sen_vp == nullptr) || (sen_vs == nullptr) != (sen_rho == nullptr) ||
+        (sen_vs && !sen_off) || (lsen && !ls_off)) {
+        set_err("kernel outputs need sen_off / ls_off and all three sen arrays");
+        return DAZI_ERR_BADARG;
+    }
+    if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
+    if (!valid_form(form) || (form & 1) != DAZI_FORM_ADJOINT) {
+        set_err("plans run the adjoint form (form %d)", form);
+        return DAZI_ERR_BADARG;
+    }
+    if (!(minthk > 0.f) || !std::isfinite(minthk)) { set_err("minthk must be > 0"); return DAZI_ERR_BADARG; }
+    std::lock_guard<std::mutex> lk(g_mu);
+    int r;
+    if ((r = ensure_context())) return r;
+    Plan* P = new Plan;
+    BatchIn B{ncols, node_off, depz, vs, vp, rho, per_off, periods, minthk, sen_off, ls_off};
+    StageOut o;
+    o.pv = pv; o.svs = sen_vs; o.svp = sen_vp; o.srh = sen_rho; o.lsen = lsen; o.status = status;
+    if ((r = plan_create(B, o, form, tune != 0, (cudaStream_t)stream, *P))) {
+        P->release();
+        delete P;
+        return r;
+    }
+    *plan = P;
+    return 0;
+}
+
+int dazi_dk_plan_launch(void* plan, void* stream)
+{
+    if (!plan) { set_err("null plan"); return DAZI_ERR_BADARG; }
+    Plan* P = static_cast<Plan*>(plan);
+    int cur = -1;
+    CK(cudaGetDevice(&cur));
+    if (cur != P->device) CK(cudaSetDevice(P->device));
+    CK(cudaGraphLaunch(P->exec, (cudaStream_t)stream));
+    if (cur != P->device) CK(cudaSetDevice(cur));
+    return 0;
+}
+
+int dazi_dk_plan_status(void* plan)
+{
+    if (!plan) { set_err("null plan"); return DAZI_ERR_BADARG; }
+    Plan* P = static_cast<Plan*>(plan);
+    int flag = 0;
+    CK(cudaMemcpy(&flag, P->w.counters.as<unsigned long long>() + 1, sizeof(int), cudaMemcpyDeviceToHost));
+    if (flag) { set_err("non-finite Lsen_Gsc value (degenerate layer: Vp <= Vs?)"); return DAZI_ERR_MODEL; }
+    return 0;
+}
+
+int dazi_dk_plan_config(void* plan, int* root_block, int* adjoint_blocks_per_sm,
+                        int* ti_blocks_per_sm, float* tuned_ms)
+{
+    if (!plan) { set_err("null plan"); return DAZI_ERR_BADARG; }
+    const Plan* P = static_cast<const Plan*>(plan);
+    if (root_block) *root_block = P->cfg.root_bt;
+    if (adjoint_blocks_per_sm) *adjoint_blocks_per_sm = P->cfg.adj_minb;
+    if (ti_blocks_per_sm) *ti_blocks_per_sm = P->cfg.ti_minb;
+    if (tuned_ms) for (int i = 0; i < 3; ++i) tuned_ms[i] = P->best_ms[i];
+    return 0;
+}
+
+int dazi_dk_plan_destroy(void* plan)
+{
+    if (!plan) return 0;
+    Plan* P = static_cast<Plan*>(plan);
+    std::lock_guard<std::mutex> lk(g_mu);
+    int cur = -1;
+    cudaGetDevice(&cur);
+    if (cur != P->device) cudaSetDevice(P->device);
+    P->release();
+    if (cur != P->device) cudaSetDevice(cur);
+    delete P;
     return 0;
 }
 
@@ -900,11 +1225,11 @@ void dazi_dk_finalize(void)
     if (!g_ctx.ready) return;
     DBuf* all[] = {&g_ctx.vel, &g_ctx.vp, &g_ctx.rho, &g_ctx.per, &g_ctx.depz, &g_ctx.pv,
                    &g_ctx.svs, &g_ctx.svp, &g_ctx.srh, &g_ctx.status, &g_ctx.geo,
-                   &g_ctx.cscratch, &g_ctx.croot, &g_ctx.counters, &g_ctx.adjscr,
-                   &g_ctx.tiscr, &g_ctx.lsen, &g_ctx.keys, &g_ctx.keys2, &g_ctx.cidx, &g_ctx.cidx2,
-                   &g_ctx.rmaxb, &g_ctx.trecs, &g_ctx.ttasks, &g_ctx.tlbase, &g_ctx.ttbase,
-                   &g_ctx.cubtmp, &g_ctx.tflat, &g_ctx.tld, &g_ctx.tti, &g_ctx.tsp, &g_ctx.tch, &g_ctx.tmeta,
-                   &g_ctx.ttasklist, &g_ctx.cbufoff, &g_ctx.bnode, &g_ctx.bper, &g_ctx.bdep,
+                   &g_ctx.cscratch, &g_ctx.w.croot, &g_ctx.w.counters, &g_ctx.w.adjscr,
+                   &g_ctx.w.tiscr, &g_ctx.lsen, &g_ctx.w.keys, &g_ctx.w.keys2, &g_ctx.w.cidx, &g_ctx.w.cidx2,
+                   &g_ctx.w.rmaxb, &g_ctx.w.trecs, &g_ctx.w.ttasks, &g_ctx.w.tlbase, &g_ctx.w.ttbase,
+                   &g_ctx.w.cubtmp, &g_ctx.w.tflat, &g_ctx.w.tld, &g_ctx.w.tti, &g_ctx.w.tsp, &g_ctx.w.tch, &g_ctx.w.tmeta,
+                   &g_ctx.w.ttasklist, &g_ctx.cbufoff, &g_ctx.bnode, &g_ctx.bper, &g_ctx.bdep,
                    &g_ctx.bvs, &g_ctx.bvp, &g_ctx.brho, &g_ctx.bperiods, &g_ctx.bsenoff,
                    &g_ctx.blsoff, &g_ctx.bpv, &g_ctx.bsvs, &g_ctx.bsvp, &g_ctx.bsrh, &g_ctx.blsen,
                    &g_ctx.bstatus};

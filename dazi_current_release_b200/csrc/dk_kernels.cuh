@@ -113,9 +113,9 @@ __global__ void prep_tasks_kernel(long long ntiles, const long long* tile_tasks,
                                   const long long* tile_tbase, int2* tasks);
 __global__ void prep_build_kernel(ColSrc src, PrepOut o, Tables T, const int* sorted_col,
                                   const long long* tile_tbase);
-__global__ void root_kernel(RootArgs a);
-__global__ void adjoint_kernel(AdjArgs a);
-__global__ void ti_kernel(TiArgs a);
+template <int BT> __global__ void root_kernel(RootArgs a);        // BT in {64, 128, 256}
+template <int MINB> __global__ void adjoint_kernel(AdjArgs a);    // MINB in {2, 3, 4}
+template <int MINB> __global__ void ti_kernel(TiArgs a);          // MINB in {4, 6, 8}
 
 __global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);
 __global__ void fd_column_kernel(FdArgs a);

@@ -311,12 +311,10 @@ __device__ __forceinline__ long long next_task(unsigned* queue)
     return (long long)__shfl_sync(0xffffffffu, t, 0);
 }
 
-// Minimum resident blocks per SM the register allocation aims for.
-#ifndef DK_ADJ_MIN_BLOCKS
-#define DK_ADJ_MIN_BLOCKS 3
-#endif
-
-__global__ void __launch_bounds__(128, DK_ADJ_MIN_BLOCKS)
+// MINB: minimum resident blocks of 128 threads per SM the register
+// allocation aims for (the autotuner picks one of the instantiations).
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB)
 adjoint_kernel(AdjArgs a)
 {
     const Tables& T = a.T;
@@ -460,5 +458,9 @@ adjoint_kernel(AdjArgs a)
         }
     }
 }
+
+template __global__ void adjoint_kernel<2>(AdjArgs);
+template __global__ void adjoint_kernel<3>(AdjArgs);
+template __global__ void adjoint_kernel<4>(AdjArgs);
 
 }  // namespace dk

@@ -245,12 +245,10 @@ struct TableModel {
     __device__ __forceinline__ float4 layerf(int m) const { return flat[base + (long long)m * TILE]; }
 };
 
-// Minimum resident blocks per SM the register allocation aims for.
-#ifndef DK_ROOT_MIN_BLOCKS
-#define DK_ROOT_MIN_BLOCKS 1
-#endif
-
-__global__ void __launch_bounds__(128, DK_ROOT_MIN_BLOCKS)
+// BT: threads per block (one thread per column; the autotuner picks one of
+// the instantiations).
+template <int BT>
+__global__ void __launch_bounds__(BT)
 root_kernel(RootArgs a)
 {
     const Tables& T = a.T;
@@ -281,5 +279,9 @@ root_kernel(RootArgs a)
         if ((threadIdx.x & 31) == 0 && w) { atomicAdd(a.nevals, w); atomicAdd(a.nevals + 3, wl); }
     }
 }
+
+template __global__ void root_kernel<64>(RootArgs);
+template __global__ void root_kernel<128>(RootArgs);
+template __global__ void root_kernel<256>(RootArgs);
 
 }  // namespace dk

@@ -860,11 +860,6 @@ __device__ __forceinline__ long long ti_next_task(unsigned* queue)
     return (long long)__shfl_sync(0xffffffffu, t, 0);
 }
 
-// Minimum resident blocks per SM the register allocation aims for.
-#ifndef DK_TI_MIN_BLOCKS
-#define DK_TI_MIN_BLOCKS 8
-#endif
-
 // One (column, period) of the Gc/Gs kernel: lane `lane` of task `task`,
 // with the thread's scratch block at scr (layer m, entry q at
 // scr[(m * TI_SCR_Q + q) * TILE]).
@@ -1064,7 +1059,10 @@ __device__ __forceinline__ void ti_task(const TiArgs& a, long long task, int lan
     }
 }
 
-__global__ void __launch_bounds__(128, DK_TI_MIN_BLOCKS)
+// MINB: minimum resident blocks of 128 threads per SM the register
+// allocation aims for (the autotuner picks one of the instantiations).
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB)
 ti_kernel(TiArgs a)
 {
     // scratch: per warp [layer][q][lane] -- compile-time strides
@@ -1077,5 +1075,9 @@ ti_kernel(TiArgs a)
         ti_task(a, task, lane, scr);
     }
 }
+
+template __global__ void ti_kernel<4>(TiArgs);
+template __global__ void ti_kernel<6>(TiArgs);
+template __global__ void ti_kernel<8>(TiArgs);
 
 }  // namespace dk

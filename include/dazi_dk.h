@@ -181,6 +181,39 @@ int dazi_dk_batch_dev(long long ncols, const long long *node_off,
                       double *sen_vp, double *sen_rho, const long long *ls_off,
                       float *lsen, int form, int *status, void *stream);
 
+/* Plans: the uneven-column batch bound once, run many times.  No
+ * counterpart in the reference (its per-call drivers rebuild everything);
+ * this replaces the fixed tile pipelines for the inversion loop, where the
+ * column structure (node depths, periods) stays while the velocities
+ * change.  dazi_dk_plan_create takes the arguments of dazi_dk_batch_dev
+ * (device pointers, adjoint form only; sen_* and/or lsen may be NULL), builds
+ * the structure of the layer tables, picks the kernel variants by timing
+ * them on this batch when tune != 0 (root-search block size; register
+ * budgets of the adjoint and Gc/Gs sweeps), and captures the per-run
+ * sequence in a CUDA graph.  The buffers stay bound: dazi_dk_plan_launch
+ * recomputes everything from the current contents of vs (vp, rho) and
+ * writes the same output buffers, as one graph launch on `stream` with no
+ * host synchronisation.  Velocities are validated at creation only; a
+ * non-finite Lsen_Gsc of a later run is reported by dazi_dk_plan_status
+ * (which reads the device flag; call it after the run completes).  A plan
+ * owns its device buffers and stream until dazi_dk_plan_destroy.  Creation
+ * synchronises with `stream` and takes several runs' time (tuning). */
+int dazi_dk_plan_create(long long ncols, const long long *node_off,
+                        const float *depz, const float *vs, const float *vp,
+                        const float *rho, const long long *per_off,
+                        const double *periods, float minthk, double *pv,
+                        const long long *sen_off, double *sen_vs,
+                        double *sen_vp, double *sen_rho,
+                        const long long *ls_off, float *lsen, int form,
+                        int *status, int tune, void *stream, void **plan);
+int dazi_dk_plan_launch(void *plan, void *stream);
+int dazi_dk_plan_status(void *plan);
+/* The tuner's choice: root-search threads per block, blocks per SM of the
+ * adjoint and Gc/Gs sweeps, and their tuned phase times (ms, 3 floats). */
+int dazi_dk_plan_config(void *plan, int *root_block, int *adjoint_blocks_per_sm,
+                        int *ti_blocks_per_sm, float *tuned_ms);
+int dazi_dk_plan_destroy(void *plan);
+
 /* Per-phase timing: with dazi_dk_set_timing(1), each call records CUDA
  * events on its stream around its phases ("prep", "fd", "root", "adjoint",
  * "ti"); dazi_dk_last_timing fills up to cap (name, milliseconds) pairs of
