@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -83,9 +84,37 @@ struct Work {
 // plan; the global entries use the defaults).
 struct LaunchCfg {
     int root_bt = 128;      // root_kernel threads per block: 64, 128, 256
+    int root_minb = 0;      // root_kernel blocks per SM of the register budget: 0, 5 (128), 10 (64)
     int adj_minb = 3;       // adjoint_kernel blocks per SM: 2, 3, 4
     int ti_minb = 8;        // ti_kernel blocks per SM: 4, 6, 8
 };
+
+// Root-search variants (threads per block, register-budget blocks per SM).
+constexpr int kRootVariants[5][2] = {{64, 0}, {128, 0}, {256, 0}, {128, 5}, {64, 10}};
+
+// Launch configuration of the per-call entries: the defaults, or
+// DAZI_DK_LAUNCH="root=BT[xMINB],adj=MINB,ti=MINB" (values outside the
+// instantiated variants are ignored).
+LaunchCfg default_cfg()
+{
+    static LaunchCfg cfg;
+    static bool done = false;
+    if (done) return cfg;
+    done = true;
+    const char* e = std::getenv("DAZI_DK_LAUNCH");
+    if (!e) return cfg;
+    int a = 0, b = 0;
+    const char* r = std::strstr(e, "root=");
+    if (r && std::sscanf(r + 5, "%dx%d", &a, &b) >= 1) {
+        for (const auto& v : kRootVariants)
+            if (v[0] == a && v[1] == b) { cfg.root_bt = a; cfg.root_minb = b; }
+    }
+    const char* j = std::strstr(e, "adj=");
+    if (j && std::sscanf(j + 4, "%d", &a) == 1 && a >= 2 && a <= 4) cfg.adj_minb = a;
+    const char* t = std::strstr(e, "ti=");
+    if (t && std::sscanf(t + 3, "%d", &a) == 1 && (a == 4 || a == 6 || a == 8)) cfg.ti_minb = a;
+    return cfg;
+}
 
 // Optional per-phase timing with CUDA events on the call's stream.
 struct PhaseTimer {
@@ -320,11 +349,6 @@ int build_tables(const ColSrc& src, long long ncols, const PrepOut& po, long lon
 }
 
 // Kernel variants (instantiations of the templated kernels).
-const void* root_fn(int bt)
-{
-    return bt == 64 ? (const void*)root_kernel<64> : bt == 256 ? (const void*)root_kernel<256>
-                                                               : (const void*)root_kernel<128>;
-}
 const void* adjoint_fn(int minb)
 {
     return minb == 2 ? (const void*)adjoint_kernel<2> : minb == 4 ? (const void*)adjoint_kernel<4>
@@ -378,11 +402,13 @@ int run_root(const Tables& T, const double* per, const StageOut& o, int form, bo
     a.pv = o.pv; a.croot = adj ? W.croot.as<double>() : nullptr; a.status = o.status;
     a.nevals = W.counters.as<unsigned long long>();
     a.scan32 = (form & DAZI_FORM_SCAN_FP32) ? 1 : 0;
-    const int bt = cfg.root_bt;
+    const int bt = cfg.root_bt, mb = cfg.root_minb;
     const unsigned nb = (unsigned)((T.ncols + bt - 1) / bt);
-    if (bt == 64) root_kernel<64><<<nb, 64, 0, st>>>(a);
-    else if (bt == 256) root_kernel<256><<<nb, 256, 0, st>>>(a);
-    else root_kernel<128><<<nb, 128, 0, st>>>(a);
+    if (bt == 64 && mb == 10) root_kernel<64, 10><<<nb, 64, 0, st>>>(a);
+    else if (bt == 64) root_kernel<64, 0><<<nb, 64, 0, st>>>(a);
+    else if (bt == 256) root_kernel<256, 0><<<nb, 256, 0, st>>>(a);
+    else if (mb == 5) root_kernel<128, 5><<<nb, 128, 0, st>>>(a);
+    else root_kernel<128, 0><<<nb, 128, 0, st>>>(a);
     CK(cudaGetLastError());
     ++g_ctx.last_launches;
     phase_mark("root", st);
@@ -502,7 +528,7 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
     PrepOut po{nullptr, nullptr, g_ctx.w.counters.as<unsigned long long>() + 4};
     Tables T;
     if ((r = build_tables(src, col_count, po, ncol, ncol, ncol, st, T, g_ctx.w))) return r;
-    return run_tables(T, per, o, form, fd, st, g_ctx.w, LaunchCfg());
+    return run_tables(T, per, o, form, fd, st, g_ctx.w, default_cfg());
 }
 
 // Ragged batch on device pointers.
@@ -575,7 +601,7 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
         }
         phase_mark("fd", st);
     }
-    return run_tables(T, B.periods, o, form, fd, st, g_ctx.w, LaunchCfg());
+    return run_tables(T, B.periods, o, form, fd, st, g_ctx.w, default_cfg());
 }
 
 // ------------------------------------------------------------------ plans
@@ -641,18 +667,20 @@ int time_phase(Plan& P, F launch, float& ms)
 int plan_tune(Plan& P)
 {
     int r;
-    const int root_c[3] = {64, 128, 256}, adj_c[3] = {2, 3, 4}, ti_c[3] = {4, 6, 8};
+    const int adj_c[3] = {2, 3, 4}, ti_c[3] = {4, 6, 8};
     LaunchCfg c = P.cfg;
     float best = 1e30f;
-    for (int bt : root_c) {
-        c.root_bt = bt;
+    for (const auto& v : kRootVariants) {
+        c.root_bt = v[0];
+        c.root_minb = v[1];
         float ms;
         if ((r = time_phase(P, [&] { return run_root(P.T, P.periods, P.o, P.form, P.adj, P.w, c, P.cs); }, ms)))
             return r;
-        if (ms < best) { best = ms; P.cfg.root_bt = bt; }
+        if (ms < best) { best = ms; P.cfg.root_bt = v[0]; P.cfg.root_minb = v[1]; }
     }
     P.best_ms[0] = best;
     c.root_bt = P.cfg.root_bt;
+    c.root_minb = P.cfg.root_minb;
     if (P.adj) {
         best = 1e30f;
         for (int mb : adj_c) {
@@ -1194,7 +1222,7 @@ int dazi_dk_plan_config(void* plan, int* root_block, int* adjoint_blocks_per_sm,
 {
     if (!plan) { set_err("null plan"); return DAZI_ERR_BADARG; }
     const Plan* P = static_cast<const Plan*>(plan);
-    if (root_block) *root_block = P->cfg.root_bt;
+    if (root_block) *root_block = P->cfg.root_bt * 100 + P->cfg.root_minb;
     if (adjoint_blocks_per_sm) *adjoint_blocks_per_sm = P->cfg.adj_minb;
     if (ti_blocks_per_sm) *ti_blocks_per_sm = P->cfg.ti_minb;
     if (tuned_ms) for (int i = 0; i < 3; ++i) tuned_ms[i] = P->best_ms[i];

@@ -113,7 +113,7 @@ __global__ void prep_tasks_kernel(long long ntiles, const long long* tile_tasks,
                                   const long long* tile_tbase, int2* tasks);
 __global__ void prep_build_kernel(ColSrc src, PrepOut o, Tables T, const int* sorted_col,
                                   const long long* tile_tbase);
-template <int BT> __global__ void root_kernel(RootArgs a);        // BT in {64, 128, 256}
+template <int BT, int MINB> __global__ void root_kernel(RootArgs a);  // (64|128|256, 0), (128, 5), (64, 10)
 template <int MINB> __global__ void adjoint_kernel(AdjArgs a);    // MINB in {2, 3, 4}
 template <int MINB> __global__ void ti_kernel(TiArgs a);          // MINB in {4, 6, 8}
 

@@ -245,10 +245,11 @@ struct TableModel {
     __device__ __forceinline__ float4 layerf(int m) const { return flat[base + (long long)m * TILE]; }
 };
 
-// BT: threads per block (one thread per column; the autotuner picks one of
-// the instantiations).
-template <int BT>
-__global__ void __launch_bounds__(BT)
+// BT: threads per block (one thread per column); MINB: minimum resident
+// blocks per SM the register allocation aims for (0: no constraint).  The
+// autotuner picks one of the instantiations.
+template <int BT, int MINB>
+__global__ void __launch_bounds__(BT, MINB)
 root_kernel(RootArgs a)
 {
     const Tables& T = a.T;
@@ -280,8 +281,10 @@ root_kernel(RootArgs a)
     }
 }
 
-template __global__ void root_kernel<64>(RootArgs);
-template __global__ void root_kernel<128>(RootArgs);
-template __global__ void root_kernel<256>(RootArgs);
+template __global__ void root_kernel<64, 0>(RootArgs);
+template __global__ void root_kernel<128, 0>(RootArgs);
+template __global__ void root_kernel<256, 0>(RootArgs);
+template __global__ void root_kernel<128, 5>(RootArgs);
+template __global__ void root_kernel<64, 10>(RootArgs);
 
 }  // namespace dk

@@ -71,7 +71,8 @@ class BatchPlan:
         ms = (ctypes.c_float * 3)()
         _lib.check(self.L.dazi_dk_plan_config(self.handle, ctypes.byref(a), ctypes.byref(b),
                                               ctypes.byref(c), ms))
-        return {"root_block": a.value, "adjoint_blocks_per_sm": b.value,
+        return {"root_block": a.value // 100, "root_blocks_per_sm": a.value % 100,
+                "adjoint_blocks_per_sm": b.value,
                 "ti_blocks_per_sm": c.value, "tuned_ms": list(ms)}
 
     def close(self):

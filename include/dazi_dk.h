@@ -208,8 +208,11 @@ int dazi_dk_plan_create(long long ncols, const long long *node_off,
                         int *status, int tune, void *stream, void **plan);
 int dazi_dk_plan_launch(void *plan, void *stream);
 int dazi_dk_plan_status(void *plan);
-/* The tuner's choice: root-search threads per block, blocks per SM of the
- * adjoint and Gc/Gs sweeps, and their tuned phase times (ms, 3 floats). */
+/* The tuner's choice: root-search variant (100 x threads per block +
+ * register-budget blocks per SM, 0 = unconstrained), blocks per SM of the
+ * adjoint and Gc/Gs sweeps, and their tuned phase times (ms, 3 floats).
+ * The per-call entries use 128x0 / 3 / 8, or the environment variable
+ * DAZI_DK_LAUNCH="root=BT[xMINB],adj=MINB,ti=MINB" when set. */
 int dazi_dk_plan_config(void *plan, int *root_block, int *adjoint_blocks_per_sm,
                         int *ti_blocks_per_sm, float *tuned_ms);
 int dazi_dk_plan_destroy(void *plan);

@@ -107,7 +107,7 @@ extern "C" int emu_root_batch(long long ncols, const long long* node_off, const 
     for (long long s = 0; s < ncols; ++s) {
         blockIdx.x = (unsigned)(s / 128);
         threadIdx.x = (unsigned)(s % 128);
-        root_kernel<128>(a);
+        root_kernel<128, 0>(a);
     }
     *evals = (long long)counters[0];
     return 0;
