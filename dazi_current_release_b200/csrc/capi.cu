@@ -137,6 +137,8 @@ struct Context {
     // per-call layer tables, counters and sweep scratch
     Work w;
     DBuf cbufoff;
+    // G-row epilogue: ray offsets, scan storage, error flag
+    DBuf goff, gtmp, gerr;
     // batch staging (host entry)
     DBuf bnode, bper, bdep, bvs, bvp, brho, bperiods, bsenoff, blsoff, bpv, bsvs, bsvp, bsrh, blsen, bstatus;
     int last_launches = 0;
@@ -1240,6 +1242,64 @@ int dazi_dk_plan_destroy(void* plan)
     P->release();
     if (cur != P->device) cudaSetDevice(cur);
     delete P;
+    return 0;
+}
+
+int dazi_dk_grows_dev(int nvx, int nvz, int nz, int kmaxRc, const float* vels, const double* sen_vsRc,
+                      const double* sen_vpRc, const double* sen_rhoRc, const float* Lsen_Gsc,
+                      long long nrays, const int* ray_period, const int* ray_id,
+                      const long long* cell_off, const int* cell, const float* fdm,
+                      const float* fdmc, const float* fdms, float ftol, long long cap, float* rw,
+                      int* iw, int* col, long long* nnz_ray, long long* nnz_total, void* stream)
+{
+    if (nvx < 1 || nvz < 1 || nz < 2 || nz > NZMAX || kmaxRc < 1 || kmaxRc > NP || nrays < 0) {
+        set_err("grid or ray count out of range");
+        return DAZI_ERR_BADARG;
+    }
+    if (!vels || !sen_vsRc || !sen_vpRc || !sen_rhoRc || !ray_period || !ray_id || !cell_off ||
+        !cell || !fdm || !nnz_ray || !nnz_total || (Lsen_Gsc && (!fdmc || !fdms)) ||
+        (cap > 0 && (!rw || !iw || !col))) {
+        set_err("null argument");
+        return DAZI_ERR_BADARG;
+    }
+    if (!(ftol >= 0.f) || !std::isfinite(ftol)) { set_err("ftol must be >= 0"); return DAZI_ERR_BADARG; }
+    *nnz_total = 0;
+    if (nrays == 0) return 0;
+    std::lock_guard<std::mutex> lk(g_mu);
+    int r;
+    if ((r = ensure_context())) return r;
+    cudaStream_t st = (cudaStream_t)stream;
+    if ((r = g_ctx.goff.ensure(sizeof(long long) * (nrays + 1))) || (r = g_ctx.gerr.ensure(sizeof(int) * 4)))
+        return r;
+    CK(cudaMemsetAsync(g_ctx.gerr.p, 0, sizeof(int), st));
+    GrowsArgs a;
+    a.nvx = nvx; a.nvz = nvz; a.nz = nz; a.K = kmaxRc;
+    a.vels = vels; a.svs = sen_vsRc; a.svp = sen_vpRc; a.srh = sen_rhoRc; a.lsen = Lsen_Gsc;
+    a.nrays = nrays; a.ray_period = ray_period; a.ray_id = ray_id; a.cell_off = cell_off; a.cell = cell;
+    a.fdm = fdm; a.fdmc = fdmc; a.fdms = fdms; a.ftol = ftol;
+    a.nnz_ray = nnz_ray; a.off = g_ctx.goff.as<long long>();
+    a.rw = rw; a.iw = iw; a.col = col; a.err = g_ctx.gerr.as<int>();
+    const unsigned nb = (unsigned)((nrays * 32 + 127) / 128);
+    grows_kernel<false><<<nb, 128, 0, st>>>(a);
+    CK(cudaGetLastError());
+    size_t tb = 0;
+    CK(cub::DeviceScan::ExclusiveSum(nullptr, tb, nnz_ray, g_ctx.goff.as<long long>(), (int)nrays, st));
+    if ((r = g_ctx.gtmp.ensure(tb + 16))) return r;
+    CK(cub::DeviceScan::ExclusiveSum(g_ctx.gtmp.p, tb, nnz_ray, g_ctx.goff.as<long long>(), (int)nrays, st));
+    long long last[2] = {0, 0};
+    int herr = 0;
+    CK(cudaMemcpyAsync(&last[0], g_ctx.goff.as<long long>() + nrays - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&last[1], nnz_ray + nrays - 1, sizeof(long long), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(&herr, g_ctx.gerr.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (herr) { set_err("invalid ray: period index, or cells not ascending inside the grid"); return DAZI_ERR_BADARG; }
+    *nnz_total = last[0] + last[1];
+    if (*nnz_total > cap) {
+        set_err("%lld entries exceed the capacity %lld", *nnz_total, cap);
+        return DAZI_ERR_LIMITS;
+    }
+    grows_kernel<true><<<nb, 128, 0, st>>>(a);
+    CK(cudaGetLastError());
     return 0;
 }
 

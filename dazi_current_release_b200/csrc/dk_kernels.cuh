@@ -71,6 +71,33 @@ struct TiArgs {
     int* errflag;           // set to 1 when an Lsen_Gsc value is not finite
 };
 
+// G-row epilogue (k_grows.cu): kernels of the grid interface to sparse
+// rows of the LSMR system.
+struct GrowsArgs {
+    int nvx, nvz, nz, K;
+    const float* vels;              // (nvx+2, nvz+2, nz) real*4
+    const double* svs;              // (nxy, K, nz) real*8
+    const double* svp;
+    const double* srh;
+    const float* lsen;              // (nxy, K, nz-1) real*4, or nullptr (isotropic rows)
+    long long nrays;
+    const int* ray_period;          // 0-based period index of each ray
+    const int* ray_id;              // data-row id of each ray (iw)
+    const long long* cell_off;      // CSR over rays
+    const int* cell;                // (jj-1)*nvx + kk-1, ascending within a ray
+    const float* fdm;
+    const float* fdmc;
+    const float* fdms;
+    float ftol;
+    long long* nnz_ray;             // count pass: entries per ray
+    const long long* off;           // fill pass: first entry of each ray
+    float* rw;
+    int* iw;
+    int* col;
+    int* err;                       // bit 1: invalid ray
+};
+template <bool FILL> __global__ void grows_kernel(GrowsArgs a);
+
 // Column source: regular grid (Fortran (nx,ny,nz) arrays, shared depz and
 // periods) or ragged batch (CSR node and period arrays).
 struct ColSrc {

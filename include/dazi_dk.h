@@ -217,6 +217,30 @@ int dazi_dk_plan_config(void *plan, int *root_block, int *adjoint_blocks_per_sm,
                         int *ti_blocks_per_sm, float *tuned_ms);
 int dazi_dk_plan_destroy(void *plan);
 
+/* G rows of the LSMR system from the kernels: the consumer of the stage,
+ * CalSurfG_parallel.f90:2363-2400 (iso_phase_only, use_aniso_active), on
+ * device pointers.  Grid interface: nvx x nvz inner model cells, kernel
+ * arrays of the (nvx+2) x (nvz+2) grid in the reference's layouts
+ * (sen_*Rc (nxy, kmaxRc, nz) real*8, Lsen_Gsc (nxy, kmaxRc, nz-1) real*4, or
+ * NULL for isotropic rows), vels (nvx+2, nvz+2, nz) real*4.  Rays in CSR:
+ * ray r (data row ray_id[r], period index ray_period[r], 0-based) crosses
+ * cells cell[cell_off[r] .. cell_off[r+1]-1] ((jj-1)*nvx + kk-1, strictly
+ * ascending) with path weights fdm (and fdmc, fdms for Gc, Gs).  Writes
+ * the entries |row| > ftol in the reference's order: rw (real*4), iw (ray
+ * id), col (1-based parameter: iso block, then Gc, then Gs, each ordered
+ * by depth interval then cell), the count of every ray in nnz_ray
+ * (device) and the total in *nnz_total (host).  Returns DAZI_ERR_LIMITS
+ * (with *nnz_total set) when the total exceeds cap; one small
+ * synchronisation sizes the output. */
+int dazi_dk_grows_dev(int nvx, int nvz, int nz, int kmaxRc, const float *vels,
+                      const double *sen_vsRc, const double *sen_vpRc,
+                      const double *sen_rhoRc, const float *Lsen_Gsc,
+                      long long nrays, const int *ray_period, const int *ray_id,
+                      const long long *cell_off, const int *cell,
+                      const float *fdm, const float *fdmc, const float *fdms,
+                      float ftol, long long cap, float *rw, int *iw, int *col,
+                      long long *nnz_ray, long long *nnz_total, void *stream);
+
 /* Per-phase timing: with dazi_dk_set_timing(1), each call records CUDA
  * events on its stream around its phases ("prep", "fd", "root", "adjoint",
  * "ti"); dazi_dk_last_timing fills up to cap (name, milliseconds) pairs of

@@ -78,6 +78,11 @@ def lib():
         L.or_batch.argtypes = [ctypes.c_long, _i64p, _f32p, _f32p, _i64p, _f64p, ctypes.c_float,
                                _f64p, _i64p, _f64p, _f64p, _f64p, _i64p, _f32p, ctypes.c_int]
         L.or_batch.restype = ctypes.c_int
+        L.or_grows.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f64p,
+                               _f64p, _f64p, _f32p, ctypes.c_long, _i32p, _i32p, _i64p, _i32p,
+                               _f32p, _f32p, _f32p, ctypes.c_float, ctypes.c_long, _f32p, _i32p,
+                               _i32p, _i64p]
+        L.or_grows.restype = ctypes.c_long
         _lib = L
     return _lib
 
@@ -266,3 +271,35 @@ def batch(node_off, depz, vs, per_off, periods, minthk, kernels=True, lsen=True,
         raise RuntimeError("oracle batch failed")
     return dict(pv=pv, sen_vs=sen[0], sen_vp=sen[1], sen_rho=sen[2], lsen=ls,
                 sen_off=sen_off, ls_off=ls_off)
+
+
+def grows(nvx, nvz, vels, sen_vs, sen_vp, sen_rho, lsen, ray_period, ray_id, cell_off, cell, fdm,
+          fdmc=None, fdms=None, ftol=1e-4, cap=None):
+    """Oracle of the G-row epilogue (CalSurfG_parallel.f90:2363-2400):
+    sparse entries (rw float32, iw ray id, col 1-based parameter) and the
+    entry count of every ray.  vels (nvx+2, nvz+2, nz) float32, kernels
+    (nxy, K, nz) float64, lsen (nxy, K, nz-1) float32 or None."""
+    vels = np.asfortranarray(vels, np.float32)
+    nz = vels.shape[2]
+    K = sen_vs.shape[1]
+    f64 = lambda a: np.asfortranarray(a, np.float64)  # noqa: E731
+    ls = None if lsen is None else np.asfortranarray(lsen, np.float32)
+    cell_off = np.ascontiguousarray(cell_off, np.int64)
+    nrays = cell_off.size - 1
+    i32 = lambda a: np.ascontiguousarray(a, np.int32)  # noqa: E731
+    f32 = lambda a: None if a is None else np.ascontiguousarray(a, np.float32)  # noqa: E731
+    if cap is None:
+        cap = int(cell_off[-1]) * (nz - 1) * (3 if ls is not None else 1) + 1
+    rw = np.zeros(cap, np.float32)
+    iw = np.zeros(cap, np.int32)
+    col = np.zeros(cap, np.int32)
+    nnz = np.zeros(max(nrays, 1), np.int64)
+    a = [i32(ray_period), i32(ray_id), i32(cell), f32(fdm), f32(fdmc), f32(fdms)]
+    n = lib().or_grows(nvx, nvz, nz, K, _p(vels, _f32p), _p(f64(sen_vs), _f64p),
+                       _p(f64(sen_vp), _f64p), _p(f64(sen_rho), _f64p), _p(ls, _f32p), nrays,
+                       _p(a[0], _i32p), _p(a[1], _i32p), _p(cell_off, _i64p), _p(a[2], _i32p),
+                       _p(a[3], _f32p), _p(a[4], _f32p), _p(a[5], _f32p), ctypes.c_float(ftol),
+                       cap, _p(rw, _f32p), _p(iw, _i32p), _p(col, _i32p), _p(nnz, _i64p))
+    if n < 0:
+        raise RuntimeError("oracle grows: capacity exceeded or invalid cell")
+    return rw[:n], iw[:n], col[:n], nnz[:nrays]

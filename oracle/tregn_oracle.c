@@ -915,3 +915,80 @@ int or_batch(long ncols, const long *node_off, const float *depz, const float *v
     }
     return bad ? -1 : 0;
 }
+
+/* G rows of the LSMR system from the depth kernels, CalSurfG_parallel.f90
+ * :2363-2400 (iso_phase_only, use_aniso_active): for each ray (a data row,
+ * id ray_id[r], period index ray_period[r]) and each of its model cells
+ * with |fdm| >= ftol (cell = (jj-1)*nvx + kk-1 of the nvx x nvz inner grid,
+ * ascending within the ray), the dense parameter row
+ *   row(i, cell)            = (sen_vp*coe_a + sen_rho*coe_rho + sen_vs)*fdm
+ *   row(nparpi + i, cell)   = Lsen*fdmc,  row(2 nparpi + i, cell) = Lsen*fdms
+ * (i = 1..nz-1, real*4 row; coe_a, coe_rho the Brocher derivatives at the
+ * node velocity in real*4), then the entries |row| > ftol in parameter
+ * order as (rw real*4, iw = ray id, col 1-based).  Kernel column of cell
+ * (kk, jj): post = jj*(nvx+2)+kk (0-based), arrays in the reference's
+ * layouts.  lsen == NULL: isotropic rows only.  Returns the number of
+ * entries, or -1 when cap is exceeded / a cell index is invalid. */
+static inline float or_coe_a(float v)
+{
+    const float v2 = v * v, v3 = v2 * v;
+    return ((2.0947f - (float)(0.8206f * 2.0f) * v) + (float)(0.2683f * 3.0f) * v2) - (float)(0.0251f * 4.0f) * v3;
+}
+
+static inline float or_coe_rho(float v, float ca)
+{
+    const float v2 = v * v, v3 = v2 * v, v4 = v2 * v2;
+    const float vp = (((0.9409f + 2.0947f * v) - 0.8206f * v2) + 0.2683f * v3) - 0.0251f * v4;
+    const float p2 = vp * vp, p3 = p2 * vp, p4 = p2 * p2;
+    const float poly = (((1.6612f - (float)(0.4721f * 2.0f) * vp) + (float)(0.0671f * 3.0f) * p2)
+                        - (float)(0.0043f * 4.0f) * p3) + (float)(0.000106f * 5.0f) * p4;
+    return ca * poly;
+}
+
+long or_grows(int nvx, int nvz, int nz, int K, const float *vels, const double *svs,
+              const double *svp, const double *srh, const float *lsen, long nrays,
+              const int *ray_period, const int *ray_id, const long *cell_off, const int *cell,
+              const float *fdm, const float *fdmc, const float *fdms, float ftol, long cap,
+              float *rw, int *iw, int *col, long *nnz_ray)
+{
+    const int nx = nvx + 2, ny = nvz + 2;
+    const long nxy = (long)nx * ny, ncell = (long)nvx * nvz;
+    const long nparpi = ncell * (nz - 1);
+    const int nblk = lsen ? 3 : 1;
+    float *row = malloc(sizeof(float) * nparpi * nblk);
+    if (!row) return -1;
+    long out = 0;
+    for (long r = 0; r < nrays; ++r) {
+        memset(row, 0, sizeof(float) * nparpi * nblk);
+        const int k = ray_period[r];
+        for (long e = cell_off[r]; e < cell_off[r + 1]; ++e) {
+            const int c = cell[e];
+            if (c < 0 || c >= ncell) { free(row); return -1; }
+            if (!(fabsf(fdm[e]) >= ftol)) continue;
+            const int kk = c % nvx + 1, jj = c / nvx + 1;
+            const long post = (long)jj * nx + kk;
+            for (int i = 0; i < nz - 1; ++i) {
+                const float v = vels[post + nxy * i];
+                const float ca = or_coe_a(v), cr = or_coe_rho(v, ca);
+                const long ks = post + nxy * (k + (long)K * i);
+                const double s = (svp[ks] * (double)ca + srh[ks] * (double)cr) + svs[ks];
+                row[(long)i * ncell + c] = (float)(s * (double)fdm[e]);
+                if (lsen) {
+                    const float L = lsen[post + nxy * (k + (long)K * i)];
+                    row[nparpi + (long)i * ncell + c] = L * fdmc[e];
+                    row[2 * nparpi + (long)i * ncell + c] = L * fdms[e];
+                }
+            }
+        }
+        long n = 0;
+        for (long q = 0; q < nparpi * nblk; ++q)
+            if (fabsf(row[q]) > ftol) {
+                if (out >= cap) { free(row); return -1; }
+                rw[out] = row[q]; iw[out] = ray_id[r]; col[out] = (int)(q + 1);
+                ++out; ++n;
+            }
+        if (nnz_ray) nnz_ray[r] = n;
+    }
+    free(row);
+    return out;
+}
