@@ -36,6 +36,7 @@ EXPORTS = (
     "dazi_dk_iso_noalloc_dev", "dazi_dk_batch", "dazi_dk_batch_dev", "dazi_dk_set_timing",
     "dazi_dk_last_timing", "dazi_dk_last_items", "dazi_dk_plan_create", "dazi_dk_plan_launch",
     "dazi_dk_plan_status", "dazi_dk_plan_config", "dazi_dk_plan_destroy", "dazi_dk_grows_dev",
+    "dazi_dk_azimuthal_map_dev",
 )
 
 
@@ -122,6 +123,8 @@ def load(build_if_missing: bool = True):
     L.dazi_dk_grows_dev.argtypes = ([_int] * 4 + [vp_] * 5 + [ll] + [vp_] * 7 + [ctypes.c_float, ll] +
                                     [vp_] * 4 + [ctypes.POINTER(ctypes.c_longlong), vp_])
     L.dazi_dk_grows_dev.restype = _int
+    L.dazi_dk_azimuthal_map_dev.argtypes = [_int] * 4 + [vp_] * 10
+    L.dazi_dk_azimuthal_map_dev.restype = _int
     L.dazi_dk_fp64_peak.argtypes = [_f64p]
     L.dazi_dk_fp64_peak.restype = _int
     L.dazi_dk_finalize.argtypes = []

@@ -1303,6 +1303,31 @@ int dazi_dk_grows_dev(int nvx, int nvz, int nz, int kmaxRc, const float* vels, c
     return 0;
 }
 
+int dazi_dk_azimuthal_map_dev(int nx, int ny, int nz, int kmaxRc, const float* Lsen_Gsc,
+                              const float* gcf, const float* gsf, const double* tRcV, float* cosRc,
+                              float* sinRc, float* amp, float* amp_rel, float* angle, void* stream)
+{
+    if (nx < 3 || ny < 3 || nz < 2 || nz > NZMAX || kmaxRc < 1 || kmaxRc > NP) {
+        set_err("grid out of range");
+        return DAZI_ERR_BADARG;
+    }
+    if (!Lsen_Gsc || !gcf || !gsf || !tRcV || !cosRc || !sinRc || !amp || !amp_rel || !angle) {
+        set_err("null argument");
+        return DAZI_ERR_BADARG;
+    }
+    std::lock_guard<std::mutex> lk(g_mu);
+    int r;
+    if ((r = ensure_context())) return r;
+    AzimapArgs a;
+    a.nvx = nx - 2; a.nvz = ny - 2; a.nz = nz; a.K = kmaxRc;
+    a.lsen = Lsen_Gsc; a.gc = gcf; a.gs = gsf; a.ciso = tRcV;
+    a.cosr = cosRc; a.sinr = sinRc; a.amp = amp; a.rela = amp_rel; a.ang = angle;
+    const long long n = (long long)a.nvx * a.nvz * kmaxRc;
+    azimap_kernel<<<(unsigned)((n + 127) / 128), 128, 0, (cudaStream_t)stream>>>(a);
+    CK(cudaGetLastError());
+    return 0;
+}
+
 const char* dazi_dk_last_error(void) { return g_err; }
 
 int dazi_dk_version(void) { return 100; }

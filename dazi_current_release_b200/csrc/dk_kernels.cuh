@@ -98,6 +98,21 @@ struct GrowsArgs {
 };
 template <bool FILL> __global__ void grows_kernel(GrowsArgs a);
 
+// Azimuthal phase-velocity maps (k_epilogue.cu).
+struct AzimapArgs {
+    int nvx, nvz, nz, K;
+    const float* lsen;              // (nxy, K, nz-1) of the (nvx+2) x (nvz+2) grid
+    const float* gc;                // (nvx, nvz, nz-1)
+    const float* gs;
+    const double* ciso;             // (nvx*nvz, K) isotropic phase velocity (tRcV)
+    float* cosr;                    // (nvx*nvz, K) outputs
+    float* sinr;
+    float* amp;
+    float* rela;
+    float* ang;
+};
+__global__ void azimap_kernel(AzimapArgs a);
+
 // Column source: regular grid (Fortran (nx,ny,nz) arrays, shared depz and
 // periods) or ragged batch (CSR node and period arrays).
 struct ColSrc {

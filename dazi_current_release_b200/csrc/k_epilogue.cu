@@ -1,3 +1,6 @@
+// Epilogues of the stage: the G rows of the LSMR system and the azimuthal
+// phase-velocity maps.
+//
 // G rows of the LSMR system from the depth kernels (the consumer of the
 // stage, CalSurfG_parallel.f90:2363-2400, iso_phase_only with
 // use_aniso_active).  For each ray (a data row) and each model cell of its
@@ -109,5 +112,43 @@ __global__ void __launch_bounds__(128) grows_kernel(GrowsArgs a)
 
 template __global__ void grows_kernel<false>(GrowsArgs);
 template __global__ void grows_kernel<true>(GrowsArgs);
+
+// Azimuthal phase-velocity maps, FwdAzimuthalAniMap.f90:43-86: per inner
+// column (ii, jj) and period tt,
+//   cos = sum_k Lsen(k) gc(k),  sin = sum_k Lsen(k) gs(k)   (real*4, k ascending)
+//   amp = 0.5 sqrt(cos^2 + sin^2),  rela = amp / c_iso,
+//   ang = 0.5 (atan2(sin, cos) / pi * 180, + 360 when negative)
+// with the reference's real*4 / real*8 mix (pi real*8, the angle stored
+// real*4).  Outputs indexed (jj-1)*nvx + ii-1 + nvx*nvz*(tt-1).
+__global__ void __launch_bounds__(128) azimap_kernel(AzimapArgs a)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long ncell = (long long)a.nvx * a.nvz;
+    if (t >= ncell * a.K) return;
+    const int tt = (int)(t / ncell);
+    const long long c = t % ncell;
+    const int ii = (int)(c % a.nvx) + 1, jj = (int)(c / a.nvx) + 1;
+    const int nx = a.nvx + 2;
+    const long long nxy = (long long)nx * (a.nvz + 2);
+    const long long post = (long long)jj * nx + ii;
+    float cs = 0.0f, sn = 0.0f;
+    for (int k = 0; k < a.nz - 1; ++k) {
+        const float L = a.lsen[post + nxy * (tt + (long long)a.K * k)];
+        const long long g = (ii - 1) + (long long)a.nvx * ((jj - 1) + (long long)a.nvz * k);
+        cs = __fadd_rn(cs, __fmul_rn(L, a.gc[g]));
+        sn = __fadd_rn(sn, __fmul_rn(L, a.gs[g]));
+    }
+    const float amp = __fmul_rn(0.5f, __fsqrt_rn(__fadd_rn(__fmul_rn(cs, cs), __fmul_rn(sn, sn))));
+    const float iso = (float)a.ciso[c + ncell * tt];
+    const double pi = 3.1415926535898;
+    float ang = (float)__dmul_rn(__ddiv_rn((double)atan2f(sn, cs), pi), 180.0);
+    if (ang < 0.0f) ang = __fadd_rn(ang, 360.0f);
+    ang = __fmul_rn(0.5f, ang);
+    a.cosr[t] = cs;
+    a.sinr[t] = sn;
+    a.amp[t] = amp;
+    a.rela[t] = __fdiv_rn(amp, iso);
+    a.ang[t] = ang;
+}
 
 }  // namespace dk

@@ -241,6 +241,20 @@ int dazi_dk_grows_dev(int nvx, int nvz, int nz, int kmaxRc, const float *vels,
                       float ftol, long long cap, float *rw, int *iw, int *col,
                       long long *nnz_ray, long long *nnz_total, void *stream);
 
+/* Azimuthal phase-velocity maps, replacing the computation of
+ * FwdAzimuthalAniMap (code/src_inv_iso_joint/FwdAzimuthalAniMap.f90:43-86),
+ * device pointers: from Lsen_Gsc (nx*ny, kmaxRc, nz-1) real*4, the Gc/Gs
+ * model gcf, gsf (nx-2, ny-2, nz-1) real*4 and the isotropic phase velocity
+ * tRcV ((nx-2)*(ny-2), kmaxRc) real*8, every inner column and period gets
+ * cosRc = sum Lsen gc, sinRc = sum Lsen gs, amp = 0.5 sqrt(cos^2 + sin^2),
+ * amp_rel = amp / tRcV and the fast-axis angle (degrees, [0, 180)), all
+ * ((nx-2)*(ny-2), kmaxRc) real*4.  Stream-ordered on `stream`. */
+int dazi_dk_azimuthal_map_dev(int nx, int ny, int nz, int kmaxRc,
+                              const float *Lsen_Gsc, const float *gcf,
+                              const float *gsf, const double *tRcV,
+                              float *cosRc, float *sinRc, float *amp,
+                              float *amp_rel, float *angle, void *stream);
+
 /* Per-phase timing: with dazi_dk_set_timing(1), each call records CUDA
  * events on its stream around its phases ("prep", "fd", "root", "adjoint",
  * "ti"); dazi_dk_last_timing fills up to cap (name, milliseconds) pairs of

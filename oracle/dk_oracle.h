@@ -61,6 +61,8 @@ long or_grows(int nvx, int nvz, int nz, int K, const float *vels, const double *
               const int *ray_period, const int *ray_id, const long *cell_off, const int *cell,
               const float *fdm, const float *fdmc, const float *fdms, float ftol, long cap,
               float *rw, int *iw, int *col, long *nnz_ray);
+void or_azimap(int nx, int ny, int nz, int K, const float *lsen, const float *gc, const float *gs,
+               const double *ciso, float *cosr, float *sinr, float *amp, float *rela, float *ang);
 #ifdef __cplusplus
 }
 #endif

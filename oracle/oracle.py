@@ -83,6 +83,8 @@ def lib():
                                _f32p, _f32p, _f32p, ctypes.c_float, ctypes.c_long, _f32p, _i32p,
                                _i32p, _i64p]
         L.or_grows.restype = ctypes.c_long
+        L.or_azimap.argtypes = [ctypes.c_int] * 4 + [_f32p] * 3 + [_f64p] + [_f32p] * 5
+        L.or_azimap.restype = None
         _lib = L
     return _lib
 
@@ -303,3 +305,18 @@ def grows(nvx, nvz, vels, sen_vs, sen_vp, sen_rho, lsen, ray_period, ray_id, cel
     if n < 0:
         raise RuntimeError("oracle grows: capacity exceeded or invalid cell")
     return rw[:n], iw[:n], col[:n], nnz[:nrays]
+
+
+def azimap(lsen, gc, gs, ciso):
+    """Oracle of FwdAzimuthalAniMap.f90:43-86.  lsen (nx*ny, K, nz-1) on the
+    (nx, ny) grid, gc/gs (nx-2, ny-2, nz-1), ciso ((nx-2)*(ny-2), K).
+    Returns cos, sin, amp, amp_rel, angle, each ((nx-2)*(ny-2), K) float32."""
+    gc = np.asfortranarray(gc, np.float32)
+    nvx, nvz, nzm1 = gc.shape
+    nx, ny, nz = nvx + 2, nvz + 2, nzm1 + 1
+    K = lsen.shape[1]
+    out = [np.zeros((nvx * nvz, K), np.float32, order="F") for _ in range(5)]
+    lib().or_azimap(nx, ny, nz, K, _p(np.asfortranarray(lsen, np.float32), _f32p), _p(gc, _f32p),
+                    _p(np.asfortranarray(gs, np.float32), _f32p),
+                    _p(np.asfortranarray(ciso, np.float64), _f64p), *[_p(o, _f32p) for o in out])
+    return tuple(out)

@@ -992,3 +992,36 @@ long or_grows(int nvx, int nvz, int nz, int K, const float *vels, const double *
     free(row);
     return out;
 }
+
+/* FwdAzimuthalAniMap.f90:43-86: per inner column and period the real*4
+ * sums cos = sum Lsen gc, sin = sum Lsen gs (intervals ascending), the
+ * amplitude 0.5 sqrt(cos^2 + sin^2), its ratio to the isotropic phase
+ * velocity (real*4) and the fast-axis angle 0.5 (atan2(sin, cos)/pi*180
+ * [+360]) with pi real*8.  Outputs ((nx-2)*(ny-2), K) real*4. */
+void or_azimap(int nx, int ny, int nz, int K, const float *lsen, const float *gc, const float *gs,
+               const double *ciso, float *cosr, float *sinr, float *amp, float *rela, float *ang)
+{
+    const int nvx = nx - 2, nvz = ny - 2;
+    const long nxy = (long)nx * ny, ncell = (long)nvx * nvz;
+    const double pi = 3.1415926535898;
+    for (int tt = 0; tt < K; ++tt)
+        for (int jj = 1; jj <= nvz; ++jj)
+            for (int ii = 1; ii <= nvx; ++ii) {
+                const long post = (long)jj * nx + ii;
+                float cs = 0.0f, sn = 0.0f;
+                for (int k = 0; k < nz - 1; ++k) {
+                    const float L = lsen[post + nxy * (tt + (long)K * k)];
+                    const long g = (ii - 1) + (long)nvx * ((jj - 1) + (long)nvz * k);
+                    cs = cs + L * gc[g];
+                    sn = sn + L * gs[g];
+                }
+                const long o = (long)(jj - 1) * nvx + (ii - 1) + ncell * tt;
+                const float a = 0.5f * sqrtf(cs * cs + sn * sn);
+                float an = (float)((double)atan2f(sn, cs) / pi * 180.0);
+                if (an < 0.0f) an = an + 360.0f;
+                an = 0.5f * an;
+                cosr[o] = cs; sinr[o] = sn; amp[o] = a;
+                rela[o] = a / (float)ciso[o];
+                ang[o] = an;
+            }
+}
