@@ -154,11 +154,30 @@ struct Context {
 Context g_ctx;
 std::mutex g_mu;
 
-bool valid_form(int form)
+// A form is DAZI_FORM_PLAIN or DAZI_FORM_ADJOINT plus flags.  The Love and
+// group-velocity flags go with the plain form (or a phase-velocity-only
+// call); the adjoint form, the FP32 scan and Lsen_Gsc are Rayleigh phase.
+constexpr int kWaveFlags = DAZI_FORM_LOVE | DAZI_FORM_GROUP;
+
+int check_form(int form, bool lsen)
 {
-    const int f = form & ~DAZI_FORM_SCAN_FP32;
-    return f == DAZI_FORM_PLAIN || f == DAZI_FORM_ADJOINT;
+    constexpr int known = DAZI_FORM_ADJOINT | DAZI_FORM_SCAN_FP32 | kWaveFlags;
+    if (form & ~known) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    if (form & kWaveFlags) {
+        if (form & (DAZI_FORM_ADJOINT | DAZI_FORM_SCAN_FP32)) {
+            set_err("Love waves and group velocity run in the plain form only (form %d)", form);
+            return DAZI_ERR_BADARG;
+        }
+        if (lsen) {
+            set_err("Lsen_Gsc is a Rayleigh phase-velocity kernel (form %d)", form);
+            return DAZI_ERR_BADARG;
+        }
+    }
+    return 0;
 }
+
+int form_ifunc(int form) { return (form & DAZI_FORM_LOVE) ? 1 : 2; }
+bool form_group(int form) { return (form & DAZI_FORM_GROUP) != 0; }
 
 void phase_begin(cudaStream_t st)
 {
@@ -404,13 +423,23 @@ int run_root(const Tables& T, const double* per, const StageOut& o, int form, bo
     a.pv = o.pv; a.croot = adj ? W.croot.as<double>() : nullptr; a.status = o.status;
     a.nevals = W.counters.as<unsigned long long>();
     a.scan32 = (form & DAZI_FORM_SCAN_FP32) ? 1 : 0;
-    const int bt = cfg.root_bt, mb = cfg.root_minb;
-    const unsigned nb = (unsigned)((T.ncols + bt - 1) / bt);
-    if (bt == 64 && mb == 10) root_kernel<64, 10><<<nb, 64, 0, st>>>(a);
-    else if (bt == 64) root_kernel<64, 0><<<nb, 64, 0, st>>>(a);
-    else if (bt == 256) root_kernel<256, 0><<<nb, 256, 0, st>>>(a);
-    else if (mb == 5) root_kernel<128, 5><<<nb, 128, 0, st>>>(a);
-    else root_kernel<128, 0><<<nb, 128, 0, st>>>(a);
+    const int ifunc = form_ifunc(form);
+    const bool grp = form_group(form);
+    if (ifunc == 1 || grp) {
+        // Love and/or group velocity: one launch shape
+        const unsigned nb = (unsigned)((T.ncols + 127) / 128);
+        if (ifunc == 1 && grp) root_kernel<128, 0, 1, true><<<nb, 128, 0, st>>>(a);
+        else if (ifunc == 1) root_kernel<128, 0, 1, false><<<nb, 128, 0, st>>>(a);
+        else root_kernel<128, 0, 2, true><<<nb, 128, 0, st>>>(a);
+    } else {
+        const int bt = cfg.root_bt, mb = cfg.root_minb;
+        const unsigned nb = (unsigned)((T.ncols + bt - 1) / bt);
+        if (bt == 64 && mb == 10) root_kernel<64, 10><<<nb, 64, 0, st>>>(a);
+        else if (bt == 64) root_kernel<64, 0><<<nb, 64, 0, st>>>(a);
+        else if (bt == 256) root_kernel<256, 0><<<nb, 256, 0, st>>>(a);
+        else if (mb == 5) root_kernel<128, 5><<<nb, 128, 0, st>>>(a);
+        else root_kernel<128, 0><<<nb, 128, 0, st>>>(a);
+    }
     CK(cudaGetLastError());
     ++g_ctx.last_launches;
     phase_mark("root", st);
@@ -515,7 +544,12 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
             a.pv = o.pv; a.sen_vs = o.svs; a.sen_vp = o.svp; a.sen_rho = o.srh;
             a.status = o.status; a.cscratch = g_ctx.cscratch.as<float>();
             a.dln = 0.01f; a.tol = 1.0e-6; a.nevals = g_ctx.w.counters.as<unsigned long long>();
-            fd_column_kernel<<<(unsigned)n, threads, smem, st>>>(a);
+            const int ifunc = form_ifunc(form);
+            const bool grp = form_group(form);
+            if (ifunc == 1 && grp) fd_column_kernel<1, true><<<(unsigned)n, threads, smem, st>>>(a);
+            else if (ifunc == 1) fd_column_kernel<1, false><<<(unsigned)n, threads, smem, st>>>(a);
+            else if (grp) fd_column_kernel<2, true><<<(unsigned)n, threads, smem, st>>>(a);
+            else fd_column_kernel<2, false><<<(unsigned)n, threads, smem, st>>>(a);
             CK(cudaGetLastError());
             ++g_ctx.last_launches;
         }
@@ -527,6 +561,7 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
     src.vel = vel; src.vp = vp; src.rho = rho; src.depz = g_ctx.depz.as<float>();
     src.node_off = nullptr; src.per_off = nullptr; src.nz = nz; src.K = kmax;
     src.minthk = g_ctx.geo_minthk;
+    src.ifunc = form_ifunc(form);
     PrepOut po{nullptr, nullptr, g_ctx.w.counters.as<unsigned long long>() + 4};
     Tables T;
     if ((r = build_tables(src, col_count, po, ncol, ncol, ncol, st, T, g_ctx.w))) return r;
@@ -562,6 +597,7 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
     src.vel = B.vs; src.vp = B.vp; src.rho = B.rho; src.depz = B.depz;
     src.node_off = B.node_off; src.per_off = B.per_off; src.nz = 0; src.K = 0;
     src.minthk = B.minthk;
+    src.ifunc = form_ifunc(form);
     PrepOut po{B.sen_off, B.ls_off, g_ctx.w.counters.as<unsigned long long>() + 4};
     Tables T;
     if ((r = build_tables(src, B.ncols, po, 1, 1, 1, st, T, g_ctx.w))) return r;
@@ -596,7 +632,14 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
             FdBatch fb;
             fb.node_off = B.node_off; fb.per_off = B.per_off; fb.depz = B.depz; fb.minthk = B.minthk;
             fb.sen_off = B.sen_off; fb.cbuf_off = g_ctx.cbufoff.as<long long>();
-            fd_batch_kernel<<<(unsigned)(c1 - c0), 256, fd_batch_smem_bytes(), st>>>(a, fb);
+            const unsigned nb = (unsigned)(c1 - c0);
+            const size_t sm = fd_batch_smem_bytes();
+            const int ifunc = form_ifunc(form);
+            const bool grp = form_group(form);
+            if (ifunc == 1 && grp) fd_batch_kernel<1, true><<<nb, 256, sm, st>>>(a, fb);
+            else if (ifunc == 1) fd_batch_kernel<1, false><<<nb, 256, sm, st>>>(a, fb);
+            else if (grp) fd_batch_kernel<2, true><<<nb, 256, sm, st>>>(a, fb);
+            else fd_batch_kernel<2, false><<<nb, 256, sm, st>>>(a, fb);
             CK(cudaGetLastError());
             ++g_ctx.last_launches;
             c0 = c1;
@@ -737,6 +780,7 @@ int plan_create(const BatchIn& B, const StageOut& o, int form, bool tune, cudaSt
     P.src.vel = B.vs; P.src.vp = B.vp; P.src.rho = B.rho; P.src.depz = B.depz;
     P.src.node_off = B.node_off; P.src.per_off = B.per_off; P.src.nz = 0; P.src.K = 0;
     P.src.minthk = B.minthk;
+    P.src.ifunc = 2;
     P.po = PrepOut{B.sen_off, B.ls_off, P.w.counters.as<unsigned long long>() + 4};
     P.o = o;
     P.form = form;
@@ -792,19 +836,25 @@ int stage_host(const int* pnx, const int* pny, const int* pnz, const float* vel,
         set_err("null argument");
         return DAZI_ERR_BADARG;
     }
-    if (*iwave != 2 || *igr != 0) {
-        set_err("only Rayleigh (iwave=2) phase velocity (igr=0) is supported (got %d, %d)", *iwave, *igr);
+    if (*iwave != 1 && *iwave != 2) {
+        set_err("iwave must be 1 (Love) or 2 (Rayleigh), got %d", *iwave);
         return DAZI_ERR_BADARG;
     }
+    if (form & kWaveFlags) {
+        set_err("pass the wave and velocity type as iwave/igr, not as form flags (form %d)", form);
+        return DAZI_ERR_BADARG;
+    }
+    // surfdisp96: ifunc = 1 for iwave = 1; group velocity for igr > 0
+    form |= (*iwave == 1 ? DAZI_FORM_LOVE : 0) | (*igr > 0 ? DAZI_FORM_GROUP : 0);
     if ((svs == nullptr) != (svp == nullptr) || (svs == nullptr) != (srh == nullptr)) {
         set_err("sen_vsRc, sen_vpRc, sen_rhoRc must be all set or all NULL");
         return DAZI_ERR_BADARG;
     }
     if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
-    if (!valid_form(form)) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    int r;
+    if ((r = check_form(form, lsen != nullptr))) return r;
     const int nx = *pnx, ny = *pny, nz = *pnz, kmax = *pkmax;
     const float minthk = *pminthk;
-    int r;
     if ((r = check_grid(nx, ny, nz, kmax, depz, minthk, col_start, col_count))) return r;
     if ((r = check_periods(tRc, kmax))) return r;
     const long long ncol = (long long)nx * ny;
@@ -877,14 +927,14 @@ int stage_host(const int* pnx, const int* pny, const int* pnz, const float* vel,
 }
 
 int check_dev_common(int nz, int kmaxRc, int form, const void* vp, const void* rho,
-                     const void* svs, const void* svp, const void* srh)
+                     const void* svs, const void* svp, const void* srh, const void* lsen)
 {
     if ((svs == nullptr) != (svp == nullptr) || (svs == nullptr) != (srh == nullptr)) {
         set_err("sen_* must be all set or all NULL");
         return DAZI_ERR_BADARG;
     }
     if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
-    if (!valid_form(form)) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    if (int r = check_form(form, lsen != nullptr)) return r;
     if (nz < 2 || nz > NZMAX) { set_err("nz=%d outside [2, %d]", nz, NZMAX); return DAZI_ERR_LIMITS; }
     if (kmaxRc < 1 || kmaxRc > NP) { set_err("kmaxRc=%d outside [1, %d]", kmaxRc, NP); return DAZI_ERR_LIMITS; }
     return 0;
@@ -897,7 +947,7 @@ int stage_dev(int nx, int ny, int nz, const float* vel, const float* vp, const f
 {
     if (!vel || !pvRc || !tRc || !depz) { set_err("null argument"); return DAZI_ERR_BADARG; }
     int r;
-    if ((r = check_dev_common(nz, kmaxRc, form, vp, rho, svs, svp, srh))) return r;
+    if ((r = check_dev_common(nz, kmaxRc, form, vp, rho, svs, svp, srh, lsen))) return r;
     std::lock_guard<std::mutex> lk(g_mu);
     if ((r = ensure_context())) return r;
     cudaStream_t st = (cudaStream_t)stream;   // NULL: the legacy default stream
@@ -1008,7 +1058,7 @@ int dazi_dk_batch_dev(long long ncols, const long long* node_off, const float* d
         return DAZI_ERR_BADARG;
     }
     if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
-    if (!valid_form(form)) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    if (int r = check_form(form, lsen != nullptr)) return r;
     if (!(minthk > 0.f) || !std::isfinite(minthk)) { set_err("minthk must be > 0"); return DAZI_ERR_BADARG; }
     std::lock_guard<std::mutex> lk(g_mu);
     int r;
@@ -1034,7 +1084,7 @@ int dazi_dk_batch(long long ncols, const long long* node_off, const float* depz,
         return DAZI_ERR_BADARG;
     }
     if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
-    if (!valid_form(form)) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    if (int r = check_form(form, lsen != nullptr)) return r;
     if (!(minthk > 0.f) || !std::isfinite(minthk)) { set_err("minthk must be > 0"); return DAZI_ERR_BADARG; }
     if (ncols == 0) return DAZI_OK;
     for (long long c = 0; c < ncols; ++c)
@@ -1176,7 +1226,7 @@ int dazi_dk_plan_create(long long ncols, const long long* node_off, const float*
         return DAZI_ERR_BADARG;
     }
     if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
-    if (!valid_form(form) || (form & 1) != DAZI_FORM_ADJOINT) {
+    if (check_form(form, lsen != nullptr) || (form & 1) != DAZI_FORM_ADJOINT) {
         set_err("plans run the adjoint form (form %d)", form);
         return DAZI_ERR_BADARG;
     }

@@ -126,6 +126,7 @@ struct ColSrc {
     const long long* per_off;      // ragged
     int nz, K;                     // grid
     float minthk;
+    int ifunc;                     // 1 Love, 2 Rayleigh: sphere()'s density factor
     __device__ __forceinline__ int col_nz(long long c) const
     {
         return ragged ? (int)(node_off[c + 1] - node_off[c]) : nz;
@@ -155,12 +156,16 @@ __global__ void prep_tasks_kernel(long long ntiles, const long long* tile_tasks,
                                   const long long* tile_tbase, int2* tasks);
 __global__ void prep_build_kernel(ColSrc src, PrepOut o, Tables T, const int* sorted_col,
                                   const long long* tile_tbase);
-template <int BT, int MINB> __global__ void root_kernel(RootArgs a);  // (64|128|256, 0), (128, 5), (64, 10)
+// Rayleigh phase: (64|128|256, 0), (128, 5), (64, 10); the other wave and
+// velocity types (IFUNC 1 Love / 2 Rayleigh, GROUP): (128, 0) only.
+template <int BT, int MINB, int IFUNC = 2, bool GROUP = false>
+__global__ void root_kernel(RootArgs a);
 template <int MINB> __global__ void adjoint_kernel(AdjArgs a);    // MINB in {2, 3, 4}
 template <int MINB> __global__ void ti_kernel(TiArgs a);          // MINB in {4, 6, 8}
 
 __global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);
-__global__ void fd_column_kernel(FdArgs a);
+// IFUNC 1 (Love) / 2 (Rayleigh), GROUP: all four combinations.
+template <int IFUNC, bool GROUP> __global__ void fd_column_kernel(FdArgs a);
 size_t fd_smem_bytes();
 
 // Ragged batch source of the finite-difference kernel.
@@ -172,7 +177,7 @@ struct FdBatch {
     const long long* sen_off;     // first kernel entry of each column
     const long long* cbuf_off;    // scratch offset (floats) of each column
 };
-__global__ void fd_batch_kernel(FdArgs a, FdBatch b);
+template <int IFUNC, bool GROUP> __global__ void fd_batch_kernel(FdArgs a, FdBatch b);
 size_t fd_batch_smem_bytes();
 
 }  // namespace dk

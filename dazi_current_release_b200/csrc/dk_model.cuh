@@ -7,7 +7,8 @@
 //
 //   brocher       DepthKernel1D.f90:187-200 (depthkernel_empirical_vp_rho)
 //   layer split   CalSurfG.f90:2490-2549    (refineGrid2LayerMdl)
-//   flattening    surfdisp96.f:480-547      (sphere, ifunc = 2, Rayleigh)
+//   flattening    surfdisp96.f:480-547      (sphere; density factor
+//                 btp**(-2.275) for Rayleigh, ifunc = 2, btp**(-5) for Love)
 //
 // The layer split and the flattening depend only on the node depths, so they
 // form a "geometry" shared by every column with the same depth grid.  The
@@ -35,7 +36,8 @@ struct Geometry {
     int16_t nsub_of_node[NZMAX]; // nsublay per interval (splice bookkeeping)
     float dflat[NL];         // flattened thickness (0 for the half-space)
     float btp[NL];           // flattening velocity factor, stored real*4
-    float rhofac[NL];        // btp**(-2.275) in single precision
+    float rhofac[NL];        // btp**(-2.275) in single precision (Rayleigh)
+    float rhofac_love[NL];   // btp**(-5) in single precision (Love)
     double tmp[NL];          // flattening velocity factor in double
     float rthk[NL];          // refined thickness before flattening
     // tregn96's own flattening of the TI model (R = 6371 km,
@@ -62,6 +64,15 @@ __device__ __forceinline__ void brocher(float x, float& vp, float& rho)
     r = __fsub_rn(r, __fmul_rn(0.0043f, p4));
     r = __fadd_rn(r, __fmul_rn(0.000106f, p5));
     rho = r;
+}
+
+// Love-wave density factor btp**(-5), surfdisp96.f:539: an integer power
+// of a real*4 value, which gfortran -O3 expands as x^2 * (x^2 * x) and
+// inverts with one real*4 division.
+__device__ __forceinline__ float love_rhofac(float btp)
+{
+    const float x2 = __fmul_rn(btp, btp);
+    return __fdiv_rn(1.0f, __fmul_rn(__fmul_rn(x2, btp), x2));
 }
 
 // Midpoint-interpolated sublayer value, CalSurfG.f90:2527-2529:
@@ -115,6 +126,7 @@ __device__ inline int build_geometry(Geometry& g, const float* depz, int nz, flo
         g.btp[m] = btp;
         // powf(btp, -2.275f), formed in double and rounded once
         g.rhofac[m] = (float)pow((double)btp, (double)(-2.275f));
+        g.rhofac_love[m] = love_rhofac(btp);
         r0 = r1;
     }
     // sphere_tdisp96(): radius 6371 (a real*4 constant), the half-space
@@ -148,9 +160,10 @@ __device__ inline int build_geometry(Geometry& g, const float* depz, int nz, flo
     return rmax;
 }
 
-// Flattened layer values (a, b, rho) of layer m given the node values.
+// Flattened layer values (a, b, rho) of layer m given the node values;
+// ifunc 1 (Love) or 2 (Rayleigh) selects sphere()'s density factor.
 __device__ __forceinline__ float4 flat_layer(const Geometry& g, int m, const float* vp,
-                                             const float* vs, const float* rho)
+                                             const float* vs, const float* rho, int ifunc = 2)
 {
     int i = g.node[m];
     float rvp, rvs, rrh;
@@ -166,7 +179,7 @@ __device__ __forceinline__ float4 flat_layer(const Geometry& g, int m, const flo
     L.x = g.dflat[m];
     L.y = (float)__dmul_rn((double)rvp, t);
     L.z = (float)__dmul_rn((double)rvs, t);
-    L.w = __fmul_rn(rrh, g.rhofac[m]);
+    L.w = __fmul_rn(rrh, ifunc == 1 ? g.rhofac_love[m] : g.rhofac[m]);
     return L;
 }
 

@@ -1,10 +1,13 @@
-// Rayleigh secular function and the reference's root search, in FP64 on the
-// CUDA cores.
+// Rayleigh and Love secular functions and the reference's root search, in
+// FP64 on the CUDA cores.
 //
 //   dltar4 + var + dnka + normc   surfdisp96.f:767-865, 868-985, 1018-1062, 989-1014
+//   dltar1 (Love)                 surfdisp96.f:704-763
 //   getsol (bracket)              surfdisp96.f:384-476
 //   nevill + half (refine)        surfdisp96.f:551-680
-//   surfdisp96 period loop        surfdisp96.f:52-354 (Rayleigh, phase, mode 1)
+//   surfdisp96 period loop        surfdisp96.f:52-354 (mode 1; phase, or
+//                                 group velocity by the second root at
+//                                 period t/(1-h), :226-233, 276-303)
 //
 // Optional FP32 coarse scan (DAZI_FORM_SCAN_FP32): the getsol
 // scan steps evaluate the secular function in FP32 and use only its sign;
@@ -146,6 +149,57 @@ __device__ __forceinline__ double dltar4(const M& mdl, int mmax, double wvno, do
     return e0;
 }
 
+// Love-wave secular function, surfdisp96.f:704-763: the Haskell-Thomson
+// SH product from the half-space to the surface, each step rescaled by its
+// larger component.  Reads the real*4 layer values (d, Vp, Vs, rho) and
+// promotes them, as dble(b(m)) does; every operation is rounded on its own
+// (no fused multiply-add), in the reference's order.
+template <class M>
+__device__ __forceinline__ double dltar1(const M& mdl, int mmax, double wvno, double omega)
+{
+    float4 L = mdl.layerf(mmax - 1);
+    double beta1 = (double)L.z, rho1 = (double)L.w;
+    double xkb = __ddiv_rn(omega, beta1);
+    double rb = __dsqrt_rn(__dmul_rn(__dadd_rn(wvno, xkb), fabs(__dsub_rn(wvno, xkb))));
+    double e1 = __dmul_rn(rho1, rb);
+    double e2 = __ddiv_rn(1.0, __dmul_rn(beta1, beta1));
+#pragma unroll 1
+    for (int m = mmax - 2; m >= 0; --m) {
+        L = mdl.layerf(m);
+        beta1 = (double)L.z;
+        rho1 = (double)L.w;
+        const double dm = (double)L.x;
+        const double xmu = __dmul_rn(__dmul_rn(rho1, beta1), beta1);
+        xkb = __ddiv_rn(omega, beta1);
+        rb = __dsqrt_rn(__dmul_rn(__dadd_rn(wvno, xkb), fabs(__dsub_rn(wvno, xkb))));
+        const double q = __dmul_rn(dm, rb);
+        double y, z, cosq;
+        if (wvno < xkb) {
+            double sinq;
+            sincos(q, &sinq, &cosq);
+            y = __ddiv_rn(sinq, rb);
+            z = __dmul_rn(-rb, sinq);
+        } else if (wvno == xkb) {
+            cosq = 1.0; y = dm; z = 0.0;
+        } else {
+            const double fac = (q < 16.0) ? exp(__dmul_rn(-2.0, q)) : 0.0;
+            cosq = __dmul_rn(__dadd_rn(1.0, fac), 0.5);
+            const double sinq = __dmul_rn(__dsub_rn(1.0, fac), 0.5);
+            y = __ddiv_rn(sinq, rb);
+            z = __dmul_rn(rb, sinq);
+        }
+        const double e10 = __dadd_rn(__dmul_rn(e1, cosq), __dmul_rn(__dmul_rn(e2, xmu), z));
+        const double e20 = __dadd_rn(__ddiv_rn(__dmul_rn(e1, y), xmu), __dmul_rn(e2, cosq));
+        double xnor = fabs(e10);
+        const double ynor = fabs(e20);
+        if (ynor > xnor) xnor = ynor;
+        if (xnor < 1.0e-40) xnor = 1.0;
+        e1 = __ddiv_rn(e10, xnor);
+        e2 = __ddiv_rn(e20, xnor);
+    }
+    return e1;
+}
+
 // The same secular function in FP32, for the coarse trial-velocity scan.
 // Reads the flattened layer table (d, Vp, Vs, rho) directly; exponentials,
 // reciprocals and square roots in single precision.  Only the sign of the
@@ -264,8 +318,17 @@ __device__ __forceinline__ float dltar4_f32(LayerF layerf, int mmax, float wvno,
 // Root search state machine.  One instance per model; `next()` consumes the
 // secular value of the last requested point and advances to the next point
 // to evaluate (or to the end of the model).
+//
+// GROUP (igr > 0, surfdisp96.f:226-233, 276-303): each period k solves at
+// t1a = t/(1+h) (the phase root c(k), which also seeds period k+1), then
+// runs getsol again at t1b = t/(1-h) from c(k) - 1.5 dc with floor
+// cb(k) + 0.01 dc (cb(k) = 0 for the fundamental mode) and ifirst = 0; a
+// second search that finds no root falls back to c(k).  The output is the
+// real*4 group velocity of the two roots.  h = 0.005 (h0, surfdisp96.f:113).
+template <bool GROUP = false>
 struct RootSM {
-    enum Phase : int { START = 0, GS_FIRST, GS_SCAN, VER1, VER2, NEV_A, NEV_B, NEV_CD, DONE };
+    enum Phase : int { START = 0, GS_FIRST, GS_SCAN, VER1, VER2, NEV_A, NEV_B, NEV_CD, DONE,
+                       GR_START };
     // model constants
     double cc, cm, dc, cmax, tol;
     float betmx;
@@ -280,6 +343,10 @@ struct RootSM {
     double c1, c2, c3, del1, del2, del3, clow, del1st, cprev, omega;
     double ceval;   // point to evaluate next
     double x[11], y[11];
+    // group velocity: second search running, its period t1b, the first root
+    bool second;
+    float t1a, t1b;
+    double cph;
 
     __device__ void init(double cc_, float betmx_, int kmax_, double tol_, bool scan32 = false)
     {
@@ -288,6 +355,7 @@ struct RootSM {
         dc = fabs((double)0.005f);
         cmax = (double)betmx_ + dc;
         k = 0; phase = START; fail_k = -1; del1st = 0.0; cprev = 0.0; evals = 0;
+        second = false; t1a = t1b = 0.0f; cph = 0.0;
     }
 
     // Runs the machine until it requests an evaluation (returns true, with
@@ -302,7 +370,17 @@ struct RootSM {
             switch (phase) {
             case START: {
                 if (k >= kmax) { phase = DONE; return false; }
-                omega = TWOPI / periods[k];
+                if constexpr (GROUP) {
+                    // t1a = t1/(1.+h), t1b = t1/(1.-h): real*8 quotients
+                    // stored in real*4; the first search runs at dble(t1a)
+                    const double t = periods[k];
+                    t1a = __double2float_rn(__ddiv_rn(t, (double)__fadd_rn(1.0f, 0.005f)));
+                    t1b = __double2float_rn(__ddiv_rn(t, (double)__fsub_rn(1.0f, 0.005f)));
+                    second = false;
+                    omega = TWOPI / (double)t1a;
+                } else {
+                    omega = TWOPI / periods[k];
+                }
                 if (!p64) evals = 0;
                 if (k == 0) { c1 = cc; clow = cc; ifirst = true; }
                 else { c1 = cprev - 1.5 * dc; clow = cm; ifirst = false; }
@@ -331,7 +409,11 @@ struct RootSM {
                 c1 = c2;
                 del1 = del2;
                 d1x = d2x;
-                if (c1 < cm || c1 >= cmax) { fail(); return false; }
+                if (c1 < cm || c1 >= cmax) {
+                    if (GROUP && second) { group_out(cph, out); continue; }
+                    fail();
+                    return false;
+                }
                 return scan_next();
             }
             case VER1: {
@@ -360,14 +442,23 @@ struct RootSM {
                     return request(c3);
                 }
                 if (update(out)) return true;
-                if (phase == START) continue;
+                if (phase != DONE) continue;
                 return false;
             }
             case NEV_B: {
                 del3 = F;
                 if (update(out)) return true;
-                if (phase == START) continue;
+                if (phase != DONE) continue;
                 return false;
+            }
+            case GR_START: {
+                // second getsol of a group-velocity period
+                omega = TWOPI / (double)t1b;
+                ifirst = false;
+                clow = 0.0 + 1.0e-2 * dc;
+                c1 = cph - 1.5 * dc;
+                phase = GS_FIRST;
+                return request(c1);
             }
             default:
                 return false;
@@ -430,12 +521,46 @@ struct RootSM {
         phase = DONE;
     }
 
+    // Group velocity of period k from the roots at t1a (c0) and t1b (c1),
+    // surfdisp96.f:293-299, in real*4 without fused operations:
+    //   gvel = (1/t1a - 1/t1b) / (1/(t1a*cc0) - 1/(t1b*cc1))
+    // then the next period.
+    template <class Out>
+    __device__ void group_out(double cb, Out& out)
+    {
+        const float cc0 = __double2float_rn(cph), cc1 = __double2float_rn(cb);
+        const float num = __fsub_rn(__fdiv_rn(1.0f, t1a), __fdiv_rn(1.0f, t1b));
+        const float den = __fsub_rn(__fdiv_rn(1.0f, __fmul_rn(t1a, cc0)),
+                                    __fdiv_rn(1.0f, __fmul_rn(t1b, cc1)));
+        const double g = (double)__fdiv_rn(num, den);
+        out(k, g, g, evals);
+        ++k;
+        p64 = false;
+        second = false;
+        phase = START;
+    }
+
     // End of nevill() for this period: getsol's acceptance test, then the
-    // next period.  Returns true when the machine should keep running.
+    // next period (or, for group velocity, the second search).  Returns
+    // true when the machine should keep running.
     template <class Out>
     __device__ bool finish(Out& out)
     {
+        if constexpr (GROUP) {
+            if (second) {
+                // a root above betmx counts as none found: cb(k) = c(k)
+                group_out(c3 > (double)betmx ? cph : c3, out);
+                return true;
+            }
+        }
         if (c3 > (double)betmx) { out(k, 0.0, 0.0, evals); fail(); return false; }
+        if constexpr (GROUP) {
+            cph = c3;
+            cprev = c3;
+            second = true;
+            phase = GR_START;
+            return true;
+        }
         // secant root inside the final bracket [c1, c2] (opposite signs)
         double ct = c3;
         const double dd = del2 - del1;
@@ -517,15 +642,19 @@ __device__ void scan_start(LayerF layerf, int mmax, double& cc, float& betmx)
 
 // Drive one model per lane through the whole period list with warp-uniform
 // evaluation steps.  All 32 lanes of the warp must call this together;
-// inactive lanes pass active = false.  Returns the 0-based first failing
-// period or -1.
-template <class M, class Out>
+// inactive lanes pass active = false.  IFUNC 2 is Rayleigh (dltar4), 1 Love
+// (dltar1); GROUP selects group velocity.  The FP32 scan applies to
+// Rayleigh phase velocity only.  Returns the 0-based first failing period
+// or -1.
+template <int IFUNC = 2, bool GROUP = false, class M, class Out>
 __device__ int solve_model_warp(bool active, const M& mdl, int mmax, double cc, float betmx,
                                 const double* periods, int kmax, double tol, Out& out,
                                 int* total_evals = nullptr, bool scan32 = false)
 {
-    RootSM sm;
-    sm.init(cc, betmx, kmax, tol, M::kF32 && scan32);
+    static_assert(IFUNC == 1 || IFUNC == 2, "ifunc is 1 (Love) or 2 (Rayleigh)");
+    constexpr bool kScan32 = M::kF32 && IFUNC == 2 && !GROUP;
+    RootSM<GROUP> sm;
+    sm.init(cc, betmx, kmax, tol, kScan32 && scan32);
     bool want = active ? sm.next(0.0, periods, out) : false;
     int tot = want ? 1 : 0;
     while (__any_sync(0xffffffffu, want)) {
@@ -534,14 +663,15 @@ __device__ int solve_model_warp(bool active, const M& mdl, int mmax, double cc, 
         // on an FP32 scan step; otherwise all evaluate in FP64 (a scan lane
         // then receives an exact value)
         bool step32 = false;
-        if constexpr (M::kF32) step32 = !__any_sync(0xffffffffu, want && sm.want64);
-        if constexpr (M::kF32) {
+        if constexpr (kScan32) step32 = !__any_sync(0xffffffffu, want && sm.want64);
+        if constexpr (kScan32) {
             if (want && step32)
                 F = (double)dltar4_f32([&](int m) { return mdl.layerf(m); }, mmax,
                                        (float)(sm.omega / sm.ceval), (float)sm.omega);
         }
         if (want && !step32) {
-            F = dltar4(mdl, mmax, sm.omega / sm.ceval, sm.omega);
+            if constexpr (IFUNC == 1) F = dltar1(mdl, mmax, sm.omega / sm.ceval, sm.omega);
+            else F = dltar4(mdl, mmax, sm.omega / sm.ceval, sm.omega);
             sm.want64 = true;
         }
         if (want) {

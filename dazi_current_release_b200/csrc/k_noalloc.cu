@@ -135,7 +135,7 @@ extern "C" int dazi_dk_iso_noalloc_dev(int nx, int ny, int nz, const float* vel,
         a.pv = pvRc; a.sen_vs = sen_vsRc; a.sen_vp = sen_vpRc; a.sen_rho = sen_rhoRc;
         a.status = status; a.cscratch = D.scratch; a.nevals = nullptr;
         a.dln = 0.01f; a.tol = 1.0e-6;
-        fd_column_kernel<<<(unsigned)n, threads, fd_smem_bytes(), st>>>(a);
+        fd_column_kernel<2, false><<<(unsigned)n, threads, fd_smem_bytes(), st>>>(a);
         if (cudaGetLastError() != cudaSuccess) return fail(DAZI_ERR_CUDA, "launch failed");
     }
     return DAZI_OK;

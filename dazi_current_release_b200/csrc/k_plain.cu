@@ -6,6 +6,9 @@
 // 1 + 6*nz models: the base model and, for every depth node, Vs, Vp and rho
 // perturbed by -/+ dln/2 (dln = 0.01), then forms
 //     sen_X(k, i) = (c_plus(k) - c_minus(k)) / (dln * X_i).
+// iwave and igr pass through to surfdisp96 there, so the kernels are
+// instantiated for Rayleigh and Love (IFUNC 2 / 1), phase and group
+// velocity (GROUP); c is then the group velocity and sen_X its derivative.
 //
 // Layout on the GPU: one CTA per column, one thread per model.  The CTA
 // stages the column's node values and its flattened base layer stack (as
@@ -36,6 +39,7 @@ struct PerturbedModel {
     const LayerD* ld;
     const Geometry* g;
     const float* node_val;   // node values of the perturbed parameter
+    const float* rhof;       // sphere()'s density factor per layer
     int pnode, par, lo, hi;
     float pval;              // perturbed node value
     __device__ __forceinline__ float4 layerf(int m) const {
@@ -52,7 +56,7 @@ struct PerturbedModel {
             }
             if (par == 0)      L.z = (float)__dmul_rn((double)v, g->tmp[m]);
             else if (par == 1) L.y = (float)__dmul_rn((double)v, g->tmp[m]);
-            else               L.w = __fmul_rn(v, g->rhofac[m]);
+            else               L.w = __fmul_rn(v, rhof[m]);
         }
         return L;
     }
@@ -109,6 +113,7 @@ struct FdColumn {
 
 // Body shared by the grid and ragged kernels.  Node values and periods are
 // already in S.vs/S.vp/S.rho and S.per; the whole block participates.
+template <int IFUNC, bool GROUP>
 __device__ void fd_column_body(const FdColumn& C, FdSmem& S, const FdArgs& a)
 {
     const Geometry* g = C.g;
@@ -124,7 +129,7 @@ __device__ void fd_column_body(const FdColumn& C, FdSmem& S, const FdArgs& a)
     }
     __syncthreads();
     for (int m = tid; m < rmax; m += nthr) {
-        const float4 L = flat_layer(*g, m, S.vp, S.vs, S.rho);
+        const float4 L = flat_layer(*g, m, S.vp, S.vs, S.rho, IFUNC);
         S.lay[m] = L;
         S.ld[m] = make_layerd(L);
     }
@@ -138,6 +143,7 @@ __device__ void fd_column_body(const FdColumn& C, FdSmem& S, const FdArgs& a)
         auto out = [&](int k, double c, double ct, int ev) { myc[k] = (float)c; };
         PerturbedModel mdl;
         mdl.lay = S.lay; mdl.ld = S.ld; mdl.g = g;
+        mdl.rhof = IFUNC == 1 ? g->rhofac_love : g->rhofac;
         mdl.node_val = S.vs; mdl.pnode = 0; mdl.par = 0; mdl.pval = 0.f;
         mdl.lo = 1; mdl.hi = 0;   // empty range: the base model
         if (active && q > 0) {
@@ -155,7 +161,8 @@ __device__ void fd_column_body(const FdColumn& C, FdSmem& S, const FdArgs& a)
         float betmx = 0.f;
         if (active) scan_start([&](int m) { return mdl.layerf(m); }, rmax, cc, betmx);
         int nev = 0;
-        const int fk = solve_model_warp(active, mdl, rmax, cc, betmx, S.per, K, a.tol, out, &nev);
+        const int fk = solve_model_warp<IFUNC, GROUP>(active, mdl, rmax, cc, betmx, S.per, K, a.tol,
+                                                      out, &nev);
         if (active && q == 0 && a.status) a.status[C.status_i] = fk < 0 ? 0 : fk + 1;
         if (a.nevals) {
             const unsigned long long w = __reduce_add_sync(0xffffffffu, (unsigned)nev);
@@ -181,6 +188,7 @@ __device__ void fd_column_body(const FdColumn& C, FdSmem& S, const FdArgs& a)
     }
 }
 
+template <int IFUNC, bool GROUP>
 __global__ void __launch_bounds__(256)
 fd_column_kernel(FdArgs a)
 {
@@ -198,11 +206,12 @@ fd_column_kernel(FdArgs a)
     C.sen_b = post; C.sen_sk = ncol; C.sen_is = ncol * (long long)K;
     C.status_i = post;
     C.cbuf = a.cscratch + (size_t)blockIdx.x * (1 + 6 * nz) * K;
-    fd_column_body(C, S, a);
+    fd_column_body<IFUNC, GROUP>(C, S, a);
 }
 
 // Ragged batch: column c = col0 + blockIdx.x has its own depth grid and
 // periods (CSR offsets); its geometry is built in shared memory.
+template <int IFUNC, bool GROUP>
 __global__ void __launch_bounds__(256)
 fd_batch_kernel(FdArgs a, FdBatch b)
 {
@@ -229,8 +238,17 @@ fd_batch_kernel(FdArgs a, FdBatch b)
     C.sen_b = b.sen_off ? b.sen_off[c] : 0; C.sen_sk = 1; C.sen_is = K;
     C.status_i = c;
     C.cbuf = a.cscratch + b.cbuf_off[c] - b.cbuf_off[a.col0];
-    fd_column_body(C, S, a);
+    fd_column_body<IFUNC, GROUP>(C, S, a);
 }
+
+template __global__ void fd_column_kernel<2, false>(FdArgs);
+template __global__ void fd_column_kernel<2, true>(FdArgs);
+template __global__ void fd_column_kernel<1, false>(FdArgs);
+template __global__ void fd_column_kernel<1, true>(FdArgs);
+template __global__ void fd_batch_kernel<2, false>(FdArgs, FdBatch);
+template __global__ void fd_batch_kernel<2, true>(FdArgs, FdBatch);
+template __global__ void fd_batch_kernel<1, false>(FdArgs, FdBatch);
+template __global__ void fd_batch_kernel<1, true>(FdArgs, FdBatch);
 
 // ------------------------------------------------------------------------
 // One thread per column (sorted position): the base-model root search (pv,
@@ -247,8 +265,10 @@ struct TableModel {
 
 // BT: threads per block (one thread per column); MINB: minimum resident
 // blocks per SM the register allocation aims for (0: no constraint).  The
-// autotuner picks one of the instantiations.
-template <int BT, int MINB>
+// autotuner picks one of the instantiations.  IFUNC / GROUP: Love or
+// Rayleigh, group or phase velocity (the tables then hold the matching
+// density flattening).
+template <int BT, int MINB, int IFUNC, bool GROUP>
 __global__ void __launch_bounds__(BT, MINB)
 root_kernel(RootArgs a)
 {
@@ -271,8 +291,8 @@ root_kernel(RootArgs a)
         scan_start([&](int m) { return lf[(long long)m * TILE]; }, M.rmax, cc, betmx);
     }
     int nev = 0;
-    const int fk = solve_model_warp(active, mdl, M.rmax, cc, betmx, per, M.K, a.tol, out, &nev,
-                                    a.scan32 != 0);
+    const int fk = solve_model_warp<IFUNC, GROUP>(active, mdl, M.rmax, cc, betmx, per, M.K, a.tol,
+                                                  out, &nev, a.scan32 != 0);
     if (active && a.status) a.status[M.status_i] = fk < 0 ? 0 : fk + 1;
     if (a.nevals) {
         const unsigned long long w = __reduce_add_sync(0xffffffffu, (unsigned)nev);
@@ -281,10 +301,13 @@ root_kernel(RootArgs a)
     }
 }
 
-template __global__ void root_kernel<64, 0>(RootArgs);
-template __global__ void root_kernel<128, 0>(RootArgs);
-template __global__ void root_kernel<256, 0>(RootArgs);
-template __global__ void root_kernel<128, 5>(RootArgs);
-template __global__ void root_kernel<64, 10>(RootArgs);
+template __global__ void root_kernel<64, 0, 2, false>(RootArgs);
+template __global__ void root_kernel<128, 0, 2, false>(RootArgs);
+template __global__ void root_kernel<256, 0, 2, false>(RootArgs);
+template __global__ void root_kernel<128, 5, 2, false>(RootArgs);
+template __global__ void root_kernel<64, 10, 2, false>(RootArgs);
+template __global__ void root_kernel<128, 0, 2, true>(RootArgs);
+template __global__ void root_kernel<128, 0, 1, false>(RootArgs);
+template __global__ void root_kernel<128, 0, 1, true>(RootArgs);
 
 }  // namespace dk

@@ -151,7 +151,8 @@ __device__ __forceinline__ void prep_build_one(const ColSrc& src, const PrepOut&
             const float dflat = half ? 0.0f : (float)__dsub_rn(z1, z0);
             const double tmp = __ddiv_rn(__dadd_rn(ar, ar), __dadd_rn(r0, r1));
             const float btp = (float)tmp;
-            const float rhofac = (float)pow((double)btp, (double)(-2.275f));
+            const float rhofac = src.ifunc == 1 ? love_rhofac(btp)
+                                                : (float)pow((double)btp, (double)(-2.275f));
             r0 = r1;
             float4 L;
             L.x = dflat;

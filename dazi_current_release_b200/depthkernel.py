@@ -97,7 +97,9 @@ def depthkernel(nx, ny, nz, vel, iwave, igr, kmaxRc, tRc, depz, minthk, *, form=
 
     Returns (pvRc, sen_vsRc, sen_vpRc, sen_rhoRc) as Fortran-ordered arrays
     (pvRc only when kernels=False).  form: FORM_PLAIN / FORM_ADJOINT, or
-    None to read DAZI_DEPTHKERNEL_BACKEND.
+    None to read DAZI_DEPTHKERNEL_BACKEND.  iwave 2 (Rayleigh) or 1 (Love),
+    igr 0 (phase) or > 0 (group velocity), as surfdisp96 takes them; Love
+    and group velocity run in the plain form (or with kernels=False).
     """
     if form is None:
         form = resolve_form(ENV_ISO)

@@ -14,9 +14,13 @@
  * Fortran side can bind them without the VALUE attribute; the column range
  * and the form selector are passed by value.
  *
- * Only Rayleigh (iwave = 2) phase velocity (igr = 0) is accepted, the only
- * combination DAzi calls (CalSurfG_parallel.f90:1967-1976); other values
- * return DAZI_ERR_BADARG.
+ * Wave and velocity type: iwave = 2 (Rayleigh) or 1 (Love), igr = 0 (phase)
+ * or > 0 (group), as surfdisp96 takes them (DepthKernel1D.f90 passes both
+ * through; DAzi's inversion calls Rayleigh phase, CalSurfG_parallel.f90:
+ * 1967-1976, and holds the other three calls at CalSurfG.f90:1227-1245).
+ * The plain form and phase-velocity-only calls take all four; the adjoint
+ * form and Lsen_Gsc are Rayleigh phase only.  Other values return
+ * DAZI_ERR_BADARG.
  *
  * Limits (the reference's compiled limits, surfdisp96.f:57-59):
  *   nz <= 200, kmaxRc <= 160, refined layers <= 200.
@@ -58,6 +62,17 @@ extern "C" {
  * roots as the default all-FP64 search).  The plain form always evaluates
  * in FP64. */
 #define DAZI_FORM_SCAN_FP32 2
+/* flags, OR-ed into the form of the plain form or of a phase-velocity-only
+ * call (no sen_* and no Lsen_Gsc outputs): Love instead of Rayleigh waves
+ * (surfdisp96's iwave = 1, dltar1) and group instead of phase velocity
+ * (igr > 0; pvRc and the kernels are then the group velocity and its
+ * derivatives).  The entries with iwave/igr arguments set them from those
+ * (and reject them in form); the device and uneven-column entries take
+ * them here.  The adjoint form, DAZI_FORM_SCAN_FP32,
+ * Lsen_Gsc and plans are Rayleigh phase velocity only: combining them with
+ * these flags returns DAZI_ERR_BADARG. */
+#define DAZI_FORM_LOVE     4
+#define DAZI_FORM_GROUP    8
 
 /* Replaces depthkernel() of code/src_inv_iso_joint/CalSurfG.f90:1-15
  * (default_fortran_fd backend, CalSurfG.f90:86-107), for the 1-based column

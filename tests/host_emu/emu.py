@@ -38,9 +38,10 @@ def ti_batch(node_off, depz, vs, per_off, periods, minthk, pv):
     return rc, ls, ls_off
 
 
-def root_batch(node_off, depz, vs, per_off, periods, minthk, scan32=True):
-    """pv (sngl(c) as the library writes it), status and the number of
-    secular evaluations of the root search of a ragged batch."""
+def root_batch(node_off, depz, vs, per_off, periods, minthk, scan32=True, ifunc=2, group=False):
+    """pv (sngl(c) as the library writes it; the group velocity when
+    group), status and the number of secular evaluations of the root search
+    of a ragged batch; ifunc 1 Love, 2 Rayleigh."""
     P = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))  # noqa: E731
     node_off = np.ascontiguousarray(node_off, np.int64)
     per_off = np.ascontiguousarray(per_off, np.int64)
@@ -52,5 +53,6 @@ def root_batch(node_off, depz, vs, per_off, periods, minthk, scan32=True):
                               P(np.ascontiguousarray(depz, np.float32), f32),
                               P(np.ascontiguousarray(vs, np.float32), f32), P(per_off, i64),
                               P(np.ascontiguousarray(periods, np.float64), f64), f32(minthk),
-                              int(scan32), P(pv, f64), P(st, ctypes.c_int), ctypes.byref(ev))
+                              int(scan32), int(ifunc), int(bool(group)), P(pv, f64),
+                              P(st, ctypes.c_int), ctypes.byref(ev))
     return rc, pv, st, ev.value

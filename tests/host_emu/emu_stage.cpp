@@ -76,12 +76,13 @@ bool build_host(const ColSrc& src, long long ncols, const PrepOut& po, HostTable
 }
 
 ColSrc ragged_src(const long long* node_off, const float* depz, const float* vs,
-                  const long long* per_off, float minthk)
+                  const long long* per_off, float minthk, int ifunc = 2)
 {
     ColSrc src;
     src.ragged = true; src.ncol = 0; src.col0 = 0;
     src.vel = vs; src.vp = nullptr; src.rho = nullptr; src.depz = depz;
     src.node_off = node_off; src.per_off = per_off; src.nz = 0; src.K = 0; src.minthk = minthk;
+    src.ifunc = ifunc;
     return src;
 }
 
@@ -90,12 +91,15 @@ ColSrc ragged_src(const long long* node_off, const float* depz, const float* vs,
 // Root search of a ragged batch (root_kernel, one thread per sorted
 // column): pv[per_off[c] + k] (sngl(c), as the library writes it), status
 // per column, the secular evaluations in *evals.  scan32 selects the FP32
-// coarse scan.
+// coarse scan; ifunc 1 (Love) / 2 (Rayleigh) and group select the
+// root_kernel instantiation the library launches for that form.
 extern "C" int emu_root_batch(long long ncols, const long long* node_off, const float* depz,
                               const float* vs, const long long* per_off, const double* periods,
-                              float minthk, int scan32, double* pv, int* status, long long* evals)
+                              float minthk, int scan32, int ifunc, int group, double* pv,
+                              int* status, long long* evals)
 {
-    const ColSrc src = ragged_src(node_off, depz, vs, per_off, minthk);
+    if (ifunc != 1 && ifunc != 2) return -2;
+    const ColSrc src = ragged_src(node_off, depz, vs, per_off, minthk, ifunc);
     HostTables H;
     PrepOut po{nullptr, nullptr, nullptr};
     if (!build_host(src, ncols, po, H)) return -1;
@@ -107,7 +111,10 @@ extern "C" int emu_root_batch(long long ncols, const long long* node_off, const 
     for (long long s = 0; s < ncols; ++s) {
         blockIdx.x = (unsigned)(s / 128);
         threadIdx.x = (unsigned)(s % 128);
-        root_kernel<128, 0>(a);
+        if (ifunc == 1 && group) root_kernel<128, 0, 1, true>(a);
+        else if (ifunc == 1) root_kernel<128, 0, 1, false>(a);
+        else if (group) root_kernel<128, 0, 2, true>(a);
+        else root_kernel<128, 0>(a);
     }
     *evals = (long long)counters[0];
     return 0;

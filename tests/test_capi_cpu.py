@@ -8,7 +8,7 @@ import numpy as np
 import pytest
 
 from dazi_current_release_b200 import _lib, depthkernel as dkmod
-from dazi_current_release_b200.depthkernel import DepthKernelError, resolve_form
+from dazi_current_release_b200.depthkernel import DepthKernelError, depthkernelTI, resolve_form
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -52,8 +52,14 @@ def _call_iso(nx=2, ny=2, nz=3, iwave=2, igr=0, K=2, depz=(0.0, 3.0, 6.0), vel=3
 
 
 @pytest.mark.parametrize("kw,code", [
-    (dict(iwave=1), _lib.DAZI_ERR_BADARG),              # Love not in scope
-    (dict(igr=1), _lib.DAZI_ERR_BADARG),                # group velocity
+    (dict(iwave=3), _lib.DAZI_ERR_BADARG),              # neither Love nor Rayleigh
+    (dict(iwave=0), _lib.DAZI_ERR_BADARG),
+    (dict(iwave=1, form=_lib.FORM_ADJOINT), _lib.DAZI_ERR_BADARG),   # adjoint: Rayleigh phase
+    (dict(igr=1, form=_lib.FORM_ADJOINT), _lib.DAZI_ERR_BADARG),
+    (dict(igr=1, form=_lib.FORM_SCAN_FP32), _lib.DAZI_ERR_BADARG),   # FP32 scan: Rayleigh phase
+    (dict(form=_lib.FORM_LOVE), _lib.DAZI_ERR_BADARG),  # wave type goes through iwave here
+    (dict(form=_lib.FORM_GROUP), _lib.DAZI_ERR_BADARG),
+    (dict(form=16), _lib.DAZI_ERR_BADARG),              # unknown flag
     (dict(depz=(0.0, 3.0, 3.0)), _lib.DAZI_ERR_BADARG),  # not increasing
     (dict(col_start=0), _lib.DAZI_ERR_BADARG),
     (dict(col_start=3, col_count=3), _lib.DAZI_ERR_BADARG),
@@ -66,6 +72,25 @@ def _call_iso(nx=2, ny=2, nz=3, iwave=2, igr=0, K=2, depz=(0.0, 3.0, 6.0), vel=3
 def test_bad_arguments_rejected_without_device(kw, code):
     assert _call_iso(**kw) == code
     assert len(_lib.load().dazi_dk_last_error()) > 0
+
+
+@pytest.mark.parametrize("iwave,igr", [(1, 0), (2, 1), (1, 1), (2, 5)])
+def test_love_and_group_pass_validation(iwave, igr):
+    """Love (iwave = 1) and group velocity (igr > 0) are accepted by the
+    plain form; without a GPU the call then stops at the device check."""
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    assert _call_iso(iwave=iwave, igr=igr) == _lib.DAZI_ERR_NODEVICE
+
+
+@pytest.mark.parametrize("iwave,igr", [(1, 0), (2, 1)])
+def test_gc_gs_kernel_is_rayleigh_phase_only(iwave, igr):
+    with pytest.raises(_lib.DaziError) as ei:
+        depthkernelTI(2, 2, 3, np.full((2, 2, 3), 3.5, np.float32, order="F"), iwave, igr,
+                      2, np.array([5.0, 10.0]), np.array([0.0, 3.0, 6.0], np.float32), 4.0)
+    assert ei.value.code == _lib.DAZI_ERR_BADARG
+    assert "Rayleigh" in _lib.load().dazi_dk_last_error().decode()
 
 
 def test_no_device_is_a_loud_error():

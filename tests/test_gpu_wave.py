@@ -1,0 +1,144 @@
+"""Love waves and group velocity on the GPU (surfdisp96 iwave = 1, igr > 0),
+through the C-ABI, against the oracle and the reference's own Python surf96.
+
+Tolerances as in test_host_emu_wave.py: two root searches of one zero end
+at most 2e-6 c apart (each stops on a bracket narrower than 1e-6 c,
+surfdisp96.f:608); the group velocity's difference quotient over
+t/(1 -+ h), h = 0.005, turns that into at most ~4e-4 U.  Love evaluates
+dltar1 in the reference's operation order and matches bit for bit."""
+import numpy as np
+import pytest
+
+from conftest import assert_fd_parity
+import dazi_current_release_b200 as dk
+from dazi_current_release_b200 import synthetic as S
+from dazi_current_release_b200.batch import depthkernel_batch
+
+pytestmark = pytest.mark.gpu
+
+PHASE_MOVE = 2.0e-6
+GROUP_MOVE = 4.0e-4
+COMBOS = [(2, 0), (2, 1), (1, 0), (1, 1)]
+
+
+def _moves_ok(got, ref, iwave, igr, max_frac=0.05):
+    """pv against the oracle: equal, or moved within the root tolerance."""
+    got = np.asarray(got, np.float64).ravel()
+    ref = np.asarray(ref, np.float64).ravel()
+    moved = np.nonzero(got != ref)[0]
+    if iwave == 1:
+        assert moved.size <= max(1, got.size // 1000), moved[:5]
+    assert moved.size <= max(2, max_frac * got.size), moved.size
+    assert np.all(ref[moved] > 0)
+    bound = GROUP_MOVE if igr else PHASE_MOVE
+    assert np.all(np.abs(got[moved] / ref[moved] - 1) <= bound)
+    return moved.size
+
+
+@pytest.mark.parametrize("iwave,igr", COMBOS)
+def test_plain_form_matches_oracle(oracle, iwave, igr):
+    case = S.subgrid(S.config0(), 4, 3)
+    nx, ny, nz = case.vel.shape
+    K = case.periods.size
+    pv, svs, svp, srh = dk.depthkernel_vpvsrho(nx, ny, nz, case.vel, case.vp, case.rho, iwave, igr,
+                                               K, case.periods, case.depz, case.minthk,
+                                               form=dk.FORM_PLAIN)
+    ref = oracle.depthkernel(case.vel, case.depz, case.periods, case.minthk, vp=case.vp,
+                             rho=case.rho, iwave=iwave, igr=igr)
+    assert (ref["status"] == 0).all()
+    _moves_ok(pv, ref["pvRc"], iwave, igr)
+    tol = GROUP_MOVE / 2 if igr else PHASE_MOVE
+    cols = [(svs, ref["sen_vs"], case.vel), (svp, ref["sen_vp"], case.vp),
+            (srh, ref["sen_rho"], case.rho)]
+    nxy = nx * ny
+    for got, exp, x in cols:
+        xc = np.asarray(x).reshape(nxy, nz, order="F")
+        for c in range(nxy):
+            assert_fd_parity(got[c], exp[c], xc[c], tol=tol, max_frac=0.05)
+
+
+@pytest.mark.parametrize("iwave,igr", COMBOS)
+def test_phase_only_table_path_equals_plain_form(oracle, iwave, igr):
+    """kernels=False runs the per-column root kernel over the layer tables
+    (one thread per column); its velocities equal the plain form's base
+    model bit for bit."""
+    case = S.subgrid(S.config1(), 8, 6)
+    nx, ny, nz = case.vel.shape
+    K = case.periods.size
+    (pv,) = dk.depthkernel(nx, ny, nz, case.vel, iwave, igr, K, case.periods, case.depz,
+                           case.minthk, form=dk.FORM_PLAIN, kernels=False)
+    pvf, _, _, _ = dk.depthkernel(nx, ny, nz, case.vel, iwave, igr, K, case.periods, case.depz,
+                                  case.minthk, form=dk.FORM_PLAIN)
+    np.testing.assert_array_equal(pv, pvf)
+    ref = oracle.depthkernel(case.vel, case.depz, case.periods, case.minthk, iwave=iwave,
+                             igr=igr, kernels=False)
+    _moves_ok(pv, ref["pvRc"], iwave, igr)
+
+
+def test_gpu_matches_reference_surf96_golden():
+    """The Yunnan columns of tests/golden/surf96_wave.npz as a 1-row grid:
+    Love / Rayleigh phase and group velocity against the reference's Python
+    surf96 (an independent implementation: within the root tolerance)."""
+    import os
+    here = os.path.dirname(os.path.abspath(__file__))
+    g = np.load(os.path.join(here, "golden", "surf96_wave.npz"))
+    y = np.load(os.path.join(here, "golden", "yunnan_pv.npz"))
+    nx0, ny0, nz = (int(y[k]) for k in ("nx", "ny", "nz"))
+    cols = y["vel"].reshape(nx0 * ny0, nz, order="F")[g["columns"]]
+    n = cols.shape[0]
+    vel = np.asfortranarray(cols.reshape(n, 1, nz))
+    t = g["periods"]
+    for iwave in (1, 2):
+        for igr in (0, 1):
+            (pv,) = dk.depthkernel(n, 1, nz, vel, iwave, igr, t.size, t, y["depz"],
+                                   float(y["minthk"]), form=dk.FORM_PLAIN, kernels=False)
+            ref = g[f"cg_ifunc{iwave}_itype{igr}"]
+            rel = np.abs(pv / ref - 1)
+            assert rel.max() <= (GROUP_MOVE if igr else PHASE_MOVE), (iwave, igr, rel.max())
+
+
+def _per_column_oracle(oracle, b, iwave, igr, cols):
+    out = []
+    for c in cols:
+        n0, n1 = b.node_off[c], b.node_off[c + 1]
+        p0, p1 = b.per_off[c], b.per_off[c + 1]
+        vel = np.asfortranarray(b.vs[n0:n1].reshape(1, 1, n1 - n0))
+        out.append(oracle.depthkernel(vel, b.depz[n0:n1], b.periods[p0:p1], b.minthk,
+                                      iwave=iwave, igr=igr))
+    return out
+
+
+@pytest.mark.parametrize("iwave,igr", [(2, 1), (1, 0), (1, 1)])
+def test_uneven_batch_love_group(oracle, iwave, igr):
+    """The uneven-column entry with the form flags: plain-form kernels and
+    phase-only runs, per column against the oracle."""
+    b = S.config3(realisations=1, columns=48, base_seed=2024)
+    flags = (dk.FORM_LOVE if iwave == 1 else 0) | (dk.FORM_GROUP if igr else 0)
+    r = depthkernel_batch(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk,
+                          form=dk.FORM_PLAIN | flags, kernels=True, lsen=False)
+    r0 = depthkernel_batch(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk,
+                           form=dk.FORM_PLAIN | flags, kernels=False, lsen=False)
+    np.testing.assert_array_equal(r["pv"], r0["pv"])
+    assert (r["status"] == 0).all()
+    cols = list(range(0, 48, 6))
+    refs = _per_column_oracle(oracle, b, iwave, igr, cols)
+    tol = GROUP_MOVE / 2 if igr else PHASE_MOVE
+    for c, ref in zip(cols, refs):
+        pv, svs, svp, srh = r.column(c)
+        _moves_ok(pv, ref["pvRc"][0], iwave, igr)
+        n0, n1 = b.node_off[c], b.node_off[c + 1]
+        vs = b.vs[n0:n1]
+        vp, rho = oracle.brocher(vs)
+        for got, exp, x in ((svs, ref["sen_vs"][0], vs), (svp, ref["sen_vp"][0], vp),
+                            (srh, ref["sen_rho"][0], rho)):
+            assert_fd_parity(got, exp, x, tol=tol, max_frac=0.05)
+
+
+def test_wave_flags_rejected_where_rayleigh_phase_only():
+    b = S.config3(realisations=1, columns=4, base_seed=7)
+    args = (b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk)
+    for form, kw in ((dk.FORM_ADJOINT | dk.FORM_LOVE, {}), (dk.FORM_ADJOINT | dk.FORM_GROUP, {}),
+                     (dk.FORM_PLAIN | dk.FORM_LOVE, dict(lsen=True, kernels=False))):
+        with pytest.raises(dk.DaziError) as ei:
+            depthkernel_batch(*args, form=form, **kw)
+        assert ei.value.code == -1
