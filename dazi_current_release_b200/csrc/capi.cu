@@ -86,7 +86,7 @@ struct LaunchCfg {
     int root_bt = 128;      // root_kernel threads per block: 64, 128, 256
     int root_minb = 0;      // root_kernel blocks per SM of the register budget: 0, 5 (128), 10 (64)
     int adj_minb = 3;       // adjoint_kernel blocks per SM: 2, 3, 4
-    int ti_minb = 8;        // ti_kernel blocks per SM: 4, 6, 8
+    int ti_minb = 4;        // ti_kernel blocks per SM: 2, 3, 4, 6, 8
 };
 
 // Root-search variants (threads per block, register-budget blocks per SM).
@@ -112,7 +112,8 @@ LaunchCfg default_cfg()
     const char* j = std::strstr(e, "adj=");
     if (j && std::sscanf(j + 4, "%d", &a) == 1 && a >= 2 && a <= 4) cfg.adj_minb = a;
     const char* t = std::strstr(e, "ti=");
-    if (t && std::sscanf(t + 3, "%d", &a) == 1 && (a == 4 || a == 6 || a == 8)) cfg.ti_minb = a;
+    if (t && std::sscanf(t + 3, "%d", &a) == 1 && (a == 2 || a == 3 || a == 4 || a == 6 || a == 8))
+        cfg.ti_minb = a;
     return cfg;
 }
 
@@ -377,8 +378,13 @@ const void* adjoint_fn(int minb)
 }
 const void* ti_fn(int minb)
 {
-    return minb == 4 ? (const void*)ti_kernel<4> : minb == 6 ? (const void*)ti_kernel<6>
-                                                             : (const void*)ti_kernel<8>;
+    switch (minb) {
+    case 2: return (const void*)ti_kernel<2>;
+    case 3: return (const void*)ti_kernel<3>;
+    case 6: return (const void*)ti_kernel<6>;
+    case 8: return (const void*)ti_kernel<8>;
+    default: return (const void*)ti_kernel<4>;
+    }
 }
 
 // Largest refined layer count of the tables (first sorted column): one
@@ -480,7 +486,9 @@ int run_ti(const Tables& T, const double* per, const StageOut& o, long long maxr
     t.T = T; t.periods = per; t.pv = o.pv; t.lsen = o.lsen;
     t.scratch = W.tiscr.as<double>(); t.scr_layers = maxr; t.queue = queues + 1;
     t.errflag = reinterpret_cast<int*>(c + 1);
-    if (cfg.ti_minb == 4) ti_kernel<4><<<(unsigned)nblk, 128, 0, st>>>(t);
+    if (cfg.ti_minb == 2) ti_kernel<2><<<(unsigned)nblk, 128, 0, st>>>(t);
+    else if (cfg.ti_minb == 3) ti_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(t);
+    else if (cfg.ti_minb == 4) ti_kernel<4><<<(unsigned)nblk, 128, 0, st>>>(t);
     else if (cfg.ti_minb == 6) ti_kernel<6><<<(unsigned)nblk, 128, 0, st>>>(t);
     else ti_kernel<8><<<(unsigned)nblk, 128, 0, st>>>(t);
     CK(cudaGetLastError());
@@ -712,7 +720,7 @@ int time_phase(Plan& P, F launch, float& ms)
 int plan_tune(Plan& P)
 {
     int r;
-    const int adj_c[3] = {2, 3, 4}, ti_c[3] = {4, 6, 8};
+    const int adj_c[3] = {2, 3, 4}, ti_c[5] = {2, 3, 4, 6, 8};
     LaunchCfg c = P.cfg;
     float best = 1e30f;
     for (const auto& v : kRootVariants) {

@@ -36,9 +36,30 @@ constexpr double TWOPI = 2.0 * 3.141592653589793;
 
 __device__ __forceinline__ double fsign1(double x) { return signbit(x) ? -1.0 : 1.0; }
 
+// normc() between layers: the reference divides the vector by its largest
+// component t1 (unless t1 < 1e-40).  The value returned is the top layer's
+// f0 / max|f|, which any exact positive rescaling of the intermediate
+// vectors leaves unchanged, so the intermediate layers are scaled by
+// 2^-e (e the exponent of max|f|, read from the bits; exact, no rounding)
+// and only the last vector is divided by its largest component.  The
+// result differs from the reference's per-layer divisions only in rounding.
+__device__ __forceinline__ void normc_pow2(double& e0, double& e1, double& e2, double& e3, double& e4)
+{
+    // high words of |e_i|: ordered as the magnitudes (to 2^-20)
+    const int h = max(max(max(__double2hiint(e0) & 0x7fffffff, __double2hiint(e1) & 0x7fffffff),
+                          max(__double2hiint(e2) & 0x7fffffff, __double2hiint(e3) & 0x7fffffff)),
+                      __double2hiint(e4) & 0x7fffffff);
+    // below 1e-40 (high word 0x37a16c26) the reference leaves the vector
+    // as it is
+    if (h < 0x37a16c26) return;
+    const int ex = min((h >> 20) - 1023, 1022);
+    const double sc = __hiloint2double((1023 - ex) << 20, 0);   // 2^-ex
+    e0 *= sc; e1 *= sc; e2 *= sc; e3 *= sc; e4 *= sc;
+}
+
 // Secular-function value at wavenumber wvno, angular frequency omega.
-// Each layer product is rescaled by its largest component (normc); the
-// factors are discarded, as in the reference, since they do not move roots.
+// Each layer product is rescaled (normc_pow2); the factors are discarded,
+// as in the reference, since they do not move roots.
 template <class M>
 __device__ __forceinline__ double dltar4(const M& mdl, int mmax, double wvno, double omega)
 {
@@ -140,13 +161,14 @@ __device__ __forceinline__ double dltar4(const M& mdl, int mmax, double wvno, do
         const double f2 = e0 * c13 + e1 * c23 + e2 * c33 + e3 * c43 + e4 * c53;
         const double f3 = e0 * c14 + e1 * c24 + e2 * c34 + e3 * c22 + e4 * c21;
         const double f4 = e0 * c15 + e1 * c14 + e2 * c35 + e3 * c12 + e4 * c11;
-        // normc()
-        double t1 = fmax(fmax(fmax(fabs(f0), fabs(f1)), fmax(fabs(f2), fabs(f3))), fabs(f4));
-        if (t1 < 1.0e-40) t1 = 1.0;
-        const double tinv = 1.0 / t1;
-        e0 = f0 * tinv; e1 = f1 * tinv; e2 = f2 * tinv; e3 = f3 * tinv; e4 = f4 * tinv;
+        e0 = f0; e1 = f1; e2 = f2; e3 = f3; e4 = f4;
+        normc_pow2(e0, e1, e2, e3, e4);
     }
-    return e0;
+    if (mmax < 2) return e0;   // no layer above the half-space: no normc
+    // the top layer's normc(): e0 / max|e|
+    double t1 = fmax(fmax(fmax(fabs(e0), fabs(e1)), fmax(fabs(e2), fabs(e3))), fabs(e4));
+    if (t1 < 1.0e-40) t1 = 1.0;
+    return e0 / t1;
 }
 
 // Love-wave secular function, surfdisp96.f:704-763: the Haskell-Thomson

@@ -28,6 +28,45 @@
 
 namespace dk {
 
+// ------------------------------------------------ reciprocal, square root
+// The sweep's results are held to 1e-5 of the oracle, not to bit parity, so
+// its divisions and square roots use the hardware approximations
+// (rcp.approx / rsqrt.approx, about 22 correct bits) refined by two
+// Newton-Raphson steps, each of which squares the relative error (below
+// 2^-52 after two): a few fused multiply-adds with no branch and no slow
+// path, where an IEEE division or sqrt inlines both.  Arguments are finite
+// and normal where these are used; a zero divisor gives inf/NaN as a
+// division would.
+__device__ __forceinline__ double ti_rcp(double x)
+{
+#ifdef __CUDA_ARCH__
+    double r;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+#else
+    return 1.0 / x;
+#endif
+}
+
+// sqrt(x), x >= 0: x / sqrt(x) by the refined reciprocal square root
+// (y <- y (3 - x y^2) / 2, twice).
+__device__ __forceinline__ double ti_sqrt(double x)
+{
+#ifdef __CUDA_ARCH__
+    double y;
+    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    const double h = 0.5 * x;
+    y = y * fma(-h * y, y, 1.5);
+    y = y * fma(-h * y, y, 1.5);
+    return x > 0.0 ? x * y : 0.0;
+#else
+    return sqrt(x);
+#endif
+}
+
 // ------------------------------------------------------------ complex
 struct zc { double re, im; };
 __device__ __forceinline__ zc Z(double r, double i = 0.0) { return {r, i}; }
@@ -36,23 +75,22 @@ __device__ __forceinline__ zc operator-(zc a, zc b) { return {a.re - b.re, a.im 
 __device__ __forceinline__ zc operator-(zc a) { return {-a.re, -a.im}; }
 __device__ __forceinline__ zc operator*(zc a, zc b) { return {a.re * b.re - a.im * b.im, a.re * b.im + a.im * b.re}; }
 __device__ __forceinline__ zc operator*(double s, zc a) { return {s * a.re, s * a.im}; }
+// |b|^2 of the layer quantities here (wavenumbers, eigenvalues, their
+// products) stays far inside the double range, so a / b is formed as
+// a conj(b) / |b|^2 without rescaling, and |z| is compared through |z|^2.
+__device__ __forceinline__ double znorm2(zc a) { return a.re * a.re + a.im * a.im; }
 __device__ __forceinline__ zc zdiv(zc a, zc b)
 {
-    if (fabs(b.re) >= fabs(b.im)) {
-        const double r = b.im / b.re, den = b.re + b.im * r;
-        return {(a.re + a.im * r) / den, (a.im - a.re * r) / den};
-    }
-    const double r = b.re / b.im, den = b.re * r + b.im;
-    return {(a.re * r + a.im) / den, (a.im * r - a.re) / den};
+    const double in = ti_rcp(znorm2(b));
+    return {(a.re * b.re + a.im * b.im) * in, (a.im * b.re - a.re * b.im) * in};
 }
-__device__ __forceinline__ double zabs(zc a) { return hypot(a.re, a.im); }
 __device__ __forceinline__ zc zsqrt(zc a)
 {
     // principal square root (branch cut on the negative real axis)
-    const double m = hypot(a.re, a.im);
-    double re = sqrt(0.5 * (m + fabs(a.re)));
+    const double m = ti_sqrt(znorm2(a));
+    double re = ti_sqrt(0.5 * (m + fabs(a.re)));
     if (re == 0.0) return Z(0.0, 0.0);
-    double im = a.im / (2.0 * re);
+    double im = a.im * ti_rcp(2.0 * re);
     if (a.re < 0.0) { const double t = fabs(im); im = copysign(re, a.im); re = t; }
     return {re, im};
 }
@@ -102,14 +140,14 @@ __device__ __forceinline__ void ti_eigen(const TiLayer& L, double omg, double wv
     const double cc = ddef * aabc;
     const double disc = bb * bb - 4.0 * cc;
     o.ok = disc >= 0.0;
-    const double srt = sqrt(fmax(disc, 0.0));
+    const double srt = ti_sqrt(fmax(disc, 0.0));
     double L1 = 0.5 * (bb + srt);
-    double L2 = fabs(L1) > 0.0 ? cc / L1 : 0.5 * (bb - srt);
+    double L2 = fabs(L1) > 0.0 ? cc * ti_rcp(L1) : 0.5 * (bb - srt);
     if (fabs(wvno2 - L2) < fabs(wvno2 - L1)) { const double t = L1; L1 = L2; L2 = t; }
     o.oscp = L1 < 0.0;
     o.oscs = L2 < 0.0;
-    o.rp = sqrt(fabs(L1));
-    o.rsv = sqrt(fabs(L2));
+    o.rp = ti_sqrt(fabs(L1));
+    o.rsv = ti_sqrt(fabs(L2));
     const double bcaa = b * c + a * a, ddef2 = d * d + e * f;
     double x12 = b * d - a * e;
     double x22 = b * L2 - e * bcaa;
@@ -120,9 +158,9 @@ __device__ __forceinline__ void ti_eigen(const TiLayer& L, double omg, double wv
     double x31 = d * L1 - a * ddef2;
     double x41 = -(L1 - a * d - b * f);
     if (wvn != 0.0) {
-        const double z1 = wvn / x11;
+        const double z1 = wvn * ti_rcp(x11);
         x11 *= z1; x21 *= z1; x31 *= z1; x41 *= z1;
-        const double z2 = wvn / x22;
+        const double z2 = wvn * ti_rcp(x22);
         x12 *= z2; x22 *= z2; x32 *= z2; x42 *= z2;
     }
     o.x11 = x11; o.x21 = x21; o.x31 = x31; o.x41 = x41;
@@ -146,7 +184,7 @@ __device__ __forceinline__ void ti_var_one(double r, bool osc, double dm, double
         cosf = 0.5 * (1.0 + fac);
         const double sn = 0.5 * (1.0 - fac);
         rsin = r * sn;
-        sinr = (fabs(pr) < 1.0e-5 && r < 1.0e-5) ? dm : sn / r;
+        sinr = (fabs(pr) < 1.0e-5 && r < 1.0e-5) ? dm : sn * ti_rcp(r);
     } else {
         const double pi = r * dm;
         ex = 0.0;
@@ -154,7 +192,7 @@ __device__ __forceinline__ void ti_var_one(double r, bool osc, double dm, double
         sincos(pi, &sn, &cs);
         cosf = cs;
         rsin = -r * sn;                               // (i r)(i sin)
-        sinr = (r < 1.0e-5) ? dm : sn / r;            // (i sin)/(i r)
+        sinr = (r < 1.0e-5) ? dm : sn * ti_rcp(r);    // (i sin)/(i r)
     }
 }
 
@@ -261,7 +299,7 @@ __device__ __forceinline__ void ti_compound_apply(const TiEig& E, const TiVar& v
 {
     const double ex = v.pex + v.svex;
     const double dfac = ex > 35.0 ? 0.0 : exp(-ex);
-    const double a1 = 0.5 / E.np, a2 = 0.5 / E.nsv;
+    const double a1 = 0.5 * ti_rcp(E.np), a2 = 0.5 * ti_rcp(E.nsv);
     double fac[3][4];
     fac[1][0] = 2.0 * a1 * v.cosp; fac[1][1] = 2.0 * a1 * v.sinpr; fac[1][2] = 2.0 * a1 * v.rsinp;
     fac[1][3] = 4.0 * a1 * a1 * dfac;
@@ -325,7 +363,7 @@ __device__ __forceinline__ void eig_to_z(const TiEig& E, TiEigZ& o)
 // ffunc/gfunc/h1func/h2func (tregn96.f:1385-1473)
 __device__ __forceinline__ zc ti_f(zc nub, double dm)
 {
-    if (zabs(nub) < 1.0e-08) return Z(dm);
+    if (znorm2(nub) < 1.0e-16) return Z(dm);
     const zc arg = dm * nub;
     const zc ex = arg.re < 40.0 ? zexp(-2.0 * arg) : Z(0.0);
     return zdiv(Z(1.0) - ex, 2.0 * nub);
@@ -338,14 +376,14 @@ __device__ __forceinline__ zc ti_g(zc nub, double dm)
 __device__ __forceinline__ zc ti_h1(zc nua, zc nub, double dm)
 {
     const zc s = nub + nua;
-    if (zabs(s) < 1.0e-08) return Z(dm);
+    if (znorm2(s) < 1.0e-16) return Z(dm);
     const zc arg = dm * s;
     const zc ex = arg.re < 40.0 ? zexp(-arg) : Z(0.0);
     return zdiv(Z(1.0) - ex, s);
 }
 __device__ __forceinline__ zc ti_h2(zc nua, zc nub, double dm)
 {
-    if (zabs(nub - nua) < 1.0e-08) return Z(dm);
+    if (znorm2(nub - nua) < 1.0e-16) return Z(dm);
     const zc ap = dm * nua, aq = dm * nub;
     const zc ep = ap.re < 40.0 ? zexp(-ap) : Z(0.0);
     const zc eq = aq.re < 40.0 ? zexp(-aq) : Z(0.0);
@@ -424,7 +462,7 @@ __device__ __forceinline__ TiWave ti_wave(double r, bool osc, double dm)
         w.cosf = 0.5 * (1.0 + fac);
         const double sn = 0.5 * (1.0 - fac);
         w.rsin = r * sn;
-        w.sinr = (fabs(pr) < 1.0e-5 && r < 1.0e-5) ? dm : sn / r;
+        w.sinr = (fabs(pr) < 1.0e-5 && r < 1.0e-5) ? dm : sn * ti_rcp(r);
         w.er = e1;
         w.ei = 0.0;
     } else {
@@ -434,7 +472,7 @@ __device__ __forceinline__ TiWave ti_wave(double r, bool osc, double dm)
         sincos(pi, &sn, &cs);
         w.cosf = cs;
         w.rsin = -r * sn;                             // (i r)(i sin)
-        w.sinr = (r < 1.0e-5) ? dm : sn / r;          // (i sin)/(i r)
+        w.sinr = (r < 1.0e-5) ? dm : sn * ti_rcp(r);  // (i sin)/(i r)
         w.er = cs;
         w.ei = -sn;
     }
@@ -450,17 +488,17 @@ __device__ __forceinline__ void ti_integrals_real(const TiEig& E, const TiWave& 
     const double ra = E.rp, rb = E.rsv;
     const double xa = dm * ra, xb = dm * rb;
     const double ea = P.er, eb = S.er;
-    const double FA = ra < 1.0e-08 ? dm : (1.0 - (xa < 40.0 ? ea * ea : 0.0)) / (2.0 * ra);
-    const double FB = rb < 1.0e-08 ? dm : (1.0 - (xb < 40.0 ? eb * eb : 0.0)) / (2.0 * rb);
+    const double FA = ra < 1.0e-08 ? dm : (1.0 - (xa < 40.0 ? ea * ea : 0.0)) * ti_rcp(2.0 * ra);
+    const double FB = rb < 1.0e-08 ? dm : (1.0 - (xb < 40.0 ? eb * eb : 0.0)) * ti_rcp(2.0 * rb);
     const double GA = xa < 75.0 ? dm * ea : 0.0;
     const double GB = xb < 75.0 ? dm * eb : 0.0;
     const double sab = rb + ra;
-    const double H1 = sab < 1.0e-08 ? dm : (1.0 - (dm * sab < 40.0 ? ea * eb : 0.0)) / sab;
+    const double H1 = sab < 1.0e-08 ? dm : (1.0 - (dm * sab < 40.0 ? ea * eb : 0.0)) * ti_rcp(sab);
     const double H2 = fabs(rb - ra) < 1.0e-08 ? dm
-                      : ((xb < 40.0 ? eb : 0.0) - (xa < 40.0 ? ea : 0.0)) / (ra - rb);
+                      : ((xb < 40.0 ? eb : 0.0) - (xa < 40.0 ? ea : 0.0)) * ti_rcp(ra - rb);
     const double x11 = E.x11, x21 = E.x21, x31 = E.x31, x41 = E.x41;
     const double x12 = E.x12, x22 = E.x22, x32 = E.x32, x42 = E.x42;
-    const double i1 = 1.0 / ((2.0 * ra) * E.np), i2 = 1.0 / ((2.0 * rb) * E.nsv);
+    const double i1 = ti_rcp((2.0 * ra) * E.np), i2 = ti_rcp((2.0 * rb) * E.nsv);
     double e[4][4], ei[4][4];
     ei[0][0] = (x41 * ra) * i1;    ei[1][0] = x42 * i2;
     ei[2][0] = (x41 * ra) * i1;    ei[3][0] = -(x42 * i2);
@@ -522,12 +560,12 @@ __device__ void ti_eigen_z(const TiLayer& L, double omg, double wvn, double wvno
     zc L1, L2;
     if (bb.re < 0.0 && srt.re < 0.0) {
         L2 = 0.5 * (bb - srt);
-        L1 = zabs(L2) > 0.0 ? zdiv(cc, L2) : 0.5 * (bb + srt);
+        L1 = znorm2(L2) > 0.0 ? zdiv(cc, L2) : 0.5 * (bb + srt);
     } else {
         L1 = 0.5 * (bb + srt);
-        L2 = zabs(L1) > 0.0 ? zdiv(cc, L1) : 0.5 * (bb - srt);
+        L2 = znorm2(L1) > 0.0 ? zdiv(cc, L1) : 0.5 * (bb - srt);
     }
-    if (zabs(Z(wvno2) - L2) < zabs(Z(wvno2) - L1)) { const zc t = L1; L1 = L2; L2 = t; }
+    if (znorm2(Z(wvno2) - L2) < znorm2(Z(wvno2) - L1)) { const zc t = L1; L1 = L2; L2 = t; }
     zc rp = zsqrt(L1), rsv = zsqrt(L2);
     if (rp.re < 0.0) rp = -rp;
     if (rsv.re < 0.0) rsv = -rsv;
@@ -570,7 +608,7 @@ __device__ __forceinline__ void ti_var_z_one(zc r, double dm, zc& cosf, zc& rsin
     cosf = ep + fac * em;
     const zc s = ep - fac * em;
     rsin = r * s;
-    sinr = (fabs(p.re) < 1.0e-5 && zabs(r) < 1.0e-5) ? Z(dm) : zdiv(s, r);
+    sinr = (fabs(p.re) < 1.0e-5 && znorm2(r) < 1.0e-10) ? Z(dm) : zdiv(s, r);
 }
 
 __device__ void ti_compound_z(const TiEigZ& E, const TiVarZ& v, double ca[5][5])
@@ -614,16 +652,11 @@ __device__ void ti_compound_z(const TiEigZ& E, const TiVarZ& v, double ca[5][5])
 
 __device__ void ti_haskell_z(const TiEigZ& E, const TiVarZ& V, double v[4], double& cpex)
 {
-    double fp = 1.0, fs = 1.0;
-    if (V.pex > V.svex) {
-        const double dd = V.pex - V.svex;
-        fs = dd > 40.0 ? 0.0 : exp(-dd);
-        cpex = V.pex;
-    } else {
-        const double dd = V.svex - V.pex;
-        fp = dd > 40.0 ? 0.0 : exp(-dd);
-        cpex = V.svex;
-    }
+    const bool pbig = V.pex > V.svex;
+    const double dd = fabs(V.pex - V.svex);
+    const double f = dd > 40.0 ? 0.0 : exp(-dd);
+    const double fp = pbig ? 1.0 : f, fs = pbig ? f : 1.0;
+    cpex = pbig ? V.pex : V.svex;
     const zc cosp = zdiv(fp * V.cosp, E.np), sinpr = zdiv(fp * V.sinpr, E.np), rsinp = zdiv(fp * V.rsinp, E.np);
     const zc cossv = zdiv(fs * V.cosq, E.nsv), sinsvr = zdiv(fs * V.sinqr, E.nsv), rsinsv = zdiv(fs * V.rsinq, E.nsv);
     const zc x11 = E.x11, x21 = E.x21, x31 = E.x31, x41 = E.x41;
@@ -649,17 +682,14 @@ __device__ void ti_haskell_z(const TiEigZ& E, const TiVarZ& V, double v[4], doub
 // Haskell matrix (hska, tregn96.f:3477-3559) applied to v: v <- AA v.
 __device__ __forceinline__ void ti_haskell(const TiEig& E, const TiVar& V, double v[4], double& cpex)
 {
-    double fp = 1.0, fs = 1.0;
-    if (V.pex > V.svex) {
-        const double dd = V.pex - V.svex;
-        fs = dd > 40.0 ? 0.0 : exp(-dd);
-        cpex = V.pex;
-    } else {
-        const double dd = V.svex - V.pex;
-        fp = dd > 40.0 ? 0.0 : exp(-dd);
-        cpex = V.svex;
-    }
-    const double inp = 1.0 / E.np, ins = 1.0 / E.nsv;
+    // the larger exponent is factored out; the other wave is scaled by
+    // exp(-|pex - svex|) (0 beyond 40)
+    const bool pbig = V.pex > V.svex;
+    const double dd = fabs(V.pex - V.svex);
+    const double f = dd > 40.0 ? 0.0 : exp(-dd);
+    const double fp = pbig ? 1.0 : f, fs = pbig ? f : 1.0;
+    cpex = pbig ? V.pex : V.svex;
+    const double inp = ti_rcp(E.np), ins = ti_rcp(E.nsv);
     const double cosp = fp * V.cosp * inp, sinpr = fp * V.sinpr * inp, rsinp = fp * V.rsinp * inp;
     const double cossv = fs * V.cosq * ins, sinsvr = fs * V.sinqr * ins, rsinsv = fs * V.rsinq * ins;
     const double x11 = E.x11, x21 = E.x21, x31 = E.x31, x41 = E.x41;
@@ -699,14 +729,14 @@ __device__ __forceinline__ void ti_fgh_w(zc ra, zc rb, const TiWave& P, const Ti
 {
     const zc ea = Z(P.er, P.ei), eb = Z(S.er, S.ei);
     const double xa = dm * ra.re, xb = dm * rb.re;
-    fg[0] = zabs(ra) < 1.0e-08 ? Z(dm) : zdiv(Z(1.0) - (xa < 40.0 ? ea * ea : Z(0.0)), 2.0 * ra);
+    fg[0] = znorm2(ra) < 1.0e-16 ? Z(dm) : zdiv(Z(1.0) - (xa < 40.0 ? ea * ea : Z(0.0)), 2.0 * ra);
     fg[1] = xa < 75.0 ? dm * ea : Z(0.0);
-    fg[2] = zabs(rb) < 1.0e-08 ? Z(dm) : zdiv(Z(1.0) - (xb < 40.0 ? eb * eb : Z(0.0)), 2.0 * rb);
+    fg[2] = znorm2(rb) < 1.0e-16 ? Z(dm) : zdiv(Z(1.0) - (xb < 40.0 ? eb * eb : Z(0.0)), 2.0 * rb);
     fg[3] = xb < 75.0 ? dm * eb : Z(0.0);
     const zc sab = rb + ra;
-    fg[4] = zabs(sab) < 1.0e-08 ? Z(dm)
+    fg[4] = znorm2(sab) < 1.0e-16 ? Z(dm)
             : zdiv(Z(1.0) - (dm * sab.re < 40.0 ? ea * eb : Z(0.0)), sab);
-    fg[5] = zabs(rb - ra) < 1.0e-08 ? Z(dm)
+    fg[5] = znorm2(rb - ra) < 1.0e-16 ? Z(dm)
             : zdiv((xb < 40.0 ? eb : Z(0.0)) - (xa < 40.0 ? ea : Z(0.0)), ra - rb);
 }
 
@@ -910,7 +940,13 @@ __device__ __forceinline__ void ti_task(const TiArgs& a, long long task, int lan
             double ee[5];
             double pexsv;
             if (E.ok) {
-                const TiWave P = ti_wave(E.rp, E.oscp, L.td), S = ti_wave(E.rsv, E.oscs, L.td);
+                // P and S waves through one copy of the wave code
+                TiWave P, S;
+#pragma unroll 1
+                for (int w = 0; w < 2; ++w) {
+                    const TiWave t = ti_wave(w ? E.rsv : E.rp, w ? E.oscs : E.oscp, L.td);
+                    if (w) S = t; else P = t;
+                }
                 TiVar V;
                 V.cosp = P.cosf; V.rsinp = P.rsin; V.sinpr = P.sinr; V.pex = P.ex;
                 V.cosq = S.cosf; V.rsinq = S.rsin; V.sinqr = S.sinr; V.svex = S.ex;
@@ -1076,6 +1112,8 @@ ti_kernel(TiArgs a)
     }
 }
 
+template __global__ void ti_kernel<2>(TiArgs);
+template __global__ void ti_kernel<3>(TiArgs);
 template __global__ void ti_kernel<4>(TiArgs);
 template __global__ void ti_kernel<6>(TiArgs);
 template __global__ void ti_kernel<8>(TiArgs);

@@ -39,6 +39,19 @@ static inline double __dsub_rn(double a, double b) { return a - b; }
 static inline double __ddiv_rn(double a, double b) { return a / b; }
 static inline double __dsqrt_rn(double a) { return std::sqrt(a); }
 static inline float __double2float_rn(double a) { return (float)a; }
+static inline int __double2hiint(double a)
+{
+    uint64_t u;
+    std::memcpy(&u, &a, 8);
+    return (int)(uint32_t)(u >> 32);
+}
+static inline double __hiloint2double(int hi, int lo)
+{
+    const uint64_t u = ((uint64_t)(uint32_t)hi << 32) | (uint32_t)lo;
+    double d;
+    std::memcpy(&d, &u, 8);
+    return d;
+}
 static inline double rsqrt(double x) { return 1.0 / std::sqrt(x); }
 static inline float rsqrtf(float x) { return 1.0f / std::sqrt(x); }
 static inline void __syncthreads() {}
