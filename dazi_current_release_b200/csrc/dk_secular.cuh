@@ -80,9 +80,14 @@ __device__ __forceinline__ double dltar4(const M& mdl, int mmax, double wvno, do
     double e2 = rho1 * (gamm1 - gammk * ra * rb);
     double e3 = rho1 * rb;
     double e4 = wvno2 - ra * rb;
+    // the next layer's record is loaded one step ahead: the loads of a
+    // column's table come from L2/DRAM (the resident columns' tables exceed
+    // L2) and a layer step is long enough to cover that latency
+    LayerD Ln = mdl.layer(mmax >= 2 ? mmax - 2 : 0);
 #pragma unroll 1
     for (int m = mmax - 2; m >= 0; --m) {
-        L = mdl.layer(m);
+        L = Ln;
+        Ln = mdl.layer(m > 0 ? m - 1 : 0);
         const double dpth = L.d;
         xka = omega * L.ia; xkb = omega * L.ib;
         gammk = L.b2 * tio2;
