@@ -314,9 +314,10 @@ def _events_timed(step, steps, warmup, dev, stream, flush, ws):
 
 
 def _work_constants():
-    """FP64 operations per layer item of the adjoint and Gc/Gs sweeps,
-    counted by ncu (dadd + dmul + 2 dfma per thread instruction) on a sample
-    of the uneven batch and divided by the sample's layer items."""
+    """FP64 operations and DRAM bytes per unit (root layer evaluation,
+    Gc/Gs layer item), counted by ncu (dadd + dmul + 2 dfma per thread
+    instruction; dram__bytes_read + write) on a 100000-column capture of the
+    uneven batch and divided by its units."""
     path = os.path.join(ROOT, "profiles", "kernel_work.json")
     try:
         return json.load(open(path))
@@ -485,7 +486,8 @@ def main_ragged(args, ws, rank, local):
             "frac": achieved / peak_tf if achieved and peak_tf > 0 else None,
             "traffic": traffic,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per unit on a "
-                              "12500-column sample, scaled by the units of this launch",
+                              "100000-column capture of this workload (profiles/kernel_work.json), "
+                              "scaled by the units of this launch",
             "phase_tflops": {k: flops[k] / (ph[k] * 1e-3) / 1e12 for k in flops if k in ph},
             "peak_source": "measured in-run FP64 FMA probe (dazi_dk_fp64_peak)",
             "kernel_ms": ph[dom], "flops_per_launch": flops.get(dom),

@@ -360,36 +360,6 @@ __device__ __forceinline__ void eig_to_z(const TiEig& E, TiEigZ& o)
     o.rsv = E.oscs ? Z(0.0, E.rsv) : Z(E.rsv);
 }
 
-// ffunc/gfunc/h1func/h2func (tregn96.f:1385-1473)
-__device__ __forceinline__ zc ti_f(zc nub, double dm)
-{
-    if (znorm2(nub) < 1.0e-16) return Z(dm);
-    const zc arg = dm * nub;
-    const zc ex = arg.re < 40.0 ? zexp(-2.0 * arg) : Z(0.0);
-    return zdiv(Z(1.0) - ex, 2.0 * nub);
-}
-__device__ __forceinline__ zc ti_g(zc nub, double dm)
-{
-    const zc arg = dm * nub;
-    return arg.re < 75.0 ? dm * zexp(-arg) : Z(0.0);
-}
-__device__ __forceinline__ zc ti_h1(zc nua, zc nub, double dm)
-{
-    const zc s = nub + nua;
-    if (znorm2(s) < 1.0e-16) return Z(dm);
-    const zc arg = dm * s;
-    const zc ex = arg.re < 40.0 ? zexp(-arg) : Z(0.0);
-    return zdiv(Z(1.0) - ex, s);
-}
-__device__ __forceinline__ zc ti_h2(zc nua, zc nub, double dm)
-{
-    if (znorm2(nub - nua) < 1.0e-16) return Z(dm);
-    const zc ap = dm * nua, aq = dm * nub;
-    const zc ep = ap.re < 40.0 ? zexp(-ap) : Z(0.0);
-    const zc eq = aq.re < 40.0 ? zexp(-aq) : Z(0.0);
-    return zdiv(eq - ep, nua - nub);
-}
-
 // The six energy integrals of a layer (intijr, tregn96.f:4073-4245):
 // (1,1) (1,3) (2,2) (2,4) (3,3) (4,4).  top/bot = (ur, uz, tz, tr) at the
 // layer's top and bottom interface; half = the lower half-space.  fg holds
@@ -544,7 +514,7 @@ __device__ __forceinline__ void ti_integrals_real(const TiEig& E, const TiWave& 
 // departs from 1).  The layer's propagators are real by construction; as in
 // tregn96 the compound and Haskell matrices are formed in complex arithmetic
 // and their real parts carried on.
-__device__ void ti_eigen_z(const TiLayer& L, double omg, double wvn, double wvno2, TiEigZ& o)
+__device__ __noinline__ void ti_eigen_z(const TiLayer& L, double omg, double wvn, double wvno2, TiEigZ& o)
 {
     const double om2 = omg * omg;
     const double wvn2 = wvn * wvn;
@@ -597,7 +567,7 @@ struct TiVarZ {
     double pex, svex;
 };
 
-__device__ __forceinline__ void ti_var_z_one(zc r, double dm, zc& cosf, zc& rsin, zc& sinr, double& ex)
+__device__ __noinline__ void ti_var_z_one(zc r, double dm, zc& cosf, zc& rsin, zc& sinr, double& ex)
 {
     const zc p = dm * r;
     ex = p.re;
@@ -714,13 +684,26 @@ __device__ __forceinline__ void ti_haskell(const TiEig& E, const TiVar& V, doubl
     for (int i = 0; i < 4; ++i) v[i] = o[i];
 }
 
-// ffunc/gfunc/h1func/h2func values (FA, GA, FB, GB, H1, H2) of a layer by
-// complex exponentials (layers with complex eigenvalues).
+// ffunc/gfunc/h1func/h2func values (tregn96.f:1385-1473: FA, GA, FB, GB,
+// H1, H2) of a layer by complex exponentials (layers with complex
+// eigenvalues): exp(-nu d) of the
+// two waves once, exp(-2 nu d) and exp(-(nu_a + nu_b) d) as their products,
+// with the reference's cut-offs on the real part of the exponent (40, and
+// 75 for gfunc).  Re(nu) >= 0, so the products cannot overflow.
 __device__ __forceinline__ void ti_fgh_z(zc ra, zc rb, double dm, zc fg[6])
 {
-    fg[0] = ti_f(ra, dm); fg[1] = ti_g(ra, dm);
-    fg[2] = ti_f(rb, dm); fg[3] = ti_g(rb, dm);
-    fg[4] = ti_h1(ra, rb, dm); fg[5] = ti_h2(ra, rb, dm);
+    const zc aa = dm * ra, ab = dm * rb;
+    const zc ea = aa.re < 75.0 ? zexp(-aa) : Z(0.0);
+    const zc eb = ab.re < 75.0 ? zexp(-ab) : Z(0.0);
+    fg[0] = znorm2(ra) < 1.0e-16 ? Z(dm) : zdiv(Z(1.0) - (aa.re < 40.0 ? ea * ea : Z(0.0)), 2.0 * ra);
+    fg[1] = dm * ea;
+    fg[2] = znorm2(rb) < 1.0e-16 ? Z(dm) : zdiv(Z(1.0) - (ab.re < 40.0 ? eb * eb : Z(0.0)), 2.0 * rb);
+    fg[3] = dm * eb;
+    const zc sab = rb + ra;
+    fg[4] = znorm2(sab) < 1.0e-16 ? Z(dm)
+            : zdiv(Z(1.0) - (dm * sab.re < 40.0 ? ea * eb : Z(0.0)), sab);
+    fg[5] = znorm2(rb - ra) < 1.0e-16 ? Z(dm)
+            : zdiv((ab.re < 40.0 ? eb : Z(0.0)) - (aa.re < 40.0 ? ea : Z(0.0)), ra - rb);
 }
 
 // The same from the waves' ea = exp(-nu d) (real eigenvalues).
