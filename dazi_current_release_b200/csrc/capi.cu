@@ -131,6 +131,11 @@ struct Context {
     PhaseTimer timer;
     int device = -1;
     cudaStream_t stream = nullptr;
+    // host entries: results that are final before the Gc/Gs sweep (pv and
+    // the sensitivity kernels) are copied to the host on cstream, after
+    // outs_ready, while the sweep runs on stream
+    cudaStream_t cstream = nullptr;
+    cudaEvent_t outs_ready = nullptr;
     // host-entry staging
     DBuf vel, vp, rho, per, depz, pv, svs, svp, srh, status;
     // work buffers
@@ -213,6 +218,8 @@ int ensure_context()
     }
     CK(cudaGetDevice(&g_ctx.device));
     CK(cudaStreamCreateWithFlags(&g_ctx.stream, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&g_ctx.cstream, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&g_ctx.outs_ready, cudaEventDisableTiming));
     g_ctx.ready = true;
     return 0;
 }
@@ -498,8 +505,10 @@ int run_ti(const Tables& T, const double* per, const StageOut& o, long long maxr
 }
 
 // The per-(column, period) kernels and the root search over built tables.
+// outs_ready (optional) is recorded once pv and the sensitivity kernels are
+// final, before the Gc/Gs sweep.
 int run_tables(const Tables& T, const double* per, const StageOut& o, int form, bool fd_done,
-               cudaStream_t st, Work& W, const LaunchCfg& cfg)
+               cudaStream_t st, Work& W, const LaunchCfg& cfg, cudaEvent_t outs_ready = nullptr)
 {
     int r;
     const bool adj = o.svs && (form & 1) == DAZI_FORM_ADJOINT;
@@ -508,6 +517,7 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
     if ((r = ensure_sweep_scratch(T, adj, o.lsen != nullptr, maxr, cfg, W))) return r;
     if (!fd_done && (r = run_root(T, per, o, form, adj, W, cfg, st))) return r;
     if (adj && (r = run_adjoint(T, per, o, maxr, W, cfg, st))) return r;
+    if (outs_ready) CK(cudaEventRecord(outs_ready, st));
     if (o.lsen && (r = run_ti(T, per, o, maxr, W, cfg, st))) return r;
     return 0;
 }
@@ -520,7 +530,7 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
 //   Lsen requested   : per-(column, period) TI sweeps from the phase velocity
 int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, const float* rho,
                  const StageOut& o, int kmax, const double* per, long long col_start,
-                 long long col_count, int form, cudaStream_t st)
+                 long long col_count, int form, cudaStream_t st, cudaEvent_t outs_ready = nullptr)
 {
     const long long ncol = (long long)nx * ny;
     if (col_count == 0) return 0;
@@ -562,7 +572,10 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
             ++g_ctx.last_launches;
         }
         phase_mark("fd", st);
-        if (!o.lsen) return 0;
+        if (!o.lsen) {
+            if (outs_ready) CK(cudaEventRecord(outs_ready, st));
+            return 0;
+        }
     }
     ColSrc src;
     src.ragged = false; src.ncol = ncol; src.col0 = col_start - 1;
@@ -573,7 +586,7 @@ int stage_device(int nx, int ny, int nz, const float* vel, const float* vp, cons
     PrepOut po{nullptr, nullptr, g_ctx.w.counters.as<unsigned long long>() + 4};
     Tables T;
     if ((r = build_tables(src, col_count, po, ncol, ncol, ncol, st, T, g_ctx.w))) return r;
-    return run_tables(T, per, o, form, fd, st, g_ctx.w, default_cfg());
+    return run_tables(T, per, o, form, fd, st, g_ctx.w, default_cfg(), outs_ready);
 }
 
 // Ragged batch on device pointers.
@@ -591,7 +604,8 @@ struct BatchIn {
     const long long* ls_off;
 };
 
-int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
+int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st,
+                 cudaEvent_t outs_ready = nullptr)
 {
     if (B.ncols == 0) return 0;
     int r;
@@ -654,7 +668,7 @@ int batch_device(const BatchIn& B, const StageOut& o, int form, cudaStream_t st)
         }
         phase_mark("fd", st);
     }
-    return run_tables(T, B.periods, o, form, fd, st, g_ctx.w, default_cfg());
+    return run_tables(T, B.periods, o, form, fd, st, g_ctx.w, default_cfg(), outs_ready);
 }
 
 // ------------------------------------------------------------------ plans
@@ -899,20 +913,23 @@ int stage_host(const int* pnx, const int* pny, const int* pnz, const float* vel,
     o.status = g_ctx.status.as<int>();
     r = stage_device(nx, ny, nz, g_ctx.vel.as<float>(), vp ? g_ctx.vp.as<float>() : nullptr,
                      vp ? g_ctx.rho.as<float>() : nullptr, o, kmax, g_ctx.per.as<double>(),
-                     col_start, col_count, form, st);
+                     col_start, col_count, form, st, g_ctx.outs_ready);
     if (r) return r;
     // Copy back only the written columns: every (k[, i]) slab holds the
-    // column range contiguously.
+    // column range contiguously.  pv and the sensitivity kernels go on the
+    // copy stream as soon as they are final, overlapping the Gc/Gs sweep.
     const size_t c0 = (size_t)(col_start - 1), cn = (size_t)col_count;
+    cudaStream_t cs = g_ctx.cstream;
+    CK(cudaStreamWaitEvent(cs, g_ctx.outs_ready, 0));
     CK(cudaMemcpy2DAsync(pv + c0, sizeof(double) * ncol, g_ctx.pv.as<double>() + c0, sizeof(double) * ncol,
-                         sizeof(double) * cn, kmax, cudaMemcpyDeviceToHost, st));
+                         sizeof(double) * cn, kmax, cudaMemcpyDeviceToHost, cs));
     if (kern) {
         double* hs[3] = {svs, svp, srh};
         DBuf* ds[3] = {&g_ctx.svs, &g_ctx.svp, &g_ctx.srh};
         for (int q = 0; q < 3; ++q)
             CK(cudaMemcpy2DAsync(hs[q] + c0, sizeof(double) * ncol, ds[q]->as<double>() + c0,
                                  sizeof(double) * ncol, sizeof(double) * cn, (size_t)kmax * nz,
-                                 cudaMemcpyDeviceToHost, st));
+                                 cudaMemcpyDeviceToHost, cs));
     }
     if (lsen)
         CK(cudaMemcpy2DAsync(lsen + c0, sizeof(float) * ncol, g_ctx.lsen.as<float>() + c0,
@@ -924,6 +941,7 @@ int stage_host(const int* pnx, const int* pny, const int* pnz, const float* vel,
     CK(cudaMemcpyAsync(hflag, g_ctx.w.counters.as<unsigned long long>() + 1, sizeof(int) * 2,
                        cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    CK(cudaStreamSynchronize(cs));
     g_ctx.last_ncol = ncol;
     if (hflag[0]) {
         set_err("non-finite Lsen_Gsc value (degenerate layer: Vp <= Vs?)");
@@ -1145,12 +1163,16 @@ int dazi_dk_batch(long long ncols, const long long* node_off, const float* depz,
     o.srh = sen_vs ? g_ctx.bsrh.as<double>() : nullptr;
     o.lsen = lsen ? g_ctx.blsen.as<float>() : nullptr;
     o.status = g_ctx.bstatus.as<int>();
-    if ((r = batch_device(B, o, form, st))) return r;
-    CK(cudaMemcpyAsync(pv, o.pv, sizeof(double) * np_, cudaMemcpyDeviceToHost, st));
+    // the kernels are queued first; pv and the sensitivity kernels then go to
+    // the host on the copy stream while the Gc/Gs sweep runs
+    if ((r = batch_device(B, o, form, st, g_ctx.outs_ready))) return r;
+    cudaStream_t cs = g_ctx.cstream;
+    CK(cudaStreamWaitEvent(cs, g_ctx.outs_ready, 0));
+    CK(cudaMemcpyAsync(pv, o.pv, sizeof(double) * np_, cudaMemcpyDeviceToHost, cs));
     if (sen_vs) {
-        CK(cudaMemcpyAsync(sen_vs, o.svs, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(sen_vp, o.svp, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
-        CK(cudaMemcpyAsync(sen_rho, o.srh, sizeof(double) * ns, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(sen_vs, o.svs, sizeof(double) * ns, cudaMemcpyDeviceToHost, cs));
+        CK(cudaMemcpyAsync(sen_vp, o.svp, sizeof(double) * ns, cudaMemcpyDeviceToHost, cs));
+        CK(cudaMemcpyAsync(sen_rho, o.srh, sizeof(double) * ns, cudaMemcpyDeviceToHost, cs));
     }
     if (lsen) CK(cudaMemcpyAsync(lsen, o.lsen, sizeof(float) * nl, cudaMemcpyDeviceToHost, st));
     std::vector<int> hst(ncols);
@@ -1158,6 +1180,7 @@ int dazi_dk_batch(long long ncols, const long long* node_off, const float* depz,
     int hflag = 0;
     CK(cudaMemcpyAsync(&hflag, g_ctx.w.counters.as<unsigned long long>() + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
+    CK(cudaStreamSynchronize(cs));
     if (status) std::memcpy(status, hst.data(), sizeof(int) * ncols);
     if (hflag) { set_err("non-finite Lsen_Gsc value (degenerate layer: Vp <= Vs?)"); return DAZI_ERR_MODEL; }
     for (long long c = 0; c < ncols; ++c)
@@ -1403,8 +1426,10 @@ void dazi_dk_finalize(void)
                    &g_ctx.w.ttasklist, &g_ctx.cbufoff, &g_ctx.bnode, &g_ctx.bper, &g_ctx.bdep,
                    &g_ctx.bvs, &g_ctx.bvp, &g_ctx.brho, &g_ctx.bperiods, &g_ctx.bsenoff,
                    &g_ctx.blsoff, &g_ctx.bpv, &g_ctx.bsvs, &g_ctx.bsvp, &g_ctx.bsrh, &g_ctx.blsen,
-                   &g_ctx.bstatus};
+                   &g_ctx.bstatus, &g_ctx.goff, &g_ctx.gtmp, &g_ctx.gerr};
     for (DBuf* b : all) b->release();
+    if (g_ctx.outs_ready) cudaEventDestroy(g_ctx.outs_ready);
+    if (g_ctx.cstream) cudaStreamDestroy(g_ctx.cstream);
     if (g_ctx.stream) cudaStreamDestroy(g_ctx.stream);
     g_ctx = Context();
 }
