@@ -493,6 +493,17 @@ def main_ragged(args, ws, rank, local):
             "kernel_ms": ph[dom], "flops_per_launch": flops.get(dom),
             "phase_ms": ph, "layer_items": layer_items, "secular_evals": evals,
             "root_layer_evals": layer_evals}
+    # algorithmic work of the whole step: sum over column-periods of
+    # rmax x 180 x (E + 4), E = the root search's secular evaluations (the
+    # reference's sequence of points), 180 FP64 flops per layer of one
+    # evaluation (sqrt and division counted as one, transcendentals not
+    # counted), + 4 forward-equivalent sweeps for the adjoint and Gc/Gs
+    # kernels; sum rmax x E = root_layer_evals, sum rmax = layer_items
+    alg = FLOP_PER_LAYER_EVAL * (layer_evals + 4 * layer_items)
+    roof["algorithmic"] = {
+        "flop_per_step": alg, "tflops": alg / (ms_per_step * 1e-3) / 1e12,
+        "frac": alg / (ms_per_step * 1e-3) / 1e12 / peak_tf if peak_tf > 0 else None,
+        "formula": "sum over column-periods of rmax x 180 x (E_ref + 4), over the whole step"}
     line = {
         "metric": "kernel column-periods/s", "value": value, "unit": "column-periods/s",
         "n_gpus": ws, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step,
