@@ -449,65 +449,6 @@ __device__ __forceinline__ TiWave ti_wave(double r, bool osc, double dm)
     return w;
 }
 
-// Energy integrals of an evanescent layer (both vertical wavenumbers real):
-// the same sums as ti_integrals_z in real arithmetic.
-__device__ __forceinline__ void ti_integrals_real(const TiEig& E, const TiWave& P, const TiWave& S,
-                                                  double dm, const double top[4], const double bot[4],
-                                                  double out[6])
-{
-    const double ra = E.rp, rb = E.rsv;
-    const double xa = dm * ra, xb = dm * rb;
-    const double ea = P.er, eb = S.er;
-    const double FA = ra < 1.0e-08 ? dm : (1.0 - (xa < 40.0 ? ea * ea : 0.0)) * ti_rcp(2.0 * ra);
-    const double FB = rb < 1.0e-08 ? dm : (1.0 - (xb < 40.0 ? eb * eb : 0.0)) * ti_rcp(2.0 * rb);
-    const double GA = xa < 75.0 ? dm * ea : 0.0;
-    const double GB = xb < 75.0 ? dm * eb : 0.0;
-    const double sab = rb + ra;
-    const double H1 = sab < 1.0e-08 ? dm : (1.0 - (dm * sab < 40.0 ? ea * eb : 0.0)) * ti_rcp(sab);
-    const double H2 = fabs(rb - ra) < 1.0e-08 ? dm
-                      : ((xb < 40.0 ? eb : 0.0) - (xa < 40.0 ? ea : 0.0)) * ti_rcp(ra - rb);
-    const double x11 = E.x11, x21 = E.x21, x31 = E.x31, x41 = E.x41;
-    const double x12 = E.x12, x22 = E.x22, x32 = E.x32, x42 = E.x42;
-    const double i1 = ti_rcp((2.0 * ra) * E.np), i2 = ti_rcp((2.0 * rb) * E.nsv);
-    double e[4][4], ei[4][4];
-    ei[0][0] = (x41 * ra) * i1;    ei[1][0] = x42 * i2;
-    ei[2][0] = (x41 * ra) * i1;    ei[3][0] = -(x42 * i2);
-    ei[0][1] = -(x31 * i1);        ei[1][1] = -((x32 * rb) * i2);
-    ei[2][1] = x31 * i1;           ei[3][1] = -((x32 * rb) * i2);
-    ei[0][2] = -((x21 * ra) * i1); ei[1][2] = -(x22 * i2);
-    ei[2][2] = -((x21 * ra) * i1); ei[3][2] = x22 * i2;
-    ei[0][3] = x11 * i1;           ei[1][3] = (x12 * rb) * i2;
-    ei[2][3] = -(x11 * i1);        ei[3][3] = (x12 * rb) * i2;
-    e[0][0] = x11; e[1][0] = x21 * ra; e[2][0] = x31; e[3][0] = x41 * ra;
-    e[0][1] = x12 * rb; e[1][1] = x22; e[2][1] = x32 * rb; e[3][1] = x42;
-    e[0][2] = x11; e[1][2] = -(x21 * ra); e[2][2] = x31; e[3][2] = -(x41 * ra);
-    e[0][3] = -(x12 * rb); e[1][3] = x22; e[2][3] = -(x32 * rb); e[3][3] = x42;
-    auto pot = [&](int r, const double u[4]) {
-        return (u[0] * ei[r][0] + u[1] * ei[r][1]) + (u[2] * ei[r][2] + u[3] * ei[r][3]);
-    };
-    const double km1pd = pot(2, top), km1sd = pot(3, top);
-    const double kmpu = pot(0, bot), kmsu = pot(1, bot);
-    const double pu2 = kmpu * kmpu, pd2 = km1pd * km1pd, su2 = kmsu * kmsu, sd2 = km1sd * km1sd;
-    const double pusu = kmpu * kmsu, pdsd = km1pd * km1sd, pusd = kmpu * km1sd, pdsu = km1pd * kmsu;
-    const double pupd = kmpu * km1pd, susd = kmsu * km1sd;
-    constexpr int IJ[6][2] = {{0, 0}, {0, 2}, {1, 1}, {1, 3}, {2, 2}, {3, 3}};
-#pragma unroll
-    for (int q = 0; q < 6; ++q) {
-        const int i = IJ[q][0], j = IJ[q][1];
-        auto EE = [&](int a, int b) { return e[i][a] * e[j][b]; };
-        auto SY = [&](int a, int b) { return EE(a, b) + EE(b, a); };
-        double r = (EE(0, 0) * pu2) * FA;
-        r = r + (EE(2, 2) * pd2) * FA;
-        r = r + (EE(1, 1) * su2) * FB;
-        r = r + (EE(3, 3) * sd2) * FB;
-        r = r + H1 * (SY(0, 1) * pusu + SY(2, 3) * pdsd);
-        r = r + H2 * (SY(0, 3) * pusd + SY(1, 2) * pdsu);
-        r = r + GA * (SY(0, 2) * pupd);
-        r = r + GB * (SY(1, 3) * susd);
-        out[q] = r;
-    }
-}
-
 // ----------------------------------------------------- complex layer path
 // A layer whose TI eigenvalues form a complex-conjugate pair (deep layers
 // at short periods, where tregn96's flattening leaves F unmapped and eta
@@ -685,11 +626,10 @@ __device__ __forceinline__ void ti_haskell(const TiEig& E, const TiVar& V, doubl
 }
 
 // ffunc/gfunc/h1func/h2func values (tregn96.f:1385-1473: FA, GA, FB, GB,
-// H1, H2) of a layer by complex exponentials (layers with complex
-// eigenvalues): exp(-nu d) of the
-// two waves once, exp(-2 nu d) and exp(-(nu_a + nu_b) d) as their products,
-// with the reference's cut-offs on the real part of the exponent (40, and
-// 75 for gfunc).  Re(nu) >= 0, so the products cannot overflow.
+// H1, H2) of a layer with complex eigenvalues: exp(-nu d) of the two waves
+// once, exp(-2 nu d) and exp(-(nu_a + nu_b) d) as their products, with the
+// reference's cut-offs on the real part of the exponent (40, and 75 for
+// gfunc).  Re(nu) >= 0, so the products cannot overflow.
 __device__ __forceinline__ void ti_fgh_z(zc ra, zc rb, double dm, zc fg[6])
 {
     const zc aa = dm * ra, ab = dm * rb;
@@ -706,21 +646,90 @@ __device__ __forceinline__ void ti_fgh_z(zc ra, zc rb, double dm, zc fg[6])
             : zdiv((ab.re < 40.0 ? eb : Z(0.0)) - (aa.re < 40.0 ? ea : Z(0.0)), ra - rb);
 }
 
-// The same from the waves' ea = exp(-nu d) (real eigenvalues).
-__device__ __forceinline__ void ti_fgh_w(zc ra, zc rb, const TiWave& P, const TiWave& S, double dm,
-                                         zc fg[6])
+// Energy integrals of a layer with real eigenvalues, evanescent and
+// oscillatory waves alike: the sums of ti_integrals_z, in mostly real
+// arithmetic, with one code path for both kinds of layer (so the lanes of a
+// warp do not split between them).
+//   - Each entry of E is a real factor times 1, nu_a or nu_b (nu = r for an
+//     evanescent wave, i r for an oscillatory one).  The six integrals pair
+//     rows (i, j) of equal parity, so e[i][a] e[j][b] is real for two P or
+//     two S columns (times nu^2 = +-r^2 where the rows carry nu), and real
+//     times nu_b (even rows) or nu_a (odd rows) for a P and an S column.
+//   - The potentials are A + B / nu with A, B real.
+//   - With the ten products W = (potential product) x (ffunc, gfunc,
+//     h1func, h2func value), each integral is a real combination of Re W
+//     and Re(nu W).
+__device__ __forceinline__ zc ti_over_nu(double A, double B, double ir, bool osc)
 {
+    // A + B / nu: 1 / nu = 1 / r, or -i / r
+    return osc ? Z(A, -B * ir) : Z(A + B * ir, 0.0);
+}
+__device__ __forceinline__ double ti_re_nu(double r, bool osc, zc w)
+{
+    // Re(nu w)
+    return osc ? -r * w.im : r * w.re;
+}
+__device__ __forceinline__ void ti_integrals_wave(const TiEig& E, const TiWave& P, const TiWave& S,
+                                                  double dm, const double top[4], const double bot[4],
+                                                  double out[6])
+{
+    const double ra = E.rp, rb = E.rsv;
+    const bool oa = E.oscp, ob = E.oscs;
+    const double ira = ti_rcp(ra), irb = ti_rcp(rb);
+    const double x11 = E.x11, x21 = E.x21, x31 = E.x31, x41 = E.x41;
+    const double x12 = E.x12, x22 = E.x22, x32 = E.x32, x42 = E.x42;
+    // potentials: rows 0 / 2 of E^-1 (P up / down) and 1 / 3 (S up / down)
+    const double hp = 0.5 * ti_rcp(E.np), hs = 0.5 * ti_rcp(E.nsv);
+    const zc kmpu = ti_over_nu((bot[0] * x41 - bot[2] * x21) * hp, (bot[3] * x11 - bot[1] * x31) * hp, ira, oa);
+    const zc km1pd = ti_over_nu((top[0] * x41 - top[2] * x21) * hp, (top[1] * x31 - top[3] * x11) * hp, ira, oa);
+    const zc kmsu = ti_over_nu((bot[3] * x12 - bot[1] * x32) * hs, (bot[0] * x42 - bot[2] * x22) * hs, irb, ob);
+    const zc km1sd = ti_over_nu((top[3] * x12 - top[1] * x32) * hs, (top[2] * x22 - top[0] * x42) * hs, irb, ob);
+    // ffunc/gfunc/h1func/h2func from the waves' exp(-nu d), with the
+    // reference's cut-offs on the real part of nu d (40; 75 for gfunc)
     const zc ea = Z(P.er, P.ei), eb = Z(S.er, S.ei);
-    const double xa = dm * ra.re, xb = dm * rb.re;
-    fg[0] = znorm2(ra) < 1.0e-16 ? Z(dm) : zdiv(Z(1.0) - (xa < 40.0 ? ea * ea : Z(0.0)), 2.0 * ra);
-    fg[1] = xa < 75.0 ? dm * ea : Z(0.0);
-    fg[2] = znorm2(rb) < 1.0e-16 ? Z(dm) : zdiv(Z(1.0) - (xb < 40.0 ? eb * eb : Z(0.0)), 2.0 * rb);
-    fg[3] = xb < 75.0 ? dm * eb : Z(0.0);
-    const zc sab = rb + ra;
-    fg[4] = znorm2(sab) < 1.0e-16 ? Z(dm)
-            : zdiv(Z(1.0) - (dm * sab.re < 40.0 ? ea * eb : Z(0.0)), sab);
-    fg[5] = znorm2(rb - ra) < 1.0e-16 ? Z(dm)
-            : zdiv((xb < 40.0 ? eb : Z(0.0)) - (xa < 40.0 ? ea : Z(0.0)), ra - rb);
+    const double xa = oa ? 0.0 : dm * ra, xb = ob ? 0.0 : dm * rb;
+    auto ffun = [&](double r, bool osc, double x, zc e) {
+        if (r < 1.0e-08) return Z(dm);
+        const zc n = Z(1.0) - (x < 40.0 ? e * e : Z(0.0));
+        const double h = 0.5 * ti_rcp(r);           // n / (2 nu)
+        return osc ? Z(n.im * h, -n.re * h) : Z(n.re * h, n.im * h);
+    };
+    const zc FA = ffun(ra, oa, xa, ea), FB = ffun(rb, ob, xb, eb);
+    const zc GA = xa < 75.0 ? dm * ea : Z(0.0);
+    const zc GB = xb < 75.0 ? dm * eb : Z(0.0);
+    const zc nua = oa ? Z(0.0, ra) : Z(ra), nub = ob ? Z(0.0, rb) : Z(rb);
+    const zc sab = nub + nua;
+    const zc H1 = znorm2(sab) < 1.0e-16 ? Z(dm)
+                  : zdiv(Z(1.0) - (dm * sab.re < 40.0 ? ea * eb : Z(0.0)), sab);
+    const zc H2 = znorm2(nub - nua) < 1.0e-16 ? Z(dm)
+                  : zdiv((xb < 40.0 ? eb : Z(0.0)) - (xa < 40.0 ? ea : Z(0.0)), nua - nub);
+    // the ten products
+    const zc W1 = (kmpu * kmpu) * FA, W2 = (km1pd * km1pd) * FA;
+    const zc W3 = (kmsu * kmsu) * FB, W4 = (km1sd * km1sd) * FB;
+    const zc W5 = (kmpu * kmsu) * H1, W6 = (km1pd * km1sd) * H1;
+    const zc W7 = (kmpu * km1sd) * H2, W8 = (km1pd * kmsu) * H2;
+    const zc W9 = (kmpu * km1pd) * GA, W10 = (kmsu * km1sd) * GB;
+    const double U5a = ti_re_nu(ra, oa, W5), U6a = ti_re_nu(ra, oa, W6);
+    const double U7a = ti_re_nu(ra, oa, W7), U8a = ti_re_nu(ra, oa, W8);
+    const double U5b = ti_re_nu(rb, ob, W5), U6b = ti_re_nu(rb, ob, W6);
+    const double U7b = ti_re_nu(rb, ob, W7), U8b = ti_re_nu(rb, ob, W8);
+    const double kaa = oa ? -(ra * ra) : ra * ra, kbb = ob ? -(rb * rb) : rb * rb;   // nu^2
+    // real factors of E (the nu factors taken out)
+    const double ep[4][4] = {{x11, x12, x11, -x12}, {x21, x22, -x21, x22},
+                             {x31, x32, x31, -x32}, {x41, x42, -x41, x42}};
+    constexpr int IJ[6][2] = {{0, 0}, {0, 2}, {1, 1}, {1, 3}, {2, 2}, {3, 3}};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const int i = IJ[q][0], j = IJ[q][1];
+        const bool odd = (i & 1) != 0;
+        auto ee = [&](int a, int b) { return ep[i][a] * ep[j][b]; };
+        auto sy = [&](int a, int b) { return ee(a, b) + ee(b, a); };
+        const double pp = ee(0, 0) * W1.re + ee(2, 2) * W2.re + sy(0, 2) * W9.re;
+        const double ss = ee(1, 1) * W3.re + ee(3, 3) * W4.re + sy(1, 3) * W10.re;
+        const double mx = odd ? sy(0, 1) * U5a + sy(2, 3) * U6a + sy(0, 3) * U7a + sy(1, 2) * U8a
+                              : sy(0, 1) * U5b + sy(2, 3) * U6b + sy(0, 3) * U7b + sy(1, 2) * U8b;
+        out[q] = (odd ? kaa : 1.0) * pp + (odd ? 1.0 : kbb) * ss + mx;
+    }
 }
 
 // Small fixed-size vectors passed by value to the out-of-line paths (so
@@ -760,20 +769,6 @@ __device__ __noinline__ DownOut ti_down_general(TiLayer L, double omega, double 
     DownOut o;
     o.vv = vv;
     ti_haskell_z(EZ, VZ, o.vv.v, o.cpex);
-    return o;
-}
-
-// Energy integrals of a layer with an oscillatory wave (real eigenvalues,
-// imaginary vertical wavenumber): complex arithmetic, exponentials from the
-// waves.
-__device__ __noinline__ D6 ti_integrals_osc(TiEig E, TiWave P, TiWave S, double dm, D4 top, D4 bot)
-{
-    TiEigZ EZ;
-    eig_to_z(E, EZ);
-    zc fg[6];
-    ti_fgh_w(EZ.rp, EZ.rsv, P, S, dm, fg);
-    D6 o;
-    ti_integrals_z(EZ, fg, top.v, bot.v, false, o.v);
     return o;
 }
 
@@ -1005,14 +1000,14 @@ __device__ __forceinline__ void ti_task(const TiArgs& a, long long task, int lan
             }
             // energy integrals of layer m (typelyr 0, or 1 for the half-space)
             double I[6];
-            if (fast && !E.oscp && !E.oscs) {
-                ti_integrals_real(E, P, S, L.td, top, bot, I);
+            if (fast) {
+                // real eigenvalues, evanescent or oscillatory waves: one path
+                ti_integrals_wave(E, P, S, L.td, top, bot, I);
             } else {
                 D4 t4, b4;
 #pragma unroll
                 for (int i = 0; i < 4; ++i) { t4.v[i] = top[i]; b4.v[i] = bot[i]; }
-                const D6 r = fast ? ti_integrals_osc(E, P, S, L.td, t4, b4)
-                                  : ti_integrals_general(L, omega, wvno, wvno2, t4, b4, half);
+                const D6 r = ti_integrals_general(L, omega, wvno, wvno2, t4, b4, half);
 #pragma unroll
                 for (int i = 0; i < 6; ++i) I[i] = r.v[i];
             }
