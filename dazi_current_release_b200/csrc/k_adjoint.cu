@@ -30,6 +30,7 @@
 // root.  The root itself is the phase-1 root refined by a secant step inside
 // the reference's final Neville bracket.
 #include "dk_secular.cuh"
+#include "dk_fastmath.cuh"
 #include "dk_kernels.cuh"
 
 namespace dk {
@@ -64,6 +65,7 @@ __device__ __forceinline__ D3 div_by(const D3& a, const D3& b, double ib)
 struct WaveD3 {
     D3 r, cosf, sinr, rsin;   // cos, sin/r, r*sin  (x = -r sin in the oscillatory case)
     double scale_exp;         // factored-out exponent (0 when oscillatory)
+    double escale;            // exp(-scale_exp) (1 when oscillatory)
     bool evan;
 };
 
@@ -73,8 +75,8 @@ __device__ __forceinline__ void wave_d3(const D3& wvno, const D3& xk, double d, 
     const D3 t = wvno - xk;
     const double sg = t.v < 0.0 ? -1.0 : 1.0;
     const D3 prod = s * (sg * t);                 // (wvno + xk) |wvno - xk|
-    const double r = sqrt(prod.v);
-    const double ir = r > 0.0 ? 1.0 / r : 0.0;
+    const double r = fast_sqrt(prod.v);
+    const double ir = r > 0.0 ? fast_rcp(r) : 0.0;
     const double h = 0.5 * ir;
     o.r = {r, prod.d0 * h, prod.d1 * h, prod.d2 * h};
     const D3 p = o.r * d;
@@ -83,6 +85,7 @@ __device__ __forceinline__ void wave_d3(const D3& wvno, const D3& xk, double d, 
         sincos(p.v, &sp, &cp);
         o.evan = false;
         o.scale_exp = 0.0;
+        o.escale = 1.0;
         o.cosf = {cp, -sp * p.d0, -sp * p.d1, -sp * p.d2};
         const D3 sn = {sp, cp * p.d0, cp * p.d1, cp * p.d2};
         o.sinr = div_by(sn, o.r, ir);
@@ -90,6 +93,7 @@ __device__ __forceinline__ void wave_d3(const D3& wvno, const D3& xk, double d, 
     } else if (wvno.v == xk.v) {
         o.evan = false;
         o.scale_exp = 0.0;
+        o.escale = 1.0;
         o.cosf = mk(1.0);
         o.sinr = mk(d);
         o.rsin = mk(0.0);
@@ -99,6 +103,7 @@ __device__ __forceinline__ void wave_d3(const D3& wvno, const D3& xk, double d, 
         const double cs = (1.0 + fac) * 0.5, ss = (1.0 - fac) * 0.5;
         o.evan = true;
         o.scale_exp = p.v;
+        o.escale = ep;
         // d(cosh) = sinh dp, d(sinh) = cosh dp, with the scale e^-p held
         o.cosf = {cs, ss * p.d0, ss * p.d1, ss * p.d2};
         const D3 sn = {ss, cs * p.d0, cs * p.d1, cs * p.d2};
@@ -157,8 +162,8 @@ __device__ __forceinline__ void halfspace_d3(const D3& wvno, const D3& xka, cons
     const D3 pa = sa * ((ta.v < 0.0 ? -1.0 : 1.0) * ta);
     const D3 sb = wvno + xkb, tb = wvno - xkb;
     const D3 pb = sb * ((tb.v < 0.0 ? -1.0 : 1.0) * tb);
-    const double ra = sqrt(pa.v), rb = sqrt(pb.v);
-    const double ha = ra > 0 ? 0.5 / ra : 0.0, hb = rb > 0 ? 0.5 / rb : 0.0;
+    const double ra = fast_sqrt(pa.v), rb = fast_sqrt(pb.v);
+    const double ha = ra > 0 ? 0.5 * fast_rcp(ra) : 0.0, hb = rb > 0 ? 0.5 * fast_rcp(rb) : 0.0;
     const D3 Ra = {ra, pa.d0 * ha, pa.d1 * ha, pa.d2 * ha};
     const D3 Rb = {rb, pb.d0 * hb, pb.d1 * hb, pb.d2 * hb};
     const D3 gam = gammk * wvno2;
@@ -228,12 +233,12 @@ __device__ __forceinline__ void layer_ca_d3(const float4& L, double wvno_v, doub
                                             CAset<D3>& C)
 {
     const double a = (double)L.y, b = (double)L.z, rho = (double)L.w, d = (double)L.x;
-    const double ia = 1.0 / a, ib = 1.0 / b;
+    const double ia = fast_rcp(a), ib = fast_rcp(b), iom = fast_rcp(omega);
     const D3 wvno = {wvno_v, 0.0, 0.0, 1.0};
     const double xka_v = omega * ia, xkb_v = omega * ib;
     const D3 xka = {xka_v, -xka_v * ia, 0.0, 0.0};     // d(omega/a)/da
     const D3 xkb = {xkb_v, 0.0, -xkb_v * ib, 0.0};
-    const double gk = 2.0 * b * b / (omega * omega);
+    const double gk = 2.0 * b * b * (iom * iom);
     const D3 gammk = {gk, 0.0, 2.0 * gk * ib, 0.0};
     const D3 wvno2 = wvno * wvno;
     const D3 gam = gammk * wvno2;
@@ -241,37 +246,33 @@ __device__ __forceinline__ void layer_ca_d3(const float4& L, double wvno_v, doub
     wave_d3(wvno, xka, d, P);
     wave_d3(wvno, xkb, d, S);
     const double exa = (P.evan ? P.scale_exp : 0.0) + (S.evan ? S.scale_exp : 0.0);
-    double a0v = 0.0;
-    if (exa < 60.0) {
-        const double ep = P.evan ? exp(-P.scale_exp) : 1.0;
-        const double eq = S.evan ? exp(-S.scale_exp) : 1.0;
-        a0v = ep * eq;
-    }
-    const D3 a0 = mk(a0v);   // the "1" of cosh^2 - sinh^2 under the held scale
-    dnka_t(C, wvno2, gam, gammk, rho, 1.0 / rho, a0, P.cosf, P.sinr, P.rsin, S.cosf, S.sinr, S.rsin);
+    // exp(-exa) from the waves' own exponentials
+    const D3 a0 = mk(exa < 60.0 ? P.escale * S.escale : 0.0);   // the "1" of cosh^2 - sinh^2
+    dnka_t(C, wvno2, gam, gammk, rho, fast_rcp(rho), a0, P.cosf, P.sinr, P.rsin, S.cosf, S.sinr, S.rsin);
 }
 
 // Value-only layer functions (same expressions as wave_d3 without tangents).
 __device__ __forceinline__ void wave_val(double wvno, double xk, double d, double& cosf,
-                                         double& sinr, double& rsin, bool& evan, double& sexp)
+                                         double& sinr, double& rsin, bool& evan, double& sexp,
+                                         double& escale)
 {
-    const double r = sqrt((wvno + xk) * fabs(wvno - xk));
+    const double r = fast_sqrt((wvno + xk) * fabs(wvno - xk));
     const double p = r * d;
     if (wvno < xk) {
         double sp, cp;
         sincos(p, &sp, &cp);
-        evan = false; sexp = 0.0;
-        cosf = cp; sinr = sp / r; rsin = -r * sp;
+        evan = false; sexp = 0.0; escale = 1.0;
+        cosf = cp; sinr = sp * fast_rcp(r); rsin = -r * sp;
     } else if (wvno == xk) {
-        evan = false; sexp = 0.0;
+        evan = false; sexp = 0.0; escale = 1.0;
         cosf = 1.0; sinr = d; rsin = 0.0;
     } else {
         const double ep = exp(-p);
         const double fac = (p < 16.0) ? ep * ep : 0.0;
-        evan = true; sexp = p;
+        evan = true; sexp = p; escale = ep;
         cosf = (1.0 + fac) * 0.5;
         const double ss = (1.0 - fac) * 0.5;
-        sinr = ss / r; rsin = r * ss;
+        sinr = ss * fast_rcp(r); rsin = r * ss;
     }
 }
 
@@ -281,16 +282,17 @@ __device__ __forceinline__ double layer_step_val(const float4& L, double wvno, d
 {
     const double a = (double)L.y, b = (double)L.z, rho = (double)L.w, d = (double)L.x;
     const double wvno2 = wvno * wvno;
-    const double gammk = 2.0 * b * b / (omega * omega);
+    const double iom = fast_rcp(omega);
+    const double gammk = 2.0 * b * b * (iom * iom);
     const double gam = gammk * wvno2;
-    double cp, wp, xp, cq, yq, zq, ep_, eq_;
+    double cp, wp, xp, cq, yq, zq, ep_, eq_, sp_, sq_;
     bool evp, evq;
-    wave_val(wvno, omega / a, d, cp, wp, xp, evp, ep_);
-    wave_val(wvno, omega / b, d, cq, yq, zq, evq, eq_);
+    wave_val(wvno, omega * fast_rcp(a), d, cp, wp, xp, evp, ep_, sp_);
+    wave_val(wvno, omega * fast_rcp(b), d, cq, yq, zq, evq, eq_, sq_);
     const double exa = (evp ? ep_ : 0.0) + (evq ? eq_ : 0.0);
-    const double a0 = (exa < 60.0) ? exp(-exa) : 0.0;
+    const double a0 = (exa < 60.0) ? sp_ * sq_ : 0.0;   // exp(-exa)
     CAset<double> C;
-    dnka_t(C, wvno2, gam, gammk, rho, 1.0 / rho, a0, cp, wp, xp, cq, yq, zq);
+    dnka_t(C, wvno2, gam, gammk, rho, fast_rcp(rho), a0, cp, wp, xp, cq, yq, zq);
     f[0] = e[0] * C.c11 + e[1] * C.c21 + e[2] * C.c31 + e[3] * C.c41 + e[4] * C.c51;
     f[1] = e[0] * C.c12 + e[1] * C.c22 + e[2] * C.c32 + e[3] * C.c42 + e[4] * C.c41;
     f[2] = e[0] * C.c13 + e[1] * C.c23 + e[2] * C.c33 + e[3] * C.c43 + e[4] * C.c53;
@@ -365,7 +367,7 @@ adjoint_kernel(AdjArgs a)
             const double nrm = layer_step_val(L, wvno, omega, e, f);
             double* sp = scr + (long long)m * 6 * nslots;
             for (int q = 0; q < 5; ++q) sp[q * nslots] = e[q];
-            const double inv = 1.0 / nrm;
+            const double inv = fast_rcp(nrm);
             sp[5 * nslots] = inv;
             for (int q = 0; q < 5; ++q) e[q] = f[q] * inv;
         }
@@ -398,10 +400,10 @@ adjoint_kernel(AdjArgs a)
             const Contract sc5 = contract(C, u, gv);
             const double sc = ldexp(inv, gexp);
             dFdw = fma(sc5.d2, sc, dFdw);
-            const double dFda = sc5.d0 * sc, dFdb = sc5.d1 * sc, dFdr = sc5.drho * sc / (double)L.w;
+            const double dFda = sc5.d0 * sc, dFdb = sc5.d1 * sc, dFdr = sc5.drho * sc * fast_rcp((double)L.w);
             // chain to nodes: a_flat = tmp * ((1-f) vp_i + f vp_i+1), etc.
             const double tmpm = ch.tmp, rf = (double)ch.rhofac;
-            const double fw = (double)ch.sub / (double)ch.den;
+            const double fw = (double)ch.sub * fast_rcp((double)ch.den);
             acc_vp = fma(dFda * tmpm, 1.0 - fw, acc_vp); nxt_vp = fma(dFda * tmpm, fw, nxt_vp);
             acc_vs = fma(dFdb * tmpm, 1.0 - fw, acc_vs); nxt_vs = fma(dFdb * tmpm, fw, nxt_vs);
             acc_rh = fma(dFdr * rf, 1.0 - fw, acc_rh);   nxt_rh = fma(dFdr * rf, fw, nxt_rh);

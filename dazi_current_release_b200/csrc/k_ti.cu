@@ -24,48 +24,13 @@
 #include <utility>
 
 #include "dk_secular.cuh"
+#include "dk_fastmath.cuh"
 #include "dk_kernels.cuh"
 
 namespace dk {
 
-// ------------------------------------------------ reciprocal, square root
-// The sweep's results are held to 1e-5 of the oracle, not to bit parity, so
-// its divisions and square roots use the hardware approximations
-// (rcp.approx / rsqrt.approx, about 22 correct bits) refined by two
-// Newton-Raphson steps, each of which squares the relative error (below
-// 2^-52 after two): a few fused multiply-adds with no branch and no slow
-// path, where an IEEE division or sqrt inlines both.  Arguments are finite
-// and normal where these are used; a zero divisor gives inf/NaN as a
-// division would.
-__device__ __forceinline__ double ti_rcp(double x)
-{
-#ifdef __CUDA_ARCH__
-    double r;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(r) : "d"(x));
-    double e = fma(-x, r, 1.0);
-    r = fma(r, e, r);
-    e = fma(-x, r, 1.0);
-    return fma(r, e, r);
-#else
-    return 1.0 / x;
-#endif
-}
-
-// sqrt(x), x >= 0: x / sqrt(x) by the refined reciprocal square root
-// (y <- y (3 - x y^2) / 2, twice).
-__device__ __forceinline__ double ti_sqrt(double x)
-{
-#ifdef __CUDA_ARCH__
-    double y;
-    asm("rsqrt.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    const double h = 0.5 * x;
-    y = y * fma(-h * y, y, 1.5);
-    y = y * fma(-h * y, y, 1.5);
-    return x > 0.0 ? x * y : 0.0;
-#else
-    return sqrt(x);
-#endif
-}
+// Divisions and square roots use dk_fastmath.cuh (the sweep is held to 1e-5
+// of the oracle, not to bit parity).
 
 // ------------------------------------------------------------ complex
 struct zc { double re, im; };
@@ -81,16 +46,16 @@ __device__ __forceinline__ zc operator*(double s, zc a) { return {s * a.re, s * 
 __device__ __forceinline__ double znorm2(zc a) { return a.re * a.re + a.im * a.im; }
 __device__ __forceinline__ zc zdiv(zc a, zc b)
 {
-    const double in = ti_rcp(znorm2(b));
+    const double in = fast_rcp(znorm2(b));
     return {(a.re * b.re + a.im * b.im) * in, (a.im * b.re - a.re * b.im) * in};
 }
 __device__ __forceinline__ zc zsqrt(zc a)
 {
     // principal square root (branch cut on the negative real axis)
-    const double m = ti_sqrt(znorm2(a));
-    double re = ti_sqrt(0.5 * (m + fabs(a.re)));
+    const double m = fast_sqrt(znorm2(a));
+    double re = fast_sqrt(0.5 * (m + fabs(a.re)));
     if (re == 0.0) return Z(0.0, 0.0);
-    double im = a.im * ti_rcp(2.0 * re);
+    double im = a.im * fast_rcp(2.0 * re);
     if (a.re < 0.0) { const double t = fabs(im); im = copysign(re, a.im); re = t; }
     return {re, im};
 }
@@ -140,14 +105,14 @@ __device__ __forceinline__ void ti_eigen(const TiLayer& L, double omg, double wv
     const double cc = ddef * aabc;
     const double disc = bb * bb - 4.0 * cc;
     o.ok = disc >= 0.0;
-    const double srt = ti_sqrt(fmax(disc, 0.0));
+    const double srt = fast_sqrt(fmax(disc, 0.0));
     double L1 = 0.5 * (bb + srt);
-    double L2 = fabs(L1) > 0.0 ? cc * ti_rcp(L1) : 0.5 * (bb - srt);
+    double L2 = fabs(L1) > 0.0 ? cc * fast_rcp(L1) : 0.5 * (bb - srt);
     if (fabs(wvno2 - L2) < fabs(wvno2 - L1)) { const double t = L1; L1 = L2; L2 = t; }
     o.oscp = L1 < 0.0;
     o.oscs = L2 < 0.0;
-    o.rp = ti_sqrt(fabs(L1));
-    o.rsv = ti_sqrt(fabs(L2));
+    o.rp = fast_sqrt(fabs(L1));
+    o.rsv = fast_sqrt(fabs(L2));
     const double bcaa = b * c + a * a, ddef2 = d * d + e * f;
     double x12 = b * d - a * e;
     double x22 = b * L2 - e * bcaa;
@@ -158,9 +123,9 @@ __device__ __forceinline__ void ti_eigen(const TiLayer& L, double omg, double wv
     double x31 = d * L1 - a * ddef2;
     double x41 = -(L1 - a * d - b * f);
     if (wvn != 0.0) {
-        const double z1 = wvn * ti_rcp(x11);
+        const double z1 = wvn * fast_rcp(x11);
         x11 *= z1; x21 *= z1; x31 *= z1; x41 *= z1;
-        const double z2 = wvn * ti_rcp(x22);
+        const double z2 = wvn * fast_rcp(x22);
         x12 *= z2; x22 *= z2; x32 *= z2; x42 *= z2;
     }
     o.x11 = x11; o.x21 = x21; o.x31 = x31; o.x41 = x41;
@@ -184,7 +149,7 @@ __device__ __forceinline__ void ti_var_one(double r, bool osc, double dm, double
         cosf = 0.5 * (1.0 + fac);
         const double sn = 0.5 * (1.0 - fac);
         rsin = r * sn;
-        sinr = (fabs(pr) < 1.0e-5 && r < 1.0e-5) ? dm : sn * ti_rcp(r);
+        sinr = (fabs(pr) < 1.0e-5 && r < 1.0e-5) ? dm : sn * fast_rcp(r);
     } else {
         const double pi = r * dm;
         ex = 0.0;
@@ -192,7 +157,7 @@ __device__ __forceinline__ void ti_var_one(double r, bool osc, double dm, double
         sincos(pi, &sn, &cs);
         cosf = cs;
         rsin = -r * sn;                               // (i r)(i sin)
-        sinr = (r < 1.0e-5) ? dm : sn * ti_rcp(r);    // (i sin)/(i r)
+        sinr = (r < 1.0e-5) ? dm : sn * fast_rcp(r);    // (i sin)/(i r)
     }
 }
 
@@ -299,7 +264,7 @@ __device__ __forceinline__ void ti_compound_apply(const TiEig& E, const TiVar& v
 {
     const double ex = v.pex + v.svex;
     const double dfac = ex > 35.0 ? 0.0 : exp(-ex);
-    const double a1 = 0.5 * ti_rcp(E.np), a2 = 0.5 * ti_rcp(E.nsv);
+    const double a1 = 0.5 * fast_rcp(E.np), a2 = 0.5 * fast_rcp(E.nsv);
     double fac[3][4];
     fac[1][0] = 2.0 * a1 * v.cosp; fac[1][1] = 2.0 * a1 * v.sinpr; fac[1][2] = 2.0 * a1 * v.rsinp;
     fac[1][3] = 4.0 * a1 * a1 * dfac;
@@ -432,7 +397,7 @@ __device__ __forceinline__ TiWave ti_wave(double r, bool osc, double dm)
         w.cosf = 0.5 * (1.0 + fac);
         const double sn = 0.5 * (1.0 - fac);
         w.rsin = r * sn;
-        w.sinr = (fabs(pr) < 1.0e-5 && r < 1.0e-5) ? dm : sn * ti_rcp(r);
+        w.sinr = (fabs(pr) < 1.0e-5 && r < 1.0e-5) ? dm : sn * fast_rcp(r);
         w.er = e1;
         w.ei = 0.0;
     } else {
@@ -442,7 +407,7 @@ __device__ __forceinline__ TiWave ti_wave(double r, bool osc, double dm)
         sincos(pi, &sn, &cs);
         w.cosf = cs;
         w.rsin = -r * sn;                             // (i r)(i sin)
-        w.sinr = (r < 1.0e-5) ? dm : sn * ti_rcp(r);  // (i sin)/(i r)
+        w.sinr = (r < 1.0e-5) ? dm : sn * fast_rcp(r);  // (i sin)/(i r)
         w.er = cs;
         w.ei = -sn;
     }
@@ -600,7 +565,7 @@ __device__ __forceinline__ void ti_haskell(const TiEig& E, const TiVar& V, doubl
     const double f = dd > 40.0 ? 0.0 : exp(-dd);
     const double fp = pbig ? 1.0 : f, fs = pbig ? f : 1.0;
     cpex = pbig ? V.pex : V.svex;
-    const double inp = ti_rcp(E.np), ins = ti_rcp(E.nsv);
+    const double inp = fast_rcp(E.np), ins = fast_rcp(E.nsv);
     const double cosp = fp * V.cosp * inp, sinpr = fp * V.sinpr * inp, rsinp = fp * V.rsinp * inp;
     const double cossv = fs * V.cosq * ins, sinsvr = fs * V.sinqr * ins, rsinsv = fs * V.rsinq * ins;
     const double x11 = E.x11, x21 = E.x21, x31 = E.x31, x41 = E.x41;
@@ -675,11 +640,11 @@ __device__ __forceinline__ void ti_integrals_wave(const TiEig& E, const TiWave& 
 {
     const double ra = E.rp, rb = E.rsv;
     const bool oa = E.oscp, ob = E.oscs;
-    const double ira = ti_rcp(ra), irb = ti_rcp(rb);
+    const double ira = fast_rcp(ra), irb = fast_rcp(rb);
     const double x11 = E.x11, x21 = E.x21, x31 = E.x31, x41 = E.x41;
     const double x12 = E.x12, x22 = E.x22, x32 = E.x32, x42 = E.x42;
     // potentials: rows 0 / 2 of E^-1 (P up / down) and 1 / 3 (S up / down)
-    const double hp = 0.5 * ti_rcp(E.np), hs = 0.5 * ti_rcp(E.nsv);
+    const double hp = 0.5 * fast_rcp(E.np), hs = 0.5 * fast_rcp(E.nsv);
     const zc kmpu = ti_over_nu((bot[0] * x41 - bot[2] * x21) * hp, (bot[3] * x11 - bot[1] * x31) * hp, ira, oa);
     const zc km1pd = ti_over_nu((top[0] * x41 - top[2] * x21) * hp, (top[1] * x31 - top[3] * x11) * hp, ira, oa);
     const zc kmsu = ti_over_nu((bot[3] * x12 - bot[1] * x32) * hs, (bot[0] * x42 - bot[2] * x22) * hs, irb, ob);
@@ -691,7 +656,7 @@ __device__ __forceinline__ void ti_integrals_wave(const TiEig& E, const TiWave& 
     auto ffun = [&](double r, bool osc, double x, zc e) {
         if (r < 1.0e-08) return Z(dm);
         const zc n = Z(1.0) - (x < 40.0 ? e * e : Z(0.0));
-        const double h = 0.5 * ti_rcp(r);           // n / (2 nu)
+        const double h = 0.5 * fast_rcp(r);           // n / (2 nu)
         return osc ? Z(n.im * h, -n.re * h) : Z(n.re * h, n.im * h);
     };
     const zc FA = ffun(ra, oa, xa, ea), FB = ffun(rb, ob, xb, eb);
