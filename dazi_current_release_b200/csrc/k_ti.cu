@@ -202,24 +202,6 @@ constexpr TT kTT[72] = {
     {-1,3,4,1,4,3,2,0,0,0}, {-1,3,4,2,4,3,1,0,0,0}, {+1,3,3,1,4,4,2,1,1,0}, {+1,3,3,2,4,4,1,2,2,0}, {-1,3,4,1,4,3,1,3,3,0}, {-1,3,4,2,4,3,2,3,3,0},
 };
 constexpr int kTTo[16] = {0, 6, 10, 16, 20, 26, 30, 34, 38, 42, 48, 52, 58, 62, 66, 72};
-__constant__ int c_tto[16] = {0, 6, 10, 16, 20, 26, 30, 34, 38, 42, 48, 52, 58, 62, 66, 72};
-__constant__ TT c_tt[72] = {
-    {-1,1,3,1,2,4,1,3,3,0}, {-1,1,4,1,2,3,2,0,0,0}, {-1,1,4,2,2,3,1,0,0,0}, {+1,1,3,1,2,4,2,1,1,0}, {+1,1,3,2,2,4,1,2,2,0}, {-1,1,3,2,2,4,2,3,3,0},
-    {-1,1,4,1,2,2,2,0,1,0}, {-1,1,4,2,2,2,1,0,2,0}, {-1,1,2,1,2,4,2,0,1,1}, {-1,1,2,2,2,4,1,0,2,1},
-    {+1,1,4,1,2,1,1,3,3,0}, {+1,1,4,1,1,2,2,0,0,0}, {+1,1,4,2,2,1,1,0,0,0}, {-1,1,1,1,2,4,2,1,1,0}, {-1,1,1,2,2,4,1,2,2,0}, {+1,1,4,2,1,2,2,3,3,0},
-    {-1,1,3,1,1,2,2,1,0,0}, {-1,1,3,2,2,1,1,2,0,0}, {-1,1,1,1,2,3,2,1,0,1}, {-1,1,1,2,2,3,1,2,0,1},
-    {-1,1,2,1,1,2,2,0,0,0}, {-1,1,2,2,2,1,1,0,0,0}, {+1,1,1,1,2,2,2,1,1,0}, {+1,1,1,2,2,2,1,2,2,0}, {-1,1,2,1,2,1,1,3,3,0}, {-1,1,2,2,1,2,2,3,3,0},
-    {-1,1,4,1,3,3,2,0,2,0}, {-1,1,4,2,3,3,1,0,1,0}, {-1,1,3,1,3,4,2,1,0,1}, {-1,1,3,2,3,4,1,2,0,1},
-    {-1,1,4,1,3,2,2,0,0,0}, {+1,1,2,1,3,4,2,0,0,0}, {-1,1,4,2,3,2,1,0,0,0}, {+1,1,2,2,3,4,1,0,0,0},
-    {+1,1,4,1,3,1,2,0,2,0}, {+1,1,4,2,3,1,1,0,1,0}, {+1,1,1,1,3,4,2,1,0,1}, {+1,1,1,2,3,4,1,2,0,1},
-    {-1,1,3,1,3,1,2,1,2,0}, {-1,1,3,2,3,1,1,2,1,0}, {-1,1,1,1,3,3,2,1,2,1}, {-1,1,1,2,3,3,1,2,1,1},
-    {-1,1,4,1,4,3,2,0,0,0}, {-1,1,4,2,4,3,1,0,0,0}, {+1,1,3,2,4,4,1,2,2,0}, {+1,1,3,1,4,4,2,1,1,0}, {-1,1,4,1,4,3,1,3,3,0}, {-1,1,4,2,4,3,2,3,3,0},
-    {-1,1,4,1,4,2,2,0,1,0}, {-1,1,4,2,4,2,1,0,2,0}, {-1,1,2,1,4,4,2,0,1,1}, {-1,1,2,2,4,4,1,0,2,1},
-    {+1,1,4,1,4,1,2,0,0,0}, {+1,1,4,2,4,1,1,0,0,0}, {-1,1,1,1,4,4,2,1,1,0}, {-1,1,1,2,4,4,1,2,2,0}, {+1,1,4,1,4,1,1,3,3,0}, {+1,1,4,2,4,1,2,3,3,0},
-    {-1,2,4,1,4,3,2,2,0,0}, {-1,2,4,2,4,3,1,1,0,0}, {-1,2,3,1,4,4,2,0,1,1}, {-1,2,3,2,4,4,1,0,2,1},
-    {-1,2,4,1,4,2,2,2,1,0}, {-1,2,4,2,4,2,1,1,2,0}, {+1,2,2,1,4,4,2,2,1,0}, {+1,2,2,2,4,4,1,1,2,0},
-    {-1,3,4,1,4,3,2,0,0,0}, {-1,3,4,2,4,3,1,0,0,0}, {+1,3,3,1,4,4,2,1,1,0}, {+1,3,3,2,4,4,1,2,2,0}, {-1,3,4,1,4,3,1,3,3,0}, {-1,3,4,2,4,3,2,3,3,0},
-};
 
 // One term with compile-time indices (registers only).
 template <int I, class T, class F>
@@ -236,7 +218,7 @@ template <class T, class F, int... Is>
 __device__ __forceinline__ T tca_expand(const T (&xs)[5][3], const F (&fac)[3][4],
                                         std::integer_sequence<int, Is...>)
 {
-    T g0 = T(0.0), g1 = T(0.0);
+    T g0{}, g1{};
     ((kTT[Is].grp ? (g1 = g1 + tca_term<Is>(xs, fac)) : (g0 = g0 + tca_term<Is>(xs, fac))), ...);
     return g0 - g1;
 }
@@ -316,15 +298,6 @@ __device__ __forceinline__ void ti_emat(const TiEigZ& E, zc e[4][4], zc ei[4][4]
     e[0][3] = -(x12 * rsv); e[1][3] = x22; e[2][3] = -(x32 * rsv); e[3][3] = x42;
 }
 
-__device__ __forceinline__ void eig_to_z(const TiEig& E, TiEigZ& o)
-{
-    o.x11 = Z(E.x11); o.x21 = Z(E.x21); o.x31 = Z(E.x31); o.x41 = Z(E.x41);
-    o.x12 = Z(E.x12); o.x22 = Z(E.x22); o.x32 = Z(E.x32); o.x42 = Z(E.x42);
-    o.np = Z(E.np); o.nsv = Z(E.nsv);
-    o.rp = E.oscp ? Z(0.0, E.rp) : Z(E.rp);
-    o.rsv = E.oscs ? Z(0.0, E.rsv) : Z(E.rsv);
-}
-
 // The six energy integrals of a layer (intijr, tregn96.f:4073-4245):
 // (1,1) (1,3) (2,2) (2,4) (3,3) (4,4).  top/bot = (ur, uz, tz, tr) at the
 // layer's top and bottom interface; half = the lower half-space.  fg holds
@@ -346,20 +319,23 @@ __device__ __forceinline__ void ti_integrals_z(const TiEigZ& E, const zc fg[6], 
         const zc pu2 = kmpu * kmpu, pd2 = km1pd * km1pd, su2 = kmsu * kmsu, sd2 = km1sd * km1sd;
         const zc pusu = kmpu * kmsu, pdsd = km1pd * km1sd, pusd = kmpu * km1sd, pdsu = km1pd * kmsu;
         const zc pupd = kmpu * km1pd, susd = kmsu * km1sd;
+        // (potential product) x (ffunc/gfunc/h1func/h2func) once per layer;
+        // each integral then needs only the real part of EE x W
+        const zc W1 = pu2 * FA, W2 = pd2 * FA, W3 = su2 * FB, W4 = sd2 * FB;
+        const zc W5 = pusu * H1, W6 = pdsd * H1, W7 = pusd * H2, W8 = pdsu * H2;
+        const zc W9 = pupd * GA, W10 = susd * GB;
+        auto re_mul = [](zc a, zc b) { return a.re * b.re - a.im * b.im; };
 #pragma unroll
         for (int q = 0; q < 6; ++q) {
             const int i = IJ[q][0], j = IJ[q][1];
             auto EE = [&](int a, int b) { return e[i][a] * e[j][b]; };
             auto SY = [&](int a, int b) { return EE(a, b) + EE(b, a); };
-            zc r = (EE(0, 0) * pu2) * FA;
-            r = r + (EE(2, 2) * pd2) * FA;
-            r = r + (EE(1, 1) * su2) * FB;
-            r = r + (EE(3, 3) * sd2) * FB;
-            r = r + H1 * (SY(0, 1) * pusu + SY(2, 3) * pdsd);
-            r = r + H2 * (SY(0, 3) * pusd + SY(1, 2) * pdsu);
-            r = r + GA * (SY(0, 2) * pupd);
-            r = r + GB * (SY(1, 3) * susd);
-            out[q] = r.re;
+            double r = re_mul(EE(0, 0), W1) + re_mul(EE(2, 2), W2);
+            r += re_mul(EE(1, 1), W3) + re_mul(EE(3, 3), W4);
+            r += re_mul(SY(0, 1), W5) + re_mul(SY(2, 3), W6);
+            r += re_mul(SY(0, 3), W7) + re_mul(SY(1, 2), W8);
+            r += re_mul(SY(0, 2), W9) + re_mul(SY(1, 3), W10);
+            out[q] = r;
         }
     } else {
         const zc pd2 = km1pd * km1pd, sd2 = km1sd * km1sd, pdsd = km1pd * km1sd;
@@ -500,24 +476,16 @@ __device__ void ti_compound_z(const TiEigZ& E, const TiVarZ& v, double ca[5][5])
     zc xs[5][3];
     xs[1][1] = E.x11; xs[2][1] = E.x21; xs[3][1] = E.x31; xs[4][1] = E.x41;
     xs[1][2] = E.x12; xs[2][2] = E.x22; xs[3][2] = E.x32; xs[4][2] = E.x42;
-    double t[15];
-    for (int q = 0; q < 15; ++q) {
-        const TT* tab = c_tt;
-        const int lo = c_tto[q];
-        const int hi = c_tto[q + 1];
-        zc g0 = Z(0.0), g1 = Z(0.0);
-        for (int i = lo; i < hi; ++i) {
-            const TT tt = tab[i];
-            zc w = (xs[tt.a][tt.k] * xs[tt.b][tt.k]) * (xs[tt.c][tt.l] * xs[tt.d][tt.l]);
-            if (tt.sg < 0) w = -w;
-            w = (tt.fk == 3) ? w * fac[tt.k][3] : (w * fac[tt.k][tt.fk]) * fac[tt.l][tt.fl];
-            if (tt.grp) g1 = g1 + w; else g0 = g0 + w;
-        }
-        t[q] = (g0 - g1).re;
-    }
-    const double t11 = t[0], t12 = t[1], t13 = t[2], t15 = t[3], t16 = t[4], t21 = t[5];
-    const double t22 = t[6], t23 = t[7], t25 = t[8], t31 = t[9], t32 = t[10], t33 = t[11];
-    const double t51 = t[12], t52 = t[13], t61 = t[14];
+    // the term table expanded at compile time (as the real path does): the
+    // factors stay in registers
+    const double t11 = tca_elem<0>(xs, fac).re, t12 = tca_elem<1>(xs, fac).re;
+    const double t13 = tca_elem<2>(xs, fac).re, t15 = tca_elem<3>(xs, fac).re;
+    const double t16 = tca_elem<4>(xs, fac).re, t21 = tca_elem<5>(xs, fac).re;
+    const double t22 = tca_elem<6>(xs, fac).re, t23 = tca_elem<7>(xs, fac).re;
+    const double t25 = tca_elem<8>(xs, fac).re, t31 = tca_elem<9>(xs, fac).re;
+    const double t32 = tca_elem<10>(xs, fac).re, t33 = tca_elem<11>(xs, fac).re;
+    const double t51 = tca_elem<12>(xs, fac).re, t52 = tca_elem<13>(xs, fac).re;
+    const double t61 = tca_elem<14>(xs, fac).re;
     ca[0][0] = t11; ca[0][1] = t12; ca[0][2] = t13; ca[0][3] = t15; ca[0][4] = t16;
     ca[1][0] = t21; ca[1][1] = t22; ca[1][2] = t23; ca[1][3] = t25; ca[1][4] = t15;
     ca[2][0] = 2.0 * t31; ca[2][1] = 2.0 * t32; ca[2][2] = 2.0 * t33 - dfac;
@@ -742,15 +710,63 @@ __device__ __noinline__ DownOut ti_down_general(TiLayer L, double omega, double 
 __device__ __noinline__ D6 ti_integrals_general(TiLayer L, double omega, double wvno, double wvno2,
                                                 D4 top, D4 bot, bool half)
 {
-    TiEig E;
-    ti_eigen(L, omega, wvno, wvno2, E);
+    // only layers whose eigenvalues are complex come here (the real ones
+    // take ti_integrals_wave / ti_integrals_halfspace)
     TiEigZ EZ;
-    if (E.ok) eig_to_z(E, EZ);
-    else ti_eigen_z(L, omega, wvno, wvno2, EZ);
+    ti_eigen_z(L, omega, wvno, wvno2, EZ);
     zc fg[6];
     if (!half) ti_fgh_z(EZ.rp, EZ.rsv, L.td, fg);
     D6 o;
     ti_integrals_z(EZ, fg, top.v, bot.v, half, o.v);
+    return o;
+}
+
+// Energy integrals of the half-space (half = 1 in intijr): only its upper
+// interface's potentials (km1pd, km1sd) contribute, and for exp(-nu z) on
+// z > 0 ffunc -> 1/(2 nu), h1func -> 1/(nu_a + nu_b), gfunc = h2func = 0.
+// With real eigenvalues this is ti_integrals_wave's real form (same E
+// factors, same potentials); complex eigenvalues go through the general
+// path.  Called once per (column, period), out of line, so the warps do not
+// fetch the general path's code at the end of every task.
+__device__ __noinline__ D6 ti_integrals_halfspace(TiLayer L, double omega, double wvno, double wvno2,
+                                                  D4 top)
+{
+    TiEig E;
+    ti_eigen(L, omega, wvno, wvno2, E);
+    if (!E.ok) {
+        const D4 zero = {{0.0, 0.0, 0.0, 0.0}};
+        return ti_integrals_general(L, omega, wvno, wvno2, top, zero, true);
+    }
+    const double ra = E.rp, rb = E.rsv;
+    const bool oa = E.oscp, ob = E.oscs;
+    const double ira = fast_rcp(ra), irb = fast_rcp(rb);
+    const double x11 = E.x11, x21 = E.x21, x31 = E.x31, x41 = E.x41;
+    const double x12 = E.x12, x22 = E.x22, x32 = E.x32, x42 = E.x42;
+    const double hp = 0.5 * fast_rcp(E.np), hs = 0.5 * fast_rcp(E.nsv);
+    const double* t = top.v;
+    const zc km1pd = ti_over_nu((t[0] * x41 - t[2] * x21) * hp, (t[1] * x31 - t[3] * x11) * hp, ira, oa);
+    const zc km1sd = ti_over_nu((t[3] * x12 - t[1] * x32) * hs, (t[2] * x22 - t[0] * x42) * hs, irb, ob);
+    // 1 / (2 nu): 1/(2r) or -i/(2r)
+    const zc FA = oa ? Z(0.0, -0.5 * ira) : Z(0.5 * ira);
+    const zc FB = ob ? Z(0.0, -0.5 * irb) : Z(0.5 * irb);
+    const zc nua = oa ? Z(0.0, ra) : Z(ra), nub = ob ? Z(0.0, rb) : Z(rb);
+    const zc H1 = zdiv(Z(1.0), nua + nub);
+    const zc W2 = (km1pd * km1pd) * FA, W4 = (km1sd * km1sd) * FB, W6 = (km1pd * km1sd) * H1;
+    const double U6a = ti_re_nu(ra, oa, W6), U6b = ti_re_nu(rb, ob, W6);
+    const double kaa = oa ? -(ra * ra) : ra * ra, kbb = ob ? -(rb * rb) : rb * rb;
+    const double ep[4][4] = {{x11, x12, x11, -x12}, {x21, x22, -x21, x22},
+                             {x31, x32, x31, -x32}, {x41, x42, -x41, x42}};
+    constexpr int IJ[6][2] = {{0, 0}, {0, 2}, {1, 1}, {1, 3}, {2, 2}, {3, 3}};
+    D6 o;
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+        const int i = IJ[q][0], j = IJ[q][1];
+        const bool odd = (i & 1) != 0;
+        const double pp = ep[i][2] * ep[j][2] * W2.re;
+        const double ss = ep[i][3] * ep[j][3] * W4.re;
+        const double mx = (ep[i][2] * ep[j][3] + ep[i][3] * ep[j][2]) * (odd ? U6a : U6b);
+        o.v[q] = (odd ? kaa : 1.0) * pp + (odd ? 1.0 : kbb) * ss + mx;
+    }
     return o;
 }
 
@@ -972,7 +988,8 @@ __device__ __forceinline__ void ti_task(const TiArgs& a, long long task, int lan
                 D4 t4, b4;
 #pragma unroll
                 for (int i = 0; i < 4; ++i) { t4.v[i] = top[i]; b4.v[i] = bot[i]; }
-                const D6 r = ti_integrals_general(L, omega, wvno, wvno2, t4, b4, half);
+                const D6 r = half ? ti_integrals_halfspace(L, omega, wvno, wvno2, t4)
+                                  : ti_integrals_general(L, omega, wvno, wvno2, t4, b4, false);
 #pragma unroll
                 for (int i = 0; i < 6; ++i) I[i] = r.v[i];
             }
