@@ -99,3 +99,43 @@ def test_fp32_scan_gives_identical_roots(small_batch):
                             form=dk.FORM_ADJOINT | dk_lib.FORM_SCAN_FP32)
     for k in ("pv", "status", "sen_vs", "sen_vp", "sen_rho", "lsen"):
         np.testing.assert_array_equal(r32[k], r64[k], err_msg=k)
+
+
+def test_host_entry_equals_device_entry_twice():
+    """dazi_dk_batch (host buffers; pv and the sensitivity kernels copied
+    back on a second stream while the Gc/Gs kernel runs) against
+    dazi_dk_batch_dev on the same 6000 uneven columns, two calls in a row:
+    identical outputs, bit for bit."""
+    import ctypes
+    import torch
+    from dazi_current_release_b200.batch import output_offsets
+    b = S.config3(realisations=1, columns=6000, base_seed=4242)
+    L = dk_lib.load()
+    dev = torch.device("cuda", 0)
+    sen_off, ls_off = output_offsets(b.node_off, b.per_off)
+    T = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)  # noqa: E731
+    d = {"node": T(b.node_off, torch.int64), "dep": T(b.depz, torch.float32),
+         "vs": T(b.vs, torch.float32), "per": T(b.per_off, torch.int64),
+         "periods": T(b.periods, torch.float64), "sen": T(sen_off, torch.int64),
+         "ls": T(ls_off, torch.int64)}
+    ncols = b.node_off.size - 1
+    P = lambda t: None if t is None else ctypes.c_void_p(t.data_ptr())  # noqa: E731
+    for _ in range(2):
+        host = depthkernel_batch(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk,
+                                 form=dk.FORM_ADJOINT, kernels=True, lsen=True)
+        pv = torch.empty(int(b.per_off[-1]), dtype=torch.float64, device=dev)
+        sen = [torch.empty(int(sen_off[-1]), dtype=torch.float64, device=dev) for _ in range(3)]
+        ls = torch.empty(int(ls_off[-1]), dtype=torch.float32, device=dev)
+        st = torch.empty(ncols, dtype=torch.int32, device=dev)
+        stream = torch.cuda.current_stream(dev).cuda_stream
+        rc = L.dazi_dk_batch_dev(ncols, P(d["node"]), P(d["dep"]), P(d["vs"]), None, None,
+                                 P(d["per"]), P(d["periods"]), ctypes.c_float(b.minthk), P(pv),
+                                 P(d["sen"]), P(sen[0]), P(sen[1]), P(sen[2]), P(d["ls"]), P(ls),
+                                 dk.FORM_ADJOINT, P(st), ctypes.c_void_p(stream))
+        dk_lib.check(rc)
+        torch.cuda.synchronize()
+        np.testing.assert_array_equal(host["pv"], pv.cpu().numpy())
+        for name, t in zip(("sen_vs", "sen_vp", "sen_rho"), sen):
+            np.testing.assert_array_equal(host[name], t.cpu().numpy(), err_msg=name)
+        np.testing.assert_array_equal(host["lsen"], ls.cpu().numpy())
+        np.testing.assert_array_equal(host["status"], st.cpu().numpy())
