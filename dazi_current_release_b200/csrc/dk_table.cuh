@@ -17,17 +17,13 @@ namespace dk {
 
 constexpr int TILE = 32;
 
-// TI model of one refined layer as tregn96 holds it (real*4 stores of the
-// flattened A = C, L = N, density and thickness, widened to double) with the
-// period-independent combinations its eigenvector and energy formulas
-// divide by, formed once per layer instead of once per (layer, period).
+// TI model of one refined layer as tregn96 holds it: real*4 stores of the
+// flattened A = C, L = N and density, TF (from the unflattened values) and
+// the flattened thickness, widened to double.  The Gc/Gs kernel forms the
+// combinations its formulas divide by (1/TA, TF/TA, sqrt(TA/rho), eta, ...)
+// from these when it reads a layer: 40 bytes per layer item instead of 120.
 struct TiRec {
     double TA, TL, rho, TF;   // TF = TA - 2 TL of the unflattened values
-    double iTA, iTL;          // 1 / TC, 1 / TL           (TC = TA)
-    double TFoTA, TAF;        // TF / TC, TA - TF^2 / TC
-    double rhoTA, rhoTL;      // rho / TC, rho / TL
-    double ah, bv;            // sqrt(TA / rho) (= av), sqrt(TL / rho) (= bh)
-    double eta, ieta;         // TF / (TA - 2 TL), its reciprocal
     double td;                // flattened thickness (0 for the half-space)
 };
 

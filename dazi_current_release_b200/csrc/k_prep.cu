@@ -184,16 +184,6 @@ __device__ __forceinline__ void prep_build_one(const ColSrc& src, const PrepOut&
             tr.TL = (double)fTL;
             tr.rho = (double)frh;
             tr.TF = (double)__fsub_rn(TAu, __fmul_rn(2.0f, TLu));
-            tr.iTA = 1.0 / tr.TA;
-            tr.iTL = 1.0 / tr.TL;
-            tr.TFoTA = tr.TF / tr.TA;
-            tr.TAF = tr.TA - tr.TF * tr.TF / tr.TA;
-            tr.rhoTA = tr.rho / tr.TA;
-            tr.rhoTL = tr.rho / tr.TL;
-            tr.ah = sqrt(tr.TA / tr.rho);
-            tr.bv = sqrt(tr.TL / tr.rho);
-            tr.eta = tr.TF / (tr.TA - 2.0 * tr.TL);
-            tr.ieta = 1.0 / tr.eta;
             tr.td = half ? 0.0 : (double)td;
             // splice coefficients, real*4 as depthkernelTI.f90:152-162
             SpRec sr;

@@ -69,12 +69,36 @@ __device__ __forceinline__ zc zexp(zc a)
 
 // ------------------------------------------------------- TI layer model
 // A layer as tregn96 holds it: TiRec (dk_table.cuh) with TC = TA, TN = TL
-// (depthkernelTI.f90:124-131) and the period-independent combinations.
-using TiLayer = TiRec;
+// (depthkernelTI.f90:124-131), plus the period-independent combinations,
+// formed from the stored record where the layer is read (the compiler keeps
+// only those a call site uses).
+struct TiLayer {
+    double TA, TL, rho, TF;
+    double iTA, iTL;          // 1 / TC, 1 / TL           (TC = TA)
+    double TFoTA, TAF;        // TF / TC, TA - TF^2 / TC
+    double rhoTA, rhoTL;      // rho / TC, rho / TL
+    double ah, bv;            // sqrt(TA / rho) (= av), sqrt(TL / rho) (= bh)
+    double eta, ieta;         // TF / (TA - 2 TL), its reciprocal
+    double td;                // flattened thickness (0 for the half-space)
+};
 
 __device__ __forceinline__ TiLayer ti_layer(const TiRec* p)
 {
-    return *p;
+    const TiRec r = *p;
+    TiLayer L;
+    L.TA = r.TA; L.TL = r.TL; L.rho = r.rho; L.TF = r.TF; L.td = r.td;
+    L.iTA = fast_rcp(r.TA);
+    L.iTL = fast_rcp(r.TL);
+    const double irho = fast_rcp(r.rho);
+    L.TFoTA = r.TF * L.iTA;
+    L.TAF = r.TA - r.TF * L.TFoTA;
+    L.rhoTA = r.rho * L.iTA;
+    L.rhoTL = r.rho * L.iTL;
+    L.ah = fast_sqrt(r.TA * irho);
+    L.bv = fast_sqrt(r.TL * irho);
+    L.eta = r.TF * fast_rcp(r.TA - 2.0 * r.TL);
+    L.ieta = fast_rcp(L.eta);
+    return L;
 }
 
 // gettiegn() (tregn96.f:3166-3361) for real eigenvalues.  rp/rsv are the
