@@ -340,6 +340,12 @@ def main_ragged(args, ws, rank, local):
     d_node, d_per, d_dep, d_vs = T(b.node_off), T(b.per_off), T(b.depz), T(b.vs)
     d_periods, d_senoff, d_lsoff = T(b.periods), T(sen_off), T(ls_off)
     ncp = int(b.per_off[-1])
+    # whole-job column-periods: every rank has its own realisations
+    job_cp = float(ncp)
+    if ws > 1:
+        tcp = torch.tensor([job_cp], dtype=torch.float64, device=dev)
+        torch.distributed.all_reduce(tcp, op=torch.distributed.ReduceOp.SUM)
+        job_cp = float(tcp.item())
     pv = torch.zeros(ncp, dtype=torch.float64, device=dev)
     sen = [torch.zeros(int(sen_off[-1]), dtype=torch.float64, device=dev) for _ in range(3)]
     lsen = torch.zeros(int(ls_off[-1]), dtype=torch.float32, device=dev)
@@ -402,7 +408,7 @@ def main_ragged(args, ws, rank, local):
             ms_per_step = _events_timed(step_fn(form, ncol), args.steps, args.warmup, dev,
                                         stream, flush, ws)
         launches = L.dazi_dk_last_launches()
-    value = ws * ncp / (ms_per_step * 1e-3)
+    value = job_cp / (ms_per_step * 1e-3)
 
     # per-phase device times of one more step (events inside the library),
     # and of one step with every root-search evaluation in FP64
@@ -512,12 +518,12 @@ def main_ragged(args, ws, rank, local):
         "config": dict(ragged_config(args, b),
                        l2="inputs and outputs far larger than L2; 256 MiB flush write between "
                           "steps outside the timed events"),
-        "e2e": {"value": ws * ncp / e2e_s, "unit": "column-periods/s",
+        "e2e": {"value": job_cp / e2e_s, "unit": "column-periods/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
         "roofline": roof,
         "gpu_launches": args.steps * launches,
         "graph": graph_info,
-        "per_call": {"value": ws * ncp / (call_ms * 1e-3), "ms_per_step": call_ms,
+        "per_call": {"value": job_cp / (call_ms * 1e-3), "ms_per_step": call_ms,
                      "launches_per_call": launches_call},
     }
     if scan32:
