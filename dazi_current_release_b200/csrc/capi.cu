@@ -160,9 +160,10 @@ struct Context {
 Context g_ctx;
 std::mutex g_mu;
 
-// A form is DAZI_FORM_PLAIN or DAZI_FORM_ADJOINT plus flags.  The Love and
-// group-velocity flags go with the plain form (or a phase-velocity-only
-// call); the adjoint form, the FP32 scan and Lsen_Gsc are Rayleigh phase.
+// A form is DAZI_FORM_PLAIN or DAZI_FORM_ADJOINT plus flags.  The plain
+// form (and a phase-velocity-only call) takes Love waves and group velocity;
+// the adjoint form takes Rayleigh or Love phase velocity; the FP32 scan and
+// Lsen_Gsc are Rayleigh phase.
 constexpr int kWaveFlags = DAZI_FORM_LOVE | DAZI_FORM_GROUP;
 
 int check_form(int form, bool lsen)
@@ -170,8 +171,9 @@ int check_form(int form, bool lsen)
     constexpr int known = DAZI_FORM_ADJOINT | DAZI_FORM_SCAN_FP32 | kWaveFlags;
     if (form & ~known) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
     if (form & kWaveFlags) {
-        if (form & (DAZI_FORM_ADJOINT | DAZI_FORM_SCAN_FP32)) {
-            set_err("Love waves and group velocity run in the plain form only (form %d)", form);
+        if ((form & DAZI_FORM_SCAN_FP32) || ((form & DAZI_FORM_ADJOINT) && (form & DAZI_FORM_GROUP))) {
+            set_err("group velocity runs in the plain form only, the FP32 scan with Rayleigh phase "
+                    "velocity only (form %d)", form);
             return DAZI_ERR_BADARG;
         }
         if (lsen) {
@@ -459,8 +461,10 @@ int run_root(const Tables& T, const double* per, const StageOut& o, int form, bo
     return 0;
 }
 
+// love: Love-wave phase velocity (adjoint_love_kernel, on the grid and
+// scratch of the Rayleigh kernel's variant).
 int run_adjoint(const Tables& T, const double* per, const StageOut& o, long long maxr, Work& W,
-                const LaunchCfg& cfg, cudaStream_t st)
+                const LaunchCfg& cfg, cudaStream_t st, bool love = false)
 {
     int r;
     long long nblk;
@@ -471,7 +475,8 @@ int run_adjoint(const Tables& T, const double* per, const StageOut& o, long long
     j.T = T; j.periods = per; j.croot = W.croot.as<double>();
     j.sen_vs = o.svs; j.sen_vp = o.svp; j.sen_rho = o.srh;
     j.scratch = W.adjscr.as<double>(); j.scr_layers = maxr > 1 ? maxr - 1 : 1; j.queue = queues;
-    if (cfg.adj_minb == 2) adjoint_kernel<2><<<(unsigned)nblk, 128, 0, st>>>(j);
+    if (love) adjoint_love_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(j);
+    else if (cfg.adj_minb == 2) adjoint_kernel<2><<<(unsigned)nblk, 128, 0, st>>>(j);
     else if (cfg.adj_minb == 4) adjoint_kernel<4><<<(unsigned)nblk, 128, 0, st>>>(j);
     else adjoint_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(j);
     CK(cudaGetLastError());
@@ -516,7 +521,7 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
     if ((r = table_maxr(T, st, maxr))) return r;
     if ((r = ensure_sweep_scratch(T, adj, o.lsen != nullptr, maxr, cfg, W))) return r;
     if (!fd_done && (r = run_root(T, per, o, form, adj, W, cfg, st))) return r;
-    if (adj && (r = run_adjoint(T, per, o, maxr, W, cfg, st))) return r;
+    if (adj && (r = run_adjoint(T, per, o, maxr, W, cfg, st, form_ifunc(form) == 1))) return r;
     if (outs_ready) CK(cudaEventRecord(outs_ready, st));
     if (o.lsen && (r = run_ti(T, per, o, maxr, W, cfg, st))) return r;
     return 0;
@@ -1257,8 +1262,8 @@ int dazi_dk_plan_create(long long ncols, const long long* node_off, const float*
         return DAZI_ERR_BADARG;
     }
     if ((vp == nullptr) != (rho == nullptr)) { set_err("vp and rho must both be set or both NULL"); return DAZI_ERR_BADARG; }
-    if (check_form(form, lsen != nullptr) || (form & 1) != DAZI_FORM_ADJOINT) {
-        set_err("plans run the adjoint form (form %d)", form);
+    if (check_form(form, lsen != nullptr) || (form & 1) != DAZI_FORM_ADJOINT || (form & kWaveFlags)) {
+        set_err("plans run the adjoint form of Rayleigh phase velocity (form %d)", form);
         return DAZI_ERR_BADARG;
     }
     if (!(minthk > 0.f) || !std::isfinite(minthk)) { set_err("minthk must be > 0"); return DAZI_ERR_BADARG; }

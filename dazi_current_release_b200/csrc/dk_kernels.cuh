@@ -161,6 +161,7 @@ __global__ void prep_build_kernel(ColSrc src, PrepOut o, Tables T, const int* so
 template <int BT, int MINB, int IFUNC = 2, bool GROUP = false>
 __global__ void root_kernel(RootArgs a);
 template <int MINB> __global__ void adjoint_kernel(AdjArgs a);    // MINB in {2, 3, 4}
+template <int MINB> __global__ void adjoint_love_kernel(AdjArgs a);   // MINB = 3
 template <int MINB> __global__ void ti_kernel(TiArgs a);          // MINB in {2, 3, 4, 6, 8}
 
 __global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);

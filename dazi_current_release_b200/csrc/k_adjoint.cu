@@ -461,6 +461,219 @@ adjoint_kernel(AdjArgs a)
     }
 }
 
+// ------------------------------------------------------------------ Love
+// Adjoint form for Love waves (dltar1, surfdisp96.f:704-763).  F is the top
+// component of a chain of 2x2 Haskell-Thomson steps from the half-space up:
+//     e(m) = e(m+1) M_m / n_m,   M = [[cos q, y/mu], [mu z, cos q]],
+// mu = rho b^2, e(rmax-1) = (rho rb, 1/b^2) for the half-space.  With
+// g(0) = (1,0), g(m+1) = M_m g(m) / n_m, dF/dtheta_m = e(m+1) dM_m g(m) / n_m
+// (and dF/dtheta = (dh/dtheta) . g for the half-space), for theta = the
+// layer's flattened Vs and density and the wavenumber.  Vp does not enter:
+// its kernel is zero.  Evanescent layers hold their factored-out e^-q as a
+// constant, as in the Rayleigh kernel above, which leaves the ratio
+// dF/dtheta / dF/dwvno exact.
+struct Love3 {
+    D3 cosq, m01, m10;   // M00 = M11 = cosq, M01 = y / mu, M10 = mu z
+};
+
+// One layer's M with tangents in (b, rho, wvno).
+__device__ __forceinline__ void love_layer_d3(double b, double rho, double d, double wvno_v,
+                                              double omega, Love3& o)
+{
+    const double ib = fast_rcp(b);
+    const D3 wvno = {wvno_v, 0.0, 0.0, 1.0};
+    const double xkb_v = omega * ib;
+    const D3 xkb = {xkb_v, -xkb_v * ib, 0.0, 0.0};   // d(omega/b)/db
+    const D3 s = wvno + xkb, t = wvno - xkb;
+    const D3 prod = s * ((t.v < 0.0 ? -1.0 : 1.0) * t);
+    const double r = fast_sqrt(prod.v);
+    const double ir = r > 0.0 ? fast_rcp(r) : 0.0;
+    const double h = 0.5 * ir;
+    const D3 rb = {r, prod.d0 * h, prod.d1 * h, prod.d2 * h};
+    const D3 q = rb * d;
+    D3 cosq, y, z;
+    if (wvno_v < xkb_v) {
+        double sq, cq;
+        sincos(q.v, &sq, &cq);
+        cosq = {cq, -sq * q.d0, -sq * q.d1, -sq * q.d2};
+        const D3 sn = {sq, cq * q.d0, cq * q.d1, cq * q.d2};
+        y = div_by(sn, rb, ir);
+        z = -(rb * sn);
+    } else if (wvno_v == xkb_v) {
+        cosq = mk(1.0);
+        y = mk(d);
+        z = mk(0.0);
+    } else {
+        const double fac = q.v < 16.0 ? exp(-2.0 * q.v) : 0.0;
+        const double cs = (1.0 + fac) * 0.5, ss = (1.0 - fac) * 0.5;
+        // d(cosh) = sinh dq, d(sinh) = cosh dq under the held scale e^-q
+        cosq = {cs, ss * q.d0, ss * q.d1, ss * q.d2};
+        const D3 sn = {ss, cs * q.d0, cs * q.d1, cs * q.d2};
+        y = div_by(sn, rb, ir);
+        z = rb * sn;
+    }
+    const D3 mu = {rho * b * b, 2.0 * rho * b, b * b, 0.0};
+    o.cosq = cosq;
+    o.m01 = div_by(y, mu, fast_rcp(mu.v));
+    o.m10 = mu * z;
+}
+
+// One bottom-up step f = e M (values); returns the max-norm of f (1 below
+// 1e-40), as dltar1 normalises.
+__device__ __forceinline__ double love_step_val(double b, double rho, double d, double wvno,
+                                                double omega, const double e[2], double f[2])
+{
+    Love3 M;
+    love_layer_d3(b, rho, d, wvno, omega, M);
+    f[0] = e[0] * M.cosq.v + e[1] * M.m10.v;
+    f[1] = e[0] * M.m01.v + e[1] * M.cosq.v;
+    double t1 = fmax(fabs(f[0]), fabs(f[1]));
+    if (t1 < 1.0e-40) t1 = 1.0;
+    return t1;
+}
+
+// Half-space vector (rho rb, 1/b^2) with tangents in (b, rho, wvno).
+__device__ __forceinline__ void love_halfspace_d3(double b, double rho, double wvno_v, double omega,
+                                                  D3 h[2])
+{
+    const double ib = fast_rcp(b);
+    const D3 wvno = {wvno_v, 0.0, 0.0, 1.0};
+    const double xkb_v = omega * ib;
+    const D3 xkb = {xkb_v, -xkb_v * ib, 0.0, 0.0};
+    const D3 s = wvno + xkb, t = wvno - xkb;
+    const D3 prod = s * ((t.v < 0.0 ? -1.0 : 1.0) * t);
+    const double r = fast_sqrt(prod.v);
+    const double hh = r > 0.0 ? 0.5 * fast_rcp(r) : 0.0;
+    const D3 rb = {r, prod.d0 * hh, prod.d1 * hh, prod.d2 * hh};
+    h[0] = D3{rho, 0.0, 1.0, 0.0} * rb;
+    h[1] = {ib * ib, -2.0 * ib * ib * ib, 0.0, 0.0};
+}
+
+template <int MINB>
+__global__ void __launch_bounds__(128, MINB)
+adjoint_love_kernel(AdjArgs a)
+{
+    const Tables& T = a.T;
+    constexpr long long nslots = TILE;   // scratch per warp [layer][3 of 6][lane]
+    const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    for (;;) {
+        const long long task = next_task(a.queue);
+        if (task >= T.ntasks) break;
+        const int2 tk = T.tasks[task];
+        const long long s = (long long)tk.x * TILE + lane;
+        const int k = tk.y;
+        if (s >= T.ncols) continue;
+        const ColMeta M = T.meta[s];
+        if (k >= M.K) continue;
+        const double croot = a.croot[task * TILE + lane];
+        const int nz = M.nz, rmax = M.rmax;
+        double* dvs = a.sen_vs + M.sen_b + T.sen_sk * k;
+        double* dvp = a.sen_vp + M.sen_b + T.sen_sk * k;
+        double* drh = a.sen_rho + M.sen_b + T.sen_sk * k;
+        const long long nstride = M.sen_is;
+        for (int i = 0; i < nz; ++i) dvp[nstride * i] = 0.0;   // Love waves do not see Vp
+        if (!(croot > 0.0)) {
+            for (int i = 0; i < nz; ++i) { dvs[nstride * i] = 0.0; drh[nstride * i] = 0.0; }
+            continue;
+        }
+        const double omega = TWOPI / a.periods[M.per_b + k];
+        const double wvno = omega / croot;
+        const long long lbase = T.tile_lbase[tk.x] + lane;
+        const float4* lay = T.flat + lbase;            // layer m at lay[m * TILE]: (d, a, b, rho)
+        const ChainRec* chr = T.ch + lbase;
+        double* scr = a.scratch + (slot / TILE) * a.scr_layers * 6 * TILE + lane;
+        // ---- 1. bottom-up sweep: store e(m+1) and 1/n_m for m = rmax-2 .. 0
+        double e[2];
+        {
+            const float4 L = lay[(long long)(rmax - 1) * TILE];
+            D3 h[2];
+            love_halfspace_d3((double)L.z, (double)L.w, wvno, omega, h);
+            e[0] = h[0].v; e[1] = h[1].v;
+        }
+        for (int m = rmax - 2; m >= 0; --m) {
+            const float4 L = lay[(long long)m * TILE];
+            double f[2];
+            const double nrm = love_step_val((double)L.z, (double)L.w, (double)L.x, wvno, omega, e, f);
+            double* sp = scr + (long long)m * 6 * nslots;
+            sp[0] = e[0]; sp[nslots] = e[1];
+            const double inv = fast_rcp(nrm);
+            sp[2 * nslots] = inv;
+            e[0] = f[0] * inv; e[1] = f[1] * inv;
+        }
+        // ---- 2. top-down sweep with tangents
+        double gv[2] = {1.0, 0.0};
+        int gexp = 0;                 // g is kept as gv * 2^gexp
+        double dFdw = 0.0;
+        double acc_vs = 0.0, acc_rh = 0.0, nxt_vs = 0.0, nxt_rh = 0.0;
+        int cur_node = 0;
+        for (int m = 0; m <= rmax - 2; ++m) {
+            const ChainRec ch = chr[(long long)m * TILE];
+            const int node = ch.node;
+            if (node != cur_node) {
+                dvs[nstride * cur_node] = acc_vs;
+                drh[nstride * cur_node] = acc_rh;
+                acc_vs = nxt_vs; acc_rh = nxt_rh;
+                nxt_vs = nxt_rh = 0.0;
+                cur_node = node;
+            }
+            const float4 L = lay[(long long)m * TILE];
+            Love3 C;
+            love_layer_d3((double)L.z, (double)L.w, (double)L.x, wvno, omega, C);
+            const double* sp = scr + (long long)m * 6 * nslots;
+            const double u0 = sp[0], u1 = sp[nslots], inv = sp[2 * nslots];
+            const double sc = ldexp(inv, gexp);
+            // u . dM . g,  M = [[c, m01], [m10, c]]
+            auto contract = [&](double dc, double d01, double d10) {
+                return u0 * (dc * gv[0] + d01 * gv[1]) + u1 * (d10 * gv[0] + dc * gv[1]);
+            };
+            const double dFdb = contract(C.cosq.d0, C.m01.d0, C.m10.d0) * sc;
+            const double dFdr = contract(C.cosq.d1, C.m01.d1, C.m10.d1) * sc;
+            dFdw = fma(contract(C.cosq.d2, C.m01.d2, C.m10.d2), sc, dFdw);
+            // chain to nodes: b_flat = tmp ((1-f) vs_i + f vs_i+1), rho likewise
+            const double tmpm = ch.tmp, rf = (double)ch.rhofac;
+            const double fw = (double)ch.sub * fast_rcp((double)ch.den);
+            acc_vs = fma(dFdb * tmpm, 1.0 - fw, acc_vs); nxt_vs = fma(dFdb * tmpm, fw, nxt_vs);
+            acc_rh = fma(dFdr * rf, 1.0 - fw, acc_rh);   nxt_rh = fma(dFdr * rf, fw, nxt_rh);
+            // g <- M g / n, rescaled by a power of two
+            double g0 = (C.cosq.v * gv[0] + C.m01.v * gv[1]) * inv;
+            double g1 = (C.m10.v * gv[0] + C.cosq.v * gv[1]) * inv;
+            const double mx = fmax(fabs(g0), fabs(g1));
+            int ex = 0;
+            if (mx > 0.0) frexp(mx, &ex);
+            gv[0] = ldexp(g0, -ex); gv[1] = ldexp(g1, -ex);
+            gexp += ex;
+        }
+        // half-space: its contributions go to node nz-1
+        {
+            const int m = rmax - 1;
+            const float4 L = lay[(long long)m * TILE];
+            const ChainRec ch = chr[(long long)m * TILE];
+            D3 h[2];
+            love_halfspace_d3((double)L.z, (double)L.w, wvno, omega, h);
+            const double sc = ldexp(1.0, gexp);
+            const double s0 = (h[0].d0 * gv[0] + h[1].d0 * gv[1]) * sc;
+            const double s1 = (h[0].d1 * gv[0] + h[1].d1 * gv[1]) * sc;
+            dFdw = fma(h[0].d2 * gv[0] + h[1].d2 * gv[1], sc, dFdw);
+            const double tmpm = ch.tmp, rf = (double)ch.rhofac;
+            dvs[nstride * cur_node] = acc_vs;
+            drh[nstride * cur_node] = acc_rh;
+            nxt_vs = fma(s0, tmpm, nxt_vs);
+            nxt_rh = fma(s1, rf, nxt_rh);
+            dvs[nstride * (nz - 1)] = nxt_vs;
+            drh[nstride * (nz - 1)] = nxt_rh;
+        }
+        // ---- 3. dc/dm = -F_m / F_c = (c / (wvno F_wvno)) F_m
+        const double scale = croot / (wvno * dFdw);
+        for (int i = 0; i < nz; ++i) {
+            dvs[nstride * i] *= scale;
+            drh[nstride * i] *= scale;
+        }
+    }
+}
+
+template __global__ void adjoint_love_kernel<3>(AdjArgs);
+
 template __global__ void adjoint_kernel<2>(AdjArgs);
 template __global__ void adjoint_kernel<3>(AdjArgs);
 template __global__ void adjoint_kernel<4>(AdjArgs);

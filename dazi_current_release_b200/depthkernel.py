@@ -99,7 +99,8 @@ def depthkernel(nx, ny, nz, vel, iwave, igr, kmaxRc, tRc, depz, minthk, *, form=
     (pvRc only when kernels=False).  form: FORM_PLAIN / FORM_ADJOINT, or
     None to read DAZI_DEPTHKERNEL_BACKEND.  iwave 2 (Rayleigh) or 1 (Love),
     igr 0 (phase) or > 0 (group velocity), as surfdisp96 takes them; Love
-    and group velocity run in the plain form (or with kernels=False).
+    phase velocity runs in either form, group velocity in the plain form
+    (or with kernels=False).
     """
     if form is None:
         form = resolve_form(ENV_ISO)

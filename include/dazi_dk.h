@@ -19,8 +19,9 @@
  * through; DAzi's inversion calls Rayleigh phase, CalSurfG_parallel.f90:
  * 1967-1976, and holds the other three calls at CalSurfG.f90:1227-1245).
  * The plain form and phase-velocity-only calls take all four; the adjoint
- * form and Lsen_Gsc are Rayleigh phase only.  Other values return
- * DAZI_ERR_BADARG.
+ * form takes Rayleigh and Love phase velocity (the Love kernels come from
+ * the 2x2 Haskell-Thomson chain of dltar1, and dc/dVp is zero); Lsen_Gsc is
+ * Rayleigh phase only.  Other values return DAZI_ERR_BADARG.
  *
  * Limits (the reference's compiled limits, surfdisp96.f:57-59):
  *   nz <= 200, kmaxRc <= 160, refined layers <= 200.
@@ -68,9 +69,10 @@ extern "C" {
  * (igr > 0; pvRc and the kernels are then the group velocity and its
  * derivatives).  The entries with iwave/igr arguments set them from those
  * (and reject them in form); the device and uneven-column entries take
- * them here.  The adjoint form, DAZI_FORM_SCAN_FP32,
- * Lsen_Gsc and plans are Rayleigh phase velocity only: combining them with
- * these flags returns DAZI_ERR_BADARG. */
+ * them here.  The adjoint form takes DAZI_FORM_LOVE (phase velocity only);
+ * DAZI_FORM_SCAN_FP32, Lsen_Gsc, plans, and the adjoint form with
+ * DAZI_FORM_GROUP are Rayleigh phase velocity only: those combinations
+ * return DAZI_ERR_BADARG. */
 #define DAZI_FORM_LOVE     4
 #define DAZI_FORM_GROUP    8
 

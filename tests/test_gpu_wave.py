@@ -137,8 +137,72 @@ def test_uneven_batch_love_group(oracle, iwave, igr):
 def test_wave_flags_rejected_where_rayleigh_phase_only():
     b = S.config3(realisations=1, columns=4, base_seed=7)
     args = (b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk)
-    for form, kw in ((dk.FORM_ADJOINT | dk.FORM_LOVE, {}), (dk.FORM_ADJOINT | dk.FORM_GROUP, {}),
+    for form, kw in ((dk.FORM_ADJOINT | dk.FORM_LOVE, dict(lsen=True)),   # Lsen: Rayleigh only
+                     (dk.FORM_ADJOINT | dk.FORM_GROUP, {}),
                      (dk.FORM_PLAIN | dk.FORM_LOVE, dict(lsen=True, kernels=False))):
         with pytest.raises(dk.DaziError) as ei:
             depthkernel_batch(*args, form=form, **kw)
         assert ei.value.code == -1
+
+
+@pytest.mark.parametrize("make", [lambda: S.subgrid(S.config0(), 4, 3),
+                                  lambda: S.subgrid(S.config1(), 4, 3)])
+def test_love_adjoint_matches_exact_derivative(oracle, make):
+    """Adjoint form for Love phase velocity against the oracle's
+    high-accuracy central differences (double-precision model pipeline, root
+    converged to 1e-13, dln = 1e-4), and against the reference's own kernels
+    within their own finite-difference noise.  Love waves do not see Vp: the adjoint's dc/dVp is
+    exactly zero (the differences show only round-off)."""
+    from conftest import rel_l2
+    case = make()
+    nx, ny, nz = case.vel.shape
+    K = case.periods.size
+    if case.vp is not None:
+        pv, svs, svp, srh = dk.depthkernel_vpvsrho(nx, ny, nz, case.vel, case.vp, case.rho, 1, 0, K,
+                                                   case.periods, case.depz, case.minthk,
+                                                   form=dk.FORM_ADJOINT)
+    else:
+        pv, svs, svp, srh = dk.depthkernel(nx, ny, nz, case.vel, 1, 0, K, case.periods,
+                                           case.depz, case.minthk, form=dk.FORM_ADJOINT)
+    fine = oracle.depthkernel(case.vel, case.depz, case.periods, case.minthk, vp=case.vp,
+                              rho=case.rho, iwave=1, tol=1e-13, exact=True, dln=1e-4)
+    plain = oracle.depthkernel(case.vel, case.depz, case.periods, case.minthk, vp=case.vp,
+                               rho=case.rho, iwave=1)
+    assert (plain["status"] == 0).all()
+    _moves_ok(pv, plain["pvRc"], 1, 0)
+    assert np.count_nonzero(svp) == 0
+    assert np.abs(fine["sen_vp"]).max() <= 1e-6 * np.abs(fine["sen_vs"]).max()
+    nxy = nx * ny
+    worst = {n: max(rel_l2(g[c], fine[k][c]) for c in range(nxy))
+             for n, g, k in (("vs", svs, "sen_vs"), ("rho", srh, "sen_rho"))}
+    print("Love adjoint vs fine FD worst per-column rel-L2", worst)
+    for n, w in worst.items():
+        assert w <= 1e-5, (n, w)
+    # The reference's kernels difference FP32-rounded phase velocities at
+    # dln = 0.01; Love waves are weakly sensitive to density, so that noise
+    # is relatively large in dc/drho.  The adjoint must sit as close to the
+    # reference's kernels as the exact derivative does.
+    for n, g, k in (("vs", svs, "sen_vs"), ("rho", srh, "sen_rho")):
+        for c in range(nxy):
+            noise = rel_l2(plain[k][c], fine[k][c])
+            assert rel_l2(g[c], plain[k][c]) <= 1.5 * noise + 1e-5, (n, c, noise)
+
+
+def test_love_adjoint_uneven_batch(oracle):
+    """The uneven-column entry with FORM_ADJOINT | FORM_LOVE, per column
+    against the oracle's high-accuracy differences."""
+    from conftest import rel_l2
+    b = S.config3(realisations=1, columns=48, base_seed=2024)
+    r = depthkernel_batch(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk,
+                          form=dk.FORM_ADJOINT | dk.FORM_LOVE, kernels=True, lsen=False)
+    assert (r["status"] == 0).all()
+    assert np.count_nonzero(r["sen_vp"]) == 0
+    for c in range(0, 48, 6):
+        n0, n1 = b.node_off[c], b.node_off[c + 1]
+        p0, p1 = b.per_off[c], b.per_off[c + 1]
+        vel = np.asfortranarray(b.vs[n0:n1].reshape(1, 1, n1 - n0))
+        fine = oracle.depthkernel(vel, b.depz[n0:n1], b.periods[p0:p1], b.minthk, iwave=1,
+                                  tol=1e-13, exact=True, dln=1e-4)
+        pv, svs, svp, srh = r.column(c)
+        assert rel_l2(svs, fine["sen_vs"][0]) <= 1e-5, c
+        assert rel_l2(srh, fine["sen_rho"][0]) <= 1e-5, c
