@@ -1,7 +1,7 @@
 """B200-native depth-kernel stage of DAzi (surface-wave azimuthal anisotropy
 tomography): Rayleigh phase velocities and the dc/dVs and Gc/Gs sensitivity
-kernels (and Love phase velocities with their kernels in both forms, group
-velocities with theirs in the plain form), computed by hand-written sm_100a CUDA kernels behind a C-ABI
+kernels (and Love waves and group velocities with their kernels, in both
+forms), computed by hand-written sm_100a CUDA kernels behind a C-ABI
 (include/dazi_dk.h).  The Python side mirrors the reference's Fortran
 interfaces `depthkernel` and `depthkernelTI`.
 """

@@ -28,7 +28,7 @@ FORM_PLAIN = 0
 FORM_ADJOINT = 1
 FORM_SCAN_FP32 = 2      # flag: FP32 coarse scan verified in FP64 (default: all FP64)
 FORM_LOVE = 4           # flag: Love waves (surfdisp96 iwave = 1), plain or adjoint form
-FORM_GROUP = 8          # flag: group velocity (igr > 0), plain form / phase only
+FORM_GROUP = 8          # flag: group velocity (igr > 0), plain or adjoint form
 
 # every symbol include/dazi_dk.h declares
 EXPORTS = (

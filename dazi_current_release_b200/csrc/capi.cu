@@ -68,12 +68,12 @@ struct DBuf {
 // task list, the counters and the sweep scratch (the global entries share
 // one; every plan owns one).
 struct Work {
-    DBuf croot, counters, adjscr, tiscr;
+    DBuf croot, crootb, counters, adjscr, tiscr;
     DBuf keys, keys2, cidx, cidx2, rmaxb, trecs, ttasks, tlbase, ttbase, cubtmp;
     DBuf tflat, tld, tti, tsp, tch, tmeta, ttasklist;
     void release()
     {
-        DBuf* all[] = {&croot, &counters, &adjscr, &tiscr, &keys, &keys2, &cidx, &cidx2, &rmaxb,
+        DBuf* all[] = {&croot, &crootb, &counters, &adjscr, &tiscr, &keys, &keys2, &cidx, &cidx2, &rmaxb,
                        &trecs, &ttasks, &tlbase, &ttbase, &cubtmp, &tflat, &tld, &tti, &tsp,
                        &tch, &tmeta, &ttasklist};
         for (DBuf* b : all) b->release();
@@ -160,10 +160,9 @@ struct Context {
 Context g_ctx;
 std::mutex g_mu;
 
-// A form is DAZI_FORM_PLAIN or DAZI_FORM_ADJOINT plus flags.  The plain
-// form (and a phase-velocity-only call) takes Love waves and group velocity;
-// the adjoint form takes Rayleigh or Love phase velocity; the FP32 scan and
-// Lsen_Gsc are Rayleigh phase.
+// A form is DAZI_FORM_PLAIN or DAZI_FORM_ADJOINT plus flags.  Both forms
+// (and a phase-velocity-only call) take Love waves and group velocity; the
+// FP32 scan and Lsen_Gsc are Rayleigh phase.
 constexpr int kWaveFlags = DAZI_FORM_LOVE | DAZI_FORM_GROUP;
 
 int check_form(int form, bool lsen)
@@ -171,9 +170,8 @@ int check_form(int form, bool lsen)
     constexpr int known = DAZI_FORM_ADJOINT | DAZI_FORM_SCAN_FP32 | kWaveFlags;
     if (form & ~known) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
     if (form & kWaveFlags) {
-        if ((form & DAZI_FORM_SCAN_FP32) || ((form & DAZI_FORM_ADJOINT) && (form & DAZI_FORM_GROUP))) {
-            set_err("group velocity runs in the plain form only, the FP32 scan with Rayleigh phase "
-                    "velocity only (form %d)", form);
+        if (form & DAZI_FORM_SCAN_FP32) {
+            set_err("the FP32 scan runs with Rayleigh phase velocity only (form %d)", form);
             return DAZI_ERR_BADARG;
         }
         if (lsen) {
@@ -410,13 +408,14 @@ int table_maxr(const Tables& T, cudaStream_t st, long long& maxr)
 // Scratch of the sweeps, sized for the persistent grids of the chosen
 // variants (allocation happens here, never inside a graph capture).
 int ensure_sweep_scratch(const Tables& T, bool adj, bool ti, long long maxr, const LaunchCfg& cfg,
-                         Work& W)
+                         Work& W, bool group = false)
 {
     int r;
     const long long nitems = T.ntasks * TILE;
     if (adj) {
         long long nblk;
         if ((r = W.croot.ensure(sizeof(double) * TILE * (size_t)T.ntasks))) return r;
+        if (group && (r = W.crootb.ensure(sizeof(double) * TILE * (size_t)T.ntasks))) return r;
         if ((r = launch_persistent_grid(adjoint_fn(cfg.adj_minb), nitems, 128, nblk))) return r;
         const size_t scr = sizeof(double) * 6 * (size_t)(maxr > 1 ? maxr - 1 : 1) * (size_t)(nblk * 128);
         if ((r = W.adjscr.ensure(scr))) return r;
@@ -436,6 +435,7 @@ int run_root(const Tables& T, const double* per, const StageOut& o, int form, bo
     RootArgs a;
     a.T = T; a.periods = per; a.tol = 1.0e-6;   // surfdisp96.f:608
     a.pv = o.pv; a.croot = adj ? W.croot.as<double>() : nullptr; a.status = o.status;
+    a.croot_b = adj && form_group(form) ? W.crootb.as<double>() : nullptr;
     a.nevals = W.counters.as<unsigned long long>();
     a.scan32 = (form & DAZI_FORM_SCAN_FP32) ? 1 : 0;
     const int ifunc = form_ifunc(form);
@@ -461,10 +461,11 @@ int run_root(const Tables& T, const double* per, const StageOut& o, int form, bo
     return 0;
 }
 
-// love: Love-wave phase velocity (adjoint_love_kernel, on the grid and
-// scratch of the Rayleigh kernel's variant).
+// love: Love waves (adjoint_love_kernel); group: group velocity, from the
+// roots at t1a and t1b (adjoint_group_kernel, adjoint_love_group_kernel).
+// All run on the grid and scratch of the Rayleigh phase kernel's variant.
 int run_adjoint(const Tables& T, const double* per, const StageOut& o, long long maxr, Work& W,
-                const LaunchCfg& cfg, cudaStream_t st, bool love = false)
+                const LaunchCfg& cfg, cudaStream_t st, bool love = false, bool group = false)
 {
     int r;
     long long nblk;
@@ -475,7 +476,10 @@ int run_adjoint(const Tables& T, const double* per, const StageOut& o, long long
     j.T = T; j.periods = per; j.croot = W.croot.as<double>();
     j.sen_vs = o.svs; j.sen_vp = o.svp; j.sen_rho = o.srh;
     j.scratch = W.adjscr.as<double>(); j.scr_layers = maxr > 1 ? maxr - 1 : 1; j.queue = queues;
-    if (love) adjoint_love_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(j);
+    j.croot_b = group ? W.crootb.as<double>() : nullptr;
+    if (love && group) adjoint_love_group_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(j);
+    else if (group) adjoint_group_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(j);
+    else if (love) adjoint_love_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(j);
     else if (cfg.adj_minb == 2) adjoint_kernel<2><<<(unsigned)nblk, 128, 0, st>>>(j);
     else if (cfg.adj_minb == 4) adjoint_kernel<4><<<(unsigned)nblk, 128, 0, st>>>(j);
     else adjoint_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(j);
@@ -519,9 +523,10 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
     const bool adj = o.svs && (form & 1) == DAZI_FORM_ADJOINT;
     long long maxr = 0;
     if ((r = table_maxr(T, st, maxr))) return r;
-    if ((r = ensure_sweep_scratch(T, adj, o.lsen != nullptr, maxr, cfg, W))) return r;
+    if ((r = ensure_sweep_scratch(T, adj, o.lsen != nullptr, maxr, cfg, W, form_group(form)))) return r;
     if (!fd_done && (r = run_root(T, per, o, form, adj, W, cfg, st))) return r;
-    if (adj && (r = run_adjoint(T, per, o, maxr, W, cfg, st, form_ifunc(form) == 1))) return r;
+    if (adj && (r = run_adjoint(T, per, o, maxr, W, cfg, st, form_ifunc(form) == 1, form_group(form))))
+        return r;
     if (outs_ready) CK(cudaEventRecord(outs_ready, st));
     if (o.lsen && (r = run_ti(T, per, o, maxr, W, cfg, st))) return r;
     return 0;
@@ -1424,7 +1429,7 @@ void dazi_dk_finalize(void)
     if (!g_ctx.ready) return;
     DBuf* all[] = {&g_ctx.vel, &g_ctx.vp, &g_ctx.rho, &g_ctx.per, &g_ctx.depz, &g_ctx.pv,
                    &g_ctx.svs, &g_ctx.svp, &g_ctx.srh, &g_ctx.status, &g_ctx.geo,
-                   &g_ctx.cscratch, &g_ctx.w.croot, &g_ctx.w.counters, &g_ctx.w.adjscr,
+                   &g_ctx.cscratch, &g_ctx.w.croot, &g_ctx.w.crootb, &g_ctx.w.counters, &g_ctx.w.adjscr,
                    &g_ctx.w.tiscr, &g_ctx.lsen, &g_ctx.w.keys, &g_ctx.w.keys2, &g_ctx.w.cidx, &g_ctx.w.cidx2,
                    &g_ctx.w.rmaxb, &g_ctx.w.trecs, &g_ctx.w.ttasks, &g_ctx.w.tlbase, &g_ctx.w.ttbase,
                    &g_ctx.w.cubtmp, &g_ctx.w.tflat, &g_ctx.w.tld, &g_ctx.w.tti, &g_ctx.w.tsp, &g_ctx.w.tch, &g_ctx.w.tmeta,

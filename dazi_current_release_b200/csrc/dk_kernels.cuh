@@ -37,6 +37,7 @@ struct RootArgs {
     double tol;
     double* pv;             // FP32-valued phase velocities (reference output)
     double* croot;          // [task * 32 + lane] FP64 roots for the adjoint, or nullptr
+    double* croot_b = nullptr;   // group velocity: roots at t1b (croot: at t1a)
     int* status;            // [status_i] first failing period (1-based) or 0
     unsigned long long* nevals;  // secular evaluations (accumulated), or nullptr
     int scan32;             // FP32 coarse scan (with FP64 verification)
@@ -52,6 +53,7 @@ struct AdjArgs {
     double* scratch;        // per warp [scr_layers][6][32 lanes]
     long long scr_layers;   // layer capacity of a warp's scratch block
     unsigned* queue;        // work-queue counter (zeroed before the launch)
+    const double* croot_b = nullptr;   // group velocity: roots at t1b (0: none)
 };
 
 // Doubles per refined layer in each persistent thread's Gc/Gs scratch:
@@ -162,6 +164,10 @@ template <int BT, int MINB, int IFUNC = 2, bool GROUP = false>
 __global__ void root_kernel(RootArgs a);
 template <int MINB> __global__ void adjoint_kernel(AdjArgs a);    // MINB in {2, 3, 4}
 template <int MINB> __global__ void adjoint_love_kernel(AdjArgs a);   // MINB = 3
+// Group velocity (surfdisp96's igr > 0): the derivative of the reference's
+// quotient of the roots at t1a and t1b, from the phase adjoint at both.
+template <int MINB> __global__ void adjoint_group_kernel(AdjArgs a);        // MINB = 3
+template <int MINB> __global__ void adjoint_love_group_kernel(AdjArgs a);   // MINB = 3
 template <int MINB> __global__ void ti_kernel(TiArgs a);          // MINB in {2, 3, 4, 6, 8}
 
 __global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);

@@ -29,6 +29,7 @@
 // evaluation points is the reference's, step for step.
 #pragma once
 #include "dk_model.cuh"
+#include <utility>
 
 namespace dk {
 
@@ -352,6 +353,25 @@ __device__ __forceinline__ float dltar4_f32(LayerF layerf, int mmax, float wvno,
 // cb(k) + 0.01 dc (cb(k) = 0 for the fundamental mode) and ifirst = 0; a
 // second search that finds no root falls back to c(k).  The output is the
 // real*4 group velocity of the two roots.  h = 0.005 (h0, surfdisp96.f:113).
+// The two periods of a group-velocity period t (surfdisp96.f:226-233):
+// t1a = t/(1.+h), t1b = t/(1.-h), real*8 quotients stored in real*4, h = 0.005.
+__device__ __forceinline__ void group_periods(double t, float& t1a, float& t1b)
+{
+    t1a = __double2float_rn(__ddiv_rn(t, (double)__fadd_rn(1.0f, 0.005f)));
+    t1b = __double2float_rn(__ddiv_rn(t, (double)__fsub_rn(1.0f, 0.005f)));
+}
+
+// An output object of the root search may also take the two roots behind a
+// group velocity: out.group_roots(k, c0, c1), c0 the secant-refined root at
+// t1a, c1 the one at t1b, or 0 where the second search found no root and
+// surfdisp96 used c0 in its place.  Detected at compile time.
+template <class O, class = void>
+struct HasGroupRoots { static constexpr bool value = false; };
+template <class O>
+struct HasGroupRoots<O, decltype((void)std::declval<O&>().group_roots(0, 0.0, 0.0))> {
+    static constexpr bool value = true;
+};
+
 template <bool GROUP = false>
 struct RootSM {
     enum Phase : int { START = 0, GS_FIRST, GS_SCAN, VER1, VER2, NEV_A, NEV_B, NEV_CD, DONE,
@@ -371,9 +391,10 @@ struct RootSM {
     double ceval;   // point to evaluate next
     double x[11], y[11];
     // group velocity: second search running, its period t1b, the first root
+    // (and its secant refinement)
     bool second;
     float t1a, t1b;
-    double cph;
+    double cph, cph_t;
 
     __device__ void init(double cc_, float betmx_, int kmax_, double tol_, bool scan32 = false)
     {
@@ -382,7 +403,7 @@ struct RootSM {
         dc = fabs((double)0.005f);
         cmax = (double)betmx_ + dc;
         k = 0; phase = START; fail_k = -1; del1st = 0.0; cprev = 0.0; evals = 0;
-        second = false; t1a = t1b = 0.0f; cph = 0.0;
+        second = false; t1a = t1b = 0.0f; cph = 0.0; cph_t = 0.0;
     }
 
     // Runs the machine until it requests an evaluation (returns true, with
@@ -398,11 +419,8 @@ struct RootSM {
             case START: {
                 if (k >= kmax) { phase = DONE; return false; }
                 if constexpr (GROUP) {
-                    // t1a = t1/(1.+h), t1b = t1/(1.-h): real*8 quotients
-                    // stored in real*4; the first search runs at dble(t1a)
-                    const double t = periods[k];
-                    t1a = __double2float_rn(__ddiv_rn(t, (double)__fadd_rn(1.0f, 0.005f)));
-                    t1b = __double2float_rn(__ddiv_rn(t, (double)__fsub_rn(1.0f, 0.005f)));
+                    // the first search runs at dble(t1a)
+                    group_periods(periods[k], t1a, t1b);
                     second = false;
                     omega = TWOPI / (double)t1a;
                 } else {
@@ -437,7 +455,7 @@ struct RootSM {
                 del1 = del2;
                 d1x = d2x;
                 if (c1 < cm || c1 >= cmax) {
-                    if (GROUP && second) { group_out(cph, out); continue; }
+                    if (GROUP && second) { group_out(cph, 0.0, out); continue; }
                     fail();
                     return false;
                 }
@@ -496,6 +514,19 @@ struct RootSM {
     }
 
   private:
+    // The secant root inside the final bracket [c1, c2] (c3 when the
+    // bracket does not straddle a sign change): error O(bracket^2).  The
+    // same step as finish()'s for phase velocity, written out there.
+    __device__ double secant_root() const
+    {
+        const double dd = del2 - del1;
+        if (dd != 0.0 && fsign1(del1) != fsign1(del2)) {
+            const double s = c1 - del1 * (c2 - c1) / dd;
+            if (s >= fmin(c1, c2) && s <= fmax(c1, c2)) return s;
+        }
+        return c3;
+    }
+
     __device__ bool request(double c)
     {
         ceval = c;
@@ -551,9 +582,10 @@ struct RootSM {
     // Group velocity of period k from the roots at t1a (c0) and t1b (c1),
     // surfdisp96.f:293-299, in real*4 without fused operations:
     //   gvel = (1/t1a - 1/t1b) / (1/(t1a*cc0) - 1/(t1b*cc1))
-    // then the next period.
+    // then the next period.  cbt: the secant-refined second root, 0 when
+    // the second search fell back to c0.
     template <class Out>
-    __device__ void group_out(double cb, Out& out)
+    __device__ void group_out(double cb, double cbt, Out& out)
     {
         const float cc0 = __double2float_rn(cph), cc1 = __double2float_rn(cb);
         const float num = __fsub_rn(__fdiv_rn(1.0f, t1a), __fdiv_rn(1.0f, t1b));
@@ -561,6 +593,7 @@ struct RootSM {
                                     __fdiv_rn(1.0f, __fmul_rn(t1b, cc1)));
         const double g = (double)__fdiv_rn(num, den);
         out(k, g, g, evals);
+        if constexpr (HasGroupRoots<Out>::value) out.group_roots(k, cph_t, cbt);
         ++k;
         p64 = false;
         second = false;
@@ -576,13 +609,17 @@ struct RootSM {
         if constexpr (GROUP) {
             if (second) {
                 // a root above betmx counts as none found: cb(k) = c(k)
-                group_out(c3 > (double)betmx ? cph : c3, out);
+                const bool none = c3 > (double)betmx;
+                double cbt = 0.0;
+                if constexpr (HasGroupRoots<Out>::value) cbt = none ? 0.0 : secant_root();
+                group_out(none ? cph : c3, cbt, out);
                 return true;
             }
         }
         if (c3 > (double)betmx) { out(k, 0.0, 0.0, evals); fail(); return false; }
         if constexpr (GROUP) {
             cph = c3;
+            if constexpr (HasGroupRoots<Out>::value) cph_t = secant_root();
             cprev = c3;
             second = true;
             phase = GR_START;

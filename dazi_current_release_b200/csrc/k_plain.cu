@@ -263,6 +263,26 @@ struct TableModel {
     __device__ __forceinline__ float4 layerf(int m) const { return flat[base + (long long)m * TILE]; }
 };
 
+// Root-search output of one column: pv (FP32-valued), and for the adjoint
+// form the secant-refined FP64 roots, task-major.  For group velocity croot
+// holds the root at t1a and croot_b the one at t1b (0: none, c0 used).
+struct RootOut {
+    const RootArgs& a;
+    const ColMeta& M;
+    __device__ __forceinline__ void operator()(int k, double cval, double ctight, int) const
+    {
+        a.pv[M.pv_b + a.T.pv_sk * k] = (double)(float)cval;
+        if (a.croot) a.croot[M.cr_b + (long long)TILE * k] = ctight;
+    }
+    __device__ __forceinline__ void group_roots(int k, double c0, double c1) const
+    {
+        if (a.croot_b) {
+            a.croot[M.cr_b + (long long)TILE * k] = c0;
+            a.croot_b[M.cr_b + (long long)TILE * k] = c1;
+        }
+    }
+};
+
 // BT: threads per block (one thread per column); MINB: minimum resident
 // blocks per SM the register allocation aims for (0: no constraint).  The
 // autotuner picks one of the instantiations.  IFUNC / GROUP: Love or
@@ -280,10 +300,7 @@ root_kernel(RootArgs a)
     const long long base = T.tile_lbase[ss / TILE] + (ss % TILE);
     const double* per = a.periods + M.per_b;
     TableModel mdl{T.ld, T.flat, base};
-    auto out = [&](int k, double cval, double ctight, int ev) {
-        a.pv[M.pv_b + T.pv_sk * k] = (double)(float)cval;
-        if (a.croot) a.croot[M.cr_b + (long long)TILE * k] = ctight;
-    };
+    RootOut out{a, M};
     double cc = 0.0;
     float betmx = 0.f;
     if (active) {

@@ -98,9 +98,8 @@ def depthkernel(nx, ny, nz, vel, iwave, igr, kmaxRc, tRc, depz, minthk, *, form=
     Returns (pvRc, sen_vsRc, sen_vpRc, sen_rhoRc) as Fortran-ordered arrays
     (pvRc only when kernels=False).  form: FORM_PLAIN / FORM_ADJOINT, or
     None to read DAZI_DEPTHKERNEL_BACKEND.  iwave 2 (Rayleigh) or 1 (Love),
-    igr 0 (phase) or > 0 (group velocity), as surfdisp96 takes them; Love
-    phase velocity runs in either form, group velocity in the plain form
-    (or with kernels=False).
+    igr 0 (phase) or > 0 (group velocity), as surfdisp96 takes them, in
+    either form.
     """
     if form is None:
         form = resolve_form(ENV_ISO)

@@ -18,9 +18,10 @@
  * or > 0 (group), as surfdisp96 takes them (DepthKernel1D.f90 passes both
  * through; DAzi's inversion calls Rayleigh phase, CalSurfG_parallel.f90:
  * 1967-1976, and holds the other three calls at CalSurfG.f90:1227-1245).
- * The plain form and phase-velocity-only calls take all four; the adjoint
- * form takes Rayleigh and Love phase velocity (the Love kernels come from
- * the 2x2 Haskell-Thomson chain of dltar1, and dc/dVp is zero); Lsen_Gsc is
+ * The plain form, the adjoint form and phase-velocity-only calls take all
+ * four (Love: the adjoint differentiates dltar1's 2x2 Haskell-Thomson chain
+ * and dc/dVp is zero; group velocity: the adjoint differentiates the
+ * reference's quotient of the roots at t/(1+h) and t/(1-h)); Lsen_Gsc is
  * Rayleigh phase only.  Other values return DAZI_ERR_BADARG.
  *
  * Limits (the reference's compiled limits, surfdisp96.f:57-59):
@@ -63,16 +64,15 @@ extern "C" {
  * roots as the default all-FP64 search).  The plain form always evaluates
  * in FP64. */
 #define DAZI_FORM_SCAN_FP32 2
-/* flags, OR-ed into the form of the plain form or of a phase-velocity-only
- * call (no sen_* and no Lsen_Gsc outputs): Love instead of Rayleigh waves
+/* flags, OR-ed into the form (plain or adjoint, or a phase-velocity-only
+ * call; no Lsen_Gsc output): Love instead of Rayleigh waves
  * (surfdisp96's iwave = 1, dltar1) and group instead of phase velocity
  * (igr > 0; pvRc and the kernels are then the group velocity and its
  * derivatives).  The entries with iwave/igr arguments set them from those
  * (and reject them in form); the device and uneven-column entries take
- * them here.  The adjoint form takes DAZI_FORM_LOVE (phase velocity only);
- * DAZI_FORM_SCAN_FP32, Lsen_Gsc, plans, and the adjoint form with
- * DAZI_FORM_GROUP are Rayleigh phase velocity only: those combinations
- * return DAZI_ERR_BADARG. */
+ * them here.  Both forms take them.  DAZI_FORM_SCAN_FP32, Lsen_Gsc and
+ * plans are Rayleigh phase velocity only: combining them with these flags
+ * returns DAZI_ERR_BADARG. */
 #define DAZI_FORM_LOVE     4
 #define DAZI_FORM_GROUP    8
 

@@ -600,10 +600,15 @@ static int sd_run(const double *thkm, const double *vpm, const double *vsm,
                 float ccb = (float)c1;
                 if (igr == 0) {
                     cg[k - 1] = round_f32 ? (double)cc0 : c[k - 1];
-                } else {
+                } else if (m->f32) {
                     float gvel = (1.0f / t1a - 1.0f / t1b) /
                                  (1.0f / (t1a * cc0) - 1.0f / (t1b * ccb));
                     cg[k - 1] = (double)gvel;
+                } else {
+                    /* exact-model checker: the same quotient of the FP64 roots
+                     * in double, so that differences resolve its derivative */
+                    const double ia = 1.0 / (double)t1a, ib = 1.0 / (double)t1b;
+                    cg[k - 1] = (ia - ib) / (ia / c[k - 1] - ib / c1);
                 }
             }
             if (failed) {

@@ -54,9 +54,8 @@ def _call_iso(nx=2, ny=2, nz=3, iwave=2, igr=0, K=2, depz=(0.0, 3.0, 6.0), vel=3
 @pytest.mark.parametrize("kw,code", [
     (dict(iwave=3), _lib.DAZI_ERR_BADARG),              # neither Love nor Rayleigh
     (dict(iwave=0), _lib.DAZI_ERR_BADARG),
-    (dict(igr=1, form=_lib.FORM_ADJOINT), _lib.DAZI_ERR_BADARG),     # adjoint: phase velocity
-    (dict(iwave=1, igr=1, form=_lib.FORM_ADJOINT), _lib.DAZI_ERR_BADARG),
     (dict(igr=1, form=_lib.FORM_SCAN_FP32), _lib.DAZI_ERR_BADARG),   # FP32 scan: Rayleigh phase
+    (dict(iwave=1, form=_lib.FORM_ADJOINT | _lib.FORM_SCAN_FP32), _lib.DAZI_ERR_BADARG),
     (dict(form=_lib.FORM_LOVE), _lib.DAZI_ERR_BADARG),  # wave type goes through iwave here
     (dict(form=_lib.FORM_GROUP), _lib.DAZI_ERR_BADARG),
     (dict(form=16), _lib.DAZI_ERR_BADARG),              # unknown flag
@@ -74,11 +73,12 @@ def test_bad_arguments_rejected_without_device(kw, code):
     assert len(_lib.load().dazi_dk_last_error()) > 0
 
 
-@pytest.mark.parametrize("iwave,igr,form", [(1, 0, 0), (2, 1, 0), (1, 1, 0), (2, 5, 0), (1, 0, 1)])
+@pytest.mark.parametrize("iwave,igr,form", [(1, 0, 0), (2, 1, 0), (1, 1, 0), (2, 5, 0), (1, 0, 1),
+                                            (2, 1, 1), (1, 1, 1)])
 def test_love_and_group_pass_validation(iwave, igr, form):
     """Love (iwave = 1) and group velocity (igr > 0) are accepted by the
-    plain form, Love phase velocity by the adjoint form too; without a GPU
-    the call then stops at the device check."""
+    plain and the adjoint form; without a GPU the call then stops at the
+    device check."""
     import torch
     if torch.cuda.is_available():
         pytest.skip("a CUDA device is present")

@@ -138,7 +138,8 @@ def test_wave_flags_rejected_where_rayleigh_phase_only():
     b = S.config3(realisations=1, columns=4, base_seed=7)
     args = (b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk)
     for form, kw in ((dk.FORM_ADJOINT | dk.FORM_LOVE, dict(lsen=True)),   # Lsen: Rayleigh only
-                     (dk.FORM_ADJOINT | dk.FORM_GROUP, {}),
+                     (dk.FORM_ADJOINT | dk.FORM_GROUP, dict(lsen=True)),
+                     (dk.FORM_ADJOINT | dk.FORM_GROUP | dk.FORM_SCAN_FP32, {}),  # FP32 scan: phase
                      (dk.FORM_PLAIN | dk.FORM_LOVE, dict(lsen=True, kernels=False))):
         with pytest.raises(dk.DaziError) as ei:
             depthkernel_batch(*args, form=form, **kw)
@@ -206,3 +207,74 @@ def test_love_adjoint_uneven_batch(oracle):
         pv, svs, svp, srh = r.column(c)
         assert rel_l2(svs, fine["sen_vs"][0]) <= 1e-5, c
         assert rel_l2(srh, fine["sen_rho"][0]) <= 1e-5, c
+
+
+def _group_fd_pair(oracle, vel, depz, periods, minthk, iwave, vp=None, rho=None):
+    """The oracle's exact-model group velocity differenced at dln = 1e-4 and
+    4e-4.  The quotient over t/(1 -+ h) amplifies root round-off ~1/(2h) =
+    100-fold, so the two differ by the differences' own noise (largest in
+    the weakly sensitive density kernels)."""
+    kw = dict(vp=vp, rho=rho, iwave=iwave, igr=1, tol=1e-13, exact=True)
+    return (oracle.depthkernel(vel, depz, periods, minthk, dln=1e-4, **kw),
+            oracle.depthkernel(vel, depz, periods, minthk, dln=4e-4, **kw))
+
+
+def _assert_group_kernels(rel_l2, got, f1, f2, c, names):
+    """Per column: within 3x the exact differences' own noise (+1e-6), and
+    within the 1e-4 rel-L2 kernel bar."""
+    for n in names:
+        noise = rel_l2(f1["sen_" + n][c], f2["sen_" + n][c])
+        err = rel_l2(got[n], f1["sen_" + n][c])
+        assert err <= min(3.0 * noise + 1.0e-6, 1.0e-4), (n, c, err, noise)
+
+
+@pytest.mark.parametrize("iwave", [2, 1])
+@pytest.mark.parametrize("make", [lambda: S.subgrid(S.config0(), 4, 3),
+                                  lambda: S.subgrid(S.config1(), 4, 3)])
+def test_group_adjoint_matches_exact_derivative(oracle, make, iwave):
+    """Adjoint form for group velocity: the derivative of the reference's
+    quotient of the roots at t1a and t1b, from phase adjoints at both,
+    against the oracle's exact-model differences of the same quotient."""
+    from conftest import rel_l2
+    case = make()
+    nx, ny, nz = case.vel.shape
+    K = case.periods.size
+    if case.vp is not None:
+        pv, svs, svp, srh = dk.depthkernel_vpvsrho(nx, ny, nz, case.vel, case.vp, case.rho, iwave,
+                                                   1, K, case.periods, case.depz, case.minthk,
+                                                   form=dk.FORM_ADJOINT)
+    else:
+        pv, svs, svp, srh = dk.depthkernel(nx, ny, nz, case.vel, iwave, 1, K, case.periods,
+                                           case.depz, case.minthk, form=dk.FORM_ADJOINT)
+    plain = oracle.depthkernel(case.vel, case.depz, case.periods, case.minthk, vp=case.vp,
+                               rho=case.rho, iwave=iwave, igr=1)
+    assert (plain["status"] == 0).all()
+    _moves_ok(pv, plain["pvRc"], iwave, 1)
+    f1, f2 = _group_fd_pair(oracle, case.vel, case.depz, case.periods, case.minthk, iwave,
+                            vp=case.vp, rho=case.rho)
+    names = ("vs", "rho") if iwave == 1 else ("vs", "vp", "rho")
+    if iwave == 1:
+        assert np.count_nonzero(svp) == 0
+    for c in range(nx * ny):
+        got = {"vs": svs[c], "vp": svp[c], "rho": srh[c]}
+        _assert_group_kernels(rel_l2, got, f1, f2, c, names)
+
+
+@pytest.mark.parametrize("iwave", [2, 1])
+def test_group_adjoint_uneven_batch(oracle, iwave):
+    """The uneven-column entry with FORM_ADJOINT | FORM_GROUP (| FORM_LOVE),
+    per column against the oracle's exact-model differences."""
+    from conftest import rel_l2
+    b = S.config3(realisations=1, columns=48, base_seed=2024)
+    form = dk.FORM_ADJOINT | dk.FORM_GROUP | (dk.FORM_LOVE if iwave == 1 else 0)
+    r = depthkernel_batch(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk,
+                          form=form, kernels=True, lsen=False)
+    assert (r["status"] == 0).all()
+    names = ("vs", "rho") if iwave == 1 else ("vs", "vp", "rho")
+    for c in range(0, 48, 6):
+        n0, n1 = b.node_off[c], b.node_off[c + 1]
+        p0, p1 = b.per_off[c], b.per_off[c + 1]
+        vel = np.asfortranarray(b.vs[n0:n1].reshape(1, 1, n1 - n0))
+        f1, f2 = _group_fd_pair(oracle, vel, b.depz[n0:n1], b.periods[p0:p1], b.minthk, iwave)
+        pv, svs, svp, srh = r.column(c)
+        _assert_group_kernels(rel_l2, {"vs": svs, "vp": svp, "rho": srh}, f1, f2, 0, names)
