@@ -1,5 +1,7 @@
 """PyTorch binding with gradients: phase velocities of a column batch as a
-differentiable function of the node velocities.
+differentiable function of the node velocities (Rayleigh phase velocity
+with the Gc/Gs kernel; Love waves and group velocity through
+`dispersion_velocity`).
 
 Forward: the library's adjoint form (dazi_dk_batch_dev, form ADJOINT) on the
 tensors' CUDA stream computes c(T) for every (column, period), the three
@@ -85,8 +87,9 @@ class ColumnBatch:
                    np.arange(n + 1) * K, np.tile(np.asarray(periods, np.float64), n), minthk,
                    device)
 
-    def run(self, vs, vp=None, rho=None, lsen=True):
+    def run(self, vs, vp=None, rho=None, lsen=True, flags=0):
         """Forward call of the library on the current stream (no autograd).
+        flags: FORM_LOVE / FORM_GROUP (then lsen=False).
         Returns pv, (sen_vs, sen_vp, sen_rho), lsen, status."""
         L = _lib.load()
         dev = self.device
@@ -104,7 +107,7 @@ class ColumnBatch:
                                  P(rho), P(self.per_off), P(self.periods),
                                  ctypes.c_float(self.minthk), P(pv), P(self.sen_off), P(sen[0]),
                                  P(sen[1]), P(sen[2]), P(self.ls_off) if lsen else None, P(ls),
-                                 _lib.FORM_ADJOINT, P(status), ctypes.c_void_p(stream))
+                                 _lib.FORM_ADJOINT | flags, P(status), ctypes.c_void_p(stream))
         _lib.check(rc)
         return pv, sen, ls, status
 
@@ -131,8 +134,10 @@ def brocher_derivatives(vs):
 
 class _PhaseVelocity(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, vs, vp, rho, batch: ColumnBatch):
-        pv, sen, ls, status = batch.run(vs, vp, rho, lsen=True)
+    def forward(ctx, vs, vp, rho, batch: ColumnBatch, flags: int):
+        pv, sen, ls, status = batch.run(vs, vp, rho, lsen=flags == 0, flags=flags)
+        if ls is None:
+            ls = torch.empty(0, dtype=torch.float32, device=pv.device)
         ctx.batch = batch
         ctx.explicit = vp is not None
         if ctx.explicit:
@@ -150,9 +155,9 @@ class _PhaseVelocity(torch.autograd.Function):
         if ctx.explicit:
             s_vs, s_vp, s_rho = ctx.saved_tensors
             g = [b.vjp(grad_pv, s).to(torch.float32) for s in (s_vs, s_vp, s_rho)]
-            return g[0], g[1], g[2], None
+            return g[0], g[1], g[2], None, None
         (k_tot,) = ctx.saved_tensors
-        return b.vjp(grad_pv, k_tot).to(torch.float32), None, None, None
+        return b.vjp(grad_pv, k_tot).to(torch.float32), None, None, None, None
 
 
 def phase_velocity(vs, batch: ColumnBatch, vp=None, rho=None):
@@ -161,7 +166,24 @@ def phase_velocity(vs, batch: ColumnBatch, vp=None, rho=None):
     Returns (c [nper] float64, lsen [nls] float32, status [ncols] int32)."""
     if (vp is None) != (rho is None):
         raise ValueError("vp and rho must be given together")
-    return _PhaseVelocity.apply(vs, vp, rho, batch)
+    return _PhaseVelocity.apply(vs, vp, rho, batch, 0)
+
+
+def dispersion_velocity(vs, batch: ColumnBatch, vp=None, rho=None, iwave=2, igr=0):
+    """Love (iwave = 1) or Rayleigh (iwave = 2) phase (igr = 0) or group
+    (igr > 0) velocity of every (column, period), as surfdisp96 takes
+    iwave/igr, differentiable in vs (and vp, rho when given).  Group
+    velocity is the reference's quotient of the phase roots at t/(1+h) and
+    t/(1-h); its gradient is the exact derivative of that quotient.  No
+    Gc/Gs kernel (a Rayleigh phase kernel: `phase_velocity`).
+    Returns (c [nper] float64, status [ncols] int32)."""
+    if (vp is None) != (rho is None):
+        raise ValueError("vp and rho must be given together")
+    if iwave not in (1, 2):
+        raise ValueError(f"iwave must be 1 (Love) or 2 (Rayleigh), got {iwave}")
+    flags = (_lib.FORM_LOVE if iwave == 1 else 0) | (_lib.FORM_GROUP if igr > 0 else 0)
+    c, _, status = _PhaseVelocity.apply(vs, vp, rho, batch, flags)
+    return c, status
 
 
 def azimuthal_phase_velocity(c0, lsen, gc, gs, psi, batch: ColumnBatch):

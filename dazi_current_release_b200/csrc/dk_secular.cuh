@@ -218,12 +218,20 @@ __device__ __forceinline__ double dltar1(const M& mdl, int mmax, double wvno, do
         }
         const double e10 = __dadd_rn(__dmul_rn(e1, cosq), __dmul_rn(__dmul_rn(e2, xmu), z));
         const double e20 = __dadd_rn(__ddiv_rn(__dmul_rn(e1, y), xmu), __dmul_rn(e2, cosq));
-        double xnor = fabs(e10);
-        const double ynor = fabs(e20);
-        if (ynor > xnor) xnor = ynor;
-        if (xnor < 1.0e-40) xnor = 1.0;
-        e1 = __ddiv_rn(e10, xnor);
-        e2 = __ddiv_rn(e20, xnor);
+        // normalise by xnor = max(|e10|, |e20|) (1 below 1e-40): the larger
+        // component's quotient is exactly +-1, so one division gives the
+        // reference's two quotients bit for bit
+        const double xnor = fabs(e10), ynor = fabs(e20);
+        if (fmax(xnor, ynor) < 1.0e-40) {
+            e1 = e10;
+            e2 = e20;
+        } else if (ynor > xnor) {
+            e1 = __ddiv_rn(e10, ynor);
+            e2 = copysign(1.0, e20);
+        } else {
+            e1 = copysign(1.0, e10);
+            e2 = __ddiv_rn(e20, xnor);
+        }
     }
     return e1;
 }

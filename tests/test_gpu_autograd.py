@@ -15,7 +15,8 @@ import torch
 from conftest import rel_l2
 from dazi_current_release_b200 import synthetic as S
 from dazi_current_release_b200.autograd import (ColumnBatch, azimuthal_phase_velocity,
-                                                brocher_derivatives, phase_velocity)
+                                                brocher_derivatives, dispersion_velocity,
+                                                phase_velocity)
 
 pytestmark = pytest.mark.gpu
 
@@ -101,3 +102,35 @@ def test_explicit_vp_rho_gradients(oracle):
         e = rel_l2(x.grad.double().cpu().numpy().reshape(n, nz), exp)
         print(name, "VJP rel-L2 vs FP64 central FD", e)
         assert e <= 1e-5
+
+
+@pytest.mark.parametrize("iwave,igr", [(2, 0), (1, 0), (2, 1), (1, 1)])
+def test_dispersion_velocity_gradient(oracle, iwave, igr):
+    """Love / Rayleigh, phase / group velocity through the torch binding:
+    the gradient of a weighted sum of c against the oracle's exact-model
+    differences (root to 1e-13, dln = 1e-4) chained through the Brocher
+    relations.  Group velocity's differences carry ~1/(2h) = 100 times the
+    root round-off, hence the wider bound (the 1e-4 kernel bar)."""
+    case = S.subgrid(S.config1(), 3, 2)
+    nx, ny, nz = case.vel.shape
+    n, K = nx * ny, case.periods.size
+    dev = torch.device("cuda")
+    batch = ColumnBatch.from_grid(nx, ny, case.depz, case.periods, case.minthk, device=dev)
+    vs = torch.tensor(_flat(case.vel), device=dev, requires_grad=True)
+    w = torch.as_tensor(np.random.default_rng(5).standard_normal(batch.nper), device=dev)
+    c, status = dispersion_velocity(vs, batch, iwave=iwave, igr=igr)
+    assert int(status.abs().sum()) == 0
+    (c * w).sum().backward()
+    g = vs.grad.double().cpu().numpy().reshape(n, nz)
+    plain = oracle.depthkernel(case.vel, case.depz, case.periods, case.minthk, iwave=iwave, igr=igr)
+    move = np.abs(c.detach().cpu().numpy().reshape(n, K) / plain["pvRc"] - 1)
+    assert move.max() <= (4.0e-4 if igr else 2.0e-6), move.max()
+    fine = oracle.depthkernel(case.vel, case.depz, case.periods, case.minthk, iwave=iwave,
+                              igr=igr, tol=1e-13, exact=True, dln=1e-4)
+    dvp, drho = (t.cpu().numpy().reshape(n, nz) for t in
+                 brocher_derivatives(torch.as_tensor(_flat(case.vel))))
+    k_tot = fine["sen_vs"] + dvp[:, None, :] * fine["sen_vp"] + drho[:, None, :] * fine["sen_rho"]
+    expect = np.einsum("ck,cki->ci", w.cpu().numpy().reshape(n, K), k_tot)
+    worst = max(rel_l2(g[i], expect[i]) for i in range(n))
+    print("dispersion_velocity gradient vs exact differences, worst column", iwave, igr, worst)
+    assert worst <= (1.0e-4 if igr else 1.0e-5), worst
