@@ -354,189 +354,197 @@ __device__ __forceinline__ double* scr_row(double* scr, int m)
     return scr + (long long)m * 6 * TILE;
 }
 
-// The Rayleigh adjoint of one task per warp, phase velocity or (GROUP) the
-// group velocity's two passes.  The second pass stages its node values in
+// The Rayleigh adjoint of one (column, period): lane `lane` of task `task`
+// (tile, period), with scr the lane's column of its warp's scratch block;
+// phase velocity or (GROUP) the group velocity's two passes.  The second pass stages its node values in
 // scratch rows the top-down sweep has already read (node i is complete only
 // once the sweep is past layer i, since every interval holds a sublayer;
 // i <= nz - 2 < rmax - 1 rows) and the half-space node in registers, then
 // adds them to the first pass's outputs.
 template <bool GROUP>
-__device__ __forceinline__ void adjoint_rayleigh(const AdjArgs& a)
+__device__ __forceinline__ void adjoint_rayleigh_task(const AdjArgs& a, long long task, int lane, double* scr)
 {
     const Tables& T = a.T;
-    // scratch: per warp [layer][6][lane] -- compile-time strides
     constexpr long long nslots = TILE;
+    const int2 tk = T.tasks[task];
+    const long long s = (long long)tk.x * TILE + lane;
+    const int k = tk.y;
+    if (s >= T.ncols) return;
+    const ColMeta M = T.meta[s];
+    if (k >= M.K) return;
+    const double c0 = a.croot[task * TILE + lane];
+    const int nz = M.nz, rmax = M.rmax;
+    double* dvs = a.sen_vs + M.sen_b + T.sen_sk * k;
+    double* dvp = a.sen_vp + M.sen_b + T.sen_sk * k;
+    double* drh = a.sen_rho + M.sen_b + T.sen_sk * k;
+    const long long nstride = M.sen_is;   // node stride in the outputs
+    if (!(c0 > 0.0)) {
+        for (int i = 0; i < nz; ++i) { dvs[nstride * i] = 0.0; dvp[nstride * i] = 0.0; drh[nstride * i] = 0.0; }
+        return;
+    }
+    double omega = TWOPI / a.periods[M.per_b + k];
+    double wvno = omega / c0;
+    GroupPasses gp{};
+    int npass = 1;
+    if constexpr (GROUP) {
+        gp = group_passes(a.periods[M.per_b + k], c0, a.croot_b[task * TILE + lane]);
+        npass = gp.n;
+    }
+    const long long lbase = T.tile_lbase[tk.x] + lane;
+    const float4* lay = T.flat + lbase;            // layer m at lay[m * TILE]
+    const ChainRec* chr = T.ch + lbase;
+#pragma unroll 1
+    for (int pass = 0; pass < npass; ++pass) {
+        const bool staged = GROUP && pass > 0;   // second group pass
+        double croot = c0;
+        if constexpr (GROUP) {
+            croot = pass ? a.croot_b[task * TILE + lane] : c0;
+            omega = TWOPI / (pass ? gp.per_b : gp.per_a);
+            wvno = omega / croot;
+        }
+        auto put = [&](int node, double vs, double vp, double rh) {
+            if (staged) {
+                double* row = scr_row(scr, node);
+                row[0] = vs; row[TILE] = vp; row[2 * TILE] = rh;
+            } else {
+                dvs[nstride * node] = vs; dvp[nstride * node] = vp; drh[nstride * node] = rh;
+            }
+        };
+        // ---- 1. bottom-up sweep: store e(m+1) and 1/n_m for m = rmax-2 .. 0
+        double e[5];
+        {
+            const float4 L = lay[(long long)(rmax - 1) * TILE];
+            const double aa = L.y, bb = L.z;
+            const D3 w = mk(wvno);
+            const D3 xka = mk(omega / aa), xkb = mk(omega / bb);
+            const D3 gk = mk(2.0 * bb * bb / (omega * omega));
+            D3 h[5];
+            halfspace_d3(w, xka, xkb, gk, (double)L.w, h);
+            for (int q = 0; q < 5; ++q) e[q] = h[q].v;
+        }
+        for (int m = rmax - 2; m >= 0; --m) {
+            const float4 L = lay[(long long)m * TILE];
+            double f[5];
+            const double nrm = layer_step_val(L, wvno, omega, e, f);
+            double* sp = scr + (long long)m * 6 * nslots;
+            for (int q = 0; q < 5; ++q) sp[q * nslots] = e[q];
+            const double inv = fast_rcp(nrm);
+            sp[5 * nslots] = inv;
+            for (int q = 0; q < 5; ++q) e[q] = f[q] * inv;
+        }
+        // ---- 2. top-down sweep with tangents
+        double gv[5] = {1.0, 0.0, 0.0, 0.0, 0.0};
+        double dFdw = 0.0;
+        double acc_vs = 0.0, acc_vp = 0.0, acc_rh = 0.0;   // current node (top of interval)
+        double nxt_vs = 0.0, nxt_vp = 0.0, nxt_rh = 0.0;   // next node (bottom of interval)
+        int cur_node = 0;
+        int gexp = 0;   // g is kept as gv * 2^gexp
+        for (int m = 0; m <= rmax - 2; ++m) {
+            const ChainRec ch = chr[(long long)m * TILE];
+            const int node = ch.node;
+            if (node != cur_node) {
+                // interval cur_node finished: node cur_node is complete
+                put(cur_node, acc_vs, acc_vp, acc_rh);
+                acc_vs = nxt_vs; acc_vp = nxt_vp; acc_rh = nxt_rh;
+                nxt_vs = nxt_vp = nxt_rh = 0.0;
+                cur_node = node;
+            }
+            const float4 L = lay[(long long)m * TILE];
+            CAset<D3> C;
+            layer_ca_d3(L, wvno, omega, C);
+            const double* sp = scr + (long long)m * 6 * nslots;
+            double u[5];
+            for (int q = 0; q < 5; ++q) u[q] = sp[q * nslots];
+            const double inv = sp[5 * nslots];
+            const Contract sc5 = contract(C, u, gv);
+            const double sc = ldexp(inv, gexp);
+            dFdw = fma(sc5.d2, sc, dFdw);
+            const double dFda = sc5.d0 * sc, dFdb = sc5.d1 * sc, dFdr = sc5.drho * sc * fast_rcp((double)L.w);
+            // chain to nodes: a_flat = tmp * ((1-f) vp_i + f vp_i+1), etc.
+            const double tmpm = ch.tmp, rf = (double)ch.rhofac;
+            const double fw = (double)ch.sub * fast_rcp((double)ch.den);
+            acc_vp = fma(dFda * tmpm, 1.0 - fw, acc_vp); nxt_vp = fma(dFda * tmpm, fw, nxt_vp);
+            acc_vs = fma(dFdb * tmpm, 1.0 - fw, acc_vs); nxt_vs = fma(dFdb * tmpm, fw, nxt_vs);
+            acc_rh = fma(dFdr * rf, 1.0 - fw, acc_rh);   nxt_rh = fma(dFdr * rf, fw, nxt_rh);
+            double gn[5];
+            matvec(C, gv, gn);
+            double mx = 0.0;
+            for (int q = 0; q < 5; ++q) { gn[q] *= inv; mx = fmax(mx, fabs(gn[q])); }
+            int ex = 0;
+            if (mx > 0.0) frexp(mx, &ex);
+            for (int q = 0; q < 5; ++q) gv[q] = ldexp(gn[q], -ex);
+            gexp += ex;
+        }
+        // half-space: the remaining contributions go to node nz-1 (together
+        // with the bottom sublayers of interval nz-2 already in nxt_*)
+        {
+            const int m = rmax - 1;
+            const float4 L = lay[(long long)m * TILE];
+            const ChainRec ch = chr[(long long)m * TILE];
+            const double aa = L.y, bb = L.z, rho = L.w;
+            const D3 w = {wvno, 0.0, 0.0, 1.0};
+            const D3 xka = {omega / aa, -omega / (aa * aa), 0.0, 0.0};
+            const D3 xkb = {omega / bb, 0.0, -omega / (bb * bb), 0.0};
+            const double gkv = 2.0 * bb * bb / (omega * omega);
+            const D3 gk = {gkv, 0.0, 2.0 * gkv / bb, 0.0};
+            D3 h[5];
+            halfspace_d3(w, xka, xkb, gk, rho, h);
+            const double sc = ldexp(1.0, gexp);
+            double s0 = 0, s1 = 0, s2 = 0, sr = 0;
+            const int pw[5] = {2, 1, 1, 1, 0};
+            for (int q = 0; q < 5; ++q) {
+                s0 = fma(h[q].d0, gv[q], s0);
+                s1 = fma(h[q].d1, gv[q], s1);
+                s2 = fma(h[q].d2, gv[q], s2);
+                sr = fma((double)pw[q] * h[q].v, gv[q], sr);
+            }
+            dFdw = fma(s2, sc, dFdw);
+            const double tmpm = ch.tmp, rf = (double)ch.rhofac;
+            put(cur_node, acc_vs, acc_vp, acc_rh);
+            nxt_vp = fma(s0 * sc, tmpm, nxt_vp);
+            nxt_vs = fma(s1 * sc, tmpm, nxt_vs);
+            nxt_rh = fma(sr * sc / rho, rf, nxt_rh);
+            if (!staged) {
+                dvs[nstride * (nz - 1)] = nxt_vs;
+                dvp[nstride * (nz - 1)] = nxt_vp;
+                drh[nstride * (nz - 1)] = nxt_rh;
+            }
+        }
+        // ---- 3. dc/dm = -F_m / F_c = (c / (wvno F_wvno)) F_m
+        double scale = croot / (wvno * dFdw);
+        if constexpr (GROUP) scale *= pass ? gp.wb : gp.wa;
+        if (!staged) {
+            for (int i = 0; i < nz; ++i) {
+                dvs[nstride * i] *= scale;
+                dvp[nstride * i] *= scale;
+                drh[nstride * i] *= scale;
+            }
+        } else {
+            for (int i = 0; i < nz - 1; ++i) {
+                const double* row = scr_row(scr, i);
+                dvs[nstride * i] = fma(scale, row[0], dvs[nstride * i]);
+                dvp[nstride * i] = fma(scale, row[TILE], dvp[nstride * i]);
+                drh[nstride * i] = fma(scale, row[2 * TILE], drh[nstride * i]);
+            }
+            dvs[nstride * (nz - 1)] = fma(scale, nxt_vs, dvs[nstride * (nz - 1)]);
+            dvp[nstride * (nz - 1)] = fma(scale, nxt_vp, dvp[nstride * (nz - 1)]);
+            drh[nstride * (nz - 1)] = fma(scale, nxt_rh, drh[nstride * (nz - 1)]);
+        }
+    }   // pass
+}
+
+// The persistent loop: a warp takes (tile, period) tasks off the queue;
+// scr is its lane's column of the warp's scratch block.
+template <bool GROUP>
+__device__ __forceinline__ void adjoint_rayleigh(const AdjArgs& a)
+{
     const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
+    double* scr = a.scratch + (slot / TILE) * a.scr_layers * 6 * TILE + lane;
     for (;;) {
         const long long task = next_task(a.queue);
-        if (task >= T.ntasks) break;
-        const int2 tk = T.tasks[task];
-        const long long s = (long long)tk.x * TILE + lane;
-        const int k = tk.y;
-        if (s >= T.ncols) continue;
-        const ColMeta M = T.meta[s];
-        if (k >= M.K) continue;
-        const double c0 = a.croot[task * TILE + lane];
-        const int nz = M.nz, rmax = M.rmax;
-        double* dvs = a.sen_vs + M.sen_b + T.sen_sk * k;
-        double* dvp = a.sen_vp + M.sen_b + T.sen_sk * k;
-        double* drh = a.sen_rho + M.sen_b + T.sen_sk * k;
-        const long long nstride = M.sen_is;   // node stride in the outputs
-        if (!(c0 > 0.0)) {
-            for (int i = 0; i < nz; ++i) { dvs[nstride * i] = 0.0; dvp[nstride * i] = 0.0; drh[nstride * i] = 0.0; }
-            continue;
-        }
-        double omega = TWOPI / a.periods[M.per_b + k];
-        double wvno = omega / c0;
-        GroupPasses gp{};
-        int npass = 1;
-        if constexpr (GROUP) {
-            gp = group_passes(a.periods[M.per_b + k], c0, a.croot_b[task * TILE + lane]);
-            npass = gp.n;
-        }
-        const long long lbase = T.tile_lbase[tk.x] + lane;
-        const float4* lay = T.flat + lbase;            // layer m at lay[m * TILE]
-        const ChainRec* chr = T.ch + lbase;
-        double* scr = a.scratch + (slot / TILE) * a.scr_layers * 6 * TILE + lane;
-#pragma unroll 1
-        for (int pass = 0; pass < npass; ++pass) {
-            const bool staged = GROUP && pass > 0;   // second group pass
-            double croot = c0;
-            if constexpr (GROUP) {
-                croot = pass ? a.croot_b[task * TILE + lane] : c0;
-                omega = TWOPI / (pass ? gp.per_b : gp.per_a);
-                wvno = omega / croot;
-            }
-            auto put = [&](int node, double vs, double vp, double rh) {
-                if (staged) {
-                    double* row = scr_row(scr, node);
-                    row[0] = vs; row[TILE] = vp; row[2 * TILE] = rh;
-                } else {
-                    dvs[nstride * node] = vs; dvp[nstride * node] = vp; drh[nstride * node] = rh;
-                }
-            };
-            // ---- 1. bottom-up sweep: store e(m+1) and 1/n_m for m = rmax-2 .. 0
-            double e[5];
-            {
-                const float4 L = lay[(long long)(rmax - 1) * TILE];
-                const double aa = L.y, bb = L.z;
-                const D3 w = mk(wvno);
-                const D3 xka = mk(omega / aa), xkb = mk(omega / bb);
-                const D3 gk = mk(2.0 * bb * bb / (omega * omega));
-                D3 h[5];
-                halfspace_d3(w, xka, xkb, gk, (double)L.w, h);
-                for (int q = 0; q < 5; ++q) e[q] = h[q].v;
-            }
-            for (int m = rmax - 2; m >= 0; --m) {
-                const float4 L = lay[(long long)m * TILE];
-                double f[5];
-                const double nrm = layer_step_val(L, wvno, omega, e, f);
-                double* sp = scr + (long long)m * 6 * nslots;
-                for (int q = 0; q < 5; ++q) sp[q * nslots] = e[q];
-                const double inv = fast_rcp(nrm);
-                sp[5 * nslots] = inv;
-                for (int q = 0; q < 5; ++q) e[q] = f[q] * inv;
-            }
-            // ---- 2. top-down sweep with tangents
-            double gv[5] = {1.0, 0.0, 0.0, 0.0, 0.0};
-            double dFdw = 0.0;
-            double acc_vs = 0.0, acc_vp = 0.0, acc_rh = 0.0;   // current node (top of interval)
-            double nxt_vs = 0.0, nxt_vp = 0.0, nxt_rh = 0.0;   // next node (bottom of interval)
-            int cur_node = 0;
-            int gexp = 0;   // g is kept as gv * 2^gexp
-            for (int m = 0; m <= rmax - 2; ++m) {
-                const ChainRec ch = chr[(long long)m * TILE];
-                const int node = ch.node;
-                if (node != cur_node) {
-                    // interval cur_node finished: node cur_node is complete
-                    put(cur_node, acc_vs, acc_vp, acc_rh);
-                    acc_vs = nxt_vs; acc_vp = nxt_vp; acc_rh = nxt_rh;
-                    nxt_vs = nxt_vp = nxt_rh = 0.0;
-                    cur_node = node;
-                }
-                const float4 L = lay[(long long)m * TILE];
-                CAset<D3> C;
-                layer_ca_d3(L, wvno, omega, C);
-                const double* sp = scr + (long long)m * 6 * nslots;
-                double u[5];
-                for (int q = 0; q < 5; ++q) u[q] = sp[q * nslots];
-                const double inv = sp[5 * nslots];
-                const Contract sc5 = contract(C, u, gv);
-                const double sc = ldexp(inv, gexp);
-                dFdw = fma(sc5.d2, sc, dFdw);
-                const double dFda = sc5.d0 * sc, dFdb = sc5.d1 * sc, dFdr = sc5.drho * sc * fast_rcp((double)L.w);
-                // chain to nodes: a_flat = tmp * ((1-f) vp_i + f vp_i+1), etc.
-                const double tmpm = ch.tmp, rf = (double)ch.rhofac;
-                const double fw = (double)ch.sub * fast_rcp((double)ch.den);
-                acc_vp = fma(dFda * tmpm, 1.0 - fw, acc_vp); nxt_vp = fma(dFda * tmpm, fw, nxt_vp);
-                acc_vs = fma(dFdb * tmpm, 1.0 - fw, acc_vs); nxt_vs = fma(dFdb * tmpm, fw, nxt_vs);
-                acc_rh = fma(dFdr * rf, 1.0 - fw, acc_rh);   nxt_rh = fma(dFdr * rf, fw, nxt_rh);
-                double gn[5];
-                matvec(C, gv, gn);
-                double mx = 0.0;
-                for (int q = 0; q < 5; ++q) { gn[q] *= inv; mx = fmax(mx, fabs(gn[q])); }
-                int ex = 0;
-                if (mx > 0.0) frexp(mx, &ex);
-                for (int q = 0; q < 5; ++q) gv[q] = ldexp(gn[q], -ex);
-                gexp += ex;
-            }
-            // half-space: the remaining contributions go to node nz-1 (together
-            // with the bottom sublayers of interval nz-2 already in nxt_*)
-            {
-                const int m = rmax - 1;
-                const float4 L = lay[(long long)m * TILE];
-                const ChainRec ch = chr[(long long)m * TILE];
-                const double aa = L.y, bb = L.z, rho = L.w;
-                const D3 w = {wvno, 0.0, 0.0, 1.0};
-                const D3 xka = {omega / aa, -omega / (aa * aa), 0.0, 0.0};
-                const D3 xkb = {omega / bb, 0.0, -omega / (bb * bb), 0.0};
-                const double gkv = 2.0 * bb * bb / (omega * omega);
-                const D3 gk = {gkv, 0.0, 2.0 * gkv / bb, 0.0};
-                D3 h[5];
-                halfspace_d3(w, xka, xkb, gk, rho, h);
-                const double sc = ldexp(1.0, gexp);
-                double s0 = 0, s1 = 0, s2 = 0, sr = 0;
-                const int pw[5] = {2, 1, 1, 1, 0};
-                for (int q = 0; q < 5; ++q) {
-                    s0 = fma(h[q].d0, gv[q], s0);
-                    s1 = fma(h[q].d1, gv[q], s1);
-                    s2 = fma(h[q].d2, gv[q], s2);
-                    sr = fma((double)pw[q] * h[q].v, gv[q], sr);
-                }
-                dFdw = fma(s2, sc, dFdw);
-                const double tmpm = ch.tmp, rf = (double)ch.rhofac;
-                put(cur_node, acc_vs, acc_vp, acc_rh);
-                nxt_vp = fma(s0 * sc, tmpm, nxt_vp);
-                nxt_vs = fma(s1 * sc, tmpm, nxt_vs);
-                nxt_rh = fma(sr * sc / rho, rf, nxt_rh);
-                if (!staged) {
-                    dvs[nstride * (nz - 1)] = nxt_vs;
-                    dvp[nstride * (nz - 1)] = nxt_vp;
-                    drh[nstride * (nz - 1)] = nxt_rh;
-                }
-            }
-            // ---- 3. dc/dm = -F_m / F_c = (c / (wvno F_wvno)) F_m
-            double scale = croot / (wvno * dFdw);
-            if constexpr (GROUP) scale *= pass ? gp.wb : gp.wa;
-            if (!staged) {
-                for (int i = 0; i < nz; ++i) {
-                    dvs[nstride * i] *= scale;
-                    dvp[nstride * i] *= scale;
-                    drh[nstride * i] *= scale;
-                }
-            } else {
-                for (int i = 0; i < nz - 1; ++i) {
-                    const double* row = scr_row(scr, i);
-                    dvs[nstride * i] = fma(scale, row[0], dvs[nstride * i]);
-                    dvp[nstride * i] = fma(scale, row[TILE], dvp[nstride * i]);
-                    drh[nstride * i] = fma(scale, row[2 * TILE], drh[nstride * i]);
-                }
-                dvs[nstride * (nz - 1)] = fma(scale, nxt_vs, dvs[nstride * (nz - 1)]);
-                dvp[nstride * (nz - 1)] = fma(scale, nxt_vp, dvp[nstride * (nz - 1)]);
-                drh[nstride * (nz - 1)] = fma(scale, nxt_rh, drh[nstride * (nz - 1)]);
-            }
-        }   // pass
+        if (task >= a.T.ntasks) break;
+        adjoint_rayleigh_task<GROUP>(a, task, lane, scr);
     }
 }
 
@@ -644,162 +652,169 @@ __device__ __forceinline__ void love_halfspace_d3(double b, double rho, double w
     h[1] = {ib * ib, -2.0 * ib * ib * ib, 0.0, 0.0};
 }
 
-// The Love adjoint of one task per warp, phase velocity or (GROUP) the
-// group velocity's two passes, staged as in adjoint_rayleigh.
+// The Love adjoint of one (column, period), as adjoint_rayleigh_task: phase
+// velocity or (GROUP) the group velocity's two passes, staged likewise.
 template <bool GROUP>
-__device__ __forceinline__ void adjoint_love(const AdjArgs& a)
+__device__ __forceinline__ void adjoint_love_task(const AdjArgs& a, long long task, int lane, double* scr)
 {
     const Tables& T = a.T;
     constexpr long long nslots = TILE;   // scratch per warp [layer][3 of 6][lane]
+    const int2 tk = T.tasks[task];
+    const long long s = (long long)tk.x * TILE + lane;
+    const int k = tk.y;
+    if (s >= T.ncols) return;
+    const ColMeta M = T.meta[s];
+    if (k >= M.K) return;
+    const double c0 = a.croot[task * TILE + lane];
+    const int nz = M.nz, rmax = M.rmax;
+    double* dvs = a.sen_vs + M.sen_b + T.sen_sk * k;
+    double* dvp = a.sen_vp + M.sen_b + T.sen_sk * k;
+    double* drh = a.sen_rho + M.sen_b + T.sen_sk * k;
+    const long long nstride = M.sen_is;
+    for (int i = 0; i < nz; ++i) dvp[nstride * i] = 0.0;   // Love waves do not see Vp
+    if (!(c0 > 0.0)) {
+        for (int i = 0; i < nz; ++i) { dvs[nstride * i] = 0.0; drh[nstride * i] = 0.0; }
+        return;
+    }
+    double omega = TWOPI / a.periods[M.per_b + k];
+    double wvno = omega / c0;
+    GroupPasses gp{};
+    int npass = 1;
+    if constexpr (GROUP) {
+        gp = group_passes(a.periods[M.per_b + k], c0, a.croot_b[task * TILE + lane]);
+        npass = gp.n;
+    }
+    const long long lbase = T.tile_lbase[tk.x] + lane;
+    const float4* lay = T.flat + lbase;            // layer m at lay[m * TILE]: (d, a, b, rho)
+    const ChainRec* chr = T.ch + lbase;
+#pragma unroll 1
+    for (int pass = 0; pass < npass; ++pass) {
+        const bool staged = GROUP && pass > 0;   // second group pass
+        double croot = c0;
+        if constexpr (GROUP) {
+            croot = pass ? a.croot_b[task * TILE + lane] : c0;
+            omega = TWOPI / (pass ? gp.per_b : gp.per_a);
+            wvno = omega / croot;
+        }
+        auto put = [&](int node, double vs, double rh) {
+            if (staged) {
+                double* row = scr_row(scr, node);
+                row[3 * TILE] = vs; row[4 * TILE] = rh;
+            } else {
+                dvs[nstride * node] = vs; drh[nstride * node] = rh;
+            }
+        };
+        // ---- 1. bottom-up sweep: store e(m+1) and 1/n_m for m = rmax-2 .. 0
+        double e[2];
+        {
+            const float4 L = lay[(long long)(rmax - 1) * TILE];
+            D3 h[2];
+            love_halfspace_d3((double)L.z, (double)L.w, wvno, omega, h);
+            e[0] = h[0].v; e[1] = h[1].v;
+        }
+        for (int m = rmax - 2; m >= 0; --m) {
+            const float4 L = lay[(long long)m * TILE];
+            double f[2];
+            const double nrm = love_step_val((double)L.z, (double)L.w, (double)L.x, wvno, omega, e, f);
+            double* sp = scr + (long long)m * 6 * nslots;
+            sp[0] = e[0]; sp[nslots] = e[1];
+            const double inv = fast_rcp(nrm);
+            sp[2 * nslots] = inv;
+            e[0] = f[0] * inv; e[1] = f[1] * inv;
+        }
+        // ---- 2. top-down sweep with tangents
+        double gv[2] = {1.0, 0.0};
+        int gexp = 0;                 // g is kept as gv * 2^gexp
+        double dFdw = 0.0;
+        double acc_vs = 0.0, acc_rh = 0.0, nxt_vs = 0.0, nxt_rh = 0.0;
+        int cur_node = 0;
+        for (int m = 0; m <= rmax - 2; ++m) {
+            const ChainRec ch = chr[(long long)m * TILE];
+            const int node = ch.node;
+            if (node != cur_node) {
+                put(cur_node, acc_vs, acc_rh);
+                acc_vs = nxt_vs; acc_rh = nxt_rh;
+                nxt_vs = nxt_rh = 0.0;
+                cur_node = node;
+            }
+            const float4 L = lay[(long long)m * TILE];
+            Love3 C;
+            love_layer_d3((double)L.z, (double)L.w, (double)L.x, wvno, omega, C);
+            const double* sp = scr + (long long)m * 6 * nslots;
+            const double u0 = sp[0], u1 = sp[nslots], inv = sp[2 * nslots];
+            const double sc = ldexp(inv, gexp);
+            // u . dM . g,  M = [[c, m01], [m10, c]]
+            auto contract = [&](double dc, double d01, double d10) {
+                return u0 * (dc * gv[0] + d01 * gv[1]) + u1 * (d10 * gv[0] + dc * gv[1]);
+            };
+            const double dFdb = contract(C.cosq.d0, C.m01.d0, C.m10.d0) * sc;
+            const double dFdr = contract(C.cosq.d1, C.m01.d1, C.m10.d1) * sc;
+            dFdw = fma(contract(C.cosq.d2, C.m01.d2, C.m10.d2), sc, dFdw);
+            // chain to nodes: b_flat = tmp ((1-f) vs_i + f vs_i+1), rho likewise
+            const double tmpm = ch.tmp, rf = (double)ch.rhofac;
+            const double fw = (double)ch.sub * fast_rcp((double)ch.den);
+            acc_vs = fma(dFdb * tmpm, 1.0 - fw, acc_vs); nxt_vs = fma(dFdb * tmpm, fw, nxt_vs);
+            acc_rh = fma(dFdr * rf, 1.0 - fw, acc_rh);   nxt_rh = fma(dFdr * rf, fw, nxt_rh);
+            // g <- M g / n, rescaled by a power of two
+            double g0 = (C.cosq.v * gv[0] + C.m01.v * gv[1]) * inv;
+            double g1 = (C.m10.v * gv[0] + C.cosq.v * gv[1]) * inv;
+            const double mx = fmax(fabs(g0), fabs(g1));
+            int ex = 0;
+            if (mx > 0.0) frexp(mx, &ex);
+            gv[0] = ldexp(g0, -ex); gv[1] = ldexp(g1, -ex);
+            gexp += ex;
+        }
+        // half-space: its contributions go to node nz-1
+        {
+            const int m = rmax - 1;
+            const float4 L = lay[(long long)m * TILE];
+            const ChainRec ch = chr[(long long)m * TILE];
+            D3 h[2];
+            love_halfspace_d3((double)L.z, (double)L.w, wvno, omega, h);
+            const double sc = ldexp(1.0, gexp);
+            const double s0 = (h[0].d0 * gv[0] + h[1].d0 * gv[1]) * sc;
+            const double s1 = (h[0].d1 * gv[0] + h[1].d1 * gv[1]) * sc;
+            dFdw = fma(h[0].d2 * gv[0] + h[1].d2 * gv[1], sc, dFdw);
+            const double tmpm = ch.tmp, rf = (double)ch.rhofac;
+            put(cur_node, acc_vs, acc_rh);
+            nxt_vs = fma(s0, tmpm, nxt_vs);
+            nxt_rh = fma(s1, rf, nxt_rh);
+            if (!staged) {
+                dvs[nstride * (nz - 1)] = nxt_vs;
+                drh[nstride * (nz - 1)] = nxt_rh;
+            }
+        }
+        // ---- 3. dc/dm = -F_m / F_c = (c / (wvno F_wvno)) F_m
+        double scale = croot / (wvno * dFdw);
+        if constexpr (GROUP) scale *= pass ? gp.wb : gp.wa;
+        if (!staged) {
+            for (int i = 0; i < nz; ++i) {
+                dvs[nstride * i] *= scale;
+                drh[nstride * i] *= scale;
+            }
+        } else {
+            for (int i = 0; i < nz - 1; ++i) {
+                const double* row = scr_row(scr, i);
+                dvs[nstride * i] = fma(scale, row[3 * TILE], dvs[nstride * i]);
+                drh[nstride * i] = fma(scale, row[4 * TILE], drh[nstride * i]);
+            }
+            dvs[nstride * (nz - 1)] = fma(scale, nxt_vs, dvs[nstride * (nz - 1)]);
+            drh[nstride * (nz - 1)] = fma(scale, nxt_rh, drh[nstride * (nz - 1)]);
+        }
+    }   // pass
+}
+
+// The persistent loop of the Love adjoint (as adjoint_rayleigh).
+template <bool GROUP>
+__device__ __forceinline__ void adjoint_love(const AdjArgs& a)
+{
     const long long slot = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x & 31;
+    double* scr = a.scratch + (slot / TILE) * a.scr_layers * 6 * TILE + lane;
     for (;;) {
         const long long task = next_task(a.queue);
-        if (task >= T.ntasks) break;
-        const int2 tk = T.tasks[task];
-        const long long s = (long long)tk.x * TILE + lane;
-        const int k = tk.y;
-        if (s >= T.ncols) continue;
-        const ColMeta M = T.meta[s];
-        if (k >= M.K) continue;
-        const double c0 = a.croot[task * TILE + lane];
-        const int nz = M.nz, rmax = M.rmax;
-        double* dvs = a.sen_vs + M.sen_b + T.sen_sk * k;
-        double* dvp = a.sen_vp + M.sen_b + T.sen_sk * k;
-        double* drh = a.sen_rho + M.sen_b + T.sen_sk * k;
-        const long long nstride = M.sen_is;
-        for (int i = 0; i < nz; ++i) dvp[nstride * i] = 0.0;   // Love waves do not see Vp
-        if (!(c0 > 0.0)) {
-            for (int i = 0; i < nz; ++i) { dvs[nstride * i] = 0.0; drh[nstride * i] = 0.0; }
-            continue;
-        }
-        double omega = TWOPI / a.periods[M.per_b + k];
-        double wvno = omega / c0;
-        GroupPasses gp{};
-        int npass = 1;
-        if constexpr (GROUP) {
-            gp = group_passes(a.periods[M.per_b + k], c0, a.croot_b[task * TILE + lane]);
-            npass = gp.n;
-        }
-        const long long lbase = T.tile_lbase[tk.x] + lane;
-        const float4* lay = T.flat + lbase;            // layer m at lay[m * TILE]: (d, a, b, rho)
-        const ChainRec* chr = T.ch + lbase;
-        double* scr = a.scratch + (slot / TILE) * a.scr_layers * 6 * TILE + lane;
-#pragma unroll 1
-        for (int pass = 0; pass < npass; ++pass) {
-            const bool staged = GROUP && pass > 0;   // second group pass
-            double croot = c0;
-            if constexpr (GROUP) {
-                croot = pass ? a.croot_b[task * TILE + lane] : c0;
-                omega = TWOPI / (pass ? gp.per_b : gp.per_a);
-                wvno = omega / croot;
-            }
-            auto put = [&](int node, double vs, double rh) {
-                if (staged) {
-                    double* row = scr_row(scr, node);
-                    row[3 * TILE] = vs; row[4 * TILE] = rh;
-                } else {
-                    dvs[nstride * node] = vs; drh[nstride * node] = rh;
-                }
-            };
-            // ---- 1. bottom-up sweep: store e(m+1) and 1/n_m for m = rmax-2 .. 0
-            double e[2];
-            {
-                const float4 L = lay[(long long)(rmax - 1) * TILE];
-                D3 h[2];
-                love_halfspace_d3((double)L.z, (double)L.w, wvno, omega, h);
-                e[0] = h[0].v; e[1] = h[1].v;
-            }
-            for (int m = rmax - 2; m >= 0; --m) {
-                const float4 L = lay[(long long)m * TILE];
-                double f[2];
-                const double nrm = love_step_val((double)L.z, (double)L.w, (double)L.x, wvno, omega, e, f);
-                double* sp = scr + (long long)m * 6 * nslots;
-                sp[0] = e[0]; sp[nslots] = e[1];
-                const double inv = fast_rcp(nrm);
-                sp[2 * nslots] = inv;
-                e[0] = f[0] * inv; e[1] = f[1] * inv;
-            }
-            // ---- 2. top-down sweep with tangents
-            double gv[2] = {1.0, 0.0};
-            int gexp = 0;                 // g is kept as gv * 2^gexp
-            double dFdw = 0.0;
-            double acc_vs = 0.0, acc_rh = 0.0, nxt_vs = 0.0, nxt_rh = 0.0;
-            int cur_node = 0;
-            for (int m = 0; m <= rmax - 2; ++m) {
-                const ChainRec ch = chr[(long long)m * TILE];
-                const int node = ch.node;
-                if (node != cur_node) {
-                    put(cur_node, acc_vs, acc_rh);
-                    acc_vs = nxt_vs; acc_rh = nxt_rh;
-                    nxt_vs = nxt_rh = 0.0;
-                    cur_node = node;
-                }
-                const float4 L = lay[(long long)m * TILE];
-                Love3 C;
-                love_layer_d3((double)L.z, (double)L.w, (double)L.x, wvno, omega, C);
-                const double* sp = scr + (long long)m * 6 * nslots;
-                const double u0 = sp[0], u1 = sp[nslots], inv = sp[2 * nslots];
-                const double sc = ldexp(inv, gexp);
-                // u . dM . g,  M = [[c, m01], [m10, c]]
-                auto contract = [&](double dc, double d01, double d10) {
-                    return u0 * (dc * gv[0] + d01 * gv[1]) + u1 * (d10 * gv[0] + dc * gv[1]);
-                };
-                const double dFdb = contract(C.cosq.d0, C.m01.d0, C.m10.d0) * sc;
-                const double dFdr = contract(C.cosq.d1, C.m01.d1, C.m10.d1) * sc;
-                dFdw = fma(contract(C.cosq.d2, C.m01.d2, C.m10.d2), sc, dFdw);
-                // chain to nodes: b_flat = tmp ((1-f) vs_i + f vs_i+1), rho likewise
-                const double tmpm = ch.tmp, rf = (double)ch.rhofac;
-                const double fw = (double)ch.sub * fast_rcp((double)ch.den);
-                acc_vs = fma(dFdb * tmpm, 1.0 - fw, acc_vs); nxt_vs = fma(dFdb * tmpm, fw, nxt_vs);
-                acc_rh = fma(dFdr * rf, 1.0 - fw, acc_rh);   nxt_rh = fma(dFdr * rf, fw, nxt_rh);
-                // g <- M g / n, rescaled by a power of two
-                double g0 = (C.cosq.v * gv[0] + C.m01.v * gv[1]) * inv;
-                double g1 = (C.m10.v * gv[0] + C.cosq.v * gv[1]) * inv;
-                const double mx = fmax(fabs(g0), fabs(g1));
-                int ex = 0;
-                if (mx > 0.0) frexp(mx, &ex);
-                gv[0] = ldexp(g0, -ex); gv[1] = ldexp(g1, -ex);
-                gexp += ex;
-            }
-            // half-space: its contributions go to node nz-1
-            {
-                const int m = rmax - 1;
-                const float4 L = lay[(long long)m * TILE];
-                const ChainRec ch = chr[(long long)m * TILE];
-                D3 h[2];
-                love_halfspace_d3((double)L.z, (double)L.w, wvno, omega, h);
-                const double sc = ldexp(1.0, gexp);
-                const double s0 = (h[0].d0 * gv[0] + h[1].d0 * gv[1]) * sc;
-                const double s1 = (h[0].d1 * gv[0] + h[1].d1 * gv[1]) * sc;
-                dFdw = fma(h[0].d2 * gv[0] + h[1].d2 * gv[1], sc, dFdw);
-                const double tmpm = ch.tmp, rf = (double)ch.rhofac;
-                put(cur_node, acc_vs, acc_rh);
-                nxt_vs = fma(s0, tmpm, nxt_vs);
-                nxt_rh = fma(s1, rf, nxt_rh);
-                if (!staged) {
-                    dvs[nstride * (nz - 1)] = nxt_vs;
-                    drh[nstride * (nz - 1)] = nxt_rh;
-                }
-            }
-            // ---- 3. dc/dm = -F_m / F_c = (c / (wvno F_wvno)) F_m
-            double scale = croot / (wvno * dFdw);
-            if constexpr (GROUP) scale *= pass ? gp.wb : gp.wa;
-            if (!staged) {
-                for (int i = 0; i < nz; ++i) {
-                    dvs[nstride * i] *= scale;
-                    drh[nstride * i] *= scale;
-                }
-            } else {
-                for (int i = 0; i < nz - 1; ++i) {
-                    const double* row = scr_row(scr, i);
-                    dvs[nstride * i] = fma(scale, row[3 * TILE], dvs[nstride * i]);
-                    drh[nstride * i] = fma(scale, row[4 * TILE], drh[nstride * i]);
-                }
-                dvs[nstride * (nz - 1)] = fma(scale, nxt_vs, dvs[nstride * (nz - 1)]);
-                drh[nstride * (nz - 1)] = fma(scale, nxt_rh, drh[nstride * (nz - 1)]);
-            }
-        }   // pass
+        if (task >= a.T.ntasks) break;
+        adjoint_love_task<GROUP>(a, task, lane, scr);
     }
 }
 

@@ -56,3 +56,31 @@ def root_batch(node_off, depz, vs, per_off, periods, minthk, scan32=True, ifunc=
                               int(scan32), int(ifunc), int(bool(group)), P(pv, f64),
                               P(st, ctypes.c_int), ctypes.byref(ev))
     return rc, pv, st, ev.value
+
+
+def adjoint_batch(node_off, depz, vs, per_off, periods, minthk, ifunc=2, group=False,
+                  drop_every=0):
+    """Adjoint form of a ragged batch by the device code built for the host:
+    rc, pv, status, (sen_vs, sen_vp, sen_rho) in the batch layout, sen_off,
+    and the mask of (column, period) entries whose root at t1b was set to 0
+    (drop_every > 0, group only: the planted group fallback)."""
+    P = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))  # noqa: E731
+    node_off = np.ascontiguousarray(node_off, np.int64)
+    per_off = np.ascontiguousarray(per_off, np.int64)
+    nz = np.diff(node_off)
+    K = np.diff(per_off)
+    sen_off = np.concatenate([[0], np.cumsum(K * nz)]).astype(np.int64)
+    npv = max(int(per_off[-1]), 1)
+    pv = np.zeros(npv)
+    st = np.zeros(max(node_off.size - 1, 1), np.int32)
+    sen = [np.zeros(max(int(sen_off[-1]), 1)) for _ in range(3)]
+    dropped = np.zeros(npv, np.uint8)
+    i64, f32, f64 = ctypes.c_longlong, ctypes.c_float, ctypes.c_double
+    rc = lib().emu_adjoint_batch(i64(node_off.size - 1), P(node_off, i64),
+                                 P(np.ascontiguousarray(depz, np.float32), f32),
+                                 P(np.ascontiguousarray(vs, np.float32), f32), P(per_off, i64),
+                                 P(np.ascontiguousarray(periods, np.float64), f64), f32(minthk),
+                                 int(ifunc), int(bool(group)), int(drop_every), P(pv, f64),
+                                 P(st, ctypes.c_int), P(sen_off, i64), P(sen[0], f64),
+                                 P(sen[1], f64), P(sen[2], f64), P(dropped, ctypes.c_ubyte))
+    return rc, pv, st, sen, sen_off, dropped.astype(bool)

@@ -1,5 +1,6 @@
 // TEST INFRASTRUCTURE ONLY: the table build (k_prep.cu), the root search
-// (root_kernel, k_plain.cu) and the Gc/Gs sweep (k_ti.cu) of the library
+// (root_kernel, k_plain.cu), the adjoint sweeps (k_adjoint.cu) and the
+// Gc/Gs sweep (k_ti.cu) of the library
 // compiled as host code and driven in the order the library drives them
 // (build_tables, run_tables in csrc/capi.cu: columns sorted by (refined
 // layers, periods), 32-column tiles, one task per (tile, period), one lane
@@ -13,6 +14,7 @@ namespace dk { alignas(16) unsigned char smem_raw[1 << 16]; }
 #include "../../dazi_current_release_b200/csrc/k_prep.cu"
 #include "../../dazi_current_release_b200/csrc/k_plain.cu"
 #include "../../dazi_current_release_b200/csrc/k_ti.cu"
+#include "../../dazi_current_release_b200/csrc/k_adjoint.cu"
 using namespace dk;
 
 namespace {
@@ -140,4 +142,64 @@ extern "C" int emu_ti_batch(long long ncols, const long long* node_off, const fl
     for (long long task = 0; task < H.T.ntasks; ++task)
         for (int lane = 0; lane < TILE; ++lane) ti_task(a, task, lane, scratch.data() + lane);
     return errflag ? -2 : 0;
+}
+
+// Adjoint form of a ragged batch (the root search with FP64 roots, then the
+// adjoint sweep of every (column, period), as run_tables drives them):
+// pv, status and the three kernels in the dazi_dk_batch layout (sen_off).
+// ifunc 1 (Love) / 2 (Rayleigh); group selects group velocity.  A test may
+// plant the group fallback (the second root search found no root): with
+// drop_every > 0 every drop_every-th root at t1b is set to 0 before the
+// sweep, and dropped[pv index] = 1 marks those (column, period) entries.
+extern "C" int emu_adjoint_batch(long long ncols, const long long* node_off, const float* depz,
+                                 const float* vs, const long long* per_off, const double* periods,
+                                 float minthk, int ifunc, int group, int drop_every, double* pv,
+                                 int* status, const long long* sen_off, double* svs, double* svp,
+                                 double* srh, unsigned char* dropped)
+{
+    if (ifunc != 1 && ifunc != 2) return -2;
+    const ColSrc src = ragged_src(node_off, depz, vs, per_off, minthk, ifunc);
+    HostTables H;
+    PrepOut po{sen_off, nullptr, nullptr};
+    if (!build_host(src, ncols, po, H)) return -1;
+    const size_t nroots = (size_t)H.T.ntasks * TILE;
+    std::vector<double> croot(nroots, 0.0), crootb(nroots, 0.0);
+    unsigned long long counters[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    RootArgs a;
+    a.T = H.T; a.periods = periods; a.tol = 1.0e-6; a.pv = pv; a.croot = croot.data();
+    a.croot_b = group ? crootb.data() : nullptr;
+    a.status = status; a.nevals = counters; a.scan32 = 0;
+    blockDim.x = 128;
+    for (long long s = 0; s < ncols; ++s) {
+        blockIdx.x = (unsigned)(s / 128);
+        threadIdx.x = (unsigned)(s % 128);
+        if (ifunc == 1 && group) root_kernel<128, 0, 1, true>(a);
+        else if (ifunc == 1) root_kernel<128, 0, 1, false>(a);
+        else if (group) root_kernel<128, 0, 2, true>(a);
+        else root_kernel<128, 0>(a);
+    }
+    for (long long task = 0; task < H.T.ntasks; ++task)
+        for (int lane = 0; lane < TILE; ++lane) {
+            const size_t i = (size_t)task * TILE + lane;
+            const long long s = (long long)H.T.tasks[task].x * TILE + lane;
+            const int k = H.T.tasks[task].y;
+            if (!group || drop_every <= 0 || i % (size_t)drop_every != 0) continue;
+            if (s >= H.T.ncols || k >= H.T.meta[s].K || !(croot[i] > 0.0)) continue;
+            crootb[i] = 0.0;
+            dropped[H.T.meta[s].pv_b + H.T.pv_sk * k] = 1;
+        }
+    std::vector<double> scratch((size_t)H.maxr * 6 * TILE);
+    AdjArgs j;
+    j.T = H.T; j.periods = periods; j.croot = croot.data(); j.sen_vs = svs; j.sen_vp = svp;
+    j.sen_rho = srh; j.scratch = scratch.data(); j.scr_layers = H.maxr > 1 ? H.maxr - 1 : 1;
+    j.queue = nullptr; j.croot_b = group ? crootb.data() : nullptr;
+    for (long long task = 0; task < H.T.ntasks; ++task)
+        for (int lane = 0; lane < TILE; ++lane) {
+            double* scr = scratch.data() + lane;
+            if (ifunc == 1 && group) adjoint_love_task<true>(j, task, lane, scr);
+            else if (ifunc == 1) adjoint_love_task<false>(j, task, lane, scr);
+            else if (group) adjoint_rayleigh_task<true>(j, task, lane, scr);
+            else adjoint_rayleigh_task<false>(j, task, lane, scr);
+        }
+    return 0;
 }
