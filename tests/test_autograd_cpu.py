@@ -1,13 +1,18 @@
 """Host-side bookkeeping of the torch binding (no device needed): the maps
 from kernel entries to (period, node) and from Lsen entries to (period,
 interval), the vector-Jacobian product and the azimuthal epilogue, against
-explicit loops over the batch layout."""
+explicit loops over the batch layout; the autograd functions with the
+library call replaced by fixed kernels."""
 import numpy as np
 import torch
 
 from dazi_current_release_b200 import synthetic as S
+import pytest
+
+from dazi_current_release_b200 import _lib
 from dazi_current_release_b200.autograd import (ColumnBatch, azimuthal_phase_velocity,
-                                                brocher_derivatives)
+                                                brocher_derivatives, dispersion_velocity,
+                                                phase_velocity)
 
 
 def _batch():
@@ -70,3 +75,61 @@ def test_brocher_derivatives_match_fd():
     (p1, r1), (p0, r0) = f(vs + h), f(vs - h)
     torch.testing.assert_close(dvp, (p1 - p0) / (2 * h), rtol=1e-7, atol=1e-8)
     torch.testing.assert_close(drho, (r1 - r0) / (2 * h), rtol=1e-7, atol=1e-8)
+
+
+def _stub_run(cb, calls):
+    """Replaces the library call of cb by fixed kernels, recording flags."""
+    rng = np.random.default_rng(2)
+    sen = [torch.as_tensor(rng.standard_normal(cb.nsen)) for _ in range(3)]
+    pv = torch.as_tensor(rng.uniform(2.0, 4.0, cb.nper))
+
+    def run(vs, vp=None, rho=None, lsen=True, flags=0):
+        calls.append((lsen, flags))
+        ls = torch.zeros(cb.nls, dtype=torch.float32) if lsen else None
+        return pv.clone(), [t.clone() for t in sen], ls, torch.zeros(cb.ncols, dtype=torch.int32)
+
+    cb.run = run
+    return pv, sen
+
+
+@pytest.mark.parametrize("iwave,igr,flags", [(2, 0, 0), (1, 0, _lib.FORM_LOVE),
+                                             (2, 1, _lib.FORM_GROUP),
+                                             (1, 3, _lib.FORM_LOVE | _lib.FORM_GROUP)])
+def test_dispersion_velocity_flags_and_gradient(iwave, igr, flags):
+    """iwave/igr become the library's form flags (no Lsen_Gsc with them),
+    and the gradient is the VJP of the returned kernels: the total Vs
+    derivative through the Brocher relations, or one partial per input."""
+    b, cb = _batch()
+    calls = []
+    pv, sen = _stub_run(cb, calls)
+    rng = np.random.default_rng(3)
+    w = torch.as_tensor(rng.standard_normal(cb.nper))
+    vs = torch.as_tensor(np.asarray(b.vs, np.float32)).requires_grad_(True)
+    c, status = dispersion_velocity(vs, cb, iwave=iwave, igr=igr)
+    assert calls == [(flags == 0, flags)]
+    torch.testing.assert_close(c, pv)
+    (c * w).sum().backward()
+    dvp, drho = brocher_derivatives(vs.detach())
+    k_tot = sen[0] + dvp[cb._sen_node] * sen[1] + drho[cb._sen_node] * sen[2]
+    torch.testing.assert_close(vs.grad.double(), cb.vjp(w, k_tot).to(torch.float32).double())
+    # explicit Vp and rho: one partial kernel each
+    vp = (1.75 * vs.detach()).requires_grad_(True)
+    rho = torch.full_like(vp, 2.7).requires_grad_(True)
+    vs.grad = None
+    c, _ = dispersion_velocity(vs, cb, vp=vp, rho=rho, iwave=iwave, igr=igr)
+    (c * w).sum().backward()
+    for x, k in ((vs, sen[0]), (vp, sen[1]), (rho, sen[2])):
+        torch.testing.assert_close(x.grad, cb.vjp(w, k).to(torch.float32))
+
+
+def test_phase_velocity_keeps_lsen_and_rejects_bad_arguments():
+    b, cb = _batch()
+    calls = []
+    _stub_run(cb, calls)
+    vs = torch.as_tensor(np.asarray(b.vs, np.float32))
+    c0, ls, status = phase_velocity(vs, cb)
+    assert calls == [(True, 0)] and ls.numel() == cb.nls
+    with pytest.raises(ValueError):
+        dispersion_velocity(vs, cb, iwave=3)
+    with pytest.raises(ValueError):
+        dispersion_velocity(vs, cb, vp=vs)
