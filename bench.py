@@ -87,7 +87,9 @@ def dist_setup(args):
         import torch
         import torch.distributed as dist
         from datetime import timedelta
-        torch.cuda.set_device(local)
+        if args.impl == "ours":
+            torch.cuda.set_device(local)
+        # the reference arm runs on the host cores: no device, gloo
         backend = "nccl" if args.impl == "ours" else "gloo"
         dist.init_process_group(backend=backend, timeout=timedelta(seconds=300))
     return ws, rank, local
