@@ -47,8 +47,11 @@ class BatchResult(dict):
 def depthkernel_batch(node_off, depz, vs, per_off, periods, minthk, *, vp=None, rho=None,
                       form=_lib.FORM_ADJOINT, kernels=True, lsen=True) -> BatchResult:
     """Run the stage on a ragged batch through the host C-ABI entry
-    dazi_dk_batch.  Raises DaziError for errors; status (per column) holds
-    the first period without a root (0 when all have one)."""
+    dazi_dk_batch.  form: FORM_PLAIN or FORM_ADJOINT, optionally OR-ed with
+    FORM_LOVE / FORM_GROUP (then lsen=False: Lsen_Gsc is a Rayleigh phase
+    kernel) or, for Rayleigh phase velocity, FORM_SCAN_FP32.  Raises
+    DaziError for errors; status (per column) holds the first period without
+    a root (0 when all have one)."""
     L = _lib.load()
     node_off = np.ascontiguousarray(node_off, np.int64)
     per_off = np.ascontiguousarray(per_off, np.int64)
