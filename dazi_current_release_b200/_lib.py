@@ -88,7 +88,9 @@ def load(build_if_missing: bool = True):
     L.dazi_dk_fused_dev.argtypes = [_int, _int, _int, vp_, vp_, vp_, vp_, vp_, vp_, vp_, vp_, _int,
                                     vp_, vp_, ctypes.c_float, _int, _int, _int, vp_, vp_]
     L.dazi_dk_fused_dev.restype = _int
-    L.dazi_dk_iso_noalloc_dev.argtypes = L.dazi_dk_iso_dev.argtypes
+    # dazi_dk_iso_dev's list without `form` (the entry runs the plain form only)
+    L.dazi_dk_iso_noalloc_dev.argtypes = [_int, _int, _int, vp_, vp_, vp_, vp_, vp_, vp_, vp_, _int,
+                                          vp_, vp_, ctypes.c_float, _int, _int, vp_, vp_]
     L.dazi_dk_iso_noalloc_dev.restype = _int
     i64p = ctypes.POINTER(ctypes.c_longlong)
     ll = ctypes.c_longlong

@@ -19,7 +19,7 @@ struct FdArgs {
     double* sen_vp;
     double* sen_rho;
     int* status;         // (ncol) first failing period (1-based) or 0
-    float* cscratch;     // [columns in launch][1 + 6 nz][K]
+    float* cscratch;     // [columns in launch][fd_model_count(nz, sen_vs != nullptr)][K]
     unsigned long long* nevals;  // secular evaluations (accumulated), or nullptr
     float dln;
     double tol;
@@ -171,6 +171,10 @@ template <int MINB> __global__ void adjoint_love_group_kernel(AdjArgs a);   // M
 template <int MINB> __global__ void ti_kernel(TiArgs a);          // MINB in {2, 3, 4, 6, 8}
 
 __global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);
+// Models one column of the finite-difference kernel solves: the base model
+// and, when kernels are requested, 6 perturbed models per node.  Its FP32
+// phase velocities take fd_model_count * K scratch floats.
+__host__ __device__ inline int fd_model_count(int nz, bool kernels) { return kernels ? 1 + 6 * nz : 1; }
 // IFUNC 1 (Love) / 2 (Rayleigh), GROUP: all four combinations.
 template <int IFUNC, bool GROUP> __global__ void fd_column_kernel(FdArgs a);
 size_t fd_smem_bytes();

@@ -20,6 +20,13 @@
 // The first call on a device looks up the arrays' device addresses there
 // (cudaGetSymbolAddress, which also loads the module on that device); make
 // that first call before any stream capture.
+//
+// Each call waits on `stream` twice: it reads the depth grid and periods
+// back to validate them, then the refined layer count of the grid.  So it
+// returns only after the work queued on `stream` before it has finished and
+// the geometry is built; the finite-difference launches themselves are
+// queued and not waited for.  With sen_* NULL only the base model of each
+// column runs (phase velocities alone).
 #include <cuda_runtime.h>
 #include <cmath>
 #include <cstdio>
@@ -62,6 +69,15 @@ extern "C" int dazi_dk_iso_noalloc_dev(int nx, int ny, int nz, const float* vel,
                                        int col_start, int col_count, int* status, void* stream)
 {
     using namespace dk;
+    // An error left pending by the caller's earlier work is reported as
+    // such and left pending, rather than being taken for one of ours.
+    const cudaError_t pending = cudaPeekAtLastError();
+    if (pending != cudaSuccess) {
+        char m[200];
+        snprintf(m, sizeof m, "a CUDA error was already pending before this call: %s",
+                 cudaGetErrorString(pending));
+        return fail(DAZI_ERR_CUDA, m);
+    }
     if (!vel || !pvRc || !tRc || !depz) return fail(DAZI_ERR_BADARG, "null argument");
     if ((sen_vsRc == nullptr) != (sen_vpRc == nullptr) || (sen_vsRc == nullptr) != (sen_rhoRc == nullptr))
         return fail(DAZI_ERR_BADARG, "sen_* must be all set or all NULL");
@@ -74,8 +90,10 @@ extern "C" int dazi_dk_iso_noalloc_dev(int nx, int ny, int nz, const float* vel,
     if (col_start < 1 || col_count < 0 || (long long)col_start - 1 + col_count > ncol)
         return fail(DAZI_ERR_BADARG, "column range outside the grid");
     if (!(minthk > 0.f) || !std::isfinite(minthk)) return fail(DAZI_ERR_BADARG, "minthk must be > 0");
-    // one column's 1 + 6 nz models must fit the static scratch at least once
-    const size_t per_col = (size_t)(1 + 6 * nz) * (size_t)kmaxRc;
+    // one column's models (1 + 6 nz with kernels, 1 without) must fit the
+    // static scratch at least once
+    const int nmod = fd_model_count(nz, sen_vsRc != nullptr);
+    const size_t per_col = (size_t)nmod * (size_t)kmaxRc;
     if (per_col > kNoAllocFloats) {
         char m[160];
         snprintf(m, sizeof m, "one column needs %zu scratch floats; the static array holds %zu",
@@ -123,7 +141,6 @@ extern "C" int dazi_dk_iso_noalloc_dev(int nx, int ny, int nz, const float* vel,
     }
     if (rmax <= 0) return fail(DAZI_ERR_LIMITS, "refined layer count exceeds 200");
     const long long tile = (long long)(kNoAllocFloats / per_col);
-    const int nmod = 1 + 6 * nz;
     int threads = ((nmod + 31) / 32) * 32;
     if (threads > 256) threads = 256;
     for (long long c0 = 0; c0 < col_count; c0 += tile) {

@@ -108,7 +108,7 @@ struct FdColumn {
     long long pv_b, pv_sk;            // pv index = pv_b + pv_sk * k
     long long sen_b, sen_sk, sen_is;  // kernel index = sen_b + sen_sk * k + sen_is * i
     long long status_i;
-    float* cbuf;                      // [1 + 6 nz][K] FP32 phase velocities
+    float* cbuf;                      // [fd_model_count][K] FP32 phase velocities
 };
 
 // Body shared by the grid and ragged kernels.  Node values and periods are
@@ -118,7 +118,7 @@ __device__ void fd_column_body(const FdColumn& C, FdSmem& S, const FdArgs& a)
 {
     const Geometry* g = C.g;
     const int nz = C.nz, K = C.K, rmax = g->rmax;
-    const int nmod = 1 + 6 * nz;
+    const int nmod = fd_model_count(nz, a.sen_vs != nullptr);
     const int tid = threadIdx.x, nthr = blockDim.x;
     float* cbuf = C.cbuf;
     if (tid == 0) {
@@ -205,7 +205,7 @@ fd_column_kernel(FdArgs a)
     C.pv_b = post; C.pv_sk = ncol;
     C.sen_b = post; C.sen_sk = ncol; C.sen_is = ncol * (long long)K;
     C.status_i = post;
-    C.cbuf = a.cscratch + (size_t)blockIdx.x * (1 + 6 * nz) * K;
+    C.cbuf = a.cscratch + (size_t)blockIdx.x * fd_model_count(nz, a.sen_vs != nullptr) * K;
     fd_column_body<IFUNC, GROUP>(C, S, a);
 }
 

@@ -155,13 +155,18 @@ int dazi_dk_fused_dev(int nx, int ny, int nz, const float *vel, const float *vp,
  * synchronisation): the caller passes device inputs and outputs; the only
  * other device memory is a file-scope static array of 4 Mi floats (16 MiB)
  * plus the depth-grid geometry, held on every GPU that loads the library
- * until exit.  Columns run in tiles of 16 MiB / (4 (1 + 6 nz) kmaxRc) bytes;
- * a column whose scratch exceeds the array is rejected with
- * DAZI_ERR_LIMITS.  All calls share the array: calls whose GPU work overlaps
- * race and must be ordered by the caller.  The first call on a device does
- * that device's set-up (cudaGetSymbolAddress); make it before any stream
- * capture.  Returns once the work is queued on `stream` (NULL = legacy
- * default stream); no-root periods are reported through `status`. */
+ * until exit.  Columns run in tiles of 16 MiB / (4 M kmaxRc) bytes, with
+ * M = 1 + 6 nz models per column when sen_* are given and M = 1 (phase
+ * velocities only) when they are NULL; a column whose scratch exceeds the
+ * array is rejected with DAZI_ERR_LIMITS.  All calls share the array: calls
+ * whose GPU work overlaps race and must be ordered by the caller.  The first
+ * call on a device does that device's set-up (cudaGetSymbolAddress); make it
+ * before any stream capture.  Each call synchronises `stream` (NULL = legacy
+ * default stream) twice, to read back the depth grid, the periods and the
+ * refined layer count for validation; the finite-difference launches that
+ * follow are queued and not waited for.  A CUDA error already pending when
+ * the call starts is reported (DAZI_ERR_CUDA) and left pending.  No-root
+ * periods are reported through `status`. */
 int dazi_dk_iso_noalloc_dev(int nx, int ny, int nz, const float *vel,
                             const float *vp, const float *rho, double *pvRc,
                             double *sen_vsRc, double *sen_vpRc,

@@ -28,6 +28,27 @@ def test_library_exports_every_declared_symbol():
     assert set(names) == set(_lib.EXPORTS)
 
 
+def header_arity():
+    """Parameter count of every function the public header declares."""
+    text = open(os.path.join(ROOT, "include", "dazi_dk.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for name, params in re.findall(r"\b(dazi_dk_\w+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+        params = params.strip()
+        out[name] = 0 if params in ("", "void") else params.count(",") + 1
+    return out
+
+
+def test_bindings_match_header_arity():
+    """Each ctypes binding declares as many arguments as the C prototype
+    (a mismatch shifts arguments silently, e.g. an int into a pointer)."""
+    L = _lib.load()
+    arity = header_arity()
+    assert set(arity) == set(_lib.EXPORTS)
+    for name, n in arity.items():
+        assert len(getattr(L, name).argtypes) == n, name
+
+
 def test_version():
     assert _lib.load().dazi_dk_version() >= 100
 
