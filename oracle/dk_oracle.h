@@ -48,6 +48,23 @@ int or_tregn96_ex(int nl, const float *d_in, const float *TA_in, const float *TC
                   const float *frefsi_in, int nt, const float *t_in, const float *cp_in,
                   float *dcdah_out, float *dcdbv_out, float *dcdn_out, int nsph, int dogam,
                   double *full);
+int or_tregn96_cd(int nl, const float *d_in, const float *TA_in, const float *TC_in,
+                  const float *TF_in, const float *TL_in, const float *TN_in,
+                  const float *TRho_in, const float *qai_in, const float *qbi_in,
+                  const float *etapi_in, const float *etasi_in, const float *frefpi_in,
+                  const float *frefsi_in, int nt, const float *t_in, const double *cp_d,
+                  float *dcdah_out, float *dcdbv_out, float *dcdn_out, int nsph, int dogam,
+                  double *full);
+double or_ti_secular_d(int nl, const double *d, const double *TA, const double *TC,
+                       const double *TF, const double *TL, const double *TN, const double *rho,
+                       double omega, double c);
+int or_ti_root_d(int nl, const double *d, const double *TA, const double *TC, const double *TF,
+                 const double *TL, const double *TN, const double *rho, double omega, double c0,
+                 double xtol, double *root);
+int or_ti_root_fd(int nl, const double *d, const double *TA, const double *TC, const double *TF,
+                  const double *TL, const double *TN, const double *rho, double omega,
+                  double c0, double h, double xtol, int npert, const int *lo, const int *hi,
+                  const int *kind, double *dcdp, int nthreads);
 int or_depthkernelTI(int nx, int ny, int nz, const float *vel, const float *vp_in,
                      const float *rho_in, double *pvRc, int iwave, int igr, int kmax,
                      const double *tRc, const float *depz, float minthk, float *Lsen,

@@ -72,6 +72,17 @@ def lib():
             L.or_tregn96.restype = ctypes.c_int
             L.or_tregn96_ex.argtypes = L.or_tregn96.argtypes + [ctypes.c_int, ctypes.c_int, _f64p]
             L.or_tregn96_ex.restype = ctypes.c_int
+            L.or_tregn96_cd.argtypes = L.or_tregn96.argtypes[:16] + [_f64p] + \
+                L.or_tregn96.argtypes[17:] + [ctypes.c_int, ctypes.c_int, _f64p]
+            L.or_tregn96_cd.restype = ctypes.c_int
+            d7 = [ctypes.c_int] + [_f64p] * 7
+            L.or_ti_secular_d.argtypes = d7 + [ctypes.c_double, ctypes.c_double]
+            L.or_ti_secular_d.restype = ctypes.c_double
+            L.or_ti_root_d.argtypes = d7 + [ctypes.c_double] * 3 + [_f64p]
+            L.or_ti_root_d.restype = ctypes.c_int
+            L.or_ti_root_fd.argtypes = d7 + [ctypes.c_double] * 4 + [ctypes.c_int, _i32p, _i32p,
+                                                                      _i32p, _f64p, ctypes.c_int]
+            L.or_ti_root_fd.restype = ctypes.c_int
         L.or_surfdisp96_d.argtypes = [_f64p, _f64p, _f64p, _f64p, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int, _f64p, _f64p, ctypes.c_double]
         L.or_surfdisp96_d.restype = ctypes.c_int
@@ -226,10 +237,12 @@ def surfdisp96_d(thk, vp, vs, rho, periods, iflsph=1, tol=1e-13):
     return cg, st
 
 
-def tregn96(thk, TA, TC, TF, TL, TN, rho, periods, cp, nsph=1, dogam=1, full=False):
+def tregn96(thk, TA, TC, TF, TL, TN, rho, periods, cp, nsph=1, dogam=1, full=False,
+            cp_double=False):
     """tregn96 partials (dcdah, dcdbv, dcdn as (K, nl) float32); with
     full=True also the FP64 partials [K, 7, nl] (ah, av, bh, bv, n, r, and
-    c after the Q shift in [:, 6, 0])."""
+    c after the Q shift in [:, 6, 0]).  cp_double=True evaluates them at the
+    double phase velocities cp instead of their real*4 values."""
     nl = len(thk)
     f = lambda x: np.ascontiguousarray(x, np.float32)  # noqa: E731
     arr = [f(thk), f(TA), f(TC), f(TF), f(TL), f(TN), f(rho)]
@@ -238,17 +251,63 @@ def tregn96(thk, TA, TC, TF, TL, TN, rho, periods, cp, nsph=1, dogam=1, full=Fal
     z = np.zeros(nl, np.float32)
     one = np.ones(nl, np.float32)
     t = f(periods)
-    c = f(cp)
     K = t.size
     out = [np.zeros((K, nl), np.float32) for _ in range(3)]
     fb = np.zeros((K, 7, nl)) if full else None
-    r = lib().or_tregn96_ex(nl, *[_p(x, _f32p) for x in arr], _p(qp, _f32p), _p(qs, _f32p),
-                            _p(z, _f32p), _p(z, _f32p), _p(one, _f32p), _p(one, _f32p), K,
-                            _p(t, _f32p), _p(c, _f32p), *[_p(o, _f32p) for o in out],
-                            int(nsph), int(dogam), _p(fb, _f64p))
+    head = [_p(x, _f32p) for x in arr] + [_p(qp, _f32p), _p(qs, _f32p), _p(z, _f32p),
+                                          _p(z, _f32p), _p(one, _f32p), _p(one, _f32p)]
+    if cp_double:
+        c = np.ascontiguousarray(cp, np.float64)
+        r = lib().or_tregn96_cd(nl, *head, K, _p(t, _f32p), _p(c, _f64p),
+                                *[_p(o, _f32p) for o in out], int(nsph), int(dogam),
+                                _p(fb, _f64p))
+    else:
+        c = f(cp)
+        r = lib().or_tregn96_ex(nl, *head, K, _p(t, _f32p), _p(c, _f32p),
+                                *[_p(o, _f32p) for o in out], int(nsph), int(dogam),
+                                _p(fb, _f64p))
     if r != 0:
         raise RuntimeError("oracle tregn96 failed")
     return (tuple(out) + (fb,)) if full else tuple(out)
+
+
+def _d7(thk, TA, TC, TF, TL, TN, rho):
+    return [np.ascontiguousarray(x, np.float64) for x in (thk, TA, TC, TF, TL, TN, rho)]
+
+
+def ti_secular(thk, TA, TC, TF, TL, TN, rho, omega, c):
+    """TI Rayleigh secular function (up()'s top compound entry) of a flat
+    double-precision model at (omega, c): a checker."""
+    a = _d7(thk, TA, TC, TF, TL, TN, rho)
+    return lib().or_ti_secular_d(len(a[0]), *[_p(x, _f64p) for x in a], omega, c)
+
+
+def ti_root(thk, TA, TC, TF, TL, TN, rho, omega, c0, xtol=1e-14):
+    """Root of the TI secular function nearest c0 (bracketed, Brent)."""
+    a = _d7(thk, TA, TC, TF, TL, TN, rho)
+    out = ctypes.c_double(0.0)
+    r = lib().or_ti_root_d(len(a[0]), *[_p(x, _f64p) for x in a], omega, c0, xtol * c0,
+                           ctypes.byref(out))
+    if r != 0:
+        raise RuntimeError("no TI root near c0")
+    return out.value
+
+
+def ti_root_fd(thk, TA, TC, TF, TL, TN, rho, omega, c0, perts, h=1e-5, xtol=1e-15,
+               nthreads=0):
+    """Central differences of the TI root: perts is a list of (lo, hi,
+    kind), kind 0..4 = A, C, F, L, N of layer lo (= hi): dc/d(modulus);
+    kind 5 = A and L of layers lo..hi scaled together: dc/dh."""
+    a = _d7(thk, TA, TC, TF, TL, TN, rho)
+    p = np.asarray(perts, np.int32).reshape(-1, 3)
+    lo, hi, kind = (np.ascontiguousarray(p[:, i]) for i in range(3))
+    out = np.zeros(len(p))
+    r = lib().or_ti_root_fd(len(a[0]), *[_p(x, _f64p) for x in a], omega, c0, h, xtol * c0,
+                            len(p), _p(lo, _i32p), _p(hi, _i32p), _p(kind, _i32p),
+                            _p(out, _f64p), nthreads)
+    if r != 0:
+        raise RuntimeError(f"{r} TI roots failed")
+    return out
 
 
 def batch(node_off, depz, vs, per_off, periods, minthk, kernels=True, lsen=True, nthreads=0):

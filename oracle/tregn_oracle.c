@@ -27,8 +27,11 @@
  *
  * Parity status: no golden vector of the reference pins Lsen_Gsc (its dump
  * files live outside the repository).  The restatement is checked by
- * physics: with sphericity and Q switched off the isotropic combinations of
- * its partials equal finite differences of surfdisp96 (tests).
+ * physics against a second code path: the root of the TI secular function
+ * (up()'s compound sweep) equals surfdisp96's golden-pinned root at
+ * isotropic moduli, central differences of that root in A, C, F, L, N
+ * equal the energy-integral partials converted to moduli, and sprayl,
+ * gammap and the splice are checked in closed form (tests).
  */
 #include <math.h>
 #include <stdlib.h>
@@ -602,13 +605,13 @@ static double gammap(ti_state *s, double omega, double *wvno)
  * the scope).  Outputs dcdah/dcdbv/dcdn as real*4 (np x nl, period-major:
  * out[k*nl + layer]).  nsph / dogam switch sphericity and Q (the reference
  * uses 1 / 1).  Returns 0, or -1 on a fluid layer or bad sizes.           */
-int or_tregn96_ex(int nl, const float *d_in, const float *TA_in, const float *TC_in,
-                  const float *TF_in, const float *TL_in, const float *TN_in,
-                  const float *TRho_in, const float *qai_in, const float *qbi_in,
-                  const float *etapi_in, const float *etasi_in, const float *frefpi_in,
-                  const float *frefsi_in, int nt, const float *t_in, const float *cp_in,
-                  float *dcdah_out, float *dcdbv_out, float *dcdn_out, int nsph, int dogam,
-                  double *full)
+static int tregn96_run(int nl, const float *d_in, const float *TA_in, const float *TC_in,
+                       const float *TF_in, const float *TL_in, const float *TN_in,
+                       const float *TRho_in, const float *qai_in, const float *qbi_in,
+                       const float *etapi_in, const float *etasi_in, const float *frefpi_in,
+                       const float *frefsi_in, int nt, const float *t_in, const float *cp_in,
+                       const double *cp_d, float *dcdah_out, float *dcdbv_out,
+                       float *dcdn_out, int nsph, int dogam, double *full)
 {
     if (nl < 2 || nl > NL || nt < 1 || nt > NP) return -1;
     ti_state *s = calloc(1, sizeof(ti_state));
@@ -687,7 +690,7 @@ int or_tregn96_ex(int nl, const float *d_in, const float *TA_in, const float *TC
     for (int k = 0; k < nt; ++k) {
         double t = (double)t_in[k];
         double omega = (double)twopi / t;
-        double c = (double)cp_in[k];
+        double c = cp_d ? cp_d[k] : (double)cp_in[k];
         double wvno = omega / c;
         svfunc(s, omega, wvno);
         energy(s, omega, wvno);
@@ -730,6 +733,184 @@ int or_tregn96_ex(int nl, const float *d_in, const float *TA_in, const float *TC
     }
     free(s);
     return 0;
+}
+
+int or_tregn96_ex(int nl, const float *d_in, const float *TA_in, const float *TC_in,
+                  const float *TF_in, const float *TL_in, const float *TN_in,
+                  const float *TRho_in, const float *qai_in, const float *qbi_in,
+                  const float *etapi_in, const float *etasi_in, const float *frefpi_in,
+                  const float *frefsi_in, int nt, const float *t_in, const float *cp_in,
+                  float *dcdah_out, float *dcdbv_out, float *dcdn_out, int nsph, int dogam,
+                  double *full)
+{
+    return tregn96_run(nl, d_in, TA_in, TC_in, TF_in, TL_in, TN_in, TRho_in, qai_in, qbi_in,
+                       etapi_in, etasi_in, frefpi_in, frefsi_in, nt, t_in, cp_in, NULL,
+                       dcdah_out, dcdbv_out, dcdn_out, nsph, dogam, full);
+}
+
+/* The same with the phase velocities given in double (cp_d): a checker
+ * entry that evaluates the partials at an exact root instead of at the
+ * real*4 value depthkernelTI passes. */
+int or_tregn96_cd(int nl, const float *d_in, const float *TA_in, const float *TC_in,
+                  const float *TF_in, const float *TL_in, const float *TN_in,
+                  const float *TRho_in, const float *qai_in, const float *qbi_in,
+                  const float *etapi_in, const float *etasi_in, const float *frefpi_in,
+                  const float *frefsi_in, int nt, const float *t_in, const double *cp_d,
+                  float *dcdah_out, float *dcdbv_out, float *dcdn_out, int nsph, int dogam,
+                  double *full)
+{
+    float cpf[NP];
+    if (nt < 1 || nt > NP) return -1;
+    for (int k = 0; k < nt; ++k) cpf[k] = (float)cp_d[k];
+    return tregn96_run(nl, d_in, TA_in, TC_in, TF_in, TL_in, TN_in, TRho_in, qai_in, qbi_in,
+                       etapi_in, etasi_in, frefpi_in, frefsi_in, nt, t_in, cpf, cp_d,
+                       dcdah_out, dcdbv_out, dcdn_out, nsph, dogam, full);
+}
+
+/* ------------------------------------------------------------------------
+ * Checker functions with no reference counterpart.  The TI Rayleigh secular
+ * function of a flat double-precision model (no sphericity, no Q) is the
+ * top entry of up()'s compound vector: the chain gettiegn -> varsv ->
+ * dnka_tregn -> cnormc from the half-space (evalg) up.  Its fundamental
+ * root, found by bracketing and Brent's method, and central differences of
+ * that root with respect to the moduli of chosen layers give dc/dA, dc/dC,
+ * dc/dF, dc/dL, dc/dN without svfunc/down/energy/intijr, the path that
+ * forms tregn96's partials; the tests compare the two.                   */
+static void ti_flat_model(ti_state *s, int nl, const double *d, const double *TA,
+                          const double *TC, const double *TF, const double *TL,
+                          const double *TN, const double *rho)
+{
+    s->mmax = nl;
+    s->nsph = 0;
+    s->dogam = 0;
+    for (int i = 0; i < nl; ++i) {
+        s->zd[i] = d[i]; s->zta[i] = TA[i]; s->ztc[i] = TC[i]; s->ztf[i] = TF[i];
+        s->ztl[i] = TL[i]; s->ztn[i] = TN[i]; s->zrho[i] = rho[i];
+        s->iwat[i] = 0;
+    }
+}
+
+double or_ti_secular_d(int nl, const double *d, const double *TA, const double *TC,
+                       const double *TF, const double *TL, const double *TN, const double *rho,
+                       double omega, double c)
+{
+    if (nl < 2 || nl > NL) return NAN;
+    ti_state *s = calloc(1, sizeof(ti_state));
+    if (!s) return NAN;
+    ti_flat_model(s, nl, d, TA, TC, TF, TL, TN, rho);
+    double f = up(s, omega, omega / c);
+    free(s);
+    return f;
+}
+
+/* Root of F(c) = up() near c0: the bracket grows geometrically around c0
+ * (first sign change on either side, nearest first), then Brent's method
+ * (inverse quadratic interpolation / secant / bisection, R. P. Brent,
+ * Algorithms for Minimization without Derivatives, 1973, ch. 4) until the
+ * bracket is below xtol.  Returns 0, or -1 when no sign change lies within
+ * 5 % of c0. */
+static int ti_root(ti_state *s, double omega, double c0, double xtol, double *root)
+{
+#define TIF(c) up(s, omega, omega / (c))
+    double f0 = TIF(c0);
+    if (f0 == 0.0) { *root = c0; return 0; }
+    double a = 0, b = 0, fa = 0, fb = 0;
+    int found = 0;
+    for (double del = 1e-9 * c0; del < 0.05 * c0 && !found; del *= 2.0) {
+        double cl = c0 - del, cu = c0 + del;
+        double fl = TIF(cl), fu = TIF(cu);
+        if ((fu < 0) != (f0 < 0)) { a = c0; fa = f0; b = cu; fb = fu; found = 1; }
+        else if ((fl < 0) != (f0 < 0)) { a = cl; fa = fl; b = c0; fb = f0; found = 1; }
+    }
+    if (!found) return -1;
+    double c = a, fc = fa, dd = b - a, e = dd;
+    for (int it = 0; it < 200; ++it) {
+        if ((fb > 0) == (fc > 0)) { c = a; fc = fa; dd = b - a; e = dd; }
+        if (fabs(fc) < fabs(fb)) { a = b; b = c; c = a; fa = fb; fb = fc; fc = fa; }
+        double tol1 = 2.0 * 2.220446049250313e-16 * fabs(b) + 0.5 * xtol;
+        double xm = 0.5 * (c - b);
+        if (fabs(xm) <= tol1 || fb == 0.0) { *root = b; return 0; }
+        if (fabs(e) >= tol1 && fabs(fa) > fabs(fb)) {
+            double sr = fb / fa, p, q;
+            if (a == c) { p = 2.0 * xm * sr; q = 1.0 - sr; }
+            else {
+                double qa = fa / fc, r = fb / fc;
+                p = sr * (2.0 * xm * qa * (qa - r) - (b - a) * (r - 1.0));
+                q = (qa - 1.0) * (r - 1.0) * (sr - 1.0);
+            }
+            if (p > 0) q = -q; else p = -p;
+            double m1 = 3.0 * xm * q - fabs(tol1 * q), m2 = fabs(e * q);
+            if (2.0 * p < (m1 < m2 ? m1 : m2)) { e = dd; dd = p / q; }
+            else { dd = xm; e = dd; }
+        } else { dd = xm; e = dd; }
+        a = b; fa = fb;
+        b += fabs(dd) > tol1 ? dd : (xm > 0 ? tol1 : -tol1);
+        fb = TIF(b);
+    }
+#undef TIF
+    *root = b;
+    return 0;
+}
+
+int or_ti_root_d(int nl, const double *d, const double *TA, const double *TC, const double *TF,
+                 const double *TL, const double *TN, const double *rho, double omega, double c0,
+                 double xtol, double *root)
+{
+    if (nl < 2 || nl > NL) return -1;
+    ti_state *s = calloc(1, sizeof(ti_state));
+    if (!s) return -1;
+    ti_flat_model(s, nl, d, TA, TC, TF, TL, TN, rho);
+    int r = ti_root(s, omega, c0, xtol, root);
+    free(s);
+    return r;
+}
+
+/* Central differences of the root.  Perturbation p scales, in layers
+ * lo[p]..hi[p] (0-based), the modulus kind[p] (0 A, 1 C, 2 F, 3 L, 4 N) by
+ * (1 +- h), or with kind 5 both A and L (F, C, N and rho held).  For kinds
+ * 0-4 on one layer dcdp[p] is dc/d(modulus); for kind 5 it is
+ * dc/dh = sum over the layers of A dc/dA + L dc/dL.  OpenMP over the
+ * perturbations.  Returns 0, or the number of failed roots. */
+int or_ti_root_fd(int nl, const double *d, const double *TA, const double *TC, const double *TF,
+                  const double *TL, const double *TN, const double *rho, double omega,
+                  double c0, double h, double xtol, int npert, const int *lo, const int *hi,
+                  const int *kind, double *dcdp, int nthreads)
+{
+    if (nl < 2 || nl > NL) return -1;
+    int bad = 0;
+#ifdef _OPENMP
+    if (nthreads < 1) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic) num_threads(nthreads) reduction(+:bad)
+#endif
+    for (int p = 0; p < npert; ++p) {
+        ti_state *s = calloc(1, sizeof(ti_state));
+        if (!s) { ++bad; continue; }
+        double cr[2];
+        for (int sg = 0; sg < 2; ++sg) {
+            const double f = sg == 0 ? 1.0 + h : 1.0 - h;
+            ti_flat_model(s, nl, d, TA, TC, TF, TL, TN, rho);
+            for (int m = lo[p]; m <= hi[p]; ++m) {
+                switch (kind[p]) {
+                case 0: s->zta[m] *= f; break;
+                case 1: s->ztc[m] *= f; break;
+                case 2: s->ztf[m] *= f; break;
+                case 3: s->ztl[m] *= f; break;
+                case 4: s->ztn[m] *= f; break;
+                default: s->zta[m] *= f; s->ztl[m] *= f; break;
+                }
+            }
+            if (ti_root(s, omega, c0, xtol, &cr[sg]) != 0) { ++bad; cr[sg] = NAN; }
+        }
+        double q = (cr[0] - cr[1]) / (2.0 * h);
+        if (kind[p] <= 4) {
+            const double *th = kind[p] == 0 ? TA : kind[p] == 1 ? TC : kind[p] == 2 ? TF
+                             : kind[p] == 3 ? TL : TN;
+            q /= th[lo[p]];
+        }
+        dcdp[p] = q;
+        free(s);
+    }
+    return bad;
 }
 
 int or_tregn96(int nl, const float *d_in, const float *TA_in, const float *TC_in,
