@@ -57,8 +57,10 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-FLOP_PER_LAYER_EVAL = 180   # hand count of dltar4's FP64 arithmetic per layer (fallback when
-                             # the ncu-counted figure is absent)
+FLOP_PER_LAYER_EVAL = 180   # hand count of dltar4's FP64 arithmetic per layer of one secular
+                             # evaluation (sqrt and division as one, transcendentals not counted)
+SWEEP_FWD_EQUIV = 2          # forward-equivalent sweeps per layer item of the adjoint and of the
+                             # Gc/Gs kernel (2 + 2 = the + 4 of the whole-step count)
 
 
 def parse():
@@ -74,7 +76,10 @@ def parse():
     p.add_argument("--form", default="adjoint", choices=["plain", "adjoint"])
     p.add_argument("--no-other-form", action="store_true")
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--cpu-sample-s", type=float, default=15.0)
+    p.add_argument("--cpu-cols-per-thread", type=int, default=CPU_COLS_PER_THREAD,
+                   help="uneven workload: columns per host thread in each CPU sample")
+    p.add_argument("--cpu-sample-s", type=float, default=15.0,
+                   help="grid workloads: seconds of CPU work in the cpu_baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
     return p.parse_args()
 
@@ -106,29 +111,46 @@ def load_ragged(args, rank):
     return S.config3(realisations=args.realisations, base_seed=1000 + 100000 * rank)
 
 
-def ragged_cpu_baseline(b, sample_s, cores=None):
+CPU_COLS_PER_THREAD = 8   # default CPU sample: uneven columns per host thread (load-balanced)
+
+
+def sample_columns(b, n, seed):
+    """n columns drawn without replacement, seeded, from the whole batch
+    (every realisation), in batch order."""
+    return np.sort(np.random.default_rng(seed).choice(b.ncol, min(n, b.ncol), replace=False))
+
+
+def sub_batch(b, idx):
+    """The CSR batch of the columns idx."""
+    from dazi_current_release_b200 import synthetic as S
+    nz = np.diff(b.node_off)[idx]
+    K = np.diff(b.per_off)[idx]
+    cat = lambda arr, off: np.concatenate([arr[off[c]:off[c + 1]] for c in idx])  # noqa: E731
+    return S.RaggedBatch(np.concatenate([[0], np.cumsum(nz)]).astype(np.int64),
+                         cat(b.depz, b.node_off), cat(b.vs, b.node_off),
+                         np.concatenate([[0], np.cumsum(K)]).astype(np.int64),
+                         cat(b.periods, b.per_off), b.minthk)
+
+
+def ragged_cpu_baseline(b, seed=0, cores=None, per_thread=CPU_COLS_PER_THREAD):
     """Oracle of the reference stage (depthkernel FD + depthkernelTI per
-    column, OpenMP over columns) on the first columns of the batch, as many
-    as fit in about sample_s seconds; returns column-periods/s."""
+    column, OpenMP over columns) on a seeded sample of per_thread columns per
+    host thread drawn from the whole batch; returns (the cpu_baseline entry,
+    the sampled column indices, the sub-batch, the oracle outputs)."""
     from oracle import oracle as O
     cores = cores or os.cpu_count() or 1
-
-    def run(n):
-        no, po = b.node_off[:n + 1], b.per_off[:n + 1]
-        t0 = time.perf_counter()
-        O.batch(no, b.depz[:no[-1]], b.vs[:no[-1]], po, b.periods[:po[-1]], b.minthk,
-                nthreads=cores)
-        return time.perf_counter() - t0
-
-    n1 = min(b.ncol, cores)
-    dt1 = run(n1)
-    n2 = int(min(b.ncol, max(n1, sample_s / max(dt1, 1e-9) * n1)))
-    dt = run(n2) if n2 > n1 else dt1
-    cp = int(b.per_off[n2])
-    return {"value": cp / dt, "unit": "column-periods/s", "cores": cores, "kind": "port",
-            "sample": f"first {n2} of {b.ncol} columns ({cp} column-periods), oracle of "
-                      f"depthkernel (FD: 1+6nz surfdisp96 per column) + depthkernelTI, "
-                      f"{dt:.1f} s on {cores} threads"}
+    idx = sample_columns(b, per_thread * cores, seed)
+    sb = sub_batch(b, idx)
+    t0 = time.perf_counter()
+    out = O.batch(sb.node_off, sb.depz, sb.vs, sb.per_off, sb.periods, sb.minthk, nthreads=cores)
+    dt = time.perf_counter() - t0
+    cp = sb.column_periods
+    cb = {"value": cp / dt, "unit": "column-periods/s", "cores": cores, "kind": "port",
+          "sample": f"{idx.size} seeded columns (seed {seed}) drawn from the {b.ncol} of the "
+                    f"batch ({cp} column-periods), oracle of depthkernel (FD: 1+6nz "
+                    f"surfdisp96 per column) + depthkernelTI at -O3, {dt:.1f} s on {cores} "
+                    f"threads"}
+    return cb, idx, sb, out
 
 
 class ClockSampler:
@@ -227,22 +249,40 @@ def cpu_baseline(case, sample_s, form_kernels=True):
 
 
 def run_reference_ragged(args, ws, rank):
+    """The reference's CPU path (the oracle restatement: the Fortran cannot
+    be built here) on the host cores: each step times a fresh seeded sample
+    of --cpu-cols-per-thread columns per thread drawn from the whole batch
+    (8 by default: about 10 s of work on 16 threads); warm-up steps run one
+    column per thread.  ms_per_step is the measured time of one sampled
+    step."""
     if rank != 0:
         return
+    from oracle import oracle as O
     b = load_ragged(args, 0)
-    vals = []
-    for _ in range(args.steps):
-        cb = ragged_cpu_baseline(b, args.cpu_sample_s / max(args.steps, 1))
+    cores = os.cpu_count() or 1
+    for w in range(args.warmup):
+        sb = sub_batch(b, sample_columns(b, cores, 10_000 + w))
+        O.batch(sb.node_off, sb.depz, sb.vs, sb.per_off, sb.periods, sb.minthk, nthreads=cores)
+    vals, secs, cps = [], [], []
+    for i in range(args.steps):
+        cb, idx, sb, _ = ragged_cpu_baseline(b, seed=i, cores=cores,
+                                             per_thread=args.cpu_cols_per_thread)
         vals.append(cb["value"])
+        cps.append(sb.column_periods)
+        secs.append(sb.column_periods / cb["value"])
     v = float(np.median(vals))
-    cp = b.column_periods
     line = {"impl": "reference", "metric": "kernel column-periods/s", "value": v,
             "unit": "column-periods/s", "n_gpus": ws, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": cp / v * 1e3,
+            "warmup": args.warmup, "ms_per_step": float(np.median(secs)) * 1e3,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic", "config": ragged_config(args, b),
-            "cpu_baseline": {"value": v, "unit": "column-periods/s", "cores": cb["cores"],
-                             "kind": cb["kind"], "sample": cb["sample"]},
+            "cpu_baseline": {"value": v, "unit": "column-periods/s", "cores": cores,
+                             "kind": "port",
+                             "sample": f"median over {args.steps} steps; each step "
+                                       f"{args.cpu_cols_per_thread * cores} seeded columns (seed = "
+                                       f"step) of the {b.ncol}, {int(np.median(cps))} "
+                                       f"column-periods (median), oracle of depthkernel (FD) "
+                                       f"+ depthkernelTI at -O3 on {cores} threads"},
             "e2e": {"value": v, "unit": "column-periods/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -256,7 +296,88 @@ def ragged_config(args, b):
             "layers_per_column": [int(nz.min()) - 1, int(nz.max()) - 1],
             "mean_layers": float(nz.mean() - 1), "periods_per_column": [int(K.min()), int(K.max())],
             "mean_periods": float(K.mean()), "minthk": b.minthk,
-            "parallelism": "columns, one batch per GPU"}
+            "parallelism": "columns, one batch per GPU",
+            "l2": "inputs and outputs far larger than L2; 256 MiB flush write between steps "
+                  "outside the timed events"}
+
+
+def _per_column_rel_l2(got, ref, off, K, nz, mask_k):
+    """Worst per-column rel-L2 over the columns' (period, node) entries,
+    periods k < mask_k[c] only (the periods with a root)."""
+    worst = 0.0
+    for c in range(K.size):
+        kk = int(mask_k[c])
+        if kk == 0:
+            continue
+        g = got[off[c]:off[c + 1]].reshape(nz[c], K[c])[:, :kk]
+        r = ref[off[c]:off[c + 1]].reshape(nz[c], K[c])[:, :kk]
+        den = np.linalg.norm(r)
+        if den > 0:
+            worst = max(worst, float(np.linalg.norm(g - r) / den))
+    return worst
+
+
+def accuracy_block(sb, gpu, ora, exact, plain):
+    """Errors of the timed form on the sampled columns against the oracle:
+    gpu / plain = the library's adjoint-form and plain-form outputs of those
+    columns, ora = the oracle in the reference's arithmetic (FD kernels,
+    Lsen_Gsc), exact = the oracle's exact-model differences (double model,
+    roots to 1e-13, dln 1e-4)."""
+    K = np.diff(sb.per_off)
+    nz = np.diff(sb.node_off)
+    sen_off = np.concatenate([[0], np.cumsum(K * nz)])
+    ls_off = np.concatenate([[0], np.cumsum(K * (nz - 1))])
+    pv_ref = ora["pv"]
+    # status: first period without a root (1-based), 0 if none
+    st_ref = np.zeros(K.size, np.int64)
+    for c in range(K.size):
+        z = np.nonzero(pv_ref[sb.per_off[c]:sb.per_off[c + 1]] == 0)[0]
+        st_ref[c] = z[0] + 1 if z.size else 0
+    good = np.where(st_ref > 0, st_ref - 1, K)
+    ok = pv_ref > 0
+    rel = np.abs(gpu["pv"][ok] / pv_ref[ok] - 1.0)
+    same_status = gpu["status"] == st_ref
+    within = np.zeros(pv_ref.size, bool)
+    within[ok] = rel <= 1e-6
+    ident = int(sum(bool(same_status[c]) and bool(within[sb.per_off[c]:sb.per_off[c] + good[c]].all())
+                    for c in range(K.size)))
+    ls_worst = 0.0
+    for c in range(K.size):
+        kk = int(good[c])
+        if kk == 0:
+            continue
+        g = gpu["lsen"][ls_off[c]:ls_off[c + 1]].reshape(nz[c] - 1, K[c])[:, :kk]
+        r = ora["lsen"][ls_off[c]:ls_off[c + 1]].reshape(nz[c] - 1, K[c])[:, :kk]
+        den = np.linalg.norm(r.astype(np.float64))
+        if den > 0:
+            ls_worst = max(ls_worst, float(np.linalg.norm((g - r).astype(np.float64)) / den))
+    names = ("sen_vs", "sen_vp", "sen_rho")
+    acc = {
+        "columns": int(K.size), "column_periods": int(sb.column_periods),
+        "pv_max_rel_err": float(rel.max()) if rel.size else 0.0,
+        "pv_bit_identical": int(np.count_nonzero(gpu["pv"] == pv_ref)),
+        "status_equal_columns": int(same_status.sum()),
+        "fundamental_mode_identity_columns": ident,
+        "adjoint_kernels_vs_exact_worst_column_rel_l2":
+            {n: _per_column_rel_l2(gpu[n], exact[n], sen_off, K, nz, good) for n in names},
+        "adjoint_kernels_vs_reference_fd_worst_column_rel_l2":
+            {n: _per_column_rel_l2(gpu[n], ora[n], sen_off, K, nz, good) for n in names},
+        "lsen_worst_column_rel_l2": ls_worst,
+        "tolerances": {"pv": 1e-6, "kernels_vs_exact": 1e-4,
+                       "kernels_vs_reference_fd_gate": {"sen_vs": 1e-3, "sen_vp": 2e-3,
+                                                        "sen_rho": 2e-3},
+                       "lsen": 1e-5},
+    }
+    if plain is not None:
+        acc["plain_form"] = {
+            "pv_max_rel_err": float(np.abs(plain["pv"][ok] / pv_ref[ok] - 1.0).max()),
+            "pv_bit_identical": int(np.count_nonzero(plain["pv"] == pv_ref)),
+            "kernel_entries_bit_identical": int(sum(np.count_nonzero(plain[n] == ora[n])
+                                                    for n in names)),
+            "kernel_entries": int(3 * sen_off[-1]),
+            "kernels_vs_reference_fd_worst_column_rel_l2":
+                {n: _per_column_rel_l2(plain[n], ora[n], sen_off, K, nz, good) for n in names}}
+    return acc
 
 
 def run_reference(args, ws, rank):
@@ -418,6 +539,13 @@ def main_ragged(args, ws, rank, local):
     torch.cuda.synchronize(dev)
     step_fn(form, ncol)()
     phases = _lib.last_timing()
+    # outputs of the sampled columns (the CPU baseline's sample) for the
+    # accuracy block, taken from this full-batch step
+    acc_cols = None
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        acc_cols = sample_columns(b, args.cpu_cols_per_thread * (os.cpu_count() or 1), 0)
+        gpu_sample = _gather_columns(torch, dev, b, acc_cols, sen_off, ls_off, pv, sen, lsen,
+                                     status)
     scan32 = None
     if form == _lib.FORM_ADJOINT:
         pv64 = pv.clone()
@@ -467,26 +595,35 @@ def main_ragged(args, ws, rank, local):
     h2d = sum(h[k].nbytes for k in h)
     d2h = h_pv.nbytes + sum(x.nbytes for x in h_sen) + h_ls.nbytes + h_st.nbytes
 
-    # roofline of the dominant kernel
+    # roofline of the dominant kernel.  achieved = algorithmic FP64 flops
+    # (the hand count of 180 per layer of one secular evaluation) / the
+    # kernel's event-timed duration: root search 180 x sum over column-periods
+    # of rmax x E_ref (E_ref = the reference's evaluation count, which the
+    # device search reproduces point for point); adjoint and Gc/Gs sweeps
+    # 180 x 2 x layer items each (two forward-equivalent sweeps, the + 4 of
+    # the whole-step count split between them).  pipe_frac: the FP64
+    # operations ncu counts as executed (exp/sqrt/division included).
     peak = ctypes.c_double(0.0)
     _lib.check(L.dazi_dk_fp64_peak(ctypes.byref(peak)))
     peak_tf = peak.value / 1e3
     consts = _work_constants()
     units = {"root": ("layer_eval", layer_evals), "adjoint": ("layer_item", layer_items),
              "ti": ("layer_item", layer_items)}
-    flops, traffic_of = {}, {}
+    alg_flops = {"root": FLOP_PER_LAYER_EVAL * layer_evals,
+                 "adjoint": FLOP_PER_LAYER_EVAL * SWEEP_FWD_EQUIV * layer_items,
+                 "ti": FLOP_PER_LAYER_EVAL * SWEEP_FWD_EQUIV * layer_items}
+    exec_flops, traffic_of = {}, {}
     for k, (uname, n) in units.items():
         f = consts.get(f"{k}_fp64_ops_per_{uname}")
-        if f is None and k == "root":
-            f = FLOP_PER_LAYER_EVAL
         if f:
-            flops[k] = f * n
+            exec_flops[k] = f * n
         t = consts.get(f"{k}_dram_bytes_per_{uname}")
         if t:
             traffic_of[k] = t * n
     ph = dict(phases)
     dom = max((n for n in ph if n != "prep"), key=lambda n: ph[n])
-    achieved = flops[dom] / (ph[dom] * 1e-3) / 1e12 if dom in flops else None
+    tf = lambda fl, k: fl / (ph[k] * 1e-3) / 1e12  # noqa: E731
+    achieved = tf(alg_flops[dom], dom) if dom in alg_flops else None
     traffic = traffic_of.get(dom)
     roof = {"bound": "fp64", "kernel": {"root": "root_kernel", "adjoint": "adjoint_kernel",
                                          "ti": "ti_kernel", "fd": "fd_batch_kernel"}.get(dom, dom),
@@ -494,13 +631,19 @@ def main_ragged(args, ws, rank, local):
             "frac": achieved / peak_tf if achieved and peak_tf > 0 else None,
             "traffic": traffic,
             "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum per unit on a "
-                              "100000-column capture of this workload (profiles/kernel_work.json), "
-                              "scaled by the units of this launch",
-            "phase_tflops": {k: flops[k] / (ph[k] * 1e-3) / 1e12 for k in flops if k in ph},
-            "peak_source": "measured in-run FP64 FMA probe (dazi_dk_fp64_peak)",
-            "kernel_ms": ph[dom], "flops_per_launch": flops.get(dom),
+                              "capture of this workload (profiles/kernel_work.json), scaled by "
+                              "the units of this launch",
+            "peak_source": "measured in-run FP64 FMA probe (dazi_dk_fp64_peak); "
+                           "MEASURED_PEAKS.json holds no FP64 figure",
+            "kernel_ms": ph[dom], "flops_per_launch": alg_flops.get(dom),
+            "formula": {"root": "180 x root_layer_evals_ref", "adjoint": "180 x 2 x layer_items",
+                        "ti": "180 x 2 x layer_items", "frac": "flops_per_launch / kernel_ms / peak"},
+            "flop_per_layer_eval": FLOP_PER_LAYER_EVAL,
+            "phase_tflops": {k: tf(alg_flops[k], k) for k in alg_flops if k in ph},
+            "phase_frac": {k: tf(alg_flops[k], k) / peak_tf for k in alg_flops if k in ph},
+            "pipe_frac": {k: tf(exec_flops[k], k) / peak_tf for k in exec_flops if k in ph},
             "phase_ms": ph, "layer_items": layer_items, "secular_evals": evals,
-            "root_layer_evals": layer_evals}
+            "root_layer_evals_ref": layer_evals}
     # algorithmic work of the whole step: sum over column-periods of
     # rmax x 180 x (E + 4), E = the root search's secular evaluations (the
     # reference's sequence of points), 180 FP64 flops per layer of one
@@ -537,13 +680,56 @@ def main_ragged(args, ws, rank, local):
     clocks = clk.summary()
     if clocks:
         line["clocks"] = clocks
-    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = ragged_cpu_baseline(b, args.cpu_sample_s)
+    if acc_cols is not None:
+        from oracle import oracle as O
+        cb, idx, sb, ora = ragged_cpu_baseline(b, seed=0, per_thread=args.cpu_cols_per_thread)
+        assert np.array_equal(idx, acc_cols)
+        line["cpu_baseline"] = cb
+        t0 = time.perf_counter()
+        exact = O.batch_fd(sb.node_off, sb.depz, sb.vs, sb.per_off, sb.periods, sb.minthk,
+                           exact=True)
+        plain = _run_sub_batch(torch, dev, L, _lib, sb, _lib.FORM_PLAIN)
+        acc = accuracy_block(sb, gpu_sample, ora, exact, plain)
+        acc["sample"] = (f"the cpu_baseline's {sb.ncol} columns; the adjoint form's outputs from "
+                         f"the full-batch step, the plain form run on those columns alone; "
+                         f"exact differences {time.perf_counter() - t0:.1f} s")
+        line["accuracy"] = acc
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def _gather_columns(torch, dev, b, idx, sen_off, ls_off, pv, sen, lsen, status):
+    """Host copies of the outputs of columns idx (batch layout, in order)."""
+    rng = lambda off: np.concatenate([np.arange(off[c], off[c + 1]) for c in idx])  # noqa: E731
+    take = lambda t, i: t.index_select(0, torch.from_numpy(i).to(dev)).cpu().numpy()  # noqa: E731
+    ip, isn, il = rng(b.per_off), rng(sen_off), rng(ls_off)
+    return {"pv": take(pv, ip), "sen_vs": take(sen[0], isn), "sen_vp": take(sen[1], isn),
+            "sen_rho": take(sen[2], isn), "lsen": take(lsen, il),
+            "status": take(status, idx.astype(np.int64))}
+
+
+def _run_sub_batch(torch, dev, L, _lib, sb, form):
+    """One dazi_dk_batch_dev call on a small batch; host copies of its
+    outputs (kernels, no Lsen_Gsc)."""
+    from dazi_current_release_b200.batch import output_offsets
+    sen_off, _ = output_offsets(sb.node_off, sb.per_off)
+    T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    d = [T(sb.node_off), T(sb.depz), T(sb.vs), T(sb.per_off), T(sb.periods), T(sen_off)]
+    pv = torch.zeros(sb.column_periods, dtype=torch.float64, device=dev)
+    sen = [torch.zeros(int(sen_off[-1]), dtype=torch.float64, device=dev) for _ in range(3)]
+    st = torch.zeros(sb.ncol, dtype=torch.int32, device=dev)
+    P = lambda x: ctypes.c_void_p(x.data_ptr())  # noqa: E731
+    _lib.check(L.dazi_dk_batch_dev(sb.ncol, P(d[0]), P(d[1]), P(d[2]), None, None, P(d[3]),
+                                   P(d[4]), ctypes.c_float(sb.minthk), P(pv), P(d[5]),
+                                   P(sen[0]), P(sen[1]), P(sen[2]), None, None, form, P(st),
+                                   ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)))
+    torch.cuda.synchronize(dev)
+    return {"pv": pv.cpu().numpy(), "sen_vs": sen[0].cpu().numpy(),
+            "sen_vp": sen[1].cpu().numpy(), "sen_rho": sen[2].cpu().numpy(),
+            "status": st.cpu().numpy()}
 
 
 def main():

@@ -73,6 +73,10 @@ int or_batch(long ncols, const long *node_off, const float *depz, const float *v
              const long *per_off, const double *periods, float minthk, double *pv,
              const long *sen_off, double *svs, double *svp, double *srh, const long *ls_off,
              float *lsen, int nthreads);
+int or_batch_fd(long ncols, const long *node_off, const float *depz, const float *vs_all,
+                const long *per_off, const double *periods, float minthk, double *pv,
+                const long *sen_off, double *svs, double *svp, double *srh, int precision,
+                double tol, float dln, int *status, int nthreads);
 long or_grows(int nvx, int nvz, int nz, int K, const float *vels, const double *svs,
               const double *svp, const double *srh, const float *lsen, long nrays,
               const int *ray_period, const int *ray_id, const long *cell_off, const int *cell,

@@ -89,6 +89,10 @@ def lib():
         L.or_batch.argtypes = [ctypes.c_long, _i64p, _f32p, _f32p, _i64p, _f64p, ctypes.c_float,
                                _f64p, _i64p, _f64p, _f64p, _f64p, _i64p, _f32p, ctypes.c_int]
         L.or_batch.restype = ctypes.c_int
+        L.or_batch_fd.argtypes = [ctypes.c_long, _i64p, _f32p, _f32p, _i64p, _f64p,
+                                  ctypes.c_float, _f64p, _i64p, _f64p, _f64p, _f64p, ctypes.c_int,
+                                  ctypes.c_double, ctypes.c_float, _i32p, ctypes.c_int]
+        L.or_batch_fd.restype = ctypes.c_int
         L.or_grows.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f64p,
                                _f64p, _f64p, _f32p, ctypes.c_long, _i32p, _i32p, _i64p, _i32p,
                                _f32p, _f32p, _f32p, ctypes.c_float, ctypes.c_long, _f32p, _i32p,
@@ -332,6 +336,35 @@ def batch(node_off, depz, vs, per_off, periods, minthk, kernels=True, lsen=True,
         raise RuntimeError("oracle batch failed")
     return dict(pv=pv, sen_vs=sen[0], sen_vp=sen[1], sen_rho=sen[2], lsen=ls,
                 sen_off=sen_off, ls_off=ls_off)
+
+
+def batch_fd(node_off, depz, vs, per_off, periods, minthk, exact=False, tol=None, dln=None,
+             nthreads=0):
+    """Vs-type kernels of a ragged batch: the reference's arithmetic, or
+    (exact=True) the exact-model checker (double model, unrounded roots, tol
+    1e-13 and dln 1e-4 unless given).  Returns pv, sen_vs, sen_vp, sen_rho
+    in the batch layout, sen_off and status."""
+    node_off = np.ascontiguousarray(node_off, np.int64)
+    per_off = np.ascontiguousarray(per_off, np.int64)
+    nz = np.diff(node_off)
+    K = np.diff(per_off)
+    sen_off = np.concatenate([[0], np.cumsum(K * nz)]).astype(np.int64)
+    pv = np.zeros(int(per_off[-1]))
+    sen = [np.zeros(max(int(sen_off[-1]), 1)) for _ in range(3)]
+    st = np.zeros(max(node_off.size - 1, 1), np.int32)
+    tol = tol if tol is not None else (1e-13 if exact else 1e-6)
+    dln = dln if dln is not None else (1e-4 if exact else 0.01)
+    r = lib().or_batch_fd(node_off.size - 1, _p(node_off, _i64p),
+                          _p(np.ascontiguousarray(depz, np.float32), _f32p),
+                          _p(np.ascontiguousarray(vs, np.float32), _f32p), _p(per_off, _i64p),
+                          _p(np.ascontiguousarray(periods, np.float64), _f64p),
+                          ctypes.c_float(minthk), _p(pv, _f64p), _p(sen_off, _i64p),
+                          _p(sen[0], _f64p), _p(sen[1], _f64p), _p(sen[2], _f64p),
+                          2 if exact else 0, tol, ctypes.c_float(dln), _p(st, _i32p), nthreads)
+    if r != 0:
+        raise RuntimeError("oracle batch_fd failed")
+    return dict(pv=pv, sen_vs=sen[0], sen_vp=sen[1], sen_rho=sen[2], sen_off=sen_off,
+                status=st[:node_off.size - 1])
 
 
 def grows(nvx, nvz, vels, sen_vs, sen_vp, sen_rho, lsen, ray_period, ray_id, cell_off, cell, fdm,

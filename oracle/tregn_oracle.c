@@ -1097,6 +1097,37 @@ int or_batch(long ncols, const long *node_off, const float *depz, const float *v
     return bad ? -1 : 0;
 }
 
+/* Vs-type kernels of a ragged batch with a chosen arithmetic: precision 0
+ * is the reference's (real*4 model stores, sngl(c) roots, or_column_fd as
+ * or_batch uses it), 2 the checker's exact-model pipeline (double model,
+ * unrounded roots) with its own tol and dln.  status[c] as or_phase (first
+ * failing period, 1-based, or 0).  OpenMP over columns.                    */
+int or_batch_fd(long ncols, const long *node_off, const float *depz, const float *vs_all,
+                const long *per_off, const double *periods, float minthk, double *pv,
+                const long *sen_off, double *svs, double *svp, double *srh, int precision,
+                double tol, float dln, int *status, int nthreads)
+{
+    int bad = 0;
+#ifdef _OPENMP
+    if (nthreads < 1) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic) num_threads(nthreads) reduction(|:bad)
+#endif
+    for (long c = 0; c < ncols; ++c) {
+        const int nz = (int)(node_off[c + 1] - node_off[c]);
+        const int K = (int)(per_off[c + 1] - per_off[c]);
+        if (nz < 2 || nz > NL || K < 1 || K > NP) { bad |= 1; continue; }
+        const float *vs = vs_all + node_off[c];
+        float vp[NL], rho[NL];
+        or_brocher(nz, vs, vp, rho);
+        int st = or_column_fd(nz, vs, vp, rho, K, periods + per_off[c], 2, 0, depz + node_off[c],
+                              minthk, dln, dln, dln, tol, precision, pv + per_off[c],
+                              svs + sen_off[c], svp + sen_off[c], srh + sen_off[c], NULL);
+        if (st < 0) bad |= 1;
+        if (status) status[c] = st < 0 ? -1 : st;
+    }
+    return bad ? -1 : 0;
+}
+
 /* G rows of the LSMR system from the depth kernels, CalSurfG_parallel.f90
  * :2363-2400 (iso_phase_only, use_aniso_active): for each ray (a data row,
  * id ray_id[r], period index ray_period[r]) and each of its model cells

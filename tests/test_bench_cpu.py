@@ -8,7 +8,7 @@ import subprocess
 import sys
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-ARGS = ["--impl", "reference", "--steps", "1", "--warmup", "1", "--cpu-sample-s", "0.3",
+ARGS = ["--impl", "reference", "--steps", "2", "--warmup", "1", "--cpu-cols-per-thread", "1",
         "--realisations", "1"]
 
 
@@ -25,6 +25,9 @@ def _check(line):
     assert line["e2e"] == {"value": line["value"], "unit": line["unit"],
                            "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}
     assert line["config"]["workload"] == "config3"
+    # the same config keys as our arm's line (the l2 note included)
+    assert {"columns", "column_periods", "minthk", "parallelism", "l2"} <= set(line["config"])
+    assert line["steps"] == 2 and line["ms_per_step"] > 0
 
 
 def test_reference_arm_one_process():
@@ -61,3 +64,43 @@ def test_our_arm_fails_loudly_without_a_gpu():
                        capture_output=True, text=True, timeout=600, env=env)
     assert r.returncode != 0
     assert _lines(r.stdout) == []
+
+
+def test_accuracy_block_bookkeeping():
+    """bench.py's accuracy block on CPU data: the oracle's own outputs as the
+    'library' outputs give zero errors and full identity counts; a planted
+    error in one column's kernels and one phase velocity shows up."""
+    sys.path.insert(0, ROOT)
+    import numpy as np
+    import bench
+    from oracle import oracle as O
+    from dazi_current_release_b200 import synthetic as S
+    b = S.config3(realisations=1, columns=60)
+    idx = bench.sample_columns(b, 6, 0)
+    sb = bench.sub_batch(b, idx)
+    for j, c in enumerate(idx):
+        d, v, p = b.column(int(c))
+        d2, v2, p2 = sb.column(j)
+        assert np.array_equal(d, d2) and np.array_equal(v, v2) and np.array_equal(p, p2)
+    ora = O.batch(sb.node_off, sb.depz, sb.vs, sb.per_off, sb.periods, sb.minthk)
+    exact = O.batch_fd(sb.node_off, sb.depz, sb.vs, sb.per_off, sb.periods, sb.minthk,
+                       exact=True)
+    gpu = {k: ora[k].copy() for k in ("pv", "sen_vs", "sen_vp", "sen_rho", "lsen")}
+    gpu["status"] = exact["status"].copy()
+    acc = bench.accuracy_block(sb, gpu, ora, exact, dict(gpu))
+    assert acc["pv_max_rel_err"] == 0.0 and acc["pv_bit_identical"] == sb.column_periods
+    assert acc["status_equal_columns"] == sb.ncol
+    assert acc["fundamental_mode_identity_columns"] == sb.ncol
+    assert acc["lsen_worst_column_rel_l2"] == 0.0
+    # the reference's FD kernels against the exact derivative: within its A/B gate
+    for n, v in acc["adjoint_kernels_vs_exact_worst_column_rel_l2"].items():
+        assert 0.0 < v <= 3e-3, (n, v)
+    assert acc["plain_form"]["kernel_entries_bit_identical"] == acc["plain_form"]["kernel_entries"]
+    # planted errors
+    gpu["pv"][sb.per_off[2]] *= 1.0 + 3e-6
+    gpu["sen_vs"][:] = exact["sen_vs"]
+    acc = bench.accuracy_block(sb, gpu, ora, exact, None)
+    assert 2e-6 < acc["pv_max_rel_err"] < 4e-6
+    assert acc["fundamental_mode_identity_columns"] == sb.ncol - 1
+    assert acc["adjoint_kernels_vs_exact_worst_column_rel_l2"]["sen_vs"] == 0.0
+    assert "plain_form" not in acc
