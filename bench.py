@@ -16,7 +16,9 @@ ragged batch entries dazi_dk_batch_dev / dazi_dk_batch.  The grid workloads
 dazi_dk_fused_dev / dazi_dk_fused.
 
 value      device-timed throughput of the chosen form (--form, default the
-           adjoint form) on the whole batch, inputs resident in HBM: a plan
+           adjoint form; --root brent: each period's bracket, the reference's
+           getsol scan, refined by Brent's method, DAZI_FORM_FAST_ROOT) on the
+           whole batch, inputs resident in HBM: a plan
            (dazi_dk_plan_*: structure bound once, kernel variants autotuned,
            each step one CUDA-graph launch) on torch's stream, CUDA events per
            step, L2 flushed between steps outside the timed events; the
@@ -27,11 +29,13 @@ same_columns  both forms timed the same way on the first --plain-cols
 e2e        the same stage through the host C-ABI entry with pinned host
            buffers: host->device inputs and device->host outputs every step
 roofline   FP64 CUDA-core bound of the dominant kernel (per-phase CUDA events
-           inside the library): root search 180 FP64 flops per layer per
-           secular evaluation (evaluations counted by the kernel); adjoint and
-           Gc/Gs sweeps the FP64 operations per layer item counted by ncu
-           (profiles/kernel_work.json) x the layer items of the call; peak the
-           FP64 FMA rate measured live by dazi_dk_fp64_peak
+           inside the library): algorithmic flops = root search 180 per layer
+           of each of the reference's secular evaluations (E_ref, counted by a
+           run of the reference's search), adjoint and Gc/Gs sweeps 180 x 2 per
+           layer item; pipe_frac from the FP64 operations ncu counts as executed
+           (profiles/kernel_work.json); peak the FP64 FMA rate measured live by
+           dazi_dk_fp64_peak
+accuracy   errors on the cpu_baseline's sampled columns against the oracle
 cpu_baseline  the CPU oracle (C restatement of the reference Fortran, OpenMP
            over columns) on a bounded sample of the same workload
 
@@ -74,6 +78,9 @@ def parse():
     p.add_argument("--plain-cols", type=int, default=25000,
                    help="ragged workload: columns the plain form is timed on")
     p.add_argument("--form", default="adjoint", choices=["plain", "adjoint"])
+    p.add_argument("--root", default="brent", choices=["brent", "reference"],
+                   help="adjoint form: refine each period's bracket by Brent's method "
+                        "(DAZI_FORM_FAST_ROOT) or by the reference's nevill()")
     p.add_argument("--no-other-form", action="store_true")
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
     p.add_argument("--cpu-cols-per-thread", type=int, default=CPU_COLS_PER_THREAD,
@@ -352,9 +359,12 @@ def accuracy_block(sb, gpu, ora, exact, plain):
         if den > 0:
             ls_worst = max(ls_worst, float(np.linalg.norm((g - r).astype(np.float64)) / den))
     names = ("sen_vs", "sen_vp", "sen_rho")
+    ex_ok = ok & (exact["pv"] > 0)
     acc = {
         "columns": int(K.size), "column_periods": int(sb.column_periods),
         "pv_max_rel_err": float(rel.max()) if rel.size else 0.0,
+        "pv_max_rel_err_vs_exact_root": float(np.abs(gpu["pv"][ex_ok] / exact["pv"][ex_ok] - 1.0).max())
+        if ex_ok.any() else 0.0,
         "pv_bit_identical": int(np.count_nonzero(gpu["pv"] == pv_ref)),
         "status_equal_columns": int(same_status.sum()),
         "fundamental_mode_identity_columns": ident,
@@ -459,6 +469,9 @@ def main_ragged(args, ws, rank, local):
     ncol = b.ncol
     sen_off, ls_off = output_offsets(b.node_off, b.per_off)
     form = _lib.FORM_PLAIN if args.form == "plain" else _lib.FORM_ADJOINT
+    fast = form == _lib.FORM_ADJOINT and args.root == "brent"
+    if fast:
+        form |= _lib.FORM_FAST_ROOT
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
     d_node, d_per, d_dep, d_vs = T(b.node_off), T(b.per_off), T(b.depz), T(b.vs)
     d_periods, d_senoff, d_lsoff = T(b.periods), T(sen_off), T(ls_off)
@@ -499,7 +512,7 @@ def main_ragged(args, ws, rank, local):
     ns_cp = int(b.per_off[ns])
     sample = {}
     if not args.no_other_form:
-        for fname, f in (("plain", _lib.FORM_PLAIN), ("adjoint", _lib.FORM_ADJOINT)):
+        for fname, f in (("plain", _lib.FORM_PLAIN), ("adjoint", form)):
             ms = _events_timed(step_fn(f, ns), 1 if f == _lib.FORM_PLAIN else 2, 1, dev, stream,
                                flush, ws)
             sample[fname] = {"value": ws * ns_cp / (ms * 1e-3), "ms_per_step": ms}
@@ -516,7 +529,7 @@ def main_ragged(args, ws, rank, local):
         from dazi_current_release_b200.plan import BatchPlan
         t0 = time.perf_counter()
         plan = BatchPlan(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk, tune=True,
-                         scan32=bool(form & _lib.FORM_SCAN_FP32), device=dev)
+                         scan32=bool(form & _lib.FORM_SCAN_FP32), fast_root=fast, device=dev)
         plan_setup_s = time.perf_counter() - t0
         with ClockSampler(local) as clk:
             ms_per_step = _events_timed(plan.run, args.steps, args.warmup, dev, stream, flush, ws)
@@ -547,12 +560,34 @@ def main_ragged(args, ws, rank, local):
         gpu_sample = _gather_columns(torch, dev, b, acc_cols, sen_off, ls_off, pv, sen, lsen,
                                      status)
     scan32 = None
-    if form == _lib.FORM_ADJOINT:
-        pv64 = pv.clone()
+    root_search = None
+    if form & _lib.FORM_ADJOINT:
+        pv_t, st_t = pv.clone(), status.clone()
+        if fast:
+            # the reference's search on the same batch: its evaluation count
+            # (E_ref of the roofline) and the mode check of every root
+            step_fn(_lib.FORM_ADJOINT, ncol)()
+            ph_ref = _lib.last_timing()
+            ev_ref, layer_evals_ref, _ = work()
+            ok = pv > 0
+            rel = torch.where(ok, (pv_t / torch.where(ok, pv, 1.0) - 1.0).abs(), 0.0)
+            root_search = {
+                "refinement": "brent (DAZI_FORM_FAST_ROOT): the reference's getsol scan, Brent "
+                              "to 1e-10 c",
+                "evals_per_column_period": evals / ncp,
+                "reference_evals_per_column_period": ev_ref / ncp,
+                "root_ms": phases.get("root"), "reference_root_ms": ph_ref.get("root"),
+                "columns_same_status": int((st_t == status).sum().item()),
+                "columns": ncol,
+                "periods_same_root_presence": int(((pv_t > 0) == ok).sum().item()),
+                "max_rel_diff_vs_reference_search": float(rel.max().item()),
+                "within_reference_tolerance": int((rel <= 1e-6 + 1.3e-7).sum().item()),
+                "column_periods": ncp}
+            layer_evals = layer_evals_ref
         step_fn(form | _lib.FORM_SCAN_FP32, ncol)()
         ph32 = _lib.last_timing()
         scan32 = {"root_ms_fp64_scan": phases.get("root"), "root_ms_fp32_scan": ph32.get("root"),
-                  "identical_roots": bool(torch.equal(pv64, pv))}
+                  "identical_roots": bool(torch.equal(pv_t, pv))}
     _lib.check(L.dazi_dk_set_timing(0))
 
     # end to end: host C-ABI dazi_dk_batch with pinned host buffers
@@ -661,8 +696,7 @@ def main_ragged(args, ws, rank, local):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": dict(ragged_config(args, b),
-                       l2="inputs and outputs far larger than L2; 256 MiB flush write between "
-                          "steps outside the timed events"),
+                       root_refinement="brent" if fast else "reference nevill"),
         "e2e": {"value": job_cp / e2e_s, "unit": "column-periods/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
         "roofline": roof,
@@ -673,6 +707,8 @@ def main_ragged(args, ws, rank, local):
     }
     if scan32:
         line["root_scan"] = scan32
+    if root_search:
+        line["root_search"] = root_search
     if sample:
         line["same_columns"] = dict(sample, columns=ns, column_periods=ns_cp,
                                     adjoint_over_plain=sample["adjoint"]["value"] /

@@ -29,6 +29,7 @@ FORM_ADJOINT = 1
 FORM_SCAN_FP32 = 2      # flag: FP32 coarse scan verified in FP64 (default: all FP64)
 FORM_LOVE = 4           # flag: Love waves (surfdisp96 iwave = 1), plain or adjoint form
 FORM_GROUP = 8          # flag: group velocity (igr > 0), plain or adjoint form
+FORM_FAST_ROOT = 16     # flag: Brent refinement of the reference's bracket (Rayleigh phase)
 
 # every symbol include/dazi_dk.h declares
 EXPORTS = (

@@ -167,8 +167,14 @@ constexpr int kWaveFlags = DAZI_FORM_LOVE | DAZI_FORM_GROUP;
 
 int check_form(int form, bool lsen)
 {
-    constexpr int known = DAZI_FORM_ADJOINT | DAZI_FORM_SCAN_FP32 | kWaveFlags;
+    constexpr int known = DAZI_FORM_ADJOINT | DAZI_FORM_SCAN_FP32 | kWaveFlags | DAZI_FORM_FAST_ROOT;
     if (form & ~known) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
+    if (form & DAZI_FORM_FAST_ROOT) {
+        if (form & kWaveFlags) {
+            set_err("the Brent root refinement runs with Rayleigh phase velocity only (form %d)", form);
+            return DAZI_ERR_BADARG;
+        }
+    }
     if (form & kWaveFlags) {
         if (form & DAZI_FORM_SCAN_FP32) {
             set_err("the FP32 scan runs with Rayleigh phase velocity only (form %d)", form);
@@ -446,6 +452,14 @@ int run_root(const Tables& T, const double* per, const StageOut& o, int form, bo
         if (ifunc == 1 && grp) root_kernel<128, 0, 1, true><<<nb, 128, 0, st>>>(a);
         else if (ifunc == 1) root_kernel<128, 0, 1, false><<<nb, 128, 0, st>>>(a);
         else root_kernel<128, 0, 2, true><<<nb, 128, 0, st>>>(a);
+    } else if (form & DAZI_FORM_FAST_ROOT) {
+        const int bt = cfg.root_bt, mb = cfg.root_minb;
+        const unsigned nb = (unsigned)((T.ncols + bt - 1) / bt);
+        if (bt == 64 && mb == 10) root_kernel<64, 10, 2, false, true><<<nb, 64, 0, st>>>(a);
+        else if (bt == 64) root_kernel<64, 0, 2, false, true><<<nb, 64, 0, st>>>(a);
+        else if (bt == 256) root_kernel<256, 0, 2, false, true><<<nb, 256, 0, st>>>(a);
+        else if (mb == 5) root_kernel<128, 5, 2, false, true><<<nb, 128, 0, st>>>(a);
+        else root_kernel<128, 0, 2, false, true><<<nb, 128, 0, st>>>(a);
     } else {
         const int bt = cfg.root_bt, mb = cfg.root_minb;
         const unsigned nb = (unsigned)((T.ncols + bt - 1) / bt);

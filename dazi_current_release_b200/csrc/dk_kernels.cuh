@@ -158,9 +158,10 @@ __global__ void prep_tasks_kernel(long long ntiles, const long long* tile_tasks,
                                   const long long* tile_tbase, int2* tasks);
 __global__ void prep_build_kernel(ColSrc src, PrepOut o, Tables T, const int* sorted_col,
                                   const long long* tile_tbase);
-// Rayleigh phase: (64|128|256, 0), (128, 5), (64, 10); the other wave and
-// velocity types (IFUNC 1 Love / 2 Rayleigh, GROUP): (128, 0) only.
-template <int BT, int MINB, int IFUNC = 2, bool GROUP = false>
+// Rayleigh phase: (64|128|256, 0), (128, 5), (64, 10), each with the
+// reference's nevill() refinement or (FAST) Brent's; the other wave and
+// velocity types (IFUNC 1 Love / 2 Rayleigh, GROUP): (128, 0), nevill().
+template <int BT, int MINB, int IFUNC = 2, bool GROUP = false, bool FAST = false>
 __global__ void root_kernel(RootArgs a);
 template <int MINB> __global__ void adjoint_kernel(AdjArgs a);    // MINB in {2, 3, 4}
 template <int MINB> __global__ void adjoint_love_kernel(AdjArgs a);   // MINB = 3

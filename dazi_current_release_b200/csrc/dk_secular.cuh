@@ -380,10 +380,22 @@ struct HasGroupRoots<O, decltype((void)std::declval<O&>().group_roots(0, 0.0, 0.
     static constexpr bool value = true;
 };
 
-template <bool GROUP = false>
+// FAST (DAZI_FORM_FAST_ROOT, Rayleigh/Love phase velocity): the scan is
+// getsol's, point for point, so the bracket and with it the mode are the
+// reference's; the bracket is then refined by Brent's method (inverse
+// quadratic interpolation / secant / bisection; R. P. Brent, Algorithms for
+// Minimization without Derivatives, 1973, ch. 4) to kFastRootTol * c instead
+// of nevill()'s hybrid to 1e-6 * c.  The root is the exact one to that
+// tolerance (the reference's lies anywhere in its final 1e-6 * c bracket);
+// the next period's scan starts 1.5 dc below it.  About 3.5 instead of 12
+// refinement evaluations per period on uneven columns.
+constexpr double kFastRootTol = 1.0e-10;
+
+template <bool GROUP = false, bool FAST = false>
 struct RootSM {
+    static_assert(!(GROUP && FAST), "the Brent refinement serves phase velocity");
     enum Phase : int { START = 0, GS_FIRST, GS_SCAN, VER1, VER2, NEV_A, NEV_B, NEV_CD, DONE,
-                       GR_START };
+                       GR_START, BRENT_INIT, BRENT };
     // model constants
     double cc, cm, dc, cmax, tol;
     float betmx;
@@ -403,6 +415,8 @@ struct RootSM {
     bool second;
     float t1a, t1b;
     double cph, cph_t;
+    // Brent (FAST): the last step and the one before
+    double bd, be;
 
     __device__ void init(double cc_, float betmx_, int kmax_, double tol_, bool scan32 = false)
     {
@@ -457,6 +471,7 @@ struct RootSM {
                     // bracketed: both end values in FP64 before nevill()
                     if (!d1x) { phase = VER1; return request(c1); }
                     if (!d2x) { phase = VER2; return request(c2); }
+                    if constexpr (FAST) { phase = BRENT_INIT; continue; }
                     return begin_nevill();
                 }
                 c1 = c2;
@@ -474,13 +489,30 @@ struct RootSM {
                 del1 = F;
                 d1x = true;
                 if (!d2x) { phase = VER2; return request(c2); }
+                if constexpr (FAST) { phase = BRENT_INIT; continue; }
                 return begin_nevill();
             }
             case VER2: {
                 if (fsign1(F) != fsign1(del2)) { restart_fp64(); continue; }
                 del2 = F;
                 d2x = true;
+                if constexpr (FAST) { phase = BRENT_INIT; continue; }
                 return begin_nevill();
+            }
+            case BRENT_INIT: {
+                // a = c1 (del1), b = c2 (del2): getsol's bracket; c = a
+                c3 = c1; del3 = del1;
+                bd = c2 - c1; be = bd;
+                nctrl = 0;
+                if (brent_iter(out)) return true;
+                if (phase != DONE) continue;
+                return false;
+            }
+            case BRENT: {
+                del2 = F;
+                if (brent_iter(out)) return true;
+                if (phase != DONE) continue;
+                return false;
             }
             case NEV_A:
             case NEV_CD: {
@@ -648,6 +680,53 @@ struct RootSM {
         return true;
     }
 
+    // One step of Brent's method on the bracket [b, c] = [c2, c3] with the
+    // previous iterate a = c1 (values del2, del3, del1).  Returns true when a
+    // new evaluation was requested; otherwise the period finished (phase
+    // START) or the model failed (phase DONE).
+    template <class Out>
+    __device__ bool brent_iter(Out& out)
+    {
+        if ((del2 > 0.0) == (del3 > 0.0)) { c3 = c1; del3 = del1; bd = c2 - c1; be = bd; }
+        if (fabs(del3) < fabs(del2)) {
+            c1 = c2; c2 = c3; c3 = c1;
+            del1 = del2; del2 = del3; del3 = del1;
+        }
+        const double tol1 = 2.0 * 2.220446049250313e-16 * fabs(c2) + 0.5 * kFastRootTol * fabs(c2);
+        const double xm = 0.5 * (c3 - c2);
+        if (fabs(xm) <= tol1 || del2 == 0.0 || ++nctrl >= 100) {
+            // getsol's acceptance test, then the next period
+            if (c2 > (double)betmx) { out(k, 0.0, 0.0, evals); fail(); return false; }
+            out(k, c2, c2, evals);
+            cprev = c2;
+            ++k;
+            p64 = false;
+            phase = START;
+            return false;
+        }
+        if (fabs(be) >= tol1 && fabs(del1) > fabs(del2)) {
+            const double sr = del2 / del1;
+            double p, q;
+            if (c1 == c3) {
+                p = 2.0 * xm * sr;
+                q = 1.0 - sr;
+            } else {
+                const double qa = del1 / del3, r = del2 / del3;
+                p = sr * (2.0 * xm * qa * (qa - r) - (c2 - c1) * (r - 1.0));
+                q = (qa - 1.0) * (r - 1.0) * (sr - 1.0);
+            }
+            if (p > 0.0) q = -q; else p = -p;
+            if (2.0 * p < fmin(3.0 * xm * q - fabs(tol1 * q), fabs(be * q))) { be = bd; bd = p / q; }
+            else { bd = xm; be = bd; }
+        } else {
+            bd = xm; be = bd;
+        }
+        c1 = c2; del1 = del2;
+        c2 += fabs(bd) > tol1 ? bd : (xm > 0.0 ? tol1 : -tol1);
+        phase = BRENT;
+        return request(c2);
+    }
+
     // Bracket update, convergence test and choice of the next point (the
     // body of the nevill loop after c3 is known).  Returns true when a new
     // evaluation was requested; otherwise the period finished (phase START)
@@ -718,14 +797,14 @@ __device__ void scan_start(LayerF layerf, int mmax, double& cc, float& betmx)
 // (dltar1); GROUP selects group velocity.  The FP32 scan applies to
 // Rayleigh phase velocity only.  Returns the 0-based first failing period
 // or -1.
-template <int IFUNC = 2, bool GROUP = false, class M, class Out>
+template <int IFUNC = 2, bool GROUP = false, bool FAST = false, class M, class Out>
 __device__ int solve_model_warp(bool active, const M& mdl, int mmax, double cc, float betmx,
                                 const double* periods, int kmax, double tol, Out& out,
                                 int* total_evals = nullptr, bool scan32 = false)
 {
     static_assert(IFUNC == 1 || IFUNC == 2, "ifunc is 1 (Love) or 2 (Rayleigh)");
     constexpr bool kScan32 = M::kF32 && IFUNC == 2 && !GROUP;
-    RootSM<GROUP> sm;
+    RootSM<GROUP, FAST> sm;
     sm.init(cc, betmx, kmax, tol, kScan32 && scan32);
     bool want = active ? sm.next(0.0, periods, out) : false;
     int tot = want ? 1 : 0;

@@ -288,7 +288,7 @@ struct RootOut {
 // autotuner picks one of the instantiations.  IFUNC / GROUP: Love or
 // Rayleigh, group or phase velocity (the tables then hold the matching
 // density flattening).
-template <int BT, int MINB, int IFUNC, bool GROUP>
+template <int BT, int MINB, int IFUNC, bool GROUP, bool FAST>
 __global__ void __launch_bounds__(BT, MINB)
 root_kernel(RootArgs a)
 {
@@ -308,8 +308,8 @@ root_kernel(RootArgs a)
         scan_start([&](int m) { return lf[(long long)m * TILE]; }, M.rmax, cc, betmx);
     }
     int nev = 0;
-    const int fk = solve_model_warp<IFUNC, GROUP>(active, mdl, M.rmax, cc, betmx, per, M.K, a.tol,
-                                                  out, &nev, a.scan32 != 0);
+    const int fk = solve_model_warp<IFUNC, GROUP, FAST>(active, mdl, M.rmax, cc, betmx, per, M.K,
+                                                        a.tol, out, &nev, a.scan32 != 0);
     if (active && a.status) a.status[M.status_i] = fk < 0 ? 0 : fk + 1;
     if (a.nevals) {
         const unsigned long long w = __reduce_add_sync(0xffffffffu, (unsigned)nev);
@@ -318,13 +318,19 @@ root_kernel(RootArgs a)
     }
 }
 
-template __global__ void root_kernel<64, 0, 2, false>(RootArgs);
-template __global__ void root_kernel<128, 0, 2, false>(RootArgs);
-template __global__ void root_kernel<256, 0, 2, false>(RootArgs);
-template __global__ void root_kernel<128, 5, 2, false>(RootArgs);
-template __global__ void root_kernel<64, 10, 2, false>(RootArgs);
-template __global__ void root_kernel<128, 0, 2, true>(RootArgs);
-template __global__ void root_kernel<128, 0, 1, false>(RootArgs);
-template __global__ void root_kernel<128, 0, 1, true>(RootArgs);
+template __global__ void root_kernel<64, 0, 2, false, false>(RootArgs);
+template __global__ void root_kernel<128, 0, 2, false, false>(RootArgs);
+template __global__ void root_kernel<256, 0, 2, false, false>(RootArgs);
+template __global__ void root_kernel<128, 5, 2, false, false>(RootArgs);
+template __global__ void root_kernel<64, 10, 2, false, false>(RootArgs);
+template __global__ void root_kernel<128, 0, 2, true, false>(RootArgs);
+template __global__ void root_kernel<128, 0, 1, false, false>(RootArgs);
+template __global__ void root_kernel<128, 0, 1, true, false>(RootArgs);
+// the Brent refinement of the bracket (DAZI_FORM_FAST_ROOT), Rayleigh phase
+template __global__ void root_kernel<64, 0, 2, false, true>(RootArgs);
+template __global__ void root_kernel<128, 0, 2, false, true>(RootArgs);
+template __global__ void root_kernel<256, 0, 2, false, true>(RootArgs);
+template __global__ void root_kernel<128, 5, 2, false, true>(RootArgs);
+template __global__ void root_kernel<64, 10, 2, false, true>(RootArgs);
 
 }  // namespace dk

@@ -75,6 +75,16 @@ extern "C" {
  * returns DAZI_ERR_BADARG. */
 #define DAZI_FORM_LOVE     4
 #define DAZI_FORM_GROUP    8
+/* flag, OR-ed into the form: the root search (adjoint form, phase-velocity-
+ * or Lsen-only calls, plans) keeps the reference's getsol scan, point for
+ * point, so each period's bracket and mode are the reference's, but refines
+ * the bracket by Brent's method to 1e-10 c instead of nevill() to 1e-6 c
+ * (about 3.5 instead of 12 evaluations per period).  pvRc is then the
+ * float32 of the exact root, within the reference's own 1e-6 c of its
+ * value; the default search reproduces its value bit for bit.  Rayleigh
+ * phase velocity; with DAZI_FORM_LOVE or DAZI_FORM_GROUP it returns
+ * DAZI_ERR_BADARG.  The plain form's finite differences ignore it. */
+#define DAZI_FORM_FAST_ROOT 16
 
 /* Replaces depthkernel() of code/src_inv_iso_joint/CalSurfG.f90:1-15
  * (default_fortran_fd backend, CalSurfG.f90:86-107), for the 1-based column

@@ -115,6 +115,7 @@ typedef struct {
     double del1st;        /* SAVE del1st of getsol()                         */
     double tol;           /* nevill relative tolerance (reference: 1e-6)     */
     long evals;           /* secular-function evaluations                    */
+    long scan_evals;      /* of which getsol's bracket scan (checker counter) */
 } sd_model;
 
 /* A store into a real*4 model array; identity in exact-model mode. */
@@ -462,6 +463,7 @@ static int sd_getsol(sd_model *m, double t1, double *c1p, double clow,
 {
     double c1 = *c1p, c2, del1, del2;
     double omega = TWOPI / t1;
+    const long e_in = m->evals;
     del1 = sd_dltar(m, omega / c1, omega, ifunc);
     if (ifirst == 1) m->del1st = del1;
     double plmn = fsign1(m->del1st) * fsign1(del1);
@@ -480,9 +482,10 @@ static int sd_getsol(sd_model *m, double t1, double *c1p, double clow,
         if (fsign1(del1) != fsign1(del2)) break;
         c1 = c2;
         del1 = del2;
-        if (c1 < cm) { *c1p = c1; return -1; }
-        if (c1 >= ((double)betmx + dc)) { *c1p = c1; return -1; }
+        if (c1 < cm) { *c1p = c1; m->scan_evals += m->evals - e_in; return -1; }
+        if (c1 >= ((double)betmx + dc)) { *c1p = c1; m->scan_evals += m->evals - e_in; return -1; }
     }
+    m->scan_evals += m->evals - e_in;
     c1 = sd_nevill(m, t1, c1, c2, del1, del2, ifunc);
     *c1p = c1;
     if (c1 > (double)betmx) return -1;
@@ -498,7 +501,8 @@ static int sd_getsol(sd_model *m, double t1, double *c1p, double clow,
 static int sd_run(const double *thkm, const double *vpm, const double *vsm,
                   const double *rhom, int nlayer, int iflsph, int iwave, int mode,
                   int igr, int kmax, const double *t, double *cg, double tol,
-                  int model_f32, int round_f32, int *evals_per_period)
+                  int model_f32, int round_f32, int *evals_per_period,
+                  int *scan_per_period)
 {
     if (nlayer < 1 || nlayer > NL || kmax < 1 || kmax > NP) return -1;
     sd_model mdl;
@@ -507,6 +511,7 @@ static int sd_run(const double *thkm, const double *vpm, const double *vsm,
     m->f32 = model_f32 ? 1 : 0;
     m->tol = tol;
     m->evals = 0;
+    m->scan_evals = 0;
     m->del1st = 0.0;
     for (int i = 0; i < nlayer; ++i) {
         m->b[i] = vsm[i]; m->a[i] = vpm[i]; m->d[i] = thkm[i]; m->rho[i] = rhom[i];
@@ -576,8 +581,9 @@ static int sd_run(const double *thkm, const double *vpm, const double *vsm,
                     c1 = c[k - 2] - onea * dc;
                     clow = cm;
                 }
-                long e0 = m->evals;
+                long e0 = m->evals, s0 = m->scan_evals;
                 int iret = sd_getsol(m, t1, &c1, clow, dc, cm, betmx, ifunc, ifirst);
+                if (scan_per_period) scan_per_period[k - 1] = (int)(m->scan_evals - s0);
                 if (iret == -1) {
                     if (evals_per_period) evals_per_period[k - 1] = (int)(m->evals - e0);
                     failed = 1;
@@ -596,6 +602,7 @@ static int sd_run(const double *thkm, const double *vpm, const double *vsm,
                     c1 = 0.0;
                 }
                 if (evals_per_period) evals_per_period[k - 1] = (int)(m->evals - e0);
+                if (scan_per_period) scan_per_period[k - 1] = (int)(m->scan_evals - s0);
                 float cc0 = (float)c[k - 1];
                 float ccb = (float)c1;
                 if (igr == 0) {
@@ -619,6 +626,7 @@ static int sd_run(const double *thkm, const double *vpm, const double *vsm,
                 for (int i = k; i <= ie; ++i) {
                     cg[i - 1] = 0.0;
                     if (evals_per_period && i > k) evals_per_period[i - 1] = 0;
+                    if (scan_per_period && i > k) scan_per_period[i - 1] = 0;
                 }
             }
         }
@@ -636,7 +644,21 @@ int or_surfdisp96_ex(const float *thkm, const float *vpm, const float *vsm,
     for (int i = 0; i < nlayer; ++i) { d[i] = thkm[i]; a[i] = vpm[i]; b[i] = vsm[i]; r[i] = rhom[i]; }
     /* the reference model is real*4 whatever the output rounding */
     return sd_run(d, a, b, r, nlayer, iflsph, iwave, mode, igr, kmax, t, cg, tol, 1,
-                  round_f32, evals_per_period);
+                  round_f32, evals_per_period, NULL);
+}
+
+/* The same with the evaluation count of every period split: scan_per_period
+ * receives getsol's bracket-scan evaluations (the rest of evals_per_period
+ * are nevill's).  A checker counter; the arithmetic is or_surfdisp96_ex's. */
+int or_surfdisp96_split(const float *thkm, const float *vpm, const float *vsm,
+                        const float *rhom, int nlayer, int kmax, const double *t, double *cg,
+                        int *evals_per_period, int *scan_per_period)
+{
+    double d[NL], a[NL], b[NL], r[NL];
+    if (nlayer < 1 || nlayer > NL) return -1;
+    for (int i = 0; i < nlayer; ++i) { d[i] = thkm[i]; a[i] = vpm[i]; b[i] = vsm[i]; r[i] = rhom[i]; }
+    return sd_run(d, a, b, r, nlayer, 1, 2, 1, 0, kmax, t, cg, 1.0e-6, 1, 1, evals_per_period,
+                  scan_per_period);
 }
 
 /* Exact-model variant (checker): double model arrays, no real*4 stores. */
@@ -644,7 +666,8 @@ int or_surfdisp96_d(const double *thkm, const double *vpm, const double *vsm,
                     const double *rhom, int nlayer, int iflsph, int kmax,
                     const double *t, double *cg, double tol)
 {
-    return sd_run(thkm, vpm, vsm, rhom, nlayer, iflsph, 2, 1, 0, kmax, t, cg, tol, 0, 0, NULL);
+    return sd_run(thkm, vpm, vsm, rhom, nlayer, iflsph, 2, 1, 0, kmax, t, cg, tol, 0, 0, NULL,
+                  NULL);
 }
 
 int or_surfdisp96(const float *thkm, const float *vpm, const float *vsm,
@@ -728,7 +751,7 @@ int or_column_fd(int nz, const float *vs, const float *vp, const float *rho,
             if (rm_ < 0) return -2;                                                   \
         }                                                                             \
         st_ = sd_run(rthk, rvp, rvs, rrho, rm_, 1, iwave, 1, igr, kmax, periods, CG,  \
-                     tol, model_f32, out_f32, ev);                                    \
+                     tol, model_f32, out_f32, ev, NULL);                              \
         for (int k_ = 0; k_ < kmax; ++k_) tot += ev[k_];                              \
     } while (0)
     int st_ = 0;

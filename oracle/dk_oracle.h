@@ -32,6 +32,9 @@ int or_phase(int nx, int ny, int nz, const float *vel, const float *vp_in,
              const float *rho_in, double *pvRc, int iwave, int igr, int kmax,
              const double *tRc, const float *depz, float minthk, int nthreads,
              double tol, int round_f32, int *evals_cp, int *status_out);
+int or_surfdisp96_split(const float *thkm, const float *vpm, const float *vsm,
+                        const float *rhom, int nlayer, int kmax, const double *t, double *cg,
+                        int *evals_per_period, int *scan_per_period);
 int or_surfdisp96_d(const double *thkm, const double *vpm, const double *vsm,
                     const double *rhom, int nlayer, int iflsph, int kmax,
                     const double *t, double *cg, double tol);

@@ -83,6 +83,9 @@ def lib():
             L.or_ti_root_fd.argtypes = d7 + [ctypes.c_double] * 4 + [ctypes.c_int, _i32p, _i32p,
                                                                       _i32p, _f64p, ctypes.c_int]
             L.or_ti_root_fd.restype = ctypes.c_int
+        L.or_surfdisp96_split.argtypes = [_f32p] * 4 + [ctypes.c_int] * 2 + [_f64p, _f64p, _i32p,
+                                                                             _i32p]
+        L.or_surfdisp96_split.restype = ctypes.c_int
         L.or_surfdisp96_d.argtypes = [_f64p, _f64p, _f64p, _f64p, ctypes.c_int, ctypes.c_int,
                                       ctypes.c_int, _f64p, _f64p, ctypes.c_double]
         L.or_surfdisp96_d.restype = ctypes.c_int
@@ -146,6 +149,21 @@ def surfdisp96(thk, vp, vs, rho, periods, iwave=2, igr=0, mode=1, iflsph=1,
                                 thk.size, iflsph, iwave, mode, igr, t.size, _p(t, _f64p),
                                 _p(cg, _f64p), tol, int(round_f32), _p(ev, _i32p))
     return cg, st, ev
+
+
+def surfdisp96_split(thk, vp, vs, rho, periods):
+    """Rayleigh phase velocity (reference arithmetic) with the secular
+    evaluations of every period split: returns (cg, status, evals, scan)
+    where scan counts getsol's bracket scan and evals - scan nevill's."""
+    f = lambda x: np.ascontiguousarray(x, np.float32)  # noqa: E731
+    t = np.ascontiguousarray(periods, np.float64)
+    cg = np.zeros(t.size)
+    ev = np.zeros(t.size, np.int32)
+    sc = np.zeros(t.size, np.int32)
+    st = lib().or_surfdisp96_split(*[_p(f(x), _f32p) for x in (thk, vp, vs, rho)], len(thk),
+                                   t.size, _p(t, _f64p), _p(cg, _f64p), _p(ev, _i32p),
+                                   _p(sc, _i32p))
+    return cg, st, ev, sc
 
 
 def depthkernel(vel, depz, periods, minthk, vp=None, rho=None, iwave=2, igr=0,

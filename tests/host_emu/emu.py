@@ -38,10 +38,11 @@ def ti_batch(node_off, depz, vs, per_off, periods, minthk, pv):
     return rc, ls, ls_off
 
 
-def root_batch(node_off, depz, vs, per_off, periods, minthk, scan32=True, ifunc=2, group=False):
+def root_batch(node_off, depz, vs, per_off, periods, minthk, scan32=True, ifunc=2, group=False,
+               fast=False):
     """pv (sngl(c) as the library writes it; the group velocity when
     group), status and the number of secular evaluations of the root search
-    of a ragged batch; ifunc 1 Love, 2 Rayleigh."""
+    of a ragged batch; ifunc 1 Love, 2 Rayleigh; fast the Brent refinement."""
     P = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))  # noqa: E731
     node_off = np.ascontiguousarray(node_off, np.int64)
     per_off = np.ascontiguousarray(per_off, np.int64)
@@ -53,13 +54,14 @@ def root_batch(node_off, depz, vs, per_off, periods, minthk, scan32=True, ifunc=
                               P(np.ascontiguousarray(depz, np.float32), f32),
                               P(np.ascontiguousarray(vs, np.float32), f32), P(per_off, i64),
                               P(np.ascontiguousarray(periods, np.float64), f64), f32(minthk),
-                              int(scan32), int(ifunc), int(bool(group)), P(pv, f64),
+                              int(scan32), int(ifunc), int(bool(group)), int(bool(fast)),
+                              P(pv, f64),
                               P(st, ctypes.c_int), ctypes.byref(ev))
     return rc, pv, st, ev.value
 
 
 def adjoint_batch(node_off, depz, vs, per_off, periods, minthk, ifunc=2, group=False,
-                  drop_every=0):
+                  drop_every=0, fast=False):
     """Adjoint form of a ragged batch by the device code built for the host:
     rc, pv, status, (sen_vs, sen_vp, sen_rho) in the batch layout, sen_off,
     and the mask of (column, period) entries whose root at t1b was set to 0
@@ -80,7 +82,8 @@ def adjoint_batch(node_off, depz, vs, per_off, periods, minthk, ifunc=2, group=F
                                  P(np.ascontiguousarray(depz, np.float32), f32),
                                  P(np.ascontiguousarray(vs, np.float32), f32), P(per_off, i64),
                                  P(np.ascontiguousarray(periods, np.float64), f64), f32(minthk),
-                                 int(ifunc), int(bool(group)), int(drop_every), P(pv, f64),
+                                 int(ifunc), int(bool(group)), int(drop_every),
+                                 int(bool(fast)), P(pv, f64),
                                  P(st, ctypes.c_int), P(sen_off, i64), P(sen[0], f64),
                                  P(sen[1], f64), P(sen[2], f64), P(dropped, ctypes.c_ubyte))
     return rc, pv, st, sen, sen_off, dropped.astype(bool)

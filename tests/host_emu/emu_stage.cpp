@@ -94,13 +94,15 @@ ColSrc ragged_src(const long long* node_off, const float* depz, const float* vs,
 // column): pv[per_off[c] + k] (sngl(c), as the library writes it), status
 // per column, the secular evaluations in *evals.  scan32 selects the FP32
 // coarse scan; ifunc 1 (Love) / 2 (Rayleigh) and group select the
-// root_kernel instantiation the library launches for that form.
+// root_kernel instantiation the library launches for that form; fast the
+// Brent refinement (Rayleigh phase).
 extern "C" int emu_root_batch(long long ncols, const long long* node_off, const float* depz,
                               const float* vs, const long long* per_off, const double* periods,
-                              float minthk, int scan32, int ifunc, int group, double* pv,
-                              int* status, long long* evals)
+                              float minthk, int scan32, int ifunc, int group, int fast,
+                              double* pv, int* status, long long* evals)
 {
     if (ifunc != 1 && ifunc != 2) return -2;
+    if (fast && (ifunc != 2 || group)) return -2;
     const ColSrc src = ragged_src(node_off, depz, vs, per_off, minthk, ifunc);
     HostTables H;
     PrepOut po{nullptr, nullptr, nullptr};
@@ -113,7 +115,8 @@ extern "C" int emu_root_batch(long long ncols, const long long* node_off, const 
     for (long long s = 0; s < ncols; ++s) {
         blockIdx.x = (unsigned)(s / 128);
         threadIdx.x = (unsigned)(s % 128);
-        if (ifunc == 1 && group) root_kernel<128, 0, 1, true>(a);
+        if (fast) root_kernel<128, 0, 2, false, true>(a);
+        else if (ifunc == 1 && group) root_kernel<128, 0, 1, true>(a);
         else if (ifunc == 1) root_kernel<128, 0, 1, false>(a);
         else if (group) root_kernel<128, 0, 2, true>(a);
         else root_kernel<128, 0>(a);
@@ -153,11 +156,12 @@ extern "C" int emu_ti_batch(long long ncols, const long long* node_off, const fl
 // sweep, and dropped[pv index] = 1 marks those (column, period) entries.
 extern "C" int emu_adjoint_batch(long long ncols, const long long* node_off, const float* depz,
                                  const float* vs, const long long* per_off, const double* periods,
-                                 float minthk, int ifunc, int group, int drop_every, double* pv,
-                                 int* status, const long long* sen_off, double* svs, double* svp,
-                                 double* srh, unsigned char* dropped)
+                                 float minthk, int ifunc, int group, int drop_every, int fast,
+                                 double* pv, int* status, const long long* sen_off, double* svs,
+                                 double* svp, double* srh, unsigned char* dropped)
 {
     if (ifunc != 1 && ifunc != 2) return -2;
+    if (fast && (ifunc != 2 || group)) return -2;
     const ColSrc src = ragged_src(node_off, depz, vs, per_off, minthk, ifunc);
     HostTables H;
     PrepOut po{sen_off, nullptr, nullptr};
@@ -173,7 +177,8 @@ extern "C" int emu_adjoint_batch(long long ncols, const long long* node_off, con
     for (long long s = 0; s < ncols; ++s) {
         blockIdx.x = (unsigned)(s / 128);
         threadIdx.x = (unsigned)(s % 128);
-        if (ifunc == 1 && group) root_kernel<128, 0, 1, true>(a);
+        if (fast) root_kernel<128, 0, 2, false, true>(a);
+        else if (ifunc == 1 && group) root_kernel<128, 0, 1, true>(a);
         else if (ifunc == 1) root_kernel<128, 0, 1, false>(a);
         else if (group) root_kernel<128, 0, 2, true>(a);
         else root_kernel<128, 0>(a);

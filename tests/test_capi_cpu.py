@@ -79,7 +79,6 @@ def _call_iso(nx=2, ny=2, nz=3, iwave=2, igr=0, K=2, depz=(0.0, 3.0, 6.0), vel=3
     (dict(iwave=1, form=_lib.FORM_ADJOINT | _lib.FORM_SCAN_FP32), _lib.DAZI_ERR_BADARG),
     (dict(form=_lib.FORM_LOVE), _lib.DAZI_ERR_BADARG),  # wave type goes through iwave here
     (dict(form=_lib.FORM_GROUP), _lib.DAZI_ERR_BADARG),
-    (dict(form=16), _lib.DAZI_ERR_BADARG),              # unknown flag
     (dict(depz=(0.0, 3.0, 3.0)), _lib.DAZI_ERR_BADARG),  # not increasing
     (dict(col_start=0), _lib.DAZI_ERR_BADARG),
     (dict(col_start=3, col_count=3), _lib.DAZI_ERR_BADARG),
@@ -88,6 +87,9 @@ def _call_iso(nx=2, ny=2, nz=3, iwave=2, igr=0, K=2, depz=(0.0, 3.0, 6.0), vel=3
     (dict(periods=(5.0, 0.0)), _lib.DAZI_ERR_BADARG),
     (dict(nz=1, depz=(0.0,)), _lib.DAZI_ERR_LIMITS),
     (dict(form=7), _lib.DAZI_ERR_BADARG),
+    (dict(form=32), _lib.DAZI_ERR_BADARG),              # unknown flag
+    (dict(iwave=1, form=_lib.FORM_ADJOINT | _lib.FORM_FAST_ROOT), _lib.DAZI_ERR_BADARG),
+    (dict(igr=1, form=_lib.FORM_ADJOINT | _lib.FORM_FAST_ROOT), _lib.DAZI_ERR_BADARG),
 ])
 def test_bad_arguments_rejected_without_device(kw, code):
     assert _call_iso(**kw) == code
@@ -95,7 +97,7 @@ def test_bad_arguments_rejected_without_device(kw, code):
 
 
 @pytest.mark.parametrize("iwave,igr,form", [(1, 0, 0), (2, 1, 0), (1, 1, 0), (2, 5, 0), (1, 0, 1),
-                                            (2, 1, 1), (1, 1, 1)])
+                                            (2, 1, 1), (1, 1, 1), (2, 0, 17), (2, 0, 19)])
 def test_love_and_group_pass_validation(iwave, igr, form):
     """Love (iwave = 1) and group velocity (igr > 0) are accepted by the
     plain and the adjoint form; without a GPU the call then stops at the

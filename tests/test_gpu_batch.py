@@ -139,3 +139,54 @@ def test_host_entry_equals_device_entry_twice():
             np.testing.assert_array_equal(host[name], t.cpu().numpy(), err_msg=name)
         np.testing.assert_array_equal(host["lsen"], ls.cpu().numpy())
         np.testing.assert_array_equal(host["status"], st.cpu().numpy())
+
+
+def test_fast_root_matches_reference_search_and_exact_roots(oracle):
+    """DAZI_FORM_FAST_ROOT (Brent refinement of the reference's bracket) on
+    2,500 uneven columns against the reference's search: the same statuses,
+    roots within the reference's own 1e-6 c tolerance (plus the two float32
+    roundings), kernels within 1e-5 per column and Lsen_Gsc within 1e-5;
+    on 40 of the columns the roots are within one float32 ulp of the
+    oracle's roots converged to 1e-13."""
+    b = S.config3(realisations=1, columns=2500, base_seed=1003)
+    args = (b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk)
+    r0 = depthkernel_batch(*args, form=dk.FORM_ADJOINT)
+    r1 = depthkernel_batch(*args, form=dk.FORM_ADJOINT | dk.FORM_FAST_ROOT)
+    np.testing.assert_array_equal(r1["status"], r0["status"])
+    ok = r0["pv"] > 0
+    np.testing.assert_array_equal(r1["pv"] > 0, ok)
+    assert (np.abs(r1["pv"][ok] / r0["pv"][ok] - 1.0) <= 1e-6 + 1.3e-7).all()
+    worst_k, worst_l = 0.0, 0.0
+    for c in range(b.ncol):
+        if r0["status"][c]:
+            continue
+        g, r = r1.column(c), r0.column(c)
+        worst_k = max(worst_k, max(rel_l2(g[i], r[i]) for i in (1, 2, 3)))
+        worst_l = max(worst_l, rel_l2(g[4], r[4]))
+    print("Brent roots: kernels vs reference-search kernels", worst_k, "Lsen", worst_l)
+    assert worst_k <= 1e-5 and worst_l <= 1e-5
+    for c in range(0, b.ncol, 62):
+        dep, vs, per = b.column(c)
+        vp, rho = oracle.brocher(vs)
+        thk, rvp, rvs, rr, _ = oracle.refine(b.minthk, dep, vp, vs, rho)
+        tight, st, _ = oracle.surfdisp96(thk, rvp, rvs, rr, per, tol=1e-13)
+        got = r1.column(c)[0]
+        m = tight > 0
+        ulp = np.spacing(tight[m].astype(np.float32)).astype(np.float64)
+        assert (np.abs(got[m] - tight[m]) <= ulp).all(), c
+
+
+def test_fast_root_plan_equals_per_call():
+    """A plan with fast_root=True gives the per-call entry's results."""
+    import torch
+    from dazi_current_release_b200.plan import BatchPlan
+    b = S.config3(realisations=1, columns=600, base_seed=1004)
+    args = (b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk)
+    r = depthkernel_batch(*args, form=dk.FORM_ADJOINT | dk.FORM_FAST_ROOT)
+    plan = BatchPlan(*args, tune=False, fast_root=True)
+    plan.run()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(plan.pv.cpu().numpy(), r["pv"])
+    np.testing.assert_array_equal(plan.status.cpu().numpy(), r["status"])
+    np.testing.assert_allclose(plan.sen_vs.cpu().numpy(), r["sen_vs"], rtol=1e-9, atol=1e-12)
+    plan.close()
