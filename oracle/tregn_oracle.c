@@ -1040,7 +1040,6 @@ int or_batch(long ncols, const long *node_off, const float *depz, const float *v
         } else {
             (void)tmp1;
         }
-        if (!lsen) continue;
         float rthk[NL], rvp[NL], rvs[NL], rrho[NL];
         int nsub[NL];
         int rmax = or_refine(minthk, nz, dep, vp, vs, rho, rthk, rvp, rvs, rrho, nsub);
@@ -1048,9 +1047,11 @@ int or_batch(long ncols, const long *node_off, const float *depz, const float *v
         double cg[NP];
         if (svs) { for (int k = 0; k < K; ++k) cg[k] = cpv[k]; }
         else {
+            /* phase velocities alone when no kernel is asked for */
             or_surfdisp96_ex(rthk, rvp, rvs, rrho, rmax, 1, 2, 1, 0, K, per, cg, 1.0e-6, 1, NULL);
             for (int k = 0; k < K; ++k) cpv[k] = cg[k];
         }
+        if (!lsen) continue;
         float TA[NL], TC[NL], TF[NL], TL[NL], TN[NL], TR[NL], qp[NL], qs[NL], z0[NL], one[NL];
         for (int i = 0; i < rmax; ++i) {
             TA[i] = rrho[i] * (rvp[i] * rvp[i]);

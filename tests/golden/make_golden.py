@@ -10,14 +10,16 @@ and the two golden phase-velocity maps written by WTPeriodPhaseV
 Both hold surfdisp96 phase velocities of the inner (nx-2)*(ny-2) columns at
 36 periods, printed with f10.4.  They are stored as integers (value * 1e4).
 
-Usage: python tests/golden/make_golden.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_golden.py REFERENCE_ROOT
 """
 import os
 import sys
 
 import numpy as np
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit(__doc__)
+ref = sys.argv[1]   # the reference checkout (the root of the DAzi project)
 base = os.path.join(ref, "examples", "test4_Yunnan", "voro")
 legacy = os.path.join(ref, "examples", "test4_Yunnan_legacy_old_para", "voro")
 nx, ny, nz = 38, 42, 18

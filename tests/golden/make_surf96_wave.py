@@ -14,7 +14,7 @@ The module is executed from its source text (not imported), with numba's
 jit and guvectorize forced to cache=False, so nothing precompiled that ships
 beside it is loaded.
 
-Usage: python tests/golden/make_surf96_wave.py [REFERENCE_ROOT]
+Usage: python tests/golden/make_surf96_wave.py REFERENCE_ROOT
 """
 import os
 import sys
@@ -26,7 +26,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, ROOT)
 
-ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+if len(sys.argv) != 2:
+    sys.exit(__doc__)
+ref = sys.argv[1]   # the reference checkout (the root of the DAzi project)
 src_path = os.path.join(ref, "code", "pDSurfTomo-main", "bin", "surf96_disba.py")
 
 
