@@ -16,9 +16,10 @@ ragged batch entries dazi_dk_batch_dev / dazi_dk_batch.  The grid workloads
 dazi_dk_fused_dev / dazi_dk_fused.
 
 value      device-timed throughput of the chosen form (--form, default the
-           adjoint form; --root brent: each period's bracket, the reference's
-           getsol scan, refined by Brent's method, DAZI_FORM_FAST_ROOT) on the
-           whole batch, inputs resident in HBM: a plan
+           adjoint form; --root reference: the reference's point sequence, or
+           brent: each period's bracket refined by Brent's method,
+           DAZI_FORM_FAST_ROOT; the other one is timed beside it in
+           root_search) on the whole batch, inputs resident in HBM: a plan
            (dazi_dk_plan_*: structure bound once, kernel variants autotuned,
            each step one CUDA-graph launch) on torch's stream, CUDA events per
            step, L2 flushed between steps outside the timed events; the
@@ -78,7 +79,7 @@ def parse():
     p.add_argument("--plain-cols", type=int, default=25000,
                    help="ragged workload: columns the plain form is timed on")
     p.add_argument("--form", default="adjoint", choices=["plain", "adjoint"])
-    p.add_argument("--root", default="brent", choices=["brent", "reference"],
+    p.add_argument("--root", default="reference", choices=["brent", "reference"],
                    help="adjoint form: refine each period's bracket by Brent's method "
                         "(DAZI_FORM_FAST_ROOT) or by the reference's nevill()")
     p.add_argument("--no-other-form", action="store_true")
@@ -561,29 +562,59 @@ def main_ragged(args, ws, rank, local):
                                      status)
     scan32 = None
     root_search = None
+    alt_sample = None
+    alt_is_brent = False
     if form & _lib.FORM_ADJOINT:
         pv_t, st_t = pv.clone(), status.clone()
-        if fast:
-            # the reference's search on the same batch: its evaluation count
-            # (E_ref of the roofline) and the mode check of every root
-            step_fn(_lib.FORM_ADJOINT, ncol)()
-            ph_ref = _lib.last_timing()
-            ev_ref, layer_evals_ref, _ = work()
-            ok = pv > 0
-            rel = torch.where(ok, (pv_t / torch.where(ok, pv, 1.0) - 1.0).abs(), 0.0)
-            root_search = {
-                "refinement": "brent (DAZI_FORM_FAST_ROOT): the reference's getsol scan, Brent "
-                              "to 1e-10 c",
-                "evals_per_column_period": evals / ncp,
-                "reference_evals_per_column_period": ev_ref / ncp,
-                "root_ms": phases.get("root"), "reference_root_ms": ph_ref.get("root"),
-                "columns_same_status": int((st_t == status).sum().item()),
-                "columns": ncol,
-                "periods_same_root_presence": int(((pv_t > 0) == ok).sum().item()),
-                "max_rel_diff_vs_reference_search": float(rel.max().item()),
-                "within_reference_tolerance": int((rel <= 1e-6 + 1.3e-7).sum().item()),
-                "column_periods": ncp}
-            layer_evals = layer_evals_ref
+        sen_t = [x.clone() for x in sen]
+        ls_t = lsen.clone()
+        evals_t = evals
+        # the other refinement of each period's bracket (the reference's
+        # nevill() or Brent's, DAZI_FORM_FAST_ROOT), timed per call on the
+        # same batch, and every output compared with the headline form's
+        alt = form ^ _lib.FORM_FAST_ROOT
+        _lib.check(L.dazi_dk_set_timing(0))
+        alt_ms = _events_timed(step_fn(alt, ncol), max(2, args.steps // 2), 1, dev, stream, flush,
+                               ws)
+        _lib.check(L.dazi_dk_set_timing(1))
+        step_fn(alt, ncol)()
+        ph_alt = _lib.last_timing()
+        ev_alt, lev_alt, _ = work()
+        if acc_cols is not None:
+            alt_sample = _gather_columns(torch, dev, b, acc_cols, sen_off, ls_off, pv, sen, lsen,
+                                         status)
+        ok = pv_t > 0
+        rel = torch.where(ok, (pv / torch.where(ok, pv_t, 1.0) - 1.0).abs(), 0.0)
+        grl = lambda a, r: float((torch.linalg.vector_norm(a - r) /  # noqa: E731
+                                  torch.linalg.vector_norm(r)).item())
+        brent = alt_is_brent = bool(alt & _lib.FORM_FAST_ROOT)
+        ref_ph, brent_ph = (phases, ph_alt) if brent else (ph_alt, phases)
+        root_search = {
+            "refinement": "headline: " + ("reference nevill()" if brent else "Brent") +
+                          "; other: " + ("Brent (DAZI_FORM_FAST_ROOT)" if brent else
+                                         "reference nevill()") +
+                          ".  Both run the reference's getsol scan point for point (same "
+                          "bracket, same mode); Brent refines it to 1e-10 c, nevill() to 1e-6 c",
+            "brent": {"value_per_call": job_cp / ((alt_ms if brent else call_ms) * 1e-3),
+                      "root_ms": brent_ph.get("root"),
+                      "evals_per_column_period": (ev_alt if brent else evals_t) / ncp},
+            "reference": {"value_per_call": job_cp / ((call_ms if brent else alt_ms) * 1e-3),
+                          "root_ms": ref_ph.get("root"),
+                          "evals_per_column_period": (evals_t if brent else ev_alt) / ncp},
+            "columns_same_status": int((st_t == status).sum().item()), "columns": ncol,
+            "periods_same_root_presence": int(((pv > 0) == ok).sum().item()),
+            "pv_max_rel_diff": float(rel.max().item()),
+            "pv_within_reference_tolerance": int((rel <= 1e-6 + 1.3e-7).sum().item()),
+            "column_periods": ncp,
+            "kernels_rel_l2": {n: grl(sen[i], sen_t[i])
+                               for i, n in enumerate(("sen_vs", "sen_vp", "sen_rho"))},
+            "lsen_rel_l2": grl(lsen, ls_t),
+            "note": "Lsen_Gsc follows the root: tregn96's partials at the reference's root "
+                    "(converged to 1e-6 c) and at the exact root differ by up to 1 % per "
+                    "period on sediment columns at short periods"}
+        if not brent:
+            layer_evals = lev_alt      # E_ref: the reference's evaluation sequence
+        del sen_t, ls_t
         step_fn(form | _lib.FORM_SCAN_FP32, ncol)()
         ph32 = _lib.last_timing()
         scan32 = {"root_ms_fp64_scan": phases.get("root"), "root_ms_fp32_scan": ph32.get("root"),
@@ -696,7 +727,7 @@ def main_ragged(args, ws, rank, local):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": dict(ragged_config(args, b),
-                       root_refinement="brent" if fast else "reference nevill"),
+                       root_refinement="brent" if fast else "reference nevill()"),
         "e2e": {"value": job_cp / e2e_s, "unit": "column-periods/s",
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h), "steps": e2e_steps},
         "roofline": roof,
@@ -716,6 +747,8 @@ def main_ragged(args, ws, rank, local):
     clocks = clk.summary()
     if clocks:
         line["clocks"] = clocks
+    if ws > 1:
+        line["gather"] = _timed_gather(torch, dev, stream, pv, status, sen, lsen)
     if acc_cols is not None:
         from oracle import oracle as O
         cb, idx, sb, ora = ragged_cpu_baseline(b, seed=0, per_thread=args.cpu_cols_per_thread)
@@ -729,12 +762,74 @@ def main_ragged(args, ws, rank, local):
         acc["sample"] = (f"the cpu_baseline's {sb.ncol} columns; the adjoint form's outputs from "
                          f"the full-batch step, the plain form run on those columns alone; "
                          f"exact differences {time.perf_counter() - t0:.1f} s")
+        if alt_sample is not None:
+            brent_s = alt_sample if alt_is_brent else gpu_sample
+            a2 = accuracy_block(sb, brent_s, ora, exact, None)
+            args_sb = (sb.node_off, sb.depz, sb.vs, sb.per_off, sb.periods, sb.minthk)
+            at_pv = O.batch_ti(*args_sb, pv=brent_s["pv"])
+            tight = O.batch_ti(*args_sb, root_tol=1e-13)
+            K = np.diff(sb.per_off)
+            good = np.array([int(np.argmin(ora["pv"][sb.per_off[c]:sb.per_off[c + 1]] > 0))
+                             if (ora["pv"][sb.per_off[c]:sb.per_off[c + 1]] <= 0).any() else K[c]
+                             for c in range(sb.ncol)])
+            lsen_w = lambda ref: max(  # noqa: E731
+                (float(np.linalg.norm((brent_s["lsen"][a:e] - ref[a:e]).astype(np.float64)) /
+                       np.linalg.norm(ref[a:e].astype(np.float64)))
+                 for a, e in zip(at_pv["ls_off"][:-1], at_pv["ls_off"][1:])
+                 if e > a and np.linalg.norm(ref[a:e]) > 0), default=0.0)
+            tk = tight["pv"] > 0
+            acc["brent_root"] = {
+                "pv_max_rel_err": a2["pv_max_rel_err"],
+                "pv_max_rel_err_vs_tight_root": float(np.abs(brent_s["pv"][tk] / tight["pv"][tk]
+                                                              - 1.0).max()),
+                "status_equal_columns": a2["status_equal_columns"],
+                "fundamental_mode_identity_columns": a2["fundamental_mode_identity_columns"],
+                "adjoint_kernels_vs_exact_worst_column_rel_l2":
+                    a2["adjoint_kernels_vs_exact_worst_column_rel_l2"],
+                "lsen_vs_oracle_at_same_pv_worst_column_rel_l2": lsen_w(at_pv["lsen"]),
+                "lsen_vs_oracle_at_tight_root_worst_column_rel_l2": lsen_w(tight["lsen"]),
+                "lsen_vs_oracle_reference_root_worst_column_rel_l2": a2["lsen_worst_column_rel_l2"],
+                "tight_root": "surfdisp96 on the real*4 model converged to 1e-13, rounded to "
+                              "float32", "periods_with_root": int(good.sum())}
         line["accuracy"] = acc
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def _timed_gather(torch, dev, stream, pv, status, sen, lsen):
+    """The stage's one communication step: every rank's outputs (pv,
+    status, the three kernels, Lsen_Gsc) gathered to rank 0 in rank order
+    (shard.gather_blocks: size exchange, NCCL point-to-point receives into
+    slices of rank 0's arrays).  Device time with CUDA events, max over
+    ranks; the bytes rank 0 receives from the others."""
+    import torch.distributed as dist
+    from dazi_current_release_b200.shard import gather_blocks
+    blocks = {"pv": pv, "status": status, "sen_vs": sen[0], "sen_vp": sen[1],
+              "sen_rho": sen[2], "lsen": lsen}
+    own = sum(t.numel() * t.element_size() for t in blocks.values())
+    gather_blocks({"pv": pv[:1]})          # warm-up (NCCL communicators)
+    torch.cuda.synchronize(dev)
+    dist.barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    out = gather_blocks(blocks)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    dist.all_reduce(ms, op=dist.ReduceOp.MAX)
+    tot = torch.tensor([own], dtype=torch.float64, device=dev)
+    dist.all_reduce(tot, op=dist.ReduceOp.SUM)
+    received = float(tot.item()) - own if dist.get_rank() == 0 else None
+    del out
+    res = {"ms": float(ms.item()), "bytes_to_rank0": received,
+           "what": "pv, status, sen_vs/vp/rho, Lsen_Gsc of every rank to rank 0 (NCCL "
+                   "point-to-point into slices of preallocated arrays)"}
+    if received:
+        res["GB_per_s"] = received / (res["ms"] * 1e-3) / 1e9
+    return res
 
 
 def _gather_columns(torch, dev, b, idx, sen_off, ls_off, pv, sen, lsen, status):

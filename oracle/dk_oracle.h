@@ -76,6 +76,9 @@ int or_batch(long ncols, const long *node_off, const float *depz, const float *v
              const long *per_off, const double *periods, float minthk, double *pv,
              const long *sen_off, double *svs, double *svp, double *srh, const long *ls_off,
              float *lsen, int nthreads);
+int or_batch_ti(long ncols, const long *node_off, const float *depz, const float *vs_all,
+                const long *per_off, const double *periods, float minthk, const double *pv_in,
+                double root_tol, double *pv_out, const long *ls_off, float *lsen, int nthreads);
 int or_batch_fd(long ncols, const long *node_off, const float *depz, const float *vs_all,
                 const long *per_off, const double *periods, float minthk, double *pv,
                 const long *sen_off, double *svs, double *svp, double *srh, int precision,

@@ -92,6 +92,10 @@ def lib():
         L.or_batch.argtypes = [ctypes.c_long, _i64p, _f32p, _f32p, _i64p, _f64p, ctypes.c_float,
                                _f64p, _i64p, _f64p, _f64p, _f64p, _i64p, _f32p, ctypes.c_int]
         L.or_batch.restype = ctypes.c_int
+        L.or_batch_ti.argtypes = [ctypes.c_long, _i64p, _f32p, _f32p, _i64p, _f64p,
+                                  ctypes.c_float, _f64p, ctypes.c_double, _f64p, _i64p, _f32p,
+                                  ctypes.c_int]
+        L.or_batch_ti.restype = ctypes.c_int
         L.or_batch_fd.argtypes = [ctypes.c_long, _i64p, _f32p, _f32p, _i64p, _f64p,
                                   ctypes.c_float, _f64p, _i64p, _f64p, _f64p, _f64p, ctypes.c_int,
                                   ctypes.c_double, ctypes.c_float, _i32p, ctypes.c_int]
@@ -354,6 +358,30 @@ def batch(node_off, depz, vs, per_off, periods, minthk, kernels=True, lsen=True,
         raise RuntimeError("oracle batch failed")
     return dict(pv=pv, sen_vs=sen[0], sen_vp=sen[1], sen_rho=sen[2], lsen=ls,
                 sen_off=sen_off, ls_off=ls_off)
+
+
+def batch_ti(node_off, depz, vs, per_off, periods, minthk, pv=None, root_tol=1e-6,
+             nthreads=0):
+    """Lsen_Gsc of a ragged batch (depthkernelTI's tregn96 + splice) at the
+    given phase velocities pv (batch layout), or at surfdisp96's roots
+    converged to root_tol.  Returns pv (the ones used), lsen and ls_off."""
+    node_off = np.ascontiguousarray(node_off, np.int64)
+    per_off = np.ascontiguousarray(per_off, np.int64)
+    nz = np.diff(node_off)
+    K = np.diff(per_off)
+    ls_off = np.concatenate([[0], np.cumsum(K * (nz - 1))]).astype(np.int64)
+    ls = np.zeros(max(int(ls_off[-1]), 1), np.float32)
+    pv_out = np.zeros(int(per_off[-1]))
+    pv_in = None if pv is None else np.ascontiguousarray(pv, np.float64)
+    r = lib().or_batch_ti(node_off.size - 1, _p(node_off, _i64p),
+                          _p(np.ascontiguousarray(depz, np.float32), _f32p),
+                          _p(np.ascontiguousarray(vs, np.float32), _f32p), _p(per_off, _i64p),
+                          _p(np.ascontiguousarray(periods, np.float64), _f64p),
+                          ctypes.c_float(minthk), _p(pv_in, _f64p), root_tol, _p(pv_out, _f64p),
+                          _p(ls_off, _i64p), _p(ls, _f32p), nthreads)
+    if r != 0:
+        raise RuntimeError("oracle batch_ti failed")
+    return dict(pv=pv_out, lsen=ls[:int(ls_off[-1])], ls_off=ls_off)
 
 
 def batch_fd(node_off, depz, vs, per_off, periods, minthk, exact=False, tol=None, dln=None,

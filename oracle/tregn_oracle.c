@@ -1011,6 +1011,10 @@ int or_depthkernelTI(int nx, int ny, int nz, const float *vel, const float *vp_i
  * path (depthkernelTI.f90:93-162), with OpenMP over columns.  Outputs use the
  * batch layout: pv[per_off[c]+k], sen[sen_off[c] + k + K_c i],
  * lsen[ls_off[c] + k + K_c j].  Brocher Vp/rho.  Returns 0 or -1. */
+static int ti_splice_column(int nz, int K, const double *per, int rmax, const float *rthk,
+                            const float *rvp, const float *rvs, const float *rrho,
+                            const int *nsub, const double *cg, float *L);
+
 int or_batch(long ncols, const long *node_off, const float *depz, const float *vs_all,
              const long *per_off, const double *periods, float minthk, double *pv,
              const long *sen_off, double *svs, double *svp, double *srh, const long *ls_off,
@@ -1052,48 +1056,98 @@ int or_batch(long ncols, const long *node_off, const float *depz, const float *v
             for (int k = 0; k < K; ++k) cpv[k] = cg[k];
         }
         if (!lsen) continue;
-        float TA[NL], TC[NL], TF[NL], TL[NL], TN[NL], TR[NL], qp[NL], qs[NL], z0[NL], one[NL];
-        for (int i = 0; i < rmax; ++i) {
-            TA[i] = rrho[i] * (rvp[i] * rvp[i]);
-            TC[i] = TA[i];
-            TL[i] = rrho[i] * (rvs[i] * rvs[i]);
-            TN[i] = TL[i];
-            TF[i] = 1.0f * (TA[i] - 2.0f * TL[i]);
-            TR[i] = rrho[i];
-            qp[i] = 150.0f; qs[i] = 50.0f; z0[i] = 0.0f; one[i] = 1.0f;
-        }
-        float cp[NP], tt[NP];
-        int kgood = K;
-        for (int k = 0; k < K; ++k) {
-            cp[k] = (float)cg[k]; tt[k] = (float)per[k];
-            if (!(cp[k] > 0.0f) && kgood == K) kgood = k;
-        }
-        float *dah = malloc(sizeof(float) * 3 * (size_t)K * rmax);
-        if (!dah) { bad |= 1; continue; }
-        float *dbv = dah + (size_t)K * rmax, *dn = dbv + (size_t)K * rmax;
-        if (kgood > 0 && or_tregn96(rmax, rthk, TA, TC, TF, TL, TN, TR, qp, qs, z0, z0, one, one,
-                                    kgood, tt, cp, dah, dbv, dn) != 0) {
-            bad |= 1; free(dah); continue;
-        }
-        float *L = lsen + ls_off[c];
-        for (int i = 0; i < K; ++i) {
-            for (int j = 0; j < nz - 1; ++j) L[i + (long)K * j] = 0.0f;
-            if (i >= kgood) continue;
-            int k = 0;
-            for (int j = 0; j < nz - 1; ++j) {
-                float acc = 0.0f;
-                for (int jj = 0; jj < nsub[j]; ++jj, ++k) {
-                    float tfd = TA[k] - 2.0f * TL[k];
-                    float dA = 0.5f / (rrho[k] * rvp[k]) * dah[(size_t)i * rmax + k]
-                               - TF[k] / (tfd * tfd) * dn[(size_t)i * rmax + k];
-                    float dL = 0.5f / (rrho[k] * rvs[k]) * dbv[(size_t)i * rmax + k]
-                               + 2.0f * TF[k] / (tfd * tfd) * dn[(size_t)i * rmax + k];
-                    acc = acc + dA * TA[k] + dL * TL[k];
-                }
-                L[i + (long)K * j] = acc;
-            }
-        }
+        if (ti_splice_column(nz, K, per, rmax, rthk, rvp, rvs, rrho, nsub, cg,
+                             lsen + ls_off[c]) != 0) bad |= 1;
+    }
+    return bad ? -1 : 0;
+}
+
+/* depthkernelTI's tregn96 call and splice for one refined column
+ * (depthkernelTI.f90:124-162): the real*4 moduli, tregn96 with Q 150/50
+ * and sphericity at the phase velocities cg (real*4 cp_in = sngl(cg); a
+ * period without a root and all after it give 0), Lsen_Gsc (K x nz-1,
+ * column-major) in real*4.  Returns 0 or -1. */
+static int ti_splice_column(int nz, int K, const double *per, int rmax, const float *rthk,
+                            const float *rvp, const float *rvs, const float *rrho,
+                            const int *nsub, const double *cg, float *L)
+{
+    float TA[NL], TC[NL], TF[NL], TL[NL], TN[NL], TR[NL], qp[NL], qs[NL], z0[NL], one[NL];
+    for (int i = 0; i < rmax; ++i) {
+        TA[i] = rrho[i] * (rvp[i] * rvp[i]);
+        TC[i] = TA[i];
+        TL[i] = rrho[i] * (rvs[i] * rvs[i]);
+        TN[i] = TL[i];
+        TF[i] = 1.0f * (TA[i] - 2.0f * TL[i]);
+        TR[i] = rrho[i];
+        qp[i] = 150.0f; qs[i] = 50.0f; z0[i] = 0.0f; one[i] = 1.0f;
+    }
+    float cp[NP], tt[NP];
+    int kgood = K;
+    for (int k = 0; k < K; ++k) {
+        cp[k] = (float)cg[k]; tt[k] = (float)per[k];
+        if (!(cp[k] > 0.0f) && kgood == K) kgood = k;
+    }
+    float *dah = malloc(sizeof(float) * 3 * (size_t)K * rmax);
+    if (!dah) return -1;
+    float *dbv = dah + (size_t)K * rmax, *dn = dbv + (size_t)K * rmax;
+    if (kgood > 0 && or_tregn96(rmax, rthk, TA, TC, TF, TL, TN, TR, qp, qs, z0, z0, one, one,
+                                kgood, tt, cp, dah, dbv, dn) != 0) {
         free(dah);
+        return -1;
+    }
+    for (int i = 0; i < K; ++i) {
+        for (int j = 0; j < nz - 1; ++j) L[i + (long)K * j] = 0.0f;
+        if (i >= kgood) continue;
+        int k = 0;
+        for (int j = 0; j < nz - 1; ++j) {
+            float acc = 0.0f;
+            for (int jj = 0; jj < nsub[j]; ++jj, ++k) {
+                float tfd = TA[k] - 2.0f * TL[k];
+                float dA = 0.5f / (rrho[k] * rvp[k]) * dah[(size_t)i * rmax + k]
+                           - TF[k] / (tfd * tfd) * dn[(size_t)i * rmax + k];
+                float dL = 0.5f / (rrho[k] * rvs[k]) * dbv[(size_t)i * rmax + k]
+                           + 2.0f * TF[k] / (tfd * tfd) * dn[(size_t)i * rmax + k];
+                acc = acc + dA * TA[k] + dL * TL[k];
+            }
+            L[i + (long)K * j] = acc;
+        }
+    }
+    free(dah);
+    return 0;
+}
+
+/* Lsen_Gsc of a ragged batch at given phase velocities (pv_in, batch
+ * layout: tregn96 is called at sngl(pv_in), as depthkernelTI passes its
+ * real*4 roots) or, with pv_in NULL, at surfdisp96's roots converged to
+ * root_tol (1e-6: the reference's; smaller: a checker of the partials at
+ * the exact root), which are written to pv_out.  OpenMP over columns. */
+int or_batch_ti(long ncols, const long *node_off, const float *depz, const float *vs_all,
+                const long *per_off, const double *periods, float minthk, const double *pv_in,
+                double root_tol, double *pv_out, const long *ls_off, float *lsen, int nthreads)
+{
+    int bad = 0;
+#ifdef _OPENMP
+    if (nthreads < 1) nthreads = omp_get_max_threads();
+#pragma omp parallel for schedule(dynamic) num_threads(nthreads) reduction(|:bad)
+#endif
+    for (long c = 0; c < ncols; ++c) {
+        const int nz = (int)(node_off[c + 1] - node_off[c]);
+        const int K = (int)(per_off[c + 1] - per_off[c]);
+        if (nz < 2 || nz > NL || K < 1 || K > NP) { bad |= 1; continue; }
+        const float *dep = depz + node_off[c];
+        const float *vs = vs_all + node_off[c];
+        const double *per = periods + per_off[c];
+        float vp[NL], rho[NL], rthk[NL], rvp[NL], rvs[NL], rrho[NL];
+        int nsub[NL];
+        or_brocher(nz, vs, vp, rho);
+        int rmax = or_refine(minthk, nz, dep, vp, vs, rho, rthk, rvp, rvs, rrho, nsub);
+        if (rmax < 0) { bad |= 1; continue; }
+        double cg[NP];
+        if (pv_in) { for (int k = 0; k < K; ++k) cg[k] = pv_in[per_off[c] + k]; }
+        else or_surfdisp96_ex(rthk, rvp, rvs, rrho, rmax, 1, 2, 1, 0, K, per, cg, root_tol, 1, NULL);
+        if (pv_out) for (int k = 0; k < K; ++k) pv_out[per_off[c] + k] = cg[k];
+        if (ti_splice_column(nz, K, per, rmax, rthk, rvp, rvs, rrho, nsub, cg,
+                             lsen + ls_off[c]) != 0) bad |= 1;
     }
     return bad ? -1 : 0;
 }

@@ -145,9 +145,13 @@ def test_fast_root_matches_reference_search_and_exact_roots(oracle):
     """DAZI_FORM_FAST_ROOT (Brent refinement of the reference's bracket) on
     2,500 uneven columns against the reference's search: the same statuses,
     roots within the reference's own 1e-6 c tolerance (plus the two float32
-    roundings), kernels within 1e-5 per column and Lsen_Gsc within 1e-5;
-    on 40 of the columns the roots are within one float32 ulp of the
-    oracle's roots converged to 1e-13."""
+    roundings), the Vs-type kernels within 1e-5 per column; on 40 of the
+    columns the roots are within one float32 ulp of the oracle's roots
+    converged to 1e-13, and on 100 columns Lsen_Gsc is within 1e-5 of the
+    oracle's tregn96 + splice at the same phase velocities.  (Lsen_Gsc moves
+    with the root: on sediment columns at short periods tregn96's partials
+    change by up to 1 % per period between the reference's root, converged
+    to 1e-6 c, and the exact one; the printed figure is that shift.)"""
     b = S.config3(realisations=1, columns=2500, base_seed=1003)
     args = (b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk)
     r0 = depthkernel_batch(*args, form=dk.FORM_ADJOINT)
@@ -163,8 +167,25 @@ def test_fast_root_matches_reference_search_and_exact_roots(oracle):
         g, r = r1.column(c), r0.column(c)
         worst_k = max(worst_k, max(rel_l2(g[i], r[i]) for i in (1, 2, 3)))
         worst_l = max(worst_l, rel_l2(g[4], r[4]))
-    print("Brent roots: kernels vs reference-search kernels", worst_k, "Lsen", worst_l)
-    assert worst_k <= 1e-5 and worst_l <= 1e-5
+    print("Brent roots: kernels vs reference-search kernels", worst_k,
+          "Lsen shift with the root", worst_l)
+    assert worst_k <= 1e-5
+    sub = np.arange(0, b.ncol, 25)
+    nz, K = np.diff(b.node_off)[sub], np.diff(b.per_off)[sub]
+    cols = [b.column(int(c)) for c in sub]
+    sb = S.RaggedBatch(np.concatenate([[0], np.cumsum(nz)]).astype(np.int64),
+                       np.concatenate([x[0] for x in cols]), np.concatenate([x[1] for x in cols]),
+                       np.concatenate([[0], np.cumsum(K)]).astype(np.int64),
+                       np.concatenate([x[2] for x in cols]), b.minthk)
+    pv_sub = np.concatenate([r1.column(int(c))[0] for c in sub])
+    ti = oracle.batch_ti(sb.node_off, sb.depz, sb.vs, sb.per_off, sb.periods, sb.minthk,
+                         pv=pv_sub)
+    worst_t = 0.0
+    for j, c in enumerate(sub):
+        lo, hi = ti["ls_off"][j], ti["ls_off"][j + 1]
+        worst_t = max(worst_t, rel_l2(r1.column(int(c))[4].ravel(order="F"), ti["lsen"][lo:hi]))
+    print("Brent roots: Lsen vs the oracle at the same phase velocities", worst_t)
+    assert worst_t <= 1e-5
     for c in range(0, b.ncol, 62):
         dep, vs, per = b.column(c)
         vp, rho = oracle.brocher(vs)

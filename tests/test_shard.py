@@ -1,5 +1,7 @@
 """Multi-GPU host logic on the CPU: shard boundaries, CSR slicing and the
-gather of the outputs, run as world-size-2 (and 3) gloo process groups.
+gather of the outputs (size exchange + point-to-point receives into slices
+of the destination's arrays), run as world-size-2 (and 3) gloo process
+groups.
 The per-shard computation is the oracle here (the library needs a GPU);
 the test checks that the sharded, gathered result equals the oracle run on
 the whole batch in one process."""
@@ -73,7 +75,10 @@ def _worker(rank, world, port, path):
         out = shard.run_sharded(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk,
                                 compute=_oracle_compute)
         if rank == 0:
-            np.savez(path, **{k: v for k, v in out.items() if v is not None})
+            np.savez(path, **{k: (v.numpy() if hasattr(v, "numpy") else v)
+                              for k, v in out.items() if v is not None})
+        else:
+            assert out is None
         dist.barrier()
     finally:
         dist.destroy_process_group()
@@ -90,3 +95,37 @@ def test_sharded_run_equals_single_process(tmp_path, world):
                                periods=b.periods), b.minthk, 1)
     for k in ("pv", "sen_vs", "sen_vp", "sen_rho", "lsen", "status"):
         np.testing.assert_array_equal(got[k], ref[k], err_msg=k)
+
+
+def _gather_worker(rank, world, port, path):
+    import sys
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    sys.path.insert(0, root)
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=120))
+    try:
+        # uneven blocks, one rank with empty ones, two dtypes
+        n = [5, 0, 3][rank]
+        blocks = {"a": torch.arange(n, dtype=torch.float64) + 100 * rank,
+                  "b": torch.full((2 * n,), rank, dtype=torch.int32)}
+        out = shard.gather_blocks(blocks, dst=world - 1)
+        if rank == world - 1:
+            np.savez(path, a=out["a"].numpy(), b=out["b"].numpy())
+        else:
+            assert out is None
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_gather_blocks_concatenates_in_rank_order(tmp_path):
+    path = str(tmp_path / "g.npz")
+    mp.start_processes(_gather_worker, args=(3, _free_port(), path), nprocs=3, join=True,
+                       start_method="spawn")
+    g = np.load(path)
+    np.testing.assert_array_equal(g["a"], np.concatenate([np.arange(5.0), 200 + np.arange(3.0)]))
+    np.testing.assert_array_equal(g["b"], np.array([0] * 10 + [2] * 6, np.int32))
