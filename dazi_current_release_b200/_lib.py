@@ -39,7 +39,7 @@ EXPORTS = (
     "dazi_dk_iso_noalloc_dev", "dazi_dk_batch", "dazi_dk_batch_dev", "dazi_dk_set_timing",
     "dazi_dk_last_timing", "dazi_dk_last_items", "dazi_dk_plan_create", "dazi_dk_plan_launch",
     "dazi_dk_plan_status", "dazi_dk_plan_config", "dazi_dk_plan_destroy", "dazi_dk_grows_dev",
-    "dazi_dk_azimuthal_map_dev",
+    "dazi_dk_azimuthal_map_dev", "dazi_lsmr", "dazi_lsmr_dev",
 )
 
 
@@ -130,6 +130,14 @@ def load(build_if_missing: bool = True):
     L.dazi_dk_grows_dev.restype = _int
     L.dazi_dk_azimuthal_map_dev.argtypes = [_int] * 4 + [vp_] * 10
     L.dazi_dk_azimuthal_map_dev.restype = _int
+    ll_p = ctypes.POINTER(ctypes.c_longlong)
+    L.dazi_lsmr.argtypes = [ip, ip, ll_p, ll_p, ip, fp, _f64p, _f64p, _f64p, _f64p, _f64p, ip, ip,
+                            ip, _f64p, ip, ip, _f64p, _f64p, _f64p, _f64p, _f64p]
+    L.dazi_lsmr.restype = _int
+    L.dazi_lsmr_dev.argtypes = [_int, _int, ll, vp_, vp_, vp_, _int, vp_, ctypes.c_double,
+                                ctypes.c_double, ctypes.c_double, ctypes.c_double, _int, vp_,
+                                ip, ip, _f64p, vp_]
+    L.dazi_lsmr_dev.restype = _int
     L.dazi_dk_fp64_peak.argtypes = [_f64p]
     L.dazi_dk_fp64_peak.restype = _int
     L.dazi_dk_finalize.argtypes = []

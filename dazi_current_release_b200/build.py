@@ -12,7 +12,7 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libdazi_dk.so")
-SOURCES = ["capi.cu", "k_plain.cu", "k_adjoint.cu", "k_ti.cu", "k_prep.cu", "k_probe.cu", "k_noalloc.cu", "k_epilogue.cu"]
+SOURCES = ["capi.cu", "k_plain.cu", "k_adjoint.cu", "k_ti.cu", "k_prep.cu", "k_probe.cu", "k_noalloc.cu", "k_epilogue.cu", "k_lsmr.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

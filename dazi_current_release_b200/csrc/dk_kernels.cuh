@@ -56,11 +56,11 @@ struct AdjArgs {
     const double* croot_b = nullptr;   // group velocity: roots at t1b (0: none)
 };
 
-// Doubles per refined layer in each persistent thread's Gc/Gs scratch:
-// the up-sweep's compound vector and exponent sum (6), then the layer's
-// eigen-solution (12), its two waves (5 + 5) and flags (1), which the
-// down-sweep reads back instead of recomputing them.
-constexpr int TI_SCR_Q = 29;
+// Doubles per refined layer in each persistent thread's Gc/Gs scratch: the
+// up-sweep's compound vector and exponent sum (6); the down-sweep forms the
+// layer's eigen-solution and waves again and overwrites entries 0..2 with
+// the layer's raw partials once the vector is consumed.
+constexpr int TI_SCR_Q = 6;
 
 struct TiArgs {
     Tables T;

@@ -29,6 +29,7 @@
 // evaluation points is the reference's, step for step.
 #pragma once
 #include "dk_model.cuh"
+#include <type_traits>
 #include <utility>
 
 namespace dk {
@@ -391,8 +392,12 @@ struct HasGroupRoots<O, decltype((void)std::declval<O&>().group_roots(0, 0.0, 0.
 // refinement evaluations per period on uneven columns.
 constexpr double kFastRootTol = 1.0e-10;
 
+// Brent's state: the last step and the one before (FAST instantiations only)
+struct BrentSteps { double bd, be; };
+struct NoBrentSteps {};
+
 template <bool GROUP = false, bool FAST = false>
-struct RootSM {
+struct RootSM : std::conditional_t<FAST, BrentSteps, NoBrentSteps> {
     static_assert(!(GROUP && FAST), "the Brent refinement serves phase velocity");
     enum Phase : int { START = 0, GS_FIRST, GS_SCAN, VER1, VER2, NEV_A, NEV_B, NEV_CD, DONE,
                        GR_START, BRENT_INIT, BRENT };
@@ -415,8 +420,6 @@ struct RootSM {
     bool second;
     float t1a, t1b;
     double cph, cph_t;
-    // Brent (FAST): the last step and the one before
-    double bd, be;
 
     __device__ void init(double cc_, float betmx_, int kmax_, double tol_, bool scan32 = false)
     {
@@ -500,18 +503,22 @@ struct RootSM {
                 return begin_nevill();
             }
             case BRENT_INIT: {
-                // a = c1 (del1), b = c2 (del2): getsol's bracket; c = a
-                c3 = c1; del3 = del1;
-                bd = c2 - c1; be = bd;
-                nctrl = 0;
-                if (brent_iter(out)) return true;
-                if (phase != DONE) continue;
+                if constexpr (FAST) {
+                    // a = c1 (del1), b = c2 (del2): getsol's bracket; c = a
+                    c3 = c1; del3 = del1;
+                    this->bd = c2 - c1; this->be = this->bd;
+                    nctrl = 0;
+                    if (brent_iter(out)) return true;
+                    if (phase != DONE) continue;
+                }
                 return false;
             }
             case BRENT: {
-                del2 = F;
-                if (brent_iter(out)) return true;
-                if (phase != DONE) continue;
+                if constexpr (FAST) {
+                    del2 = F;
+                    if (brent_iter(out)) return true;
+                    if (phase != DONE) continue;
+                }
                 return false;
             }
             case NEV_A:
@@ -687,6 +694,8 @@ struct RootSM {
     template <class Out>
     __device__ bool brent_iter(Out& out)
     {
+        double& bd = this->bd;
+        double& be = this->be;
         if ((del2 > 0.0) == (del3 > 0.0)) { c3 = c1; del3 = del1; bd = c2 - c1; be = bd; }
         if (fabs(del3) < fabs(del2)) {
             c1 = c2; c2 = c3; c3 = c1;

@@ -835,37 +835,6 @@ __device__ __noinline__ D5 ti_halfspace_cdv(TiLayer L, double omega, double wvno
     return c;
 }
 
-// Layer stash (scratch entries 6..28 of a layer): eigen-solution, waves
-// (cosf, rsin, sinr, ex or ei, er: an oscillatory wave has ex = 0, an
-// evanescent one ei = 0) and flags (1 real eigenvalues, 2 oscp, 4 oscs).
-__device__ __forceinline__ void ti_stash_store(double* st, long long ns, const TiEig& E, const TiWave& P,
-                                               const TiWave& S)
-{
-    st[6 * ns] = E.x11; st[7 * ns] = E.x21; st[8 * ns] = E.x31; st[9 * ns] = E.x41;
-    st[10 * ns] = E.x12; st[11 * ns] = E.x22; st[12 * ns] = E.x32; st[13 * ns] = E.x42;
-    st[14 * ns] = E.np; st[15 * ns] = E.nsv; st[16 * ns] = E.rp; st[17 * ns] = E.rsv;
-    st[18 * ns] = P.cosf; st[19 * ns] = P.rsin; st[20 * ns] = P.sinr;
-    st[21 * ns] = E.oscp ? P.ei : P.ex; st[22 * ns] = P.er;
-    st[23 * ns] = S.cosf; st[24 * ns] = S.rsin; st[25 * ns] = S.sinr;
-    st[26 * ns] = E.oscs ? S.ei : S.ex; st[27 * ns] = S.er;
-    st[28 * ns] = (double)(1 | (E.oscp ? 2 : 0) | (E.oscs ? 4 : 0));
-}
-
-__device__ __forceinline__ void ti_stash_load(const double* st, long long ns, int fl, TiEig& E, TiWave& P,
-                                              TiWave& S)
-{
-    E.x11 = st[6 * ns]; E.x21 = st[7 * ns]; E.x31 = st[8 * ns]; E.x41 = st[9 * ns];
-    E.x12 = st[10 * ns]; E.x22 = st[11 * ns]; E.x32 = st[12 * ns]; E.x42 = st[13 * ns];
-    E.np = st[14 * ns]; E.nsv = st[15 * ns]; E.rp = st[16 * ns]; E.rsv = st[17 * ns];
-    E.ok = true; E.oscp = (fl & 2) != 0; E.oscs = (fl & 4) != 0;
-    P.cosf = st[18 * ns]; P.rsin = st[19 * ns]; P.sinr = st[20 * ns];
-    const double p4 = st[21 * ns];
-    P.ex = E.oscp ? 0.0 : p4; P.ei = E.oscp ? p4 : 0.0; P.er = st[22 * ns];
-    S.cosf = st[23 * ns]; S.rsin = st[24 * ns]; S.sinr = st[25 * ns];
-    const double s4 = st[26 * ns];
-    S.ex = E.oscs ? 0.0 : s4; S.ei = E.oscs ? s4 : 0.0; S.er = st[27 * ns];
-}
-
 __device__ __forceinline__ long long ti_next_task(unsigned* queue)
 {
     unsigned t = 0;
@@ -904,7 +873,14 @@ __device__ __forceinline__ void ti_task(const TiArgs& a, long long task, int lan
         const double wvno = omega / (double)cpf;
         const double wvno2 = wvno * wvno;
         const double iwvno = 1.0 / wvno, iwvno2 = 1.0 / wvno2;
-        // ---- up(): compound vectors from the half-space upward
+        // ---- up() (compound vectors from the half-space upward), then
+        // down() + svfunc() + energy() (interface by interface), as one loop
+        // of 2 rmax - 1 steps: steps 0 .. rmax-2 are up-sweep layers
+        // rmax-2 .. 0, the rest down-sweep layers 0 .. rmax-1.  A layer's
+        // eigen-solution and waves are formed at the top of the step by the
+        // one copy of that code, in both sweeps, so the down-sweep forms
+        // them again instead of reading them back: the per-layer scratch is
+        // the compound vector and its exponent sum only.
         constexpr int Q = TI_SCR_Q;
         double cdv[5];
         double exsum = 0.0;
@@ -915,63 +891,68 @@ __device__ __forceinline__ void ti_task(const TiArgs& a, long long task, int lan
             for (int q = 0; q < 5; ++q) { cdv[q] = c.v[q]; sp[q * nslots] = cdv[q]; }
             sp[5 * nslots] = 0.0;
         }
-        for (int m = rmax - 2; m >= 0; --m) {
-            const TiLayer L = ti_layer(tir + (long long)m * TILE);
-            double* sp = scr + (long long)m * Q * nslots;
-            TiEig E;
-            ti_eigen(L, omega, wvno, wvno2, E);
-            double ee[5];
-            double pexsv;
-            if (E.ok) {
-                // P and S waves through one copy of the wave code
-                TiWave P, S;
-#pragma unroll 1
-                for (int w = 0; w < 2; ++w) {
-                    const TiWave t = ti_wave(w ? E.rsv : E.rp, w ? E.oscs : E.oscp, L.td);
-                    if (w) S = t; else P = t;
-                }
-                TiVar V;
-                V.cosp = P.cosf; V.rsinp = P.rsin; V.sinpr = P.sinr; V.pex = P.ex;
-                V.cosq = S.cosf; V.rsinq = S.rsin; V.sinqr = S.sinr; V.svex = S.ex;
-                ti_compound_apply(E, V, cdv, ee);
-                pexsv = P.ex + S.ex;
-                ti_stash_store(sp, nslots, E, P, S);
-            } else {
-                D5 c5;
-#pragma unroll
-                for (int i = 0; i < 5; ++i) c5.v[i] = cdv[i];
-                const UpOut u = ti_up_general(L, omega, wvno, wvno2, c5);
-#pragma unroll
-                for (int i = 0; i < 5; ++i) ee[i] = u.ee.v[i];
-                pexsv = u.pexsv;
-                sp[28 * nslots] = 0.0;
-            }
-            const double exn = pow2_normalise(ee, 5);
-            exsum = exsum + pexsv + exn;
-#pragma unroll
-            for (int q = 0; q < 5; ++q) { cdv[q] = ee[q]; sp[q * nslots] = ee[q]; }
-            sp[5 * nslots] = exsum;
-        }
-        // ---- down() + svfunc() + energy(): interface by interface
-        const double exe0 = exsum;     // exe(1)
-        const double f1213 = -cdv[1];
-        const double if1213 = 1.0 / f1213;
-        double top[4] = {cdv[2] / cdv[1], 1.0, 0.0, 0.0};   // ur, uz, tz, tr at the surface
-        double vv[4] = {1.0, 0.0, 0.0, 0.0};
+        double exe0 = 0.0, if1213 = 0.0;
+        double top[4] = {0.0, 0.0, 0.0, 0.0}, vv[4] = {1.0, 0.0, 0.0, 0.0};
         double exa = 0.0;
         double sumi0 = 0.0, sumi1 = 0.0, sumi2 = 0.0, gsum = 0.0;
         const double pi_ = 3.141592653589493;   // gammap's constant, as in the reference
         const double lw = log(omega / (2.0 * pi_ * 1.0)) / pi_;
-        for (int m = 0; m < rmax; ++m) {
-            const TiLayer L = ti_layer(tir + (long long)m * TILE);
-            double bot[4] = {0.0, 0.0, 0.0, 0.0};
+        const int nsteps = 2 * rmax - 1;
+        for (int step = 0; step < nsteps; ++step) {
+            const bool up = step < rmax - 1;
+            const int m = up ? rmax - 2 - step : step - (rmax - 1);
             const bool half = (m == rmax - 1);
-            const double* st = scr + (long long)m * Q * nslots;
-            const int fl = half ? 0 : (int)st[28 * nslots];
-            const bool fast = (fl & 1) != 0;
+            const TiLayer L = ti_layer(tir + (long long)m * TILE);
             TiEig E;
             TiWave P, S;
-            if (fast) ti_stash_load(st, nslots, fl, E, P, S);
+            E.ok = false;
+            if (!half) {
+                ti_eigen(L, omega, wvno, wvno2, E);
+                if (E.ok) {
+                    // P and S waves through one copy of the wave code
+#pragma unroll 1
+                    for (int w = 0; w < 2; ++w) {
+                        const TiWave t = ti_wave(w ? E.rsv : E.rp, w ? E.oscs : E.oscp, L.td);
+                        if (w) S = t; else P = t;
+                    }
+                }
+            }
+            const bool fast = E.ok;
+            if (up) {
+                double* sp = scr + (long long)m * Q * nslots;
+                double ee[5];
+                double pexsv;
+                if (fast) {
+                    TiVar V;
+                    V.cosp = P.cosf; V.rsinp = P.rsin; V.sinpr = P.sinr; V.pex = P.ex;
+                    V.cosq = S.cosf; V.rsinq = S.rsin; V.sinqr = S.sinr; V.svex = S.ex;
+                    ti_compound_apply(E, V, cdv, ee);
+                    pexsv = P.ex + S.ex;
+                } else {
+                    D5 c5;
+#pragma unroll
+                    for (int i = 0; i < 5; ++i) c5.v[i] = cdv[i];
+                    const UpOut u = ti_up_general(L, omega, wvno, wvno2, c5);
+#pragma unroll
+                    for (int i = 0; i < 5; ++i) ee[i] = u.ee.v[i];
+                    pexsv = u.pexsv;
+                }
+                const double exn = pow2_normalise(ee, 5);
+                exsum = exsum + pexsv + exn;
+#pragma unroll
+                for (int q = 0; q < 5; ++q) { cdv[q] = ee[q]; sp[q * nslots] = ee[q]; }
+                sp[5 * nslots] = exsum;
+                continue;
+            }
+            if (m == 0) {
+                // the surface: exe(1), and ur, uz, tz, tr from the top
+                // compound vector
+                exe0 = exsum;
+                const double f1213 = -cdv[1];
+                if1213 = 1.0 / f1213;
+                top[0] = cdv[2] / cdv[1]; top[1] = 1.0; top[2] = 0.0; top[3] = 0.0;
+            }
+            double bot[4] = {0.0, 0.0, 0.0, 0.0};
             if (!half) {
                 double cpex;
                 if (fast) {

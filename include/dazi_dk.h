@@ -287,6 +287,39 @@ int dazi_dk_azimuthal_map_dev(int nx, int ny, int nz, int kmaxRc,
                               float *cosRc, float *sinRc, float *amp,
                               float *amp_rel, float *angle, void *stream);
 
+/* LSMR least squares on the system the G rows fill: replaces LSMR(m, n,
+ * leniw, lenrw, iw, rw, b, damp, atol, btol, conlim, itnlim, localSize,
+ * nout, x, istop, itn, normA, condA, normr, normAr, normx) of
+ * code/src_inv_iso_joint/lsmrModule.f90:36 (the matrix as aprod.f90 reads
+ * it: row indices iw(1:lenrw), column indices iw(lenrw+1:2*lenrw),
+ * 1-based, values rw(1:lenrw) real*4; b, x real*8), all arguments by
+ * reference as the Fortran passes them.  Solves min ||(A; damp I) x -
+ * (b; 0)|| by LSMR (Fong & Saunders 2011) in FP64 on the GPU with the
+ * stopping rules atol, btol, conlim, itnlim and the outputs istop (0..7),
+ * itn and the estimates normA, condA, normr, normAr, normx.  Like the
+ * reference's SciPy backend (scipy_lsmr_solve, which calls
+ * scipy.sparse.linalg.lsmr), it does no local reorthogonalization:
+ * localSize and nout are accepted and not used.  Duplicate (row, col)
+ * entries add. */
+int dazi_lsmr(const int *m, const int *n, const long long *leniw,
+              const long long *lenrw, const int *iw, const float *rw,
+              const double *b, const double *damp, const double *atol,
+              const double *btol, const double *conlim, const int *itnlim,
+              const int *localSize, const int *nout, double *x, int *istop,
+              int *itn, double *normA, double *condA, double *normr,
+              double *normAr, double *normx);
+
+/* Device-pointer form: nnz triplets (row, col, val) with 0- or 1-based
+ * indices (index_base), b (m) and x (n) real*8 in device memory;
+ * norms[0..4] (host, may be NULL) = normA, condA, normr, normAr, normx.
+ * Stream-ordered on `stream`; the host waits once per 16 iterations to
+ * read the stop flag, and returns when the solve has finished. */
+int dazi_lsmr_dev(int m, int n, long long nnz, const int *row, const int *col,
+                  const float *val, int index_base, const double *b,
+                  double damp, double atol, double btol, double conlim,
+                  int itnlim, double *x, int *istop, int *itn, double *norms,
+                  void *stream);
+
 /* Per-phase timing: with dazi_dk_set_timing(1), each call records CUDA
  * events on its stream around its phases ("prep", "fd", "root", "adjoint",
  * "ti"); dazi_dk_last_timing fills up to cap (name, milliseconds) pairs of

@@ -16,7 +16,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 def header_functions():
     text = open(os.path.join(ROOT, "include", "dazi_dk.h")).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
-    return sorted(set(re.findall(r"\b(dazi_dk_\w+)\s*\(", text)))
+    return sorted(set(re.findall(r"\b(dazi_\w+)\s*\(", text)))
 
 
 def test_library_exports_every_declared_symbol():
@@ -33,7 +33,7 @@ def header_arity():
     text = open(os.path.join(ROOT, "include", "dazi_dk.h")).read()
     text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
     out = {}
-    for name, params in re.findall(r"\b(dazi_dk_\w+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
+    for name, params in re.findall(r"\b(dazi_\w+)\s*\(([^;{]*?)\)\s*;", text, flags=re.S):
         params = params.strip()
         out[name] = 0 if params in ("", "void") else params.count(",") + 1
     return out

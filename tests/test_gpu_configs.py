@@ -99,7 +99,7 @@ def test_config4_fp32_scan_fp64_scan_and_oracle(oracle):
     nx, ny, nz = case.vel.shape
     K = case.periods.size
     run = lambda form: dk.depthkernel(nx, ny, nz, case.vel, 2, 0, K, case.periods,  # noqa: E731
-                                      case.depz, case.minthk, form=form, kernels=False)
+                                      case.depz, case.minthk, form=form, kernels=False)[0]
     pv64 = run(dk.FORM_ADJOINT)
     st64 = last_status(nx * ny)
     pv32 = run(dk.FORM_ADJOINT | dk.FORM_SCAN_FP32)
