@@ -59,114 +59,9 @@ __device__ __forceinline__ void normc_pow2(double& e0, double& e1, double& e2, d
     e0 *= sc; e1 *= sc; e2 *= sc; e3 *= sc; e4 *= sc;
 }
 
-// Entries of one layer's Dunkin compound matrix (dnka(), surfdisp96.f:
-// 1018-1062, with var()'s wave factors, :868-985): what the product with
-// the vector needs, using ca's symmetries.  They depend on the layer and on
-// (omega, wvno) only, not on the vector from below.
-struct Dunkin {
-    double c11, c12, c13, c14, c15, c21, c22, c23, c24, c33, c41, c42, c43, c51, c53;
-};
-
-__device__ __forceinline__ Dunkin dunkin_layer(const LayerD& L, double wvno, double wvno2,
-                                               double omega, double tio2)
-{
-    const double dpth = L.d;
-    const double xka = omega * L.ia, xkb = omega * L.ib;
-    const double gammk = L.b2 * tio2;
-    const double gam = gammk * wvno2;
-    const double pa = (wvno + xka) * fabs(wvno - xka);
-    const double pb = (wvno + xkb) * fabs(wvno - xkb);
-    const double ira = rsqrt(pa), irb = rsqrt(pb);
-    const double ra = pa * ira, rb = pb * irb;
-    const double p = ra * dpth, q = rb * dpth;
-    // var(): cos/sin (oscillatory) or scaled cosh/sinh (evanescent)
-    double w, x, cosp, y, z, cosq, ep = 1.0, eq = 1.0;
-    bool evp = false, evq = false;
-    if (wvno < xka) {
-        double sp, cp;
-        sincos(p, &sp, &cp);
-        w = sp * ira; x = -ra * sp; cosp = cp;
-    } else if (wvno == xka) {
-        cosp = 1.0; w = dpth; x = 0.0;
-    } else {
-        evp = true;
-        ep = exp(-p);
-        const double fac = (p < 16.0) ? ep * ep : 0.0;
-        cosp = (1.0 + fac) * 0.5;
-        const double sinp = (1.0 - fac) * 0.5;
-        w = sinp * ira; x = ra * sinp;
-    }
-    if (wvno < xkb) {
-        double sq, cq;
-        sincos(q, &sq, &cq);
-        y = sq * irb; z = -rb * sq; cosq = cq;
-    } else if (wvno == xkb) {
-        cosq = 1.0; y = dpth; z = 0.0;
-    } else {
-        evq = true;
-        eq = exp(-q);
-        const double fac = (q < 16.0) ? eq * eq : 0.0;
-        cosq = (1.0 + fac) * 0.5;
-        const double sinq = (1.0 - fac) * 0.5;
-        y = sinq * irb; z = rb * sinq;
-    }
-    // a0 = exp(-(pex + sex)), 0 once the exponent reaches 60
-    const double exa = (evp ? p : 0.0) + (evq ? q : 0.0);
-    const double a0 = (exa < 60.0) ? ep * eq : 0.0;
-    const double cpcq = cosp * cosq, cpy = cosp * y, cpz = cosp * z;
-    const double cqw = cosq * w, cqx = cosq * x;
-    const double xy = x * y, xz = x * z, wy = w * y, wz = w * z;
-    // dnka(): Dunkin compound matrix
-    const double rho1 = L.rho;
-    const double rinv = L.irho, rho2 = rho1 * rho1, r2inv = rinv * rinv;
-    const double gamm1l = gam - 1.0, twgm1 = gam + gamm1l, gmgmk = gam * gammk;
-    const double gmgm1 = gam * gamm1l, gm1sq = gamm1l * gamm1l;
-    const double a0pq = a0 - cpcq;
-    Dunkin C;
-    C.c11 = cpcq - 2.0 * gmgm1 * a0pq - gmgmk * xz - wvno2 * gm1sq * wy;
-    C.c12 = (wvno2 * cpy - cqx) * rinv;
-    C.c13 = -(twgm1 * a0pq + gammk * xz + wvno2 * gamm1l * wy) * rinv;
-    C.c14 = (cpz - wvno2 * cqw) * rinv;
-    C.c15 = -(2.0 * wvno2 * a0pq + xz + wvno2 * wvno2 * wy) * r2inv;
-    C.c21 = (gmgmk * cpz - gm1sq * cqw) * rho1;
-    C.c22 = cpcq;
-    C.c23 = gammk * cpz - gamm1l * cqw;
-    C.c24 = -wz;
-    C.c41 = (gm1sq * cpy - gmgmk * cqx) * rho1;
-    C.c42 = -xy;
-    C.c43 = gamm1l * cpy - gammk * cqx;
-    C.c51 = -(2.0 * gmgmk * gm1sq * a0pq + gmgmk * gmgmk * xz + gm1sq * gm1sq * wy) * rho2;
-    C.c53 = -(gammk * gamm1l * twgm1 * a0pq + gam * gammk * gammk * xz + gamm1l * gm1sq * wy) * rho1;
-    C.c33 = a0 + 2.0 * (cpcq - C.c11);
-    return C;
-}
-
-// e <- e * CA, then normc (scaled by a power of two)
-__device__ __forceinline__ void dunkin_apply(const Dunkin& C, double wvno2, double& e0, double& e1,
-                                             double& e2, double& e3, double& e4)
-{
-    const double tt = -2.0 * wvno2;
-    const double c31 = tt * C.c53, c32 = tt * C.c43;
-    const double c34 = tt * C.c23, c35 = tt * C.c13;
-    // ee(i) = sum_j e(j) * ca(j,i), using ca's symmetries
-    //   ca(2,5)=ca(1,4) ca(4,4)=ca(2,2) ca(4,5)=ca(1,2) ca(5,2)=ca(4,1)
-    //   ca(5,4)=ca(2,1) ca(5,5)=ca(1,1)
-    const double f0 = e0 * C.c11 + e1 * C.c21 + e2 * c31 + e3 * C.c41 + e4 * C.c51;
-    const double f1 = e0 * C.c12 + e1 * C.c22 + e2 * c32 + e3 * C.c42 + e4 * C.c41;
-    const double f2 = e0 * C.c13 + e1 * C.c23 + e2 * C.c33 + e3 * C.c43 + e4 * C.c53;
-    const double f3 = e0 * C.c14 + e1 * C.c24 + e2 * c34 + e3 * C.c22 + e4 * C.c21;
-    const double f4 = e0 * C.c15 + e1 * C.c14 + e2 * c35 + e3 * C.c12 + e4 * C.c11;
-    e0 = f0; e1 = f1; e2 = f2; e3 = f3; e4 = f4;
-    normc_pow2(e0, e1, e2, e3, e4);
-}
-
 // Secular-function value at wavenumber wvno, angular frequency omega.
 // Each layer product is rescaled (normc_pow2); the factors are discarded,
-// as in the reference, since they do not move roots.  The loop forms the
-// next layer's matrix (independent of the vector) before it applies the
-// current one, so each step carries two independent chains of work; the
-// layer record two steps ahead is loaded at the top of the step (the
-// columns' tables exceed L2, and a step covers that latency).
+// as in the reference, since they do not move roots.
 template <class M>
 __device__ __forceinline__ double dltar4(const M& mdl, int mmax, double wvno, double omega)
 {
@@ -174,31 +69,109 @@ __device__ __forceinline__ double dltar4(const M& mdl, int mmax, double wvno, do
     const double wvno2 = wvno * wvno;
     const double iom = 1.0 / omega;
     const double tio2 = 2.0 * iom * iom;
-    const LayerD H = mdl.layer(mmax - 1);
-    const double xka = omega * H.ia, xkb = omega * H.ib;
-    const double ra = sqrt((wvno + xka) * fabs(wvno - xka));
-    const double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
-    const double gammk = H.b2 * tio2;
-    const double gam = gammk * wvno2;
-    const double gamm1 = gam - 1.0;
-    const double rho1 = H.rho;
+    LayerD L = mdl.layer(mmax - 1);
+    double xka = omega * L.ia, xkb = omega * L.ib;
+    double ra = sqrt((wvno + xka) * fabs(wvno - xka));
+    double rb = sqrt((wvno + xkb) * fabs(wvno - xkb));
+    double gammk = L.b2 * tio2;
+    double gam = gammk * wvno2;
+    double gamm1 = gam - 1.0;
+    double rho1 = L.rho;
     double e0 = rho1 * rho1 * (gamm1 * gamm1 - gam * gammk * ra * rb);
     double e1 = -rho1 * ra;
     double e2 = rho1 * (gamm1 - gammk * ra * rb);
     double e3 = rho1 * rb;
     double e4 = wvno2 - ra * rb;
-    if (mmax < 2) return e0;   // no layer above the half-space: no normc
-    Dunkin C = dunkin_layer(mdl.layer(mmax - 2), wvno, wvno2, omega, tio2);
-    LayerD Ln = mdl.layer(mmax >= 3 ? mmax - 3 : 0);
+    // the next layer's record is loaded one step ahead: the loads of a
+    // column's table come from L2/DRAM (the resident columns' tables exceed
+    // L2) and a layer step is long enough to cover that latency
+    LayerD Ln = mdl.layer(mmax >= 2 ? mmax - 2 : 0);
 #pragma unroll 1
     for (int m = mmax - 2; m >= 0; --m) {
-        const LayerD L = Ln;                          // layer m-1
-        Ln = mdl.layer(m >= 2 ? m - 2 : 0);
-        Dunkin Cn;
-        if (m > 0) Cn = dunkin_layer(L, wvno, wvno2, omega, tio2);
-        dunkin_apply(C, wvno2, e0, e1, e2, e3, e4);
-        C = Cn;
+        L = Ln;
+        Ln = mdl.layer(m > 0 ? m - 1 : 0);
+        const double dpth = L.d;
+        xka = omega * L.ia; xkb = omega * L.ib;
+        gammk = L.b2 * tio2;
+        gam = gammk * wvno2;
+        const double pa = (wvno + xka) * fabs(wvno - xka);
+        const double pb = (wvno + xkb) * fabs(wvno - xkb);
+        const double ira = rsqrt(pa), irb = rsqrt(pb);
+        ra = pa * ira; rb = pb * irb;
+        const double p = ra * dpth, q = rb * dpth;
+        // var(): cos/sin (oscillatory) or scaled cosh/sinh (evanescent)
+        double w, x, cosp, y, z, cosq, ep = 1.0, eq = 1.0;
+        bool evp = false, evq = false;
+        if (wvno < xka) {
+            double sp, cp;
+            sincos(p, &sp, &cp);
+            w = sp * ira; x = -ra * sp; cosp = cp;
+        } else if (wvno == xka) {
+            cosp = 1.0; w = dpth; x = 0.0;
+        } else {
+            evp = true;
+            ep = exp(-p);
+            const double fac = (p < 16.0) ? ep * ep : 0.0;
+            cosp = (1.0 + fac) * 0.5;
+            const double sinp = (1.0 - fac) * 0.5;
+            w = sinp * ira; x = ra * sinp;
+        }
+        if (wvno < xkb) {
+            double sq, cq;
+            sincos(q, &sq, &cq);
+            y = sq * irb; z = -rb * sq; cosq = cq;
+        } else if (wvno == xkb) {
+            cosq = 1.0; y = dpth; z = 0.0;
+        } else {
+            evq = true;
+            eq = exp(-q);
+            const double fac = (q < 16.0) ? eq * eq : 0.0;
+            cosq = (1.0 + fac) * 0.5;
+            const double sinq = (1.0 - fac) * 0.5;
+            y = sinq * irb; z = rb * sinq;
+        }
+        // a0 = exp(-(pex + sex)), 0 once the exponent reaches 60
+        const double exa = (evp ? p : 0.0) + (evq ? q : 0.0);
+        const double a0 = (exa < 60.0) ? ep * eq : 0.0;
+        const double cpcq = cosp * cosq, cpy = cosp * y, cpz = cosp * z;
+        const double cqw = cosq * w, cqx = cosq * x;
+        const double xy = x * y, xz = x * z, wy = w * y, wz = w * z;
+        // dnka(): Dunkin compound matrix
+        rho1 = L.rho;
+        const double rinv = L.irho, rho2 = rho1 * rho1, r2inv = rinv * rinv;
+        const double gamm1l = gam - 1.0, twgm1 = gam + gamm1l, gmgmk = gam * gammk;
+        const double gmgm1 = gam * gamm1l, gm1sq = gamm1l * gamm1l;
+        const double a0pq = a0 - cpcq;
+        const double c11 = cpcq - 2.0 * gmgm1 * a0pq - gmgmk * xz - wvno2 * gm1sq * wy;
+        const double c12 = (wvno2 * cpy - cqx) * rinv;
+        const double c13 = -(twgm1 * a0pq + gammk * xz + wvno2 * gamm1l * wy) * rinv;
+        const double c14 = (cpz - wvno2 * cqw) * rinv;
+        const double c15 = -(2.0 * wvno2 * a0pq + xz + wvno2 * wvno2 * wy) * r2inv;
+        const double c21 = (gmgmk * cpz - gm1sq * cqw) * rho1;
+        const double c22 = cpcq;
+        const double c23 = gammk * cpz - gamm1l * cqw;
+        const double c24 = -wz;
+        const double c41 = (gm1sq * cpy - gmgmk * cqx) * rho1;
+        const double c42 = -xy;
+        const double c43 = gamm1l * cpy - gammk * cqx;
+        const double c51 = -(2.0 * gmgmk * gm1sq * a0pq + gmgmk * gmgmk * xz + gm1sq * gm1sq * wy) * rho2;
+        const double c53 = -(gammk * gamm1l * twgm1 * a0pq + gam * gammk * gammk * xz + gamm1l * gm1sq * wy) * rho1;
+        const double tt = -2.0 * wvno2;
+        const double c31 = tt * c53, c32 = tt * c43;
+        const double c33 = a0 + 2.0 * (cpcq - c11);
+        const double c34 = tt * c23, c35 = tt * c13;
+        // ee(i) = sum_j e(j) * ca(j,i), using ca's symmetries
+        //   ca(2,5)=ca(1,4) ca(4,4)=ca(2,2) ca(4,5)=ca(1,2) ca(5,2)=ca(4,1)
+        //   ca(5,4)=ca(2,1) ca(5,5)=ca(1,1)
+        const double f0 = e0 * c11 + e1 * c21 + e2 * c31 + e3 * c41 + e4 * c51;
+        const double f1 = e0 * c12 + e1 * c22 + e2 * c32 + e3 * c42 + e4 * c41;
+        const double f2 = e0 * c13 + e1 * c23 + e2 * c33 + e3 * c43 + e4 * c53;
+        const double f3 = e0 * c14 + e1 * c24 + e2 * c34 + e3 * c22 + e4 * c21;
+        const double f4 = e0 * c15 + e1 * c14 + e2 * c35 + e3 * c12 + e4 * c11;
+        e0 = f0; e1 = f1; e2 = f2; e3 = f3; e4 = f4;
+        normc_pow2(e0, e1, e2, e3, e4);
     }
+    if (mmax < 2) return e0;   // no layer above the half-space: no normc
     // the top layer's normc(): e0 / max|e|
     double t1 = fmax(fmax(fmax(fabs(e0), fabs(e1)), fmax(fabs(e2), fabs(e3))), fabs(e4));
     if (t1 < 1.0e-40) t1 = 1.0;
