@@ -68,12 +68,12 @@ struct DBuf {
 // task list, the counters and the sweep scratch (the global entries share
 // one; every plan owns one).
 struct Work {
-    DBuf croot, crootb, counters, adjscr, tiscr;
+    DBuf croot, crootb, counters, adjscr, tiscr, tiord;
     DBuf keys, keys2, cidx, cidx2, rmaxb, trecs, ttasks, tlbase, ttbase, cubtmp;
     DBuf tflat, tld, tti, tsp, tch, tmeta, ttasklist;
     void release()
     {
-        DBuf* all[] = {&croot, &crootb, &counters, &adjscr, &tiscr, &keys, &keys2, &cidx, &cidx2, &rmaxb,
+        DBuf* all[] = {&croot, &crootb, &counters, &adjscr, &tiscr, &tiord, &keys, &keys2, &cidx, &cidx2, &rmaxb,
                        &trecs, &ttasks, &tlbase, &ttbase, &cubtmp, &tflat, &tld, &tti, &tsp,
                        &tch, &tmeta, &ttasklist};
         for (DBuf* b : all) b->release();
@@ -431,6 +431,7 @@ int ensure_sweep_scratch(const Tables& T, bool adj, bool ti, long long maxr, con
         if ((r = launch_persistent_grid(ti_fn(cfg.ti_minb), nitems, 128, nblk))) return r;
         const size_t scr = sizeof(double) * TI_SCR_Q * (size_t)maxr * (size_t)(nblk * 128);
         if ((r = W.tiscr.ensure(scr))) return r;
+        if ((r = W.tiord.ensure(sizeof(int) * (size_t)nitems))) return r;
     }
     return 0;
 }
@@ -516,6 +517,12 @@ int run_ti(const Tables& T, const double* per, const StageOut& o, long long maxr
     t.T = T; t.periods = per; t.pv = o.pv; t.lsen = o.lsen;
     t.scratch = W.tiscr.as<double>(); t.scr_layers = maxr; t.queue = queues + 1;
     t.errflag = reinterpret_cast<int*>(c + 1);
+    t.order = W.tiord.as<int>();
+    const long long ntiles = (T.ncols + TILE - 1) / TILE;
+    ti_order_kernel<<<(unsigned)ntiles, TI_ORDER_THREADS, 0, st>>>(t, W.ttbase.as<long long>(),
+                                                                 W.ttasks.as<long long>());
+    CK(cudaGetLastError());
+    ++g_ctx.last_launches;
     if (cfg.ti_minb == 2) ti_kernel<2><<<(unsigned)nblk, 128, 0, st>>>(t);
     else if (cfg.ti_minb == 3) ti_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(t);
     else if (cfg.ti_minb == 4) ti_kernel<4><<<(unsigned)nblk, 128, 0, st>>>(t);
@@ -1444,7 +1451,7 @@ void dazi_dk_finalize(void)
     DBuf* all[] = {&g_ctx.vel, &g_ctx.vp, &g_ctx.rho, &g_ctx.per, &g_ctx.depz, &g_ctx.pv,
                    &g_ctx.svs, &g_ctx.svp, &g_ctx.srh, &g_ctx.status, &g_ctx.geo,
                    &g_ctx.cscratch, &g_ctx.w.croot, &g_ctx.w.crootb, &g_ctx.w.counters, &g_ctx.w.adjscr,
-                   &g_ctx.w.tiscr, &g_ctx.lsen, &g_ctx.w.keys, &g_ctx.w.keys2, &g_ctx.w.cidx, &g_ctx.w.cidx2,
+                   &g_ctx.w.tiscr, &g_ctx.w.tiord, &g_ctx.lsen, &g_ctx.w.keys, &g_ctx.w.keys2, &g_ctx.w.cidx, &g_ctx.w.cidx2,
                    &g_ctx.w.rmaxb, &g_ctx.w.trecs, &g_ctx.w.ttasks, &g_ctx.w.tlbase, &g_ctx.w.ttbase,
                    &g_ctx.w.cubtmp, &g_ctx.w.tflat, &g_ctx.w.tld, &g_ctx.w.tti, &g_ctx.w.tsp, &g_ctx.w.tch, &g_ctx.w.tmeta,
                    &g_ctx.w.ttasklist, &g_ctx.cbufoff, &g_ctx.bnode, &g_ctx.bper, &g_ctx.bdep,

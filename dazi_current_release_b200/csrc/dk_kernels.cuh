@@ -71,6 +71,8 @@ struct TiArgs {
     long long scr_layers;   // layer capacity of a warp's scratch block
     unsigned* queue;        // work-queue counter (zeroed before the launch)
     int* errflag;           // set to 1 when an Lsen_Gsc value is not finite
+    int* order;             // [task * 32 + lane]: (key << 16) | (period * 32 + column lane),
+                            // written by ti_order_kernel (key: ti_pair_key)
 };
 
 // G-row epilogue (k_grows.cu): kernels of the grid interface to sparse
@@ -170,6 +172,10 @@ template <int MINB> __global__ void adjoint_love_kernel(AdjArgs a);   // MINB = 
 template <int MINB> __global__ void adjoint_group_kernel(AdjArgs a);        // MINB = 3
 template <int MINB> __global__ void adjoint_love_group_kernel(AdjArgs a);   // MINB = 3
 template <int MINB> __global__ void ti_kernel(TiArgs a);          // MINB in {2, 3, 4, 6, 8}
+// One block per tile: the order of the tile's (column, period) pairs for
+// ti_kernel's tasks (a.order), by the depth at which each pair's sweep stops.
+__global__ void ti_order_kernel(TiArgs a, const long long* tile_tbase, const long long* tile_tasks);
+constexpr int TI_ORDER_THREADS = 256;
 
 __global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);
 // Models one column of the finite-difference kernel solves: the base model

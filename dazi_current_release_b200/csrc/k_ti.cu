@@ -32,6 +32,14 @@ namespace dk {
 // Divisions and square roots use dk_fastmath.cuh (the sweep is held to 1e-5
 // of the oracle, not to bit parity).
 
+// Depth cut of the Gc/Gs sweep: the accumulated vertical decay exponent
+// (sum of nu d from the surface) at which a layer is taken as the
+// half-space.  Against the full sweep, on 400 columns of the uneven
+// workload (host build): per-column rel-L2 of Lsen_Gsc 5e-11 at 16
+// (2.6e-19 at 25, 3.9e-8 at 12), i.e. far below the real*4 output's
+// resolution, while 18 % of the layer items are left out.
+constexpr double kTiDepthCut = 16.0;
+
 // ------------------------------------------------------------ complex
 struct zc { double re, im; };
 __device__ __forceinline__ zc Z(double r, double i = 0.0) { return {r, i}; }
@@ -842,51 +850,101 @@ __device__ __forceinline__ long long ti_next_task(unsigned* queue)
     return (long long)__shfl_sync(0xffffffffu, t, 0);
 }
 
-// One (column, period) of the Gc/Gs kernel: lane `lane` of task `task`,
-// with the thread's scratch block at scr (layer m, entry q at
-// scr[(m * TI_SCR_Q + q) * TILE]).
-__device__ __forceinline__ void ti_task(const TiArgs& a, long long task, int lane, double* scr)
+// Number of layers the sweep of one (column, period) covers, the last taken
+// as the half-space (the depth cut, kTiDepthCut): where the waves have
+// decayed by exp(-E) with E = sum of nu d over the layers above and
+// E >= kTiDepthCut, that layer is taken as the half-space and the ones
+// below are not swept.  The compound vectors above it and the
+// eigenfunction energy at and below it are exponentially small in E
+// against the surface's, so the partials above move by far less than a
+// real*4 ulp and the ones below the cut (of that size) are left out of the
+// splice (written as zero).  nu is the isotropic vertical S wavenumber
+// sqrt(k^2 - omega^2 rho / L) of the flattened layer (the smaller of the
+// two; the TI ones differ by well under 1 %).  Only short periods over
+// deep stacks are cut, which is where the complex-eigenvalue layers lie.
+__device__ __forceinline__ int ti_cut_layers(const TiRec* tir, int rmax, double omega, double wvno2)
+{
+    double ex = 0.0;
+    for (int m = 0; m < rmax - 1; ++m) {
+        if (ex >= kTiDepthCut) return m + 1;
+        const TiRec r = tir[(long long)m * TILE];
+        const double nb2 = wvno2 - omega * omega * r.rho / r.TL;
+        if (nb2 > 0.0) ex += sqrt(nb2) * r.td;
+    }
+    return rmax;
+}
+
+// tregn96.f:430-479: twopi real*4, t and cp real*4
+__device__ __forceinline__ double ti_omega(const TiArgs& a, const ColMeta& M, int k)
+{
+    const float twopi = 6.2831855f;
+    return (double)twopi / (double)(float)a.periods[M.per_b + k];
+}
+
+// Sort key of the pair (column lane `lane` of tile t, period k): 0 no such
+// pair, 1 no root (the period's Lsen_Gsc row is written as zero), else
+// 1 + the layers its sweep covers (ti_cut_layers, at most NL).
+__device__ __forceinline__ int ti_pair_key(const TiArgs& a, long long t, int lane, int k)
+{
+    const Tables& T = a.T;
+    const long long s = t * TILE + lane;
+    if (s >= T.ncols) return 0;
+    const ColMeta M = T.meta[s];
+    if (k >= M.K) return 0;
+    const float cpf = (float)a.pv[M.pv_b + T.pv_sk * k];
+    if (!(cpf > 0.0f)) return 1;
+    const double omega = ti_omega(a, M, k);
+    const double wvno = omega / (double)cpf;
+    return 1 + ti_cut_layers(T.ti + T.tile_lbase[t] + lane, M.rmax, omega, wvno * wvno);
+}
+
+// One (column, period) of the Gc/Gs kernel: the pair at a.order[task * 32
+// + tl] of task `task`, run by lane tl with the thread's scratch block at
+// scr (layer m, entry q at scr[(m * TI_SCR_Q + q) * TILE]).
+__device__ __forceinline__ void ti_task(const TiArgs& a, long long task, int tl, double* scr)
 {
     const Tables& T = a.T;
     constexpr long long nslots = TILE;
     {
+        const int e = a.order[task * TILE + tl];
+        const int key = e >> 16;
+        if (key == 0) return;
+        const int lane = e & 31, k = (e >> 5) & 0x7ff;
         const int2 tk = T.tasks[task];
         const long long s = (long long)tk.x * TILE + lane;
-        const int k = tk.y;
-        if (s >= T.ncols) return;
         const ColMeta M = T.meta[s];
-        if (k >= M.K) return;
         const int rmax = M.rmax, nz = M.nz;
         float* lout = a.lsen + M.ls_b + T.ls_sk * k;
         const long long jstride = M.ls_is;
-        const float cpf = (float)a.pv[M.pv_b + T.pv_sk * k];
-        if (!(cpf > 0.0f)) {
+        if (key == 1) {
             for (int j = 0; j < nz - 1; ++j) lout[jstride * j] = 0.0f;
             return;
         }
+        const int rm = key - 1;
+        const float cpf = (float)a.pv[M.pv_b + T.pv_sk * k];
         const long long lbase = T.tile_lbase[tk.x] + lane;
         const TiRec* tir = T.ti + lbase;              // layer m at tir[m * TILE]
         const ChainRec* chr = T.ch + lbase;
-        // tregn96.f:430-479: twopi real*4, t and cp real*4
-        const float twopi = 6.2831855f;
-        const double omega = (double)twopi / (double)(float)a.periods[M.per_b + k];
+        const double omega = ti_omega(a, M, k);
         const double wvno = omega / (double)cpf;
         const double wvno2 = wvno * wvno;
         const double iwvno = 1.0 / wvno, iwvno2 = 1.0 / wvno2;
         // ---- up() (compound vectors from the half-space upward), then
         // down() + svfunc() + energy() (interface by interface), as one loop
-        // of 2 rmax - 1 steps: steps 0 .. rmax-2 are up-sweep layers
-        // rmax-2 .. 0, the rest down-sweep layers 0 .. rmax-1.  A layer's
+        // of 2 rm - 1 steps (rm: the layers ti_cut_layers gives, the last
+        // as the half-space): steps 0 .. rm-2 are up-sweep layers
+        // rm-2 .. 0, the rest down-sweep layers 0 .. rm-1.  A layer's
         // eigen-solution and waves are formed at the top of the step by the
         // one copy of that code, in both sweeps, so the down-sweep forms
         // them again instead of reading them back: the per-layer scratch is
         // the compound vector and its exponent sum only.
+
         constexpr int Q = TI_SCR_Q;
         double cdv[5];
         double exsum = 0.0;
         {
-            const D5 c = ti_halfspace_cdv(ti_layer(tir + (long long)(rmax - 1) * TILE), omega, wvno, wvno2);
-            double* sp = scr + (long long)(rmax - 1) * Q * nslots;
+            const D5 c = ti_halfspace_cdv(ti_layer(tir + (long long)(rm - 1) * TILE), omega, wvno, wvno2);
+            double* sp = scr + (long long)(rm - 1) * Q * nslots;
 #pragma unroll
             for (int q = 0; q < 5; ++q) { cdv[q] = c.v[q]; sp[q * nslots] = cdv[q]; }
             sp[5 * nslots] = 0.0;
@@ -897,11 +955,11 @@ __device__ __forceinline__ void ti_task(const TiArgs& a, long long task, int lan
         double sumi0 = 0.0, sumi1 = 0.0, sumi2 = 0.0, gsum = 0.0;
         const double pi_ = 3.141592653589493;   // gammap's constant, as in the reference
         const double lw = log(omega / (2.0 * pi_ * 1.0)) / pi_;
-        const int nsteps = 2 * rmax - 1;
+        const int nsteps = 2 * rm - 1;
         for (int step = 0; step < nsteps; ++step) {
-            const bool up = step < rmax - 1;
-            const int m = up ? rmax - 2 - step : step - (rmax - 1);
-            const bool half = (m == rmax - 1);
+            const bool up = step < rm - 1;
+            const int m = up ? rm - 2 - step : step - (rm - 1);
+            const bool half = (m == rm - 1);
             const TiLayer L = ti_layer(tir + (long long)m * TILE);
             TiEig E;
             TiWave P, S;
@@ -1036,10 +1094,13 @@ __device__ __forceinline__ void ti_task(const TiArgs& a, long long task, int lan
         const double tm3 = tm * tm * tm;
         const double iun = 1.0 / un, iuntm3 = iun / tm3;
         const SpRec* spr = T.sp + lbase;
+        // the half-space (rmax - 1) and the layers below the depth cut add
+        // nothing; their records are not read
+        const int mlim = rm < rmax - 1 ? rm : rmax - 1;
         int m = 0;
         for (int j = 0; j < nz - 1; ++j) {
             float acc = 0.0f;
-            for (; m < rmax - 1 && chr[(long long)m * TILE].node == j; ++m) {
+            for (; m < mlim && chr[(long long)m * TILE].node == j; ++m) {
                 const SpRec R = spr[(long long)m * TILE];
                 const double* so = scr + (long long)m * Q * nslots;
                 const double vt = (double)R.vtp;
@@ -1074,6 +1135,44 @@ ti_kernel(TiArgs a)
         const long long task = ti_next_task(a.queue);
         if (task >= a.T.ntasks) break;
         ti_task(a, task, lane, scr);
+    }
+}
+
+// One block per tile: every (column, period) pair's key (ti_pair_key), then
+// a counting sort of the tile's pairs by key into a.order, so that the 32
+// lanes of a task sweep to nearly the same depth.  With lanes bound to the
+// tile's columns, the lanes of a task at a short period would stop at
+// depths differing by up to the whole stack, and the task would take the
+// deepest.  The results do not depend on the order: each pair is computed
+// by one lane alone, the same arithmetic on whichever lane.
+__global__ void __launch_bounds__(TI_ORDER_THREADS)
+ti_order_kernel(TiArgs a, const long long* tile_tbase, const long long* tile_tasks)
+{
+    __shared__ unsigned short key[NP * TILE];
+    __shared__ int hist[NL + 2];
+    const long long t = blockIdx.x;
+    const int np = (int)tile_tasks[t] * TILE;     // tile_tasks <= NP (checked by the table build)
+    for (int i = threadIdx.x; i < NL + 2; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        const int kk = ti_pair_key(a, t, p & 31, p >> 5);
+        key[p] = (unsigned short)kk;
+        atomicAdd(&hist[kk], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int i = 0; i < NL + 2; ++i) {
+            const int h = hist[i];
+            hist[i] = run;
+            run += h;
+        }
+    }
+    __syncthreads();
+    int* out = a.order + tile_tbase[t] * TILE;
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        const int kk = key[p];
+        out[atomicAdd(&hist[kk], 1)] = (kk << 16) | p;
     }
 }
 

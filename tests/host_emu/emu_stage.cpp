@@ -8,6 +8,7 @@
 // tests/test_host_emu_*.py suites to check the device arithmetic against
 // the oracle on the CPU; the shipped library never uses it.
 #include "emu_shim.h"
+#include <algorithm>
 #include <numeric>
 #include <vector>
 namespace dk { alignas(16) unsigned char smem_raw[1 << 16]; }
@@ -21,7 +22,7 @@ namespace {
 
 struct HostTables {
     std::vector<int> sorted;
-    std::vector<long long> lbase, tbase;
+    std::vector<long long> lbase, tbase, ttask;
     std::vector<int2> tasks;
     std::vector<float4> flat;
     std::vector<LayerD> ld;
@@ -47,7 +48,9 @@ bool build_host(const ColSrc& src, long long ncols, const PrepOut& po, HostTable
     std::stable_sort(H.sorted.begin(), H.sorted.end(), [&](int a, int b) { return keys[a] > keys[b]; });
     const long long ntiles = (ncols + TILE - 1) / TILE;
     H.lbase.resize(ntiles); H.tbase.resize(ntiles);
-    std::vector<long long> trec(ntiles), ttask(ntiles);
+    std::vector<long long> trec(ntiles);
+    std::vector<long long>& ttask = H.ttask;
+    ttask.resize(ntiles);
     for (long long t = 0; t < ntiles; ++t) {
         int rm = 0, km = 0;
         for (int l = 0; l < TILE && t * TILE + l < ncols; ++l) {
@@ -142,6 +145,18 @@ extern "C" int emu_ti_batch(long long ncols, const long long* node_off, const fl
     TiArgs a;
     a.T = H.T; a.periods = periods; a.pv = pv; a.lsen = lsen; a.scratch = scratch.data();
     a.scr_layers = H.maxr; a.queue = &queue; a.errflag = &errflag;
+    // ti_order_kernel: per tile, the pairs in ascending key order (a
+    // stable sort here; the device's counting sort may order equal keys
+    // differently, which changes no result)
+    std::vector<int> order((size_t)H.T.ntasks * TILE);
+    a.order = order.data();
+    for (long long t = 0; t < (long long)H.ttask.size(); ++t) {
+        const int np = (int)H.ttask[t] * TILE;
+        std::vector<int> pk(np);
+        for (int p = 0; p < np; ++p) pk[p] = (ti_pair_key(a, t, p & 31, p >> 5) << 16) | p;
+        std::stable_sort(pk.begin(), pk.end(), [](int x, int y) { return (x >> 16) < (y >> 16); });
+        std::copy(pk.begin(), pk.end(), order.begin() + H.tbase[t] * TILE);
+    }
     for (long long task = 0; task < H.T.ntasks; ++task)
         for (int lane = 0; lane < TILE; ++lane) ti_task(a, task, lane, scratch.data() + lane);
     return errflag ? -2 : 0;
