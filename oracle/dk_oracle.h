@@ -90,6 +90,23 @@ long or_grows(int nvx, int nvz, int nz, int K, const float *vels, const double *
               float *rw, int *iw, int *col, long *nnz_ray);
 void or_azimap(int nx, int ny, int nz, int K, const float *lsen, const float *gc, const float *gs,
                const double *ciso, float *cosr, float *sinr, float *amp, float *rela, float *ang);
+/* First-arrival traveltimes (fmm_oracle.c).  The model grid is nx x ny
+ * (x = latitude from goxd, z = longitude from gozd, degrees, spacing
+ * dvxd x dvzd); the propagation grid is (nx-3)*gdx+1 x (ny-3)*gdz+1 nodes. */
+typedef struct {
+    int nx, ny;             /* phase-velocity map (model grid) */
+    float goxd, gozd, dvxd, dvzd;
+    int gdx, gdz;           /* grid dicing (5, 5) */
+    int asgr, sgdl, sgs;    /* source-grid refinement (1, 8, 8) */
+    int fom;                /* 0 first order, 1 mixed order (1) */
+    float snb;              /* narrow-band capacity fraction (0.5) */
+    float earth;            /* 6371 */
+} OrFmmParams;
+int or_fmm_batch(const OrFmmParams *P, const double *pv, int ninst, const int *inst_period,
+                 const float *scx, const float *scz, const long *rc_off, const float *rcx,
+                 const float *rcz, float *times, float *ttn_out, int nthreads);
+int or_fmm_travel(int nnx, int nnz, float gox, float goz, float dnx, float dnz, float earth, int fom,
+                  float snb, const float *veln, float scx, float scz, float *ttn, int *nsts_out);
 #ifdef __cplusplus
 }
 #endif

@@ -34,6 +34,21 @@ def build() -> str:
     return _LIB_PATH
 
 
+class FmmParams(ctypes.Structure):
+    """OrFmmParams (dk_oracle.h): the model grid and the traveltime solver's
+    settings, defaults as CalSurfG_parallel.f90:1900-1911 sets them."""
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("goxd", ctypes.c_float),
+                ("gozd", ctypes.c_float), ("dvxd", ctypes.c_float), ("dvzd", ctypes.c_float),
+                ("gdx", ctypes.c_int), ("gdz", ctypes.c_int), ("asgr", ctypes.c_int),
+                ("sgdl", ctypes.c_int), ("sgs", ctypes.c_int), ("fom", ctypes.c_int),
+                ("snb", ctypes.c_float), ("earth", ctypes.c_float)]
+
+
+def fmm_params(nx, ny, goxd, gozd, dvxd, dvzd, gdx=5, gdz=5, asgr=1, sgdl=8, sgs=8, fom=1,
+               snb=0.5, earth=6371.0):
+    return FmmParams(nx, ny, goxd, gozd, dvxd, dvzd, gdx, gdz, asgr, sgdl, sgs, fom, snb, earth)
+
+
 def lib():
     global _lib
     if _lib is None:
@@ -107,6 +122,12 @@ def lib():
         L.or_grows.restype = ctypes.c_long
         L.or_azimap.argtypes = [ctypes.c_int] * 4 + [_f32p] * 3 + [_f64p] + [_f32p] * 5
         L.or_azimap.restype = None
+        L.or_fmm_batch.argtypes = [ctypes.POINTER(FmmParams), _f64p, ctypes.c_int, _i32p, _f32p,
+                                   _f32p, _i64p, _f32p, _f32p, _f32p, _f32p, ctypes.c_int]
+        L.or_fmm_batch.restype = ctypes.c_int
+        L.or_fmm_travel.argtypes = [ctypes.c_int, ctypes.c_int] + [ctypes.c_float] * 5 + \
+            [ctypes.c_int, ctypes.c_float, _f32p, ctypes.c_float, ctypes.c_float, _f32p, _i32p]
+        L.or_fmm_travel.restype = ctypes.c_int
         _lib = L
     return _lib
 
@@ -458,3 +479,44 @@ def azimap(lsen, gc, gs, ciso):
                     _p(np.asfortranarray(gs, np.float32), _f32p),
                     _p(np.asfortranarray(ciso, np.float64), _f64p), *[_p(o, _f32p) for o in out])
     return tuple(out)
+
+
+def fmm_batch(params, pv, inst_period, scx, scz, rc_off, rcx, rcz, nthreads=0, fields=False):
+    """Forward traveltimes of a data set (or_fmm_batch, fmm_oracle.c):
+    pv (nx*ny, K) phase-velocity maps (x index fastest, float64), one
+    instance per (period index, source) with its receivers in CSR rc_off;
+    coordinates are colatitude and longitude in radians (float32), as
+    Main_Jt.f90:412-431 converts them.  Returns the receiver times (float32)
+    and, when fields, the coarse traveltime fields (ninst, nnx, nnz)."""
+    P = params
+    pv = np.asfortranarray(pv, np.float64)
+    ninst = len(inst_period)
+    rc_off = np.ascontiguousarray(rc_off, np.int64)
+    times = np.zeros(max(int(rc_off[-1]), 1), np.float32)
+    nnx, nnz = (P.nx - 3) * P.gdx + 1, (P.ny - 3) * P.gdz + 1
+    ttn = np.zeros((ninst, nnx, nnz), np.float32) if fields else None
+    nthreads = nthreads or (os.cpu_count() or 1)
+    r = lib().or_fmm_batch(ctypes.byref(P), _p(pv, _f64p), ninst,
+                           _p(np.ascontiguousarray(inst_period, np.int32), _i32p),
+                           _p(np.ascontiguousarray(scx, np.float32), _f32p),
+                           _p(np.ascontiguousarray(scz, np.float32), _f32p), _p(rc_off, _i64p),
+                           _p(np.ascontiguousarray(rcx, np.float32), _f32p),
+                           _p(np.ascontiguousarray(rcz, np.float32), _f32p), _p(times, _f32p),
+                           None if ttn is None else _p(ttn, _f32p), nthreads)
+    if r:
+        raise RuntimeError(f"oracle fmm_batch: error {r}")
+    return (times[:int(rc_off[-1])], ttn) if fields else times[:int(rc_off[-1])]
+
+
+def fmm_travel(veln, gox, goz, dnx, dnz, scx, scz, earth=6371.0, fom=1, snb=0.5):
+    """One traveltime field on a given grid (travel with urg = 0): veln
+    (nnx, nnz) float32 (x outer); returns ttn (nnx, nnz) and the status."""
+    veln = np.ascontiguousarray(veln, np.float32)
+    nnx, nnz = veln.shape
+    ttn = np.zeros_like(veln)
+    st = np.zeros(veln.shape, np.int32)
+    r = lib().or_fmm_travel(nnx, nnz, gox, goz, dnx, dnz, earth, fom, snb, _p(veln, _f32p), scx,
+                            scz, _p(ttn, _f32p), _p(st, _i32p))
+    if r:
+        raise RuntimeError(f"oracle fmm_travel: error {r}")
+    return ttn, st
