@@ -39,8 +39,19 @@ EXPORTS = (
     "dazi_dk_iso_noalloc_dev", "dazi_dk_batch", "dazi_dk_batch_dev", "dazi_dk_set_timing",
     "dazi_dk_last_timing", "dazi_dk_last_items", "dazi_dk_plan_create", "dazi_dk_plan_launch",
     "dazi_dk_plan_status", "dazi_dk_plan_config", "dazi_dk_plan_destroy", "dazi_dk_grows_dev",
-    "dazi_dk_azimuthal_map_dev", "dazi_lsmr", "dazi_lsmr_dev",
+    "dazi_dk_azimuthal_map_dev", "dazi_lsmr", "dazi_lsmr_dev", "dazi_fmm_default_params",
+    "dazi_fmm_batch", "dazi_fmm_batch_dev", "dazi_fmm_times",
 )
+
+
+class FmmParams(ctypes.Structure):
+    """dazi_fmm_params (include/dazi_dk.h): model grid and traveltime-solver
+    settings."""
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("goxd", ctypes.c_float),
+                ("gozd", ctypes.c_float), ("dvxd", ctypes.c_float), ("dvzd", ctypes.c_float),
+                ("gdx", ctypes.c_int), ("gdz", ctypes.c_int), ("asgr", ctypes.c_int),
+                ("sgdl", ctypes.c_int), ("sgs", ctypes.c_int), ("fom", ctypes.c_int),
+                ("snb", ctypes.c_float), ("earth", ctypes.c_float)]
 
 
 class DaziError(RuntimeError):
@@ -142,6 +153,15 @@ def load(build_if_missing: bool = True):
     L.dazi_dk_fp64_peak.restype = _int
     L.dazi_dk_finalize.argtypes = []
     L.dazi_dk_finalize.restype = None
+    fpp = ctypes.POINTER(FmmParams)
+    L.dazi_fmm_default_params.argtypes = [fpp, _int, _int] + [ctypes.c_float] * 4
+    L.dazi_fmm_default_params.restype = None
+    L.dazi_fmm_batch.argtypes = [fpp, _f64p, _int, _int, ip, fp, fp, ll_p, fp, fp, fp, fp]
+    L.dazi_fmm_batch.restype = _int
+    L.dazi_fmm_batch_dev.argtypes = [fpp, vp_, _int, _int] + [vp_] * 8 + [vp_]
+    L.dazi_fmm_batch_dev.restype = _int
+    L.dazi_fmm_times.argtypes = [ip] * 6 + [_f64p, ip, ip, ip, fp, fp, fp, fp, fp, fp, fp, fp, ll_p, fp]
+    L.dazi_fmm_times.restype = _int
     _lib = L
     return L
 

@@ -12,7 +12,10 @@ PKG = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(PKG, "csrc")
 OUT_DIR = os.path.join(PKG, "_lib")
 LIB = os.path.join(OUT_DIR, "libdazi_dk.so")
-SOURCES = ["capi.cu", "k_plain.cu", "k_adjoint.cu", "k_ti.cu", "k_prep.cu", "k_probe.cu", "k_noalloc.cu", "k_epilogue.cu", "k_lsmr.cu"]
+SOURCES = ["capi.cu", "k_plain.cu", "k_adjoint.cu", "k_ti.cu", "k_prep.cu", "k_probe.cu", "k_noalloc.cu", "k_epilogue.cu", "k_lsmr.cu",
+           "k_fmm.cu"]
+# per-file flags: the traveltime solver rounds every operation on its own
+FILE_FLAGS = {"k_fmm.cu": ["-fmad=false"]}
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -39,7 +42,7 @@ def build(verbose: bool = False, force: bool = False) -> str:
     objs = []
     for src in SOURCES:
         obj = os.path.join(OUT_DIR, src.replace(".cu", ".o"))
-        cmd = [NVCC, *FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+        cmd = [NVCC, *FLAGS, *FILE_FLAGS.get(src, []), "-c", os.path.join(CSRC, src), "-o", obj]
         if verbose:
             cmd += ["-Xptxas", "-v"]
             print(" ".join(cmd), flush=True)

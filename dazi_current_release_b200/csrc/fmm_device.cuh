@@ -1,0 +1,760 @@
+// First-arrival traveltimes on the refined spherical grid for many
+// (period, source) instances at once: the reference's fast-marching solver
+// (code/src_inv_iso_joint/CalSurfG_parallel.f90:125-336, travel_parallel,
+// with fouds1/fouds2 :346-622 and the binary-heap narrow band :631-803),
+// its source-grid refinement (:2148-2325, bsplrefine_parallel :918-989),
+// the B-spline gridding of a phase-velocity map (gridder_parallel
+// :811-909) and the receiver interpolation (srtimes_parallel :997-1125).
+//
+// Fast marching pops the narrow band's minimum one node at a time, and the
+// value a node keeps depends on which neighbours were alive when it was
+// last updated, ties included; a parallel front (several nodes accepted at
+// once) changes those sets and so the times.  So each instance runs the
+// reference's sequence exactly, on one warp: lane 0 marches (heap, upwind
+// updates), the 32 lanes share the data-parallel steps (the refined grid's
+// B-spline values, status resets, the transfer from the refined to the
+// coarse grid, the receivers).  The instances (up to several thousand per
+// data set) fill the GPU: a persistent grid of warps takes them from a
+// queue, each with its own slice of the workspace.  The marching is a chain
+// of dependent loads, so its speed is set by memory latency, not by
+// bandwidth or FP32 throughput.
+//
+// Arithmetic: every value is real*4 as in the reference, every operation
+// rounds on its own in the Fortran's order (k_fmm.cu, which includes this
+// file, is compiled with -fmad=false; the one fused multiply-add, the refined grid's origin, is
+// formed on the host as the reference's example build forms it), division
+// and sqrtf are IEEE, and the ri*sin(colatitude) factors are tables the
+// host fills with the C library's sinf.  The results equal the CPU
+// restatement bit for bit.
+#pragma once
+#include <cuda_runtime.h>
+#include <cmath>
+#include <vector>
+
+#include "../../include/dazi_dk.h"
+
+namespace dk {
+namespace fmm {
+
+constexpr int kWarpsPerBlock = 4;
+
+// heap entry: the node's current time (kept equal to ttn at the node while
+// it is in the band) and its grid position
+struct HeapE {
+    float key;
+    short px, pz;
+};
+
+// One propagation grid of one instance: node (iz, ix), 1-based, at
+// a[(ix - 1) * nnz + (iz - 1)] as the reference's ttn(nnz, nnx).
+struct FField {
+    int nnx, nnz;
+    float gox, goz, dnx, dnz, earth;
+    int fom;
+    const float* veln;
+    const float* risti;   // [ix - 1]: earth * sin(gox + (ix - 1) * dnx)
+    float* ttn;
+    int* nsts;
+};
+
+#define FAT(a, iz, ix) (a)[(long long)((ix) - 1) * F.nnz + ((iz) - 1)]
+
+// error codes of one instance
+constexpr int kErrOutside = 1;   // source or receiver outside the grid
+constexpr int kErrBand = 2;      // narrow band beyond its capacity
+constexpr int kErrNoSol = 3;     // a node without an upwind solution
+constexpr int kErrSteps = 4;     // more pops than nodes (cannot happen)
+constexpr int kErrNoBand = 5;    // no close node after the refined sweep
+
+// ------------------------------------------------------------ heap
+// addtree_parallel (CalSurfG_parallel.f90:631-675)
+__device__ int heap_add(const FField& F, int iz, int ix, int& ntr, int cap, HeapE* h)
+{
+    if (ntr >= cap) return kErrBand;
+    ntr += 1;
+    const float key = FAT(F.ttn, iz, ix);
+    int tpc = ntr, tpp = tpc / 2;
+    while (tpp > 0 && key < h[tpp].key) {
+        h[tpc] = h[tpp];
+        FAT(F.nsts, h[tpc].pz, h[tpc].px) = tpc;
+        tpc = tpp;
+        tpp = tpc / 2;
+    }
+    h[tpc] = HeapE{key, (short)ix, (short)iz};
+    FAT(F.nsts, iz, ix) = tpc;
+    return 0;
+}
+
+// updtree_parallel (CalSurfG_parallel.f90:770-803): the node's time was
+// just recomputed; it moves up while smaller than its parent
+__device__ void heap_update(const FField& F, int iz, int ix, HeapE* h)
+{
+    const float key = FAT(F.ttn, iz, ix);
+    int tpc = FAT(F.nsts, iz, ix), tpp = tpc / 2;
+    while (tpp > 0 && key < h[tpp].key) {
+        h[tpc] = h[tpp];
+        FAT(F.nsts, h[tpc].pz, h[tpc].px) = tpc;
+        tpc = tpp;
+        tpp = tpc / 2;
+    }
+    h[tpc] = HeapE{key, (short)ix, (short)iz};
+    FAT(F.nsts, iz, ix) = tpc;
+}
+
+// downtree_parallel (CalSurfG_parallel.f90:686-761): the root has been
+// taken; the last entry moves to the root and down while a child is
+// smaller (the smaller child; the right one on ties only if strictly
+// smaller, as rd1 > rd2 selects it)
+__device__ void heap_pop(const FField& F, int& ntr, HeapE* h)
+{
+    if (ntr == 1) { ntr = 0; return; }
+    const HeapE last = h[ntr];
+    ntr -= 1;
+    int tpp = 1, tpc = 2;
+    while (tpc <= ntr) {
+        HeapE c = h[tpc];
+        if (tpc < ntr) {
+            const HeapE c2 = h[tpc + 1];
+            if (c.key > c2.key) { c = c2; tpc += 1; }
+        }
+        if (!(c.key < last.key)) break;
+        h[tpp] = c;
+        FAT(F.nsts, c.pz, c.px) = tpp;
+        tpp = tpc;
+        tpc = 2 * tpp;
+    }
+    h[tpp] = last;
+    FAT(F.nsts, last.pz, last.px) = tpp;
+}
+
+// ------------------------------------------------------------ upwind updates
+__device__ __forceinline__ float quad_root(float a, float b, float c)
+{
+    float rd1 = b * b - 4.0f * a * c;
+    if (rd1 < 0.0f) rd1 = 0.0f;
+    return (-b + sqrtf(rd1)) / (2.0f * a);
+}
+
+// fouds1_parallel (CalSurfG_parallel.f90:346-432): first-order upwind time
+// of node (iz, ix) from its alive neighbours, the minimum over the four
+// quadrants
+__device__ int fouds1(const FField& F, int iz, int ix)
+{
+    int tsw1 = 0;
+    float travm = 0.0f;
+    const float slown = 1.0f / FAT(F.veln, iz, ix);
+    const float ri = F.earth;
+    const float risti = F.risti[ix - 1];
+    for (int j = ix - 1; j <= ix + 1; j += 2) {
+        for (int k = iz - 1; k <= iz + 1; k += 2) {
+            if (j < 1 || j > F.nnx || k < 1 || k > F.nnz) continue;
+            int swsol = 0;
+            float a = 0.0f, b = 0.0f, c = 0.0f, tref = 0.0f;
+            if (FAT(F.nsts, iz, j) == 0) {
+                swsol = 1;
+                if (FAT(F.nsts, k, ix) == 0) {
+                    const float u = ri * F.dnx, v = risti * F.dnz;
+                    const float em = FAT(F.ttn, k, ix) - FAT(F.ttn, iz, j);
+                    a = u * u + v * v;
+                    b = -2.0f * (u * u) * em;
+                    c = (u * u) * (em * em - (v * v) * (slown * slown));
+                } else {
+                    a = 1.0f;
+                    c = -(slown * slown) * (ri * ri) * (F.dnx * F.dnx);
+                }
+                tref = FAT(F.ttn, iz, j);
+            } else if (FAT(F.nsts, k, ix) == 0) {
+                swsol = 1;
+                a = 1.0f;
+                const float t = slown * risti * F.dnz;
+                c = -(t * t);
+                tref = FAT(F.ttn, k, ix);
+            }
+            if (swsol) {
+                const float trav = tref + quad_root(a, b, c);
+                if (tsw1) travm = fminf(trav, travm);
+                else { travm = trav; tsw1 = 1; }
+            }
+        }
+    }
+    if (!tsw1) return kErrNoSol;
+    FAT(F.ttn, iz, ix) = travm;
+    return 0;
+}
+
+// fouds2_parallel (CalSurfG_parallel.f90:443-622): mixed-order upwind
+// (second-order stencils where two alive nodes line up and the time
+// decreases towards the node)
+__device__ int fouds2(const FField& F, int iz, int ix)
+{
+    int tsw1 = 0;
+    float travm = 0.0f;
+    const float slown = 1.0f / FAT(F.veln, iz, ix);
+    const float ri = F.earth;
+    const float risti = F.risti[ix - 1];
+    for (int j = ix - 1; j <= ix + 1; j += 2) {
+        if (j < 1 || j > F.nnx) continue;
+        const int j2 = j == ix - 1 ? j - 1 : j + 1;
+        const bool aj = FAT(F.nsts, iz, j) == 0;
+        bool swj = false;   // second-order operator in x
+        if (aj && j2 >= 1 && j2 <= F.nnx && FAT(F.nsts, iz, j2) == 0)
+            swj = FAT(F.ttn, iz, j) > FAT(F.ttn, iz, j2);
+        for (int k = iz - 1; k <= iz + 1; k += 2) {
+            if (k < 1 || k > F.nnz) continue;
+            const int k2 = k == iz - 1 ? k - 1 : k + 1;
+            const bool ak = FAT(F.nsts, k, ix) == 0;
+            bool swk = false;
+            if (ak && k2 >= 1 && k2 <= F.nnz && FAT(F.nsts, k2, ix) == 0)
+                swk = FAT(F.ttn, k, ix) > FAT(F.ttn, k2, ix);
+            int swsol = 0;
+            float a = 1.0f, b = 0.0f, c = 0.0f, tref = 0.0f, tdiv = 1.0f;
+            if (swj) {
+                swsol = 1;
+                if (swk) {
+                    const float u = 2.0f * ri * F.dnx, v = 2.0f * risti * F.dnz;
+                    float em = 4.0f * FAT(F.ttn, iz, j) - FAT(F.ttn, iz, j2) - 4.0f * FAT(F.ttn, k, ix);
+                    em = em + FAT(F.ttn, k2, ix);
+                    a = v * v + u * u;
+                    b = 2.0f * em * (u * u);
+                    c = (u * u) * (em * em - (slown * slown) * (v * v));
+                    tref = 4.0f * FAT(F.ttn, iz, j) - FAT(F.ttn, iz, j2);
+                    tdiv = 3.0f;
+                } else if (ak) {
+                    const float u = risti * F.dnz, v = 2.0f * ri * F.dnx;
+                    const float em = 3.0f * FAT(F.ttn, k, ix) - 4.0f * FAT(F.ttn, iz, j) + FAT(F.ttn, iz, j2);
+                    a = v * v + 9.0f * (u * u);
+                    b = 6.0f * em * (u * u);
+                    c = (u * u) * (em * em - (slown * slown) * (v * v));
+                    tref = FAT(F.ttn, k, ix);
+                } else {
+                    const float u = 2.0f * ri * F.dnx;
+                    c = -(u * u) * (slown * slown);
+                    tref = 4.0f * FAT(F.ttn, iz, j) - FAT(F.ttn, iz, j2);
+                    tdiv = 3.0f;
+                }
+            } else if (aj) {
+                swsol = 1;
+                if (swk) {
+                    const float u = ri * F.dnx, v = 2.0f * risti * F.dnz;
+                    const float em = 3.0f * FAT(F.ttn, iz, j) - 4.0f * FAT(F.ttn, k, ix) + FAT(F.ttn, k2, ix);
+                    a = v * v + 9.0f * (u * u);
+                    b = 6.0f * em * (u * u);
+                    c = (u * u) * (em * em - (v * v) * (slown * slown));
+                } else if (ak) {
+                    const float u = ri * F.dnx, v = risti * F.dnz;
+                    const float em = FAT(F.ttn, k, ix) - FAT(F.ttn, iz, j);
+                    a = u * u + v * v;
+                    b = -2.0f * (u * u) * em;
+                    c = (u * u) * (em * em - (v * v) * (slown * slown));
+                } else {
+                    c = -(slown * slown) * (ri * ri) * (F.dnx * F.dnx);
+                }
+                tref = FAT(F.ttn, iz, j);
+            } else if (swk) {
+                swsol = 1;
+                const float u = 2.0f * risti * F.dnz;
+                c = -(u * u) * (slown * slown);
+                tref = 4.0f * FAT(F.ttn, k, ix) - FAT(F.ttn, k2, ix);
+                tdiv = 3.0f;
+            } else if (ak) {
+                swsol = 1;
+                c = -(slown * slown) * (risti * risti) * (F.dnz * F.dnz);
+                tref = FAT(F.ttn, k, ix);
+            }
+            if (swsol) {
+                const float trav = (tref + quad_root(a, b, c)) / tdiv;
+                if (tsw1) travm = fminf(trav, travm);
+                else { travm = trav; tsw1 = 1; }
+            }
+        }
+    }
+    if (!tsw1) return kErrNoSol;
+    FAT(F.ttn, iz, ix) = travm;
+    return 0;
+}
+
+// bilinear_parallel (CalSurfG_parallel.f90:2543-2566); nv[i][j] = nv(i+1, j+1)
+__device__ float bilinear(const float nv[2][2], float dsx, float dsz, float dnx, float dnz)
+{
+    float biv = 0.0f;
+    for (int i = 1; i <= 2; ++i)
+        for (int j = 1; j <= 2; ++j) {
+            const float produ = (1.0f - fabsf(((float)(i - 1) * dnx - dsx) / dnx)) *
+                                (1.0f - fabsf(((float)(j - 1) * dnz - dsz) / dnz));
+            biv = biv + nv[i - 1][j - 1] * produ;
+        }
+    return biv;
+}
+
+// ------------------------------------------------------------ travel
+// travel_parallel (CalSurfG_parallel.f90:125-336) on one thread.  urg 0 / 1
+// start from the source point (nsts already -1 everywhere); urg 1 stops
+// when the popped node lies on a side of the refined grid that is not the
+// model's (compared, as in the reference, with this grid's own node counts
+// on the right and bottom sides); urg 2 starts from the close nodes
+// (nsts > 0) of the box vnl..vnr x vnt..vnb, the only place they can be.
+__device__ int travel(const FField& F, int urg, float scx, float scz, int vnl, int vnr, int vnt,
+                      int vnb, HeapE* h, int cap)
+{
+    const int nnx = F.nnx, nnz = F.nnz;
+    int isx = (int)((scx - F.gox) / F.dnx) + 1;
+    int isz = (int)((scz - F.goz) / F.dnz) + 1;
+    if (isx < 1 || isx > nnx || isz < 1 || isz > nnz) return kErrOutside;
+    if (isx == nnx) isx -= 1;
+    if (isz == nnz) isz -= 1;
+    int ntr = 0, r;
+    if (urg == 2) {
+        for (int i = vnl; i <= vnr; ++i)
+            for (int j = vnt; j <= vnb; ++j)
+                if (FAT(F.nsts, j, i) > 0 && (r = heap_add(F, j, i, ntr, cap, h))) return r;
+        // the refined sweep stopped before it reached a coarse node (a
+        // source in the last cell before the right or bottom side, whose
+        // refined sweep always stops there): the reference leaves the
+        // field as its array held it, so this is reported, not computed
+        if (ntr == 0) return kErrNoBand;
+    } else {
+        float vss[2][2];
+        for (int i = 1; i <= 2; ++i)
+            for (int j = 1; j <= 2; ++j) vss[i - 1][j - 1] = FAT(F.veln, isz - 1 + j, isx - 1 + i);
+        const float dsx = (scx - F.gox) - (float)(isx - 1) * F.dnx;
+        const float dsz = (scz - F.goz) - (float)(isz - 1) * F.dnz;
+        const float vsrc = bilinear(vss, dsx, dsz, F.dnx, F.dnz);
+        for (int i = 1; i <= 2; ++i)
+            for (int j = 1; j <= 2; ++j) {
+                const float ex = dsx - (float)(i - 1) * F.dnx, ez = dsz - (float)(j - 1) * F.dnz;
+                const float ds = sqrtf(ex * ex + ez * ez);
+                FAT(F.ttn, isz - 1 + j, isx - 1 + i) = 2.0f * ds / (vss[i - 1][j - 1] + vsrc);
+                if ((r = heap_add(F, isz - 1 + j, isx - 1 + i, ntr, cap, h))) return r;
+            }
+    }
+    const long long maxpops = (long long)nnx * nnz + 4;
+    for (long long pops = 0; ntr > 0; ++pops) {
+        if (pops > maxpops) return kErrSteps;
+        const int ix = h[1].px, iz = h[1].pz;
+        if (urg == 1 && ((ix == 1 && vnl != 1) || (ix == nnx && vnr != nnx) || (iz == 1 && vnt != 1) ||
+                         (iz == nnz && vnb != nnz))) {
+            FAT(F.nsts, iz, ix) = 0;
+            break;
+        }
+        FAT(F.nsts, iz, ix) = 0;
+        heap_pop(F, ntr, h);
+        // the neighbours in x, then in z (CalSurfG_parallel.f90:288-334)
+#pragma unroll 1
+        for (int q = 0; q < 4; ++q) {
+            const int niz = q < 2 ? iz : iz - 1 + 2 * (q - 2);
+            const int nix = q < 2 ? ix - 1 + 2 * q : ix;
+            if (nix < 1 || nix > nnx || niz < 1 || niz > nnz) continue;
+            const int st = FAT(F.nsts, niz, nix);
+            if (st == 0) continue;
+            r = F.fom == 0 ? fouds1(F, niz, nix) : fouds2(F, niz, nix);
+            if (r) return r;
+            if (st < 0) {
+                if ((r = heap_add(F, niz, nix, ntr, cap, h))) return r;
+            } else {
+                heap_update(F, niz, nix, h);
+            }
+        }
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------ gridding
+// cubic B-spline basis at u (gridder_parallel :857-876)
+__device__ __forceinline__ void bspline_basis(float u, float w[4])
+{
+    const float om = 1.0f - u, u2 = u * u, u3 = u2 * u;
+    w[0] = om * om * om / 6.0f;
+    w[1] = (4.0f - 6.0f * u2 + 3.0f * u3) / 6.0f;
+    w[2] = (1.0f + 3.0f * u + 3.0f * u2 - 3.0f * u3) / 6.0f;
+    w[3] = u3 / 6.0f;
+}
+
+// The B-spline value at global node (stz, stx) (1-based) of a grid diced
+// ncz x ncx per vertex cell, as gridder_parallel (ncz = gdz) and
+// bsplrefine_parallel (ncz = gdz * sgdl) form it: cell i, offset l within
+// it (the last cell holds one more node), velv(i, j) at velv[j * (nvz + 2) + i].
+__device__ float bspline_node(const float* velv, int nvx, int nvz, int ncz, int ncx, int stz, int stx)
+{
+    int i = (stz - 1) / ncz + 1, j = (stx - 1) / ncx + 1;
+    if (i > nvz - 1) i = nvz - 1;
+    if (j > nvx - 1) j = nvx - 1;
+    const int l = stz - ncz * (i - 1), m = stx - ncx * (j - 1);
+    float ui[4], vi[4];
+    bspline_basis((float)(m - 1) / (float)ncx, ui);
+    bspline_basis((float)(l - 1) / (float)ncz, vi);
+    const int ld = nvz + 2;
+    float sum = 0.0f;
+    for (int i1 = 1; i1 <= 4; ++i1) {
+        float s = 0.0f;
+        for (int j1 = 1; j1 <= 4; ++j1) s = s + ui[j1 - 1] * velv[(j - 2 + j1) * ld + (i - 2 + i1)];
+        sum = sum + vi[i1 - 1] * s;
+    }
+    return sum;
+}
+
+// velv of every period map (real(pv), gridder_parallel :842-849) and the
+// coarse grid's velocities veln, one thread per value
+__global__ void fmm_velv_kernel(const double* pv, int nx, int ny, int nper, float* velv)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long per = (long long)nx * ny;
+    if (t >= per * nper) return;
+    const long long p = t / per, r = t % per;
+    const int i = (int)(r / nx), j = (int)(r % nx);   // i: z (longitude) vertex, j: x vertex
+    velv[p * per + (long long)j * ny + i] = (float)pv[p * per + (long long)i * nx + j];
+}
+
+__global__ void fmm_gridder_kernel(const float* velv, int nvx, int nvz, int gdx, int gdz, int nper,
+                                   float* veln)
+{
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int nnx = (nvx - 1) * gdx + 1, nnz = (nvz - 1) * gdz + 1;
+    const long long nn = (long long)nnx * nnz;
+    if (t >= nn * nper) return;
+    const long long p = t / nn, r = t % nn;
+    const int stx = (int)(r / nnz) + 1, stz = (int)(r % nnz) + 1;
+    veln[t] = bspline_node(velv + p * (long long)(nvx + 2) * (nvz + 2), nvx, nvz, gdz, gdx, stz, stx);
+}
+
+// ------------------------------------------------------------ instances
+// One (period, source) instance, laid out by the host.
+struct FInst {
+    int period;                 // map (and coarse velocity grid) index
+    float scx, scz;             // source, colatitude / longitude (rad)
+    int vnl, vnr, vnt, vnb;     // refined box in coarse nodes (asgr)
+    int nrnx, nrnz;             // refined grid nodes
+    float gorx, gorz;           // refined grid origin
+    int cap;                    // narrow-band capacity (the reference's maxbt)
+    long long rc_b, rc_e;       // receivers
+    long long risti_r;          // offset of the refined grid's ri*sin table
+};
+
+struct FArgs {
+    int ninst;
+    const FInst* inst;
+    int nnx, nnz, nvx, nvz, gdx, gdz, sgdl, fom, asgr;
+    float gox, goz, dnx, dnz, drnx, drnz, earth, dpl;
+    const float* velv;          // [period][(nvx + 2) * (nvz + 2)]
+    const float* veln;          // [period][nnx * nnz]
+    const float* risti_c;       // [nnx]
+    const float* risti_r;
+    const float* rcx;
+    const float* rcz;
+    const float* sin_rcx;       // [receiver]: sinf(rcx)
+    float* times;
+    float* ttn_out;             // [instance][nnx * nnz] or nullptr
+    // per-warp workspace slots
+    float* w_ttn;
+    int* w_nsts;
+    float* w_vr;
+    float* w_tr;
+    int* w_nr;
+    HeapE* w_heap;
+    long long wc, wr, wh;       // slot sizes: coarse nodes, refined nodes, heap entries
+    unsigned* queue;
+    int* err;                   // first error code (0: none)
+    int* err_inst;              // its instance
+};
+
+__device__ void record_error(const FArgs& a, int code, int s)
+{
+    if (atomicCAS(a.err, 0, code) == 0) *a.err_inst = s;
+}
+
+// srtimes_parallel (CalSurfG_parallel.f90:997-1125) for receiver q of an
+// instance whose coarse field is C (dpl, the smallest node spacing, and
+// sin(rcx) come from the host)
+__device__ int srtimes(const FArgs& a, const FField& F, float scx, float scz, long long q, float& out)
+{
+    const float rcx1 = a.rcx[q], rcz1 = a.rcz[q];
+    int irx = (int)((rcx1 - F.gox) / F.dnx) + 1;
+    int irz = (int)((rcz1 - F.goz) / F.dnz) + 1;
+    if (irx < 1 || irx > F.nnx || irz < 1 || irz > F.nnz) return kErrOutside;
+    if (irx == F.nnx) irx -= 1;
+    if (irz == F.nnz) irz -= 1;
+    const int isx = (int)((scx - F.gox) / F.dnx) + 1;
+    const int isz = (int)((scz - F.goz) / F.dnz) + 1;
+    float t = (scx - rcx1) * F.earth;
+    float sred = t * t;
+    t = (scz - rcz1) * F.earth * a.sin_rcx[q];
+    sred = sred + t * t;
+    sred = sqrtf(sred);
+    const bool sw = sred < a.dpl || (isx == irx && isz == irz);
+    float trr;
+    if (sw) {
+        if (isx < 1 || isx >= F.nnx || isz < 1 || isz >= F.nnz) return kErrOutside;
+        float vss[2][2];
+        for (int k = 1; k <= 2; ++k)
+            for (int l = 1; l <= 2; ++l) vss[k - 1][l - 1] = FAT(F.veln, isz - 1 + l, isx - 1 + k);
+        float drx = (scx - F.gox) - (float)(isx - 1) * F.dnx;
+        float drz = (scz - F.goz) - (float)(isz - 1) * F.dnz;
+        const float vels = bilinear(vss, drx, drz, F.dnx, F.dnz);
+        for (int k = 1; k <= 2; ++k)
+            for (int l = 1; l <= 2; ++l) vss[k - 1][l - 1] = FAT(F.veln, irz - 1 + l, irx - 1 + k);
+        drx = (rcx1 - F.gox) - (float)(irx - 1) * F.dnx;
+        drz = (rcz1 - F.goz) - (float)(irz - 1) * F.dnz;
+        const float velr = bilinear(vss, drx, drz, F.dnx, F.dnz);
+        trr = 2.0f * sred / (vels + velr);
+    } else {
+        const float drx = (rcx1 - F.gox) - (float)(irx - 1) * F.dnx;
+        const float drz = (rcz1 - F.goz) - (float)(irz - 1) * F.dnz;
+        trr = 0.0f;
+        for (int k = 1; k <= 2; ++k)
+            for (int l = 1; l <= 2; ++l) {
+                const float produ = (1.0f - fabsf(((float)(l - 1) * F.dnz - drz) / F.dnz)) *
+                                    (1.0f - fabsf(((float)(k - 1) * F.dnx - drx) / F.dnx));
+                trr = trr + FAT(F.ttn, irz - 1 + l, irx - 1 + k) * produ;
+            }
+    }
+    out = trr;
+    return 0;
+}
+
+// The fields of instance s in workspace slot `slot`: C the coarse grid, R
+// the refined source grid.
+__device__ void inst_fields(const FArgs& a, const FInst& I, long long slot, FField& C, FField& R)
+{
+    C.nnx = a.nnx; C.nnz = a.nnz;
+    C.gox = a.gox; C.goz = a.goz; C.dnx = a.dnx; C.dnz = a.dnz; C.earth = a.earth; C.fom = a.fom;
+    C.veln = a.veln + (long long)I.period * a.nnx * a.nnz;
+    C.risti = a.risti_c;
+    C.ttn = a.w_ttn + slot * a.wc;
+    C.nsts = a.w_nsts + slot * a.wc;
+    R.nnx = I.nrnx; R.nnz = I.nrnz;
+    R.gox = I.gorx; R.goz = I.gorz; R.dnx = a.drnx; R.dnz = a.drnz; R.earth = a.earth; R.fom = a.fom;
+    R.risti = a.risti_r + I.risti_r;
+    R.veln = a.w_vr + slot * a.wr;
+    R.ttn = a.w_tr + slot * a.wr;
+    R.nsts = a.w_nr + slot * a.wr;
+}
+
+// The steps of one instance that the lanes share: lane `lane` of `nl`.
+// The refined grid's velocities (bsplrefine_parallel), every status -1.
+__device__ void step_init(const FArgs& a, const FInst& I, const FField& C, const FField& R, int lane, int nl)
+{
+    const long long nc = (long long)a.nnx * a.nnz;
+    if (a.asgr) {
+        const long long nr = (long long)I.nrnx * I.nrnz;
+        const int origx = (I.vnl - 1) * a.sgdl + 1, origz = (I.vnt - 1) * a.sgdl + 1;
+        const float* velv = a.velv + (long long)I.period * (a.nvx + 2) * (a.nvz + 2);
+        float* vr = const_cast<float*>(R.veln);
+        for (long long q = lane; q < nr; q += nl) {
+            const int idm2 = (int)(q / I.nrnz) + 1, idm1 = (int)(q % I.nrnz) + 1;
+            vr[q] = bspline_node(velv, a.nvx, a.nvz, a.gdz * a.sgdl, a.gdx * a.sgdl, origz + idm1 - 1,
+                                 origx + idm2 - 1);
+            R.nsts[q] = -1;
+        }
+    }
+    for (long long q = lane; q < nc; q += nl) C.nsts[q] = -1;
+}
+
+// Refined nodes on coarse nodes carry status and time over
+// (CalSurfG_parallel.f90:2245-2262).
+__device__ void step_map(const FArgs& a, const FInst& I, const FField& C, const FField& R, int lane, int nl)
+{
+    const int bz = I.vnb - I.vnt + 1, nbox = (I.vnr - I.vnl + 1) * bz;
+    for (int q = lane; q < nbox; q += nl) {
+        const int idm2 = I.vnl + q / bz, idm1 = I.vnt + q % bz;
+        const int l = (idm2 - I.vnl) * a.sgdl + 1, k = (idm1 - I.vnt) * a.sgdl + 1;
+        const long long rq = (long long)(l - 1) * I.nrnz + (k - 1);
+        const int st = R.nsts[rq];
+        C.nsts[(long long)(idm2 - 1) * a.nnz + (idm1 - 1)] = st;
+        if (st >= 0) C.ttn[(long long)(idm2 - 1) * a.nnz + (idm1 - 1)] = R.ttn[rq];
+    }
+}
+
+// Alive nodes next to far ones become close (:2290-2309), decided for 32
+// box nodes per lane (chunk `base`) before any is written.
+__device__ unsigned step_band_decide(const FArgs& a, const FInst& I, const FField& F, int base, int lane, int nl)
+{
+    const int bz = I.vnb - I.vnt + 1, nbox = (I.vnr - I.vnl + 1) * bz;
+    unsigned mask = 0;
+    for (int t = 0; t < 32; ++t) {
+        const int q = base + t * nl + lane;
+        if (q >= nbox) break;
+        const int ix = I.vnl + q / bz, iz = I.vnt + q % bz;
+        if (FAT(F.nsts, iz, ix) != 0) continue;
+        if ((iz > 1 && FAT(F.nsts, iz - 1, ix) == -1) || (iz < F.nnz && FAT(F.nsts, iz + 1, ix) == -1) ||
+            (ix > 1 && FAT(F.nsts, iz, ix - 1) == -1) || (ix < F.nnx && FAT(F.nsts, iz, ix + 1) == -1))
+            mask |= 1u << t;
+    }
+    return mask;
+}
+
+__device__ void step_band_write(const FArgs& a, const FInst& I, const FField& F, int base, int lane, int nl,
+                                unsigned mask)
+{
+    const int bz = I.vnb - I.vnt + 1;
+    for (int t = 0; t < 32; ++t)
+        if (mask >> t & 1u) {
+            const int q = base + t * nl + lane;
+            FAT(F.nsts, I.vnt + q % bz, I.vnl + q / bz) = 1;
+        }
+}
+
+__device__ int box_nodes(const FInst& I) { return (I.vnr - I.vnl + 1) * (I.vnb - I.vnt + 1); }
+
+// The receivers and the optional copy of the field.
+__device__ void step_receivers(const FArgs& a, const FInst& I, const FField& C, int s, int lane, int nl)
+{
+    for (long long q = I.rc_b + lane; q < I.rc_e; q += nl) {
+        float t = 0.0f;
+        const int e = srtimes(a, C, I.scx, I.scz, q, t);
+        if (e) record_error(a, e, s);
+        else a.times[q] = t;
+    }
+    if (a.ttn_out) {
+        const long long nc = (long long)a.nnx * a.nnz;
+        float* o = a.ttn_out + (long long)s * nc;
+        for (long long q = lane; q < nc; q += nl) o[q] = C.ttn[q];
+    }
+}
+
+// One instance on one warp: lane 0 marches, all lanes share the rest.
+__device__ void fmm_instance(const FArgs& a, int s, int lane, long long slot)
+{
+    const FInst I = a.inst[s];
+    FField C, R;
+    inst_fields(a, I, slot, C, R);
+    HeapE* heap = a.w_heap + slot * a.wh;
+    step_init(a, I, C, R, lane, 32);
+    __syncwarp();
+    int r = 0;
+    if (a.asgr) {
+        if (lane == 0) r = travel(R, 1, I.scx, I.scz, I.vnl, I.vnr, I.vnt, I.vnb, heap, I.cap);
+        r = __shfl_sync(0xffffffffu, r, 0);
+        if (r) { if (lane == 0) record_error(a, r, s); return; }
+        __syncwarp();
+        step_map(a, I, C, R, lane, 32);
+        __syncwarp();
+        for (int base = 0; base < box_nodes(I); base += 32 * 32) {
+            const unsigned mask = step_band_decide(a, I, C, base, lane, 32);
+            __syncwarp();
+            step_band_write(a, I, C, base, lane, 32, mask);
+            __syncwarp();
+        }
+        if (lane == 0) r = travel(C, 2, I.scx, I.scz, I.vnl, I.vnr, I.vnt, I.vnb, heap, I.cap);
+    } else {
+        if (lane == 0) r = travel(C, 0, I.scx, I.scz, 0, 0, 0, 0, heap, I.cap);
+    }
+    r = __shfl_sync(0xffffffffu, r, 0);
+    if (r) { if (lane == 0) record_error(a, r, s); return; }
+    __syncwarp();
+    step_receivers(a, I, C, s, lane, 32);
+}
+
+__global__ void __launch_bounds__(32 * kWarpsPerBlock) fmm_kernel(FArgs a)
+{
+    const int lane = threadIdx.x & 31;
+    const long long slot = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
+    for (;;) {
+        unsigned s = 0;
+        if (lane == 0) s = atomicAdd(a.queue, 1u);
+        s = __shfl_sync(0xffffffffu, s, 0);
+        if (s >= (unsigned)a.ninst) break;
+        fmm_instance(a, (int)s, lane, slot);
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------ host layout
+constexpr float kPi = 3.1415926535898f;   // the reference's REAL(i10) pi
+
+// The propagation grid of the model grid (CalSurfG_parallel.f90:1920-1930,
+// 2068-2075), in the reference's real*4 operations.
+struct FGrid {
+    int nvx, nvz, nnx, nnz;
+    float gox, goz, dvx, dvz, dnx, dnz, drnx, drnz, dpl;
+    int maxbt;
+};
+
+inline int nint_cap(float snb, int a, int b)
+{
+    return (int)llround((double)snb * (double)a * (double)b);
+}
+
+inline FGrid grid_of(const dazi_fmm_params& p)
+{
+    FGrid g;
+    g.nvx = p.nx - 2; g.nvz = p.ny - 2;
+    g.nnx = (g.nvx - 1) * p.gdx + 1; g.nnz = (g.nvz - 1) * p.gdz + 1;
+    g.dvx = p.dvxd * kPi / 180.0f; g.dvz = p.dvzd * kPi / 180.0f;
+    g.gox = (90.0f - p.goxd) * kPi / 180.0f;
+    g.goz = p.gozd * kPi / 180.0f;
+    g.dnx = g.dvx / (float)p.gdx; g.dnz = g.dvz / (float)p.gdz;
+    g.drnx = g.dvx / (float)(p.gdx * p.sgdl); g.drnz = g.dvz / (float)(p.gdz * p.sgdl);
+    // srtimes_parallel's smallest node spacing (:1068-1072)
+    g.dpl = g.dnx * p.earth;
+    float rd1 = g.dnz * p.earth * sinf(g.gox);
+    if (rd1 < g.dpl) g.dpl = rd1;
+    rd1 = g.dnz * p.earth * sinf(g.gox + (float)(g.nnx - 1) * g.dnx);
+    if (rd1 < g.dpl) g.dpl = rd1;
+    g.maxbt = nint_cap(p.snb, g.nnx, g.nnz);
+    return g;
+}
+
+inline int check_params(const dazi_fmm_params* p, const char** msg)
+{
+    if (!p) return *msg = "FMM: params is NULL", DAZI_ERR_BADARG;
+    if (p->nx < 4 || p->ny < 4 || p->gdx < 1 || p->gdz < 1 || p->sgdl < 1 || p->sgs < 1 ||
+        (p->fom != 0 && p->fom != 1) || (p->asgr != 0 && p->asgr != 1) || !(p->snb > 0.0f) ||
+        !(p->earth > 0.0f) || !(p->dvxd > 0.0f) || !(p->dvzd > 0.0f))
+        return *msg = "FMM: invalid grid or solver settings", DAZI_ERR_BADARG;
+    const long long nnx = (long long)(p->nx - 3) * p->gdx + 1, nnz = (long long)(p->ny - 3) * p->gdz + 1;
+    const long long nr = 2LL * p->sgs * p->sgdl + 1;
+    if (nnx > 32767 || nnz > 32767 || nr > 32767)
+        return *msg = "FMM: propagation grid beyond 32767 nodes per side", DAZI_ERR_LIMITS;
+    return 0;
+}
+
+// Lay out the instances on the host: the refined box and origin of each
+// source (CalSurfG_parallel.f90:2163-2200), its narrow-band capacity, and
+// the ri*sin(colatitude) tables of its refined grid.
+inline int layout(const dazi_fmm_params& p, const FGrid& g, int nper, int ninst, const int* per,
+                  const float* scx, const float* scz, const long long* rc_off, std::vector<FInst>& inst,
+                  std::vector<float>& risti_r, long long& wr, int& wh, const char** msg)
+{
+    inst.resize(ninst);
+    risti_r.clear();
+    wr = 1; wh = g.maxbt + 1;
+    for (int s = 0; s < ninst; ++s) {
+        FInst I{};
+        if (per[s] < 0 || per[s] >= nper) return *msg = "FMM: period index outside the maps", DAZI_ERR_BADARG;
+        if (rc_off[s + 1] < rc_off[s]) return *msg = "FMM: receiver offsets decrease", DAZI_ERR_BADARG;
+        I.period = per[s];
+        I.scx = scx[s]; I.scz = scz[s];
+        I.rc_b = rc_off[s]; I.rc_e = rc_off[s + 1];
+        I.cap = g.maxbt;
+        int isx = (int)((scx[s] - g.gox) / g.dnx) + 1;
+        int isz = (int)((scz[s] - g.goz) / g.dnz) + 1;
+        if (!(isx >= 1 && isx <= g.nnx && isz >= 1 && isz <= g.nnz))
+            return *msg = "FMM: source outside the model", DAZI_ERR_BADARG;
+        if (p.asgr) {
+            if (isx == g.nnx) isx -= 1;
+            if (isz == g.nnz) isz -= 1;
+            I.vnl = isx - p.sgs < 1 ? 1 : isx - p.sgs;
+            I.vnr = isx + p.sgs > g.nnx ? g.nnx : isx + p.sgs;
+            I.vnt = isz - p.sgs < 1 ? 1 : isz - p.sgs;
+            I.vnb = isz + p.sgs > g.nnz ? g.nnz : isz + p.sgs;
+            I.nrnx = (I.vnr - I.vnl) * p.sgdl + 1;
+            I.nrnz = (I.vnb - I.vnt) * p.sgdl + 1;
+            // the example build's fused multiply-add (one rounding)
+            I.gorx = fmaf(g.dnx, (float)(I.vnl - 1), g.gox);
+            I.gorz = fmaf(g.dnz, (float)(I.vnt - 1), g.goz);
+            if (I.nrnx > g.nnx || I.nrnz > g.nnz)
+                I.cap = nint_cap(p.snb, I.nrnx > g.nnx ? I.nrnx : g.nnx, I.nrnz > g.nnz ? I.nrnz : g.nnz);
+            I.risti_r = (long long)risti_r.size();
+            for (int ix = 1; ix <= I.nrnx; ++ix)
+                risti_r.push_back(p.earth * sinf(I.gorx + (float)(ix - 1) * g.drnx));
+            const long long n = (long long)I.nrnx * I.nrnz;
+            if (n > wr) wr = n;
+        }
+        if (I.cap + 1 > wh) wh = I.cap + 1;
+        inst[s] = I;
+    }
+    if (risti_r.empty()) risti_r.push_back(0.0f);
+    return 0;
+}
+
+}  // namespace fmm
+}  // namespace dk

@@ -320,6 +320,70 @@ int dazi_lsmr_dev(int m, int n, long long nnz, const int *row, const int *col,
                   int itnlim, double *x, int *istop, int *itn, double *norms,
                   void *stream);
 
+/* First-arrival traveltimes (the FMM eikonal solver).
+ *
+ * The reference computes, per (period, source), the traveltime field on the
+ * propagation grid by fast marching and interpolates it at the receivers:
+ * the OpenMP loop of code/src_inv_iso_joint/CalSurfG_parallel.f90:2061-2340
+ * (gridder_parallel :811 on the period's phase-velocity map, source-grid
+ * refinement with bsplrefine_parallel :918 and travel_parallel :125 with
+ * urg = 1, then travel_parallel with urg = 2 on the coarse grid, and
+ * srtimes_parallel :997 per receiver).  These entries run that loop on the
+ * GPU for all instances at once, with the reference's arithmetic (real*4,
+ * its operation order, its binary-heap narrow band), so that every field
+ * and time is the reference's value.  Ray paths (rpaths) are not part of
+ * it. */
+typedef struct {
+    int nx, ny;                     /* model grid: pv maps are nx*ny, x fastest */
+    float goxd, gozd, dvxd, dvzd;   /* first inner vertex (lat, lon) and spacing, degrees */
+    int gdx, gdz;                   /* grid dicing (CalSurfG_parallel.f90:1900-1911: 5, 5) */
+    int asgr, sgdl, sgs;            /* source-grid refinement on, dicing, extent (1, 8, 8) */
+    int fom;                        /* 0 first-order, 1 mixed-order upwind scheme (1) */
+    float snb;                      /* narrow-band capacity as a fraction of the nodes (0.5) */
+    float earth;                    /* Earth radius, km (6371) */
+} dazi_fmm_params;
+
+/* The reference's settings for a model grid. */
+void dazi_fmm_default_params(dazi_fmm_params *p, int nx, int ny, float goxd, float gozd,
+                             float dvxd, float dvzd);
+
+/* Traveltimes of ninst (period, source) instances: pv (nx*ny, nper) real*8
+ * phase-velocity maps; instance s uses column inst_period[s] (0-based), its
+ * source at (scx[s], scz[s]) and receivers rc_off[s] .. rc_off[s+1]-1 at
+ * (rcx, rcz), all in radians as colatitude and longitude (real*4, as
+ * Main_Jt.f90:412-431 converts them).  times (rc_off[ninst]) real*4 out;
+ * ttn, when not NULL, receives each instance's coarse field as the
+ * reference's ttn(nnz, nnx) (nnx = (nx-3)*gdx+1, nnz = (ny-3)*gdz+1).
+ * Host arrays; returns DAZI_ERR_BADARG for a source or receiver outside
+ * the grid, DAZI_ERR_LIMITS when a narrow band outgrows snb of the nodes
+ * (the reference's array bound). */
+int dazi_fmm_batch(const dazi_fmm_params *p, const double *pv, int nper, int ninst,
+                   const int *inst_period, const float *scx, const float *scz,
+                   const long long *rc_off, const float *rcx, const float *rcz,
+                   float *times, float *ttn);
+
+/* Device-pointer form of dazi_fmm_batch (all arrays in device memory),
+ * stream-ordered on `stream`; the host reads the instances' sources and
+ * receiver offsets once to lay out the work. */
+int dazi_fmm_batch_dev(const dazi_fmm_params *p, const double *pv, int nper, int ninst,
+                       const int *inst_period, const float *scx, const float *scz,
+                       const long long *rc_off, const float *rcx, const float *rcz,
+                       float *times, float *ttn, void *stream);
+
+/* The reference's own arrays, by reference (Fortran-callable): the source
+ * and receiver tables of CalSurfG_parallel.f90:1745-1850 (scxf, sczf
+ * (nsrc, kmax); rcxf, rczf (nrc, nsrc, kmax); nrc1 (nsrc, kmax); nsrc1
+ * (kmax); periods (nsrc, kmax), the 1-based column of pv for each source),
+ * pv (nx*ny, nper) real*8 and the grid of para.in; writes dsurf (dall) in
+ * the row order of countsurf (FmmBackend.f90:64-72: period, source,
+ * receiver). */
+int dazi_fmm_times(const int *nx, const int *ny, const int *kmax, const int *nsrc,
+                   const int *nrc, const int *nper, const double *pv, const int *periods,
+                   const int *nsrc1, const int *nrc1, const float *scxf, const float *sczf,
+                   const float *rcxf, const float *rczf, const float *goxd,
+                   const float *gozd, const float *dvxd, const float *dvzd,
+                   const long long *dall, float *dsurf);
+
 /* Per-phase timing: with dazi_dk_set_timing(1), each call records CUDA
  * events on its stream around its phases ("prep", "fd", "root", "adjoint",
  * "ti"); dazi_dk_last_timing fills up to cap (name, milliseconds) pairs of

@@ -329,7 +329,7 @@ static float bilinear(const float nv[2][2], float dsx, float dsz, float dnx, flo
 // sides are compared with this grid's own node counts (:249-254), so those
 // two always stop the refined run.  Returns 0, -1 (source outside the
 // grid), -2 (narrow band larger than maxbt), -3 (a node without an upwind
-// solution).
+// solution), -5 (urg 2 without a close node: the field is undefined).
 static int travel(float scx, float scz, int urg, const Grid* g, int vnl, int vnr, int vnt, int vnb,
                   int* nsts, const float* veln, float* ttn, Bt* btg, int maxbt)
 {
@@ -344,6 +344,10 @@ static int travel(float scx, float scz, int urg, const Grid* g, int vnl, int vnr
         for (int i = 1; i <= nnx; ++i)
             for (int j = 1; j <= nnz; ++j)
                 if (AT(nsts, j, i) > 0 && (r = addtree(j, i, &ntr, maxbt, nsts, ttn, btg, ld))) return r;
+        // the refined sweep stopped before it reached a coarse node (a source
+        // in the last cell before the right or bottom side, which always
+        // stops it): the reference's field is whatever its array held
+        if (ntr == 0) return -5;
     } else {
         for (int i = 1; i <= nnx; ++i)
             for (int j = 1; j <= nnz; ++j) AT(nsts, j, i) = -1;
@@ -519,6 +523,10 @@ static int srtimes(float scx, float scz, float rcx1, float rcz1, const Grid* g, 
     if (isx == irx && isz == irz) sw = 1;
     float trr;
     if (sw) {
+        // the source's cell (not clamped here, :1062-1063): a source on the
+        // last node would read past the grid, which the reference's
+        // bounds-checked build stops on
+        if (isx < 1 || isx >= nnx || isz < 1 || isz >= nnz) return -1;
         float vss[2][2];
         for (int k = 1; k <= 2; ++k)
             for (int l = 1; l <= 2; ++l) vss[k - 1][l - 1] = AT(veln, isz - 1 + l, isx - 1 + k);
@@ -568,7 +576,7 @@ static int one_source(const OrFmmParams* P, const float* velv, const float* veln
     cg.gox = (90.0f - P->goxd) * kPi / 180.0f;
     cg.goz = P->gozd * kPi / 180.0f;
     cg.earth = P->earth; cg.fom = P->fom;
-    const int maxbt = (int)lrint((double)P->snb * (double)nnx * (double)nnz);
+    const int maxbt = (int)llround((double)P->snb * (double)nnx * (double)nnz);
     int r = 0;
     Bt* btg = NULL;
     if (!P->asgr) {
@@ -605,7 +613,7 @@ static int one_source(const OrFmmParams* P, const float* velv, const float* veln
     int maxbt_r = maxbt;
     if (rg.nnx > nnx || rg.nnz > nnz) {
         const int d1 = rg.nnx > nnx ? rg.nnx : nnx, d2 = rg.nnz > nnz ? rg.nnz : nnz;
-        maxbt_r = (int)lrint((double)P->snb * (double)d1 * (double)d2);
+        maxbt_r = (int)llround((double)P->snb * (double)d1 * (double)d2);
     }
     const size_t nr = (size_t)rg.nnx * rg.nnz;
     float* velr = malloc(sizeof(float) * nr);
@@ -706,7 +714,7 @@ int or_fmm_travel(int nnx, int nnz, float gox, float goz, float dnx, float dnz, 
     Grid g;
     g.nnx = nnx; g.nnz = nnz; g.ld = nnz;
     g.gox = gox; g.goz = goz; g.dnx = dnx; g.dnz = dnz; g.earth = earth; g.fom = fom;
-    const int maxbt = (int)lrint((double)snb * (double)nnx * (double)nnz);
+    const int maxbt = (int)llround((double)snb * (double)nnx * (double)nnz);
     int* nsts = malloc(sizeof(int) * (size_t)nnx * nnz);
     Bt* btg = malloc(sizeof(Bt) * (size_t)(maxbt + 1));
     const int r = travel(scx, scz, 0, &g, 0, 0, 0, 0, nsts, veln, ttn, btg, maxbt);

@@ -87,3 +87,28 @@ def adjoint_batch(node_off, depz, vs, per_off, periods, minthk, ifunc=2, group=F
                                  P(st, ctypes.c_int), P(sen_off, i64), P(sen[0], f64),
                                  P(sen[1], f64), P(sen[2], f64), P(dropped, ctypes.c_ubyte))
     return rc, pv, st, sen, sen_off, dropped.astype(bool)
+
+
+def fmm_batch(params, pv, inst_period, scx, scz, rc_off, rcx, rcz, fields=False):
+    """Receiver times (and, when fields, the coarse fields (ninst, nnx, nnz))
+    of the library's traveltime device code built for the host; params is a
+    ctypes structure with dazi_fmm_params' layout."""
+    P = lambda a, t: a.ctypes.data_as(ctypes.POINTER(t))  # noqa: E731
+    pv = np.asfortranarray(pv, np.float64)
+    ninst = len(inst_period)
+    rc_off = np.ascontiguousarray(rc_off, np.int64)
+    times = np.zeros(max(int(rc_off[-1]), 1), np.float32)
+    nnx, nnz = (params.nx - 3) * params.gdx + 1, (params.ny - 3) * params.gdz + 1
+    ttn = np.zeros((ninst, nnx, nnz), np.float32) if fields else None
+    code = ctypes.c_int(0)
+    f32, i32 = ctypes.c_float, ctypes.c_int
+    rc = lib().emu_fmm_batch(ctypes.byref(params), P(pv, ctypes.c_double), int(pv.shape[1]), ninst,
+                             P(np.ascontiguousarray(inst_period, np.int32), i32),
+                             P(np.ascontiguousarray(scx, np.float32), f32),
+                             P(np.ascontiguousarray(scz, np.float32), f32), P(rc_off, ctypes.c_longlong),
+                             P(np.ascontiguousarray(rcx, np.float32), f32),
+                             P(np.ascontiguousarray(rcz, np.float32), f32), P(times, f32),
+                             None if ttn is None else P(ttn, f32), ctypes.byref(code))
+    if rc:
+        raise RuntimeError(f"emu fmm_batch: {rc} (instance error {code.value})")
+    return (times[:int(rc_off[-1])], ttn) if fields else times[:int(rc_off[-1])]

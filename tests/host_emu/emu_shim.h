@@ -70,6 +70,8 @@ static inline unsigned long long atomicAdd(unsigned long long* p, unsigned long 
     return o;
 }
 static inline int atomicAdd(int* p, int v) { int o = *p; *p += v; return o; }
+static inline int atomicCAS(int* p, int cmp, int v) { int o = *p; if (o == cmp) *p = v; return o; }
+static inline void __syncwarp(unsigned = 0xffffffffu) {}
 static inline int atomicOr(int* p, int v) { int o = *p; *p |= v; return o; }
 template <class T> static inline T __shfl_sync(unsigned, T v, int) { return v; }
 static inline unsigned __reduce_add_sync(unsigned, unsigned v) { return v; }

@@ -1,6 +1,7 @@
 // TEST INFRASTRUCTURE ONLY: the table build (k_prep.cu), the root search
 // (root_kernel, k_plain.cu), the adjoint sweeps (k_adjoint.cu) and the
-// Gc/Gs sweep (k_ti.cu) of the library
+// Gc/Gs sweep (k_ti.cu) and the traveltime solver (fmm_device.cuh) of the
+// library
 // compiled as host code and driven in the order the library drives them
 // (build_tables, run_tables in csrc/capi.cu: columns sorted by (refined
 // layers, periods), 32-column tiles, one task per (tile, period), one lane
@@ -16,6 +17,7 @@ namespace dk { alignas(16) unsigned char smem_raw[1 << 16]; }
 #include "../../dazi_current_release_b200/csrc/k_plain.cu"
 #include "../../dazi_current_release_b200/csrc/k_ti.cu"
 #include "../../dazi_current_release_b200/csrc/k_adjoint.cu"
+#include "../../dazi_current_release_b200/csrc/fmm_device.cuh"
 using namespace dk;
 
 namespace {
@@ -221,5 +223,82 @@ extern "C" int emu_adjoint_batch(long long ncols, const long long* node_off, con
             else if (group) adjoint_rayleigh_task<true>(j, task, lane, scr);
             else adjoint_rayleigh_task<false>(j, task, lane, scr);
         }
+    return 0;
+}
+
+// Traveltimes of a batch (dazi_fmm_batch's inputs) through the library's
+// traveltime device code, driven as run_fmm (k_fmm.cu) drives it: the maps'
+// vertex values and coarse grids by the gridding kernels' thread bodies,
+// then per instance the lane-shared steps for lanes 0..31 in turn around
+// lane 0's marching, one workspace slot.  times and, when not NULL, the
+// coarse fields ttn (as dazi_fmm_batch).  Returns 0, or the library's error
+// code with *code the instance's error.
+extern "C" int emu_fmm_batch(const dazi_fmm_params* p, const double* pv, int nper, int ninst,
+                             const int* per, const float* scx, const float* scz,
+                             const long long* rc_off, const float* rcx, const float* rcz,
+                             float* times, float* ttn, int* code)
+{
+    using namespace dk::fmm;
+    const char* msg = "";
+    int r;
+    if ((r = check_params(p, &msg))) return r;
+    const FGrid g = grid_of(*p);
+    std::vector<FInst> inst;
+    std::vector<float> risti_r;
+    long long wr = 1;
+    int wh = 1;
+    if ((r = layout(*p, g, nper, ninst, per, scx, scz, rc_off, inst, risti_r, wr, wh, &msg))) return r;
+    const long long nrc = rc_off[ninst], nc = (long long)g.nnx * g.nnz, nv = (long long)p->nx * p->ny;
+    std::vector<float> risti_c(g.nnx), sin_rcx(nrc > 0 ? nrc : 1);
+    for (int ix = 1; ix <= g.nnx; ++ix) risti_c[ix - 1] = p->earth * sinf(g.gox + (float)(ix - 1) * g.dnx);
+    for (long long q = 0; q < nrc; ++q) sin_rcx[q] = sinf(rcx[q]);
+    std::vector<float> velv(nv * nper), veln(nc * nper);
+    blockDim.x = 256;
+    for (long long t = 0; t < nv * nper; ++t) {
+        blockIdx.x = (unsigned)(t / 256); threadIdx.x = (unsigned)(t % 256);
+        fmm_velv_kernel(pv, p->nx, p->ny, nper, velv.data());
+    }
+    for (long long t = 0; t < nc * nper; ++t) {
+        blockIdx.x = (unsigned)(t / 256); threadIdx.x = (unsigned)(t % 256);
+        fmm_gridder_kernel(velv.data(), g.nvx, g.nvz, p->gdx, p->gdz, nper, veln.data());
+    }
+    std::vector<float> wt(nc), wvr(wr), wtr(wr);
+    std::vector<int> wn(nc), wnr(wr), ctl(4, 0);
+    std::vector<HeapE> heap(wh);
+    FArgs a;
+    a.ninst = ninst; a.inst = inst.data();
+    a.nnx = g.nnx; a.nnz = g.nnz; a.nvx = g.nvx; a.nvz = g.nvz; a.gdx = p->gdx; a.gdz = p->gdz;
+    a.sgdl = p->sgdl; a.fom = p->fom; a.asgr = p->asgr;
+    a.gox = g.gox; a.goz = g.goz; a.dnx = g.dnx; a.dnz = g.dnz; a.drnx = g.drnx; a.drnz = g.drnz;
+    a.earth = p->earth; a.dpl = g.dpl;
+    a.velv = velv.data(); a.veln = veln.data(); a.risti_c = risti_c.data(); a.risti_r = risti_r.data();
+    a.rcx = rcx; a.rcz = rcz; a.sin_rcx = sin_rcx.data(); a.times = times; a.ttn_out = ttn;
+    a.w_ttn = wt.data(); a.w_nsts = wn.data(); a.w_vr = wvr.data(); a.w_tr = wtr.data();
+    a.w_nr = wnr.data(); a.w_heap = heap.data(); a.wc = nc; a.wr = wr; a.wh = wh;
+    a.queue = nullptr; a.err = &ctl[1]; a.err_inst = &ctl[2];
+    for (int s = 0; s < ninst; ++s) {
+        const FInst& I = inst[s];
+        FField C, R;
+        inst_fields(a, I, 0, C, R);
+        for (int lane = 0; lane < 32; ++lane) step_init(a, I, C, R, lane, 32);
+        if (p->asgr) {
+            if ((r = travel(R, 1, I.scx, I.scz, I.vnl, I.vnr, I.vnt, I.vnb, heap.data(), I.cap))) {
+                *code = r;
+                return -1;
+            }
+            for (int lane = 0; lane < 32; ++lane) step_map(a, I, C, R, lane, 32);
+            for (int base = 0; base < box_nodes(I); base += 32 * 32) {
+                unsigned mask[32];
+                for (int lane = 0; lane < 32; ++lane) mask[lane] = step_band_decide(a, I, C, base, lane, 32);
+                for (int lane = 0; lane < 32; ++lane) step_band_write(a, I, C, base, lane, 32, mask[lane]);
+            }
+            r = travel(C, 2, I.scx, I.scz, I.vnl, I.vnr, I.vnt, I.vnb, heap.data(), I.cap);
+        } else {
+            r = travel(C, 0, I.scx, I.scz, 0, 0, 0, 0, heap.data(), I.cap);
+        }
+        if (r) { *code = r; return -1; }
+        for (int lane = 0; lane < 32; ++lane) step_receivers(a, I, C, s, lane, 32);
+        if (ctl[1]) { *code = ctl[1]; return -1; }
+    }
     return 0;
 }
