@@ -37,27 +37,50 @@ namespace dk {
 namespace fmm {
 
 constexpr int kWarpsPerBlock = 4;
+// narrow-band heap positions each warp keeps in shared memory (1 .. 1535);
+// bands larger than that (rare: the front of a 176 x 196 grid is at most
+// ~750 nodes) continue in the warp's global workspace
+constexpr int kHeapShared = 1536;
 
-// heap entry: the node's current time (kept equal to ttn at the node while
-// it is in the band) and its grid position
+// A node of a field: its time and status, the reference's ttn and nsts
+// (-1 far, 0 alive, > 0 its position in the narrow band's heap), side by
+// side so that one load brings both.
+struct Node {
+    float t;
+    int s;
+};
+
+// heap entry: the node's time (kept equal to its t while it is in the band)
+// and its grid position
 struct HeapE {
     float key;
     short px, pz;
 };
 
+struct Heap {
+    HeapE* sh;   // positions < kHeapShared (shared memory on the GPU)
+    HeapE* gl;   // all positions (global workspace; the low ones unused)
+    __device__ __forceinline__ HeapE get(int i) const { return i < kHeapShared ? sh[i] : gl[i]; }
+    __device__ __forceinline__ void put(int i, HeapE e) const
+    {
+        if (i < kHeapShared) sh[i] = e;
+        else gl[i] = e;
+    }
+};
+
 // One propagation grid of one instance: node (iz, ix), 1-based, at
-// a[(ix - 1) * nnz + (iz - 1)] as the reference's ttn(nnz, nnx).
+// [(ix - 1) * nnz + (iz - 1)] as the reference's ttn(nnz, nnx).
 struct FField {
     int nnx, nnz;
     float gox, goz, dnx, dnz, earth;
     int fom;
     const float* veln;
     const float* risti;   // [ix - 1]: earth * sin(gox + (ix - 1) * dnx)
-    float* ttn;
-    int* nsts;
+    Node* node;
 };
 
-#define FAT(a, iz, ix) (a)[(long long)((ix) - 1) * F.nnz + ((iz) - 1)]
+#define FN(iz, ix) F.node[(long long)((ix) - 1) * F.nnz + ((iz) - 1)]
+#define FV(iz, ix) F.veln[(long long)((ix) - 1) * F.nnz + ((iz) - 1)]
 
 // error codes of one instance
 constexpr int kErrOutside = 1;   // source or receiver outside the grid
@@ -67,64 +90,68 @@ constexpr int kErrSteps = 4;     // more pops than nodes (cannot happen)
 constexpr int kErrNoBand = 5;    // no close node after the refined sweep
 
 // ------------------------------------------------------------ heap
-// addtree_parallel (CalSurfG_parallel.f90:631-675)
-__device__ int heap_add(const FField& F, int iz, int ix, int& ntr, int cap, HeapE* h)
+// addtree_parallel (CalSurfG_parallel.f90:631-675): the new node enters at
+// the bottom and moves up while smaller than its parent (parents move down
+// into the hole, as the reference's swaps leave them)
+__device__ int heap_add(const FField& F, int iz, int ix, float key, int& ntr, int cap, const Heap& h)
 {
     if (ntr >= cap) return kErrBand;
     ntr += 1;
-    const float key = FAT(F.ttn, iz, ix);
     int tpc = ntr, tpp = tpc / 2;
-    while (tpp > 0 && key < h[tpp].key) {
-        h[tpc] = h[tpp];
-        FAT(F.nsts, h[tpc].pz, h[tpc].px) = tpc;
+    while (tpp > 0) {
+        const HeapE p = h.get(tpp);
+        if (!(key < p.key)) break;
+        h.put(tpc, p);
+        FN(p.pz, p.px).s = tpc;
         tpc = tpp;
         tpp = tpc / 2;
     }
-    h[tpc] = HeapE{key, (short)ix, (short)iz};
-    FAT(F.nsts, iz, ix) = tpc;
+    h.put(tpc, HeapE{key, (short)ix, (short)iz});
+    FN(iz, ix).s = tpc;
     return 0;
 }
 
-// updtree_parallel (CalSurfG_parallel.f90:770-803): the node's time was
-// just recomputed; it moves up while smaller than its parent
-__device__ void heap_update(const FField& F, int iz, int ix, HeapE* h)
+// updtree_parallel (CalSurfG_parallel.f90:770-803): the node at position
+// pos has the new time key; it moves up while smaller than its parent
+__device__ void heap_update(const FField& F, int iz, int ix, float key, int pos, const Heap& h)
 {
-    const float key = FAT(F.ttn, iz, ix);
-    int tpc = FAT(F.nsts, iz, ix), tpp = tpc / 2;
-    while (tpp > 0 && key < h[tpp].key) {
-        h[tpc] = h[tpp];
-        FAT(F.nsts, h[tpc].pz, h[tpc].px) = tpc;
+    int tpc = pos, tpp = tpc / 2;
+    while (tpp > 0) {
+        const HeapE p = h.get(tpp);
+        if (!(key < p.key)) break;
+        h.put(tpc, p);
+        FN(p.pz, p.px).s = tpc;
         tpc = tpp;
         tpp = tpc / 2;
     }
-    h[tpc] = HeapE{key, (short)ix, (short)iz};
-    FAT(F.nsts, iz, ix) = tpc;
+    h.put(tpc, HeapE{key, (short)ix, (short)iz});
+    FN(iz, ix).s = tpc;
 }
 
 // downtree_parallel (CalSurfG_parallel.f90:686-761): the root has been
 // taken; the last entry moves to the root and down while a child is
-// smaller (the smaller child; the right one on ties only if strictly
-// smaller, as rd1 > rd2 selects it)
-__device__ void heap_pop(const FField& F, int& ntr, HeapE* h)
+// smaller (the smaller child; the right one only if strictly smaller, as
+// the reference's rd1 > rd2 selects it)
+__device__ void heap_pop(const FField& F, int& ntr, const Heap& h)
 {
     if (ntr == 1) { ntr = 0; return; }
-    const HeapE last = h[ntr];
+    const HeapE last = h.get(ntr);
     ntr -= 1;
     int tpp = 1, tpc = 2;
     while (tpc <= ntr) {
-        HeapE c = h[tpc];
+        HeapE c = h.get(tpc);
         if (tpc < ntr) {
-            const HeapE c2 = h[tpc + 1];
+            const HeapE c2 = h.get(tpc + 1);
             if (c.key > c2.key) { c = c2; tpc += 1; }
         }
         if (!(c.key < last.key)) break;
-        h[tpp] = c;
-        FAT(F.nsts, c.pz, c.px) = tpp;
+        h.put(tpp, c);
+        FN(c.pz, c.px).s = tpp;
         tpp = tpc;
         tpc = 2 * tpp;
     }
-    h[tpp] = last;
-    FAT(F.nsts, last.pz, last.px) = tpp;
+    h.put(tpp, last);
+    FN(last.pz, last.px).s = tpp;
 }
 
 // ------------------------------------------------------------ upwind updates
@@ -135,141 +162,159 @@ __device__ __forceinline__ float quad_root(float a, float b, float c)
     return (-b + sqrtf(rd1)) / (2.0f * a);
 }
 
+// The nodes the upwind update of (iz, ix) reads, loaded together: along x
+// at ix-1, ix+1, ix-2, ix+2 (n[0..3]), along z at iz-1, iz+1, iz-2, iz+2
+// (n[4..7]), each with whether it lies in the grid (indices are clamped
+// into the grid for the load; nodes outside are never used).
+struct Stencil {
+    Node n[8];
+    bool in[8];
+    float slown, risti;
+};
+
+__device__ __forceinline__ void load_stencil(const FField& F, int iz, int ix, Stencil& S)
+{
+    const int d[4] = {-1, 1, -2, 2};
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int j = ix + d[q], k = iz + d[q];
+        S.in[q] = j >= 1 && j <= F.nnx;
+        S.in[4 + q] = k >= 1 && k <= F.nnz;
+        S.n[q] = FN(iz, j < 1 ? 1 : j > F.nnx ? F.nnx : j);
+        S.n[4 + q] = FN(k < 1 ? 1 : k > F.nnz ? F.nnz : k, ix);
+    }
+    S.slown = 1.0f / FV(iz, ix);
+    S.risti = F.risti[ix - 1];
+}
+
 // fouds1_parallel (CalSurfG_parallel.f90:346-432): first-order upwind time
-// of node (iz, ix) from its alive neighbours, the minimum over the four
-// quadrants
-__device__ int fouds1(const FField& F, int iz, int ix)
+// from the alive neighbours, the minimum over the four quadrants (a quadrant
+// only where both its neighbours lie in the grid)
+__device__ int fouds1(const FField& F, const Stencil& S, float& out)
 {
     int tsw1 = 0;
     float travm = 0.0f;
-    const float slown = 1.0f / FAT(F.veln, iz, ix);
-    const float ri = F.earth;
-    const float risti = F.risti[ix - 1];
-    for (int j = ix - 1; j <= ix + 1; j += 2) {
-        for (int k = iz - 1; k <= iz + 1; k += 2) {
-            if (j < 1 || j > F.nnx || k < 1 || k > F.nnz) continue;
+    const float slown = S.slown, ri = F.earth, risti = S.risti;
+    for (int a = 0; a < 2; ++a) {
+        for (int b = 0; b < 2; ++b) {
+            const int j = a, k = 4 + b;
+            if (!S.in[j] || !S.in[k]) continue;
             int swsol = 0;
-            float a = 0.0f, b = 0.0f, c = 0.0f, tref = 0.0f;
-            if (FAT(F.nsts, iz, j) == 0) {
+            float qa = 1.0f, qb = 0.0f, qc = 0.0f, tref = 0.0f;
+            if (S.n[j].s == 0) {
                 swsol = 1;
-                if (FAT(F.nsts, k, ix) == 0) {
+                if (S.n[k].s == 0) {
                     const float u = ri * F.dnx, v = risti * F.dnz;
-                    const float em = FAT(F.ttn, k, ix) - FAT(F.ttn, iz, j);
-                    a = u * u + v * v;
-                    b = -2.0f * (u * u) * em;
-                    c = (u * u) * (em * em - (v * v) * (slown * slown));
+                    const float em = S.n[k].t - S.n[j].t;
+                    qa = u * u + v * v;
+                    qb = -2.0f * (u * u) * em;
+                    qc = (u * u) * (em * em - (v * v) * (slown * slown));
                 } else {
-                    a = 1.0f;
-                    c = -(slown * slown) * (ri * ri) * (F.dnx * F.dnx);
+                    qc = -(slown * slown) * (ri * ri) * (F.dnx * F.dnx);
                 }
-                tref = FAT(F.ttn, iz, j);
-            } else if (FAT(F.nsts, k, ix) == 0) {
+                tref = S.n[j].t;
+            } else if (S.n[k].s == 0) {
                 swsol = 1;
-                a = 1.0f;
                 const float t = slown * risti * F.dnz;
-                c = -(t * t);
-                tref = FAT(F.ttn, k, ix);
+                qc = -(t * t);
+                tref = S.n[k].t;
             }
             if (swsol) {
-                const float trav = tref + quad_root(a, b, c);
+                const float trav = tref + quad_root(qa, qb, qc);
                 if (tsw1) travm = fminf(trav, travm);
                 else { travm = trav; tsw1 = 1; }
             }
         }
     }
     if (!tsw1) return kErrNoSol;
-    FAT(F.ttn, iz, ix) = travm;
+    out = travm;
     return 0;
 }
 
-// fouds2_parallel (CalSurfG_parallel.f90:443-622): mixed-order upwind
+// fouds2_parallel (CalSurfG_parallel.f90:443-622): mixed-order upwind time
 // (second-order stencils where two alive nodes line up and the time
-// decreases towards the node)
-__device__ int fouds2(const FField& F, int iz, int ix)
+// decreases towards the node), the minimum over the four quadrants
+__device__ int fouds2(const FField& F, const Stencil& S, float& out)
 {
     int tsw1 = 0;
     float travm = 0.0f;
-    const float slown = 1.0f / FAT(F.veln, iz, ix);
-    const float ri = F.earth;
-    const float risti = F.risti[ix - 1];
-    for (int j = ix - 1; j <= ix + 1; j += 2) {
-        if (j < 1 || j > F.nnx) continue;
-        const int j2 = j == ix - 1 ? j - 1 : j + 1;
-        const bool aj = FAT(F.nsts, iz, j) == 0;
-        bool swj = false;   // second-order operator in x
-        if (aj && j2 >= 1 && j2 <= F.nnx && FAT(F.nsts, iz, j2) == 0)
-            swj = FAT(F.ttn, iz, j) > FAT(F.ttn, iz, j2);
-        for (int k = iz - 1; k <= iz + 1; k += 2) {
-            if (k < 1 || k > F.nnz) continue;
-            const int k2 = k == iz - 1 ? k - 1 : k + 1;
-            const bool ak = FAT(F.nsts, k, ix) == 0;
-            bool swk = false;
-            if (ak && k2 >= 1 && k2 <= F.nnz && FAT(F.nsts, k2, ix) == 0)
-                swk = FAT(F.ttn, k, ix) > FAT(F.ttn, k2, ix);
+    const float slown = S.slown, ri = F.earth, risti = S.risti;
+    for (int a = 0; a < 2; ++a) {
+        const int j = a, j2 = 2 + a;
+        if (!S.in[j]) continue;
+        const bool aj = S.n[j].s == 0;
+        const bool swj = aj && S.in[j2] && S.n[j2].s == 0 && S.n[j].t > S.n[j2].t;
+        const float tj = S.n[j].t, tj2 = S.n[j2].t;
+        for (int b = 0; b < 2; ++b) {
+            const int k = 4 + b, k2 = 6 + b;
+            if (!S.in[k]) continue;
+            const bool ak = S.n[k].s == 0;
+            const bool swk = ak && S.in[k2] && S.n[k2].s == 0 && S.n[k].t > S.n[k2].t;
+            const float tk = S.n[k].t, tk2 = S.n[k2].t;
             int swsol = 0;
-            float a = 1.0f, b = 0.0f, c = 0.0f, tref = 0.0f, tdiv = 1.0f;
+            float qa = 1.0f, qb = 0.0f, qc = 0.0f, tref = 0.0f, tdiv = 1.0f;
             if (swj) {
                 swsol = 1;
                 if (swk) {
                     const float u = 2.0f * ri * F.dnx, v = 2.0f * risti * F.dnz;
-                    float em = 4.0f * FAT(F.ttn, iz, j) - FAT(F.ttn, iz, j2) - 4.0f * FAT(F.ttn, k, ix);
-                    em = em + FAT(F.ttn, k2, ix);
-                    a = v * v + u * u;
-                    b = 2.0f * em * (u * u);
-                    c = (u * u) * (em * em - (slown * slown) * (v * v));
-                    tref = 4.0f * FAT(F.ttn, iz, j) - FAT(F.ttn, iz, j2);
+                    float em = 4.0f * tj - tj2 - 4.0f * tk;
+                    em = em + tk2;
+                    qa = v * v + u * u;
+                    qb = 2.0f * em * (u * u);
+                    qc = (u * u) * (em * em - (slown * slown) * (v * v));
+                    tref = 4.0f * tj - tj2;
                     tdiv = 3.0f;
                 } else if (ak) {
                     const float u = risti * F.dnz, v = 2.0f * ri * F.dnx;
-                    const float em = 3.0f * FAT(F.ttn, k, ix) - 4.0f * FAT(F.ttn, iz, j) + FAT(F.ttn, iz, j2);
-                    a = v * v + 9.0f * (u * u);
-                    b = 6.0f * em * (u * u);
-                    c = (u * u) * (em * em - (slown * slown) * (v * v));
-                    tref = FAT(F.ttn, k, ix);
+                    const float em = 3.0f * tk - 4.0f * tj + tj2;
+                    qa = v * v + 9.0f * (u * u);
+                    qb = 6.0f * em * (u * u);
+                    qc = (u * u) * (em * em - (slown * slown) * (v * v));
+                    tref = tk;
                 } else {
                     const float u = 2.0f * ri * F.dnx;
-                    c = -(u * u) * (slown * slown);
-                    tref = 4.0f * FAT(F.ttn, iz, j) - FAT(F.ttn, iz, j2);
+                    qc = -(u * u) * (slown * slown);
+                    tref = 4.0f * tj - tj2;
                     tdiv = 3.0f;
                 }
             } else if (aj) {
                 swsol = 1;
                 if (swk) {
                     const float u = ri * F.dnx, v = 2.0f * risti * F.dnz;
-                    const float em = 3.0f * FAT(F.ttn, iz, j) - 4.0f * FAT(F.ttn, k, ix) + FAT(F.ttn, k2, ix);
-                    a = v * v + 9.0f * (u * u);
-                    b = 6.0f * em * (u * u);
-                    c = (u * u) * (em * em - (v * v) * (slown * slown));
+                    const float em = 3.0f * tj - 4.0f * tk + tk2;
+                    qa = v * v + 9.0f * (u * u);
+                    qb = 6.0f * em * (u * u);
+                    qc = (u * u) * (em * em - (v * v) * (slown * slown));
                 } else if (ak) {
                     const float u = ri * F.dnx, v = risti * F.dnz;
-                    const float em = FAT(F.ttn, k, ix) - FAT(F.ttn, iz, j);
-                    a = u * u + v * v;
-                    b = -2.0f * (u * u) * em;
-                    c = (u * u) * (em * em - (v * v) * (slown * slown));
+                    const float em = tk - tj;
+                    qa = u * u + v * v;
+                    qb = -2.0f * (u * u) * em;
+                    qc = (u * u) * (em * em - (v * v) * (slown * slown));
                 } else {
-                    c = -(slown * slown) * (ri * ri) * (F.dnx * F.dnx);
+                    qc = -(slown * slown) * (ri * ri) * (F.dnx * F.dnx);
                 }
-                tref = FAT(F.ttn, iz, j);
+                tref = tj;
             } else if (swk) {
                 swsol = 1;
                 const float u = 2.0f * risti * F.dnz;
-                c = -(u * u) * (slown * slown);
-                tref = 4.0f * FAT(F.ttn, k, ix) - FAT(F.ttn, k2, ix);
+                qc = -(u * u) * (slown * slown);
+                tref = 4.0f * tk - tk2;
                 tdiv = 3.0f;
             } else if (ak) {
                 swsol = 1;
-                c = -(slown * slown) * (risti * risti) * (F.dnz * F.dnz);
-                tref = FAT(F.ttn, k, ix);
+                qc = -(slown * slown) * (risti * risti) * (F.dnz * F.dnz);
+                tref = tk;
             }
             if (swsol) {
-                const float trav = (tref + quad_root(a, b, c)) / tdiv;
+                const float trav = (tref + quad_root(qa, qb, qc)) / tdiv;
                 if (tsw1) travm = fminf(trav, travm);
                 else { travm = trav; tsw1 = 1; }
             }
         }
     }
     if (!tsw1) return kErrNoSol;
-    FAT(F.ttn, iz, ix) = travm;
+    out = travm;
     return 0;
 }
 
@@ -287,75 +332,162 @@ __device__ float bilinear(const float nv[2][2], float dsx, float dsz, float dnx,
 }
 
 // ------------------------------------------------------------ travel
-// travel_parallel (CalSurfG_parallel.f90:125-336) on one thread.  urg 0 / 1
-// start from the source point (nsts already -1 everywhere); urg 1 stops
-// when the popped node lies on a side of the refined grid that is not the
-// model's (compared, as in the reference, with this grid's own node counts
-// on the right and bottom sides); urg 2 starts from the close nodes
-// (nsts > 0) of the box vnl..vnr x vnt..vnb, the only place they can be.
-__device__ int travel(const FField& F, int urg, float scx, float scz, int vnl, int vnr, int vnt,
-                      int vnb, HeapE* h, int cap)
+// travel_parallel (CalSurfG_parallel.f90:125-336), as phases:
+//   travel_start   the first band: urg 0 / 1 the four corners of the
+//                  source's cell (statuses already -1); urg 2 the close
+//                  nodes (status > 0) of the box vnl..vnr x vnt..vnb, the
+//                  only place they can be, in the reference's order;
+//   travel_pop     the band's minimum becomes alive; for urg 1 the sweep
+//                  stops instead when that node lies on a side of the
+//                  refined grid that is not the model's (compared, as in
+//                  the reference, with this grid's own node counts on the
+//                  right and bottom sides);
+//   travel_nbr     the new time of neighbour q (x-1, x+1, z-1, z+1) of the
+//                  popped node, if it is far or close;
+//   travel_commit  its band entry (added, or moved up).
+// The reference runs travel_nbr and travel_commit neighbour by neighbour;
+// the new times depend only on alive nodes, which the commits do not
+// change, so the four travel_nbr may also run first (travel_warp).
+struct Box {
+    int vnl, vnr, vnt, vnb;
+};
+
+__device__ int travel_start(const FField& F, int urg, float scx, float scz, const Box& B, const Heap& h,
+                            int cap, int& ntr)
 {
-    const int nnx = F.nnx, nnz = F.nnz;
     int isx = (int)((scx - F.gox) / F.dnx) + 1;
     int isz = (int)((scz - F.goz) / F.dnz) + 1;
-    if (isx < 1 || isx > nnx || isz < 1 || isz > nnz) return kErrOutside;
-    if (isx == nnx) isx -= 1;
-    if (isz == nnz) isz -= 1;
-    int ntr = 0, r;
+    if (isx < 1 || isx > F.nnx || isz < 1 || isz > F.nnz) return kErrOutside;
+    if (isx == F.nnx) isx -= 1;
+    if (isz == F.nnz) isz -= 1;
+    ntr = 0;
+    int r;
     if (urg == 2) {
-        for (int i = vnl; i <= vnr; ++i)
-            for (int j = vnt; j <= vnb; ++j)
-                if (FAT(F.nsts, j, i) > 0 && (r = heap_add(F, j, i, ntr, cap, h))) return r;
+        for (int i = B.vnl; i <= B.vnr; ++i)
+            for (int j = B.vnt; j <= B.vnb; ++j) {
+                const Node n = FN(j, i);
+                if (n.s > 0 && (r = heap_add(F, j, i, n.t, ntr, cap, h))) return r;
+            }
         // the refined sweep stopped before it reached a coarse node (a
         // source in the last cell before the right or bottom side, whose
         // refined sweep always stops there): the reference leaves the
         // field as its array held it, so this is reported, not computed
-        if (ntr == 0) return kErrNoBand;
-    } else {
-        float vss[2][2];
-        for (int i = 1; i <= 2; ++i)
-            for (int j = 1; j <= 2; ++j) vss[i - 1][j - 1] = FAT(F.veln, isz - 1 + j, isx - 1 + i);
-        const float dsx = (scx - F.gox) - (float)(isx - 1) * F.dnx;
-        const float dsz = (scz - F.goz) - (float)(isz - 1) * F.dnz;
-        const float vsrc = bilinear(vss, dsx, dsz, F.dnx, F.dnz);
-        for (int i = 1; i <= 2; ++i)
-            for (int j = 1; j <= 2; ++j) {
-                const float ex = dsx - (float)(i - 1) * F.dnx, ez = dsz - (float)(j - 1) * F.dnz;
-                const float ds = sqrtf(ex * ex + ez * ez);
-                FAT(F.ttn, isz - 1 + j, isx - 1 + i) = 2.0f * ds / (vss[i - 1][j - 1] + vsrc);
-                if ((r = heap_add(F, isz - 1 + j, isx - 1 + i, ntr, cap, h))) return r;
-            }
+        return ntr == 0 ? kErrNoBand : 0;
     }
-    const long long maxpops = (long long)nnx * nnz + 4;
+    float vss[2][2];
+    for (int i = 1; i <= 2; ++i)
+        for (int j = 1; j <= 2; ++j) vss[i - 1][j - 1] = FV(isz - 1 + j, isx - 1 + i);
+    const float dsx = (scx - F.gox) - (float)(isx - 1) * F.dnx;
+    const float dsz = (scz - F.goz) - (float)(isz - 1) * F.dnz;
+    const float vsrc = bilinear(vss, dsx, dsz, F.dnx, F.dnz);
+    for (int i = 1; i <= 2; ++i)
+        for (int j = 1; j <= 2; ++j) {
+            const float ex = dsx - (float)(i - 1) * F.dnx, ez = dsz - (float)(j - 1) * F.dnz;
+            const float ds = sqrtf(ex * ex + ez * ez);
+            const float t = 2.0f * ds / (vss[i - 1][j - 1] + vsrc);
+            FN(isz - 1 + j, isx - 1 + i).t = t;
+            if ((r = heap_add(F, isz - 1 + j, isx - 1 + i, t, ntr, cap, h))) return r;
+        }
+    return 0;
+}
+
+// returns true when the refined sweep stops (the node is made alive too)
+__device__ bool travel_pop(const FField& F, int urg, const Box& B, const Heap& h, int& ntr, int& ix, int& iz)
+{
+    const HeapE root = h.get(1);
+    ix = root.px;
+    iz = root.pz;
+    FN(iz, ix).s = 0;
+    if (urg == 1 && ((ix == 1 && B.vnl != 1) || (ix == F.nnx && B.vnr != F.nnx) || (iz == 1 && B.vnt != 1) ||
+                     (iz == F.nnz && B.vnb != F.nnz)))
+        return true;
+    heap_pop(F, ntr, h);
+    return false;
+}
+
+// neighbour q of the popped (iz, ix): st = its status (0: nothing to do)
+__device__ int travel_nbr(const FField& F, int iz, int ix, int q, int& niz, int& nix, int& st, float& t)
+{
+    niz = q < 2 ? iz : iz - 1 + 2 * (q - 2);
+    nix = q < 2 ? ix - 1 + 2 * q : ix;
+    st = 0;
+    if (nix < 1 || nix > F.nnx || niz < 1 || niz > F.nnz) return 0;
+    Stencil S;
+    load_stencil(F, niz, nix, S);
+    st = FN(niz, nix).s;
+    if (st == 0) return 0;
+    return F.fom == 0 ? fouds1(F, S, t) : fouds2(F, S, t);
+}
+
+__device__ int travel_commit(const FField& F, int niz, int nix, int st, float t, const Heap& h, int& ntr, int cap)
+{
+    FN(niz, nix).t = t;
+    if (st < 0) return heap_add(F, niz, nix, t, ntr, cap, h);
+    heap_update(F, niz, nix, t, st, h);
+    return 0;
+}
+
+// The reference's order on one thread.
+__device__ int travel_seq(const FField& F, int urg, float scx, float scz, const Box& B, const Heap& h, int cap)
+{
+    int ntr = 0, r;
+    if ((r = travel_start(F, urg, scx, scz, B, h, cap, ntr))) return r;
+    const long long maxpops = (long long)F.nnx * F.nnz + 4;
     for (long long pops = 0; ntr > 0; ++pops) {
         if (pops > maxpops) return kErrSteps;
-        const int ix = h[1].px, iz = h[1].pz;
-        if (urg == 1 && ((ix == 1 && vnl != 1) || (ix == nnx && vnr != nnx) || (iz == 1 && vnt != 1) ||
-                         (iz == nnz && vnb != nnz))) {
-            FAT(F.nsts, iz, ix) = 0;
-            break;
-        }
-        FAT(F.nsts, iz, ix) = 0;
-        heap_pop(F, ntr, h);
-        // the neighbours in x, then in z (CalSurfG_parallel.f90:288-334)
-#pragma unroll 1
+        int ix, iz;
+        if (travel_pop(F, urg, B, h, ntr, ix, iz)) break;
         for (int q = 0; q < 4; ++q) {
-            const int niz = q < 2 ? iz : iz - 1 + 2 * (q - 2);
-            const int nix = q < 2 ? ix - 1 + 2 * q : ix;
-            if (nix < 1 || nix > nnx || niz < 1 || niz > nnz) continue;
-            const int st = FAT(F.nsts, niz, nix);
-            if (st == 0) continue;
-            r = F.fom == 0 ? fouds1(F, niz, nix) : fouds2(F, niz, nix);
-            if (r) return r;
-            if (st < 0) {
-                if ((r = heap_add(F, niz, nix, ntr, cap, h))) return r;
-            } else {
-                heap_update(F, niz, nix, h);
-            }
+            int niz, nix, st;
+            float t = 0.0f;
+            if ((r = travel_nbr(F, iz, ix, q, niz, nix, st, t))) return r;
+            if (st != 0 && (r = travel_commit(F, niz, nix, st, t, h, ntr, cap))) return r;
         }
     }
     return 0;
+}
+
+// On a warp: lane 0 keeps the band; lanes 0..3 form the four neighbours'
+// times at once after each pop.
+__device__ int travel_warp(const FField& F, int urg, float scx, float scz, const Box& B, const Heap& h, int cap,
+                           int lane)
+{
+    const unsigned all = 0xffffffffu;
+    int ntr = 0, r = 0;
+    if (lane == 0) r = travel_start(F, urg, scx, scz, B, h, cap, ntr);
+    r = __shfl_sync(all, r, 0);
+    if (r) return r;
+    const long long maxpops = (long long)F.nnx * F.nnz + 4;
+    for (long long pops = 0;; ++pops) {
+        int code = 0;   // 1 done, 2 refined sweep stopped, 3 too many pops; else (ix << 16) | iz, +4
+        if (lane == 0) {
+            int ix, iz;
+            if (ntr == 0) code = 1;
+            else if (pops > maxpops) code = 3;
+            else if (travel_pop(F, urg, B, h, ntr, ix, iz)) code = 2;
+            else code = 4 + ((ix << 16) | iz);
+        }
+        code = __shfl_sync(all, code, 0);
+        if (code < 4) return code == 3 ? kErrSteps : 0;
+        const int ix = (code - 4) >> 16, iz = (code - 4) & 0xffff;
+        __syncwarp();
+        int niz = 0, nix = 0, st = 0, e = 0;
+        float t = 0.0f;
+        if (lane < 4) e = travel_nbr(F, iz, ix, lane, niz, nix, st, t);
+        __syncwarp();
+        for (int q = 0; q < 4; ++q) {
+            const int eq = __shfl_sync(all, e, q), sq = __shfl_sync(all, st, q);
+            const int zq = __shfl_sync(all, niz, q), xq = __shfl_sync(all, nix, q);
+            const float tq = __shfl_sync(all, t, q);
+            if (lane == 0 && !r) {
+                if (eq) r = eq;
+                else if (sq != 0) r = travel_commit(F, zq, xq, sq, tq, h, ntr, cap);
+            }
+        }
+        r = __shfl_sync(all, r, 0);
+        if (r) return r;
+        __syncwarp();
+    }
 }
 
 // ------------------------------------------------------------ gridding
@@ -444,13 +576,11 @@ struct FArgs {
     float* times;
     float* ttn_out;             // [instance][nnx * nnz] or nullptr
     // per-warp workspace slots
-    float* w_ttn;
-    int* w_nsts;
-    float* w_vr;
-    float* w_tr;
-    int* w_nr;
-    HeapE* w_heap;
-    long long wc, wr, wh;       // slot sizes: coarse nodes, refined nodes, heap entries
+    Node* w_node;               // coarse field
+    Node* w_rnode;              // refined field
+    float* w_vr;                // refined velocities
+    HeapE* w_heap;              // heap positions >= kHeapShared
+    long long wc, wr, wh;       // slot sizes: coarse nodes, refined nodes, heap positions
     unsigned* queue;
     int* err;                   // first error code (0: none)
     int* err_inst;              // its instance
@@ -461,9 +591,9 @@ __device__ void record_error(const FArgs& a, int code, int s)
     if (atomicCAS(a.err, 0, code) == 0) *a.err_inst = s;
 }
 
-// srtimes_parallel (CalSurfG_parallel.f90:997-1125) for receiver q of an
-// instance whose coarse field is C (dpl, the smallest node spacing, and
-// sin(rcx) come from the host)
+// srtimes_parallel (CalSurfG_parallel.f90:997-1125) for receiver q on the
+// coarse field F (dpl, the smallest node spacing, and sin(rcx) come from the
+// host)
 __device__ int srtimes(const FArgs& a, const FField& F, float scx, float scz, long long q, float& out)
 {
     const float rcx1 = a.rcx[q], rcz1 = a.rcz[q];
@@ -482,15 +612,18 @@ __device__ int srtimes(const FArgs& a, const FField& F, float scx, float scz, lo
     const bool sw = sred < a.dpl || (isx == irx && isz == irz);
     float trr;
     if (sw) {
+        // the source's cell is not clamped here (:1062-1063): a source on
+        // the last node would read past the grid, which the reference's
+        // bounds-checked build stops on
         if (isx < 1 || isx >= F.nnx || isz < 1 || isz >= F.nnz) return kErrOutside;
         float vss[2][2];
         for (int k = 1; k <= 2; ++k)
-            for (int l = 1; l <= 2; ++l) vss[k - 1][l - 1] = FAT(F.veln, isz - 1 + l, isx - 1 + k);
+            for (int l = 1; l <= 2; ++l) vss[k - 1][l - 1] = FV(isz - 1 + l, isx - 1 + k);
         float drx = (scx - F.gox) - (float)(isx - 1) * F.dnx;
         float drz = (scz - F.goz) - (float)(isz - 1) * F.dnz;
         const float vels = bilinear(vss, drx, drz, F.dnx, F.dnz);
         for (int k = 1; k <= 2; ++k)
-            for (int l = 1; l <= 2; ++l) vss[k - 1][l - 1] = FAT(F.veln, irz - 1 + l, irx - 1 + k);
+            for (int l = 1; l <= 2; ++l) vss[k - 1][l - 1] = FV(irz - 1 + l, irx - 1 + k);
         drx = (rcx1 - F.gox) - (float)(irx - 1) * F.dnx;
         drz = (rcz1 - F.goz) - (float)(irz - 1) * F.dnz;
         const float velr = bilinear(vss, drx, drz, F.dnx, F.dnz);
@@ -503,14 +636,14 @@ __device__ int srtimes(const FArgs& a, const FField& F, float scx, float scz, lo
             for (int l = 1; l <= 2; ++l) {
                 const float produ = (1.0f - fabsf(((float)(l - 1) * F.dnz - drz) / F.dnz)) *
                                     (1.0f - fabsf(((float)(k - 1) * F.dnx - drx) / F.dnx));
-                trr = trr + FAT(F.ttn, irz - 1 + l, irx - 1 + k) * produ;
+                trr = trr + FN(irz - 1 + l, irx - 1 + k).t * produ;
             }
     }
     out = trr;
     return 0;
 }
 
-// The fields of instance s in workspace slot `slot`: C the coarse grid, R
+// The fields of an instance in workspace slot `slot`: C the coarse grid, R
 // the refined source grid.
 __device__ void inst_fields(const FArgs& a, const FInst& I, long long slot, FField& C, FField& R)
 {
@@ -518,15 +651,15 @@ __device__ void inst_fields(const FArgs& a, const FInst& I, long long slot, FFie
     C.gox = a.gox; C.goz = a.goz; C.dnx = a.dnx; C.dnz = a.dnz; C.earth = a.earth; C.fom = a.fom;
     C.veln = a.veln + (long long)I.period * a.nnx * a.nnz;
     C.risti = a.risti_c;
-    C.ttn = a.w_ttn + slot * a.wc;
-    C.nsts = a.w_nsts + slot * a.wc;
+    C.node = a.w_node + slot * a.wc;
     R.nnx = I.nrnx; R.nnz = I.nrnz;
     R.gox = I.gorx; R.goz = I.gorz; R.dnx = a.drnx; R.dnz = a.drnz; R.earth = a.earth; R.fom = a.fom;
     R.risti = a.risti_r + I.risti_r;
     R.veln = a.w_vr + slot * a.wr;
-    R.ttn = a.w_tr + slot * a.wr;
-    R.nsts = a.w_nr + slot * a.wr;
+    R.node = a.w_rnode + slot * a.wr;
 }
+
+__device__ __forceinline__ Box inst_box(const FInst& I) { return Box{I.vnl, I.vnr, I.vnt, I.vnb}; }
 
 // The steps of one instance that the lanes share: lane `lane` of `nl`.
 // The refined grid's velocities (bsplrefine_parallel), every status -1.
@@ -542,10 +675,10 @@ __device__ void step_init(const FArgs& a, const FInst& I, const FField& C, const
             const int idm2 = (int)(q / I.nrnz) + 1, idm1 = (int)(q % I.nrnz) + 1;
             vr[q] = bspline_node(velv, a.nvx, a.nvz, a.gdz * a.sgdl, a.gdx * a.sgdl, origz + idm1 - 1,
                                  origx + idm2 - 1);
-            R.nsts[q] = -1;
+            R.node[q].s = -1;
         }
     }
-    for (long long q = lane; q < nc; q += nl) C.nsts[q] = -1;
+    for (long long q = lane; q < nc; q += nl) C.node[q].s = -1;
 }
 
 // Refined nodes on coarse nodes carry status and time over
@@ -556,10 +689,10 @@ __device__ void step_map(const FArgs& a, const FInst& I, const FField& C, const 
     for (int q = lane; q < nbox; q += nl) {
         const int idm2 = I.vnl + q / bz, idm1 = I.vnt + q % bz;
         const int l = (idm2 - I.vnl) * a.sgdl + 1, k = (idm1 - I.vnt) * a.sgdl + 1;
-        const long long rq = (long long)(l - 1) * I.nrnz + (k - 1);
-        const int st = R.nsts[rq];
-        C.nsts[(long long)(idm2 - 1) * a.nnz + (idm1 - 1)] = st;
-        if (st >= 0) C.ttn[(long long)(idm2 - 1) * a.nnz + (idm1 - 1)] = R.ttn[rq];
+        const Node rn = R.node[(long long)(l - 1) * I.nrnz + (k - 1)];
+        Node& cn = C.node[(long long)(idm2 - 1) * a.nnz + (idm1 - 1)];
+        cn.s = rn.s;
+        if (rn.s >= 0) cn.t = rn.t;
     }
 }
 
@@ -573,9 +706,9 @@ __device__ unsigned step_band_decide(const FArgs& a, const FInst& I, const FFiel
         const int q = base + t * nl + lane;
         if (q >= nbox) break;
         const int ix = I.vnl + q / bz, iz = I.vnt + q % bz;
-        if (FAT(F.nsts, iz, ix) != 0) continue;
-        if ((iz > 1 && FAT(F.nsts, iz - 1, ix) == -1) || (iz < F.nnz && FAT(F.nsts, iz + 1, ix) == -1) ||
-            (ix > 1 && FAT(F.nsts, iz, ix - 1) == -1) || (ix < F.nnx && FAT(F.nsts, iz, ix + 1) == -1))
+        if (FN(iz, ix).s != 0) continue;
+        if ((iz > 1 && FN(iz - 1, ix).s == -1) || (iz < F.nnz && FN(iz + 1, ix).s == -1) ||
+            (ix > 1 && FN(iz, ix - 1).s == -1) || (ix < F.nnx && FN(iz, ix + 1).s == -1))
             mask |= 1u << t;
     }
     return mask;
@@ -588,7 +721,7 @@ __device__ void step_band_write(const FArgs& a, const FInst& I, const FField& F,
     for (int t = 0; t < 32; ++t)
         if (mask >> t & 1u) {
             const int q = base + t * nl + lane;
-            FAT(F.nsts, I.vnt + q % bz, I.vnl + q / bz) = 1;
+            FN(I.vnt + q % bz, I.vnl + q / bz).s = 1;
         }
 }
 
@@ -606,23 +739,23 @@ __device__ void step_receivers(const FArgs& a, const FInst& I, const FField& C, 
     if (a.ttn_out) {
         const long long nc = (long long)a.nnx * a.nnz;
         float* o = a.ttn_out + (long long)s * nc;
-        for (long long q = lane; q < nc; q += nl) o[q] = C.ttn[q];
+        for (long long q = lane; q < nc; q += nl) o[q] = C.node[q].t;
     }
 }
 
-// One instance on one warp: lane 0 marches, all lanes share the rest.
-__device__ void fmm_instance(const FArgs& a, int s, int lane, long long slot)
+// One instance on one warp, its heap's first positions in `sh`.
+__device__ void fmm_instance(const FArgs& a, int s, int lane, long long slot, HeapE* sh)
 {
     const FInst I = a.inst[s];
     FField C, R;
     inst_fields(a, I, slot, C, R);
-    HeapE* heap = a.w_heap + slot * a.wh;
+    const Heap heap{sh, a.w_heap + slot * a.wh};
+    const Box B = inst_box(I);
     step_init(a, I, C, R, lane, 32);
     __syncwarp();
     int r = 0;
     if (a.asgr) {
-        if (lane == 0) r = travel(R, 1, I.scx, I.scz, I.vnl, I.vnr, I.vnt, I.vnb, heap, I.cap);
-        r = __shfl_sync(0xffffffffu, r, 0);
+        r = travel_warp(R, 1, I.scx, I.scz, B, heap, I.cap, lane);
         if (r) { if (lane == 0) record_error(a, r, s); return; }
         __syncwarp();
         step_map(a, I, C, R, lane, 32);
@@ -633,11 +766,10 @@ __device__ void fmm_instance(const FArgs& a, int s, int lane, long long slot)
             step_band_write(a, I, C, base, lane, 32, mask);
             __syncwarp();
         }
-        if (lane == 0) r = travel(C, 2, I.scx, I.scz, I.vnl, I.vnr, I.vnt, I.vnb, heap, I.cap);
+        r = travel_warp(C, 2, I.scx, I.scz, B, heap, I.cap, lane);
     } else {
-        if (lane == 0) r = travel(C, 0, I.scx, I.scz, 0, 0, 0, 0, heap, I.cap);
+        r = travel_warp(C, 0, I.scx, I.scz, B, heap, I.cap, lane);
     }
-    r = __shfl_sync(0xffffffffu, r, 0);
     if (r) { if (lane == 0) record_error(a, r, s); return; }
     __syncwarp();
     step_receivers(a, I, C, s, lane, 32);
@@ -645,14 +777,15 @@ __device__ void fmm_instance(const FArgs& a, int s, int lane, long long slot)
 
 __global__ void __launch_bounds__(32 * kWarpsPerBlock) fmm_kernel(FArgs a)
 {
-    const int lane = threadIdx.x & 31;
+    __shared__ HeapE sheap[kWarpsPerBlock][kHeapShared];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const long long slot = ((long long)blockIdx.x * blockDim.x + threadIdx.x) / 32;
     for (;;) {
         unsigned s = 0;
         if (lane == 0) s = atomicAdd(a.queue, 1u);
         s = __shfl_sync(0xffffffffu, s, 0);
         if (s >= (unsigned)a.ninst) break;
-        fmm_instance(a, (int)s, lane, slot);
+        fmm_instance(a, (int)s, lane, slot, sheap[w]);
         __syncwarp();
     }
 }

@@ -56,7 +56,7 @@ struct FBuf {
 };
 
 struct FWork {
-    FBuf velv, veln, inst, risti_c, risti_r, sin_rcx, wt, wn, wvr, wtr, wnr, wh, ctl;
+    FBuf velv, veln, inst, risti_c, risti_r, sin_rcx, wnode, wrnode, wvr, wh, ctl;
     FBuf pv, rcx, rcz, times, ttn, scx, scz, per, off;   // copies of host inputs
 };
 
@@ -100,9 +100,9 @@ int run_fmm(const dazi_fmm_params& p, const double* pv, int nper, int ninst, con
     if ((r = W.velv.ensure(sizeof(float) * nv * nper)) || (r = W.veln.ensure(sizeof(float) * nc * nper)) ||
         (r = W.inst.ensure(sizeof(FInst) * inst.size())) || (r = W.risti_c.ensure(sizeof(float) * g.nnx)) ||
         (r = W.risti_r.ensure(sizeof(float) * risti_r.size())) ||
-        (r = W.sin_rcx.ensure(sizeof(float) * sin_rcx.size())) || (r = W.wt.ensure(sizeof(float) * nc * slots)) ||
-        (r = W.wn.ensure(sizeof(int) * nc * slots)) || (r = W.wvr.ensure(sizeof(float) * wr * slots)) ||
-        (r = W.wtr.ensure(sizeof(float) * wr * slots)) || (r = W.wnr.ensure(sizeof(int) * wr * slots)) ||
+        (r = W.sin_rcx.ensure(sizeof(float) * sin_rcx.size())) ||
+        (r = W.wnode.ensure(sizeof(Node) * nc * slots)) || (r = W.wrnode.ensure(sizeof(Node) * wr * slots)) ||
+        (r = W.wvr.ensure(sizeof(float) * wr * slots)) ||
         (r = W.wh.ensure(sizeof(HeapE) * (size_t)wh * slots)) || (r = W.ctl.ensure(16)))
         return r;
     FK(cudaMemcpyAsync(W.inst.p, inst.data(), sizeof(FInst) * inst.size(), cudaMemcpyHostToDevice, st));
@@ -126,8 +126,8 @@ int run_fmm(const dazi_fmm_params& p, const double* pv, int nper, int ninst, con
     a.risti_c = W.risti_c.as<float>(); a.risti_r = W.risti_r.as<float>();
     a.rcx = rcx; a.rcz = rcz; a.sin_rcx = W.sin_rcx.as<float>();
     a.times = times; a.ttn_out = ttn;
-    a.w_ttn = W.wt.as<float>(); a.w_nsts = W.wn.as<int>(); a.w_vr = W.wvr.as<float>();
-    a.w_tr = W.wtr.as<float>(); a.w_nr = W.wnr.as<int>(); a.w_heap = W.wh.as<HeapE>();
+    a.w_node = W.wnode.as<Node>(); a.w_rnode = W.wrnode.as<Node>(); a.w_vr = W.wvr.as<float>();
+    a.w_heap = W.wh.as<HeapE>();
     a.wc = nc; a.wr = wr; a.wh = wh;
     a.queue = W.ctl.as<unsigned>(); a.err = W.ctl.as<int>() + 1; a.err_inst = W.ctl.as<int>() + 2;
     fmm_kernel<<<(unsigned)nblk, 32 * kWarpsPerBlock, 0, st>>>(a);

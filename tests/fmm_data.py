@@ -86,6 +86,13 @@ def synthetic(seed, nx=20, ny=24, nper=3, nsrc=12, nrc=15):
             "rc_off": np.array(off, np.int64), "rcx": colat_rad(rx), "rcz": lon_rad(rz)}
 
 
+def big_case():
+    """Two sources on a 1136 x 1136 propagation grid: narrow bands of more
+    than 1,535 nodes, beyond the heap positions a warp keeps in shared
+    memory on the GPU."""
+    return subset(synthetic(5, nx=230, ny=230, nper=1, nsrc=6, nrc=6), np.array([0, 4]))
+
+
 def subset(d, sel):
     """The instances sel of a data set, with their receivers."""
     off = d["rc_off"]

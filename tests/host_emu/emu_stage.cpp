@@ -230,7 +230,9 @@ extern "C" int emu_adjoint_batch(long long ncols, const long long* node_off, con
 // traveltime device code, driven as run_fmm (k_fmm.cu) drives it: the maps'
 // vertex values and coarse grids by the gridding kernels' thread bodies,
 // then per instance the lane-shared steps for lanes 0..31 in turn around
-// lane 0's marching, one workspace slot.  times and, when not NULL, the
+// the marching's phases in the reference's order (travel_seq; the GPU runs
+// the same phases with the four neighbour updates on four lanes), one
+// workspace slot.  times and, when not NULL, the
 // coarse fields ttn (as dazi_fmm_batch).  Returns 0, or the library's error
 // code with *code the instance's error.
 extern "C" int emu_fmm_batch(const dazi_fmm_params* p, const double* pv, int nper, int ninst,
@@ -262,9 +264,11 @@ extern "C" int emu_fmm_batch(const dazi_fmm_params* p, const double* pv, int npe
         blockIdx.x = (unsigned)(t / 256); threadIdx.x = (unsigned)(t % 256);
         fmm_gridder_kernel(velv.data(), g.nvx, g.nvz, p->gdx, p->gdz, nper, veln.data());
     }
-    std::vector<float> wt(nc), wvr(wr), wtr(wr);
-    std::vector<int> wn(nc), wnr(wr), ctl(4, 0);
-    std::vector<HeapE> heap(wh);
+    std::vector<Node> wnode(nc), wrnode(wr);
+    std::vector<float> wvr(wr);
+    std::vector<int> ctl(4, 0);
+    std::vector<HeapE> hglobal(wh), hshared(kHeapShared);
+    const Heap heap{hshared.data(), hglobal.data()};
     FArgs a;
     a.ninst = ninst; a.inst = inst.data();
     a.nnx = g.nnx; a.nnz = g.nnz; a.nvx = g.nvx; a.nvz = g.nvz; a.gdx = p->gdx; a.gdz = p->gdz;
@@ -273,16 +277,17 @@ extern "C" int emu_fmm_batch(const dazi_fmm_params* p, const double* pv, int npe
     a.earth = p->earth; a.dpl = g.dpl;
     a.velv = velv.data(); a.veln = veln.data(); a.risti_c = risti_c.data(); a.risti_r = risti_r.data();
     a.rcx = rcx; a.rcz = rcz; a.sin_rcx = sin_rcx.data(); a.times = times; a.ttn_out = ttn;
-    a.w_ttn = wt.data(); a.w_nsts = wn.data(); a.w_vr = wvr.data(); a.w_tr = wtr.data();
-    a.w_nr = wnr.data(); a.w_heap = heap.data(); a.wc = nc; a.wr = wr; a.wh = wh;
+    a.w_node = wnode.data(); a.w_rnode = wrnode.data(); a.w_vr = wvr.data();
+    a.w_heap = hglobal.data(); a.wc = nc; a.wr = wr; a.wh = wh;
     a.queue = nullptr; a.err = &ctl[1]; a.err_inst = &ctl[2];
     for (int s = 0; s < ninst; ++s) {
         const FInst& I = inst[s];
         FField C, R;
         inst_fields(a, I, 0, C, R);
+        const Box B = inst_box(I);
         for (int lane = 0; lane < 32; ++lane) step_init(a, I, C, R, lane, 32);
         if (p->asgr) {
-            if ((r = travel(R, 1, I.scx, I.scz, I.vnl, I.vnr, I.vnt, I.vnb, heap.data(), I.cap))) {
+            if ((r = travel_seq(R, 1, I.scx, I.scz, B, heap, I.cap))) {
                 *code = r;
                 return -1;
             }
@@ -292,9 +297,9 @@ extern "C" int emu_fmm_batch(const dazi_fmm_params* p, const double* pv, int npe
                 for (int lane = 0; lane < 32; ++lane) mask[lane] = step_band_decide(a, I, C, base, lane, 32);
                 for (int lane = 0; lane < 32; ++lane) step_band_write(a, I, C, base, lane, 32, mask[lane]);
             }
-            r = travel(C, 2, I.scx, I.scz, I.vnl, I.vnr, I.vnt, I.vnb, heap.data(), I.cap);
+            r = travel_seq(C, 2, I.scx, I.scz, B, heap, I.cap);
         } else {
-            r = travel(C, 0, I.scx, I.scz, 0, 0, 0, 0, heap.data(), I.cap);
+            r = travel_seq(C, 0, I.scx, I.scz, B, heap, I.cap);
         }
         if (r) { *code = r; return -1; }
         for (int lane = 0; lane < 32; ++lane) step_receivers(a, I, C, s, lane, 32);

@@ -5,7 +5,8 @@ dazi_fmm_times) against the oracle (oracle/fmm_oracle.c):
   maps' resolution of the reference run's own forward times (2.5e-3 s);
   the coarse fields of every 25th instance bit-identical;
 - seeded synthetic data sets reaching the solver's branches, with and
-  without source-grid refinement and with both upwind schemes;
+  without source-grid refinement and with both upwind schemes, and a large
+  grid whose narrow bands outgrow the shared-memory part of the heap;
 - the device-pointer entry equals the host entry, and the Fortran-shaped
   entry (the reference's source and receiver tables) equals the batch;
 - a source outside the grid, a narrow band beyond its capacity and a source
@@ -58,6 +59,15 @@ def test_synthetic_bit_identical(oracle, seed, kw):
     P = oracle.fmm_params(d["nx"], d["ny"], d["goxd"], d["gozd"], d["dvxd"], d["dvzd"], **kw)
     t0, f0 = oracle.fmm_batch(P, *fmm_data.args(d), fields=True)
     t1, f1 = fmm.travel_times(_params(d, **kw), *fmm_data.args(d), fields=True)
+    np.testing.assert_array_equal(t1, t0)
+    np.testing.assert_array_equal(f1, f0)
+
+
+def test_large_band_bit_identical(oracle):
+    d = fmm_data.big_case()
+    P = oracle.fmm_params(d["nx"], d["ny"], d["goxd"], d["gozd"], d["dvxd"], d["dvzd"])
+    t0, f0 = oracle.fmm_batch(P, *fmm_data.args(d), fields=True)
+    t1, f1 = fmm.travel_times(_params(d), *fmm_data.args(d), fields=True)
     np.testing.assert_array_equal(t1, t0)
     np.testing.assert_array_equal(f1, f0)
 

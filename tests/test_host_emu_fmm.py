@@ -6,7 +6,9 @@ coarse fields
 - on seeded synthetic data sets that reach the solver's branches (sources
   on nodes and in the corner cells, refined boxes cut by the model's sides,
   receivers in and next to the source's cell), with and without source-grid
-  refinement and with both upwind schemes;
+  refinement and with both upwind schemes,
+- on a large grid whose narrow bands outgrow the heap part the GPU keeps
+  in shared memory;
 and the same error where the reference's field is undefined (a source in the
 last cell before the right side) or a source lies outside the grid.  The
 same code runs on the GPU (tests/test_gpu_fmm.py)."""
@@ -38,6 +40,12 @@ def test_yunnan_subset_bit_identical(oracle):
 def test_synthetic_bit_identical(oracle, seed, kw):
     d = fmm_data.synthetic(seed)
     (t0, f0), (t1, f1) = _both(oracle, d, **kw)
+    np.testing.assert_array_equal(t1, t0)
+    np.testing.assert_array_equal(f1, f0)
+
+
+def test_large_band_bit_identical(oracle):
+    (t0, f0), (t1, f1) = _both(oracle, fmm_data.big_case())
     np.testing.assert_array_equal(t1, t0)
     np.testing.assert_array_equal(f1, f0)
 
