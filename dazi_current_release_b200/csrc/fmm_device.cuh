@@ -347,7 +347,8 @@ __device__ float bilinear(const float nv[2][2], float dsx, float dsz, float dnx,
 //   travel_commit  its band entry (added, or moved up).
 // The reference runs travel_nbr and travel_commit neighbour by neighbour;
 // the new times depend only on alive nodes, which the commits do not
-// change, so the four travel_nbr may also run first (travel_warp).
+// change, so the four travel_nbr may also run first (travel_warp), with
+// each commit reading the node's heap position afresh.
 struct Box {
     int vnl, vnr, vnt, vnb;
 };
@@ -419,16 +420,22 @@ __device__ int travel_nbr(const FField& F, int iz, int ix, int q, int& niz, int&
     return F.fom == 0 ? fouds1(F, S, t) : fouds2(F, S, t);
 }
 
-__device__ int travel_commit(const FField& F, int niz, int nix, int st, float t, const Heap& h, int& ntr, int cap)
+// A close node's status is its heap position, which the commits of the
+// neighbours before it may have moved: it is read here, not taken from
+// travel_nbr (far stays far: the four neighbours are distinct nodes).
+__device__ int travel_commit(const FField& F, int niz, int nix, float t, const Heap& h, int& ntr, int cap)
 {
-    FN(niz, nix).t = t;
+    Node& n = FN(niz, nix);
+    const int st = n.s;
+    n.t = t;
     if (st < 0) return heap_add(F, niz, nix, t, ntr, cap, h);
     heap_update(F, niz, nix, t, st, h);
     return 0;
 }
 
-// The reference's order on one thread.
-__device__ int travel_seq(const FField& F, int urg, float scx, float scz, const Box& B, const Heap& h, int cap)
+// travel_warp's order on one thread (the host build's driver): after each
+// pop the four neighbours' times first, then their commits.
+__device__ int travel_four(const FField& F, int urg, float scx, float scz, const Box& B, const Heap& h, int cap)
 {
     int ntr = 0, r;
     if ((r = travel_start(F, urg, scx, scz, B, h, cap, ntr))) return r;
@@ -437,11 +444,15 @@ __device__ int travel_seq(const FField& F, int urg, float scx, float scz, const 
         if (pops > maxpops) return kErrSteps;
         int ix, iz;
         if (travel_pop(F, urg, B, h, ntr, ix, iz)) break;
+        int niz[4], nix[4], st[4], e[4];
+        float t[4];
         for (int q = 0; q < 4; ++q) {
-            int niz, nix, st;
-            float t = 0.0f;
-            if ((r = travel_nbr(F, iz, ix, q, niz, nix, st, t))) return r;
-            if (st != 0 && (r = travel_commit(F, niz, nix, st, t, h, ntr, cap))) return r;
+            t[q] = 0.0f;
+            e[q] = travel_nbr(F, iz, ix, q, niz[q], nix[q], st[q], t[q]);
+        }
+        for (int q = 0; q < 4; ++q) {
+            if (e[q]) return e[q];
+            if (st[q] != 0 && (r = travel_commit(F, niz[q], nix[q], t[q], h, ntr, cap))) return r;
         }
     }
     return 0;
@@ -481,7 +492,7 @@ __device__ int travel_warp(const FField& F, int urg, float scx, float scz, const
             const float tq = __shfl_sync(all, t, q);
             if (lane == 0 && !r) {
                 if (eq) r = eq;
-                else if (sq != 0) r = travel_commit(F, zq, xq, sq, tq, h, ntr, cap);
+                else if (sq != 0) r = travel_commit(F, zq, xq, tq, h, ntr, cap);
             }
         }
         r = __shfl_sync(all, r, 0);

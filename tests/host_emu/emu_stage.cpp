@@ -230,9 +230,9 @@ extern "C" int emu_adjoint_batch(long long ncols, const long long* node_off, con
 // traveltime device code, driven as run_fmm (k_fmm.cu) drives it: the maps'
 // vertex values and coarse grids by the gridding kernels' thread bodies,
 // then per instance the lane-shared steps for lanes 0..31 in turn around
-// the marching's phases in the reference's order (travel_seq; the GPU runs
-// the same phases with the four neighbour updates on four lanes), one
-// workspace slot.  times and, when not NULL, the
+// the marching's phases in the order the GPU's warps run them
+// (travel_four: after each pop the four neighbours' times, then their
+// commits), one workspace slot.  times and, when not NULL, the
 // coarse fields ttn (as dazi_fmm_batch).  Returns 0, or the library's error
 // code with *code the instance's error.
 extern "C" int emu_fmm_batch(const dazi_fmm_params* p, const double* pv, int nper, int ninst,
@@ -287,7 +287,7 @@ extern "C" int emu_fmm_batch(const dazi_fmm_params* p, const double* pv, int npe
         const Box B = inst_box(I);
         for (int lane = 0; lane < 32; ++lane) step_init(a, I, C, R, lane, 32);
         if (p->asgr) {
-            if ((r = travel_seq(R, 1, I.scx, I.scz, B, heap, I.cap))) {
+            if ((r = travel_four(R, 1, I.scx, I.scz, B, heap, I.cap))) {
                 *code = r;
                 return -1;
             }
@@ -297,9 +297,9 @@ extern "C" int emu_fmm_batch(const dazi_fmm_params* p, const double* pv, int npe
                 for (int lane = 0; lane < 32; ++lane) mask[lane] = step_band_decide(a, I, C, base, lane, 32);
                 for (int lane = 0; lane < 32; ++lane) step_band_write(a, I, C, base, lane, 32, mask[lane]);
             }
-            r = travel_seq(C, 2, I.scx, I.scz, B, heap, I.cap);
+            r = travel_four(C, 2, I.scx, I.scz, B, heap, I.cap);
         } else {
-            r = travel_seq(C, 0, I.scx, I.scz, B, heap, I.cap);
+            r = travel_four(C, 0, I.scx, I.scz, B, heap, I.cap);
         }
         if (r) { *code = r; return -1; }
         for (int lane = 0; lane < 32; ++lane) step_receivers(a, I, C, s, lane, 32);
