@@ -409,8 +409,15 @@ __device__ bool travel_pop(const FField& F, int urg, const Box& B, const Heap& h
 // neighbour q of the popped (iz, ix): st = its status (0: nothing to do)
 __device__ int travel_nbr(const FField& F, int iz, int ix, int q, int& niz, int& nix, int& st, float& t)
 {
-    niz = q < 2 ? iz : iz - 1 + 2 * (q - 2);
-    nix = q < 2 ? ix - 1 + 2 * q : ix;
+    // explicit cases: written as one select per coordinate
+    // (q < 2 ? ix - 1 + 2 q : ix), lanes 0 and 1 of travel_warp got ix + 3
+    // on the GPU (sm_100a, CUDA 12.9), seen with a self-recording build
+    niz = iz;
+    nix = ix;
+    if (q == 0) nix = ix - 1;
+    else if (q == 1) nix = ix + 1;
+    else if (q == 2) niz = iz - 1;
+    else niz = iz + 1;
     st = 0;
     if (nix < 1 || nix > F.nnx || niz < 1 || niz > F.nnz) return 0;
     Stencil S;
