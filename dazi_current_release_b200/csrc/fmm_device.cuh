@@ -111,23 +111,6 @@ __device__ int heap_add(const FField& F, int iz, int ix, float key, int& ntr, in
     return 0;
 }
 
-// updtree_parallel (CalSurfG_parallel.f90:770-803): the node at position
-// pos has the new time key; it moves up while smaller than its parent
-__device__ void heap_update(const FField& F, int iz, int ix, float key, int pos, const Heap& h)
-{
-    int tpc = pos, tpp = tpc / 2;
-    while (tpp > 0) {
-        const HeapE p = h.get(tpp);
-        if (!(key < p.key)) break;
-        h.put(tpc, p);
-        FN(p.pz, p.px).s = tpc;
-        tpc = tpp;
-        tpp = tpc / 2;
-    }
-    h.put(tpc, HeapE{key, (short)ix, (short)iz});
-    FN(iz, ix).s = tpc;
-}
-
 // downtree_parallel (CalSurfG_parallel.f90:686-761): the root has been
 // taken; the last entry moves to the root and down while a child is
 // smaller (the smaller child; the right one only if strictly smaller, as
@@ -344,11 +327,12 @@ __device__ float bilinear(const float nv[2][2], float dsx, float dsz, float dnx,
 //                  right and bottom sides);
 //   travel_nbr     the new time of neighbour q (x-1, x+1, z-1, z+1) of the
 //                  popped node, if it is far or close;
-//   travel_commit  its band entry (added, or moved up).
-// The reference runs travel_nbr and travel_commit neighbour by neighbour;
+//   commit_one     its band entry (added, or moved up: addtree_parallel
+//                  :631-675, updtree_parallel :770-803).
+// The reference runs travel_nbr and commit_one neighbour by neighbour;
 // the new times depend only on alive nodes, which the commits do not
 // change, so the four travel_nbr may also run first (travel_warp), with
-// each commit reading the node's heap position afresh.
+// the commits tracking the heap positions they move (commit_one).
 struct Box {
     int vnl, vnr, vnt, vnb;
 };
@@ -427,16 +411,48 @@ __device__ int travel_nbr(const FField& F, int iz, int ix, int q, int& niz, int&
     return F.fom == 0 ? fouds1(F, S, t) : fouds2(F, S, t);
 }
 
-// A close node's status is its heap position, which the commits of the
-// neighbours before it may have moved: it is read here, not taken from
-// travel_nbr (far stays far: the four neighbours are distinct nodes).
-__device__ int travel_commit(const FField& F, int niz, int nix, float t, const Heap& h, int& ntr, int cap)
+// The commits of one pop's four neighbours, in order.  A close node's
+// status is its heap position, and an earlier commit's sift-up may move a
+// later neighbour (a parent moving down): the positions st[] are updated
+// as entries move, so no status is read back from memory (far stays far:
+// the four neighbours are distinct nodes).
+struct Pending {
+    int z[4], x[4], st[4];
+    float t[4];
+};
+
+__device__ __forceinline__ void track_move(Pending& P, int from_q, const HeapE& e, int pos)
 {
-    Node& n = FN(niz, nix);
-    const int st = n.s;
-    n.t = t;
-    if (st < 0) return heap_add(F, niz, nix, t, ntr, cap, h);
-    heap_update(F, niz, nix, t, st, h);
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+        if (r > from_q && P.st[r] > 0 && P.x[r] == e.px && P.z[r] == e.pz) P.st[r] = pos;
+}
+
+__device__ int commit_one(const FField& F, Pending& P, int q, const Heap& h, int& ntr, int cap)
+{
+    const int iz = P.z[q], ix = P.x[q];
+    const float key = P.t[q];
+    FN(iz, ix).t = key;
+    int tpc;
+    if (P.st[q] < 0) {          // addtree_parallel: enters at the bottom
+        if (ntr >= cap) return kErrBand;
+        ntr += 1;
+        tpc = ntr;
+    } else {                    // updtree_parallel: from its position
+        tpc = P.st[q];
+    }
+    int tpp = tpc / 2;
+    while (tpp > 0) {
+        const HeapE p = h.get(tpp);
+        if (!(key < p.key)) break;
+        h.put(tpc, p);
+        FN(p.pz, p.px).s = tpc;
+        track_move(P, q, p, tpc);
+        tpc = tpp;
+        tpp = tpc / 2;
+    }
+    h.put(tpc, HeapE{key, (short)ix, (short)iz});
+    FN(iz, ix).s = tpc;
     return 0;
 }
 
@@ -451,15 +467,15 @@ __device__ int travel_four(const FField& F, int urg, float scx, float scz, const
         if (pops > maxpops) return kErrSteps;
         int ix, iz;
         if (travel_pop(F, urg, B, h, ntr, ix, iz)) break;
-        int niz[4], nix[4], st[4], e[4];
-        float t[4];
+        Pending P;
+        int e[4];
         for (int q = 0; q < 4; ++q) {
-            t[q] = 0.0f;
-            e[q] = travel_nbr(F, iz, ix, q, niz[q], nix[q], st[q], t[q]);
+            P.t[q] = 0.0f;
+            e[q] = travel_nbr(F, iz, ix, q, P.z[q], P.x[q], P.st[q], P.t[q]);
         }
         for (int q = 0; q < 4; ++q) {
             if (e[q]) return e[q];
-            if (st[q] != 0 && (r = travel_commit(F, niz[q], nix[q], t[q], h, ntr, cap))) return r;
+            if (P.st[q] != 0 && (r = commit_one(F, P, q, h, ntr, cap))) return r;
         }
     }
     return 0;
@@ -493,13 +509,20 @@ __device__ int travel_warp(const FField& F, int urg, float scx, float scz, const
         float t = 0.0f;
         if (lane < 4) e = travel_nbr(F, iz, ix, lane, niz, nix, st, t);
         __syncwarp();
+        Pending P;
+        int eq[4];
+#pragma unroll
         for (int q = 0; q < 4; ++q) {
-            const int eq = __shfl_sync(all, e, q), sq = __shfl_sync(all, st, q);
-            const int zq = __shfl_sync(all, niz, q), xq = __shfl_sync(all, nix, q);
-            const float tq = __shfl_sync(all, t, q);
-            if (lane == 0 && !r) {
-                if (eq) r = eq;
-                else if (sq != 0) r = travel_commit(F, zq, xq, tq, h, ntr, cap);
+            eq[q] = __shfl_sync(all, e, q);
+            P.st[q] = __shfl_sync(all, st, q);
+            P.z[q] = __shfl_sync(all, niz, q);
+            P.x[q] = __shfl_sync(all, nix, q);
+            P.t[q] = __shfl_sync(all, t, q);
+        }
+        if (lane == 0) {
+            for (int q = 0; q < 4 && !r; ++q) {
+                if (eq[q]) r = eq[q];
+                else if (P.st[q] != 0) r = commit_one(F, P, q, h, ntr, cap);
             }
         }
         r = __shfl_sync(all, r, 0);
