@@ -75,12 +75,14 @@ struct FField {
     float gox, goz, dnx, dnz, earth;
     int fom;
     const float* veln;
+    const float* slow;    // 1 / veln, formed once per node (the reference's slown)
     const float* risti;   // [ix - 1]: earth * sin(gox + (ix - 1) * dnx)
     Node* node;
 };
 
 #define FN(iz, ix) F.node[(long long)((ix) - 1) * F.nnz + ((iz) - 1)]
 #define FV(iz, ix) F.veln[(long long)((ix) - 1) * F.nnz + ((iz) - 1)]
+#define FS(iz, ix) F.slow[(long long)((ix) - 1) * F.nnz + ((iz) - 1)]
 
 // error codes of one instance
 constexpr int kErrOutside = 1;   // source or receiver outside the grid
@@ -138,167 +140,113 @@ __device__ void heap_pop(const FField& F, int& ntr, const Heap& h)
 }
 
 // ------------------------------------------------------------ upwind updates
-__device__ __forceinline__ float quad_root(float a, float b, float c)
+// One quadrant of the upwind update of node (iz, ix): fouds1_parallel
+// (CalSurfG_parallel.f90:346-432) for fom 0, fouds2_parallel (:443-622) for
+// fom 1.  Quadrant (a, b) uses the x-neighbour j = ix - 1 + 2a, the
+// z-neighbour k = iz - 1 + 2b and, for the second-order stencils, the nodes
+// j2, k2 beyond them; it exists where j and k lie in the grid (the
+// reference skips the others).  has: it gives a time (the reference's
+// swsol); trav: that time.  The node's time is the minimum over its
+// quadrants with a time (the reference's travm), which the GPU forms on
+// four lanes at once.
+__device__ void quadrant(const FField& F, int iz, int ix, int a, int b, int& has, float& trav)
 {
-    float rd1 = b * b - 4.0f * a * c;
-    if (rd1 < 0.0f) rd1 = 0.0f;
-    return (-b + sqrtf(rd1)) / (2.0f * a);
-}
-
-// The nodes the upwind update of (iz, ix) reads, loaded together: along x
-// at ix-1, ix+1, ix-2, ix+2 (n[0..3]), along z at iz-1, iz+1, iz-2, iz+2
-// (n[4..7]), each with whether it lies in the grid (indices are clamped
-// into the grid for the load; nodes outside are never used).
-struct Stencil {
-    Node n[8];
-    bool in[8];
-    float slown, risti;
-};
-
-__device__ __forceinline__ void load_stencil(const FField& F, int iz, int ix, Stencil& S)
-{
-    const int d[4] = {-1, 1, -2, 2};
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int j = ix + d[q], k = iz + d[q];
-        S.in[q] = j >= 1 && j <= F.nnx;
-        S.in[4 + q] = k >= 1 && k <= F.nnz;
-        S.n[q] = FN(iz, j < 1 ? 1 : j > F.nnx ? F.nnx : j);
-        S.n[4 + q] = FN(k < 1 ? 1 : k > F.nnz ? F.nnz : k, ix);
-    }
-    S.slown = 1.0f / FV(iz, ix);
-    S.risti = F.risti[ix - 1];
-}
-
-// fouds1_parallel (CalSurfG_parallel.f90:346-432): first-order upwind time
-// from the alive neighbours, the minimum over the four quadrants (a quadrant
-// only where both its neighbours lie in the grid)
-__device__ int fouds1(const FField& F, const Stencil& S, float& out)
-{
-    int tsw1 = 0;
-    float travm = 0.0f;
-    const float slown = S.slown, ri = F.earth, risti = S.risti;
-    for (int a = 0; a < 2; ++a) {
-        for (int b = 0; b < 2; ++b) {
-            const int j = a, k = 4 + b;
-            if (!S.in[j] || !S.in[k]) continue;
-            int swsol = 0;
-            float qa = 1.0f, qb = 0.0f, qc = 0.0f, tref = 0.0f;
-            if (S.n[j].s == 0) {
-                swsol = 1;
-                if (S.n[k].s == 0) {
-                    const float u = ri * F.dnx, v = risti * F.dnz;
-                    const float em = S.n[k].t - S.n[j].t;
-                    qa = u * u + v * v;
-                    qb = -2.0f * (u * u) * em;
-                    qc = (u * u) * (em * em - (v * v) * (slown * slown));
-                } else {
-                    qc = -(slown * slown) * (ri * ri) * (F.dnx * F.dnx);
-                }
-                tref = S.n[j].t;
-            } else if (S.n[k].s == 0) {
-                swsol = 1;
-                const float t = slown * risti * F.dnz;
-                qc = -(t * t);
-                tref = S.n[k].t;
+    has = 0;
+    trav = 0.0f;
+    const int j = ix - 1 + 2 * a, j2 = ix - 2 + 4 * a;
+    const int k = iz - 1 + 2 * b, k2 = iz - 2 + 4 * b;
+    if (j < 1 || j > F.nnx || k < 1 || k > F.nnz) return;
+    const bool inj2 = j2 >= 1 && j2 <= F.nnx, ink2 = k2 >= 1 && k2 <= F.nnz;
+    const Node nj = FN(iz, j), nk = FN(k, ix);
+    const Node nj2 = FN(iz, inj2 ? j2 : j), nk2 = FN(ink2 ? k2 : k, ix);
+    const float slown = FS(iz, ix), ri = F.earth, risti = F.risti[ix - 1];
+    const bool aj = nj.s == 0, ak = nk.s == 0;
+    const float tj = nj.t, tk = nk.t, tj2 = nj2.t, tk2 = nk2.t;
+    float qa = 1.0f, qb = 0.0f, qc = 0.0f, tref = 0.0f;
+    bool third = false;    // tdiv = 3 (second-order operator); else 1
+    if (F.fom == 0) {
+        if (aj) {
+            has = 1;
+            if (ak) {
+                const float u = ri * F.dnx, v = risti * F.dnz;
+                const float em = tk - tj;
+                qa = u * u + v * v;
+                qb = -2.0f * (u * u) * em;
+                qc = (u * u) * (em * em - (v * v) * (slown * slown));
+            } else {
+                qc = -(slown * slown) * (ri * ri) * (F.dnx * F.dnx);
             }
-            if (swsol) {
-                const float trav = tref + quad_root(qa, qb, qc);
-                if (tsw1) travm = fminf(trav, travm);
-                else { travm = trav; tsw1 = 1; }
-            }
+            tref = tj;
+        } else if (ak) {
+            has = 1;
+            const float t = slown * risti * F.dnz;
+            qc = -(t * t);
+            tref = tk;
         }
-    }
-    if (!tsw1) return kErrNoSol;
-    out = travm;
-    return 0;
-}
-
-// fouds2_parallel (CalSurfG_parallel.f90:443-622): mixed-order upwind time
-// (second-order stencils where two alive nodes line up and the time
-// decreases towards the node), the minimum over the four quadrants
-__device__ int fouds2(const FField& F, const Stencil& S, float& out)
-{
-    int tsw1 = 0;
-    float travm = 0.0f;
-    const float slown = S.slown, ri = F.earth, risti = S.risti;
-    for (int a = 0; a < 2; ++a) {
-        const int j = a, j2 = 2 + a;
-        if (!S.in[j]) continue;
-        const bool aj = S.n[j].s == 0;
-        const bool swj = aj && S.in[j2] && S.n[j2].s == 0 && S.n[j].t > S.n[j2].t;
-        const float tj = S.n[j].t, tj2 = S.n[j2].t;
-        for (int b = 0; b < 2; ++b) {
-            const int k = 4 + b, k2 = 6 + b;
-            if (!S.in[k]) continue;
-            const bool ak = S.n[k].s == 0;
-            const bool swk = ak && S.in[k2] && S.n[k2].s == 0 && S.n[k].t > S.n[k2].t;
-            const float tk = S.n[k].t, tk2 = S.n[k2].t;
-            int swsol = 0;
-            float qa = 1.0f, qb = 0.0f, qc = 0.0f, tref = 0.0f, tdiv = 1.0f;
-            if (swj) {
-                swsol = 1;
-                if (swk) {
-                    const float u = 2.0f * ri * F.dnx, v = 2.0f * risti * F.dnz;
-                    float em = 4.0f * tj - tj2 - 4.0f * tk;
-                    em = em + tk2;
-                    qa = v * v + u * u;
-                    qb = 2.0f * em * (u * u);
-                    qc = (u * u) * (em * em - (slown * slown) * (v * v));
-                    tref = 4.0f * tj - tj2;
-                    tdiv = 3.0f;
-                } else if (ak) {
-                    const float u = risti * F.dnz, v = 2.0f * ri * F.dnx;
-                    const float em = 3.0f * tk - 4.0f * tj + tj2;
-                    qa = v * v + 9.0f * (u * u);
-                    qb = 6.0f * em * (u * u);
-                    qc = (u * u) * (em * em - (slown * slown) * (v * v));
-                    tref = tk;
-                } else {
-                    const float u = 2.0f * ri * F.dnx;
-                    qc = -(u * u) * (slown * slown);
-                    tref = 4.0f * tj - tj2;
-                    tdiv = 3.0f;
-                }
-            } else if (aj) {
-                swsol = 1;
-                if (swk) {
-                    const float u = ri * F.dnx, v = 2.0f * risti * F.dnz;
-                    const float em = 3.0f * tj - 4.0f * tk + tk2;
-                    qa = v * v + 9.0f * (u * u);
-                    qb = 6.0f * em * (u * u);
-                    qc = (u * u) * (em * em - (v * v) * (slown * slown));
-                } else if (ak) {
-                    const float u = ri * F.dnx, v = risti * F.dnz;
-                    const float em = tk - tj;
-                    qa = u * u + v * v;
-                    qb = -2.0f * (u * u) * em;
-                    qc = (u * u) * (em * em - (v * v) * (slown * slown));
-                } else {
-                    qc = -(slown * slown) * (ri * ri) * (F.dnx * F.dnx);
-                }
-                tref = tj;
-            } else if (swk) {
-                swsol = 1;
-                const float u = 2.0f * risti * F.dnz;
-                qc = -(u * u) * (slown * slown);
-                tref = 4.0f * tk - tk2;
-                tdiv = 3.0f;
+    } else {
+        const bool swj = aj && inj2 && nj2.s == 0 && tj > tj2;
+        const bool swk = ak && ink2 && nk2.s == 0 && tk > tk2;
+        if (swj) {
+            has = 1;
+            if (swk) {
+                const float u = 2.0f * ri * F.dnx, v = 2.0f * risti * F.dnz;
+                float em = 4.0f * tj - tj2 - 4.0f * tk;
+                em = em + tk2;
+                qa = v * v + u * u;
+                qb = 2.0f * em * (u * u);
+                qc = (u * u) * (em * em - (slown * slown) * (v * v));
+                tref = 4.0f * tj - tj2;
+                third = true;
             } else if (ak) {
-                swsol = 1;
-                qc = -(slown * slown) * (risti * risti) * (F.dnz * F.dnz);
+                const float u = risti * F.dnz, v = 2.0f * ri * F.dnx;
+                const float em = 3.0f * tk - 4.0f * tj + tj2;
+                qa = v * v + 9.0f * (u * u);
+                qb = 6.0f * em * (u * u);
+                qc = (u * u) * (em * em - (slown * slown) * (v * v));
                 tref = tk;
+            } else {
+                const float u = 2.0f * ri * F.dnx;
+                qc = -(u * u) * (slown * slown);
+                tref = 4.0f * tj - tj2;
+                third = true;
             }
-            if (swsol) {
-                const float trav = (tref + quad_root(qa, qb, qc)) / tdiv;
-                if (tsw1) travm = fminf(trav, travm);
-                else { travm = trav; tsw1 = 1; }
+        } else if (aj) {
+            has = 1;
+            if (swk) {
+                const float u = ri * F.dnx, v = 2.0f * risti * F.dnz;
+                const float em = 3.0f * tj - 4.0f * tk + tk2;
+                qa = v * v + 9.0f * (u * u);
+                qb = 6.0f * em * (u * u);
+                qc = (u * u) * (em * em - (v * v) * (slown * slown));
+            } else if (ak) {
+                const float u = ri * F.dnx, v = risti * F.dnz;
+                const float em = tk - tj;
+                qa = u * u + v * v;
+                qb = -2.0f * (u * u) * em;
+                qc = (u * u) * (em * em - (v * v) * (slown * slown));
+            } else {
+                qc = -(slown * slown) * (ri * ri) * (F.dnx * F.dnx);
             }
+            tref = tj;
+        } else if (swk) {
+            has = 1;
+            const float u = 2.0f * risti * F.dnz;
+            qc = -(u * u) * (slown * slown);
+            tref = 4.0f * tk - tk2;
+            third = true;
+        } else if (ak) {
+            has = 1;
+            qc = -(slown * slown) * (risti * risti) * (F.dnz * F.dnz);
+            tref = tk;
         }
     }
-    if (!tsw1) return kErrNoSol;
-    out = travm;
-    return 0;
+    if (!has) return;
+    // the positive root of qa t^2 + qb t + qc (the reference's rd1, tdsh);
+    // trav = (tref + tdsh) / tdiv, and x / 1 = x exactly
+    float rd1 = qb * qb - 4.0f * qa * qc;
+    if (rd1 < 0.0f) rd1 = 0.0f;
+    const float tdsh = (-qb + sqrtf(rd1)) / (2.0f * qa);
+    trav = third ? (tref + tdsh) / 3.0f : tref + tdsh;
 }
 
 // bilinear_parallel (CalSurfG_parallel.f90:2543-2566); nv[i][j] = nv(i+1, j+1)
@@ -390,25 +338,44 @@ __device__ bool travel_pop(const FField& F, int urg, const Box& B, const Heap& h
     return false;
 }
 
-// neighbour q of the popped (iz, ix): st = its status (0: nothing to do)
-__device__ int travel_nbr(const FField& F, int iz, int ix, int q, int& niz, int& nix, int& st, float& t)
+// Neighbour q (x-1, x+1, z-1, z+1) of the popped (iz, ix), as explicit
+// cases: written as one select per coordinate (q < 2 ? ix - 1 + 2 q : ix),
+// lanes 0 and 1 of the warp got ix + 3 on the GPU (sm_100a, CUDA 12.9),
+// seen with a self-recording build.
+__device__ __forceinline__ bool nbr_of(const FField& F, int iz, int ix, int q, int& niz, int& nix)
 {
-    // explicit cases: written as one select per coordinate
-    // (q < 2 ? ix - 1 + 2 q : ix), lanes 0 and 1 of travel_warp got ix + 3
-    // on the GPU (sm_100a, CUDA 12.9), seen with a self-recording build
     niz = iz;
     nix = ix;
     if (q == 0) nix = ix - 1;
     else if (q == 1) nix = ix + 1;
     else if (q == 2) niz = iz - 1;
     else niz = iz + 1;
+    return nix >= 1 && nix <= F.nnx && niz >= 1 && niz <= F.nnz;
+}
+
+// Neighbour q's status st (0: alive or outside the grid, nothing to do)
+// and, otherwise, its new time: the minimum over its quadrants.
+__device__ int travel_nbr(const FField& F, int iz, int ix, int q, int& niz, int& nix, int& st, float& t)
+{
     st = 0;
-    if (nix < 1 || nix > F.nnx || niz < 1 || niz > F.nnz) return 0;
-    Stencil S;
-    load_stencil(F, niz, nix, S);
+    if (!nbr_of(F, iz, ix, q, niz, nix)) return 0;
     st = FN(niz, nix).s;
     if (st == 0) return 0;
-    return F.fom == 0 ? fouds1(F, S, t) : fouds2(F, S, t);
+    int any = 0;
+    float m = 0.0f;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            int has;
+            float tr;
+            quadrant(F, niz, nix, a, b, has, tr);
+            if (has) {
+                m = any ? fminf(tr, m) : tr;
+                any = 1;
+            }
+        }
+    if (!any) return kErrNoSol;
+    t = m;
+    return 0;
 }
 
 // The commits of one pop's four neighbours, in order.  A close node's
@@ -481,8 +448,9 @@ __device__ int travel_four(const FField& F, int urg, float scx, float scz, const
     return 0;
 }
 
-// On a warp: lane 0 keeps the band; lanes 0..3 form the four neighbours'
-// times at once after each pop.
+// On a warp: lane 0 keeps the band; after each pop lanes 0..15 form the
+// four neighbours' quadrant times at once (lane 4q + 2a + b: quadrant (a, b)
+// of neighbour q) and each group of four takes its minimum.
 __device__ int travel_warp(const FField& F, int urg, float scx, float scz, const Box& B, const Heap& h, int cap,
                            int lane)
 {
@@ -505,19 +473,31 @@ __device__ int travel_warp(const FField& F, int urg, float scx, float scz, const
         if (code < 4) return code == 3 ? kErrSteps : 0;
         const int ix = (code - 4) >> 16, iz = (code - 4) & 0xffff;
         __syncwarp();
-        int niz = 0, nix = 0, st = 0, e = 0;
-        float t = 0.0f;
-        if (lane < 4) e = travel_nbr(F, iz, ix, lane, niz, nix, st, t);
+        // lane 4q + 2a + b: quadrant (a, b) of neighbour q
+        int niz = 0, nix = 0, st = 0, has = 0;
+        float tr = 0.0f;
+        if (lane < 16 && nbr_of(F, iz, ix, lane >> 2, niz, nix)) {
+            st = FN(niz, nix).s;
+            if (st != 0) quadrant(F, niz, nix, (lane >> 1) & 1, lane & 1, has, tr);
+        }
+        // minimum over the quadrants with a time, within each group of four
+        float m = has ? tr : __int_as_float(0x7f800000);
+#pragma unroll
+        for (int o = 1; o <= 2; o <<= 1) {
+            m = fminf(m, __shfl_xor_sync(all, m, o));
+            has |= __shfl_xor_sync(all, has, o);
+        }
+        const int e = (st != 0 && !has) ? kErrNoSol : 0;
         __syncwarp();
         Pending P;
         int eq[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            eq[q] = __shfl_sync(all, e, q);
-            P.st[q] = __shfl_sync(all, st, q);
-            P.z[q] = __shfl_sync(all, niz, q);
-            P.x[q] = __shfl_sync(all, nix, q);
-            P.t[q] = __shfl_sync(all, t, q);
+            eq[q] = __shfl_sync(all, e, 4 * q);
+            P.st[q] = __shfl_sync(all, st, 4 * q);
+            P.z[q] = __shfl_sync(all, niz, 4 * q);
+            P.x[q] = __shfl_sync(all, nix, 4 * q);
+            P.t[q] = __shfl_sync(all, m, 4 * q);
         }
         if (lane == 0) {
             for (int q = 0; q < 4 && !r; ++q) {
@@ -566,7 +546,8 @@ __device__ float bspline_node(const float* velv, int nvx, int nvz, int ncz, int 
 }
 
 // velv of every period map (real(pv), gridder_parallel :842-849) and the
-// coarse grid's velocities veln, one thread per value
+// coarse grid's velocities veln and slownesses 1 / veln, one thread per
+// value
 __global__ void fmm_velv_kernel(const double* pv, int nx, int ny, int nper, float* velv)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -578,7 +559,7 @@ __global__ void fmm_velv_kernel(const double* pv, int nx, int ny, int nper, floa
 }
 
 __global__ void fmm_gridder_kernel(const float* velv, int nvx, int nvz, int gdx, int gdz, int nper,
-                                   float* veln)
+                                   float* veln, float* slow)
 {
     const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     const int nnx = (nvx - 1) * gdx + 1, nnz = (nvz - 1) * gdz + 1;
@@ -586,7 +567,9 @@ __global__ void fmm_gridder_kernel(const float* velv, int nvx, int nvz, int gdx,
     if (t >= nn * nper) return;
     const long long p = t / nn, r = t % nn;
     const int stx = (int)(r / nnz) + 1, stz = (int)(r % nnz) + 1;
-    veln[t] = bspline_node(velv + p * (long long)(nvx + 2) * (nvz + 2), nvx, nvz, gdz, gdx, stz, stx);
+    const float v = bspline_node(velv + p * (long long)(nvx + 2) * (nvz + 2), nvx, nvz, gdz, gdx, stz, stx);
+    veln[t] = v;
+    slow[t] = 1.0f / v;
 }
 
 // ------------------------------------------------------------ instances
@@ -609,6 +592,7 @@ struct FArgs {
     float gox, goz, dnx, dnz, drnx, drnz, earth, dpl;
     const float* velv;          // [period][(nvx + 2) * (nvz + 2)]
     const float* veln;          // [period][nnx * nnz]
+    const float* slow;          // [period][nnx * nnz]: 1 / veln
     const float* risti_c;       // [nnx]
     const float* risti_r;
     const float* rcx;
@@ -620,6 +604,7 @@ struct FArgs {
     Node* w_node;               // coarse field
     Node* w_rnode;              // refined field
     float* w_vr;                // refined velocities
+    float* w_sr;                // refined slownesses
     HeapE* w_heap;              // heap positions >= kHeapShared
     long long wc, wr, wh;       // slot sizes: coarse nodes, refined nodes, heap positions
     unsigned* queue;
@@ -691,12 +676,14 @@ __device__ void inst_fields(const FArgs& a, const FInst& I, long long slot, FFie
     C.nnx = a.nnx; C.nnz = a.nnz;
     C.gox = a.gox; C.goz = a.goz; C.dnx = a.dnx; C.dnz = a.dnz; C.earth = a.earth; C.fom = a.fom;
     C.veln = a.veln + (long long)I.period * a.nnx * a.nnz;
+    C.slow = a.slow + (long long)I.period * a.nnx * a.nnz;
     C.risti = a.risti_c;
     C.node = a.w_node + slot * a.wc;
     R.nnx = I.nrnx; R.nnz = I.nrnz;
     R.gox = I.gorx; R.goz = I.gorz; R.dnx = a.drnx; R.dnz = a.drnz; R.earth = a.earth; R.fom = a.fom;
     R.risti = a.risti_r + I.risti_r;
     R.veln = a.w_vr + slot * a.wr;
+    R.slow = a.w_sr + slot * a.wr;
     R.node = a.w_rnode + slot * a.wr;
 }
 
@@ -712,10 +699,13 @@ __device__ void step_init(const FArgs& a, const FInst& I, const FField& C, const
         const int origx = (I.vnl - 1) * a.sgdl + 1, origz = (I.vnt - 1) * a.sgdl + 1;
         const float* velv = a.velv + (long long)I.period * (a.nvx + 2) * (a.nvz + 2);
         float* vr = const_cast<float*>(R.veln);
+        float* sr = const_cast<float*>(R.slow);
         for (long long q = lane; q < nr; q += nl) {
             const int idm2 = (int)(q / I.nrnz) + 1, idm1 = (int)(q % I.nrnz) + 1;
-            vr[q] = bspline_node(velv, a.nvx, a.nvz, a.gdz * a.sgdl, a.gdx * a.sgdl, origz + idm1 - 1,
-                                 origx + idm2 - 1);
+            const float v = bspline_node(velv, a.nvx, a.nvz, a.gdz * a.sgdl, a.gdx * a.sgdl,
+                                         origz + idm1 - 1, origx + idm2 - 1);
+            vr[q] = v;
+            sr[q] = 1.0f / v;
             R.node[q].s = -1;
         }
     }

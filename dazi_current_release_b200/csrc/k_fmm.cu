@@ -56,7 +56,7 @@ struct FBuf {
 };
 
 struct FWork {
-    FBuf velv, veln, inst, risti_c, risti_r, sin_rcx, wnode, wrnode, wvr, wh, ctl;
+    FBuf velv, veln, slow, inst, risti_c, risti_r, sin_rcx, wnode, wrnode, wvr, wsr, wh, ctl;
     FBuf pv, rcx, rcz, times, ttn, scx, scz, per, off;   // copies of host inputs
 };
 
@@ -98,11 +98,12 @@ int run_fmm(const dazi_fmm_params& p, const double* pv, int nper, int ninst, con
     const long long nc = (long long)g.nnx * g.nnz;
     const long long nv = (long long)p.nx * p.ny;
     if ((r = W.velv.ensure(sizeof(float) * nv * nper)) || (r = W.veln.ensure(sizeof(float) * nc * nper)) ||
+        (r = W.slow.ensure(sizeof(float) * nc * nper)) ||
         (r = W.inst.ensure(sizeof(FInst) * inst.size())) || (r = W.risti_c.ensure(sizeof(float) * g.nnx)) ||
         (r = W.risti_r.ensure(sizeof(float) * risti_r.size())) ||
         (r = W.sin_rcx.ensure(sizeof(float) * sin_rcx.size())) ||
         (r = W.wnode.ensure(sizeof(Node) * nc * slots)) || (r = W.wrnode.ensure(sizeof(Node) * wr * slots)) ||
-        (r = W.wvr.ensure(sizeof(float) * wr * slots)) ||
+        (r = W.wvr.ensure(sizeof(float) * wr * slots)) || (r = W.wsr.ensure(sizeof(float) * wr * slots)) ||
         (r = W.wh.ensure(sizeof(HeapE) * (size_t)wh * slots)) || (r = W.ctl.ensure(16)))
         return r;
     FK(cudaMemcpyAsync(W.inst.p, inst.data(), sizeof(FInst) * inst.size(), cudaMemcpyHostToDevice, st));
@@ -114,7 +115,8 @@ int run_fmm(const dazi_fmm_params& p, const double* pv, int nper, int ninst, con
     fmm_velv_kernel<<<(unsigned)((nv * nper + bt - 1) / bt), bt, 0, st>>>(pv, p.nx, p.ny, nper, W.velv.as<float>());
     FK(cudaGetLastError());
     fmm_gridder_kernel<<<(unsigned)((nc * nper + bt - 1) / bt), bt, 0, st>>>(W.velv.as<float>(), g.nvx, g.nvz,
-                                                                             p.gdx, p.gdz, nper, W.veln.as<float>());
+                                                                             p.gdx, p.gdz, nper, W.veln.as<float>(),
+                                                                             W.slow.as<float>());
     FK(cudaGetLastError());
     FArgs a;
     a.ninst = ninst; a.inst = W.inst.as<FInst>();
@@ -122,11 +124,11 @@ int run_fmm(const dazi_fmm_params& p, const double* pv, int nper, int ninst, con
     a.sgdl = p.sgdl; a.fom = p.fom; a.asgr = p.asgr;
     a.gox = g.gox; a.goz = g.goz; a.dnx = g.dnx; a.dnz = g.dnz; a.drnx = g.drnx; a.drnz = g.drnz;
     a.earth = p.earth; a.dpl = g.dpl;
-    a.velv = W.velv.as<float>(); a.veln = W.veln.as<float>();
+    a.velv = W.velv.as<float>(); a.veln = W.veln.as<float>(); a.slow = W.slow.as<float>();
     a.risti_c = W.risti_c.as<float>(); a.risti_r = W.risti_r.as<float>();
     a.rcx = rcx; a.rcz = rcz; a.sin_rcx = W.sin_rcx.as<float>();
     a.times = times; a.ttn_out = ttn;
-    a.w_node = W.wnode.as<Node>(); a.w_rnode = W.wrnode.as<Node>(); a.w_vr = W.wvr.as<float>();
+    a.w_node = W.wnode.as<Node>(); a.w_rnode = W.wrnode.as<Node>(); a.w_vr = W.wvr.as<float>(); a.w_sr = W.wsr.as<float>();
     a.w_heap = W.wh.as<HeapE>();
     a.wc = nc; a.wr = wr; a.wh = wh;
     a.queue = W.ctl.as<unsigned>(); a.err = W.ctl.as<int>() + 1; a.err_inst = W.ctl.as<int>() + 2;

@@ -74,5 +74,7 @@ static inline int atomicCAS(int* p, int cmp, int v) { int o = *p; if (o == cmp) 
 static inline void __syncwarp(unsigned = 0xffffffffu) {}
 static inline int atomicOr(int* p, int v) { int o = *p; *p |= v; return o; }
 template <class T> static inline T __shfl_sync(unsigned, T v, int) { return v; }
+template <class T> static inline T __shfl_xor_sync(unsigned, T v, int) { return v; }
+static inline float __int_as_float(int i) { float f; std::memcpy(&f, &i, 4); return f; }
 static inline unsigned __reduce_add_sync(unsigned, unsigned v) { return v; }
 static inline bool __any_sync(unsigned, bool v) { return v; }

@@ -254,7 +254,7 @@ extern "C" int emu_fmm_batch(const dazi_fmm_params* p, const double* pv, int npe
     std::vector<float> risti_c(g.nnx), sin_rcx(nrc > 0 ? nrc : 1);
     for (int ix = 1; ix <= g.nnx; ++ix) risti_c[ix - 1] = p->earth * sinf(g.gox + (float)(ix - 1) * g.dnx);
     for (long long q = 0; q < nrc; ++q) sin_rcx[q] = sinf(rcx[q]);
-    std::vector<float> velv(nv * nper), veln(nc * nper);
+    std::vector<float> velv(nv * nper), veln(nc * nper), slow(nc * nper);
     blockDim.x = 256;
     for (long long t = 0; t < nv * nper; ++t) {
         blockIdx.x = (unsigned)(t / 256); threadIdx.x = (unsigned)(t % 256);
@@ -262,10 +262,10 @@ extern "C" int emu_fmm_batch(const dazi_fmm_params* p, const double* pv, int npe
     }
     for (long long t = 0; t < nc * nper; ++t) {
         blockIdx.x = (unsigned)(t / 256); threadIdx.x = (unsigned)(t % 256);
-        fmm_gridder_kernel(velv.data(), g.nvx, g.nvz, p->gdx, p->gdz, nper, veln.data());
+        fmm_gridder_kernel(velv.data(), g.nvx, g.nvz, p->gdx, p->gdz, nper, veln.data(), slow.data());
     }
     std::vector<Node> wnode(nc), wrnode(wr);
-    std::vector<float> wvr(wr);
+    std::vector<float> wvr(wr), wsr(wr);
     std::vector<int> ctl(4, 0);
     std::vector<HeapE> hglobal(wh), hshared(kHeapShared);
     const Heap heap{hshared.data(), hglobal.data()};
@@ -275,9 +275,9 @@ extern "C" int emu_fmm_batch(const dazi_fmm_params* p, const double* pv, int npe
     a.sgdl = p->sgdl; a.fom = p->fom; a.asgr = p->asgr;
     a.gox = g.gox; a.goz = g.goz; a.dnx = g.dnx; a.dnz = g.dnz; a.drnx = g.drnx; a.drnz = g.drnz;
     a.earth = p->earth; a.dpl = g.dpl;
-    a.velv = velv.data(); a.veln = veln.data(); a.risti_c = risti_c.data(); a.risti_r = risti_r.data();
+    a.velv = velv.data(); a.veln = veln.data(); a.slow = slow.data(); a.risti_c = risti_c.data(); a.risti_r = risti_r.data();
     a.rcx = rcx; a.rcz = rcz; a.sin_rcx = sin_rcx.data(); a.times = times; a.ttn_out = ttn;
-    a.w_node = wnode.data(); a.w_rnode = wrnode.data(); a.w_vr = wvr.data();
+    a.w_node = wnode.data(); a.w_rnode = wrnode.data(); a.w_vr = wvr.data(); a.w_sr = wsr.data();
     a.w_heap = hglobal.data(); a.wc = nc; a.wr = wr; a.wh = wh;
     a.queue = nullptr; a.err = &ctl[1]; a.err_inst = &ctl[2];
     for (int s = 0; s < ninst; ++s) {
