@@ -80,9 +80,10 @@ struct FField {
     Node* node;
 };
 
-#define FN(iz, ix) F.node[(long long)((ix) - 1) * F.nnz + ((iz) - 1)]
-#define FV(iz, ix) F.veln[(long long)((ix) - 1) * F.nnz + ((iz) - 1)]
-#define FS(iz, ix) F.slow[(long long)((ix) - 1) * F.nnz + ((iz) - 1)]
+// (a field has at most 32767 x 32767 nodes: 32-bit offsets)
+#define FN(iz, ix) F.node[((ix) - 1) * F.nnz + ((iz) - 1)]
+#define FV(iz, ix) F.veln[((ix) - 1) * F.nnz + ((iz) - 1)]
+#define FS(iz, ix) F.slow[((ix) - 1) * F.nnz + ((iz) - 1)]
 
 // error codes of one instance
 constexpr int kErrOutside = 1;   // source or receiver outside the grid
@@ -477,8 +478,11 @@ __device__ int travel_warp(const FField& F, int urg, float scx, float scz, const
         int niz = 0, nix = 0, st = 0, has = 0;
         float tr = 0.0f;
         if (lane < 16 && nbr_of(F, iz, ix, lane >> 2, niz, nix)) {
+            // the status and the quadrant's nodes in one round of loads; the
+            // quadrant's time is dropped for an alive neighbour
             st = FN(niz, nix).s;
-            if (st != 0) quadrant(F, niz, nix, (lane >> 1) & 1, lane & 1, has, tr);
+            quadrant(F, niz, nix, (lane >> 1) & 1, lane & 1, has, tr);
+            if (st == 0) has = 0;
         }
         // minimum over the quadrants with a time, within each group of four
         float m = has ? tr : __int_as_float(0x7f800000);
