@@ -89,6 +89,8 @@ def parse():
     p.add_argument("--cpu-sample-s", type=float, default=15.0,
                    help="grid workloads: seconds of CPU work in the cpu_baseline sample")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-fmm", action="store_true",
+                   help="skip the traveltime-solver measurement (fmm block)")
     return p.parse_args()
 
 
@@ -792,11 +794,90 @@ def main_ragged(args, ws, rank, local):
                 "tight_root": "surfdisp96 on the real*4 model converged to 1e-13, rounded to "
                               "float32", "periods_with_root": int(good.sum())}
         line["accuracy"] = acc
+    if rank == 0 and ws == 1 and not args.no_fmm:
+        line["fmm"] = fmm_block(torch, dev, stream, not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
         torch.distributed.barrier()
         torch.distributed.destroy_process_group()
+
+
+def fmm_block(torch, dev, stream, with_cpu):
+    """The traveltime solver on the Yunnan example's data set (1,469
+    (period, source) fields, 20,877 receivers; tests/golden/yunnan_fmm.npz)
+    through the initial model's phase-velocity maps (the library's
+    surfdisp96 on tests/golden/yunnan_pv.npz's MOD, all 38 x 42 columns, 36
+    periods): device-resident time (CUDA events, 3 runs after 2 warm-up),
+    the host entry end to end (maps and coordinates copied in, times out),
+    and the oracle on all host threads on the same input, whose times the
+    GPU's must equal bit for bit."""
+    import dazi_current_release_b200 as dk
+    from dazi_current_release_b200 import fmm
+    g = np.load(os.path.join(ROOT, "tests", "golden", "yunnan_fmm.npz"))
+    m = np.load(os.path.join(ROOT, "tests", "golden", "yunnan_pv.npz"))
+    vel, depz, per = m["vel"], m["depz"], m["periods"]
+    nx, ny, nz = vel.shape
+    pv = np.asfortranarray(dk.depthkernel(nx, ny, nz, vel, 2, 0, per.size, per, depz,
+                                          float(m["minthk"]), form=dk.FORM_PLAIN,
+                                          kernels=False)[0], np.float64).reshape(nx * ny, per.size,
+                                                                                  order="F")
+    st = g["station"][g["rc_station"]]
+    inst = g["src_period"].astype(np.int32) - 1
+    scx, scz = fmm.colatitude(g["src_lat"]), fmm.longitude(g["src_lon"])
+    rcx, rcz = fmm.colatitude(st[:, 0]), fmm.longitude(st[:, 1])
+    off = g["rc_off"].astype(np.int64)
+    goxd, gozd, dvxd, dvzd = (float(v) for v in g["grid"])
+    P = fmm.params(nx, ny, goxd, gozd, dvxd, dvzd)
+    host_args = (pv, inst, scx, scz, off, rcx, rcz)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    dargs = (t(pv.T.copy().ravel()), t(inst), t(scx), t(scz), t(off), t(rcx), t(rcz))
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            fmm.travel_times_dev(P, *dargs, stream=stream)
+        stream.synchronize()
+        ms = []
+        for _ in range(3):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            out = fmm.travel_times_dev(P, *dargs, stream=stream)
+            e1.record(stream)
+            stream.synchronize()
+            ms.append(e0.elapsed_time(e1))
+    e2e = []
+    for _ in range(3):
+        t0 = time.perf_counter()
+        times = fmm.travel_times(P, *host_args)
+        e2e.append((time.perf_counter() - t0) * 1e3)
+    assert np.array_equal(times, out.cpu().numpy())
+    ninst, nrc = int(inst.size), int(off[-1])
+    nnx, nnz = fmm.field_shape(P)
+    dev_ms = float(np.median(ms))
+    blk = {"workload": "Yunnan example data set: 1469 (period, source) traveltime fields on the "
+                       f"{nnx} x {nnz} propagation grid with 129 x 129 refined source grids, "
+                       f"{nrc} receiver times, initial-model phase-velocity maps",
+           "instances": ninst, "receivers": nrc,
+           "value": ninst / (dev_ms * 1e-3), "unit": "fields/s", "ms": dev_ms, "ms_runs": ms,
+           "e2e": {"value": ninst / (float(np.median(e2e)) * 1e-3), "unit": "fields/s",
+                   "ms": float(np.median(e2e)),
+                   "h2d_bytes": int(pv.nbytes + 8 * ninst + 8 * (ninst + 1) + 8 * nrc),
+                   "d2h_bytes": int(4 * nrc)},
+           "bound": "latency: each field is one sequential narrow-band march (the reference's "
+                    "heap order), one warp per field, all fields at once",
+           "ns_per_node": dev_ms * 1e6 / (nnx * nnz + 129 * 129)}
+    if with_cpu:
+        from oracle import oracle as O
+        cores = os.cpu_count() or 1
+        PO = O.fmm_params(nx, ny, goxd, gozd, dvxd, dvzd)
+        t0 = time.perf_counter()
+        ref = O.fmm_batch(PO, *host_args, nthreads=cores)
+        cpu_s = time.perf_counter() - t0
+        blk["cpu_baseline"] = {"value": ninst / cpu_s, "unit": "fields/s", "cores": cores,
+                               "kind": "port", "sample": "the whole data set, oracle of "
+                               "CalSurfG_parallel's per-(period, source) loop, one field per "
+                               "thread at a time", "ms": cpu_s * 1e3}
+        blk["times_equal_oracle"] = int(np.count_nonzero(times == ref))
+    return blk
 
 
 def _timed_gather(torch, dev, stream, pv, status, sen, lsen):
