@@ -51,21 +51,35 @@ struct Node {
 };
 
 // heap entry: the node's time (kept equal to its t while it is in the band)
-// and its grid position
+// and its offset in the field's arrays ((ix - 1) * nnz + (iz - 1))
 struct HeapE {
     float key;
-    short px, pz;
+    int idx;
 };
 
-struct Heap {
-    HeapE* sh;   // positions < kHeapShared (shared memory on the GPU)
-    HeapE* gl;   // all positions (global workspace; the low ones unused)
+// The band's heap: positions below kHeapShared in shared memory, the rest in
+// the global workspace.  ShHeap is the fast path for a band that fits in
+// shared memory (the usual case), MixHeap the general one.
+struct ShHeap {
+    HeapE* sh;
+    __device__ __forceinline__ HeapE get(int i) const { return sh[i]; }
+    __device__ __forceinline__ void put(int i, HeapE e) const { sh[i] = e; }
+};
+
+struct MixHeap {
+    HeapE* sh;
+    HeapE* gl;
     __device__ __forceinline__ HeapE get(int i) const { return i < kHeapShared ? sh[i] : gl[i]; }
     __device__ __forceinline__ void put(int i, HeapE e) const
     {
         if (i < kHeapShared) sh[i] = e;
         else gl[i] = e;
     }
+};
+
+struct Heap {
+    HeapE* sh;   // positions < kHeapShared (shared memory on the GPU)
+    HeapE* gl;   // all positions (global workspace; the low ones unused)
 };
 
 // One propagation grid of one instance: node (iz, ix), 1-based, at
@@ -82,6 +96,7 @@ struct FField {
 
 // (a field has at most 32767 x 32767 nodes: 32-bit offsets)
 #define FN(iz, ix) F.node[((ix) - 1) * F.nnz + ((iz) - 1)]
+#define FIDX(iz, ix) (((ix) - 1) * F.nnz + ((iz) - 1))
 #define FV(iz, ix) F.veln[((ix) - 1) * F.nnz + ((iz) - 1)]
 #define FS(iz, ix) F.slow[((ix) - 1) * F.nnz + ((iz) - 1)]
 
@@ -96,21 +111,28 @@ constexpr int kErrNoBand = 5;    // no close node after the refined sweep
 // addtree_parallel (CalSurfG_parallel.f90:631-675): the new node enters at
 // the bottom and moves up while smaller than its parent (parents move down
 // into the hole, as the reference's swaps leave them)
-__device__ int heap_add(const FField& F, int iz, int ix, float key, int& ntr, int cap, const Heap& h)
+template <class H>
+__device__ __forceinline__ void heap_add_in(const FField& F, int idx, float key, int ntr, const H& h)
 {
-    if (ntr >= cap) return kErrBand;
-    ntr += 1;
     int tpc = ntr, tpp = tpc / 2;
     while (tpp > 0) {
         const HeapE p = h.get(tpp);
         if (!(key < p.key)) break;
         h.put(tpc, p);
-        FN(p.pz, p.px).s = tpc;
+        F.node[p.idx].s = tpc;
         tpc = tpp;
         tpp = tpc / 2;
     }
-    h.put(tpc, HeapE{key, (short)ix, (short)iz});
-    FN(iz, ix).s = tpc;
+    h.put(tpc, HeapE{key, idx});
+    F.node[idx].s = tpc;
+}
+
+__device__ int heap_add(const FField& F, int iz, int ix, float key, int& ntr, int cap, const Heap& h)
+{
+    if (ntr >= cap) return kErrBand;
+    ntr += 1;
+    if (ntr < kHeapShared) heap_add_in(F, FIDX(iz, ix), key, ntr, ShHeap{h.sh});
+    else heap_add_in(F, FIDX(iz, ix), key, ntr, MixHeap{h.sh, h.gl});
     return 0;
 }
 
@@ -118,7 +140,8 @@ __device__ int heap_add(const FField& F, int iz, int ix, float key, int& ntr, in
 // taken; the last entry moves to the root and down while a child is
 // smaller (the smaller child; the right one only if strictly smaller, as
 // the reference's rd1 > rd2 selects it)
-__device__ void heap_pop(const FField& F, int& ntr, const Heap& h)
+template <class H>
+__device__ __forceinline__ void heap_pop_in(const FField& F, int& ntr, const H& h)
 {
     if (ntr == 1) { ntr = 0; return; }
     const HeapE last = h.get(ntr);
@@ -132,12 +155,18 @@ __device__ void heap_pop(const FField& F, int& ntr, const Heap& h)
         }
         if (!(c.key < last.key)) break;
         h.put(tpp, c);
-        FN(c.pz, c.px).s = tpp;
+        F.node[c.idx].s = tpp;
         tpp = tpc;
         tpc = 2 * tpp;
     }
     h.put(tpp, last);
-    FN(last.pz, last.px).s = tpp;
+    F.node[last.idx].s = tpp;
+}
+
+__device__ void heap_pop(const FField& F, int& ntr, const Heap& h)
+{
+    if (ntr < kHeapShared) heap_pop_in(F, ntr, ShHeap{h.sh});
+    else heap_pop_in(F, ntr, MixHeap{h.sh, h.gl});
 }
 
 // ------------------------------------------------------------ upwind updates
@@ -328,10 +357,10 @@ __device__ int travel_start(const FField& F, int urg, float scx, float scz, cons
 // returns true when the refined sweep stops (the node is made alive too)
 __device__ bool travel_pop(const FField& F, int urg, const Box& B, const Heap& h, int& ntr, int& ix, int& iz)
 {
-    const HeapE root = h.get(1);
-    ix = root.px;
-    iz = root.pz;
-    FN(iz, ix).s = 0;
+    const HeapE root = h.sh[1];
+    ix = root.idx / F.nnz + 1;
+    iz = root.idx - (ix - 1) * F.nnz + 1;
+    F.node[root.idx].s = 0;
     if (urg == 1 && ((ix == 1 && B.vnl != 1) || (ix == F.nnx && B.vnr != F.nnx) || (iz == 1 && B.vnt != 1) ||
                      (iz == F.nnz && B.vnb != F.nnz)))
         return true;
@@ -389,18 +418,31 @@ struct Pending {
     float t[4];
 };
 
-__device__ __forceinline__ void track_move(Pending& P, int from_q, const HeapE& e, int pos)
+template <class H>
+__device__ __forceinline__ void commit_in(const FField& F, Pending& P, int q, int tpc, const H& h)
 {
+    const int idx = FIDX(P.z[q], P.x[q]);
+    const float key = P.t[q];
+    int tpp = tpc / 2;
+    while (tpp > 0) {
+        const HeapE p = h.get(tpp);
+        if (!(key < p.key)) break;
+        h.put(tpc, p);
+        F.node[p.idx].s = tpc;
+        // a later neighbour moved down: its position follows
 #pragma unroll
-    for (int r = 0; r < 4; ++r)
-        if (r > from_q && P.st[r] > 0 && P.x[r] == e.px && P.z[r] == e.pz) P.st[r] = pos;
+        for (int r = 0; r < 4; ++r)
+            if (r > q && P.st[r] > 0 && FIDX(P.z[r], P.x[r]) == p.idx) P.st[r] = tpc;
+        tpc = tpp;
+        tpp = tpc / 2;
+    }
+    h.put(tpc, HeapE{key, idx});
+    F.node[idx].s = tpc;
 }
 
 __device__ int commit_one(const FField& F, Pending& P, int q, const Heap& h, int& ntr, int cap)
 {
-    const int iz = P.z[q], ix = P.x[q];
-    const float key = P.t[q];
-    FN(iz, ix).t = key;
+    F.node[FIDX(P.z[q], P.x[q])].t = P.t[q];
     int tpc;
     if (P.st[q] < 0) {          // addtree_parallel: enters at the bottom
         if (ntr >= cap) return kErrBand;
@@ -409,18 +451,8 @@ __device__ int commit_one(const FField& F, Pending& P, int q, const Heap& h, int
     } else {                    // updtree_parallel: from its position
         tpc = P.st[q];
     }
-    int tpp = tpc / 2;
-    while (tpp > 0) {
-        const HeapE p = h.get(tpp);
-        if (!(key < p.key)) break;
-        h.put(tpc, p);
-        FN(p.pz, p.px).s = tpc;
-        track_move(P, q, p, tpc);
-        tpc = tpp;
-        tpp = tpc / 2;
-    }
-    h.put(tpc, HeapE{key, (short)ix, (short)iz});
-    FN(iz, ix).s = tpc;
+    if (ntr < kHeapShared) commit_in(F, P, q, tpc, ShHeap{h.sh});
+    else commit_in(F, P, q, tpc, MixHeap{h.sh, h.gl});
     return 0;
 }
 
