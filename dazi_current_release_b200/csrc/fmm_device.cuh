@@ -214,61 +214,51 @@ __device__ void quadrant(const FField& F, int iz, int ix, int a, int b, int& has
             tref = tk;
         }
     } else {
+        // fouds2_parallel's eight cases in one form (the lanes of a warp sit
+        // in different cases), with the reference's operation order:
+        //   two neighbours:  qa = P + Q, qb = (c em) R, qc = R (em em - S (s s)),
+        //                    em = ((x1 - x2) - x3) + x4;
+        //   one neighbour:   qa = 1, qb = 0, qc = ((-(s s)) G) H;
+        //   tref = g tA - tB.
+        // Scaling by a power of two and swapping the factors of one product
+        // are exact, so e.g. (-2 u^2) em = (-2 em) u^2 and (-u^2) s^2 =
+        // ((-(s s)) u^2) 1 bit for bit; subtracting or adding 0 is exact.
         const bool swj = aj && inj2 && nj2.s == 0 && tj > tj2;
         const bool swk = ak && ink2 && nk2.s == 0 && tk > tk2;
-        if (swj) {
-            has = 1;
-            if (swk) {
-                const float u = 2.0f * ri * F.dnx, v = 2.0f * risti * F.dnz;
-                float em = 4.0f * tj - tj2 - 4.0f * tk;
-                em = em + tk2;
-                qa = v * v + u * u;
-                qb = 2.0f * em * (u * u);
-                qc = (u * u) * (em * em - (slown * slown) * (v * v));
-                tref = 4.0f * tj - tj2;
-                third = true;
-            } else if (ak) {
-                const float u = risti * F.dnz, v = 2.0f * ri * F.dnx;
-                const float em = 3.0f * tk - 4.0f * tj + tj2;
-                qa = v * v + 9.0f * (u * u);
-                qb = 6.0f * em * (u * u);
-                qc = (u * u) * (em * em - (slown * slown) * (v * v));
-                tref = tk;
-            } else {
-                const float u = 2.0f * ri * F.dnx;
-                qc = -(u * u) * (slown * slown);
-                tref = 4.0f * tj - tj2;
-                third = true;
-            }
-        } else if (aj) {
-            has = 1;
-            if (swk) {
-                const float u = ri * F.dnx, v = 2.0f * risti * F.dnz;
-                const float em = 3.0f * tj - 4.0f * tk + tk2;
-                qa = v * v + 9.0f * (u * u);
-                qb = 6.0f * em * (u * u);
-                qc = (u * u) * (em * em - (v * v) * (slown * slown));
-            } else if (ak) {
-                const float u = ri * F.dnx, v = risti * F.dnz;
-                const float em = tk - tj;
-                qa = u * u + v * v;
-                qb = -2.0f * (u * u) * em;
-                qc = (u * u) * (em * em - (v * v) * (slown * slown));
-            } else {
-                qc = -(slown * slown) * (ri * ri) * (F.dnx * F.dnx);
-            }
-            tref = tj;
-        } else if (swk) {
-            has = 1;
-            const float u = 2.0f * risti * F.dnz;
-            qc = -(u * u) * (slown * slown);
-            tref = 4.0f * tk - tk2;
-            third = true;
-        } else if (ak) {
-            has = 1;
-            qc = -(slown * slown) * (risti * risti) * (F.dnz * F.dnz);
-            tref = tk;
+        const float u1 = ri * F.dnx, u2 = 2.0f * ri * F.dnx;
+        const float v1 = risti * F.dnz, v2 = 2.0f * risti * F.dnz;
+        const float u1s = u1 * u1, u2s = u2 * u2, v1s = v1 * v1, v2s = v2 * v2;
+        const float ss = slown * slown;
+        const bool two = (swj || aj) && (swk || ak);
+        has = (swj || aj || swk || ak) ? 1 : 0;
+        // two neighbours: (swj, swk) (swj, ak) (aj, swk) (aj, ak)
+        const float P = swj ? (swk ? v2s : u2s) : (swk ? v2s : u1s);
+        const float Q = swj ? (swk ? u2s : 9.0f * v1s) : (swk ? 9.0f * u1s : v1s);
+        const float cc = swj ? (swk ? 2.0f : 6.0f) : (swk ? 6.0f : -2.0f);
+        const float R = swj ? (swk ? u2s : v1s) : u1s;
+        const float S2 = swj ? (swk ? v2s : u2s) : (swk ? v2s : v1s);
+        const float x1 = swj ? (swk ? 4.0f * tj : 3.0f * tk) : (swk ? 3.0f * tj : tk);
+        const float x2 = (swj && swk) ? tj2 : 0.0f;
+        const float x3 = swj ? 4.0f * (swk ? tk : tj) : (swk ? 4.0f * tk : tj);
+        const float x4 = swj ? (swk ? tk2 : tj2) : (swk ? tk2 : 0.0f);
+        // one neighbour: swj, aj, swk, ak alone
+        const float G = swj ? u2s : aj ? ri * ri : swk ? v2s : risti * risti;
+        const float H = swj ? 1.0f : aj ? F.dnx * F.dnx : swk ? 1.0f : F.dnz * F.dnz;
+        if (two) {
+            const float em = ((x1 - x2) - x3) + x4;
+            qa = P + Q;
+            qb = (cc * em) * R;
+            qc = R * (em * em - S2 * ss);
+        } else {
+            qc = (-ss * G) * H;
         }
+        // tref: 4 tj - tj2 (swj), tj (aj), 4 tk - tk2 (swk), tk (ak); with two
+        // neighbours the x side's, but tk for (swj, ak)
+        const bool xside = two ? !(swj && !swk) : (swj || aj);
+        const bool second = two ? (swj && swk) : (swj || (!aj && swk));
+        const float tA = xside ? tj : tk, tB = second ? (xside ? tj2 : tk2) : 0.0f;
+        tref = (second ? 4.0f : 1.0f) * tA - tB;
+        third = second;
     }
     if (!has) return;
     // the positive root of qa t^2 + qb t + qc (the reference's rd1, tdsh);
@@ -414,14 +404,14 @@ __device__ int travel_nbr(const FField& F, int iz, int ix, int q, int& niz, int&
 // as entries move, so no status is read back from memory (far stays far:
 // the four neighbours are distinct nodes).
 struct Pending {
-    int z[4], x[4], st[4];
+    int z[4], x[4], st[4], idx[4];
     float t[4];
 };
 
 template <class H>
 __device__ __forceinline__ void commit_in(const FField& F, Pending& P, int q, int tpc, const H& h)
 {
-    const int idx = FIDX(P.z[q], P.x[q]);
+    const int idx = P.idx[q];
     const float key = P.t[q];
     int tpp = tpc / 2;
     while (tpp > 0) {
@@ -432,7 +422,7 @@ __device__ __forceinline__ void commit_in(const FField& F, Pending& P, int q, in
         // a later neighbour moved down: its position follows
 #pragma unroll
         for (int r = 0; r < 4; ++r)
-            if (r > q && P.st[r] > 0 && FIDX(P.z[r], P.x[r]) == p.idx) P.st[r] = tpc;
+            if (r > q && P.st[r] > 0 && P.idx[r] == p.idx) P.st[r] = tpc;
         tpc = tpp;
         tpp = tpc / 2;
     }
@@ -442,7 +432,7 @@ __device__ __forceinline__ void commit_in(const FField& F, Pending& P, int q, in
 
 __device__ int commit_one(const FField& F, Pending& P, int q, const Heap& h, int& ntr, int cap)
 {
-    F.node[FIDX(P.z[q], P.x[q])].t = P.t[q];
+    F.node[P.idx[q]].t = P.t[q];
     int tpc;
     if (P.st[q] < 0) {          // addtree_parallel: enters at the bottom
         if (ntr >= cap) return kErrBand;
@@ -472,6 +462,7 @@ __device__ int travel_four(const FField& F, int urg, float scx, float scz, const
         for (int q = 0; q < 4; ++q) {
             P.t[q] = 0.0f;
             e[q] = travel_nbr(F, iz, ix, q, P.z[q], P.x[q], P.st[q], P.t[q]);
+            P.idx[q] = FIDX(P.z[q], P.x[q]);
         }
         for (int q = 0; q < 4; ++q) {
             if (e[q]) return e[q];
@@ -534,6 +525,7 @@ __device__ int travel_warp(const FField& F, int urg, float scx, float scz, const
             P.z[q] = __shfl_sync(all, niz, 4 * q);
             P.x[q] = __shfl_sync(all, nix, 4 * q);
             P.t[q] = __shfl_sync(all, m, 4 * q);
+            P.idx[q] = FIDX(P.z[q], P.x[q]);
         }
         if (lane == 0) {
             for (int q = 0; q < 4 && !r; ++q) {
