@@ -541,7 +541,8 @@ def main_ragged(args, ws, rank, local):
                       "same_roots_as_per_call": bool(torch.equal(plan.pv, pv))
                       and bool(torch.equal(plan.status, status))}
         plan.close()
-        launches = 5   # graph kernels per run: table values, root, adjoint, Gc/Gs order, Gc/Gs
+        launches = 6   # graph kernels per run: table values, root, adjoint order, adjoint,
+        #                Gc/Gs order, Gc/Gs
     else:
         with ClockSampler(local) as clk:
             ms_per_step = _events_timed(step_fn(form, ncol), args.steps, args.warmup, dev,

@@ -68,12 +68,12 @@ struct DBuf {
 // task list, the counters and the sweep scratch (the global entries share
 // one; every plan owns one).
 struct Work {
-    DBuf croot, crootb, counters, adjscr, tiscr, tiord;
+    DBuf croot, crootb, counters, adjscr, adjord, tiscr, tiord;
     DBuf keys, keys2, cidx, cidx2, rmaxb, trecs, ttasks, tlbase, ttbase, cubtmp;
     DBuf tflat, tld, tti, tsp, tch, tmeta, ttasklist;
     void release()
     {
-        DBuf* all[] = {&croot, &crootb, &counters, &adjscr, &tiscr, &tiord, &keys, &keys2, &cidx, &cidx2, &rmaxb,
+        DBuf* all[] = {&croot, &crootb, &counters, &adjscr, &adjord, &tiscr, &tiord, &keys, &keys2, &cidx, &cidx2, &rmaxb,
                        &trecs, &ttasks, &tlbase, &ttbase, &cubtmp, &tflat, &tld, &tti, &tsp,
                        &tch, &tmeta, &ttasklist};
         for (DBuf* b : all) b->release();
@@ -425,6 +425,7 @@ int ensure_sweep_scratch(const Tables& T, bool adj, bool ti, long long maxr, con
         if ((r = launch_persistent_grid(adjoint_fn(cfg.adj_minb), nitems, 128, nblk))) return r;
         const size_t scr = sizeof(double) * 6 * (size_t)(maxr > 1 ? maxr - 1 : 1) * (size_t)(nblk * 128);
         if ((r = W.adjscr.ensure(scr))) return r;
+        if ((r = W.adjord.ensure(sizeof(int) * (size_t)nitems))) return r;
     }
     if (ti) {
         long long nblk;
@@ -492,6 +493,16 @@ int run_adjoint(const Tables& T, const double* per, const StageOut& o, long long
     j.sen_vs = o.svs; j.sen_vp = o.svp; j.sen_rho = o.srh;
     j.scratch = W.adjscr.as<double>(); j.scr_layers = maxr > 1 ? maxr - 1 : 1; j.queue = queues;
     j.croot_b = group ? W.crootb.as<double>() : nullptr;
+    if (!love && !group) {
+        // Rayleigh phase velocity: the pairs of each tile by the depth their
+        // sweep reaches (adj_order_kernel)
+        const long long ntiles = (T.ncols + TILE - 1) / TILE;
+        adj_order_kernel<<<(unsigned)ntiles, TI_ORDER_THREADS, 0, st>>>(j, W.adjord.as<int>(), W.ttbase.as<long long>(),
+                                                                      W.ttasks.as<long long>());
+        CK(cudaGetLastError());
+        ++g_ctx.last_launches;
+        j.order = W.adjord.as<int>();
+    }
     if (love && group) adjoint_love_group_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(j);
     else if (group) adjoint_group_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(j);
     else if (love) adjoint_love_kernel<3><<<(unsigned)nblk, 128, 0, st>>>(j);
@@ -1450,7 +1461,7 @@ void dazi_dk_finalize(void)
     if (!g_ctx.ready) return;
     DBuf* all[] = {&g_ctx.vel, &g_ctx.vp, &g_ctx.rho, &g_ctx.per, &g_ctx.depz, &g_ctx.pv,
                    &g_ctx.svs, &g_ctx.svp, &g_ctx.srh, &g_ctx.status, &g_ctx.geo,
-                   &g_ctx.cscratch, &g_ctx.w.croot, &g_ctx.w.crootb, &g_ctx.w.counters, &g_ctx.w.adjscr,
+                   &g_ctx.cscratch, &g_ctx.w.croot, &g_ctx.w.crootb, &g_ctx.w.counters, &g_ctx.w.adjscr, &g_ctx.w.adjord,
                    &g_ctx.w.tiscr, &g_ctx.w.tiord, &g_ctx.lsen, &g_ctx.w.keys, &g_ctx.w.keys2, &g_ctx.w.cidx, &g_ctx.w.cidx2,
                    &g_ctx.w.rmaxb, &g_ctx.w.trecs, &g_ctx.w.ttasks, &g_ctx.w.tlbase, &g_ctx.w.ttbase,
                    &g_ctx.w.cubtmp, &g_ctx.w.tflat, &g_ctx.w.tld, &g_ctx.w.tti, &g_ctx.w.tsp, &g_ctx.w.tch, &g_ctx.w.tmeta,

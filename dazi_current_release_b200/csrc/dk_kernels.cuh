@@ -54,6 +54,9 @@ struct AdjArgs {
     long long scr_layers;   // layer capacity of a warp's scratch block
     unsigned* queue;        // work-queue counter (zeroed before the launch)
     const double* croot_b = nullptr;   // group velocity: roots at t1b (0: none)
+    const int* order = nullptr;        // phase velocity, or nullptr: [task * 32 + lane]
+                                       // (key << 16) | (period * 32 + column lane),
+                                       // written by adj_order_kernel (key: adj_pair_key)
 };
 
 // Doubles per refined layer in each persistent thread's Gc/Gs scratch: the
@@ -175,6 +178,7 @@ template <int MINB> __global__ void ti_kernel(TiArgs a);          // MINB in {2,
 // One block per tile: the order of the tile's (column, period) pairs for
 // ti_kernel's tasks (a.order), by the depth at which each pair's sweep stops.
 __global__ void ti_order_kernel(TiArgs a, const long long* tile_tbase, const long long* tile_tasks);
+__global__ void adj_order_kernel(AdjArgs a, int* order, const long long* tile_tbase, const long long* tile_tasks);
 constexpr int TI_ORDER_THREADS = 256;
 
 __global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);

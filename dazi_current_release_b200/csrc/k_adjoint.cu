@@ -354,9 +354,56 @@ __device__ __forceinline__ double* scr_row(double* scr, int m)
     return scr + (long long)m * 6 * TILE;
 }
 
+// Depth cut of the phase-velocity sweep: below a depth where the shear
+// waves have decayed by E = sum over the layers above of nu_b d, nu_b =
+// sqrt(k^2 - (omega / b)^2) (layers with c < b), the stack's effect on the
+// secular function and its partials is of relative order exp(-2 E); the
+// first layer with E >= kAdjDepthCut above it is taken as the half-space
+// and the ones below are not swept (their partials, of that relative
+// order, are written as zero).
+constexpr double kAdjDepthCut = 16.0;
+
+// Layers the sweep of one (column, period) covers, the last one taken as
+// the half-space: rmax, or m + 1 for the first solid layer m with E >=
+// kAdjDepthCut above it.  lay: the column's flat layers (d, a, b, rho), layer
+// m at lay[m * TILE].
+__device__ __forceinline__ int adj_cut_layers(const float4* lay, int rmax, double omega, double wvno)
+{
+    const double k2 = wvno * wvno;
+    double ex = 0.0;
+    for (int m = 0; m < rmax - 1; ++m) {
+        const float4 L = lay[(long long)m * TILE];
+        if (ex >= kAdjDepthCut && L.z > 0.0f) return m + 1;
+        if (L.z > 0.0f) {
+            const double kb = omega / (double)L.z;
+            const double nb2 = k2 - kb * kb;
+            if (nb2 > 0.0) ex += sqrt(nb2) * (double)L.x;
+        }
+    }
+    return rmax;
+}
+
+// Sort key of the pair (column lane `lane` of tile t, period k): 0 no such
+// pair, 1 no root (the kernels are written as zero), else 1 + the layers
+// its sweep covers (adj_cut_layers, at most NL).
+__device__ __forceinline__ int adj_pair_key(const AdjArgs& a, long long t, int lane, int k)
+{
+    const Tables& T = a.T;
+    const long long s = t * TILE + lane;
+    if (s >= T.ncols) return 0;
+    const ColMeta M = T.meta[s];
+    if (k >= M.K) return 0;
+    const double c0 = a.croot[M.cr_b + (long long)TILE * k];
+    if (!(c0 > 0.0)) return 1;
+    const double omega = TWOPI / a.periods[M.per_b + k];
+    return 1 + adj_cut_layers(T.flat + T.tile_lbase[t] + lane, M.rmax, omega, omega / c0);
+}
+
 // The Rayleigh adjoint of one (column, period): lane `lane` of task `task`
 // (tile, period), with scr the lane's column of its warp's scratch block;
-// phase velocity or (GROUP) the group velocity's two passes.  The second pass stages its node values in
+// phase velocity or (GROUP) the group velocity's two passes.  With a.order
+// set (phase velocity), the lane takes the pair a.order lists at its place
+// and sweeps the layers its key gives (adj_cut_layers).  The second pass stages its node values in
 // scratch rows the top-down sweep has already read (node i is complete only
 // once the sweep is past layer i, since every interval holds a sublayer;
 // i <= nz - 2 < rmax - 1 rows) and the half-space node in registers, then
@@ -367,13 +414,24 @@ __device__ __forceinline__ void adjoint_rayleigh_task(const AdjArgs& a, long lon
     const Tables& T = a.T;
     constexpr long long nslots = TILE;
     const int2 tk = T.tasks[task];
-    const long long s = (long long)tk.x * TILE + lane;
-    const int k = tk.y;
+    // the (column, period) pair: the task's period at column `lane`, or
+    // (phase velocity, a.order set) the pair adj_order_kernel placed here
+    int cl = lane, k = tk.y, key = 0;
+    if (!GROUP && a.order) {
+        const int e = a.order[task * TILE + lane];
+        key = e >> 16;
+        if (key == 0) return;
+        cl = e & 31;
+        k = (e >> 5) & 0x7ff;
+    }
+    const long long s = (long long)tk.x * TILE + cl;
     if (s >= T.ncols) return;
     const ColMeta M = T.meta[s];
     if (k >= M.K) return;
-    const double c0 = a.croot[task * TILE + lane];
+    const double c0 = a.croot[M.cr_b + (long long)TILE * k];
     const int nz = M.nz, rmax = M.rmax;
+    // layers swept, the last taken as the half-space (adj_cut_layers)
+    const int rm = key >= 2 ? key - 1 : rmax;
     double* dvs = a.sen_vs + M.sen_b + T.sen_sk * k;
     double* dvp = a.sen_vp + M.sen_b + T.sen_sk * k;
     double* drh = a.sen_rho + M.sen_b + T.sen_sk * k;
@@ -387,10 +445,10 @@ __device__ __forceinline__ void adjoint_rayleigh_task(const AdjArgs& a, long lon
     GroupPasses gp{};
     int npass = 1;
     if constexpr (GROUP) {
-        gp = group_passes(a.periods[M.per_b + k], c0, a.croot_b[task * TILE + lane]);
+        gp = group_passes(a.periods[M.per_b + k], c0, a.croot_b[M.cr_b + (long long)TILE * k]);
         npass = gp.n;
     }
-    const long long lbase = T.tile_lbase[tk.x] + lane;
+    const long long lbase = T.tile_lbase[tk.x] + cl;
     const float4* lay = T.flat + lbase;            // layer m at lay[m * TILE]
     const ChainRec* chr = T.ch + lbase;
 #pragma unroll 1
@@ -398,7 +456,7 @@ __device__ __forceinline__ void adjoint_rayleigh_task(const AdjArgs& a, long lon
         const bool staged = GROUP && pass > 0;   // second group pass
         double croot = c0;
         if constexpr (GROUP) {
-            croot = pass ? a.croot_b[task * TILE + lane] : c0;
+            croot = pass ? a.croot_b[M.cr_b + (long long)TILE * k] : c0;
             omega = TWOPI / (pass ? gp.per_b : gp.per_a);
             wvno = omega / croot;
         }
@@ -410,10 +468,10 @@ __device__ __forceinline__ void adjoint_rayleigh_task(const AdjArgs& a, long lon
                 dvs[nstride * node] = vs; dvp[nstride * node] = vp; drh[nstride * node] = rh;
             }
         };
-        // ---- 1. bottom-up sweep: store e(m+1) and 1/n_m for m = rmax-2 .. 0
+        // ---- 1. bottom-up sweep: store e(m+1) and 1/n_m for m = rm-2 .. 0
         double e[5];
         {
-            const float4 L = lay[(long long)(rmax - 1) * TILE];
+            const float4 L = lay[(long long)(rm - 1) * TILE];
             const double aa = L.y, bb = L.z;
             const D3 w = mk(wvno);
             const D3 xka = mk(omega / aa), xkb = mk(omega / bb);
@@ -422,7 +480,7 @@ __device__ __forceinline__ void adjoint_rayleigh_task(const AdjArgs& a, long lon
             halfspace_d3(w, xka, xkb, gk, (double)L.w, h);
             for (int q = 0; q < 5; ++q) e[q] = h[q].v;
         }
-        for (int m = rmax - 2; m >= 0; --m) {
+        for (int m = rm - 2; m >= 0; --m) {
             const float4 L = lay[(long long)m * TILE];
             double f[5];
             const double nrm = layer_step_val(L, wvno, omega, e, f);
@@ -439,7 +497,7 @@ __device__ __forceinline__ void adjoint_rayleigh_task(const AdjArgs& a, long lon
         double nxt_vs = 0.0, nxt_vp = 0.0, nxt_rh = 0.0;   // next node (bottom of interval)
         int cur_node = 0;
         int gexp = 0;   // g is kept as gv * 2^gexp
-        for (int m = 0; m <= rmax - 2; ++m) {
+        for (int m = 0; m <= rm - 2; ++m) {
             const ChainRec ch = chr[(long long)m * TILE];
             const int node = ch.node;
             if (node != cur_node) {
@@ -475,10 +533,13 @@ __device__ __forceinline__ void adjoint_rayleigh_task(const AdjArgs& a, long lon
             for (int q = 0; q < 5; ++q) gv[q] = ldexp(gn[q], -ex);
             gexp += ex;
         }
-        // half-space: the remaining contributions go to node nz-1 (together
-        // with the bottom sublayers of interval nz-2 already in nxt_*)
+        // half-space (layer rm - 1).  Without a cut (rm = rmax) its
+        // contributions go to node nz-1, together with the bottom sublayers
+        // of interval nz-2 already in nxt_*.  With a cut, layer rm - 1 is a
+        // sublayer of interval ch.node and is chained to that interval's two
+        // nodes as the layers above it are; the nodes below get zero.
         {
-            const int m = rmax - 1;
+            const int m = rm - 1;
             const float4 L = lay[(long long)m * TILE];
             const ChainRec ch = chr[(long long)m * TILE];
             const double aa = L.y, bb = L.z, rho = L.w;
@@ -500,14 +561,31 @@ __device__ __forceinline__ void adjoint_rayleigh_task(const AdjArgs& a, long lon
             }
             dFdw = fma(s2, sc, dFdw);
             const double tmpm = ch.tmp, rf = (double)ch.rhofac;
-            put(cur_node, acc_vs, acc_vp, acc_rh);
-            nxt_vp = fma(s0 * sc, tmpm, nxt_vp);
-            nxt_vs = fma(s1 * sc, tmpm, nxt_vs);
-            nxt_rh = fma(sr * sc / rho, rf, nxt_rh);
-            if (!staged) {
-                dvs[nstride * (nz - 1)] = nxt_vs;
-                dvp[nstride * (nz - 1)] = nxt_vp;
-                drh[nstride * (nz - 1)] = nxt_rh;
+            if (rm < rmax) {
+                if (ch.node != cur_node) {
+                    put(cur_node, acc_vs, acc_vp, acc_rh);
+                    acc_vs = nxt_vs; acc_vp = nxt_vp; acc_rh = nxt_rh;
+                    nxt_vs = nxt_vp = nxt_rh = 0.0;
+                    cur_node = ch.node;
+                }
+                const double fw = (double)ch.sub * fast_rcp((double)ch.den);
+                const double dFda = s0 * sc, dFdb = s1 * sc, dFdr = sr * sc / rho;
+                acc_vp = fma(dFda * tmpm, 1.0 - fw, acc_vp); nxt_vp = fma(dFda * tmpm, fw, nxt_vp);
+                acc_vs = fma(dFdb * tmpm, 1.0 - fw, acc_vs); nxt_vs = fma(dFdb * tmpm, fw, nxt_vs);
+                acc_rh = fma(dFdr * rf, 1.0 - fw, acc_rh);   nxt_rh = fma(dFdr * rf, fw, nxt_rh);
+                put(cur_node, acc_vs, acc_vp, acc_rh);
+                put(cur_node + 1, nxt_vs, nxt_vp, nxt_rh);
+                for (int i = cur_node + 2; i < nz; ++i) put(i, 0.0, 0.0, 0.0);
+            } else {
+                put(cur_node, acc_vs, acc_vp, acc_rh);
+                nxt_vp = fma(s0 * sc, tmpm, nxt_vp);
+                nxt_vs = fma(s1 * sc, tmpm, nxt_vs);
+                nxt_rh = fma(sr * sc / rho, rf, nxt_rh);
+                if (!staged) {
+                    dvs[nstride * (nz - 1)] = nxt_vs;
+                    dvp[nstride * (nz - 1)] = nxt_vp;
+                    drh[nstride * (nz - 1)] = nxt_rh;
+                }
             }
         }
         // ---- 3. dc/dm = -F_m / F_c = (c / (wvno F_wvno)) F_m
@@ -839,5 +917,40 @@ template __global__ void adjoint_group_kernel<3>(AdjArgs);
 template __global__ void adjoint_kernel<2>(AdjArgs);
 template __global__ void adjoint_kernel<3>(AdjArgs);
 template __global__ void adjoint_kernel<4>(AdjArgs);
+
+// One block per tile: every (column, period) pair's key (adj_pair_key),
+// then a counting sort of the tile's pairs by key into order, so that the
+// 32 lanes of a task sweep to nearly the same depth.  The results do not
+// depend on the order: each pair is computed by one lane alone.
+__global__ void __launch_bounds__(TI_ORDER_THREADS)
+adj_order_kernel(AdjArgs a, int* order, const long long* tile_tbase, const long long* tile_tasks)
+{
+    __shared__ unsigned short key[NP * TILE];
+    __shared__ int hist[NL + 2];
+    const long long t = blockIdx.x;
+    const int np = (int)tile_tasks[t] * TILE;     // tile_tasks <= NP (checked by the table build)
+    for (int i = threadIdx.x; i < NL + 2; i += blockDim.x) hist[i] = 0;
+    __syncthreads();
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        const int kk = adj_pair_key(a, t, p & 31, p >> 5);
+        key[p] = (unsigned short)kk;
+        atomicAdd(&hist[kk], 1);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int run = 0;
+        for (int i = 0; i < NL + 2; ++i) {
+            const int h = hist[i];
+            hist[i] = run;
+            run += h;
+        }
+    }
+    __syncthreads();
+    int* out = order + tile_tbase[t] * TILE;
+    for (int p = threadIdx.x; p < np; p += blockDim.x) {
+        const int kk = key[p];
+        out[atomicAdd(&hist[kk], 1)] = (kk << 16) | p;
+    }
+}
 
 }  // namespace dk

@@ -215,6 +215,20 @@ extern "C" int emu_adjoint_batch(long long ncols, const long long* node_off, con
     j.T = H.T; j.periods = periods; j.croot = croot.data(); j.sen_vs = svs; j.sen_vp = svp;
     j.sen_rho = srh; j.scratch = scratch.data(); j.scr_layers = H.maxr > 1 ? H.maxr - 1 : 1;
     j.queue = nullptr; j.croot_b = group ? crootb.data() : nullptr;
+    // adj_order_kernel (Rayleigh phase velocity): per tile, the pairs in
+    // ascending key order, as for the Gc/Gs sweep
+    std::vector<int> order;
+    if (ifunc == 2 && !group) {
+        order.resize((size_t)H.T.ntasks * TILE);
+        for (long long t = 0; t < (long long)H.ttask.size(); ++t) {
+            const int np = (int)H.ttask[t] * TILE;
+            std::vector<int> pk(np);
+            for (int p = 0; p < np; ++p) pk[p] = (adj_pair_key(j, t, p & 31, p >> 5) << 16) | p;
+            std::stable_sort(pk.begin(), pk.end(), [](int x, int y) { return (x >> 16) < (y >> 16); });
+            std::copy(pk.begin(), pk.end(), order.begin() + H.tbase[t] * TILE);
+        }
+        j.order = order.data();
+    }
     for (long long task = 0; task < H.T.ntasks; ++task)
         for (int lane = 0; lane < TILE; ++lane) {
             double* scr = scratch.data() + lane;

@@ -13,8 +13,10 @@ run_tables drives them, against the oracle on the CPU.
    must be within 3x that (+1e-6) and within 1e-4.
 3. The group fallback (surfdisp96 uses c0 when the second search at t1b
    finds no root, so U = c0): planted by zeroing roots at t1b, the kernels
-   of those entries are the phase adjoint at t1a bit for bit, and every
-   other entry is unchanged."""
+   of those entries are the phase adjoint at t1a (within 1e-10 of the
+   column's largest value: the phase sweep stops at its depth cut, the
+   group sweep passes the whole stack), and every other entry is unchanged
+   bit for bit."""
 import numpy as np
 import pytest
 
@@ -94,5 +96,11 @@ def test_group_fallback_is_the_phase_adjoint_at_t1a(ifunc):
         drop = dropped[b.per_off[c]:b.per_off[c + 1]]
         for q in range(3):
             got = _col(planted[q], sen_off, c, K, nz[c])
-            np.testing.assert_array_equal(got[drop], _col(phase[q], sen_off, c, K, nz[c])[drop])
+            # the phase adjoint sweeps to its depth cut (adj_cut_layers) and
+            # the group passes the whole stack: the cut's own share is of
+            # relative order exp(-32), and the two sweeps, started at
+            # different depths, round differently (a few 1e-12 relative)
+            ref = _col(phase[q], sen_off, c, K, nz[c])[drop]
+            tol = 1.0e-10 * np.abs(ref).max(axis=-1, keepdims=True)
+            np.testing.assert_allclose(got[drop], ref, rtol=0, atol=tol.max() if tol.size else 0)
             np.testing.assert_array_equal(got[~drop], _col(full[q], sen_off, c, K, nz[c])[~drop])
