@@ -451,9 +451,9 @@ def _events_timed(step, steps, warmup, dev, stream, flush, ws):
 
 def _work_constants():
     """FP64 operations and DRAM bytes per unit (root layer evaluation,
-    Gc/Gs layer item), counted by ncu (dadd + dmul + 2 dfma per thread
-    instruction; dram__bytes_read + write) on a 100000-column capture of the
-    uneven batch and divided by its units."""
+    adjoint and Gc/Gs layer item), counted by ncu (dadd + dmul + 2 dfma per
+    thread instruction; dram__bytes_read + write) on captures of the uneven
+    batch (the file names each) and divided by their units."""
     path = os.path.join(ROOT, "profiles", "kernel_work.json")
     try:
         return json.load(open(path))
