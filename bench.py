@@ -91,6 +91,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-fmm", action="store_true",
                    help="skip the traveltime-solver measurement (fmm block)")
+    p.add_argument("--no-lsmr", action="store_true",
+                   help="skip the LSMR solver measurement (lsmr block)")
     return p.parse_args()
 
 
@@ -797,6 +799,8 @@ def main_ragged(args, ws, rank, local):
         line["accuracy"] = acc
     if rank == 0 and ws == 1 and not args.no_fmm:
         line["fmm"] = fmm_block(torch, dev, stream, not args.no_cpu_baseline)
+    if rank == 0 and ws == 1 and not args.no_lsmr:
+        line["lsmr"] = lsmr_block(torch, dev, stream, not args.no_cpu_baseline)
     if rank == 0:
         print(json.dumps(line), flush=True)
     if ws > 1:
@@ -878,6 +882,125 @@ def fmm_block(torch, dev, stream, with_cpu):
                                "CalSurfG_parallel's per-(period, source) loop, one field per "
                                "thread at a time", "ms": cpu_s * 1e3}
         blk["times_equal_oracle"] = int(np.count_nonzero(times == ref))
+    return blk
+
+
+HBM_FALLBACK_GBS = 6650.0    # copy bandwidth of this pool's B200s, used when no measured file exists
+
+
+def _hbm_peak():
+    """(GB/s, source): MEASURED_PEAKS.json's copy bandwidth, else the
+    fallback figure."""
+    try:
+        v = float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["hbm_gbs"])
+        return v, "measured copy bandwidth (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, ValueError, KeyError, TypeError):
+        return HBM_FALLBACK_GBS, "fallback 6.65 TB/s copy bandwidth (no measured file)"
+
+
+def lsmr_block(torch, dev, stream, with_cpu):
+    """The LSMR solver (dazi_lsmr_dev / dazi_lsmr) on a seeded G-like system
+    with the Yunnan example's shape: 20,877 ray rows over the 38 x 42 cells,
+    17 depth layers each (synthetic.g_like_system), plus one smoothing row
+    per parameter; all tolerances 0, so every run takes exactly its
+    iteration count.  Device-resident time with CUDA events (the call
+    includes the CSR build); the marginal time per iteration from runs of
+    ITERS and ITERS / 4 iterations, against the HBM roofline of its
+    algorithmic bytes (both CSR copies, 8 B per non-zero each, the row
+    pointers and the dense vectors); the host entry end to end; SciPy's
+    lsmr (the reference's SciPy backend, oracle/lsmr_ref.py) on one host
+    thread for CPU_ITERS iterations; and the first 10 iterations against
+    SciPy's."""
+    from dazi_current_release_b200 import _lib
+    from dazi_current_release_b200.lsmr import lsmr
+    from dazi_current_release_b200.synthetic import g_like_system
+    ITERS, CPU_ITERS = 400, 100
+    row, col, val, b, m, n = g_like_system(nvx=38, nvz=42, nz=17, nrays=20877, seed=0)
+    nnz = int(val.size)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
+    drow, dcol, dval, db = t(row), t(col), t(val), t(b)
+    kw = dict(atol=0.0, btol=0.0, conlim=0.0)
+
+    def run(iters):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = lsmr(drow, dcol, dval, db, m, n, maxiter=iters, stream=stream.cuda_stream, **kw)
+        e1.record(stream)
+        stream.synchronize()
+        assert (r.istop, r.itn) == (7, iters)
+        return e0.elapsed_time(e1), r
+
+    with torch.cuda.stream(stream):
+        for _ in range(2):
+            run(ITERS)
+        full = [run(ITERS)[0] for _ in range(3)]
+        part = [run(ITERS // 4)[0] for _ in range(3)]
+        _, r10 = run(10)
+        _, rk = run(ITERS)
+    ms_full, ms_part = float(np.median(full)), float(np.median(part))
+    it_ms = (ms_full - ms_part) / (ITERS - ITERS // 4)
+    # algorithmic bytes of one iteration: A v and A^T u (values 4 B + column
+    # 4 B per non-zero, 8 B row pointers, the result read and written, the
+    # gathered vector once), the vector update (h, h-bar, x, v read; h,
+    # h-bar, x written)
+    it_bytes = 2 * 8 * nnz + 8 * (m + 1) + 8 * (n + 1) + 8 * (3 * m + n) + 8 * (3 * n + m) + 8 * 7 * n
+    peak, peak_src = _hbm_peak()
+    # host entry: the Fortran-shaped call (iw = rows then columns, rw,
+    # b in, x out), wall clock
+    L = _lib.load()
+    iw = np.concatenate([row, col]).astype(np.int32)
+    ci, cl, cd = ctypes.c_int, ctypes.c_longlong, ctypes.c_double
+    P = lambda a, ty: a.ctypes.data_as(ctypes.POINTER(ty))  # noqa: E731
+    xh = np.zeros(n, np.float64)
+    e2e = []
+    for _ in range(3):
+        istop, itn = ci(0), ci(0)
+        outs = [cd(0.0) for _ in range(5)]
+        t0 = time.perf_counter()
+        rc = L.dazi_lsmr(ctypes.byref(ci(m)), ctypes.byref(ci(n)), ctypes.byref(cl(iw.size)),
+                         ctypes.byref(cl(nnz)), P(iw, ci), P(val, ctypes.c_float), P(b, cd),
+                         ctypes.byref(cd(0.0)), ctypes.byref(cd(0.0)), ctypes.byref(cd(0.0)),
+                         ctypes.byref(cd(0.0)), ctypes.byref(ci(ITERS)), ctypes.byref(ci(0)),
+                         ctypes.byref(ci(6)), P(xh, cd), ctypes.byref(istop), ctypes.byref(itn),
+                         *[ctypes.byref(o) for o in outs])
+        e2e.append((time.perf_counter() - t0) * 1e3)
+        _lib.check(rc)
+    assert np.array_equal(xh, rk.x.cpu().numpy())
+    e2e_ms = float(np.median(e2e))
+    blk = {"workload": f"G-like system with the Yunnan example's shape: {m} x {n} ({20877} ray "
+                       f"rows over 38 x 42 cells x 17 layers, plus {n} smoothing rows), "
+                       f"{nnz} non-zeros, real*4 values, all tolerances 0",
+           "m": m, "n": n, "nnz": nnz,
+           "value": ITERS / (ms_full * 1e-3), "unit": "iterations/s",
+           "solve_ms": ms_full, "iterations": ITERS, "solve_ms_runs": full,
+           "ms_per_iteration": it_ms,
+           "e2e": {"value": ITERS / (e2e_ms * 1e-3), "unit": "iterations/s", "ms": e2e_ms,
+                   "h2d_bytes": int(iw.nbytes + val.nbytes + b.nbytes), "d2h_bytes": int(8 * n)},
+           "roofline": {"bound": "hbm", "achieved": it_bytes / (it_ms * 1e-3) / 1e9,
+                        "peak": peak, "unit": "GB/s",
+                        "frac": it_bytes / (it_ms * 1e-3) / 1e9 / peak,
+                        "bytes_per_iteration": it_bytes, "peak_source": peak_src,
+                        "note": "marginal time per iteration, (t(ITERS) - t(ITERS/4)) / "
+                                "(3 ITERS / 4), 6 launches per iteration in 16-iteration CUDA "
+                                "graphs; the two CSR copies (143 MB) are about L2's size. The "
+                                "products are bound by their gathers, not by HBM: each lane "
+                                "reads an 8-byte vector entry from its own cache line (the "
+                                "columns of a ray row and the rays of a cell are scattered), "
+                                "about one L1 wavefront per non-zero"}}
+    if with_cpu:
+        from oracle import lsmr_ref
+        t0 = time.perf_counter()
+        ref = lsmr_ref.lsmr(row, col, val, b, m, n, maxiter=CPU_ITERS, **kw)
+        cpu_s = time.perf_counter() - t0
+        ref10 = lsmr_ref.lsmr(row, col, val, b, m, n, maxiter=10, **kw)
+        x10 = r10.x.cpu().numpy()
+        blk["cpu_baseline"] = {"value": CPU_ITERS / cpu_s, "unit": "iterations/s", "cores": 1,
+                               "kind": "port", "sample": f"{CPU_ITERS} iterations of SciPy's lsmr "
+                               "on the same triplets (coo -> csr, float64), as the reference's "
+                               "SciPy backend runs it; SciPy's sparse products use one thread",
+                               "ms": cpu_s * 1e3, "itn": int(ref[2])}
+        blk["x_rel_diff_vs_scipy_10_iterations"] = float(
+            np.linalg.norm(x10 - ref10[0]) / np.linalg.norm(ref10[0]))
     return blk
 
 

@@ -48,7 +48,7 @@ namespace {
 
 constexpr int kThreads = 256;
 constexpr int kWarps = kThreads / 32;
-constexpr int kRedBlocks = 592;      // fixed grid of the reducing kernels (148 SMs x 4)
+constexpr int kRedBlocks = 1184;     // fixed grid of the reducing kernels (148 SMs x 8)
 constexpr int kChunk = 16;           // iterations per graph launch
 
 // Solver state in device memory (one instance per solve).
@@ -112,8 +112,26 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(Mat M, const double* __r
     double sq = 0.0;
     for (long long r = gw; r < M.nrows; r += nw) {
         const long long a = M.ptr[r], b = M.ptr[r + 1];
+        // the lane's products in the order k = a + lane, + 32, + 64, ...;
+        // four of them in flight at once (the column and value loads, then
+        // the gathers), added in that order
         double acc = 0.0;
-        for (long long k = a + lane; k < b; k += 32) acc += (double)M.val[k] * x[M.idx[k]];
+        for (long long k0 = a + lane; k0 < b; k0 += 4 * 32) {
+            int ix[4];
+            float vv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const long long k = k0 + 32 * j;
+                ix[j] = k < b ? M.idx[k] : -1;
+                vv[j] = k < b ? M.val[k] : 0.0f;
+            }
+            double xv[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) xv[j] = ix[j] >= 0 ? x[ix[j]] : 0.0;
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+                if (ix[j] >= 0) acc += (double)vv[j] * xv[j];
+        }
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
         if (lane == 0) {
             const double yr = xs * acc - (ys != 0.0 ? ys * y[r] : 0.0);
@@ -125,11 +143,15 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(Mat M, const double* __r
     if (threadIdx.x == 0) part[blockIdx.x] = s;
 }
 
-__device__ __forceinline__ double sum_parts(const double* part)
+// The sum of the kRedBlocks partials by one block of kThreads threads, in a
+// fixed order (thread t adds part[t], part[t + kThreads], ...; then
+// block_sum), so that the result does not depend on the run; valid in
+// thread 0.  Every thread of the block must call it.
+__device__ __forceinline__ double sum_parts(const double* part, double* sh)
 {
     double s = 0.0;
-    for (int i = 0; i < kRedBlocks; ++i) s += part[i];
-    return s;
+    for (int i = threadIdx.x; i < kRedBlocks; i += kThreads) s += part[i];
+    return block_sum(s, sh);
 }
 
 __device__ __forceinline__ double sgn(double a) { return a > 0.0 ? 1.0 : (a < 0.0 ? -1.0 : 0.0); }
@@ -171,9 +193,12 @@ __global__ void __launch_bounds__(kThreads) copy_b_kernel(const double* __restri
 }
 
 // beta = ||b||, u = b / beta
-__global__ void init_beta_kernel(State* S, const double* part)
+__global__ void __launch_bounds__(kThreads) init_beta_kernel(State* S, const double* part)
 {
-    const double beta = sqrt(sum_parts(part));
+    __shared__ double sh[kWarps];
+    const double ss = sum_parts(part, sh);
+    if (threadIdx.x != 0) return;
+    const double beta = sqrt(ss);
     S->beta = beta;
     S->normb = beta;
     S->beta_pos = beta > 0.0;
@@ -187,9 +212,12 @@ __global__ void init_beta_kernel(State* S, const double* part)
 
 // alpha = ||A^T u||, v = A^T u / alpha; the starting values of the
 // recurrences; stop at once when ||A^T b|| = 0 (x = 0 solves the problem)
-__global__ void init_alpha_kernel(State* S, const double* part)
+__global__ void __launch_bounds__(kThreads) init_alpha_kernel(State* S, const double* part)
 {
-    const double alpha = S->beta_pos ? sqrt(sum_parts(part)) : 0.0;
+    __shared__ double sh[kWarps];
+    const double ss = sum_parts(part, sh);   // stale partials when beta = 0: not used
+    if (threadIdx.x != 0) return;
+    const double alpha = S->beta_pos ? sqrt(ss) : 0.0;
     S->alpha = alpha;
     S->sv = alpha > 0.0 ? 1.0 / alpha : 1.0;
     S->zetabar = alpha * S->beta;
@@ -220,11 +248,14 @@ __global__ void __launch_bounds__(kThreads) init_vectors_kernel(const double* __
 }
 
 // after u = A v - alpha u: the iteration count, beta
-__global__ void beta_kernel(State* S, const double* part)
+__global__ void __launch_bounds__(kThreads) beta_kernel(State* S, const double* part)
 {
-    if (S->done) return;
+    __shared__ double sh[kWarps];
+    if (S->done) return;   // read by every thread before thread 0 writes anything
+    const double ss = sum_parts(part, sh);
+    if (threadIdx.x != 0) return;
     S->itn += 1;
-    const double beta = sqrt(sum_parts(part));
+    const double beta = sqrt(ss);
     S->beta = beta;
     S->beta_pos = beta > 0.0;
     if (beta > 0.0) S->su = 1.0 / beta;
@@ -232,12 +263,15 @@ __global__ void beta_kernel(State* S, const double* part)
 
 // after v = A^T u - beta v: alpha, the rotations, the coefficients of the
 // vector update and the estimates of ||r||, ||A||, cond(A) and ||A^T r||
-__global__ void rotate_kernel(State* S, const double* part)
+__global__ void __launch_bounds__(kThreads) rotate_kernel(State* S, const double* part)
 {
+    __shared__ double sh[kWarps];
     if (S->done) return;
+    const double ss = sum_parts(part, sh);   // stale partials when beta = 0: not used
+    if (threadIdx.x != 0) return;
     State& T = *S;
     if (T.beta_pos) {
-        const double alpha = sqrt(sum_parts(part));
+        const double alpha = sqrt(ss);
         T.alpha = alpha;
         if (alpha > 0.0) T.sv = 1.0 / alpha;
     }
@@ -319,11 +353,14 @@ __global__ void __launch_bounds__(kThreads) update_kernel(const double* __restri
 }
 
 // ||x|| and the stopping rules (istop 1..7, the paper's order of precedence)
-__global__ void test_kernel(State* S, const double* part)
+__global__ void __launch_bounds__(kThreads) test_kernel(State* S, const double* part)
 {
+    __shared__ double sh[kWarps];
     if (S->done) return;
+    const double ss = sum_parts(part, sh);
+    if (threadIdx.x != 0) return;
     State& T = *S;
-    T.normx = sqrt(sum_parts(part));
+    T.normx = sqrt(ss);
     const double test1 = T.normr / T.normb;
     const double test2 = (T.normA * T.normr) != 0.0 ? T.normar / (T.normA * T.normr) : INFINITY;
     const double test3 = 1.0 / T.condA;
@@ -510,9 +547,9 @@ extern "C" int dazi_lsmr_dev(int m, int n, long long nnz, const int* row, const 
     LK(cudaMemcpyAsync(S, &hs, sizeof(State), cudaMemcpyHostToDevice, st));
     // u = b / ||b||, v = A^T u / ||A^T u||, h = v, h-bar = x = 0
     copy_b_kernel<<<kRedBlocks, kThreads, 0, st>>>(b, u.as<double>(), m, p0);
-    init_beta_kernel<<<1, 1, 0, st>>>(S, p0);
+    init_beta_kernel<<<1, kThreads, 0, st>>>(S, p0);
     spmv_kernel<2><<<kRedBlocks, kThreads, 0, st>>>(At, u.as<double>(), v.as<double>(), p1, S);
-    init_alpha_kernel<<<1, 1, 0, st>>>(S, p1);
+    init_alpha_kernel<<<1, kThreads, 0, st>>>(S, p1);
     init_vectors_kernel<<<kRedBlocks, kThreads, 0, st>>>(v.as<double>(), h.as<double>(),
                                                         hbar.as<double>(), x, n, S);
     LK(cudaGetLastError());
@@ -534,12 +571,12 @@ extern "C" int dazi_lsmr_dev(int m, int n, long long nnz, const int* row, const 
     }
     for (int it = 0; it < kChunk; ++it) {
         spmv_kernel<0><<<kRedBlocks, kThreads, 0, cs>>>(A, v.as<double>(), u.as<double>(), p0, S);
-        beta_kernel<<<1, 1, 0, cs>>>(S, p0);
+        beta_kernel<<<1, kThreads, 0, cs>>>(S, p0);
         spmv_kernel<1><<<kRedBlocks, kThreads, 0, cs>>>(At, u.as<double>(), v.as<double>(), p1, S);
-        rotate_kernel<<<1, 1, 0, cs>>>(S, p1);
+        rotate_kernel<<<1, kThreads, 0, cs>>>(S, p1);
         update_kernel<<<kRedBlocks, kThreads, 0, cs>>>(v.as<double>(), h.as<double>(),
                                                        hbar.as<double>(), x, n, p2, S);
-        test_kernel<<<1, 1, 0, cs>>>(S, p2);
+        test_kernel<<<1, kThreads, 0, cs>>>(S, p2);
     }
     if (cudaStreamEndCapture(cs, &g) != cudaSuccess ||
         cudaGraphInstantiate(&ge, g, 0) != cudaSuccess) {
