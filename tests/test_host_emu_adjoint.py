@@ -4,7 +4,8 @@ run_tables drives them, against the oracle on the CPU.
 
 1. Phase velocity: against the oracle's exact-model central differences
    (double-precision model pipeline, root converged to 1e-13, dln = 1e-4),
-   within 1e-5 rel-L2 per column.
+   within 1e-5 rel-L2 per column, with the Rayleigh sweep's depth cut
+   reached (the deepest node of some pairs is zero).
 2. Group velocity, U = (1/t1a - 1/t1b) / (1/(t1a c0) - 1/(t1b c1)),
    t1a,b = t/(1 -+ h), h = 0.005: against the same differences of the
    oracle's exact-model quotient.  The quotient amplifies root round-off
@@ -50,6 +51,13 @@ def test_phase_adjoint_matches_exact_derivative(oracle, ifunc):
     names = ("vs", "rho") if ifunc == 1 else ("vs", "vp", "rho")
     if ifunc == 1:
         assert np.count_nonzero(sen[1]) == 0
+    else:
+        # the Rayleigh sweep's depth cut is exercised: pairs whose deepest
+        # node, below the cut, is written as zero
+        nzs = np.diff(b.node_off)
+        cut = sum(int(np.count_nonzero(_col(sen[0], sen_off, c, int(b.per_off[c + 1] - b.per_off[c]),
+                                            nzs[c])[:, -1] == 0.0)) for c in range(nzs.size))
+        assert cut > 0
     for c in range(0, 16, 6):
         vel, depz, per, K, nz = _column(b, c)
         fine = oracle.depthkernel(vel, depz, per, b.minthk, iwave=ifunc, tol=1e-13, exact=True,
