@@ -24,6 +24,14 @@
  * reference's quotient of the roots at t/(1+h) and t/(1-h)); Lsen_Gsc is
  * Rayleigh phase only.  Other values return DAZI_ERR_BADARG.
  *
+ * Depth cut: the Lsen_Gsc sweep and the adjoint form's Rayleigh
+ * phase-velocity sweep stop at the first layer below which the shear wave
+ * has decayed by exp(-16) (E = sum of nu_b d >= 16, nu_b = sqrt(k^2 -
+ * (omega/Vs)^2)); that layer is the sweep's half-space and the kernels of
+ * the nodes below it are zero (their values are of relative order
+ * exp(-32)).  Love waves, group velocity and the plain form sweep the whole
+ * stack.
+ *
  * Limits (the reference's compiled limits, surfdisp96.f:57-59):
  *   nz <= 200, kmaxRc <= 160, refined layers <= 200.
  *
