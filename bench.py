@@ -983,10 +983,9 @@ def lsmr_block(torch, dev, stream, with_cpu):
                         "note": "marginal time per iteration, (t(ITERS) - t(ITERS/4)) / "
                                 "(3 ITERS / 4), 6 launches per iteration in 16-iteration CUDA "
                                 "graphs; the two CSR copies (143 MB) are about L2's size. The "
-                                "products are bound by their gathers, not by HBM: each lane "
-                                "reads an 8-byte vector entry from its own cache line (the "
-                                "columns of a ray row and the rays of a cell are scattered), "
-                                "about one L1 wavefront per non-zero"}}
+                                "products are bound by load latency, not by HBM: each warp "
+                                "walks its rows one after another (rounds of column and value "
+                                "loads, then their gathers), over uneven rows"}}
     if with_cpu:
         from oracle import lsmr_ref
         t0 = time.perf_counter()
