@@ -8,9 +8,9 @@ interfaces `depthkernel` and `depthkernelTI`.
 from .depthkernel import (depthkernel, depthkernel_vpvsrho, depthkernelTI,  # noqa: F401
                           depthkernel_fused, DepthKernelError)
 from ._lib import (DaziError, FORM_PLAIN, FORM_ADJOINT, FORM_SCAN_FP32,  # noqa: F401
-                   FORM_LOVE, FORM_GROUP, FORM_FAST_ROOT)
+                   FORM_LOVE, FORM_GROUP, FORM_FAST_ROOT, FORM_FULL_STACK)
 
 __all__ = ["depthkernel", "depthkernel_vpvsrho", "depthkernelTI", "depthkernel_fused",
            "DepthKernelError", "DaziError",
            "FORM_PLAIN", "FORM_ADJOINT", "FORM_SCAN_FP32", "FORM_LOVE", "FORM_GROUP",
-           "FORM_FAST_ROOT"]
+           "FORM_FAST_ROOT", "FORM_FULL_STACK"]

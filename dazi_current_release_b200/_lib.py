@@ -30,6 +30,7 @@ FORM_SCAN_FP32 = 2      # flag: FP32 coarse scan verified in FP64 (default: all 
 FORM_LOVE = 4           # flag: Love waves (surfdisp96 iwave = 1), plain or adjoint form
 FORM_GROUP = 8          # flag: group velocity (igr > 0), plain or adjoint form
 FORM_FAST_ROOT = 16     # flag: Brent refinement of the reference's bracket (Rayleigh phase)
+FORM_FULL_STACK = 32    # flag: adjoint and Lsen_Gsc sweeps over the whole stack (no depth cut)
 
 # every symbol include/dazi_dk.h declares
 EXPORTS = (

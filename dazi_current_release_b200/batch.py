@@ -49,7 +49,9 @@ def depthkernel_batch(node_off, depz, vs, per_off, periods, minthk, *, vp=None, 
     """Run the stage on a ragged batch through the host C-ABI entry
     dazi_dk_batch.  form: FORM_PLAIN or FORM_ADJOINT, optionally OR-ed with
     FORM_LOVE / FORM_GROUP (then lsen=False: Lsen_Gsc is a Rayleigh phase
-    kernel) or, for Rayleigh phase velocity, FORM_SCAN_FP32.  Raises
+    kernel) or, for Rayleigh phase velocity, FORM_SCAN_FP32, and
+    FORM_FULL_STACK (the adjoint and Lsen_Gsc sweeps without the depth
+    cut).  Raises
     DaziError for errors; status (per column) holds the first period without
     a root (0 when all have one)."""
     L = _lib.load()

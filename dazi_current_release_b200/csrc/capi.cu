@@ -87,6 +87,8 @@ struct LaunchCfg {
     int root_minb = 0;      // root_kernel blocks per SM of the register budget: 0, 5 (128), 10 (64)
     int adj_minb = 3;       // adjoint_kernel blocks per SM: 2, 3, 4
     int ti_minb = 4;        // ti_kernel blocks per SM: 2, 3, 4, 6, 8
+    bool cut = true;        // depth cut of the Rayleigh phase adjoint and Gc/Gs sweeps
+                            // (off with DAZI_FORM_FULL_STACK)
 };
 
 // Root-search variants (threads per block, register-budget blocks per SM).
@@ -167,7 +169,8 @@ constexpr int kWaveFlags = DAZI_FORM_LOVE | DAZI_FORM_GROUP;
 
 int check_form(int form, bool lsen)
 {
-    constexpr int known = DAZI_FORM_ADJOINT | DAZI_FORM_SCAN_FP32 | kWaveFlags | DAZI_FORM_FAST_ROOT;
+    constexpr int known = DAZI_FORM_ADJOINT | DAZI_FORM_SCAN_FP32 | kWaveFlags | DAZI_FORM_FAST_ROOT |
+                          DAZI_FORM_FULL_STACK;
     if (form & ~known) { set_err("unknown form %d", form); return DAZI_ERR_BADARG; }
     if (form & DAZI_FORM_FAST_ROOT) {
         if (form & kWaveFlags) {
@@ -493,7 +496,7 @@ int run_adjoint(const Tables& T, const double* per, const StageOut& o, long long
     j.sen_vs = o.svs; j.sen_vp = o.svp; j.sen_rho = o.srh;
     j.scratch = W.adjscr.as<double>(); j.scr_layers = maxr > 1 ? maxr - 1 : 1; j.queue = queues;
     j.croot_b = group ? W.crootb.as<double>() : nullptr;
-    if (!love && !group) {
+    if (!love && !group && cfg.cut) {
         // Rayleigh phase velocity: the pairs of each tile by the depth their
         // sweep reaches (adj_order_kernel)
         const long long ntiles = (T.ncols + TILE - 1) / TILE;
@@ -529,6 +532,7 @@ int run_ti(const Tables& T, const double* per, const StageOut& o, long long maxr
     t.scratch = W.tiscr.as<double>(); t.scr_layers = maxr; t.queue = queues + 1;
     t.errflag = reinterpret_cast<int*>(c + 1);
     t.order = W.tiord.as<int>();
+    t.cut = cfg.cut ? 1 : 0;
     const long long ntiles = (T.ncols + TILE - 1) / TILE;
     ti_order_kernel<<<(unsigned)ntiles, TI_ORDER_THREADS, 0, st>>>(t, W.ttbase.as<long long>(),
                                                                  W.ttasks.as<long long>());
@@ -553,14 +557,16 @@ int run_tables(const Tables& T, const double* per, const StageOut& o, int form, 
 {
     int r;
     const bool adj = o.svs && (form & 1) == DAZI_FORM_ADJOINT;
+    LaunchCfg cf = cfg;
+    cf.cut = (form & DAZI_FORM_FULL_STACK) == 0;
     long long maxr = 0;
     if ((r = table_maxr(T, st, maxr))) return r;
     if ((r = ensure_sweep_scratch(T, adj, o.lsen != nullptr, maxr, cfg, W, form_group(form)))) return r;
-    if (!fd_done && (r = run_root(T, per, o, form, adj, W, cfg, st))) return r;
-    if (adj && (r = run_adjoint(T, per, o, maxr, W, cfg, st, form_ifunc(form) == 1, form_group(form))))
+    if (!fd_done && (r = run_root(T, per, o, form, adj, W, cf, st))) return r;
+    if (adj && (r = run_adjoint(T, per, o, maxr, W, cf, st, form_ifunc(form) == 1, form_group(form))))
         return r;
     if (outs_ready) CK(cudaEventRecord(outs_ready, st));
-    if (o.lsen && (r = run_ti(T, per, o, maxr, W, cfg, st))) return r;
+    if (o.lsen && (r = run_ti(T, per, o, maxr, W, cf, st))) return r;
     return 0;
 }
 
@@ -848,6 +854,7 @@ int plan_create(const BatchIn& B, const StageOut& o, int form, bool tune, cudaSt
     P.po = PrepOut{B.sen_off, B.ls_off, P.w.counters.as<unsigned long long>() + 4};
     P.o = o;
     P.form = form;
+    P.cfg.cut = (form & DAZI_FORM_FULL_STACK) == 0;
     P.periods = B.periods;
     P.adj = o.svs != nullptr;
     if ((r = build_tables(P.src, B.ncols, P.po, 1, 1, 1, P.cs, P.T, P.w))) return r;

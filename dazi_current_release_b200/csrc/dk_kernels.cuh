@@ -76,6 +76,7 @@ struct TiArgs {
     int* errflag;           // set to 1 when an Lsen_Gsc value is not finite
     int* order;             // [task * 32 + lane]: (key << 16) | (period * 32 + column lane),
                             // written by ti_order_kernel (key: ti_pair_key)
+    int cut = 1;            // 0: every pair sweeps its whole stack (no depth cut)
 };
 
 // G-row epilogue (k_grows.cu): kernels of the grid interface to sparse

@@ -893,6 +893,7 @@ __device__ __forceinline__ int ti_pair_key(const TiArgs& a, long long t, int lan
     if (k >= M.K) return 0;
     const float cpf = (float)a.pv[M.pv_b + T.pv_sk * k];
     if (!(cpf > 0.0f)) return 1;
+    if (!a.cut) return 1 + M.rmax;
     const double omega = ti_omega(a, M, k);
     const double wvno = omega / (double)cpf;
     return 1 + ti_cut_layers(T.ti + T.tile_lbase[t] + lane, M.rmax, omega, wvno * wvno);

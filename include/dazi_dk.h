@@ -29,8 +29,8 @@
  * has decayed by exp(-16) (E = sum of nu_b d >= 16, nu_b = sqrt(k^2 -
  * (omega/Vs)^2)); that layer is the sweep's half-space and the kernels of
  * the nodes below it are zero (their values are of relative order
- * exp(-32)).  Love waves, group velocity and the plain form sweep the whole
- * stack.
+ * exp(-32)); DAZI_FORM_FULL_STACK turns it off.  Love waves, group
+ * velocity and the plain form's finite differences sweep the whole stack.
  *
  * Limits (the reference's compiled limits, surfdisp96.f:57-59):
  *   nz <= 200, kmaxRc <= 160, refined layers <= 200.
@@ -93,6 +93,12 @@ extern "C" {
  * phase velocity; with DAZI_FORM_LOVE or DAZI_FORM_GROUP it returns
  * DAZI_ERR_BADARG.  The plain form's finite differences ignore it. */
 #define DAZI_FORM_FAST_ROOT 16
+/* flag, OR-ed into the form (adjoint form, Lsen_Gsc, plans): the Lsen_Gsc
+ * sweep and the adjoint form's Rayleigh phase-velocity sweep run over the
+ * whole layer stack, without the depth cut described above (slower; the
+ * kernels below the cut are then their exp(-32)-small values instead of
+ * zero). */
+#define DAZI_FORM_FULL_STACK 32
 
 /* Replaces depthkernel() of code/src_inv_iso_joint/CalSurfG.f90:1-15
  * (default_fortran_fd backend, CalSurfG.f90:86-107), for the 1-based column

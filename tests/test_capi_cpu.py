@@ -87,7 +87,7 @@ def _call_iso(nx=2, ny=2, nz=3, iwave=2, igr=0, K=2, depz=(0.0, 3.0, 6.0), vel=3
     (dict(periods=(5.0, 0.0)), _lib.DAZI_ERR_BADARG),
     (dict(nz=1, depz=(0.0,)), _lib.DAZI_ERR_LIMITS),
     (dict(form=7), _lib.DAZI_ERR_BADARG),
-    (dict(form=32), _lib.DAZI_ERR_BADARG),              # unknown flag
+    (dict(form=64), _lib.DAZI_ERR_BADARG),              # unknown flag
     (dict(iwave=1, form=_lib.FORM_ADJOINT | _lib.FORM_FAST_ROOT), _lib.DAZI_ERR_BADARG),
     (dict(igr=1, form=_lib.FORM_ADJOINT | _lib.FORM_FAST_ROOT), _lib.DAZI_ERR_BADARG),
 ])
