@@ -94,12 +94,13 @@ __device__ __forceinline__ double block_sum(double v, double* sh)
 // block's sum of y_raw^2.  MODE 0: M = A (u step: xs = sv, ys = alpha su);
 // MODE 1: M = A^T (v step: xs = su, ys = beta sv, skipped when beta = 0);
 // MODE 2: the first v = A^T u (ys = 0).
+// Each warp writes its own partial sum of squares (part[warp]), so a warp
+// with fewer or shorter rows does not wait at a block barrier.
 template <int MODE>
 __global__ void __launch_bounds__(kThreads) spmv_kernel(Mat M, const double* __restrict__ x,
                                                         double* __restrict__ y,
                                                         double* __restrict__ part, State* S)
 {
-    __shared__ double sh[kWarps];
     if (S->done) return;
     if (MODE == 1 && !S->beta_pos) return;
     double xs, ys;
@@ -139,18 +140,21 @@ __global__ void __launch_bounds__(kThreads) spmv_kernel(Mat M, const double* __r
             sq += yr * yr;
         }
     }
-    const double s = block_sum(sq, sh);
-    if (threadIdx.x == 0) part[blockIdx.x] = s;
+    if (lane == 0) part[gw] = sq;
 }
 
-// The sum of the kRedBlocks partials by one block of kThreads threads, in a
-// fixed order (thread t adds part[t], part[t + kThreads], ...; then
-// block_sum), so that the result does not depend on the run; valid in
-// thread 0.  Every thread of the block must call it.
-__device__ __forceinline__ double sum_parts(const double* part, double* sh)
+// The sum of n partials by one block of kThreads threads, in a fixed order
+// (thread t adds part[t], part[t + kThreads], ...; then block_sum), so that
+// the result does not depend on the run; valid in thread 0.  Every thread
+// of the block must call it.  n: kRedBlocks (per-block partials of the
+// vector kernels) or kRedWarps (per-warp partials of the products).
+constexpr int kRedWarps = kRedBlocks * kWarps;
+
+__device__ __forceinline__ double sum_parts(const double* part, int n, double* sh)
 {
     double s = 0.0;
-    for (int i = threadIdx.x; i < kRedBlocks; i += kThreads) s += part[i];
+#pragma unroll 8
+    for (int i = threadIdx.x; i < n; i += kThreads) s += part[i];   // loads in flight, adds in order
     return block_sum(s, sh);
 }
 
@@ -196,7 +200,7 @@ __global__ void __launch_bounds__(kThreads) copy_b_kernel(const double* __restri
 __global__ void __launch_bounds__(kThreads) init_beta_kernel(State* S, const double* part)
 {
     __shared__ double sh[kWarps];
-    const double ss = sum_parts(part, sh);
+    const double ss = sum_parts(part, kRedBlocks, sh);
     if (threadIdx.x != 0) return;
     const double beta = sqrt(ss);
     S->beta = beta;
@@ -215,7 +219,7 @@ __global__ void __launch_bounds__(kThreads) init_beta_kernel(State* S, const dou
 __global__ void __launch_bounds__(kThreads) init_alpha_kernel(State* S, const double* part)
 {
     __shared__ double sh[kWarps];
-    const double ss = sum_parts(part, sh);   // stale partials when beta = 0: not used
+    const double ss = sum_parts(part, kRedWarps, sh);   // stale partials when beta = 0: not used
     if (threadIdx.x != 0) return;
     const double alpha = S->beta_pos ? sqrt(ss) : 0.0;
     S->alpha = alpha;
@@ -252,7 +256,7 @@ __global__ void __launch_bounds__(kThreads) beta_kernel(State* S, const double* 
 {
     __shared__ double sh[kWarps];
     if (S->done) return;   // read by every thread before thread 0 writes anything
-    const double ss = sum_parts(part, sh);
+    const double ss = sum_parts(part, kRedWarps, sh);
     if (threadIdx.x != 0) return;
     S->itn += 1;
     const double beta = sqrt(ss);
@@ -267,7 +271,7 @@ __global__ void __launch_bounds__(kThreads) rotate_kernel(State* S, const double
 {
     __shared__ double sh[kWarps];
     if (S->done) return;
-    const double ss = sum_parts(part, sh);   // stale partials when beta = 0: not used
+    const double ss = sum_parts(part, kRedWarps, sh);   // stale partials when beta = 0: not used
     if (threadIdx.x != 0) return;
     State& T = *S;
     if (T.beta_pos) {
@@ -357,7 +361,7 @@ __global__ void __launch_bounds__(kThreads) test_kernel(State* S, const double* 
 {
     __shared__ double sh[kWarps];
     if (S->done) return;
-    const double ss = sum_parts(part, sh);
+    const double ss = sum_parts(part, kRedBlocks, sh);
     if (threadIdx.x != 0) return;
     State& T = *S;
     T.normx = sqrt(ss);
@@ -535,11 +539,11 @@ extern "C" int dazi_lsmr_dev(int m, int n, long long nnz, const int* row, const 
     Buf u, v, h, hbar, part, sbuf;
     if ((r = alloc(u, sizeof(double) * m)) || (r = alloc(v, sizeof(double) * n)) ||
         (r = alloc(h, sizeof(double) * n)) || (r = alloc(hbar, sizeof(double) * n)) ||
-        (r = alloc(part, sizeof(double) * kRedBlocks * 3)) || (r = alloc(sbuf, sizeof(State))))
+        (r = alloc(part, sizeof(double) * kRedWarps * 3)) || (r = alloc(sbuf, sizeof(State))))
         return r;
     double* p0 = part.as<double>();
-    double* p1 = p0 + kRedBlocks;
-    double* p2 = p1 + kRedBlocks;
+    double* p1 = p0 + kRedWarps;
+    double* p2 = p1 + kRedWarps;
     State hs{};
     hs.damp = damp; hs.atol = atol; hs.btol = btol; hs.itnlim = itnlim;
     hs.ctol = conlim > 0.0 ? 1.0 / conlim : 0.0;
