@@ -562,10 +562,15 @@ extern "C" int dazi_lsmr_dev(int m, int n, long long nnz, const int* row, const 
     LK(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaGraph_t g = nullptr;
     cudaGraphExec_t ge = nullptr;
+    int* hdone = nullptr;                  // pinned: the stop flag after two chunks in turn
+    cudaEvent_t ev[2] = {nullptr, nullptr};
     auto cleanup = [&]() {
         if (ge) cudaGraphExecDestroy(ge);
         if (g) cudaGraphDestroy(g);
         cudaStreamDestroy(cs);
+        if (hdone) cudaFreeHost(hdone);
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
     };
     if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
         cudaGetLastError();
@@ -589,19 +594,40 @@ extern "C" int dazi_lsmr_dev(int m, int n, long long nnz, const int* row, const 
         dk::set_last_error("LSMR: graph capture failed");
         return DAZI_ERR_CUDA;
     }
-    // the graph runs on the caller's stream, in order with the set-up
-    int done = 0;
+    if (cudaHostAlloc((void**)&hdone, 2 * sizeof(int), cudaHostAllocDefault) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev[0], cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&ev[1], cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        cleanup();
+        dk::set_last_error("LSMR: host flag allocation failed");
+        return DAZI_ERR_CUDA;
+    }
+    // The graph runs on the caller's stream, in order with the set-up.  One
+    // chunk runs ahead of the host's check of the stop flag: chunk c + 1 is
+    // queued before the host waits for chunk c's flag, so the device does
+    // not idle while the host reads it (a chunk queued after the stop does
+    // nothing: every kernel returns once the solve is done).
     const int chunks = itnlim / kChunk + 2;
     int rc = 0;
-    for (int c = 0; c < chunks && !done; ++c) {
-        if (cudaGraphLaunch(ge, st) != cudaSuccess ||
-            cudaMemcpyAsync(&done, &S->done, sizeof(int), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
-            cudaStreamSynchronize(st) != cudaSuccess) {
-            cudaGetLastError();
-            dk::set_last_error("LSMR: iteration launch failed");
-            rc = DAZI_ERR_CUDA;
-            break;
-        }
+    auto issue = [&](int c) {
+        return cudaGraphLaunch(ge, st) == cudaSuccess &&
+               cudaMemcpyAsync(&hdone[c & 1], &S->done, sizeof(int), cudaMemcpyDeviceToHost, st) ==
+                   cudaSuccess &&
+               cudaEventRecord(ev[c & 1], st) == cudaSuccess;
+    };
+    if (!issue(0)) rc = DAZI_ERR_CUDA;
+    for (int c = 0; c < chunks && !rc; ++c) {
+        if (c + 1 < chunks && !issue(c + 1)) { rc = DAZI_ERR_CUDA; break; }
+        if (cudaEventSynchronize(ev[c & 1]) != cudaSuccess) { rc = DAZI_ERR_CUDA; break; }
+        if (hdone[c & 1]) break;
+    }
+    // every queued chunk finishes before the graph, the flags and the
+    // buffers go
+    const cudaError_t se = cudaStreamSynchronize(st);
+    if (rc || se != cudaSuccess) {
+        cudaGetLastError();
+        dk::set_last_error("LSMR: iteration launch failed");
+        rc = DAZI_ERR_CUDA;
     }
     cleanup();
     if (rc) return rc;

@@ -326,8 +326,9 @@ int dazi_lsmr(const int *m, const int *n, const long long *leniw,
 /* Device-pointer form: nnz triplets (row, col, val) with 0- or 1-based
  * indices (index_base), b (m) and x (n) real*8 in device memory;
  * norms[0..4] (host, may be NULL) = normA, condA, normr, normAr, normx.
- * Stream-ordered on `stream`; the host waits once per 16 iterations to
- * read the stop flag, and returns when the solve has finished. */
+ * Stream-ordered on `stream`; the host reads the stop flag once per 16
+ * iterations (with the next 16 already queued), and returns when the solve
+ * has finished. */
 int dazi_lsmr_dev(int m, int n, long long nnz, const int *row, const int *col,
                   const float *val, int index_base, const double *b,
                   double damp, double atol, double btol, double conlim,
