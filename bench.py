@@ -93,6 +93,8 @@ def parse():
                    help="skip the traveltime-solver measurement (fmm block)")
     p.add_argument("--no-lsmr", action="store_true",
                    help="skip the LSMR solver measurement (lsmr block)")
+    p.add_argument("--full-stack", action="store_true",
+                   help="adjoint and Gc/Gs sweeps over the whole layer stack (no depth cut)")
     return p.parse_args()
 
 
@@ -309,6 +311,7 @@ def ragged_config(args, b):
             "mean_layers": float(nz.mean() - 1), "periods_per_column": [int(K.min()), int(K.max())],
             "mean_periods": float(K.mean()), "minthk": b.minthk,
             "parallelism": "columns, one batch per GPU",
+            "depth_cut": not getattr(args, "full_stack", False),
             "l2": "inputs and outputs far larger than L2; 256 MiB flush write between steps "
                   "outside the timed events"}
 
@@ -477,6 +480,8 @@ def main_ragged(args, ws, rank, local):
     fast = form == _lib.FORM_ADJOINT and args.root == "brent"
     if fast:
         form |= _lib.FORM_FAST_ROOT
+    if args.full_stack:
+        form |= _lib.FORM_FULL_STACK
     T = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)  # noqa: E731
     d_node, d_per, d_dep, d_vs = T(b.node_off), T(b.per_off), T(b.depz), T(b.vs)
     d_periods, d_senoff, d_lsoff = T(b.periods), T(sen_off), T(ls_off)
@@ -534,7 +539,8 @@ def main_ragged(args, ws, rank, local):
         from dazi_current_release_b200.plan import BatchPlan
         t0 = time.perf_counter()
         plan = BatchPlan(b.node_off, b.depz, b.vs, b.per_off, b.periods, b.minthk, tune=True,
-                         scan32=bool(form & _lib.FORM_SCAN_FP32), fast_root=fast, device=dev)
+                         scan32=bool(form & _lib.FORM_SCAN_FP32), fast_root=fast,
+                         full_stack=args.full_stack, device=dev)
         plan_setup_s = time.perf_counter() - t0
         with ClockSampler(local) as clk:
             ms_per_step = _events_timed(plan.run, args.steps, args.warmup, dev, stream, flush, ws)

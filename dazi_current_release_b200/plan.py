@@ -8,7 +8,9 @@ times as one CUDA-graph launch (dazi_dk_plan_* in include/dazi_dk.h).
 The structure (node depths, periods) is fixed at creation; the velocities
 may change between runs (write into p.vs).  The autotuner's choice is in
 p.config().  fast_root=True refines each period's bracket by Brent's method
-(DAZI_FORM_FAST_ROOT) instead of the reference's nevill().
+(DAZI_FORM_FAST_ROOT) instead of the reference's nevill(); full_stack=True
+runs the adjoint and Gc/Gs sweeps without the depth cut
+(DAZI_FORM_FULL_STACK).
 """
 from __future__ import annotations
 
@@ -24,7 +26,7 @@ from .batch import output_offsets
 class BatchPlan:
     def __init__(self, node_off, depz, vs, per_off, periods, minthk, *, vp=None, rho=None,
                  kernels=True, lsen=True, tune=True, scan32=False, fast_root=False,
-                 device="cuda"):
+                 full_stack=False, device="cuda"):
         dev = torch.device(device)
         self.L = _lib.load()
         t = lambda a, dt: torch.as_tensor(np.ascontiguousarray(a), dtype=dt, device=dev)  # noqa: E731
@@ -48,7 +50,8 @@ class BatchPlan:
         self.status = z(self.ncols, torch.int32)
         P = lambda x: None if x is None else ctypes.c_void_p(x.data_ptr())  # noqa: E731
         form = (_lib.FORM_ADJOINT | (_lib.FORM_SCAN_FP32 if scan32 else 0) |
-                (_lib.FORM_FAST_ROOT if fast_root else 0))
+                (_lib.FORM_FAST_ROOT if fast_root else 0) |
+                (_lib.FORM_FULL_STACK if full_stack else 0))
         h = ctypes.c_void_p(None)
         stream = torch.cuda.current_stream(dev).cuda_stream
         rc = self.L.dazi_dk_plan_create(
