@@ -986,9 +986,12 @@ def lsmr_block(torch, dev, stream, with_cpu):
            "part_ms_runs": part,
            "e2e": {"value": ITERS / (e2e_ms * 1e-3), "unit": "iterations/s", "ms": e2e_ms,
                    "h2d_bytes": int(iw.nbytes + val.nbytes + b.nbytes), "d2h_bytes": int(8 * n)},
-           "roofline": {"bound": "hbm", "achieved": it_bytes / (it_ms * 1e-3) / 1e9,
+           "roofline": {"bound": "hbm", "achieved": it_bytes / (it_ms_best * 1e-3) / 1e9,
                         "peak": peak, "unit": "GB/s",
-                        "frac": it_bytes / (it_ms * 1e-3) / 1e9 / peak,
+                        "frac": it_bytes / (it_ms_best * 1e-3) / 1e9 / peak,
+                        "time": "ms_per_iteration_best_runs (each call also allocates its "
+                                "buffers and builds its CSR copies on the host's schedule, so "
+                                "busy hosts spread the medians)",
                         "bytes_per_iteration": it_bytes, "peak_source": peak_src,
                         "note": "marginal time per iteration, (t(ITERS) - t(ITERS/4)) / "
                                 "(3 ITERS / 4), 6 launches per iteration in 16-iteration CUDA "
