@@ -1464,6 +1464,7 @@ int dazi_dk_version(void) { return 100; }
 
 void dazi_dk_finalize(void)
 {
+    lsmr_release();
     std::lock_guard<std::mutex> lk(g_mu);
     if (!g_ctx.ready) return;
     DBuf* all[] = {&g_ctx.vel, &g_ctx.vp, &g_ctx.rho, &g_ctx.per, &g_ctx.depz, &g_ctx.pv,

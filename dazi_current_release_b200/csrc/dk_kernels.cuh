@@ -180,6 +180,9 @@ template <int MINB> __global__ void ti_kernel(TiArgs a);          // MINB in {2,
 // ti_kernel's tasks (a.order), by the depth at which each pair's sweep stops.
 __global__ void ti_order_kernel(TiArgs a, const long long* tile_tbase, const long long* tile_tasks);
 __global__ void adj_order_kernel(AdjArgs a, int* order, const long long* tile_tbase, const long long* tile_tasks);
+
+// Gives back the LSMR entries' device memory pools (k_lsmr.cu).
+void lsmr_release();
 constexpr int TI_ORDER_THREADS = 256;
 
 __global__ void geometry_kernel(const float* depz, int nz, float minthk, Geometry* g);

@@ -35,13 +35,54 @@
 #include <cuda_runtime.h>
 #include <cub/cub.cuh>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
+#include <mutex>
 #include <vector>
 
 #include "../../include/dazi_dk.h"
 
 namespace dk {
 void set_last_error(const char* msg);
+
+// Device memory of the LSMR entries comes from a private stream-ordered
+// pool per device that keeps what it has been given between calls, so
+// repeated solves of similar sizes take nothing from the driver after the
+// first; dazi_dk_finalize gives it back (lsmr_release).
+static std::mutex g_pool_mu;
+static cudaMemPool_t g_pools[64] = {};
+
+cudaMemPool_t lsmr_pool(int dev)
+{
+    if (dev < 0 || dev >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    if (!g_pools[dev]) {
+        cudaMemPoolProps props = {};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.handleTypes = cudaMemHandleTypeNone;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = dev;
+        cudaMemPool_t p = nullptr;
+        if (cudaMemPoolCreate(&p, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = UINT64_MAX;
+        cudaMemPoolSetAttribute(p, cudaMemPoolAttrReleaseThreshold, &keep);
+        g_pools[dev] = p;
+    }
+    return g_pools[dev];
+}
+
+void lsmr_release()
+{
+    std::lock_guard<std::mutex> lk(g_pool_mu);
+    for (cudaMemPool_t& p : g_pools)
+        if (p) {
+            cudaMemPoolDestroy(p);   // released once its outstanding allocations are freed
+            p = nullptr;
+        }
+}
 }
 
 namespace {
@@ -419,20 +460,26 @@ __global__ void ptr_kernel(const int* __restrict__ skeys, long long nnz, int nro
     }
 }
 
+// A pool allocation, freed in stream order on the stream it was made on
+// (after every kernel queued there that uses it).
 struct Buf {
     void* p = nullptr;
-    ~Buf() { if (p) cudaFree(p); }
+    cudaStream_t s = nullptr;
+    ~Buf() { if (p) cudaFreeAsync(p, s); }
     template <class T> T* as() { return (T*)p; }
 };
 
-int alloc(Buf& b, size_t bytes)
+int alloc(Buf& b, size_t bytes, cudaStream_t st)
 {
-    if (cudaMalloc(&b.p, bytes ? bytes : 16) != cudaSuccess) {
+    int dev = 0;
+    cudaMemPool_t pool = cudaGetDevice(&dev) == cudaSuccess ? dk::lsmr_pool(dev) : nullptr;
+    if (!pool || cudaMallocFromPoolAsync(&b.p, bytes ? bytes : 16, pool, st) != cudaSuccess) {
         b.p = nullptr;
         cudaGetLastError();
         dk::set_last_error("LSMR: device allocation failed");
         return DAZI_ERR_NOMEM;
     }
+    b.s = st;
     return 0;
 }
 
@@ -456,10 +503,10 @@ int build_csr(const int* key, const int* other, const float* val, int base, long
 {
     int r;
     Buf keys, skeys, ord, sord, bad, tmp;
-    if ((r = alloc(keys, sizeof(int) * nnz)) || (r = alloc(skeys, sizeof(int) * nnz)) ||
-        (r = alloc(ord, sizeof(int) * nnz)) || (r = alloc(sord, sizeof(int) * nnz)) ||
-        (r = alloc(bad, sizeof(int))) || (r = alloc(ptr, sizeof(long long) * (nrows + 1))) ||
-        (r = alloc(idx, sizeof(int) * nnz)) || (r = alloc(v, sizeof(float) * nnz)))
+    if ((r = alloc(keys, sizeof(int) * nnz, st)) || (r = alloc(skeys, sizeof(int) * nnz, st)) ||
+        (r = alloc(ord, sizeof(int) * nnz, st)) || (r = alloc(sord, sizeof(int) * nnz, st)) ||
+        (r = alloc(bad, sizeof(int), st)) || (r = alloc(ptr, sizeof(long long) * (nrows + 1), st)) ||
+        (r = alloc(idx, sizeof(int) * nnz, st)) || (r = alloc(v, sizeof(float) * nnz, st)))
         return r;
     LK(cudaMemsetAsync(bad.p, 0, sizeof(int), st));
     const int nb = 148 * 8;
@@ -481,7 +528,7 @@ int build_csr(const int* key, const int* other, const float* val, int base, long
     size_t tb = 0;
     LK(cub::DeviceRadixSort::SortPairs(nullptr, tb, keys.as<int>(), skeys.as<int>(), ord.as<int>(),
                                        sord.as<int>(), (int)nnz, 0, bits, st));
-    if ((r = alloc(tmp, tb))) return r;
+    if ((r = alloc(tmp, tb, st))) return r;
     LK(cub::DeviceRadixSort::SortPairs(tmp.p, tb, keys.as<int>(), skeys.as<int>(), ord.as<int>(),
                                        sord.as<int>(), (int)nnz, 0, bits, st));
     gather_kernel<<<nb, 256, 0, st>>>(sord.as<int>(), other, base, val, nnz, idx.as<int>(),
@@ -537,9 +584,9 @@ extern "C" int dazi_lsmr_dev(int m, int n, long long nnz, const int* row, const 
     const Mat A{aptr.as<long long>(), aidx.as<int>(), aval.as<float>(), m};
     const Mat At{tptr.as<long long>(), tidx.as<int>(), tval.as<float>(), n};
     Buf u, v, h, hbar, part, sbuf;
-    if ((r = alloc(u, sizeof(double) * m)) || (r = alloc(v, sizeof(double) * n)) ||
-        (r = alloc(h, sizeof(double) * n)) || (r = alloc(hbar, sizeof(double) * n)) ||
-        (r = alloc(part, sizeof(double) * kRedWarps * 3)) || (r = alloc(sbuf, sizeof(State))))
+    if ((r = alloc(u, sizeof(double) * m, st)) || (r = alloc(v, sizeof(double) * n, st)) ||
+        (r = alloc(h, sizeof(double) * n, st)) || (r = alloc(hbar, sizeof(double) * n, st)) ||
+        (r = alloc(part, sizeof(double) * kRedWarps * 3, st)) || (r = alloc(sbuf, sizeof(State), st)))
         return r;
     double* p0 = part.as<double>();
     double* p1 = p0 + kRedWarps;
@@ -668,12 +715,12 @@ extern "C" int dazi_lsmr(const int* m, const int* n, const long long* leniw, con
         dk::set_last_error("no CUDA device");
         return DAZI_ERR_NODEVICE;
     }
-    Buf dr, dc, dv, db, dx;
-    if ((r = alloc(dr, sizeof(int) * nnz)) || (r = alloc(dc, sizeof(int) * nnz)) ||
-        (r = alloc(dv, sizeof(float) * nnz)) || (r = alloc(db, sizeof(double) * *m)) ||
-        (r = alloc(dx, sizeof(double) * *n)))
-        return r;
     cudaStream_t st = nullptr;
+    Buf dr, dc, dv, db, dx;
+    if ((r = alloc(dr, sizeof(int) * nnz, st)) || (r = alloc(dc, sizeof(int) * nnz, st)) ||
+        (r = alloc(dv, sizeof(float) * nnz, st)) || (r = alloc(db, sizeof(double) * *m, st)) ||
+        (r = alloc(dx, sizeof(double) * *n, st)))
+        return r;
     LK(cudaMemcpyAsync(dr.p, iw, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
     LK(cudaMemcpyAsync(dc.p, iw + nnz, sizeof(int) * nnz, cudaMemcpyHostToDevice, st));
     LK(cudaMemcpyAsync(dv.p, rw, sizeof(float) * nnz, cudaMemcpyHostToDevice, st));

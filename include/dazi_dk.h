@@ -328,7 +328,8 @@ int dazi_lsmr(const int *m, const int *n, const long long *leniw,
  * norms[0..4] (host, may be NULL) = normA, condA, normr, normAr, normx.
  * Stream-ordered on `stream`; the host reads the stop flag once per 16
  * iterations (with the next 16 already queued), and returns when the solve
- * has finished. */
+ * has finished.  Device memory comes from a private pool per device that
+ * keeps it between calls; dazi_dk_finalize gives it back. */
 int dazi_lsmr_dev(int m, int n, long long nnz, const int *row, const int *col,
                   const float *val, int index_base, const double *b,
                   double damp, double atol, double btol, double conlim,
